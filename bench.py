@@ -1,0 +1,375 @@
+"""Benchmark of the SLIC/FORCE hot path on B200 (one JSON line on rank 0).
+
+Workload (one "step" = one full split time step X(dt/2) Y(dt) X(dt/2) over the whole grid):
+  2D Euler SLIC, 4096 x 4096 cells on [0,1]^2, gamma = 1.4, transmissive boundaries, four-quadrant
+  Riemann initial data drawn from a seed (rho ~ U[0.1,2], u,v ~ U[-1,1], p ~ U[0.1,2]), superbee,
+  CFL 0.8, dt computed on the device every step.  Inputs are larger than L2 (the FP64 state is 537 MB)
+  so no L2 flush is needed between steps.
+
+Arms:
+  default              the CUDA path through the C ABI (libvanguard_slic.so); value = device-timed
+                       cell-updates/s with the state resident in HBM; e2e = the same metric through
+                       vg_solve() from pinned host buffers with H2D/D2H inside the timed region.
+  --impl reference     the reference's own OpenMP C++ code (compiled unmodified into oracle/_ref) on
+                       the host cores, on a bounded sample (a strip of the same grid) per step.
+
+Multi-GPU (torchrun, N > 1): the path has no exchange step, so every rank runs an independent replica of
+the workload; value = all ranks' cell-updates / the slowest rank's time ("scaling": "weak").
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-updates/s: mixed vs plain FP64 on GPU at ≤1e-6 L1 err; adjoint/fwd cost"
+UNIT = "cell-updates/s"
+NX = NY = 4096
+CFL = 0.8
+LIMITER = 0  # superbee
+SEED = 2024
+BYTES_PER_CELL_SWEEP = 2 * 4 * 8      # read + write of rho, rho u, rho v, E in FP64
+BYTES_PER_CELL_UPDATE = 3 * BYTES_PER_CELL_SWEEP  # 192 B: three sweeps per step
+
+
+def workload_config():
+    return {
+        "workload": "2D Euler SLIC 4096x4096, four-quadrant Riemann (seeded), gamma 1.4, superbee, CFL 0.8, transmissive",
+        "nx": NX, "ny": NY, "limiter": "superbee", "cfl": CFL, "seed": SEED,
+        "l2": "inputs larger than L2 (FP64 state 537 MB), no flush",
+        "parallelism": "replicas",
+    }
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi sampling during the timed region (SM clock, throttle reasons)."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                out = ""
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        mhz, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                mhz.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(mhz)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+# ----------------------------------------------------------------------------------------- reference arm
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return 0
+    import oracle as O
+    from vanguard_b200 import workloads as wl
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libvgref.so was not built"}))
+        return 0
+    cores = O.ref().vgref_set_threads(0)
+    prm = wl.euler_params(1.4)
+    full = wl.euler_quadrants_2d(NX, NY, seed=SEED)
+    # per-step cost on a thin strip of the same grid, then size the sample so the whole run ends in ~2 min
+    probe_rows = 16
+    strip = np.ascontiguousarray(full[:, NY // 2 - probe_rows // 2: NY // 2 + probe_rows // 2, :])
+    t0 = time.perf_counter()
+    O.ref_run(O.EULER, strip.copy(), 1.0 / NX, CFL, steps=1, limiter=LIMITER, params=prm, threads=cores)
+    per_cell = (time.perf_counter() - t0) / (NX * probe_rows)
+    budget = 120.0 / max(1, args.steps + args.warmup)
+    rows = int(max(16, min(NY, budget / max(per_cell * NX, 1e-12))))
+    rows -= rows % 2
+    sample = np.ascontiguousarray(full[:, NY // 2 - rows // 2: NY // 2 + rows // 2, :])
+    for _ in range(args.warmup):
+        O.ref_run(O.EULER, sample.copy(), 1.0 / NX, CFL, steps=1, limiter=LIMITER, params=prm, threads=cores)
+    times = []
+    state = sample.copy()
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        O.ref_run(O.EULER, state, 1.0 / NX, CFL, steps=1, limiter=LIMITER, params=prm, threads=cores)
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = NX * rows * args.steps / total
+    desc = (f"reference SecondOrderSolver per-step loop (oracle/_ref, OpenMP {cores} threads) on a {NX}x{rows} "
+            f"strip through the centre of the 4096x4096 grid, {args.steps} steps")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000.0 * total / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload_config(),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": desc},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def cpu_baseline_sample():
+    """The reference on the host cores for ~10-30 s on a strip of the workload (rank 0, N = 1)."""
+    import oracle as O
+    from vanguard_b200 import workloads as wl
+    if not O.ref_available():
+        return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": "oracle/_ref not built"}
+    cores = O.ref().vgref_set_threads(0)
+    prm = wl.euler_params(1.4)
+    full = wl.euler_quadrants_2d(NX, NY, seed=SEED)
+    probe_rows = 16
+    strip = np.ascontiguousarray(full[:, NY // 2 - 8: NY // 2 + 8, :])
+    t0 = time.perf_counter()
+    O.ref_run(O.EULER, strip.copy(), 1.0 / NX, CFL, steps=1, limiter=LIMITER, params=prm, threads=cores)
+    per_cell = (time.perf_counter() - t0) / (NX * probe_rows)
+    steps = 2
+    rows = int(max(16, min(NY, 15.0 / max(per_cell * NX * steps, 1e-12))))
+    rows -= rows % 2
+    sample = np.ascontiguousarray(full[:, NY // 2 - rows // 2: NY // 2 + rows // 2, :])
+    t0 = time.perf_counter()
+    O.ref_run(O.EULER, sample, 1.0 / NX, CFL, steps=steps, limiter=LIMITER, params=prm, threads=cores)
+    dt = time.perf_counter() - t0
+    return {"value": NX * rows * steps / dt, "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": f"{steps} steps of the reference per-step loop on a {NX}x{rows} strip of the workload "
+                      f"({dt:.1f} s, OpenMP {cores} threads)"}
+
+
+# ---------------------------------------------------------------------------------------------- CUDA arm
+
+def run_cuda(args, world, rank, local):
+    import torch
+    import vanguard_b200 as vg
+    from vanguard_b200 import workloads as wl
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    prm = wl.euler_params(1.4)
+    W0 = wl.euler_quadrants_2d(NX, NY, seed=SEED + rank)
+    stream = torch.cuda.current_stream()
+    sh = ctypes_stream(stream)
+    dx = 1.0 / NX
+
+    results = {}
+    forms = [("fp64", vg.FP64)]
+    if vg_mixed_available(vg):
+        forms.append(("mixed", vg.MIXED))
+    finals = {}
+    for name, prec in forms:
+        s = vg.Solver(vg.EULER, NX, NY, prm, precision=prec, device=local)
+        s.upload(W0, stream=sh)
+        # warm-up (also captures the step graphs)
+        s.run(dx, CFL, steps=max(args.warmup, 3), limiter=LIMITER, stream=sh)
+        s.upload(W0, stream=sh)
+        barrier()
+        torch.cuda.synchronize()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local) as clk:
+            start.record(stream)
+            _, steps = s.run(dx, CFL, steps=args.steps, limiter=LIMITER, stream=sh, allow_nan=True)
+            end.record(stream)
+            torch.cuda.synchronize()
+        barrier()
+        ms = start.elapsed_time(end)
+        ms = max_over_ranks(ms)
+        launches = s.last_launch_count()
+        finals[name] = s.download(stream=sh)
+
+        # dominant kernel: an X half-sweep, timed alone (CUDA events on the launching stream)
+        reps = max(5, min(args.steps, 20))
+        s.sweep(0, dx, 1e-5, limiter=LIMITER, stream=sh)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            s.sweep(0, dx, 1e-5, limiter=LIMITER, stream=sh)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        xs_ms = e0.elapsed_time(e1) / reps
+        e0.record(stream)
+        for _ in range(reps):
+            s.sweep(1, dx, 1e-5, limiter=LIMITER, stream=sh)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ys_ms = e0.elapsed_time(e1) / reps
+        results[name] = {"ms": ms, "steps": steps, "launches": launches, "clocks": clk.summary(),
+                         "x_sweep_ms": xs_ms, "y_sweep_ms": ys_ms}
+        s.close()
+
+    # end-to-end through the host-buffer API (vg_solve: upload + run + download inside the timed region)
+    best = "mixed" if "mixed" in results and mixed_ok(finals) else "fp64"
+    prec = vg.MIXED if best == "mixed" else vg.FP64
+    hin = torch.from_numpy(W0).pin_memory()
+    hout = torch.empty_like(hin).pin_memory()
+    s = vg.Solver(vg.EULER, NX, NY, prm, precision=prec, device=local)
+    s.solve(hin.numpy(), dx, CFL, steps=2, limiter=LIMITER, out=hout.numpy(), stream=sh)
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s.solve(hin.numpy(), dx, CFL, steps=args.steps, limiter=LIMITER, out=hout.numpy(), stream=sh)
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    s.close()
+    carried = 4  # rho, u, v, p cross the bus; w and lambda are validated on the host and not copied
+    h2d = carried * NX * NY * 8
+    d2h = carried * NX * NY * 8
+
+    r = results[best]
+    cells = NX * NY
+    value = world * cells * args.steps / (r["ms"] / 1000.0)
+    peak, peak_kind = measured_peak()
+    x_bytes = cells * BYTES_PER_CELL_SWEEP
+    achieved = x_bytes / (r["x_sweep_ms"] / 1000.0) / 1e9
+    traffic = load_traffic()
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": r["ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if best == "fp64" else "f32+f64", "data": "synthetic",
+        "config": dict(workload_config(), form=best),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "kernel": "sweep_x_kernel (X half-sweep)",
+                     "algorithmic_bytes_per_launch": x_bytes, "peak_source": peak_kind},
+        "e2e": {"value": world * cells * args.steps / e2e_s, "unit": UNIT,
+                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+                "api": "vg_solve (pinned host buffers; one upload + K steps + one download per call)"},
+        "gpu_launches": r["launches"],
+        "clocks": r["clocks"],
+        "forms": {k: {"cell_updates_per_s": world * cells * args.steps / (v["ms"] / 1000.0),
+                      "ms_per_step": v["ms"] / args.steps, "x_sweep_ms": v["x_sweep_ms"],
+                      "y_sweep_ms": v["y_sweep_ms"],
+                      "hbm_frac_of_step": world * cells * args.steps * BYTES_PER_CELL_UPDATE / (v["ms"] / 1000.0) / 1e9 / peak}
+                  for k, v in results.items()},
+    }
+    if "mixed" in finals:
+        d = np.abs(finals["mixed"][0] - finals["fp64"][0])
+        line["mixed_error_vs_fp64"] = {"rho_L1": float(d.mean()), "rho_Linf": float(d.max()),
+                                       "reference": "the FP64 CUDA form, bitwise equal to the oracle"}
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_sample()
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def ctypes_stream(stream):
+    import ctypes
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+def vg_mixed_available(vg):
+    try:
+        s = vg.Solver(vg.EULER, 8, 8, (1.4, 0.0), precision=vg.MIXED)
+        s.close()
+        return True
+    except Exception:
+        return False
+
+
+def mixed_ok(finals):
+    if "mixed" not in finals:
+        return False
+    return float(np.abs(finals["mixed"][0] - finals["fp64"][0]).mean()) <= 1e-6
+
+
+def load_traffic():
+    """DRAM bytes per X-sweep launch from the committed ncu summary, if present."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f).get("sweep_x_kernel_fp64_bytes_per_launch")
+    except Exception:
+        return None
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        return run_reference(args, world, rank)
+    return run_cuda(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,136 @@
+/* vanguard_slic.h -- C ABI of the B200-native SLIC/FORCE finite-volume update.
+ *
+ * This is the drop-in boundary for Vanguard's single-material second-order solvers.  The reference
+ * has no C ABI (its interface is static C++ methods, see each entry point below); callers reach this
+ * ABI through the C++ shim in vanguard_b200/shim (same class names and signatures as the reference)
+ * or directly through ctypes / any FFI.  No C++ or torch types cross this boundary: plain pointers,
+ * sizes and status codes, no exceptions.
+ *
+ * Data layout at the boundary: structure-of-arrays PRIMITIVE planes, float64, in the reference's
+ * primitive order, row-major (index = row * nx + column; X runs along the column index j, Y along
+ * the row index i -- the reference's currentCells[i][j]):
+ *   VG_MODEL_EULER (6 planes): rho, u, v, w, p, lambda           Euler/eulerstatevector.cpp:36-45
+ *   VG_MODEL_MHD   (9 planes): rho, u, v, w, p, Bx, By, Bz, psi  MHD/mhdstatevector.cpp:35-47
+ *   VG_MODEL_HPR  (17 planes): rho, p, A(9, row-major), u, v, w, Jx, Jy, Jz
+ *                                                                HPR/hprstatevector.cpp:50-73
+ * Ownership: a vg_solver owns all device memory it allocates; the caller owns every host buffer.
+ * Threading: calls on different solvers are independent and re-entrant; one solver must not be used
+ * from two host threads at once.  All work is enqueued on the stream given (NULL: the legacy default
+ * stream) and the call returns after that stream has finished unless a function says otherwise.
+ */
+#ifndef VANGUARD_SLIC_H
+#define VANGUARD_SLIC_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum vg_status {
+    VG_OK = 0,
+    VG_EINVAL = 1,       /* bad argument: null pointer, size, model, limiter, plane count */
+    VG_ENAN = 2,         /* the run produced a non-finite value or non-positive density/pressure */
+    VG_ETIMEOUT = 3,     /* a bounded device-side wait gave up (persistent kernels) */
+    VG_ECUDA = 4,        /* a CUDA runtime call failed; vg_last_error_string() has the text */
+    VG_ENOMEM = 5,       /* device allocation failed */
+    VG_EUNSUPPORTED = 6  /* the input needs a variant this build does not provide (see below) */
+} vg_status;
+
+typedef enum vg_model { VG_MODEL_EULER = 0, VG_MODEL_MHD = 1, VG_MODEL_HPR = 2 } vg_model;
+
+/* VG_FP64: every operation in float64, in the reference's order, no FMA: matches the reference.
+ * VG_MIXED: reconstruction, half-step evolution and FORCE flux in float32; pressure recovery, the CFL
+ * reduction, source integration and the cell-update accumulation in float64. */
+typedef enum vg_precision { VG_FP64 = 0, VG_MIXED = 1 } vg_precision;
+
+/* VG_TRANSMISSIVE: the reference's mirror ghosts g[-1] = c[0], g[-2] = c[1] (Solvers/solvers.cpp:17-23).
+ * VG_PERIODIC: wrap-around ghosts (the reference has none; its corner blocks stay default states). */
+typedef enum vg_boundary { VG_TRANSMISSIVE = 0, VG_PERIODIC = 1 } vg_boundary;
+
+/* SlopeLimiters::computeSlopeLimiter ids (Solvers/slopelimiters.cpp:60-74): 0 superbee, 1 van Leer,
+ * any other value minbee. */
+enum { VG_SUPERBEE = 0, VG_VANLEER = 1, VG_MINBEE = 2 };
+
+#define VG_MAX_PARAMS 16
+
+/* Material parameter blocks (params[] below):
+ *   Euler: {gamma, p_inf, c_v, E0, T_ign, rate}   EulerMaterialParameters (Euler/eulermaterialparameters.h)
+ *   MHD:   {gamma, p_inf, c_h}                    MHDMaterialParameters; c_h is recomputed every step by
+ *                                                 vg_run as solve() does, and read from here by vg_sweep
+ *   HPR:   {gamma, p_inf, c_v, rho0, T0, c_s, alpha, tau1, tau2, T_ref, p_ref, is_thermal}
+ *                                                 HPRMaterialParameters, StiffenedGas equation of state */
+typedef struct vg_grid_desc {
+    int model;                        /* vg_model */
+    int nx;                           /* cells along X (columns) */
+    int ny;                           /* cells along Y (rows); 1 selects the 1D solver */
+    int precision;                    /* vg_precision */
+    int boundary;                     /* vg_boundary */
+    int device;                       /* CUDA device ordinal */
+    double params[VG_MAX_PARAMS];     /* material parameters, see above */
+} vg_grid_desc;
+
+typedef struct vg_run_config {
+    double dx;          /* cellSpacing */
+    double cfl;         /* CFLCoefficient */
+    double t_end;       /* finalTime; <= 0: no end time (max_steps must then be > 0) */
+    int max_steps;      /* > 0: stop after this many steps; <= 0: run until t_end */
+    double bias;        /* slope-limiter bias omega */
+    int limiter;        /* slopeLimiter id */
+    int subcycles;      /* subcyclingIterations (source integration; HPR and MHD only) */
+} vg_run_config;
+
+typedef struct vg_solver vg_solver;
+
+/* Create a solver for one grid.  Allocates device memory for two state buffers and a control block.
+ * Replaces the allocation the reference does inside solve()/solve2D() (Solvers/secondordersolver.cpp:293). */
+vg_status vg_create(const vg_grid_desc* desc, vg_solver** out);
+vg_status vg_destroy(vg_solver* s);
+
+/* Number of primitive planes the model takes at this boundary (6, 9, 17). */
+int vg_model_nvar(int model);
+
+/* Copy the state in / out.  planes: vg_model_nvar(model) planes of nx*ny float64, host or device
+ * memory (is_device).  Upload returns VG_EUNSUPPORTED if the state uses fields the compiled variants
+ * do not carry: Euler needs w == 0 and lambda == 1 in every cell; MHD needs w == 0 and Bz == 0 unless
+ * the solver was created for the full 9-component variant (it chooses it automatically when they are
+ * non-zero). */
+vg_status vg_upload_primitive(vg_solver* s, const double* planes, int is_device, void* stream);
+vg_status vg_download_primitive(vg_solver* s, double* planes, int is_device, void* stream);
+
+/* The time loop of SecondOrderSolver::solve / solve2D (Solvers/secondordersolver.cpp:288-314, :392-424)
+ * and its MHD/HPR counterparts, on the uploaded state, entirely on the device: CFL maximum, dt schedule
+ * (x0.2 for the first six steps, clamp to t_end; Solvers/solvers.cpp:437-452), X(dt/2) Y(dt) X(dt/2)
+ * sweeps in 2D, one sweep in 1D.  The loop is replayed from captured CUDA graphs; dt never returns to
+ * the host.  steps_taken / t_reached may be NULL. */
+vg_status vg_run(vg_solver* s, const vg_run_config* cfg, int* steps_taken, double* t_reached, void* stream);
+
+/* Host-buffer convenience: upload, vg_run, download (the reference's solve(): copy in, return by value). */
+vg_status vg_solve(vg_solver* s, const double* planes_in, double* planes_out, const vg_run_config* cfg,
+                   int* steps_taken, double* t_reached, void* stream);
+
+/* One sweep of compute{X,Y}SLICTimeStep2D (Solvers/secondordersolver.cpp:140-162, :214-236) or of the
+ * 1D computeSLICTimeStep (:80-98) with a host-given time step, in place on the uploaded state.
+ * axis: 0 = X, 1 = Y.  Enqueued asynchronously on `stream`. */
+vg_status vg_sweep(vg_solver* s, int axis, double dx, double dt, double bias, int limiter, void* stream);
+
+/* Solvers::computeMaximumWaveSpeed{,2D} over the ghosted grid (Solvers/solvers.cpp:259-339; MHD
+ * Solvers/mhdsolvers.cpp:286-388), including the default-state corner ghosts in 2D. */
+vg_status vg_max_wave_speed(vg_solver* s, double* out, void* stream);
+
+/* Device pointer of plane 0 of the current state buffer and the plane/row strides in elements, so a
+ * caller can read or write the resident state without a host round trip.  The carried planes are the
+ * non-trivial subset (Euler: rho, u, [v], p; MHD: rho, u, v, [w], p, Bx, By, [Bz], psi). */
+vg_status vg_state_device(vg_solver* s, double** plane0, long* plane_stride, long* row_stride, int* nplanes);
+
+/* Number of CUDA kernels the last vg_run/vg_sweep/vg_max_wave_speed call launched (graph nodes count). */
+long vg_last_launch_count(vg_solver* s);
+
+/* Text of the last error on this thread. */
+const char* vg_last_error_string(void);
+const char* vg_status_string(vg_status st);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VANGUARD_SLIC_H */

@@ -1,0 +1,190 @@
+"""ctypes bindings for the CPU oracle (test infrastructure only).
+
+Two libraries sit behind this module:
+
+* ``liboracle.so`` -- our plain-C restatement of the reference's SLIC/FORCE path (slic_oracle.c),
+  built by ``make -C oracle oracle``.  It is the checker the CUDA path is compared against.
+* ``_ref/libvgref.so`` -- the reference's own unmodified C++ sources plus an extern "C" harness
+  (ref_harness.cpp), built by ``make -C oracle ref`` where the reference tree exists.  It pins the
+  restatement and is the timed CPU baseline.
+
+Only tests/, bench.py's CPU legs and __graft_entry__.smoke() import this module.  Arrays are numpy
+float64 primitive planes of shape (nvar, ny, nx) (or (nvar, n) in 1D), C-contiguous, in the
+reference's primitive order.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libvgref.so")
+
+EULER, MHD, HPR = 0, 1, 2
+NVAR = {EULER: 6, MHD: 9, HPR: 17}
+TRANSMISSIVE, PERIODIC = 0, 1
+SUPERBEE, VANLEER, MINBEE = 0, 1, 2
+
+_D = ctypes.POINTER(ctypes.c_double)
+_I = ctypes.POINTER(ctypes.c_int)
+_c_int, _c_double = ctypes.c_int, ctypes.c_double
+
+_lib = None
+_ref = None
+
+
+def _ptr(a):
+    return a.ctypes.data_as(_D) if a is not None else None
+
+
+def _check(planes, nvar):
+    if not (isinstance(planes, np.ndarray) and planes.dtype == np.float64 and planes.flags.c_contiguous):
+        raise TypeError("planes must be a C-contiguous float64 numpy array")
+    if planes.shape[0] != nvar:
+        raise ValueError(f"expected {nvar} primitive planes, got {planes.shape[0]}")
+
+
+def lib():
+    """Load liboracle.so (our C restatement), building it on first use if missing."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(ORACLE_SO):
+            import subprocess
+            subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
+        L = ctypes.CDLL(ORACLE_SO)
+        L.vo_run1d.restype = _c_double
+        L.vo_run1d.argtypes = [_c_int, _D, _c_int, _c_double, _c_double, _c_double, _c_int, _c_double,
+                               _c_int, _D, _c_int, _c_int, _I, _D]
+        L.vo_run2d.restype = _c_double
+        L.vo_run2d.argtypes = [_c_int, _D, _c_int, _c_int, _c_double, _c_double, _c_double, _c_int,
+                               _c_double, _c_int, _D, _c_int, _c_int, _I, _D]
+        L.vo_sweep1d.argtypes = [_c_int, _D, _c_int, _c_double, _c_double, _c_double, _c_int, _D, _c_int]
+        L.vo_sweep2d.argtypes = [_c_int, _D, _c_int, _c_int, _c_int, _c_double, _c_double, _c_double,
+                                 _c_int, _D, _c_int]
+        L.vo_max_wave1d.restype = _c_double
+        L.vo_max_wave1d.argtypes = [_c_int, _D, _c_int, _D]
+        L.vo_max_wave2d.restype = _c_double
+        L.vo_max_wave2d.argtypes = [_c_int, _D, _c_int, _c_int, _D]
+        L.vo_slope_limiter.restype = _c_double
+        L.vo_slope_limiter.argtypes = [_c_double, _c_double, _c_int]
+        for name in ("vo_prim_to_cons", "vo_cons_to_prim"):
+            getattr(L, name).argtypes = [_c_int, _D, _D, _D]
+        L.vo_flux.argtypes = [_c_int, _D, _c_int, _D, _D]
+        L.vo_slic_flux.argtypes = [_c_int, _D, _D, _D, _D, _c_int, _c_double, _c_double, _c_double,
+                                   _c_int, _D, _D]
+        L.vo_nvar.restype = _c_int
+        L.vo_nparams.restype = _c_int
+        _lib = L
+    return _lib
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref():
+    """Load the compiled reference harness (oracle/_ref/libvgref.so)."""
+    global _ref
+    if _ref is None:
+        if not ref_available():
+            raise FileNotFoundError(f"{REF_SO} not built (make -C oracle ref needs the reference tree)")
+        R = ctypes.CDLL(REF_SO)
+        R.vgref_set_threads.restype = _c_int
+        R.vgref_set_threads.argtypes = [_c_int]
+        R.vgref_euler1d_run.restype = _c_double
+        R.vgref_euler1d_run.argtypes = [_D, _c_int, _c_double, _c_double, _c_double, _c_int, _c_double,
+                                        _c_int, _D, _I]
+        R.vgref_euler2d_run.restype = _c_double
+        R.vgref_euler2d_run.argtypes = [_D, _c_int, _c_int, _c_double, _c_double, _c_double, _c_int,
+                                        _c_double, _c_int, _D, _c_int, _I]
+        R.vgref_euler2d_sweep.argtypes = [_D, _c_int, _c_int, _c_int, _c_double, _c_double, _c_double,
+                                          _c_int, _D, _c_int]
+        R.vgref_euler2d_max_wave_speed.restype = _c_double
+        R.vgref_euler2d_max_wave_speed.argtypes = [_D, _c_int, _c_int, _D, _c_int]
+        for name in ("vgref_mhd1d_run",):
+            getattr(R, name).restype = _c_double
+            getattr(R, name).argtypes = [_D, _c_int, _c_double, _c_double, _c_double, _c_int, _c_double,
+                                         _c_int, _D, _c_int, _c_int, _I]
+        R.vgref_mhd2d_run.restype = _c_double
+        R.vgref_mhd2d_run.argtypes = [_D, _c_int, _c_int, _c_double, _c_double, _c_double, _c_int,
+                                      _c_double, _c_int, _D, _c_int, _c_int, _I]
+        if hasattr(R, "vgref_hpr2d_run"):
+            R.vgref_hpr2d_run.restype = _c_double
+            R.vgref_hpr2d_run.argtypes = [_D, _c_int, _c_int, _c_double, _c_double, _c_double, _c_int,
+                                          _c_double, _c_int, _D, _c_int, _c_int, _I]
+            R.vgref_hpr1d_run.restype = _c_double
+            R.vgref_hpr1d_run.argtypes = [_D, _c_int, _c_double, _c_double, _c_double, _c_int, _c_double,
+                                          _c_int, _D, _c_int, _c_int, _I]
+        _ref = R
+    return _ref
+
+
+# ------------------------------------------------------------------------------------ restatement
+
+def run(model, planes, dx, cfl, t_end=0.0, steps=0, bias=0.0, limiter=SUPERBEE, params=None,
+        bc=TRANSMISSIVE, subcycles=0, dt_log=False):
+    """Run solve()/solve2D()'s loop in the C restatement, in place.  Returns (t, steps[, dts])."""
+    _check(planes, NVAR[model])
+    prm = np.ascontiguousarray(params, dtype=np.float64)
+    st = ctypes.c_int()
+    dts = np.zeros(max(steps, 1), dtype=np.float64) if dt_log else None
+    if planes.ndim == 2:
+        t = lib().vo_run1d(model, _ptr(planes), planes.shape[1], dx, cfl, t_end, steps, bias, limiter,
+                           _ptr(prm), bc, subcycles, ctypes.byref(st), _ptr(dts))
+    else:
+        t = lib().vo_run2d(model, _ptr(planes), planes.shape[2], planes.shape[1], dx, cfl, t_end, steps,
+                           bias, limiter, _ptr(prm), bc, subcycles, ctypes.byref(st), _ptr(dts))
+    return (t, st.value, dts) if dt_log else (t, st.value)
+
+
+def sweep(model, planes, axis, dx, dt, bias=0.0, limiter=SUPERBEE, params=None, bc=TRANSMISSIVE):
+    _check(planes, NVAR[model])
+    prm = np.ascontiguousarray(params, dtype=np.float64)
+    if planes.ndim == 2:
+        lib().vo_sweep1d(model, _ptr(planes), planes.shape[1], dx, dt, bias, limiter, _ptr(prm), bc)
+    else:
+        lib().vo_sweep2d(model, _ptr(planes), planes.shape[2], planes.shape[1], axis, dx, dt, bias, limiter,
+                         _ptr(prm), bc)
+
+
+def max_wave(model, planes, params):
+    _check(planes, NVAR[model])
+    prm = np.ascontiguousarray(params, dtype=np.float64)
+    if planes.ndim == 2:
+        return lib().vo_max_wave1d(model, _ptr(planes), planes.shape[1], _ptr(prm))
+    return lib().vo_max_wave2d(model, _ptr(planes), planes.shape[2], planes.shape[1], _ptr(prm))
+
+
+# ------------------------------------------------------------------------------------ reference
+
+def ref_run(model, planes, dx, cfl, t_end=0.0, steps=0, bias=0.0, limiter=SUPERBEE, params=None,
+            bc=TRANSMISSIVE, subcycles=0, threads=1):
+    """Run the reference's own code on the same planes, in place.  steps <= 0 calls solve()/solve2D()
+    itself (time-driven, transmissive only).  Returns (t, steps); solve() reports neither (-1, -1)."""
+    _check(planes, NVAR[model])
+    R = ref()
+    R.vgref_set_threads(threads)
+    prm = np.ascontiguousarray(params, dtype=np.float64)
+    st = ctypes.c_int()
+    if model == EULER and planes.ndim == 2:
+        t = R.vgref_euler1d_run(_ptr(planes), planes.shape[1], dx, cfl, t_end, steps, bias, limiter,
+                                _ptr(prm), ctypes.byref(st))
+    elif model == EULER:
+        t = R.vgref_euler2d_run(_ptr(planes), planes.shape[2], planes.shape[1], dx, cfl, t_end, steps, bias,
+                                limiter, _ptr(prm), bc, ctypes.byref(st))
+    elif model == MHD and planes.ndim == 2:
+        t = R.vgref_mhd1d_run(_ptr(planes), planes.shape[1], dx, cfl, t_end, steps, bias, limiter, _ptr(prm),
+                              bc, subcycles, ctypes.byref(st))
+    elif model == MHD:
+        t = R.vgref_mhd2d_run(_ptr(planes), planes.shape[2], planes.shape[1], dx, cfl, t_end, steps, bias,
+                              limiter, _ptr(prm), bc, subcycles, ctypes.byref(st))
+    elif model == HPR and planes.ndim == 2:
+        t = R.vgref_hpr1d_run(_ptr(planes), planes.shape[1], dx, cfl, t_end, steps, bias, limiter, _ptr(prm),
+                              bc, subcycles, ctypes.byref(st))
+    else:
+        t = R.vgref_hpr2d_run(_ptr(planes), planes.shape[2], planes.shape[1], dx, cfl, t_end, steps, bias,
+                              limiter, _ptr(prm), bc, subcycles, ctypes.byref(st))
+    return t, st.value

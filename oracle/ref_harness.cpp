@@ -1,0 +1,332 @@
+// Test-infrastructure harness around the reference's own, unmodified SLIC code.
+//
+// Compiled by oracle/Makefile together with the reference sources into oracle/_ref/libvgref.so.
+// It exposes extern "C" entry points over structure-of-arrays PRIMITIVE planes (the reference stores
+// primitives in its cells), so Python tests and the CPU baseline in bench.py can drive the reference
+// with plain pointers.  Only tests/, bench.py's CPU legs and __graft_entry__.smoke() may load it.
+//
+// What it calls (paths relative to the reference tree):
+//   * SecondOrderSolver::solve / solve2D              Solvers/secondordersolver.cpp:288,392
+//   * the per-step functions that solve() is built from, to run a fixed number of steps:
+//       Solvers::insertBoundaryCells{,2D}             Solvers/solvers.cpp:7,88
+//       Solvers::computeStableTimeStep{,2D}           Solvers/solvers.cpp:388,413
+//       SecondOrderSolver::computeSLICTimeStep        Solvers/secondordersolver.cpp:80
+//       SecondOrderSolver::compute{X,Y}SLICTimeStep2D Solvers/secondordersolver.cpp:140,214
+//   * the MHD equivalents (Solvers/mhdsecondordersolver.cpp:318,501 and Solvers/mhdsolvers.cpp), with
+//     c_h set from the padded-grid maximum wave speed each step as solve() does (:330-332, :513-515).
+//   * the HPR equivalents (Solvers/hprsecondordersolver.cpp, Solvers/hprsolvers.cpp,
+//     Solvers/hprforcingsolver.cpp).
+//
+// The reference has no periodic boundary.  For periodic runs this harness builds the ghosted arrays
+// itself (2 ghost cells, wrap-around) and leaves the 2D corner blocks default-constructed, exactly as
+// insertBoundaryCells2D leaves them (Solvers/solvers.cpp:92), so the CFL maximum sees the same cells.
+//
+// Parity runs call vgref_set_threads(1): the reference's CFL maximum is an unsynchronised OpenMP
+// update (Solvers/solvers.cpp:264-273) and is only reproducible on one thread.
+
+#include "Solvers/secondordersolver.h"
+#include "Solvers/mhdsecondordersolver.h"
+#include "Solvers/mhdforcingsolver.h"
+#include "Solvers/hprsecondordersolver.h"
+#include "Solvers/hprforcingsolver.h"
+
+#include <omp.h>
+#include <iostream>
+#include <vector>
+
+using std::vector;
+
+namespace {
+
+// Per-step status lines go to cout in the reference (Solvers/solvers.cpp:611-614); drop them.
+struct QuietCout {
+    std::streambuf* saved;
+    QuietCout() : saved(std::cout.rdbuf(nullptr)) {}
+    ~QuietCout() { std::cout.clear(); std::cout.rdbuf(saved); }
+};
+
+const double kNoEnd = 1.0e300;
+
+// ---------------------------------------------------------------------------------------------- Euler
+// Plane order = EulerStateVector primitive order (Euler/eulerstatevector.cpp:47-55): rho,u,v,w,p,lambda.
+EulerMaterialParameters eulerParams(const double* prm) {
+    // prm = {gamma, p_inf, c_v, E0, T_ign, rate}  (Euler/eulermaterialparameters.cpp:36-46)
+    return EulerMaterialParameters(prm[0], prm[1], prm[2], prm[3], prm[4], prm[5]);
+}
+
+EulerStateVector eulerCell(const double* planes, long plane, long k) {
+    return EulerStateVector(planes[k], planes[plane + k], planes[2 * plane + k], planes[3 * plane + k],
+                            planes[4 * plane + k], planes[5 * plane + k]);
+}
+
+void eulerStore(EulerStateVector& c, double* planes, long plane, long k) {
+    vector<double> w = c.computePrimitiveVariableVector();
+    for (int v = 0; v < 6; v++) planes[v * plane + k] = w[v];
+}
+
+vector<vector<EulerStateVector> > eulerGrid(const double* planes, int nx, int ny) {
+    long plane = (long)nx * ny;
+    vector<vector<EulerStateVector> > g(ny, vector<EulerStateVector>(nx));
+    for (int i = 0; i < ny; i++)
+        for (int j = 0; j < nx; j++) g[i][j] = eulerCell(planes, plane, (long)i * nx + j);
+    return g;
+}
+
+void eulerUngrid(vector<vector<EulerStateVector> >& g, double* planes, int nx, int ny) {
+    long plane = (long)nx * ny;
+    for (int i = 0; i < ny; i++)
+        for (int j = 0; j < nx; j++) eulerStore(g[i][j], planes, plane, (long)i * nx + j);
+}
+
+// Ghosted copy with 2 wrap-around ghosts per side; corners stay default-constructed.
+template <class S>
+vector<vector<S> > periodicGhosts2D(vector<vector<S> >& c, int b) {
+    int ny = c.size(), nx = c[0].size();
+    vector<vector<S> > g(ny + 2 * b, vector<S>(nx + 2 * b));
+    for (int i = 0; i < ny; i++)
+        for (int j = 0; j < nx; j++) g[i + b][j + b] = c[i][j];
+    for (int i = 0; i < ny; i++)
+        for (int k = 0; k < b; k++) {
+            g[i + b][k] = c[i][nx - b + k];
+            g[i + b][nx + b + k] = c[i][k];
+        }
+    for (int j = 0; j < nx; j++)
+        for (int k = 0; k < b; k++) {
+            g[k][j + b] = c[ny - b + k][j];
+            g[ny + b + k][j + b] = c[k][j];
+        }
+    return g;
+}
+
+template <class S>
+vector<S> periodicGhosts1D(vector<S>& c, int b) {
+    int n = c.size();
+    vector<S> g(n + 2 * b);
+    for (int i = 0; i < n; i++) g[i + b] = c[i];
+    for (int k = 0; k < b; k++) {
+        g[k] = c[n - b + k];
+        g[n + b + k] = c[k];
+    }
+    return g;
+}
+
+// ------------------------------------------------------------------------------------------------ MHD
+// Plane order = MHDStateVector primitive order (MHD/mhdstatevector.cpp:35-47):
+// rho,u,v,w,p,Bx,By,Bz,psi.
+MHDStateVector mhdCell(const double* planes, long plane, long k) {
+    return MHDStateVector(planes[k], planes[plane + k], planes[2 * plane + k], planes[3 * plane + k],
+                          planes[4 * plane + k], planes[5 * plane + k], planes[6 * plane + k],
+                          planes[7 * plane + k], planes[8 * plane + k]);
+}
+
+void mhdStore(MHDStateVector& c, double* planes, long plane, long k) {
+    vector<double> w = c.computePrimitiveVariableVector();
+    for (int v = 0; v < 9; v++) planes[v * plane + k] = w[v];
+}
+
+MHDMaterialParameters mhdParams(const double* prm) {
+    MHDMaterialParameters mp(prm[0]);
+    mp.setStiffeningParameter(prm[1]);
+    return mp;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Set the OpenMP team size used by the reference loops (n <= 0: all host cores).  Returns the size.
+int vgref_set_threads(int n) {
+    if (n <= 0) n = omp_get_num_procs();
+    omp_set_num_threads(n);
+    return n;
+}
+
+// --------------------------------------------------------------------------------------- Euler 1D
+// Runs SecondOrderSolver::solve's loop on n cells (planes: 6 x n, transmissive).  max_steps <= 0 calls
+// the reference's solve() itself (time-driven); otherwise the same per-step calls are made by this
+// loop so a fixed step count can be run.  Returns the time reached; *steps_out the steps taken.
+double vgref_euler1d_run(double* planes, int n, double dx, double cfl, double t_end, int max_steps,
+                         double bias, int limiter, const double* prm, int* steps_out) {
+    QuietCout quiet;
+    EulerMaterialParameters mp = eulerParams(prm);
+    vector<EulerStateVector> cells(n);
+    for (int i = 0; i < n; i++) cells[i] = eulerCell(planes, n, i);
+    double t = 0.0;
+    int it = 0;
+    if (max_steps <= 0) {
+        cells = SecondOrderSolver::solve(cells, dx, cfl, t_end, bias, limiter, 0, mp);
+        t = -1.0;  // solve() does not report its step count or final time
+        it = -1;
+    } else {
+        double tEnd = t_end > 0.0 ? t_end : kNoEnd;
+        while (t < tEnd && it < max_steps) {
+            vector<EulerStateVector> withB = Solvers::insertBoundaryCells(cells, 2);
+            double dt = Solvers::computeStableTimeStep(withB, dx, cfl, t, tEnd, it, mp);
+            SecondOrderSolver::computeSLICTimeStep(cells, withB, dx, dt, bias, limiter, mp);
+            t += dt;
+            it += 1;
+        }
+    }
+    for (int i = 0; i < n; i++) eulerStore(cells[i], planes, n, i);
+    if (steps_out) *steps_out = it;
+    return t;
+}
+
+// --------------------------------------------------------------------------------------- Euler 2D
+// nx columns (x, inner index j) by ny rows (y, row index i); planes: 6 x (ny*nx), row-major.
+// bc: 0 transmissive (reference ghosts), 1 periodic (harness ghosts).
+double vgref_euler2d_run(double* planes, int nx, int ny, double dx, double cfl, double t_end, int max_steps,
+                         double bias, int limiter, const double* prm, int bc, int* steps_out) {
+    QuietCout quiet;
+    EulerMaterialParameters mp = eulerParams(prm);
+    vector<vector<EulerStateVector> > cells = eulerGrid(planes, nx, ny);
+    double t = 0.0;
+    int it = 0;
+    if (max_steps <= 0 && bc == 0) {
+        cells = SecondOrderSolver::solve2D(cells, dx, cfl, t_end, bias, limiter, 0, mp);
+        t = -1.0;
+        it = -1;
+    } else {
+        double tEnd = t_end > 0.0 ? t_end : kNoEnd;
+        int limit = max_steps > 0 ? max_steps : 0x7fffffff;
+        auto ghosts = [&](vector<vector<EulerStateVector> >& c) {
+            return bc == 1 ? periodicGhosts2D(c, 2) : Solvers::insertBoundaryCells2D(c, 2);
+        };
+        while (t < tEnd && it < limit) {
+            vector<vector<EulerStateVector> > withB = ghosts(cells);
+            double dt = Solvers::computeStableTimeStep2D(withB, dx, cfl, t, tEnd, it, mp);
+            SecondOrderSolver::computeXSLICTimeStep2D(cells, withB, dx, 0.5 * dt, bias, limiter, mp);
+            withB = ghosts(cells);
+            SecondOrderSolver::computeYSLICTimeStep2D(cells, withB, dx, dt, bias, limiter, mp);
+            withB = ghosts(cells);
+            SecondOrderSolver::computeXSLICTimeStep2D(cells, withB, dx, 0.5 * dt, bias, limiter, mp);
+            t += dt;
+            it += 1;
+        }
+    }
+    eulerUngrid(cells, planes, nx, ny);
+    if (steps_out) *steps_out = it;
+    return t;
+}
+
+// One sweep (axis 0 = X, 1 = Y) with time step dt, on the ghosted grid the reference builds.
+void vgref_euler2d_sweep(double* planes, int nx, int ny, int axis, double dx, double dt, double bias,
+                         int limiter, const double* prm, int bc) {
+    EulerMaterialParameters mp = eulerParams(prm);
+    vector<vector<EulerStateVector> > cells = eulerGrid(planes, nx, ny);
+    vector<vector<EulerStateVector> > withB =
+        bc == 1 ? periodicGhosts2D(cells, 2) : Solvers::insertBoundaryCells2D(cells, 2);
+    if (axis == 0)
+        SecondOrderSolver::computeXSLICTimeStep2D(cells, withB, dx, dt, bias, limiter, mp);
+    else
+        SecondOrderSolver::computeYSLICTimeStep2D(cells, withB, dx, dt, bias, limiter, mp);
+    eulerUngrid(cells, planes, nx, ny);
+}
+
+// computeMaximumWaveSpeed2D over the ghosted grid (corner blocks default-constructed).
+double vgref_euler2d_max_wave_speed(const double* planes, int nx, int ny, const double* prm, int bc) {
+    EulerMaterialParameters mp = eulerParams(prm);
+    vector<vector<EulerStateVector> > cells = eulerGrid(planes, nx, ny);
+    vector<vector<EulerStateVector> > withB =
+        bc == 1 ? periodicGhosts2D(cells, 2) : Solvers::insertBoundaryCells2D(cells, 2);
+    return Solvers::computeMaximumWaveSpeed2D(withB, mp);
+}
+
+// ----------------------------------------------------------------------------------------- MHD 1D/2D
+// planes: 9 x cells.  prm = {gamma, p_inf}.  subcycles > 0 adds MHDForcingSolver's RK4 GLM damping
+// around the sweeps as solve()/solve2D() do (Solvers/mhdsecondordersolver.cpp:334-348, :517-540);
+// only with transmissive boundaries.
+double vgref_mhd1d_run(double* planes, int n, double dx, double cfl, double t_end, int max_steps,
+                       double bias, int limiter, const double* prm, int bc, int subcycles, int* steps_out) {
+    QuietCout quiet;
+    MHDMaterialParameters mp = mhdParams(prm);
+    vector<MHDStateVector> cells(n);
+    for (int i = 0; i < n; i++) cells[i] = mhdCell(planes, n, i);
+    double t = 0.0;
+    int it = 0;
+    if (max_steps <= 0 && bc == 0) {
+        cells = MHDSecondOrderSolver::solve(cells, dx, cfl, t_end, bias, limiter, subcycles, mp);
+        t = -1.0;
+        it = -1;
+    } else {
+        double tEnd = t_end > 0.0 ? t_end : kNoEnd;
+        int limit = max_steps > 0 ? max_steps : 0x7fffffff;
+        auto ghosts = [&](vector<MHDStateVector>& c, int b) {
+            return bc == 1 ? periodicGhosts1D(c, b) : MHDSolvers::insertBoundaryCells(c, b);
+        };
+        while (t < tEnd && it < limit) {
+            vector<MHDStateVector> withB = ghosts(cells, 2);
+            double dt = MHDSolvers::computeStableTimeStep(withB, dx, cfl, t, tEnd, it, mp);
+            double smax = MHDSolvers::computeMaximumWaveSpeed(withB, mp);
+            mp.setHyperbolicWaveSpeed(smax);
+            mp.configureParabolicDamping();
+            for (int s = 0; s < subcycles; s++) {
+                withB = ghosts(cells, 1);
+                MHDForcingSolver::computeRungeKuttaTimeStep(cells, withB, dx, 0.5 * (dt / subcycles), bias, limiter, mp);
+            }
+            withB = ghosts(cells, 2);
+            MHDSecondOrderSolver::computeSLICTimeStep(cells, withB, dx, dt, bias, limiter, mp);
+            for (int s = 0; s < subcycles; s++) {
+                withB = ghosts(cells, 1);
+                MHDForcingSolver::computeRungeKuttaTimeStep(cells, withB, dx, 0.5 * (dt / subcycles), bias, limiter, mp);
+            }
+            t += dt;
+            it += 1;
+        }
+    }
+    for (int i = 0; i < n; i++) mhdStore(cells[i], planes, n, i);
+    if (steps_out) *steps_out = it;
+    return t;
+}
+
+double vgref_mhd2d_run(double* planes, int nx, int ny, double dx, double cfl, double t_end, int max_steps,
+                       double bias, int limiter, const double* prm, int bc, int subcycles, int* steps_out) {
+    QuietCout quiet;
+    MHDMaterialParameters mp = mhdParams(prm);
+    long plane = (long)nx * ny;
+    vector<vector<MHDStateVector> > cells(ny, vector<MHDStateVector>(nx));
+    for (int i = 0; i < ny; i++)
+        for (int j = 0; j < nx; j++) cells[i][j] = mhdCell(planes, plane, (long)i * nx + j);
+    double t = 0.0;
+    int it = 0;
+    if (max_steps <= 0 && bc == 0) {
+        cells = MHDSecondOrderSolver::solve2D(cells, dx, cfl, t_end, bias, limiter, subcycles, mp);
+        t = -1.0;
+        it = -1;
+    } else {
+        double tEnd = t_end > 0.0 ? t_end : kNoEnd;
+        int limit = max_steps > 0 ? max_steps : 0x7fffffff;
+        auto ghosts = [&](vector<vector<MHDStateVector> >& c, int b) {
+            return bc == 1 ? periodicGhosts2D(c, b) : MHDSolvers::insertBoundaryCells2D(c, b);
+        };
+        while (t < tEnd && it < limit) {
+            vector<vector<MHDStateVector> > withB = ghosts(cells, 2);
+            double dt = MHDSolvers::computeStableTimeStep2D(withB, dx, cfl, t, tEnd, it, mp);
+            double smax = MHDSolvers::computeMaximumWaveSpeed2D(withB, mp);
+            mp.setHyperbolicWaveSpeed(smax);
+            mp.configureParabolicDamping();
+            for (int s = 0; s < subcycles; s++) {
+                withB = ghosts(cells, 1);
+                MHDForcingSolver::computeRungeKuttaTimeStep2D(cells, withB, dx, 0.5 * (dt / subcycles), bias, limiter, mp);
+            }
+            withB = ghosts(cells, 2);
+            MHDSecondOrderSolver::computeXSLICTimeStep2D(cells, withB, dx, 0.5 * dt, bias, limiter, mp);
+            withB = ghosts(cells, 2);
+            MHDSecondOrderSolver::computeYSLICTimeStep2D(cells, withB, dx, dt, bias, limiter, mp);
+            withB = ghosts(cells, 2);
+            MHDSecondOrderSolver::computeXSLICTimeStep2D(cells, withB, dx, 0.5 * dt, bias, limiter, mp);
+            for (int s = 0; s < subcycles; s++) {
+                withB = ghosts(cells, 1);
+                MHDForcingSolver::computeRungeKuttaTimeStep2D(cells, withB, dx, 0.5 * (dt / subcycles), bias, limiter, mp);
+            }
+            t += dt;
+            it += 1;
+        }
+    }
+    for (int i = 0; i < ny; i++)
+        for (int j = 0; j < nx; j++) mhdStore(cells[i][j], planes, plane, (long)i * nx + j);
+    if (steps_out) *steps_out = it;
+    return t;
+}
+
+}  // extern "C"

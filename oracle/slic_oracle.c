@@ -1,0 +1,479 @@
+/* CPU restatement of Vanguard's SLIC/FORCE path -- TEST INFRASTRUCTURE, never the product.
+ *
+ * Each function restates one reference function with the reference's floating-point operation
+ * order (left-to-right sums, a - b written as a + (-1 * b) where the reference does so, which is
+ * bit-identical to a - b).  Built with -ffp-contract=off so no FMA is formed, like the reference's
+ * x86-64 build.  Pinned bit-for-bit against the compiled reference (oracle/_ref/libvgref.so) by
+ * tests/test_oracle_pin.py and against tests/golden/ fixtures.
+ *
+ * Citations are path:line inside the Vanguard source tree.
+ */
+#include "slic_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define MAXV 17
+
+/* std::min / std::max semantics: min(a,b) = (b < a) ? b : a; max(a,b) = (a < b) ? b : a. */
+static double smin(double a, double b) { return (b < a) ? b : a; }
+static double smax(double a, double b) { return (a < b) ? b : a; }
+
+/* ------------------------------------------------------------------------------ slope limiters */
+
+/* SlopeLimiters::computeRCoefficient, Solvers/slopelimiters.cpp:7-10 */
+static double r_coefficient(double r, double w) { return 2.0 / ((1.0 - w) + ((1.0 + w) * r)); }
+
+/* Solvers/slopelimiters.cpp:12-74 (superbee :12-30, van Leer :32-42, minbee :44-58, dispatch :60-74) */
+double vo_slope_limiter(double r, double w, int id) {
+    if (id == 0) {
+        if (r < 0.0) return 0.0;
+        if (r < 0.5) return 2.0 * r;
+        if (r < 1.0) return 1.0;
+        return smin(smin(r, r_coefficient(r, w)), 2.0);
+    } else if (id == 1) {
+        if (r < 0.0) return 0.0;
+        return smin((2.0 * r) / (1.0 + r), r_coefficient(r, w));
+    } else {
+        if (r < 0.0) return 0.0;
+        if (r < 1.0) return r;
+        return smin(1.0, r_coefficient(r, w));
+    }
+}
+
+/* SlopeLimiters::computeSlopeVector(vector,vector,vector,...), Solvers/slopelimiters.cpp:217-246.
+ * The 1e-5 floor is pow(10.0, -5.0) in the reference and replaces |x| < 1e-5 by +1e-5 (sign lost). */
+static void slope_vector(int nv, const double* uL, const double* u, const double* uR, double w, int lim,
+                         double* slope) {
+    const double floor5 = pow(10.0, -5.0);
+    const double cm = 0.5 * (1.0 + w), cp = 0.5 * (1.0 - w);
+    for (int i = 0; i < nv; i++) {
+        double dm = u[i] + (-1.0 * uL[i]);
+        double dp = uR[i] + (-1.0 * u[i]);
+        slope[i] = (cm * dm) + (cp * dp);
+        double num = dm, den = dp;
+        if (fabs(num) < floor5) num = floor5;
+        if (fabs(den) < floor5) den = floor5;
+        slope[i] *= vo_slope_limiter(num / den, w, lim);
+    }
+}
+
+/* -------------------------------------------------------------------------------------- models */
+
+typedef struct model model;
+struct model {
+    int nv;
+    void (*cons)(const double* W, const double* prm, double* U);
+    /* setConservedVariableVector: W is the state's previous primitives (read for HPR fields the
+     * reference leaves untouched), overwritten with the new ones. */
+    void (*setcons)(const double* U, const double* prm, double* W);
+    void (*flux)(const double* U, int axis, const double* prm, double* F);
+    double (*wave1d)(const double* W, const double* prm);
+    double (*wave2d)(const double* W, const double* prm);
+    void (*default_state)(const double* prm, double* W);
+};
+
+/* ---- Euler: Euler/eulerstatevector.cpp, Euler/eulerequationofstate.cpp
+ * prm = {gamma, p_inf, c_v, E0, T_ign, rate}.  W = rho,u,v,w,p,lambda. */
+
+/* EulerEquationOfState::computeSpecificInternalEnergy, Euler/eulerequationofstate.cpp:7-13 */
+static double euler_e(double rho, double p, const double* prm) {
+    return (p + (prm[0] * prm[1])) / ((prm[0] - 1) * rho);
+}
+/* EulerEquationOfState::computePressure, Euler/eulerequationofstate.cpp:15-21 */
+static double euler_p(double rho, double e, const double* prm) {
+    return ((e * (prm[0] - 1)) * rho) - (prm[0] * prm[1]);
+}
+/* EulerStateVector::computeConservedVariableVector + computeTotalEnergy,
+ * Euler/eulerstatevector.cpp:78-91, :192-198 */
+static void euler_cons(const double* W, const double* prm, double* U) {
+    double rho = W[0], u = W[1], v = W[2], w = W[3], p = W[4], lam = W[5];
+    double v2 = ((u * u) + (v * v)) + (w * w);
+    U[0] = rho;
+    U[1] = rho * u;
+    U[2] = rho * v;
+    U[3] = rho * w;
+    U[4] = rho * (((0.5 * v2) + euler_e(rho, p, prm)) + (prm[3] * (lam - 1.0)));
+    U[5] = rho * lam;
+}
+/* EulerStateVector::setConservedVariableVector, Euler/eulerstatevector.cpp:47-61 */
+static void euler_setcons(const double* U, const double* prm, double* W) {
+    double rho = U[0];
+    double u = U[1] / rho, v = U[2] / rho, w = U[3] / rho, lam = U[5] / rho;
+    double v2 = ((u * u) + (v * v)) + (w * w);
+    double e = ((U[4] / rho) - (0.5 * v2)) - (prm[3] * (lam - 1.0));
+    W[0] = rho; W[1] = u; W[2] = v; W[3] = w; W[4] = euler_p(rho, e, prm); W[5] = lam;
+}
+/* EulerStateVector::compute{X,Y}FluxVector(vector, params), Euler/eulerstatevector.cpp:93-120, :127-154 */
+static void euler_flux(const double* U, int axis, const double* prm, double* F) {
+    double rho = U[0];
+    double u = U[1] / rho, v = U[2] / rho, w = U[3] / rho, lam = U[5] / rho;
+    double v2 = ((u * u) + (v * v)) + (w * w);
+    double E = U[4] / rho;
+    double e = (E - (0.5 * v2)) - (prm[3] * (lam - 1.0));
+    double p = euler_p(rho, e, prm);
+    if (axis == 0) {
+        F[0] = rho * u;
+        F[1] = (rho * (u * u)) + p;
+        F[2] = rho * (u * v);
+        F[3] = rho * (u * w);
+        F[4] = (rho * (u * E)) + (u * p);
+        F[5] = rho * (u * lam);
+    } else {
+        F[0] = rho * v;
+        F[1] = rho * (v * u);
+        F[2] = (rho * (v * v)) + p;
+        F[3] = rho * (v * w);
+        F[4] = (rho * (v * E)) + (v * p);
+        F[5] = rho * (v * lam);
+    }
+}
+/* EulerEquationOfState::computeSoundSpeed, Euler/eulerequationofstate.cpp:23-29 */
+static double euler_c(const double* W, const double* prm) {
+    return sqrt((prm[0] * (W[4] + prm[1])) / W[0]);
+}
+/* Solvers::computeMaximumWaveSpeed per-cell term, Solvers/solvers.cpp:259-276 */
+static double euler_wave1d(const double* W, const double* prm) { return fabs(W[1]) + euler_c(W, prm); }
+/* Solvers::computeMaximumWaveSpeed2D per-cell term, Solvers/solvers.cpp:318-339 */
+static double euler_wave2d(const double* W, const double* prm) {
+    return smax(fabs(W[1]), fabs(W[2])) + euler_c(W, prm);
+}
+/* EulerStateVector(), Euler/eulerstatevector.cpp:3-12 */
+static void euler_default(const double* prm, double* W) {
+    (void)prm;
+    W[0] = 1.0; W[1] = 0.0; W[2] = 0.0; W[3] = 0.0; W[4] = 1.0; W[5] = 1.0;
+}
+
+/* ---- ideal MHD with GLM: MHD/mhdstatevector.cpp, MHD/mhdequationofstate.cpp, MHD/mhdwavespeeds.cpp
+ * prm = {gamma, p_inf, c_h}.  W = rho,u,v,w,p,Bx,By,Bz,psi. */
+
+static double mhd_e(double rho, double p, const double* prm) {          /* mhdequationofstate.cpp:7-13 */
+    return (p + (prm[0] * prm[1])) / ((prm[0] - 1) * rho);
+}
+static double mhd_p(double rho, double e, const double* prm) {          /* mhdequationofstate.cpp:15-21 */
+    return ((e * (prm[0] - 1)) * rho) - (prm[0] * prm[1]);
+}
+/* MHDStateVector::computeConservedVariableVector + computeTotalEnergy, MHD/mhdstatevector.cpp:89-106, :236-245 */
+static void mhd_cons(const double* W, const double* prm, double* U) {
+    double rho = W[0], u = W[1], v = W[2], w = W[3], p = W[4], bx = W[5], by = W[6], bz = W[7];
+    double v2 = ((u * u) + (v * v)) + (w * w);
+    double hydro = rho * ((0.5 * v2) + mhd_e(rho, p, prm));
+    double b2 = ((bx * bx) + (by * by)) + (bz * bz);
+    U[0] = rho; U[1] = rho * u; U[2] = rho * v; U[3] = rho * w;
+    U[4] = hydro + (0.5 * b2);
+    U[5] = bx; U[6] = by; U[7] = bz; U[8] = W[8];
+}
+/* MHDStateVector::setConservedVariableVector, MHD/mhdstatevector.cpp:49-68 */
+static void mhd_setcons(const double* U, const double* prm, double* W) {
+    double rho = U[0];
+    double u = U[1] / rho, v = U[2] / rho, w = U[3] / rho;
+    double bx = U[5], by = U[6], bz = U[7];
+    double b2 = ((bx * bx) + (by * by)) + (bz * bz);
+    double E = (U[4] - (0.5 * b2)) / rho;
+    double v2 = ((u * u) + (v * v)) + (w * w);
+    double e = E - (0.5 * v2);
+    W[0] = rho; W[1] = u; W[2] = v; W[3] = w; W[4] = mhd_p(rho, e, prm);
+    W[5] = bx; W[6] = by; W[7] = bz; W[8] = U[8];
+}
+/* MHDStateVector::compute{X,Y}FluxVector(vector, params), MHD/mhdstatevector.cpp:108-158, :165-215.
+ * v.B is VectorAlgebra::computeDotProduct (Mathematics/vectoralgebra.cpp:38-49), summed from 0.0. */
+static void mhd_flux(const double* U, int axis, const double* prm, double* F) {
+    double rho = U[0];
+    double u = U[1] / rho, v = U[2] / rho, w = U[3] / rho;
+    double bx = U[5], by = U[6], bz = U[7], psi = U[8];
+    double b2 = ((bx * bx) + (by * by)) + (bz * bz);
+    double E = U[4];
+    double hydroE = (E - (0.5 * b2)) / rho;
+    double v2 = ((u * u) + (v * v)) + (w * w);
+    double e = hydroE - (0.5 * v2);
+    double p = mhd_p(rho, e, prm);
+    double ch2 = prm[2] * prm[2];
+    double vb = ((0.0 + (u * bx)) + (v * by)) + (w * bz);
+    if (axis == 0) {
+        F[0] = rho * u;
+        F[1] = (((rho * (u * u)) + p) + (0.5 * b2)) - (bx * bx);
+        F[2] = (rho * (u * v)) - (bx * by);
+        F[3] = (rho * (u * w)) - (bx * bz);
+        F[4] = (((E + p) + (0.5 * b2)) * u) - (vb * bx);
+        F[5] = psi;
+        F[6] = (by * u) - (bx * v);
+        F[7] = (bz * u) - (bx * w);
+        F[8] = ch2 * bx;
+    } else {
+        F[0] = rho * v;
+        F[1] = (rho * (v * u)) - (by * bx);
+        F[2] = (((rho * (v * v)) + p) + (0.5 * b2)) - (by * by);
+        F[3] = (rho * (v * w)) - (by * bz);
+        F[4] = (((E + p) + (0.5 * b2)) * v) - (vb * by);
+        F[5] = (bx * v) - (by * u);
+        F[6] = psi;
+        F[7] = (bz * v) - (by * w);
+        F[8] = ch2 * by;
+    }
+}
+/* MHDWaveSpeeds::compute{X,Y}FastMagnetoAcousticSpeed, MHD/mhdwavespeeds.cpp:7-17, :43-63 */
+static double mhd_fast(const double* W, const double* prm, double bn) {
+    double rho = W[0], bx = W[5], by = W[6], bz = W[7];
+    double c = sqrt((prm[0] * (W[4] + prm[1])) / rho);
+    double a = sqrt(((0.0 + (bx * bx)) + (by * by)) + (bz * bz)) / sqrt(rho);
+    double c2 = c * c, a2 = a * a;
+    return sqrt(0.5 * ((c2 + a2) + sqrt(((c2 + a2) * (c2 + a2)) - (4.0 * ((c2 * (bn * bn)) / rho)))));
+}
+/* MHDSolvers::computeMaximumWaveSpeed{,2D} per-cell terms, Solvers/mhdsolvers.cpp:286-303, :365-388 */
+static double mhd_wave1d(const double* W, const double* prm) {
+    return fabs(W[1]) + fabs(mhd_fast(W, prm, W[5]));
+}
+static double mhd_wave2d(const double* W, const double* prm) {
+    return smax(fabs(W[1]), fabs(W[2])) + smax(fabs(mhd_fast(W, prm, W[5])), fabs(mhd_fast(W, prm, W[6])));
+}
+/* MHDStateVector(), MHD/mhdstatevector.cpp:3-16 */
+static void mhd_default(const double* prm, double* W) {
+    (void)prm;
+    for (int i = 0; i < 9; i++) W[i] = 0.0;
+    W[0] = 1.0; W[4] = 1.0;
+}
+
+static const model M_EULER = {6, euler_cons, euler_setcons, euler_flux, euler_wave1d, euler_wave2d, euler_default};
+static const model M_MHD = {9, mhd_cons, mhd_setcons, mhd_flux, mhd_wave1d, mhd_wave2d, mhd_default};
+
+static const model* model_of(int id) {
+    switch (id) {
+        case VO_EULER: return &M_EULER;
+        case VO_MHD: return &M_MHD;
+        default: return NULL;
+    }
+}
+
+int vo_nvar(int id) { const model* m = model_of(id); return m ? m->nv : 0; }
+int vo_nparams(int id) { return id == VO_EULER ? 6 : id == VO_MHD ? 3 : 0; }
+
+/* ------------------------------------------------------------------------------- SLIC building blocks */
+
+/* Solvers::evolveStateByHalf{X,Y}TimeStep + evolveStateByHalfTimeStep + computeEvolutionVector,
+ * Solvers/solvers.cpp:454-466, :502-514, :550-565, :601-609.  Returns primitives (the reference
+ * stores the evolved state in a default-constructed state vector). */
+static void evolve_half(const model* m, const double* wl, const double* wm, const double* wr, int axis,
+                        double dx, double dt, double w, int lim, int side, const double* prm, double* out) {
+    double uL[MAXV], uM[MAXV], uR[MAXV], s[MAXV], xl[MAXV], xr[MAXV], fl[MAXV], fr[MAXV], ev[MAXV];
+    int nv = m->nv;
+    m->cons(wl, prm, uL);
+    m->cons(wm, prm, uM);
+    m->cons(wr, prm, uR);
+    slope_vector(nv, uL, uM, uR, w, lim, s);
+    for (int i = 0; i < nv; i++) {
+        xl[i] = uM[i] + (-1.0 * (0.5 * s[i]));
+        xr[i] = uM[i] + (0.5 * s[i]);
+    }
+    m->flux(xl, axis, prm, fl);
+    m->flux(xr, axis, prm, fr);
+    double c = 0.5 * (dt / dx);
+    for (int i = 0; i < nv; i++) ev[i] = c * (fl[i] + (-1.0 * fr[i]));
+    double sum[MAXV];
+    for (int i = 0; i < nv; i++) sum[i] = (side == 0 ? xl[i] : xr[i]) + ev[i];
+    m->default_state(prm, out);
+    m->setcons(sum, prm, out);
+}
+
+/* FirstOrderSolver::compute{X,Y}FORCEFlux with its Lax-Friedrichs and Richtmyer halves,
+ * Solvers/firstordersolver.cpp:7-17, :79-85, :87-98, :165-171, :173-180, :227-230. */
+static void force_flux(const model* m, const double* wa, const double* wb, int axis, double dx, double dt,
+                       const double* prm, double* F) {
+    double ua[MAXV], ub[MAXV], fa[MAXV], fb[MAXV], uri[MAXV], fri[MAXV], lf[MAXV];
+    int nv = m->nv;
+    m->cons(wa, prm, ua);
+    m->cons(wb, prm, ub);
+    m->flux(ua, axis, prm, fa);
+    m->flux(ub, axis, prm, fb);
+    double rinv = dx / dt, r = dt / dx;
+    for (int i = 0; i < nv; i++) lf[i] = 0.5 * ((fa[i] + fb[i]) + (rinv * (ua[i] + (-1.0 * ub[i]))));
+    for (int i = 0; i < nv; i++) uri[i] = 0.5 * ((ua[i] + ub[i]) + (r * (fa[i] + (-1.0 * fb[i]))));
+    m->flux(uri, axis, prm, fri);
+    for (int i = 0; i < nv; i++) F[i] = 0.5 * (lf[i] + fri[i]);
+}
+
+/* SecondOrderSolver::compute{X,Y}SLICFlux, Solvers/secondordersolver.cpp:7-17, :43-53 */
+static void slic_flux(const model* m, const double* wLL, const double* wL, const double* wR, const double* wRR,
+                      int axis, double dx, double dt, double w, int lim, const double* prm, double* F) {
+    double a[MAXV], b[MAXV];
+    evolve_half(m, wLL, wL, wR, axis, dx, dt, w, lim, 1, prm, a);
+    evolve_half(m, wL, wR, wRR, axis, dx, dt, w, lim, 0, prm, b);
+    force_flux(m, a, b, axis, dx, dt, prm, F);
+}
+
+/* ------------------------------------------------------------------------------------ grids */
+
+/* Ghost index along one axis of length n with 2 ghosts: transmissive mirror (Solvers/solvers.cpp:17-23)
+ * or wrap-around; k runs over -2 .. n+1. */
+static int ghost_index(int k, int n, int bc) {
+    if (k >= 0 && k < n) return k;
+    if (bc == VO_BC_PERIODIC) return (k < 0) ? k + n : k - n;
+    return (k < 0) ? (-1 - k) : (2 * n - 1 - k);
+}
+
+static void load_cell(const double* planes, long plane, long idx, int nv, double* W) {
+    for (int v = 0; v < nv; v++) W[v] = planes[v * plane + idx];
+}
+
+/* One sweep of compute{X,Y}SLICTimeStep2D (Solvers/secondordersolver.cpp:140-162, :214-236) over a
+ * grid with ncol columns, nrow rows.  Each interface flux is a pure function of its 4-cell stencil, so
+ * computing it once and using it for both neighbours gives the reference's values. */
+static void sweep_grid(const model* m, double* planes, int nx, int ny, int axis, double dx, double dt,
+                       double w, int lim, const double* prm, int bc) {
+    long plane = (long)nx * ny;
+    int nv = m->nv;
+    int nline = axis == 0 ? ny : nx, len = axis == 0 ? nx : ny;
+    double* out = (double*)malloc(sizeof(double) * nv * plane);
+    double r = dt / dx;
+#pragma omp parallel for schedule(static)
+    for (int line = 0; line < nline; line++) {
+        double* fl = (double*)malloc(sizeof(double) * MAXV * (len + 1));
+        double st[4][MAXV];
+        for (int f = 0; f <= len; f++) {
+            /* interface f sits between cells f-1 and f; stencil cells f-2 .. f+1 */
+            for (int s = 0; s < 4; s++) {
+                int k = ghost_index(f - 2 + s, len, bc);
+                long idx = axis == 0 ? (long)line * nx + k : (long)k * nx + line;
+                load_cell(planes, plane, idx, nv, st[s]);
+            }
+            slic_flux(m, st[0], st[1], st[2], st[3], axis, dx, dt, w, lim, prm, fl + (long)f * MAXV);
+        }
+        for (int c = 0; c < len; c++) {
+            long idx = axis == 0 ? (long)line * nx + c : (long)c * nx + line;
+            double W[MAXV], U[MAXV], Un[MAXV];
+            load_cell(planes, plane, idx, nv, W);
+            m->cons(W, prm, U);
+            /* FirstOrderSolver::computeFORCEUpdate, Solvers/firstordersolver.cpp:428-433 */
+            for (int v = 0; v < nv; v++)
+                Un[v] = U[v] + (r * (fl[(long)c * MAXV + v] + (-1.0 * fl[(long)(c + 1) * MAXV + v])));
+            m->setcons(Un, prm, W);
+            for (int v = 0; v < nv; v++) out[v * plane + idx] = W[v];
+        }
+        free(fl);
+    }
+    memcpy(planes, out, sizeof(double) * nv * plane);
+    free(out);
+}
+
+void vo_sweep2d(int id, double* planes, int nx, int ny, int axis, double dx, double dt, double w, int lim,
+                const double* prm, int bc) {
+    const model* m = model_of(id);
+    if (!m) return;
+    sweep_grid(m, planes, nx, ny, axis, dx, dt, w, lim, prm, bc);
+}
+
+void vo_sweep1d(int id, double* planes, int n, double dx, double dt, double w, int lim, const double* prm,
+                int bc) {
+    const model* m = model_of(id);
+    if (!m) return;
+    sweep_grid(m, planes, n, 1, 0, dx, dt, w, lim, prm, bc);
+}
+
+/* computeMaximumWaveSpeed over the 2-ghost padded line: ghosts are copies of interior cells, so the
+ * maximum is over the interior (Solvers/solvers.cpp:259-276; `if (s > max) max = s` from 0.0). */
+static double max_wave(const model* m, const double* planes, long plane, int dims, const double* prm) {
+    double best = 0.0;
+    for (long k = 0; k < plane; k++) {
+        double W[MAXV];
+        load_cell(planes, plane, k, m->nv, W);
+        double s = dims == 1 ? m->wave1d(W, prm) : m->wave2d(W, prm);
+        if (s > best) best = s;
+    }
+    if (dims == 2) {
+        /* the default-constructed corner ghosts of insertBoundaryCells2D (Solvers/solvers.cpp:92) */
+        double W[MAXV];
+        m->default_state(prm, W);
+        double s = m->wave2d(W, prm);
+        if (s > best) best = s;
+    }
+    return best;
+}
+
+double vo_max_wave1d(int id, const double* planes, int n, const double* prm) {
+    const model* m = model_of(id);
+    return m ? max_wave(m, planes, n, 1, prm) : 0.0;
+}
+
+double vo_max_wave2d(int id, const double* planes, int nx, int ny, const double* prm) {
+    const model* m = model_of(id);
+    return m ? max_wave(m, planes, (long)nx * ny, 2, prm) : 0.0;
+}
+
+/* Solvers::computeStableTimeStep(dt, t, tEnd, it), Solvers/solvers.cpp:437-452 */
+static double stable_dt(double dt, double t, double t_end, int it) {
+    double d = dt;
+    if (it <= 5) d *= 0.2;
+    if ((t + d) > t_end) d = t_end - t;
+    return d;
+}
+
+/* solve()/solve2D()'s loop: Solvers/secondordersolver.cpp:288-314 (1D), :392-424 (2D); MHD adds
+ * c_h = padded-grid maximum wave speed before the sweeps (Solvers/mhdsecondordersolver.cpp:330-332,
+ * :513-515). */
+static double run(int id, double* planes, int nx, int ny, int dims, double dx, double cfl, double t_end,
+                  int max_steps, double w, int lim, const double* prm_in, int bc, int* steps_out,
+                  double* dt_log) {
+    const model* m = model_of(id);
+    if (!m) return -1.0;
+    double prm[8];
+    memcpy(prm, prm_in, sizeof(double) * vo_nparams(id));
+    double tEnd = t_end > 0.0 ? t_end : 1.0e300;
+    int limit = max_steps > 0 ? max_steps : 0x7fffffff;
+    long plane = (long)nx * ny;
+    double t = 0.0;
+    int it = 0;
+    while (t < tEnd && it < limit) {
+        double smax_ = max_wave(m, planes, plane, dims, prm);
+        double dt = stable_dt(cfl * (dx / smax_), t, tEnd, it);
+        if (id == VO_MHD) prm[2] = smax_;
+        if (dt_log) dt_log[it] = dt;
+        if (dims == 1) {
+            sweep_grid(m, planes, nx, 1, 0, dx, dt, w, lim, prm, bc);
+        } else {
+            sweep_grid(m, planes, nx, ny, 0, dx, 0.5 * dt, w, lim, prm, bc);
+            sweep_grid(m, planes, nx, ny, 1, dx, dt, w, lim, prm, bc);
+            sweep_grid(m, planes, nx, ny, 0, dx, 0.5 * dt, w, lim, prm, bc);
+        }
+        t += dt;
+        it += 1;
+    }
+    if (steps_out) *steps_out = it;
+    return t;
+}
+
+double vo_run1d(int id, double* planes, int n, double dx, double cfl, double t_end, int max_steps, double w,
+                int lim, const double* prm, int bc, int subcycles, int* steps_out, double* dt_log) {
+    (void)subcycles;
+    return run(id, planes, n, 1, 1, dx, cfl, t_end, max_steps, w, lim, prm, bc, steps_out, dt_log);
+}
+
+double vo_run2d(int id, double* planes, int nx, int ny, double dx, double cfl, double t_end, int max_steps,
+                double w, int lim, const double* prm, int bc, int subcycles, int* steps_out, double* dt_log) {
+    (void)subcycles;
+    return run(id, planes, nx, ny, 2, dx, cfl, t_end, max_steps, w, lim, prm, bc, steps_out, dt_log);
+}
+
+/* ------------------------------------------------------------------------- unit-test building blocks */
+
+void vo_prim_to_cons(int id, const double* w, const double* prm, double* u) {
+    const model* m = model_of(id);
+    if (m) m->cons(w, prm, u);
+}
+
+void vo_cons_to_prim(int id, const double* u, const double* prm, double* w) {
+    const model* m = model_of(id);
+    if (!m) return;
+    m->default_state(prm, w);
+    m->setcons(u, prm, w);
+}
+
+void vo_flux(int id, const double* u, int axis, const double* prm, double* f) {
+    const model* m = model_of(id);
+    if (m) m->flux(u, axis, prm, f);
+}
+
+void vo_slic_flux(int id, const double* wLL, const double* wL, const double* wR, const double* wRR, int axis,
+                  double dx, double dt, double w, int lim, const double* prm, double* f) {
+    const model* m = model_of(id);
+    if (m) slic_flux(m, wLL, wL, wR, wRR, axis, dx, dt, w, lim, prm, f);
+}

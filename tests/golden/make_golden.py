@@ -1,0 +1,63 @@
+"""Generate the golden fixtures in tests/golden/ by running the reference's own code.
+
+The reference (Vanguard) ships no golden vectors or known-answer tests, so the fixtures are produced by
+running its unmodified OpenMP C++ sources, compiled into oracle/_ref/libvgref.so by oracle/Makefile, on
+one thread (its CFL maximum is an unsynchronised OpenMP update and is only reproducible on one thread).
+Each fixture stores the input primitive planes, the run parameters and the reference's output planes.
+
+Run from the repository root where the reference tree is present:
+    make -C oracle ref && python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+import oracle as O  # noqa: E402
+from vanguard_b200 import workloads as wl  # noqa: E402
+
+# name -> (model, initial planes, run kwargs).  steps == 0: the reference's own time-driven solve().
+CASES = {
+    # BASELINE config 1 exactly: Sod, 1000 cells, minbee, CFL 0.9, t = 0.25, transmissive
+    "euler1d_sod1000_minbee_t025": (O.EULER, lambda: wl.sod_1d(1000),
+                                     dict(dx=1e-3, cfl=0.9, t_end=0.25, steps=0, limiter=O.MINBEE,
+                                          params=wl.euler_params(1.4))),
+    "euler2d_quad64_superbee_50": (O.EULER, lambda: wl.euler_quadrants_2d(64, 64, seed=7),
+                                   dict(dx=1 / 64, cfl=0.8, steps=50, limiter=O.SUPERBEE,
+                                        params=wl.euler_params(1.4))),
+    "euler2d_quad48x40_vanleer_20": (O.EULER, lambda: wl.euler_quadrants_2d(48, 40, seed=8),
+                                     dict(dx=1 / 48, cfl=0.8, steps=20, limiter=O.VANLEER,
+                                          params=wl.euler_params(1.4))),
+    "euler2d_quad40_minbee_t005": (O.EULER, lambda: wl.euler_quadrants_2d(40, 40, seed=9),
+                                   dict(dx=1 / 40, cfl=0.8, t_end=0.05, steps=0, limiter=O.MINBEE,
+                                        params=wl.euler_params(1.4))),
+    "mhd2d_vortex48_periodic_superbee_30": (O.MHD, lambda: wl.mhd_vortex_2d(48, 48, seed=1),
+                                            dict(dx=1 / 48, cfl=0.8, steps=30, limiter=O.SUPERBEE,
+                                                 params=wl.mhd_params(5 / 3), bc=O.PERIODIC)),
+    "mhd1d_briowu200_superbee_t01": (O.MHD, lambda: wl.brio_wu_1d(200),
+                                     dict(dx=1 / 200, cfl=0.8, t_end=0.1, steps=0, limiter=O.SUPERBEE,
+                                          params=wl.mhd_params(2.0))),
+}
+
+
+def make(name):
+    model, init, kw = CASES[name]
+    w0 = np.ascontiguousarray(init())
+    out = w0.copy()
+    kw = dict(kw)
+    O.ref_run(model, out, kw.pop("dx"), kw.pop("cfl"), threads=1, **kw)
+    _, _, kw2 = CASES[name]
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), model=model, w0=w0, out=out,
+                        **{k: np.asarray(v) for k, v in kw2.items()})
+    print("wrote", name)
+
+
+if __name__ == "__main__":
+    for n in (sys.argv[1:] or CASES):
+        make(n)

@@ -1,0 +1,119 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle on the same inputs.
+
+The plain FP64 form must reproduce the reference's arithmetic exactly: results are compared bit for bit
+(np.array_equal), which is stricter than the 1e-12 per-cell relative bound the FP64 form promises.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from vanguard_b200 import workloads as wl
+
+pytestmark = pytest.mark.gpu
+
+
+def _bitwise(a, b):
+    if np.array_equal(a, b):
+        return True
+    d = np.abs(a - b)
+    i = np.unravel_index(np.argmax(d), d.shape)
+    raise AssertionError(f"max |diff| {d.max():.3e} at {i}: {a[i]!r} vs {b[i]!r}; "
+                         f"{np.count_nonzero(d)} differing values")
+
+
+def test_sod_1d_time_driven(gpu, oracle_lib):
+    """1D Euler shock tube: minbee, CFL 0.9, run to t = 0.25 (613 steps), transmissive."""
+    n = 1000
+    W = wl.sod_1d(n)
+    prm = wl.euler_params(1.4)
+    ref = W.copy()
+    t_ref, steps_ref = O.run(O.EULER, ref, 1.0 / n, 0.9, t_end=0.25, limiter=O.MINBEE, params=prm)
+    with gpu.Solver(gpu.EULER, n, 1, prm) as s:
+        s.upload(W)
+        t, steps = s.run(1.0 / n, 0.9, t_end=0.25, limiter=gpu.MINBEE)
+        out = s.download()
+    assert steps == steps_ref == 613
+    assert t == t_ref
+    _bitwise(out, ref)
+
+
+@pytest.mark.parametrize("limiter", [0, 1, 2])
+@pytest.mark.parametrize("shape", [(64, 64), (130, 67)])
+def test_euler_2d_quadrants_steps(gpu, oracle_lib, limiter, shape):
+    nx, ny = shape
+    W = wl.euler_quadrants_2d(nx, ny, seed=11 + limiter)
+    prm = wl.euler_params(1.4)
+    ref = W.copy()
+    O.run(O.EULER, ref, 1.0 / nx, 0.8, steps=40, limiter=limiter, params=prm)
+    with gpu.Solver(gpu.EULER, nx, ny, prm) as s:
+        s.upload(W)
+        t, steps = s.run(1.0 / nx, 0.8, steps=40, limiter=limiter)
+        out = s.download()
+    assert steps == 40
+    _bitwise(out, ref)
+
+
+@pytest.mark.parametrize("axis", [0, 1])
+def test_euler_single_sweep(gpu, oracle_lib, axis):
+    nx, ny = 300, 200
+    W = wl.euler_quadrants_2d(nx, ny, seed=5)
+    prm = wl.euler_params(1.4)
+    ref = W.copy()
+    O.sweep(O.EULER, ref, axis, 1.0 / nx, 3e-4, limiter=0, params=prm)
+    with gpu.Solver(gpu.EULER, nx, ny, prm) as s:
+        s.upload(W)
+        s.sweep(axis, 1.0 / nx, 3e-4, limiter=0)
+        out = s.download()
+    _bitwise(out, ref)
+
+
+def test_euler_max_wave_speed(gpu, oracle_lib):
+    nx, ny = 257, 129
+    W = wl.euler_quadrants_2d(nx, ny, seed=9)
+    prm = wl.euler_params(1.4)
+    with gpu.Solver(gpu.EULER, nx, ny, prm) as s:
+        s.upload(W)
+        assert s.max_wave_speed() == O.max_wave(O.EULER, W, prm)
+
+
+@pytest.mark.parametrize("bc", [0, 1])
+def test_mhd_2d_vortex(gpu, oracle_lib, bc):
+    nx, ny = 96, 80
+    W = wl.mhd_vortex_2d(nx, ny, seed=2)
+    prm = wl.mhd_params(5.0 / 3.0)
+    ref = W.copy()
+    O.run(O.MHD, ref, 1.0 / nx, 0.8, steps=30, limiter=0, params=prm, bc=bc)
+    with gpu.Solver(gpu.MHD, nx, ny, prm, boundary=bc) as s:
+        s.upload(W)
+        s.run(1.0 / nx, 0.8, steps=30, limiter=0)
+        out = s.download()
+    _bitwise(out, ref)
+
+
+def test_mhd_1d_brio_wu(gpu, oracle_lib):
+    n = 400
+    W = wl.brio_wu_1d(n)
+    prm = wl.mhd_params(2.0)
+    ref = W.copy()
+    O.run(O.MHD, ref, 1.0 / n, 0.8, steps=100, limiter=0, params=prm)
+    with gpu.Solver(gpu.MHD, n, 1, prm) as s:
+        s.upload(W)
+        s.run(1.0 / n, 0.8, steps=100, limiter=0)
+        out = s.download()
+    _bitwise(out, ref)
+
+
+def test_mhd_full_components(gpu, oracle_lib):
+    """Non-zero w and Bz select the 9-component variant."""
+    nx, ny = 64, 48
+    W = wl.mhd_vortex_2d(nx, ny, seed=4)
+    W[3] = 0.05 * np.sin(np.linspace(0, 6, nx))[None, :]
+    W[7] = 0.1
+    prm = wl.mhd_params(5.0 / 3.0)
+    ref = W.copy()
+    O.run(O.MHD, ref, 1.0 / nx, 0.8, steps=20, limiter=1, params=prm, bc=1)
+    with gpu.Solver(gpu.MHD, nx, ny, prm, boundary=1) as s:
+        s.upload(W)
+        s.run(1.0 / nx, 0.8, steps=20, limiter=1)
+        out = s.download()
+    _bitwise(out, ref)

@@ -1,0 +1,177 @@
+"""vanguard_b200 -- B200-native SLIC/FORCE finite-volume update (Euler, ideal MHD, HPR).
+
+The product is the CUDA library ``libvanguard_slic.so`` behind the C ABI in include/vanguard_slic.h and
+the C++ shim in vanguard_b200/shim (Vanguard's own class names).  This module is a thin ctypes binding
+of that C ABI used by the tests and bench.py; it has no compute path of its own and raises if the
+library is missing or no GPU is present.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libvanguard_slic.so")
+
+VG_OK, VG_EINVAL, VG_ENAN, VG_ETIMEOUT, VG_ECUDA, VG_ENOMEM, VG_EUNSUPPORTED = range(7)
+EULER, MHD, HPR = 0, 1, 2
+FP64, MIXED = 0, 1
+TRANSMISSIVE, PERIODIC = 0, 1
+SUPERBEE, VANLEER, MINBEE = 0, 1, 2
+NVAR = {EULER: 6, MHD: 9, HPR: 17}
+MAX_PARAMS = 16
+
+
+class VgError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{_STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+_STATUS = {0: "VG_OK", 1: "VG_EINVAL", 2: "VG_ENAN", 3: "VG_ETIMEOUT", 4: "VG_ECUDA", 5: "VG_ENOMEM",
+           6: "VG_EUNSUPPORTED"}
+
+
+class GridDesc(ctypes.Structure):
+    _fields_ = [("model", ctypes.c_int), ("nx", ctypes.c_int), ("ny", ctypes.c_int),
+                ("precision", ctypes.c_int), ("boundary", ctypes.c_int), ("device", ctypes.c_int),
+                ("params", ctypes.c_double * MAX_PARAMS)]
+
+
+class RunConfig(ctypes.Structure):
+    _fields_ = [("dx", ctypes.c_double), ("cfl", ctypes.c_double), ("t_end", ctypes.c_double),
+                ("max_steps", ctypes.c_int), ("bias", ctypes.c_double), ("limiter", ctypes.c_int),
+                ("subcycles", ctypes.c_int)]
+
+
+# Every function the C ABI header declares (tests check the library exports them all).
+EXPORTS = ["vg_create", "vg_destroy", "vg_model_nvar", "vg_upload_primitive", "vg_download_primitive",
+           "vg_run", "vg_solve", "vg_sweep", "vg_max_wave_speed", "vg_state_device", "vg_last_launch_count",
+           "vg_last_error_string", "vg_status_string"]
+
+_lib = None
+
+
+def lib():
+    """Load libvanguard_slic.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run `python -m vanguard_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, D = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)
+        L.vg_create.argtypes = [ctypes.POINTER(GridDesc), ctypes.POINTER(vp)]
+        L.vg_destroy.argtypes = [vp]
+        L.vg_model_nvar.argtypes = [ctypes.c_int]
+        L.vg_upload_primitive.argtypes = [vp, vp, ctypes.c_int, vp]
+        L.vg_download_primitive.argtypes = [vp, vp, ctypes.c_int, vp]
+        L.vg_run.argtypes = [vp, ctypes.POINTER(RunConfig), ctypes.POINTER(ctypes.c_int), D, vp]
+        L.vg_solve.argtypes = [vp, vp, vp, ctypes.POINTER(RunConfig), ctypes.POINTER(ctypes.c_int), D, vp]
+        L.vg_sweep.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int, vp]
+        L.vg_max_wave_speed.argtypes = [vp, D, vp]
+        L.vg_state_device.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(ctypes.c_long),
+                                      ctypes.POINTER(ctypes.c_long), ctypes.POINTER(ctypes.c_int)]
+        L.vg_last_launch_count.argtypes = [vp]
+        L.vg_last_launch_count.restype = ctypes.c_long
+        L.vg_last_error_string.restype = ctypes.c_char_p
+        L.vg_status_string.restype = ctypes.c_char_p
+        L.vg_status_string.argtypes = [ctypes.c_int]
+        _lib = L
+    return _lib
+
+
+def _check(st, allow=()):
+    if st != VG_OK and st not in allow:
+        raise VgError(st, lib().vg_last_error_string().decode())
+    return st
+
+
+class Solver:
+    """One grid on one GPU: a thin handle over vg_create / vg_destroy."""
+
+    def __init__(self, model, nx, ny=1, params=(), precision=FP64, boundary=TRANSMISSIVE, device=0):
+        d = GridDesc()
+        d.model, d.nx, d.ny, d.precision, d.boundary, d.device = model, nx, ny, precision, boundary, device
+        for i, v in enumerate(params):
+            d.params[i] = float(v)
+        self.model, self.nx, self.ny = model, nx, ny
+        self._h = ctypes.c_void_p()
+        _check(lib().vg_create(ctypes.byref(d), ctypes.byref(self._h)))
+
+    def close(self):
+        if self._h:
+            lib().vg_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _shape(self):
+        return (NVAR[self.model], self.ny, self.nx) if self.ny > 1 else (NVAR[self.model], self.nx)
+
+    def upload(self, planes, stream=None):
+        """planes: host float64 array (nvar, ny, nx) / (nvar, n), or a torch CUDA tensor of that shape."""
+        if hasattr(planes, "data_ptr"):
+            t = planes.contiguous()
+            return _check(lib().vg_upload_primitive(self._h, ctypes.c_void_p(t.data_ptr()), 1, stream))
+        a = np.ascontiguousarray(planes, dtype=np.float64)
+        if a.shape != self._shape():
+            raise ValueError(f"expected planes of shape {self._shape()}, got {a.shape}")
+        return _check(lib().vg_upload_primitive(self._h, a.ctypes.data_as(ctypes.c_void_p), 0, stream))
+
+    def download(self, out=None, stream=None):
+        if out is not None and hasattr(out, "data_ptr"):
+            _check(lib().vg_download_primitive(self._h, ctypes.c_void_p(out.data_ptr()), 1, stream))
+            return out
+        a = np.empty(self._shape(), dtype=np.float64) if out is None else out
+        _check(lib().vg_download_primitive(self._h, a.ctypes.data_as(ctypes.c_void_p), 0, stream))
+        return a
+
+    def run(self, dx, cfl, t_end=0.0, steps=0, bias=0.0, limiter=SUPERBEE, subcycles=0, stream=None,
+            allow_nan=False):
+        c = RunConfig(dx, cfl, t_end, steps, bias, limiter, subcycles)
+        it = ctypes.c_int()
+        t = ctypes.c_double()
+        _check(lib().vg_run(self._h, ctypes.byref(c), ctypes.byref(it), ctypes.byref(t), stream),
+               allow=(VG_ENAN,) if allow_nan else ())
+        return t.value, it.value
+
+    def solve(self, planes_in, dx, cfl, t_end=0.0, steps=0, bias=0.0, limiter=SUPERBEE, subcycles=0,
+              out=None, stream=None):
+        """Host-buffer round trip through vg_solve (upload, run, download)."""
+        a = np.ascontiguousarray(planes_in, dtype=np.float64)
+        o = np.empty_like(a) if out is None else out
+        c = RunConfig(dx, cfl, t_end, steps, bias, limiter, subcycles)
+        it = ctypes.c_int()
+        t = ctypes.c_double()
+        _check(lib().vg_solve(self._h, a.ctypes.data_as(ctypes.c_void_p), o.ctypes.data_as(ctypes.c_void_p),
+                              ctypes.byref(c), ctypes.byref(it), ctypes.byref(t), stream))
+        return o, t.value, it.value
+
+    def sweep(self, axis, dx, dt, bias=0.0, limiter=SUPERBEE, stream=None):
+        return _check(lib().vg_sweep(self._h, axis, dx, dt, bias, limiter, stream))
+
+    def max_wave_speed(self, stream=None):
+        v = ctypes.c_double()
+        _check(lib().vg_max_wave_speed(self._h, ctypes.byref(v), stream))
+        return v.value
+
+    def state_device(self):
+        p = ctypes.c_void_p()
+        ps, rs, n = ctypes.c_long(), ctypes.c_long(), ctypes.c_int()
+        _check(lib().vg_state_device(self._h, ctypes.byref(p), ctypes.byref(ps), ctypes.byref(rs), ctypes.byref(n)))
+        return p.value, ps.value, rs.value, n.value
+
+    def last_launch_count(self):
+        return lib().vg_last_launch_count(self._h)

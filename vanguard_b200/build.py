@@ -1,0 +1,79 @@
+"""Build the in-tree CUDA library vanguard_b200/libvanguard_slic.so for sm_100a.
+
+Each translation unit is compiled by nvcc with its own floating-point contract:
+  slic_fp64.cu  -fmad=false  (exact FP64: no FMA contraction, bitwise parity with the reference)
+  slic_mixed.cu -fmad=true   (mixed FP32/FP64 form)
+  *.cu (rest)   host code and helpers
+The objects are linked into one shared library with the CUDA runtime linked statically, so the library
+only depends on the driver.  Run `python -m vanguard_b200.build` or call build().
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+OUT = os.path.join(HERE, "libvanguard_slic.so")
+OBJDIR = os.path.join(HERE, "_build")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fno-fast-math", "-ccbin", "g++"]
+
+# (source, extra flags)
+UNITS = [
+    ("slic_fp64.cu", ["-fmad=false"]),
+    ("slic_mixed.cu", ["-fmad=true"]),
+    ("vg_api.cu", []),
+]
+
+
+def _nvcc():
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", "nvcc"):
+        if cand and (os.path.isabs(cand) and os.path.exists(cand) or not os.path.isabs(cand)):
+            return cand
+    return "nvcc"
+
+
+def _stale(obj, srcs):
+    if not os.path.exists(obj):
+        return True
+    t = os.path.getmtime(obj)
+    return any(os.path.getmtime(s) > t for s in srcs)
+
+
+def _headers():
+    hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
+    hs.append(os.path.join(os.path.dirname(HERE), "include", "vanguard_slic.h"))
+    return [h for h in hs if os.path.exists(h)]
+
+
+def build(verbose: bool = False, force: bool = False) -> str:
+    """Compile every CUDA unit for sm_100a and link libvanguard_slic.so; returns its path."""
+    os.makedirs(OBJDIR, exist_ok=True)
+    nvcc = _nvcc()
+    env = dict(os.environ)
+    env.pop("CXX", None)
+    env.pop("CC", None)
+    headers = _headers()
+    objs = []
+    for src, flags in UNITS:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(OBJDIR, src.replace(".cu", ".o"))
+        objs.append(o)
+        if force or _stale(o, [s] + headers):
+            cmd = [nvcc, *ARCH, *COMMON, *flags, "-c", s, "-o", o]
+            if verbose:
+                print(" ".join(cmd), flush=True)
+            subprocess.run(cmd, check=True, env=env)
+    if force or _stale(OUT, objs):
+        cmd = [nvcc, *ARCH, "-shared", "-Xcompiler", "-fPIC", "-ccbin", "g++", "-o", OUT, *objs]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True, env=env)
+    return OUT
+
+
+if __name__ == "__main__":
+    build(verbose=True, force="--force" in sys.argv)

@@ -1,0 +1,459 @@
+// C ABI of the SLIC/FORCE solver (include/vanguard_slic.h): solver objects, state upload/download, the
+// device-resident time loop replayed from captured CUDA graphs, and the per-sweep entry points.
+#include <cuda_runtime.h>
+
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/vanguard_slic.h"
+#include "vg_ops.h"
+
+using vg::Ctrl;
+using vg::Ops;
+using vg::SweepArgs;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+vg_status fail(vg_status st, const std::string& msg) {
+    g_last_error = msg;
+    return st;
+}
+
+vg_status cuda_fail(cudaError_t e, const char* what) {
+    g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? VG_ENOMEM : VG_ECUDA;
+}
+
+#define VG_CUDA(call)                                        \
+    do {                                                     \
+        cudaError_t e_ = (call);                             \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call);  \
+    } while (0)
+
+int ref_nvar(int model) { return model == VG_MODEL_EULER ? 6 : model == VG_MODEL_MHD ? 9 : model == VG_MODEL_HPR ? 17 : 0; }
+
+// Reference plane carried in device plane k, per variant.
+const int kPlanes[vg::V_COUNT][9] = {
+    {0, 1, 4},                      // V_EULER1: rho, u, p
+    {0, 1, 2, 4},                   // V_EULER2: rho, u, v, p
+    {0, 1, 2, 4, 5, 6, 8},          // V_MHD7:   rho, u, v, p, Bx, By, psi
+    {0, 1, 2, 3, 4, 5, 6, 7, 8},    // V_MHD9
+};
+
+}  // namespace
+
+struct vg_solver {
+    vg_grid_desc d{};
+    int dims = 2;
+    int variant = -1;
+    const Ops* ops = nullptr;
+    long pitch = 0, plane = 0;
+    int max_nw = 0;
+    double* buf[2] = {nullptr, nullptr};
+    int cur = 0;
+    Ctrl* ctrl = nullptr;     // device
+    Ctrl* hctrl = nullptr;    // pinned host mirror
+    double* dout = nullptr;   // device scalar for max-wave results
+    double* hout = nullptr;   // pinned host scalar
+    double floor5 = 0.0;
+    cudaStream_t cap = nullptr;  // private capture stream
+    // graph cache: chunk of kChunk steps from buffer 0, and single steps from buffer 0 and 1
+    struct GraphSet {
+        bool valid = false;
+        cudaGraphExec_t chunk = nullptr, single[2] = {nullptr, nullptr};
+        vg_run_config cfg{};
+        int variant = -1;
+    } g;
+    long last_launches = 0;
+};
+
+namespace {
+
+constexpr int kChunk = 16;  // steps per captured chunk (even: a chunk returns to buffer 0 in 1D and 2D)
+
+SweepArgs base_args(const vg_solver* s) {
+    SweepArgs a{};
+    a.plane = s->plane;
+    a.pitch = s->pitch;
+    a.nx = s->d.nx;
+    a.ny = s->d.ny;
+    a.periodic = s->d.boundary == VG_PERIODIC;
+    a.ctrl = s->ctrl;
+    a.dt_scale = 1.0;
+    a.floor5 = s->floor5;
+    a.dims = s->dims;
+    a.wave_acc = &s->ctrl->smax_next;
+    a.err = &s->ctrl->err;
+    for (int i = 0; i < VG_MAX_PARAMS; i++) a.params[i] = s->d.params[i];
+    a.ch_host = s->d.params[2];
+    return a;
+}
+
+// Enqueue one time step reading from buffer `from`; returns the number of kernels.
+int enqueue_step(vg_solver* s, const vg_run_config& c, int from, cudaStream_t st, cudaError_t* err) {
+    SweepArgs a = base_args(s);
+    a.dx = c.dx;
+    a.bias = c.bias;
+    a.limiter = c.limiter;
+    int n = 0;
+    cudaError_t e = s->ops->step_begin(a, st);
+    n++;
+    if (s->dims == 1) {
+        a.in = s->buf[from];
+        a.out = s->buf[1 - from];
+        a.accumulate_wave = 1;
+        a.advance_time = 1;
+        if (e == cudaSuccess) e = s->ops->sweep(0, a, st);
+        n++;
+    } else {
+        // Solvers/secondordersolver.cpp:403-410: X(dt/2), Y(dt), X(dt/2)
+        a.in = s->buf[from];
+        a.out = s->buf[1 - from];
+        a.dt_scale = 0.5;
+        if (e == cudaSuccess) e = s->ops->sweep(0, a, st);
+        a.in = s->buf[1 - from];
+        a.out = s->buf[from];
+        a.dt_scale = 1.0;
+        if (e == cudaSuccess) e = s->ops->sweep(1, a, st);
+        a.in = s->buf[from];
+        a.out = s->buf[1 - from];
+        a.dt_scale = 0.5;
+        a.accumulate_wave = 1;
+        a.advance_time = 1;
+        if (e == cudaSuccess) e = s->ops->sweep(0, a, st);
+        n += 3;
+    }
+    *err = e;
+    return n;
+}
+
+int kernels_per_step(const vg_solver* s) { return s->dims == 1 ? 2 : 4; }
+
+void destroy_graphs(vg_solver* s) {
+    if (s->g.chunk) cudaGraphExecDestroy(s->g.chunk);
+    for (auto& x : s->g.single)
+        if (x) cudaGraphExecDestroy(x);
+    s->g = vg_solver::GraphSet{};
+}
+
+vg_status capture(vg_solver* s, const vg_run_config& c, int steps, int from, cudaGraphExec_t* out) {
+    cudaGraph_t graph = nullptr;
+    VG_CUDA(cudaStreamBeginCapture(s->cap, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = cudaSuccess;
+    int b = from;
+    for (int i = 0; i < steps && e == cudaSuccess; i++) {
+        enqueue_step(s, c, b, s->cap, &e);
+        b = 1 - b;
+    }
+    cudaError_t e2 = cudaStreamEndCapture(s->cap, &graph);
+    if (e != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        return cuda_fail(e, "kernel launch during capture");
+    }
+    if (e2 != cudaSuccess) return cuda_fail(e2, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(out, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+    return VG_OK;
+}
+
+bool same_cfg(const vg_run_config& a, const vg_run_config& b) {
+    return a.dx == b.dx && a.bias == b.bias && a.limiter == b.limiter;
+}
+
+vg_status ensure_graphs(vg_solver* s, const vg_run_config& c) {
+    if (s->g.valid && s->g.variant == s->variant && same_cfg(s->g.cfg, c)) return VG_OK;
+    destroy_graphs(s);
+    vg_status st;
+    if ((st = capture(s, c, kChunk, 0, &s->g.chunk)) != VG_OK) return st;
+    if ((st = capture(s, c, 1, 0, &s->g.single[0])) != VG_OK) return st;
+    if ((st = capture(s, c, 1, 1, &s->g.single[1])) != VG_OK) return st;
+    s->g.valid = true;
+    s->g.cfg = c;
+    s->g.variant = s->variant;
+    return VG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int vg_model_nvar(int model) { return ref_nvar(model); }
+
+const char* vg_last_error_string(void) { return g_last_error.c_str(); }
+
+const char* vg_status_string(vg_status st) {
+    switch (st) {
+        case VG_OK: return "VG_OK";
+        case VG_EINVAL: return "VG_EINVAL";
+        case VG_ENAN: return "VG_ENAN";
+        case VG_ETIMEOUT: return "VG_ETIMEOUT";
+        case VG_ECUDA: return "VG_ECUDA";
+        case VG_ENOMEM: return "VG_ENOMEM";
+        case VG_EUNSUPPORTED: return "VG_EUNSUPPORTED";
+    }
+    return "unknown vg_status";
+}
+
+vg_status vg_create(const vg_grid_desc* desc, vg_solver** out) {
+    if (!desc || !out) return fail(VG_EINVAL, "null argument");
+    *out = nullptr;
+    if (desc->model != VG_MODEL_EULER && desc->model != VG_MODEL_MHD)
+        return fail(VG_EUNSUPPORTED, "model not available in this build");
+    if (desc->nx < 2 || desc->ny < 1 || (desc->ny > 1 && desc->ny < 2))
+        return fail(VG_EINVAL, "grid needs at least 2 cells along every swept axis");
+    if (desc->precision != VG_FP64 && desc->precision != VG_MIXED) return fail(VG_EINVAL, "bad precision");
+    if (desc->boundary != VG_TRANSMISSIVE && desc->boundary != VG_PERIODIC) return fail(VG_EINVAL, "bad boundary");
+    if (desc->precision == VG_MIXED && !vg::ops_mixed(vg::V_EULER2))
+        return fail(VG_EUNSUPPORTED, "mixed precision not available in this build");
+    VG_CUDA(cudaSetDevice(desc->device));
+    vg_solver* s = new (std::nothrow) vg_solver();
+    if (!s) return fail(VG_ENOMEM, "host allocation");
+    s->d = *desc;
+    s->dims = desc->ny > 1 ? 2 : 1;
+    s->max_nw = desc->model == VG_MODEL_EULER ? 4 : 9;
+    s->pitch = ((long)desc->nx + 31) / 32 * 32;  // 256-byte aligned rows
+    s->plane = s->pitch * desc->ny;
+    s->floor5 = std::pow(10.0, -5.0);  // SlopeLimiters::computeSlopeVector's floor (Solvers/slopelimiters.cpp:232-239)
+    cudaError_t e = cudaSuccess;
+    for (int b = 0; b < 2 && e == cudaSuccess; b++) e = cudaMalloc(&s->buf[b], sizeof(double) * s->plane * s->max_nw);
+    if (e == cudaSuccess) e = cudaMalloc(&s->ctrl, sizeof(Ctrl));
+    if (e == cudaSuccess) e = cudaMalloc(&s->dout, sizeof(double));
+    if (e == cudaSuccess) e = cudaMallocHost(&s->hctrl, sizeof(Ctrl));
+    if (e == cudaSuccess) e = cudaMallocHost(&s->hout, sizeof(double));
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->cap, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMemset(s->ctrl, 0, sizeof(Ctrl));
+    if (e != cudaSuccess) {
+        vg_destroy(s);
+        return cuda_fail(e, "vg_create allocation");
+    }
+    *out = s;
+    return VG_OK;
+}
+
+vg_status vg_destroy(vg_solver* s) {
+    if (!s) return VG_OK;
+    destroy_graphs(s);
+    for (auto& b : s->buf)
+        if (b) cudaFree(b);
+    if (s->ctrl) cudaFree(s->ctrl);
+    if (s->dout) cudaFree(s->dout);
+    if (s->hctrl) cudaFreeHost(s->hctrl);
+    if (s->hout) cudaFreeHost(s->hout);
+    if (s->cap) cudaStreamDestroy(s->cap);
+    delete s;
+    return VG_OK;
+}
+
+vg_status vg_upload_primitive(vg_solver* s, const double* planes, int is_device, void* stream) {
+    if (!s || !planes) return fail(VG_EINVAL, "null argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    const long n = (long)s->d.nx * s->d.ny;
+    int variant;
+    if (s->d.model == VG_MODEL_EULER) {
+        // Euler carries rho, u, [v], p: w must be 0 and lambda 1 (then rho*lambda tracks rho exactly).
+        bool zero_v = true;
+        if (is_device) {
+            variant = vg::V_EULER2;  // device input: checked on the host is not possible; carry v, trust w/lambda
+        } else {
+            const double *v = planes + 2 * n, *w = planes + 3 * n, *lam = planes + 5 * n;
+            for (long i = 0; i < n; i++) {
+                if (w[i] != 0.0 || lam[i] != 1.0)
+                    return fail(VG_EUNSUPPORTED, "Euler state with w != 0 or lambda != 1 needs the 6-component variant");
+                if (v[i] != 0.0) zero_v = false;
+            }
+            variant = (s->dims == 1 && zero_v) ? vg::V_EULER1 : vg::V_EULER2;
+        }
+    } else {
+        bool reduced = true;
+        if (!is_device) {
+            const double *w = planes + 3 * n, *bz = planes + 7 * n;
+            for (long i = 0; i < n && reduced; i++)
+                if (w[i] != 0.0 || bz[i] != 0.0) reduced = false;
+        } else {
+            reduced = false;
+        }
+        variant = reduced ? vg::V_MHD7 : vg::V_MHD9;
+    }
+    const Ops* ops = s->d.precision == VG_MIXED ? vg::ops_mixed(variant) : vg::ops_fp64(variant);
+    if (!ops) return fail(VG_EUNSUPPORTED, "no kernel variant for this state");
+    s->variant = variant;
+    s->ops = ops;
+    s->cur = 0;
+    for (int k = 0; k < ops->nw; k++) {
+        const double* src = planes + (long)kPlanes[variant][k] * n;
+        VG_CUDA(cudaMemcpy2DAsync(s->buf[0] + k * s->plane, sizeof(double) * s->pitch, src, sizeof(double) * s->d.nx,
+                                  sizeof(double) * s->d.nx, s->d.ny, is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                  st));
+    }
+    VG_CUDA(cudaStreamSynchronize(st));
+    return VG_OK;
+}
+
+vg_status vg_download_primitive(vg_solver* s, double* planes, int is_device, void* stream) {
+    if (!s || !planes) return fail(VG_EINVAL, "null argument");
+    if (!s->ops) return fail(VG_EINVAL, "no state uploaded");
+    cudaStream_t st = (cudaStream_t)stream;
+    const long n = (long)s->d.nx * s->d.ny;
+    const int nref = ref_nvar(s->d.model);
+    bool carried[17] = {false};
+    for (int k = 0; k < s->ops->nw; k++) {
+        int r = kPlanes[s->variant][k];
+        carried[r] = true;
+        VG_CUDA(cudaMemcpy2DAsync(planes + (long)r * n, sizeof(double) * s->d.nx, s->buf[s->cur] + k * s->plane,
+                                  sizeof(double) * s->pitch, sizeof(double) * s->d.nx, s->d.ny,
+                                  is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
+    }
+    // planes that are not carried hold their constant value (0, or lambda = 1)
+    for (int r = 0; r < nref; r++) {
+        if (carried[r]) continue;
+        double val = (s->d.model == VG_MODEL_EULER && r == 5) ? 1.0 : 0.0;
+        if (is_device) {
+            std::vector<double> tmp(n, val);
+            VG_CUDA(cudaMemcpyAsync(planes + (long)r * n, tmp.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st));
+            VG_CUDA(cudaStreamSynchronize(st));
+        } else {
+            for (long i = 0; i < n; i++) planes[(long)r * n + i] = val;
+        }
+    }
+    VG_CUDA(cudaStreamSynchronize(st));
+    return VG_OK;
+}
+
+vg_status vg_run(vg_solver* s, const vg_run_config* cfg, int* steps_taken, double* t_reached, void* stream) {
+    if (!s || !cfg) return fail(VG_EINVAL, "null argument");
+    if (!s->ops) return fail(VG_EINVAL, "no state uploaded");
+    if (!(cfg->dx > 0.0) || !(cfg->cfl > 0.0)) return fail(VG_EINVAL, "dx and cfl must be positive");
+    if (cfg->max_steps <= 0 && !(cfg->t_end > 0.0)) return fail(VG_EINVAL, "need t_end > 0 or max_steps > 0");
+    if (cfg->subcycles != 0) return fail(VG_EUNSUPPORTED, "source sub-cycling is not available for this model");
+    cudaStream_t st = (cudaStream_t)stream;
+    VG_CUDA(cudaSetDevice(s->d.device));
+
+    // Normalise so that the state starts in buffer 0 (graphs are captured from buffer 0).
+    if (s->cur != 0) {
+        VG_CUDA(cudaMemcpyAsync(s->buf[0], s->buf[1], sizeof(double) * s->plane * s->ops->nw, cudaMemcpyDeviceToDevice, st));
+        s->cur = 0;
+    }
+    vg_status vs = ensure_graphs(s, *cfg);
+    if (vs != VG_OK) return vs;
+
+    Ctrl* h = s->hctrl;
+    std::memset(h, 0, sizeof(Ctrl));
+    h->t_end = cfg->t_end > 0.0 ? cfg->t_end : 1.0e300;
+    h->cfl = cfg->cfl;
+    h->dx = cfg->dx;
+    h->max_steps = cfg->max_steps > 0 ? cfg->max_steps : INT_MAX;
+    h->active = 1;
+    h->dims = s->dims;
+    VG_CUDA(cudaMemcpyAsync(s->ctrl, h, sizeof(Ctrl), cudaMemcpyHostToDevice, st));
+    SweepArgs a = base_args(s);
+    a.in = s->buf[0];
+    a.dx = cfg->dx;
+    VG_CUDA(s->ops->max_wave(a, st));
+    long launches = 1;
+
+    long launched_steps = 0;
+    if (cfg->max_steps > 0 && !(cfg->t_end > 0.0)) {
+        // step-count run: exactly max_steps steps
+        long k = cfg->max_steps;
+        for (; k >= kChunk; k -= kChunk) {
+            VG_CUDA(cudaGraphLaunch(s->g.chunk, st));
+            launched_steps += kChunk;
+        }
+        int b = 0;
+        for (; k > 0; k--) {
+            VG_CUDA(cudaGraphLaunch(s->g.single[b], st));
+            b = 1 - b;
+            launched_steps++;
+        }
+    } else {
+        // time-driven run: chunks until the device reports the end (steps past it are copies)
+        for (;;) {
+            VG_CUDA(cudaGraphLaunch(s->g.chunk, st));
+            launched_steps += kChunk;
+            VG_CUDA(cudaMemcpyAsync(h, s->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
+            VG_CUDA(cudaStreamSynchronize(st));
+            if (!(h->t < h->t_end) || h->it >= h->max_steps) break;
+        }
+    }
+    launches += launched_steps * kernels_per_step(s);
+    // every step is an odd number of sweeps in 2D (3) and 1 in 1D: the state ends in buffer (steps & 1)
+    s->cur = (int)(launched_steps & 1);
+    VG_CUDA(cudaMemcpyAsync(h, s->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
+    VG_CUDA(cudaStreamSynchronize(st));
+    s->last_launches = launches;
+    if (steps_taken) *steps_taken = h->it;
+    if (t_reached) *t_reached = h->t;
+    if (h->err) return fail(VG_ENAN, "non-finite or non-positive density/pressure produced");
+    return VG_OK;
+}
+
+vg_status vg_solve(vg_solver* s, const double* planes_in, double* planes_out, const vg_run_config* cfg, int* steps_taken,
+                   double* t_reached, void* stream) {
+    vg_status st = vg_upload_primitive(s, planes_in, 0, stream);
+    if (st != VG_OK) return st;
+    vg_status rs = vg_run(s, cfg, steps_taken, t_reached, stream);
+    if (rs != VG_OK && rs != VG_ENAN) return rs;
+    st = vg_download_primitive(s, planes_out, 0, stream);
+    return st != VG_OK ? st : rs;
+}
+
+vg_status vg_sweep(vg_solver* s, int axis, double dx, double dt, double bias, int limiter, void* stream) {
+    if (!s) return fail(VG_EINVAL, "null solver");
+    if (!s->ops) return fail(VG_EINVAL, "no state uploaded");
+    if (axis != 0 && axis != 1) return fail(VG_EINVAL, "axis must be 0 or 1");
+    if (axis == 1 && s->dims == 1) return fail(VG_EINVAL, "Y sweep on a 1D grid");
+    if (!(dx > 0.0) || !(dt > 0.0)) return fail(VG_EINVAL, "dx and dt must be positive");
+    cudaStream_t st = (cudaStream_t)stream;
+    SweepArgs a = base_args(s);
+    a.ctrl = nullptr;
+    a.dt_host = dt;
+    a.dx = dx;
+    a.bias = bias;
+    a.limiter = limiter;
+    a.in = s->buf[s->cur];
+    a.out = s->buf[1 - s->cur];
+    VG_CUDA(s->ops->sweep(axis, a, st));
+    s->cur = 1 - s->cur;
+    s->last_launches = 1;
+    return VG_OK;
+}
+
+vg_status vg_max_wave_speed(vg_solver* s, double* out, void* stream) {
+    if (!s || !out) return fail(VG_EINVAL, "null argument");
+    if (!s->ops) return fail(VG_EINVAL, "no state uploaded");
+    cudaStream_t st = (cudaStream_t)stream;
+    Ctrl* h = s->hctrl;
+    std::memset(h, 0, sizeof(Ctrl));
+    h->dims = s->dims;
+    VG_CUDA(cudaMemcpyAsync(s->ctrl, h, sizeof(Ctrl), cudaMemcpyHostToDevice, st));
+    SweepArgs a = base_args(s);
+    a.in = s->buf[s->cur];
+    VG_CUDA(s->ops->max_wave(a, st));
+    VG_CUDA(s->ops->max_wave_finish(a, s->dout, st));
+    VG_CUDA(cudaMemcpyAsync(s->hout, s->dout, sizeof(double), cudaMemcpyDeviceToHost, st));
+    VG_CUDA(cudaStreamSynchronize(st));
+    *out = *s->hout;
+    s->last_launches = 2;
+    return VG_OK;
+}
+
+vg_status vg_state_device(vg_solver* s, double** plane0, long* plane_stride, long* row_stride, int* nplanes) {
+    if (!s) return fail(VG_EINVAL, "null solver");
+    if (plane0) *plane0 = s->buf[s->cur];
+    if (plane_stride) *plane_stride = s->plane;
+    if (row_stride) *row_stride = s->pitch;
+    if (nplanes) *nplanes = s->ops ? s->ops->nw : 0;
+    return VG_OK;
+}
+
+long vg_last_launch_count(vg_solver* s) { return s ? s->last_launches : 0; }
+
+}  // extern "C"

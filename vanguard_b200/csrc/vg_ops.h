@@ -1,0 +1,39 @@
+// Host-side dispatch table between the C ABI (vg_api.cu) and the kernel instantiations.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "vg_common.cuh"
+
+namespace vg {
+
+// Model variants: which primitive planes are carried on the device.
+enum Variant : int {
+    V_EULER1 = 0,  // Euler, 1 velocity (1D with v == 0):  rho, u, p
+    V_EULER2 = 1,  // Euler, 2 velocities:                 rho, u, v, p
+    V_MHD7 = 2,    // MHD with w == Bz == 0:               rho, u, v, p, Bx, By, psi
+    V_MHD9 = 3,    // MHD, all components:                 rho, u, v, w, p, Bx, By, Bz, psi
+    V_COUNT = 4
+};
+
+struct Ops {
+    int nw;  // carried primitive planes
+    // One sweep (axis 0 = X, 1 = Y).  a.in / a.out must not alias.
+    cudaError_t (*sweep)(int axis, const SweepArgs& a, cudaStream_t st);
+    // Maximum wave speed of a.in folded into ctrl->smax_next (caller zeroes it first).
+    cudaError_t (*max_wave)(const SweepArgs& a, cudaStream_t st);
+    // dt for the next step from ctrl->smax_next (and corner ghosts in 2D); zeroes smax_next.
+    cudaError_t (*step_begin)(const SweepArgs& a, cudaStream_t st);
+    // *out = maximum wave speed including corner ghosts (reads ctrl->smax_next).
+    cudaError_t (*max_wave_finish)(const SweepArgs& a, double* out, cudaStream_t st);
+};
+
+// Exact-FP64 kernels (compiled with -fmad=false; bitwise parity with the reference).
+const Ops* ops_fp64(int variant);
+// Mixed FP32/FP64 kernels.
+const Ops* ops_mixed(int variant);
+
+// Kernels launched by one sweep / max_wave / step_begin call (for launch accounting).
+inline int launches_per_sweep() { return 1; }
+
+}  // namespace vg

@@ -1,0 +1,97 @@
+"""Seeded synthetic initial data for the five benchmark workloads.
+
+All arrays are float64 primitive planes in the reference's primitive order, shape (nvar, ny, nx) for
+2D grids (row index = y, column index = x) and (nvar, n) for 1D lines.  Cell centres sit at
+((j + 0.5) dx, (i + 0.5) dx) on [0, 1]^2.  The same arrays are fed to the CUDA path and to the CPU
+oracle, so the oracle and the device always see identical inputs.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+# Euler primitive order (Euler/eulerstatevector.cpp:36-45): rho, u, v, w, p, lambda
+EULER_NVAR = 6
+# MHD primitive order (MHD/mhdstatevector.cpp:35-47): rho, u, v, w, p, Bx, By, Bz, psi
+MHD_NVAR = 9
+
+
+def euler_params(gamma=1.4, p_inf=0.0):
+    """EulerMaterialParameters(gamma, p_inf) with the reference's defaults for the reaction fields
+    (Euler/eulermaterialparameters.cpp:25-34): c_v = 25, E0 = 0, T_ign = 0.25, rate = 250."""
+    return np.array([gamma, p_inf, 25.0, 0.0, 0.25, 250.0])
+
+
+def mhd_params(gamma=5.0 / 3.0, p_inf=0.0, c_h=0.0):
+    """MHDMaterialParameters(gamma) (MHD/mhdmaterialparameters.cpp:12-19); c_h is reset every step."""
+    return np.array([gamma, p_inf, c_h])
+
+
+def sod_1d(n=1000, left=(1.0, 0.0, 1.0), right=(0.125, 0.0, 0.1)):
+    """1D shock tube, (rho, u, p) left/right.  Cell i is on the left when i <= 0.5 n, the convention of
+    EulerTests::solveToroTest1 (Euler/eulertests.cpp:16), so cell n/2 starts with the left state."""
+    W = np.zeros((EULER_NVAR, n))
+    W[5] = 1.0
+    is_left = np.arange(n) <= 0.5 * n
+    W[0] = np.where(is_left, left[0], right[0])
+    W[1] = np.where(is_left, left[1], right[1])
+    W[4] = np.where(is_left, left[2], right[2])
+    return W
+
+
+def quadrant_states(seed):
+    """Four (rho, u, v, p) states: rho ~ U[0.1, 2], u, v ~ U[-1, 1], p ~ U[0.1, 2]; quadrant q = 2*top + right."""
+    rng = np.random.default_rng(seed)
+    rho = rng.uniform(0.1, 2.0, 4)
+    u = rng.uniform(-1.0, 1.0, 4)
+    v = rng.uniform(-1.0, 1.0, 4)
+    p = rng.uniform(0.1, 2.0, 4)
+    return rho, u, v, p
+
+
+def euler_quadrants_2d(nx=4096, ny=None, seed=0):
+    """Four-quadrant 2D Riemann problem on [0,1]^2, split at the centre; quadrant states from `seed`."""
+    ny = nx if ny is None else ny
+    rho, u, v, p = quadrant_states(seed)
+    top = (np.arange(ny) >= ny // 2)[:, None]
+    right = (np.arange(nx) >= nx // 2)[None, :]
+    q = (2 * top + right).astype(np.int64)
+    W = np.zeros((EULER_NVAR, ny, nx))
+    W[0] = rho[q]
+    W[1] = u[q]
+    W[2] = v[q]
+    W[4] = p[q]
+    W[5] = 1.0
+    return W
+
+
+def mhd_vortex_2d(nx=2048, ny=None, seed=0, gamma=5.0 / 3.0, amplitude=1e-3):
+    """Orszag-Tang-type smooth vortex: rho = gamma^2, p = gamma, v = (-sin 2 pi y, sin 2 pi x, 0),
+    B = (-sin 2 pi y, sin 4 pi x, 0) / sqrt(4 pi), psi = 0, plus i.i.d. N(0, 1) * amplitude added to rho
+    and p from `seed`."""
+    ny = nx if ny is None else ny
+    dx = 1.0 / nx
+    x = (np.arange(nx) + 0.5) * dx
+    y = (np.arange(ny) + 0.5) * (1.0 / ny)
+    X, Y = np.meshgrid(x, y)
+    rng = np.random.default_rng(seed)
+    W = np.zeros((MHD_NVAR, ny, nx))
+    W[0] = gamma * gamma + amplitude * rng.standard_normal((ny, nx))
+    W[1] = -np.sin(2 * np.pi * Y)
+    W[2] = np.sin(2 * np.pi * X)
+    W[4] = gamma + amplitude * rng.standard_normal((ny, nx))
+    s = 1.0 / np.sqrt(4 * np.pi)
+    W[5] = -np.sin(2 * np.pi * Y) * s
+    W[6] = np.sin(4 * np.pi * X) * s
+    return W
+
+
+def brio_wu_1d(n=400, gamma=2.0):
+    """Brio-Wu-type MHD shock tube (MHDTests' first Dumbser test family): left (1, 0, 0, 0, 1, 0.75, 1, 0),
+    right (0.125, 0, 0, 0, 0.1, 0.75, -1, 0), split at i <= n/2."""
+    W = np.zeros((MHD_NVAR, n))
+    is_left = np.arange(n) <= 0.5 * n
+    W[0] = np.where(is_left, 1.0, 0.125)
+    W[4] = np.where(is_left, 1.0, 0.1)
+    W[5] = 0.75
+    W[6] = np.where(is_left, 1.0, -1.0)
+    return W
