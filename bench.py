@@ -358,13 +358,16 @@ def load_traffic():
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--nx", type=int, default=4096, help="grid size (smaller grids are for profiling only)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    global NX, NY
+    NX = NY = args.nx
     world, rank, local = dist_setup()
     if args.impl == "reference":
         return run_reference(args, world, rank)
