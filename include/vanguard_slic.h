@@ -126,6 +126,26 @@ vg_status vg_state_device(vg_solver* s, double** plane0, long* plane_stride, lon
 /* Number of CUDA kernels the last vg_run/vg_sweep/vg_max_wave_speed call launched (graph nodes count). */
 long vg_last_launch_count(vg_solver* s);
 
+/* Rows accepted by vg_max_wave_speed_noalloc: the size of its static scratch array (8 bytes per row,
+ * 512 KiB, held on every GPU that loads the library until the process exits). */
+#define VG_NOALLOC_MAX_ROWS 65536
+
+/* No counterpart in the reference: an allocation-free variant of vg_max_wave_speed for callers that may
+ * not allocate device memory themselves or let a library do so (applications that own all device memory
+ * through their own pool allocator, where cudaMalloc/cudaFree would escape the pool's budget and
+ * cudaFree would synchronise the device under their other streams).  Computes the maximum wave speed
+ * of the padded grid exactly as vg_max_wave_speed does, from a state the caller already holds in device
+ * memory: `planes` = the model's reference-order primitive planes (Euler 6, MHD 9) with the given plane
+ * and row strides (elements), `params` = the model's parameter block (gamma, p_inf first), `out` = a
+ * device pointer to one double.  Calls neither cudaMalloc nor cudaFree: per-row partial maxima go to a
+ * file-scope __device__ array of VG_NOALLOC_MAX_ROWS doubles, so ny > VG_NOALLOC_MAX_ROWS returns
+ * VG_EINVAL.  Uses the current device.  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.  Enqueued asynchronously on
+ * `stream`.  All calls on a device share the array, so calls that may overlap on the GPU (different
+ * streams without ordering between them) race and must be serialised by the caller. */
+vg_status vg_max_wave_speed_noalloc(int model, const double* planes, long plane_stride, long row_stride, int nx,
+                                    int ny, const double* params, double* out, void* stream);
+
 /* Text of the last error on this thread. */
 const char* vg_last_error_string(void);
 const char* vg_status_string(vg_status st);

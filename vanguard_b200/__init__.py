@@ -49,7 +49,18 @@ class RunConfig(ctypes.Structure):
 # Every function the C ABI header declares (tests check the library exports them all).
 EXPORTS = ["vg_create", "vg_destroy", "vg_model_nvar", "vg_upload_primitive", "vg_download_primitive",
            "vg_run", "vg_solve", "vg_sweep", "vg_max_wave_speed", "vg_state_device", "vg_last_launch_count",
-           "vg_last_error_string", "vg_status_string"]
+           "vg_last_error_string", "vg_status_string", "vg_max_wave_speed_noalloc"]
+
+NOALLOC_MAX_ROWS = 65536
+
+
+def max_wave_speed_noalloc(model, planes_ptr, plane_stride, row_stride, nx, ny, params, out_ptr, stream=None):
+    """vg_max_wave_speed_noalloc on caller-owned device memory (raw device pointers); asynchronous."""
+    prm = np.zeros(MAX_PARAMS)
+    prm[:len(params)] = params
+    return _check(lib().vg_max_wave_speed_noalloc(model, ctypes.c_void_p(planes_ptr), plane_stride, row_stride, nx,
+                                                  ny, prm.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                                  ctypes.c_void_p(out_ptr), stream))
 
 _lib = None
 
@@ -73,6 +84,8 @@ def lib():
         L.vg_max_wave_speed.argtypes = [vp, D, vp]
         L.vg_state_device.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(ctypes.c_long),
                                       ctypes.POINTER(ctypes.c_long), ctypes.POINTER(ctypes.c_int)]
+        L.vg_max_wave_speed_noalloc.argtypes = [ctypes.c_int, vp, ctypes.c_long, ctypes.c_long, ctypes.c_int,
+                                                ctypes.c_int, D, vp, vp]
         L.vg_last_launch_count.argtypes = [vp]
         L.vg_last_launch_count.restype = ctypes.c_long
         L.vg_last_error_string.restype = ctypes.c_char_p

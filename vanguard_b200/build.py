@@ -26,6 +26,7 @@ UNITS = [
     ("slic_fp64.cu", ["-fmad=false"]),
     ("slic_mixed.cu", ["-fmad=true"]),
     ("vg_api.cu", []),
+    ("vg_noalloc.cu", ["-fmad=false"]),
 ]
 
 

@@ -49,6 +49,10 @@ const int kPlanes[vg::V_COUNT][9] = {
 
 }  // namespace
 
+namespace vg {
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace vg
+
 struct vg_solver {
     vg_grid_desc d{};
     int dims = 2;

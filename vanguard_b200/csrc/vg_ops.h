@@ -3,6 +3,8 @@
 
 #include <cuda_runtime.h>
 
+#include <string>
+
 #include "vg_common.cuh"
 
 namespace vg {
@@ -32,6 +34,9 @@ struct Ops {
 const Ops* ops_fp64(int variant);
 // Mixed FP32/FP64 kernels.
 const Ops* ops_mixed(int variant);
+
+// Record the text returned by vg_last_error_string() on this thread.
+void set_last_error(const std::string& msg);
 
 // Kernels launched by one sweep / max_wave / step_begin call (for launch accounting).
 inline int launches_per_sweep() { return 1; }
