@@ -1,0 +1,210 @@
+// Mixed FP32/FP64 device models for the VG_MIXED form.
+//
+// Split of the arithmetic:
+//   FP64  conserved cell states and every evolved edge / Richtmyer state (so no state is ever rounded to
+//         float), pressure recovery from total energy (E - |m|^2 / 2 rho, where the kinetic energy cancels),
+//         the CFL wave speed, and the cell-update accumulation U + (dt/dx)(F_L - F_R) with the flux
+//         difference formed in FP64.
+//   FP32  slopes and limiter, every flux component other than the pressure, the half-step evolution
+//         increment and the Lax-Friedrichs / Richtmyer / FORCE combinations.
+// No correctly rounded FP64 division is used: 1/rho is an FP32 reciprocal refined by Newton-Raphson
+// steps in FP64 (x <- x (2 - rho x), each step doubles the correct bits: 2^-23 -> 2^-46 -> full).
+#pragma once
+
+#include "vg_common.cuh"
+
+namespace vg {
+
+// 1/a to ~2^-46 relative (one Newton step from the FP32 reciprocal).
+__device__ __forceinline__ double rcp_nr1(double a) {
+    double x = (double)__frcp_rn((float)a);
+    double e = fma(-a, x, 1.0);
+    return fma(x, e, x);
+}
+// 1/a to full double precision (two Newton steps).
+__device__ __forceinline__ double rcp_nr2(double a) {
+    double x = rcp_nr1(a);
+    double e = fma(-a, x, 1.0);
+    return fma(x, e, x);
+}
+
+// ------------------------------------------------------------------------------------------- Euler
+template <int NVEL>
+struct EulerMixed {
+    static constexpr int NW = NVEL + 2;
+    static constexpr int NU = NW;
+    static constexpr int IE = NU - 1;
+    struct P {
+        double gm1, inv_gm1, gpinf, g, pinf, ch2;
+    };
+    __device__ static P params(const double* prm, double /*ch*/) {
+        double g = prm[0], pinf = prm[1];
+        return P{g - 1.0, 1.0 / (g - 1.0), g * pinf, g, pinf, 0.0};
+    }
+    // W -> U in FP64: E = rho |v|^2 / 2 + (p + gamma p_inf) / (gamma - 1)
+    __device__ static void cons(const double* W, const P& q, double* U) {
+        double rho = W[0], u = W[1], v = (NVEL == 2) ? W[2] : 0.0, p = W[IE];
+        U[0] = rho;
+        U[1] = rho * u;
+        if constexpr (NVEL == 2) U[2] = rho * v;
+        double v2 = (NVEL == 2) ? fma(u, u, v * v) : u * u;
+        U[IE] = fma(0.5 * rho, v2, (p + q.gpinf) * q.inv_gm1);
+    }
+    // U -> W in FP64 (final cell update)
+    __device__ static void setcons(const double* U, const P& q, double* W) {
+        double rho = U[0], inv = rcp_nr2(rho);
+        double u = U[1] * inv, v = (NVEL == 2) ? U[2] * inv : 0.0;
+        double ke2 = (NVEL == 2) ? fma(U[1], u, U[2] * v) : U[1] * u;  // |m|^2 / rho
+        W[0] = rho;
+        W[1] = u;
+        if constexpr (NVEL == 2) W[2] = v;
+        W[IE] = fma(q.gm1, fma(-0.5, ke2, U[IE]), -q.gpinf);
+    }
+    // Flux of an FP64 state: pressure recovered in FP64, the other components in FP32.
+    template <int AXIS>
+    __device__ static void flux(const double* U, const P& q, float* F) {
+        double rho = U[0], inv = rcp_nr1(rho);
+        double mxd = U[1], myd = (NVEL == 2) ? U[2] : 0.0;
+        double ke2 = (NVEL == 2) ? fma(mxd, mxd, myd * myd) * inv : mxd * mxd * inv;
+        double p = fma(q.gm1, fma(-0.5, ke2, U[IE]), -q.gpinf);
+        float pf = (float)p, Ef = (float)U[IE];
+        float un = (float)((AXIS == 0 ? mxd : myd) * inv);
+        float mx = (float)mxd;
+        if constexpr (AXIS == 0) {
+            F[0] = mx;
+            F[1] = fmaf(mx, un, pf);
+            if constexpr (NVEL == 2) F[2] = (float)myd * un;
+        } else {
+            float my = (float)myd;
+            F[0] = my;
+            F[1] = mx * un;
+            F[2] = fmaf(my, un, pf);
+        }
+        F[IE] = (Ef + pf) * un;
+    }
+    __device__ static double wave(const double* W, const P& q, int dims) {
+        double c = sqrt((q.g * (W[IE] + q.pinf)) / W[0]);
+        if (dims == 1) return fabs(W[1]) + c;
+        double v = (NVEL == 2) ? W[2] : 0.0;
+        return fmax(fabs(W[1]), fabs(v)) + c;
+    }
+    __device__ static void default_state(double* W) {
+        for (int i = 0; i < NW; i++) W[i] = 0.0;
+        W[0] = 1.0;
+        W[IE] = 1.0;
+    }
+    __device__ static double density(const double* W) { return W[0]; }
+    __device__ static double pressure(const double* W) { return W[IE]; }
+};
+
+// --------------------------------------------------------------------------------------------- MHD
+template <bool FULL>
+struct MHDMixed {
+    static constexpr int NW = FULL ? 9 : 7;
+    static constexpr int NU = NW;
+    static constexpr int IP = FULL ? 4 : 3;
+    static constexpr int IBX = IP + 1;
+    static constexpr int IBY = IP + 2;
+    static constexpr int IPSI = NW - 1;
+    struct P {
+        double gm1, inv_gm1, gpinf, g, pinf, ch2;
+    };
+    __device__ static P params(const double* prm, double ch) {
+        double g = prm[0], pinf = prm[1];
+        return P{g - 1.0, 1.0 / (g - 1.0), g * pinf, g, pinf, ch * ch};
+    }
+    __device__ static double sq3(double a, double b, double c) {
+        if constexpr (FULL) return fma(a, a, fma(b, b, c * c));
+        else return fma(a, a, b * b);
+    }
+    __device__ static void cons(const double* W, const P& q, double* U) {
+        double rho = W[0], u = W[1], v = W[2], w = FULL ? W[3] : 0.0, p = W[IP];
+        double bx = W[IBX], by = W[IBY], bz = FULL ? W[7] : 0.0;
+        U[0] = rho;
+        U[1] = rho * u;
+        U[2] = rho * v;
+        if constexpr (FULL) U[3] = rho * w;
+        U[IP] = fma(0.5 * rho, sq3(u, v, w), fma(0.5, sq3(bx, by, bz), (p + q.gpinf) * q.inv_gm1));
+        U[IBX] = bx;
+        U[IBY] = by;
+        if constexpr (FULL) U[7] = bz;
+        U[IPSI] = W[IPSI];
+    }
+    __device__ static double pressure_of(const double* U, const P& q, double inv, double& u, double& v, double& w) {
+        u = U[1] * inv;
+        v = U[2] * inv;
+        w = FULL ? U[3] * inv : 0.0;
+        double ke2 = FULL ? fma(U[1], u, fma(U[2], v, U[3] * w)) : fma(U[1], u, U[2] * v);
+        double b2 = sq3(U[IBX], U[IBY], FULL ? U[7] : 0.0);
+        return fma(q.gm1, fma(-0.5, ke2 + b2, U[IP]), -q.gpinf);
+    }
+    __device__ static void setcons(const double* U, const P& q, double* W) {
+        double inv = rcp_nr2(U[0]), u, v, w;
+        double p = pressure_of(U, q, inv, u, v, w);
+        W[0] = U[0];
+        W[1] = u;
+        W[2] = v;
+        if constexpr (FULL) W[3] = w;
+        W[IP] = p;
+        W[IBX] = U[IBX];
+        W[IBY] = U[IBY];
+        if constexpr (FULL) W[7] = U[7];
+        W[IPSI] = U[IPSI];
+    }
+    template <int AXIS>
+    __device__ static void flux(const double* U, const P& q, float* F) {
+        double inv = rcp_nr1(U[0]), ud, vd, wd;
+        double p = pressure_of(U, q, inv, ud, vd, wd);
+        float rho = (float)U[0], u = (float)ud, v = (float)vd, w = (float)wd;
+        float bx = (float)U[IBX], by = (float)U[IBY], bz = FULL ? (float)U[7] : 0.0f, psi = (float)U[IPSI];
+        float E = (float)U[IP], pf = (float)p;
+        float b2 = FULL ? fmaf(bx, bx, fmaf(by, by, bz * bz)) : fmaf(bx, bx, by * by);
+        float pt = fmaf(0.5f, b2, pf);  // total pressure
+        float vb = FULL ? fmaf(u, bx, fmaf(v, by, w * bz)) : fmaf(u, bx, v * by);
+        float ch2 = (float)q.ch2;
+        if constexpr (AXIS == 0) {
+            float mx = (float)U[1];
+            F[0] = mx;
+            F[1] = fmaf(mx, u, pt) - bx * bx;
+            F[2] = fmaf(mx, v, -bx * by);
+            if constexpr (FULL) F[3] = fmaf(mx, w, -bx * bz);
+            F[IP] = fmaf(E + pt, u, -vb * bx);
+            F[IBX] = psi;
+            F[IBY] = fmaf(by, u, -bx * v);
+            if constexpr (FULL) F[7] = fmaf(bz, u, -bx * w);
+            F[IPSI] = ch2 * bx;
+        } else {
+            float my = (float)U[2];
+            F[0] = my;
+            F[1] = fmaf(my, u, -by * bx);
+            F[2] = fmaf(my, v, pt) - by * by;
+            if constexpr (FULL) F[3] = fmaf(my, w, -by * bz);
+            F[IP] = fmaf(E + pt, v, -vb * by);
+            F[IBX] = fmaf(bx, v, -by * u);
+            F[IBY] = psi;
+            if constexpr (FULL) F[7] = fmaf(bz, v, -by * w);
+            F[IPSI] = ch2 * by;
+        }
+        (void)rho;
+    }
+    __device__ static double fast(const double* W, const P& q, double bn) {
+        double rho = W[0], bx = W[IBX], by = W[IBY], bz = FULL ? W[7] : 0.0;
+        double c2 = (q.g * (W[IP] + q.pinf)) / rho;
+        double a2 = sq3(bx, by, bz) / rho;
+        double s = c2 + a2;
+        return sqrt(0.5 * (s + sqrt(fmax(s * s - 4.0 * c2 * bn * bn / rho, 0.0))));
+    }
+    __device__ static double wave(const double* W, const P& q, int dims) {
+        if (dims == 1) return fabs(W[1]) + fast(W, q, W[IBX]);
+        return fmax(fabs(W[1]), fabs(W[2])) + fmax(fast(W, q, W[IBX]), fast(W, q, W[IBY]));
+    }
+    __device__ static void default_state(double* W) {
+        for (int i = 0; i < NW; i++) W[i] = 0.0;
+        W[0] = 1.0;
+        W[IP] = 1.0;
+    }
+    __device__ static double density(const double* W) { return W[0]; }
+    __device__ static double pressure(const double* W) { return W[IP]; }
+};
+
+}  // namespace vg
