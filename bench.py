@@ -226,6 +226,9 @@ def run_cuda(args, world, rank, local):
     for name, prec in forms:
         s = vg.Solver(vg.EULER, NX, NY, prm, precision=prec, device=local)
         s.upload(W0, stream=sh)
+        # pick the sweep tile shapes on this grid (results do not depend on the choice)
+        xt, yt = s.autotune(dx, CFL, limiter=LIMITER, stream=sh)
+        tuned = s.launch_config()
         # warm-up (also captures the step graphs)
         s.run(dx, CFL, steps=max(args.warmup, 3), limiter=LIMITER, stream=sh)
         s.upload(W0, stream=sh)
@@ -261,7 +264,8 @@ def run_cuda(args, world, rank, local):
         torch.cuda.synchronize()
         ys_ms = e0.elapsed_time(e1) / reps
         results[name] = {"ms": ms, "steps": steps, "launches": launches, "clocks": clk.summary(),
-                         "x_sweep_ms": xs_ms, "y_sweep_ms": ys_ms}
+                         "x_sweep_ms": xs_ms, "y_sweep_ms": ys_ms,
+                         "tuned": {"x": tuned[2], "y": tuned[3], "x_ms": xt, "y_ms": yt}}
         s.close()
 
     # end-to-end through the host-buffer API (vg_solve: upload + run + download inside the timed region)
@@ -270,6 +274,8 @@ def run_cuda(args, world, rank, local):
     hin = torch.from_numpy(W0).pin_memory()
     hout = torch.empty_like(hin).pin_memory()
     s = vg.Solver(vg.EULER, NX, NY, prm, precision=prec, device=local)
+    s.upload(W0, stream=sh)
+    s.autotune(dx, CFL, limiter=LIMITER, measure=False, stream=sh)  # cached choice from the timed run
     s.solve(hin.numpy(), dx, CFL, steps=2, limiter=LIMITER, out=hout.numpy(), stream=sh)
     barrier()
     torch.cuda.synchronize()
@@ -309,7 +315,7 @@ def run_cuda(args, world, rank, local):
         "clocks": r["clocks"],
         "forms": {k: {"cell_updates_per_s": world * cells * args.steps / (v["ms"] / 1000.0),
                       "ms_per_step": v["ms"] / args.steps, "x_sweep_ms": v["x_sweep_ms"],
-                      "y_sweep_ms": v["y_sweep_ms"],
+                      "y_sweep_ms": v["y_sweep_ms"], "autotune": v["tuned"],
                       "hbm_frac_of_step": world * cells * args.steps * BYTES_PER_CELL_UPDATE / (v["ms"] / 1000.0) / 1e9 / peak}
                   for k, v in results.items()},
     }

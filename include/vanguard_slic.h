@@ -126,6 +126,22 @@ vg_status vg_state_device(vg_solver* s, double** plane0, long* plane_stride, lon
 /* Number of CUDA kernels the last vg_run/vg_sweep/vg_max_wave_speed call launched (graph nodes count). */
 long vg_last_launch_count(vg_solver* s);
 
+/* Launch configurations of the sweeps.  No counterpart in the reference (its sweeps are OpenMP loops).
+ * Each model and precision is compiled for VG_NUM_XCFG X-sweep tile shapes (cells per segment, segments
+ * per block, register cap) and VG_NUM_YCFG Y-sweep tile shapes (columns per block, rows marched per
+ * thread, register cap).  The tile shape never changes a cell's arithmetic, so every configuration gives
+ * identical results.
+ * vg_autotune times every candidate on the uploaded state (`reps` launches each, CUDA events on `stream`),
+ * keeps the fastest per axis and caches it by (variant, precision, boundary, nx, ny, SM count) in
+ * process memory and, when the environment variable VG_TUNE_CACHE names a file, on disk.  With
+ * times_ms == NULL a cached choice is applied without timing; otherwise times_ms receives
+ * VG_NUM_XCFG + VG_NUM_YCFG averages (X configurations first). */
+#define VG_NUM_XCFG 5
+#define VG_NUM_YCFG 6
+vg_status vg_autotune(vg_solver* s, const vg_run_config* cfg, int reps, float* times_ms, void* stream);
+vg_status vg_set_launch_config(vg_solver* s, int xcfg, int ycfg);
+vg_status vg_get_launch_config(vg_solver* s, int* xcfg, int* ycfg, const char** xname, const char** yname);
+
 /* Rows accepted by vg_max_wave_speed_noalloc: the size of its static scratch array (8 bytes per row,
  * 512 KiB, held on every GPU that loads the library until the process exits). */
 #define VG_NOALLOC_MAX_ROWS 65536

@@ -117,3 +117,42 @@ def test_mhd_full_components(gpu, oracle_lib):
         s.run(1.0 / nx, 0.8, steps=20, limiter=1)
         out = s.download()
     _bitwise(out, ref)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("model", [0, 1])
+def test_every_launch_config_gives_identical_results(gpu, model, precision):
+    """Tile shapes only move work between threads: every configuration yields the same bits."""
+    nx, ny = 150, 70
+    if model == 0:
+        W, prm = wl.euler_quadrants_2d(nx, ny, seed=61), wl.euler_params(1.4)
+    else:
+        W, prm = wl.mhd_vortex_2d(nx, ny, seed=62), wl.mhd_params(5.0 / 3.0)
+    outs = []
+    with gpu.Solver(model, nx, ny, prm, precision=precision) as s:
+        for xc in range(gpu.NUM_XCFG):
+            for yc in range(gpu.NUM_YCFG):
+                if xc and yc and xc != yc % gpu.NUM_XCFG:
+                    continue  # every X and every Y configuration appears at least once
+                s.set_launch_config(xc, yc)
+                s.upload(W)
+                s.run(1.0 / nx, 0.8, steps=6, limiter=0)
+                outs.append(((xc, yc), s.download()))
+    for cfg, o in outs[1:]:
+        assert np.array_equal(o, outs[0][1]), cfg
+
+
+def test_autotune_picks_and_keeps_results(gpu, oracle_lib):
+    nx, ny = 256, 192
+    W, prm = wl.euler_quadrants_2d(nx, ny, seed=63), wl.euler_params(1.4)
+    ref = W.copy()
+    O.run(O.EULER, ref, 1.0 / nx, 0.8, steps=10, limiter=0, params=prm)
+    with gpu.Solver(gpu.EULER, nx, ny, prm) as s:
+        s.upload(W)
+        xt, yt = s.autotune(1.0 / nx, 0.8, limiter=0)
+        assert all(t > 0 for t in xt) and all(t > 0 for t in yt)
+        x, y, _, _ = s.launch_config()
+        assert xt[x] == min(xt) and yt[y] == min(yt)
+        s.upload(W)
+        s.run(1.0 / nx, 0.8, steps=10, limiter=0)
+        _bitwise(s.download(), ref)

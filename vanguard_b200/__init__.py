@@ -49,7 +49,9 @@ class RunConfig(ctypes.Structure):
 # Every function the C ABI header declares (tests check the library exports them all).
 EXPORTS = ["vg_create", "vg_destroy", "vg_model_nvar", "vg_upload_primitive", "vg_download_primitive",
            "vg_run", "vg_solve", "vg_sweep", "vg_max_wave_speed", "vg_state_device", "vg_last_launch_count",
-           "vg_last_error_string", "vg_status_string", "vg_max_wave_speed_noalloc"]
+           "vg_last_error_string", "vg_status_string", "vg_max_wave_speed_noalloc", "vg_autotune",
+           "vg_set_launch_config", "vg_get_launch_config"]
+NUM_XCFG, NUM_YCFG = 5, 6
 
 NOALLOC_MAX_ROWS = 65536
 
@@ -86,6 +88,10 @@ def lib():
                                       ctypes.POINTER(ctypes.c_long), ctypes.POINTER(ctypes.c_int)]
         L.vg_max_wave_speed_noalloc.argtypes = [ctypes.c_int, vp, ctypes.c_long, ctypes.c_long, ctypes.c_int,
                                                 ctypes.c_int, D, vp, vp]
+        L.vg_autotune.argtypes = [vp, ctypes.POINTER(RunConfig), ctypes.c_int, ctypes.POINTER(ctypes.c_float), vp]
+        L.vg_set_launch_config.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+        L.vg_get_launch_config.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                           ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_char_p)]
         L.vg_last_launch_count.argtypes = [vp]
         L.vg_last_launch_count.restype = ctypes.c_long
         L.vg_last_error_string.restype = ctypes.c_char_p
@@ -188,3 +194,21 @@ class Solver:
 
     def last_launch_count(self):
         return lib().vg_last_launch_count(self._h)
+
+    def autotune(self, dx, cfl, bias=0.0, limiter=SUPERBEE, reps=3, measure=True, stream=None):
+        """Pick the fastest sweep tile shapes on the uploaded state; returns (x_times, y_times) in ms."""
+        c = RunConfig(dx, cfl, 0.0, 1, bias, limiter, 0)
+        times = (ctypes.c_float * (NUM_XCFG + NUM_YCFG))() if measure else None
+        _check(lib().vg_autotune(self._h, ctypes.byref(c), reps, times, stream))
+        if times is None:
+            return None
+        return list(times[:NUM_XCFG]), list(times[NUM_XCFG:])
+
+    def launch_config(self):
+        x, y = ctypes.c_int(), ctypes.c_int()
+        xn, yn = ctypes.c_char_p(), ctypes.c_char_p()
+        _check(lib().vg_get_launch_config(self._h, ctypes.byref(x), ctypes.byref(y), ctypes.byref(xn), ctypes.byref(yn)))
+        return x.value, y.value, xn.value.decode(), yn.value.decode()
+
+    def set_launch_config(self, xcfg, ycfg):
+        return _check(lib().vg_set_launch_config(self._h, xcfg, ycfg))

@@ -19,6 +19,7 @@ struct EulerF64 {
     static constexpr int NW = NVEL + 2;
     static constexpr int NU = NW;
     static constexpr int IE = NU - 1;  // energy / pressure slot
+    static constexpr bool HAS_Y = NVEL == 2;
     struct P {
         double g, pinf, ch2;
     };
@@ -105,6 +106,7 @@ struct MHDF64 {
     static constexpr int IBX = IP + 1;
     static constexpr int IBY = IP + 2;
     static constexpr int IPSI = NW - 1;
+    static constexpr bool HAS_Y = true;
     struct P {
         double g, pinf, ch2;
     };

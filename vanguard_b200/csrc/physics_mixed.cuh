@@ -2,29 +2,44 @@
 //
 // Split of the arithmetic:
 //   FP64  conserved cell states and every evolved edge / Richtmyer state (so no state is ever rounded to
-//         float), pressure recovery from total energy (E - |m|^2 / 2 rho, where the kinetic energy cancels),
-//         the CFL wave speed, and the cell-update accumulation U + (dt/dx)(F_L - F_R) with the flux
-//         difference formed in FP64.
-//   FP32  slopes and limiter, every flux component other than the pressure, the half-step evolution
-//         increment and the Lax-Friedrichs / Richtmyer / FORCE combinations.
-// No correctly rounded FP64 division is used: 1/rho is an FP32 reciprocal refined by Newton-Raphson
-// steps in FP64 (x <- x (2 - rho x), each step doubles the correct bits: 2^-23 -> 2^-46 -> full).
+//         float); the physical flux function with its pressure recovery from total energy
+//         (E - |m|^2 / 2 rho, where the kinetic energy cancels); the limiter's slope ratio; the CFL wave
+//         speed; and the cell-update accumulation U + (dt/dx)(F_L - F_R).
+//   FP32  flux values, the half-step evolution increment (dt/2dx)(F(x_L) - F(x_R)), and the
+//         Lax-Friedrichs, Richtmyer and FORCE combinations.  The update's flux difference F_L - F_R is
+//         formed in FP64 from the two FP32 interface fluxes, so the interface terms telescope exactly
+//         and mass, momentum and energy are conserved to FP64 round-off.
+// No correctly rounded FP64 division is used: 1/rho starts from the hardware reciprocal approximation
+// (PTX rcp.approx.ftz.f64, one XU operation and no precision conversion) and is refined by Newton-Raphson
+// steps x <- x + x (1 - a x), each of which doubles the number of correct bits.
+//
+// On B200 the XU pipe that executes reciprocal approximations and every float<->double conversion has a
+// quarter of the FP64 pipe's lanes, so the physical flux function (which needs the FP64 pressure anyway)
+// evaluates in FP64 with FMA and only its outputs are rounded to FP32; the arithmetic that combines fluxes
+// (half-step evolution increment, Lax-Friedrichs, Richtmyer and FORCE averages) runs in FP32.
 #pragma once
 
 #include "vg_common.cuh"
 
 namespace vg {
 
-// 1/a to ~2^-46 relative (one Newton step from the FP32 reciprocal).
+__device__ __forceinline__ double rcp_approx(double a) {
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(a));
+    return r;
+}
+// 1/a refined by one Newton step: relative error ~2^-44, far below the FP32 rounding of a flux value.
 __device__ __forceinline__ double rcp_nr1(double a) {
-    double x = (double)__frcp_rn((float)a);
+    double x = rcp_approx(a);
     double e = fma(-a, x, 1.0);
     return fma(x, e, x);
 }
-// 1/a to full double precision (two Newton steps).
+// 1/a refined by two Newton steps (full double precision), for the stored state.
 __device__ __forceinline__ double rcp_nr2(double a) {
-    double x = rcp_nr1(a);
+    double x = rcp_approx(a);
     double e = fma(-a, x, 1.0);
+    x = fma(x, e, x);
+    e = fma(-a, x, 1.0);
     return fma(x, e, x);
 }
 
@@ -34,6 +49,7 @@ struct EulerMixed {
     static constexpr int NW = NVEL + 2;
     static constexpr int NU = NW;
     static constexpr int IE = NU - 1;
+    static constexpr bool HAS_Y = NVEL == 2;
     struct P {
         double gm1, inv_gm1, gpinf, g, pinf, ch2;
     };
@@ -60,27 +76,25 @@ struct EulerMixed {
         if constexpr (NVEL == 2) W[2] = v;
         W[IE] = fma(q.gm1, fma(-0.5, ke2, U[IE]), -q.gpinf);
     }
-    // Flux of an FP64 state: pressure recovered in FP64, the other components in FP32.
+    // Flux of an FP64 state, evaluated in FP64 (pressure recovered from total energy where the kinetic energy
+    // cancels) and rounded to FP32 on output.
     template <int AXIS>
     __device__ static void flux(const double* U, const P& q, float* F) {
-        double rho = U[0], inv = rcp_nr1(rho);
+        double inv = rcp_nr1(U[0]);
         double mxd = U[1], myd = (NVEL == 2) ? U[2] : 0.0;
+        double un = (AXIS == 0 ? mxd : myd) * inv;
         double ke2 = (NVEL == 2) ? fma(mxd, mxd, myd * myd) * inv : mxd * mxd * inv;
         double p = fma(q.gm1, fma(-0.5, ke2, U[IE]), -q.gpinf);
-        float pf = (float)p, Ef = (float)U[IE];
-        float un = (float)((AXIS == 0 ? mxd : myd) * inv);
-        float mx = (float)mxd;
         if constexpr (AXIS == 0) {
-            F[0] = mx;
-            F[1] = fmaf(mx, un, pf);
-            if constexpr (NVEL == 2) F[2] = (float)myd * un;
+            F[0] = (float)mxd;
+            F[1] = (float)fma(mxd, un, p);
+            if constexpr (NVEL == 2) F[2] = (float)(myd * un);
         } else {
-            float my = (float)myd;
-            F[0] = my;
-            F[1] = mx * un;
-            F[2] = fmaf(my, un, pf);
+            F[0] = (float)myd;
+            F[1] = (float)(mxd * un);
+            F[2] = (float)fma(myd, un, p);
         }
-        F[IE] = (Ef + pf) * un;
+        F[IE] = (float)((U[IE] + p) * un);
     }
     __device__ static double wave(const double* W, const P& q, int dims) {
         double c = sqrt((q.g * (W[IE] + q.pinf)) / W[0]);
@@ -106,6 +120,7 @@ struct MHDMixed {
     static constexpr int IBX = IP + 1;
     static constexpr int IBY = IP + 2;
     static constexpr int IPSI = NW - 1;
+    static constexpr bool HAS_Y = true;
     struct P {
         double gm1, inv_gm1, gpinf, g, pinf, ch2;
     };
@@ -153,39 +168,34 @@ struct MHDMixed {
     }
     template <int AXIS>
     __device__ static void flux(const double* U, const P& q, float* F) {
-        double inv = rcp_nr1(U[0]), ud, vd, wd;
-        double p = pressure_of(U, q, inv, ud, vd, wd);
-        float rho = (float)U[0], u = (float)ud, v = (float)vd, w = (float)wd;
-        float bx = (float)U[IBX], by = (float)U[IBY], bz = FULL ? (float)U[7] : 0.0f, psi = (float)U[IPSI];
-        float E = (float)U[IP], pf = (float)p;
-        float b2 = FULL ? fmaf(bx, bx, fmaf(by, by, bz * bz)) : fmaf(bx, bx, by * by);
-        float pt = fmaf(0.5f, b2, pf);  // total pressure
-        float vb = FULL ? fmaf(u, bx, fmaf(v, by, w * bz)) : fmaf(u, bx, v * by);
-        float ch2 = (float)q.ch2;
+        double inv = rcp_nr1(U[0]), u, v, w;
+        double p = pressure_of(U, q, inv, u, v, w);
+        double bx = U[IBX], by = U[IBY], bz = FULL ? U[7] : 0.0, psi = U[IPSI];
+        double pt = fma(0.5, sq3(bx, by, bz), p);  // total pressure
+        double vb = FULL ? fma(u, bx, fma(v, by, w * bz)) : fma(u, bx, v * by);
         if constexpr (AXIS == 0) {
-            float mx = (float)U[1];
-            F[0] = mx;
-            F[1] = fmaf(mx, u, pt) - bx * bx;
-            F[2] = fmaf(mx, v, -bx * by);
-            if constexpr (FULL) F[3] = fmaf(mx, w, -bx * bz);
-            F[IP] = fmaf(E + pt, u, -vb * bx);
-            F[IBX] = psi;
-            F[IBY] = fmaf(by, u, -bx * v);
-            if constexpr (FULL) F[7] = fmaf(bz, u, -bx * w);
-            F[IPSI] = ch2 * bx;
+            double mx = U[1];
+            F[0] = (float)mx;
+            F[1] = (float)(fma(mx, u, pt) - bx * bx);
+            F[2] = (float)fma(mx, v, -bx * by);
+            if constexpr (FULL) F[3] = (float)fma(mx, w, -bx * bz);
+            F[IP] = (float)fma(U[IP] + pt, u, -vb * bx);
+            F[IBX] = (float)psi;
+            F[IBY] = (float)fma(by, u, -bx * v);
+            if constexpr (FULL) F[7] = (float)fma(bz, u, -bx * w);
+            F[IPSI] = (float)(q.ch2 * bx);
         } else {
-            float my = (float)U[2];
-            F[0] = my;
-            F[1] = fmaf(my, u, -by * bx);
-            F[2] = fmaf(my, v, pt) - by * by;
-            if constexpr (FULL) F[3] = fmaf(my, w, -by * bz);
-            F[IP] = fmaf(E + pt, v, -vb * by);
-            F[IBX] = fmaf(bx, v, -by * u);
-            F[IBY] = psi;
-            if constexpr (FULL) F[7] = fmaf(bz, v, -by * w);
-            F[IPSI] = ch2 * by;
+            double my = U[2];
+            F[0] = (float)my;
+            F[1] = (float)fma(my, u, -by * bx);
+            F[2] = (float)(fma(my, v, pt) - by * by);
+            if constexpr (FULL) F[3] = (float)fma(my, w, -by * bz);
+            F[IP] = (float)fma(U[IP] + pt, v, -vb * by);
+            F[IBX] = (float)fma(bx, v, -by * u);
+            F[IBY] = (float)psi;
+            if constexpr (FULL) F[7] = (float)fma(bz, v, -by * w);
+            F[IPSI] = (float)(q.ch2 * by);
         }
-        (void)rho;
     }
     __device__ static double fast(const double* W, const P& q, double bn) {
         double rho = W[0], bx = W[IBX], by = W[IBY], bz = FULL ? W[7] : 0.0;

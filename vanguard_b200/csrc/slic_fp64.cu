@@ -3,32 +3,24 @@
 // before it is added.
 #include "physics_fp64.cuh"
 #include "slic_kernels.cuh"
+#include "sweep_table.cuh"
 #include "vg_ops.h"
 
 namespace vg {
 namespace {
 
-constexpr int XP = 128;   // cells per X segment (126 outputs + 2 halo)
-constexpr int XL = 1;     // segments per block
-constexpr int YTX = 64;   // columns per Y block
-constexpr int YTY = 64;   // rows per Y segment
 constexpr int MW_NT = 256;
 
-template <class M>
-cudaError_t sweep_impl(int axis, const SweepArgs& a, cudaStream_t st) {
-    if (axis == 0) {
-        dim3 grid((a.nx + XP - 3) / (XP - 2), (a.ny + XL - 1) / XL);
-        sweep_x_kernel<M, XP, XL><<<grid, XP * XL, 0, st>>>(a);
-    } else {
-        if constexpr (M::NU >= 3) {
-            dim3 grid((a.nx + YTX - 1) / YTX, (a.ny + YTY - 1) / YTY);
-            sweep_y_kernel<M, YTX, YTY><<<grid, YTX, 0, st>>>(a);
-        } else {
-            return cudaErrorInvalidValue;
-        }
+struct Fp64Kernels {
+    template <class M, int P, int LPB, int MINB>
+    static void x(dim3 grid, int nt, cudaStream_t st, const SweepArgs& a) {
+        sweep_x_kernel<M, P, LPB, MINB><<<grid, nt, 0, st>>>(a);
     }
-    return cudaGetLastError();
-}
+    template <class M, int TX, int TY, int MINB>
+    static void y(dim3 grid, int nt, cudaStream_t st, const SweepArgs& a) {
+        sweep_y_kernel<M, TX, TY, MINB><<<grid, nt, 0, st>>>(a);
+    }
+};
 
 template <class M>
 cudaError_t max_wave_impl(const SweepArgs& a, cudaStream_t st) {
@@ -53,16 +45,8 @@ cudaError_t finish_impl(const SweepArgs& a, double* out, cudaStream_t st) {
 
 template <class M>
 constexpr Ops make_ops() {
-    return Ops{M::NW, &sweep_impl<M>, &max_wave_impl<M>, &step_begin_impl<M>, &finish_impl<M>};
-}
-
-// Y sweeps of the 1-velocity Euler variant are never launched (it is only chosen for 1D grids).
-template <>
-cudaError_t sweep_impl<EulerF64<1>>(int axis, const SweepArgs& a, cudaStream_t st) {
-    if (axis != 0) return cudaErrorInvalidValue;
-    dim3 grid((a.nx + XP - 3) / (XP - 2), (a.ny + XL - 1) / XL);
-    sweep_x_kernel<EulerF64<1>, XP, XL><<<grid, XP * XL, 0, st>>>(a);
-    return cudaGetLastError();
+    return Ops{M::NW, SweepTable<Fp64Kernels, M>::x, SweepTable<Fp64Kernels, M>::y, &max_wave_impl<M>,
+               &step_begin_impl<M>, &finish_impl<M>};
 }
 
 const Ops kOps[V_COUNT] = {

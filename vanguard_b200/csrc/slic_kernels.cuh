@@ -131,8 +131,8 @@ __device__ __forceinline__ bool bad_state(const double* W) {
 }
 
 // ----------------------------------------------------------------------------------------- X sweep
-template <class M, int P, int LPB>
-__global__ void __launch_bounds__(P* LPB) sweep_x_kernel(SweepArgs a) {
+template <class M, int P, int LPB, int MINB>
+__global__ void __launch_bounds__(P* LPB, MINB) sweep_x_kernel(SweepArgs a) {
     constexpr int NU = M::NU, NW = M::NW;
     constexpr int NT = P * LPB;
     __shared__ double Us[NU][LPB][P + 2];
@@ -220,8 +220,8 @@ __global__ void __launch_bounds__(P* LPB) sweep_x_kernel(SweepArgs a) {
 }
 
 // ----------------------------------------------------------------------------------------- Y sweep
-template <class M, int TX, int TY>
-__global__ void __launch_bounds__(TX) sweep_y_kernel(SweepArgs a) {
+template <class M, int TX, int TY, int MINB>
+__global__ void __launch_bounds__(TX, MINB) sweep_y_kernel(SweepArgs a) {
     constexpr int NU = M::NU, NW = M::NW;
     const int col = blockIdx.x * TX + threadIdx.x;
     const bool col_ok = col < a.nx;

@@ -2,36 +2,24 @@
 #include "physics_mixed.cuh"
 #include "slic_kernels.cuh"
 #include "slic_mixed.cuh"
+#include "sweep_table.cuh"
 #include "vg_ops.h"
 
 namespace vg {
 namespace {
 
-constexpr int XP = 128;
-constexpr int XL = 1;
-constexpr int YTX = 64;
-constexpr int YTY = 64;
 constexpr int MW_NT = 256;
 
-template <class M>
-cudaError_t sweep_impl(int axis, const SweepArgs& a, cudaStream_t st) {
-    if (axis == 0) {
-        dim3 grid((a.nx + XP - 3) / (XP - 2), (a.ny + XL - 1) / XL);
-        sweep_x_mixed_kernel<M, XP, XL><<<grid, XP * XL, 0, st>>>(a);
-    } else {
-        dim3 grid((a.nx + YTX - 1) / YTX, (a.ny + YTY - 1) / YTY);
-        sweep_y_mixed_kernel<M, YTX, YTY><<<grid, YTX, 0, st>>>(a);
+struct MixedKernels {
+    template <class M, int P, int LPB, int MINB>
+    static void x(dim3 grid, int nt, cudaStream_t st, const SweepArgs& a) {
+        sweep_x_mixed_kernel<M, P, LPB, MINB><<<grid, nt, 0, st>>>(a);
     }
-    return cudaGetLastError();
-}
-
-template <>
-cudaError_t sweep_impl<EulerMixed<1>>(int axis, const SweepArgs& a, cudaStream_t st) {
-    if (axis != 0) return cudaErrorInvalidValue;
-    dim3 grid((a.nx + XP - 3) / (XP - 2), (a.ny + XL - 1) / XL);
-    sweep_x_mixed_kernel<EulerMixed<1>, XP, XL><<<grid, XP * XL, 0, st>>>(a);
-    return cudaGetLastError();
-}
+    template <class M, int TX, int TY, int MINB>
+    static void y(dim3 grid, int nt, cudaStream_t st, const SweepArgs& a) {
+        sweep_y_mixed_kernel<M, TX, TY, MINB><<<grid, nt, 0, st>>>(a);
+    }
+};
 
 template <class M>
 cudaError_t max_wave_impl(const SweepArgs& a, cudaStream_t st) {
@@ -56,7 +44,8 @@ cudaError_t finish_impl(const SweepArgs& a, double* out, cudaStream_t st) {
 
 template <class M>
 constexpr Ops make_ops() {
-    return Ops{M::NW, &sweep_impl<M>, &max_wave_impl<M>, &step_begin_impl<M>, &finish_impl<M>};
+    return Ops{M::NW, SweepTable<MixedKernels, M>::x, SweepTable<MixedKernels, M>::y, &max_wave_impl<M>,
+               &step_begin_impl<M>, &finish_impl<M>};
 }
 
 const Ops kOps[V_COUNT] = {

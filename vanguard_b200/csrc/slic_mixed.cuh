@@ -1,29 +1,32 @@
 // Mixed FP32/FP64 SLIC sweep kernels (VG_MIXED), generic over a model policy from physics_mixed.cuh.
 // Same tiling as slic_kernels.cuh (staged shared-memory X sweep, register-marching Y sweep); states stay
-// FP64, slopes / fluxes / evolution increments are FP32, the update accumulates in FP64.
+// FP64, flux values and their combinations are FP32, the update accumulates in FP64.
 #pragma once
 
+#include "physics_mixed.cuh"
 #include "vg_common.cuh"
 
 namespace vg {
 
-__device__ __forceinline__ float limiter_f32(float r, float w, int id) {
-    if (r < 0.0f) return 0.0f;
-    float xi_r = __fdividef(2.0f, (1.0f - w) + (1.0f + w) * r);
+// Limiter of Solvers/slopelimiters.cpp:7-74 on the FP64 slope ratio; the ratio and xi_R use the hardware
+// reciprocal approximation (relative error ~2^-22), which only moves the limiter's kinks by that amount.
+__device__ __forceinline__ double limiter_approx(double r, double w, int id) {
+    if (r < 0.0) return 0.0;
+    double xi_r = 2.0 * rcp_approx((1.0 - w) + (1.0 + w) * r);
     if (id == 0) {
-        if (r < 0.5f) return 2.0f * r;
-        if (r < 1.0f) return 1.0f;
-        return fminf(fminf(r, xi_r), 2.0f);
+        if (r < 0.5) return 2.0 * r;
+        if (r < 1.0) return 1.0;
+        return fmin(fmin(r, xi_r), 2.0);
     } else if (id == 1) {
-        return fminf(__fdividef(2.0f * r, 1.0f + r), xi_r);
+        return fmin(2.0 * r * rcp_approx(1.0 + r), xi_r);
     }
-    if (r < 1.0f) return r;
-    return fminf(1.0f, xi_r);
+    if (r < 1.0) return r;
+    return fmin(1.0, xi_r);
 }
 
 struct MixedConst {
-    float half_r, r_f, rinv_f, cm, cp, bias, floor5;
-    double r;
+    float half_r, r_f, rinv_f;
+    double r, cm, cp, bias, floor5;
     int limiter;
 };
 
@@ -34,10 +37,10 @@ __device__ __forceinline__ MixedConst mixed_const(const SweepArgs& a, double& ts
     k.r_f = (float)k.r;
     k.rinv_f = (float)(a.dx / ts);
     k.half_r = (float)(0.5 * k.r);
-    k.cm = (float)(0.5 * (1.0 + a.bias));
-    k.cp = (float)(0.5 * (1.0 - a.bias));
-    k.bias = (float)a.bias;
-    k.floor5 = 1e-5f;
+    k.cm = 0.5 * (1.0 + a.bias);
+    k.cp = 0.5 * (1.0 - a.bias);
+    k.bias = a.bias;
+    k.floor5 = a.floor5;
     k.limiter = a.limiter;
     return k;
 }
@@ -52,13 +55,11 @@ __device__ __forceinline__ void evolve_edges_mixed(const double* uL, const doubl
     double xl[NU], xr[NU];
 #pragma unroll
     for (int i = 0; i < NU; i++) {
-        float dm = (float)(u[i] - uL[i]);
-        float dp = (float)(uR[i] - u[i]);
-        float s = fmaf(k.cm, dm, k.cp * dp);
-        float num = fabsf(dm) < k.floor5 ? k.floor5 : dm;
-        float den = fabsf(dp) < k.floor5 ? k.floor5 : dp;
-        s *= limiter_f32(__fdividef(num, den), k.bias, k.limiter);
-        double hs = (double)(0.5f * s);
+        double dm = u[i] - uL[i];
+        double dp = uR[i] - u[i];
+        double num = fabs(dm) < k.floor5 ? k.floor5 : dm;
+        double den = fabs(dp) < k.floor5 ? k.floor5 : dp;
+        double hs = 0.5 * fma(k.cm, dm, k.cp * dp) * limiter_approx(num * rcp_approx(den), k.bias, k.limiter);
         xl[i] = u[i] - hs;
         xr[i] = u[i] + hs;
     }
@@ -99,13 +100,13 @@ __device__ __forceinline__ bool bad_state_mixed(const double* W) {
 }
 
 // ----------------------------------------------------------------------------------------- X sweep
-template <class M, int P, int LPB>
-__global__ void __launch_bounds__(P* LPB) sweep_x_mixed_kernel(SweepArgs a) {
+template <class M, int P, int LPB, int MINB>
+__global__ void __launch_bounds__(P* LPB, MINB) sweep_x_mixed_kernel(SweepArgs a) {
     constexpr int NU = M::NU, NW = M::NW;
     constexpr int NT = P * LPB;
     __shared__ double Us[NU][LPB][P + 2];
     __shared__ double Es[NU][LPB][P];
-    __shared__ float Fs[NU][LPB][P];
+    __shared__ double Fs[NU][LPB][P];  // interface fluxes, widened once to FP64 for the update
 
     const int p = threadIdx.x % P, l = threadIdx.x / P;
     const int row = blockIdx.y * LPB + l;
@@ -161,7 +162,7 @@ __global__ void __launch_bounds__(P* LPB) sweep_x_mixed_kernel(SweepArgs a) {
         for (int v = 0; v < NU; v++) ua[v] = Es[v][l][p - 1];
         force_flux_mixed<M, 0>(ua, ub, k, q, F);
 #pragma unroll
-        for (int v = 0; v < NU; v++) Fs[v][l][p] = F[v];
+        for (int v = 0; v < NU; v++) Fs[v][l][p] = (double)F[v];
     }
     __syncthreads();
 
@@ -170,7 +171,7 @@ __global__ void __launch_bounds__(P* LPB) sweep_x_mixed_kernel(SweepArgs a) {
         double Un[NU], W[NW];
 #pragma unroll
         for (int v = 0; v < NU; v++)
-            Un[v] = fma(k.r, (double)Fs[v][l][p] - (double)Fs[v][l][p + 1], Us[v][l][p + 1]);
+            Un[v] = fma(k.r, Fs[v][l][p] - Fs[v][l][p + 1], Us[v][l][p + 1]);
         M::setcons(Un, q, W);
 #pragma unroll
         for (int v = 0; v < NW; v++) a.out[v * a.plane + rowbase + cell] = W[v];
@@ -188,8 +189,8 @@ __global__ void __launch_bounds__(P* LPB) sweep_x_mixed_kernel(SweepArgs a) {
 }
 
 // ----------------------------------------------------------------------------------------- Y sweep
-template <class M, int TX, int TY>
-__global__ void __launch_bounds__(TX) sweep_y_mixed_kernel(SweepArgs a) {
+template <class M, int TX, int TY, int MINB>
+__global__ void __launch_bounds__(TX, MINB) sweep_y_mixed_kernel(SweepArgs a) {
     constexpr int NU = M::NU, NW = M::NW;
     const int col = blockIdx.x * TX + threadIdx.x;
     const bool col_ok = col < a.nx;
@@ -208,23 +209,25 @@ __global__ void __launch_bounds__(TX) sweep_y_mixed_kernel(SweepArgs a) {
     const MixedConst k = mixed_const(a, ts);
     const typename M::P q = M::params(a.params, a.ctrl ? a.ctrl->ch : a.ch_host);
 
-    auto conserve = [&](int r, double* U) {
+    auto load = [&](int r, double* W) {
         int rr = ghost_index(r, len, a.periodic);
-        double W[NW];
 #pragma unroll
         for (int v = 0; v < NW; v++) W[v] = a.in[v * a.plane + (long)rr * a.pitch + c];
-        M::cons(W, q, U);
     };
 
-    double um1[NU], u0[NU], up1[NU], ua_prev[NU], dummy[NU];
-    float f_prev[NU];
+    double um1[NU], u0[NU], up1[NU], ua_prev[NU], dummy[NU], f_prev[NU], wnext[NW];
     double wave = 0.0;
-    conserve(r0 - 2, up1);
-    conserve(r0 - 1, um1);
-    conserve(r0, u0);
+    load(r0 - 2, wnext);
+    M::cons(wnext, q, up1);
+    load(r0 - 1, wnext);
+    M::cons(wnext, q, um1);
+    load(r0, wnext);
+    M::cons(wnext, q, u0);
+    load(r0 + 1, wnext);  // prefetched one row ahead of its use
     evolve_edges_mixed<M, 1>(up1, um1, u0, k, q, dummy, ua_prev);
     for (int r = r0; r <= r1; r++) {
-        conserve(r + 1, up1);
+        M::cons(wnext, q, up1);
+        if (r < r1) load(r + 2, wnext);
         double ub[NU], ua_next[NU];
         evolve_edges_mixed<M, 1>(um1, u0, up1, k, q, ub, ua_next);
         float F[NU];
@@ -232,7 +235,7 @@ __global__ void __launch_bounds__(TX) sweep_y_mixed_kernel(SweepArgs a) {
         if (r > r0 && col_ok) {
             double Un[NU], W[NW];
 #pragma unroll
-            for (int v = 0; v < NU; v++) Un[v] = fma(k.r, (double)f_prev[v] - (double)F[v], um1[v]);
+            for (int v = 0; v < NU; v++) Un[v] = fma(k.r, f_prev[v] - (double)F[v], um1[v]);
             M::setcons(Un, q, W);
 #pragma unroll
             for (int v = 0; v < NW; v++) a.out[v * a.plane + (long)(r - 1) * a.pitch + c] = W[v];
@@ -244,7 +247,7 @@ __global__ void __launch_bounds__(TX) sweep_y_mixed_kernel(SweepArgs a) {
         }
 #pragma unroll
         for (int v = 0; v < NU; v++) {
-            f_prev[v] = F[v];
+            f_prev[v] = (double)F[v];
             ua_prev[v] = ua_next[v];
             um1[v] = u0[v];
             u0[v] = up1[v];

@@ -1,0 +1,62 @@
+// Launch-configuration tables of the sweep kernels, shared by the FP64 and mixed translation units.
+//
+// Every model/precision instantiates the same candidate tile shapes.  The tile shape only changes which
+// thread computes which cell, never the arithmetic of a cell, so all candidates produce identical results;
+// the autotuner (vg_autotune in vg_api.cu) times them on the caller's grid and keeps the fastest.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "vg_common.cuh"
+
+namespace vg {
+
+using SweepFn = cudaError_t (*)(const SweepArgs&, cudaStream_t);
+
+constexpr int kNumXCfg = 5;
+constexpr int kNumYCfg = 6;
+
+// X sweep: P cells per segment (P-2 outputs), LPB segments per block, MINB = minimum resident blocks
+// per SM requested from the register allocator (1: no register cap).
+template <class K, class M, int P, int LPB, int MINB>
+cudaError_t launch_x(const SweepArgs& a, cudaStream_t st) {
+    dim3 grid((a.nx + P - 3) / (P - 2), (a.ny + LPB - 1) / LPB);
+    K::template x<M, P, LPB, MINB>(grid, P * LPB, st, a);
+    return cudaGetLastError();
+}
+
+// Y sweep: TX columns per block, TY rows marched per thread, MINB as above.
+template <class K, class M, int TX, int TY, int MINB>
+cudaError_t launch_y(const SweepArgs& a, cudaStream_t st) {
+    if constexpr (!M::HAS_Y) {
+        return cudaErrorInvalidValue;
+    } else {
+        dim3 grid((a.nx + TX - 1) / TX, (a.ny + TY - 1) / TY);
+        K::template y<M, TX, TY, MINB>(grid, TX, st, a);
+        return cudaGetLastError();
+    }
+}
+
+template <class K, class M>
+struct SweepTable {
+    static constexpr SweepFn x[kNumXCfg] = {
+        launch_x<K, M, 128, 1, 1>, launch_x<K, M, 64, 2, 1>, launch_x<K, M, 192, 1, 1>,
+        launch_x<K, M, 128, 1, 6>, launch_x<K, M, 128, 1, 8>,
+    };
+    static constexpr SweepFn y[kNumYCfg] = {
+        launch_y<K, M, 64, 64, 1>, launch_y<K, M, 64, 32, 1>, launch_y<K, M, 64, 64, 12>,
+        launch_y<K, M, 64, 64, 16>, launch_y<K, M, 128, 32, 5>, launch_y<K, M, 32, 64, 1>,
+    };
+};
+
+inline const char* x_cfg_name(int i) {
+    static const char* n[kNumXCfg] = {"P128xL1", "P64xL2", "P192xL1", "P128xL1/min6", "P128xL1/min8"};
+    return (i >= 0 && i < kNumXCfg) ? n[i] : "?";
+}
+inline const char* y_cfg_name(int i) {
+    static const char* n[kNumYCfg] = {"TX64xTY64", "TX64xTY32", "TX64xTY64/min12", "TX64xTY64/min16",
+                                      "TX128xTY32/min5", "TX32xTY64"};
+    return (i >= 0 && i < kNumYCfg) ? n[i] : "?";
+}
+
+}  // namespace vg

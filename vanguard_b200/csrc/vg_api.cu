@@ -5,6 +5,7 @@
 #include <climits>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -76,11 +77,64 @@ struct vg_solver {
         int variant = -1;
     } g;
     long last_launches = 0;
+    int xcfg = 0, ycfg = 0;   // launch configuration of each sweep (sweep_table.cuh)
 };
 
 namespace {
 
 constexpr int kChunk = 16;  // steps per captured chunk (even: a chunk returns to buffer 0 in 1D and 2D)
+
+cudaError_t run_sweep(const vg_solver* s, int axis, const SweepArgs& a, cudaStream_t st) {
+    return axis == 0 ? s->ops->x[s->xcfg](a, st) : s->ops->y[s->ycfg](a, st);
+}
+
+// In-process cache of tuned launch configurations keyed by variant, precision, grid and SM count;
+// optionally persisted in the text file named by VG_TUNE_CACHE ("key xcfg ycfg" per line).
+struct TuneEntry {
+    std::string key;
+    int xcfg, ycfg;
+};
+std::vector<TuneEntry> g_tune_cache;
+bool g_tune_loaded = false;
+
+std::string tune_key(const vg_solver* s) {
+    int dev = s->d.device, sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    char buf[160];
+    std::snprintf(buf, sizeof(buf), "v%d_p%d_b%d_%dx%d_sm%d", s->variant, s->d.precision, s->d.boundary, s->d.nx,
+                  s->d.ny, sms);
+    return buf;
+}
+
+void tune_cache_load() {
+    if (g_tune_loaded) return;
+    g_tune_loaded = true;
+    const char* path = std::getenv("VG_TUNE_CACHE");
+    if (!path) return;
+    FILE* f = std::fopen(path, "r");
+    if (!f) return;
+    char key[160];
+    int x, y;
+    while (std::fscanf(f, "%159s %d %d", key, &x, &y) == 3)
+        if (x >= 0 && x < vg::kNumXCfg && y >= 0 && y < vg::kNumYCfg) g_tune_cache.push_back({key, x, y});
+    std::fclose(f);
+}
+
+void tune_cache_store(const std::string& key, int x, int y) {
+    for (auto& e : g_tune_cache)
+        if (e.key == key) {
+            e.xcfg = x;
+            e.ycfg = y;
+            return;
+        }
+    g_tune_cache.push_back({key, x, y});
+    const char* path = std::getenv("VG_TUNE_CACHE");
+    if (!path) return;
+    FILE* f = std::fopen(path, "a");
+    if (!f) return;
+    std::fprintf(f, "%s %d %d\n", key.c_str(), x, y);
+    std::fclose(f);
+}
 
 SweepArgs base_args(const vg_solver* s) {
     SweepArgs a{};
@@ -114,24 +168,24 @@ int enqueue_step(vg_solver* s, const vg_run_config& c, int from, cudaStream_t st
         a.out = s->buf[1 - from];
         a.accumulate_wave = 1;
         a.advance_time = 1;
-        if (e == cudaSuccess) e = s->ops->sweep(0, a, st);
+        if (e == cudaSuccess) e = run_sweep(s, 0, a, st);
         n++;
     } else {
         // Solvers/secondordersolver.cpp:403-410: X(dt/2), Y(dt), X(dt/2)
         a.in = s->buf[from];
         a.out = s->buf[1 - from];
         a.dt_scale = 0.5;
-        if (e == cudaSuccess) e = s->ops->sweep(0, a, st);
+        if (e == cudaSuccess) e = run_sweep(s, 0, a, st);
         a.in = s->buf[1 - from];
         a.out = s->buf[from];
         a.dt_scale = 1.0;
-        if (e == cudaSuccess) e = s->ops->sweep(1, a, st);
+        if (e == cudaSuccess) e = run_sweep(s, 1, a, st);
         a.in = s->buf[from];
         a.out = s->buf[1 - from];
         a.dt_scale = 0.5;
         a.accumulate_wave = 1;
         a.advance_time = 1;
-        if (e == cudaSuccess) e = s->ops->sweep(0, a, st);
+        if (e == cudaSuccess) e = run_sweep(s, 0, a, st);
         n += 3;
     }
     *err = e;
@@ -424,7 +478,7 @@ vg_status vg_sweep(vg_solver* s, int axis, double dx, double dt, double bias, in
     a.limiter = limiter;
     a.in = s->buf[s->cur];
     a.out = s->buf[1 - s->cur];
-    VG_CUDA(s->ops->sweep(axis, a, st));
+    VG_CUDA(run_sweep(s, axis, a, st));
     s->cur = 1 - s->cur;
     s->last_launches = 1;
     return VG_OK;
@@ -459,5 +513,86 @@ vg_status vg_state_device(vg_solver* s, double** plane0, long* plane_stride, lon
 }
 
 long vg_last_launch_count(vg_solver* s) { return s ? s->last_launches : 0; }
+
+vg_status vg_set_launch_config(vg_solver* s, int xcfg, int ycfg) {
+    if (!s) return fail(VG_EINVAL, "null solver");
+    if (xcfg < 0 || xcfg >= vg::kNumXCfg || ycfg < 0 || ycfg >= vg::kNumYCfg)
+        return fail(VG_EINVAL, "launch configuration index out of range");
+    if (s->xcfg != xcfg || s->ycfg != ycfg) destroy_graphs(s);
+    s->xcfg = xcfg;
+    s->ycfg = ycfg;
+    return VG_OK;
+}
+
+vg_status vg_get_launch_config(vg_solver* s, int* xcfg, int* ycfg, const char** xname, const char** yname) {
+    if (!s) return fail(VG_EINVAL, "null solver");
+    if (xcfg) *xcfg = s->xcfg;
+    if (ycfg) *ycfg = s->ycfg;
+    if (xname) *xname = vg::x_cfg_name(s->xcfg);
+    if (yname) *yname = vg::y_cfg_name(s->ycfg);
+    return VG_OK;
+}
+
+vg_status vg_autotune(vg_solver* s, const vg_run_config* cfg, int reps, float* times_ms, void* stream) {
+    if (!s || !cfg) return fail(VG_EINVAL, "null argument");
+    if (!s->ops) return fail(VG_EINVAL, "no state uploaded");
+    if (!(cfg->dx > 0.0)) return fail(VG_EINVAL, "dx must be positive");
+    if (reps < 1) reps = 3;
+    tune_cache_load();
+    std::string key = tune_key(s);
+    if (!times_ms) {
+        for (auto& e : g_tune_cache)
+            if (e.key == key) return vg_set_launch_config(s, e.xcfg, e.ycfg);
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    // Time every candidate on the uploaded state: out-of-place sweeps into the spare buffer, with the
+    // time step the current state would take (so the limiter and flux paths are the ones a run takes).
+    double smax = 0.0;
+    vg_status vs = vg_max_wave_speed(s, &smax, stream);
+    if (vs != VG_OK) return vs;
+    double dt = cfg->cfl * (cfg->dx / (smax > 0.0 ? smax : 1.0));
+    SweepArgs a = base_args(s);
+    a.ctrl = nullptr;
+    a.dt_host = dt;
+    a.dx = cfg->dx;
+    a.bias = cfg->bias;
+    a.limiter = cfg->limiter;
+    a.in = s->buf[s->cur];
+    a.out = s->buf[1 - s->cur];
+    cudaEvent_t e0, e1;
+    VG_CUDA(cudaEventCreate(&e0));
+    VG_CUDA(cudaEventCreate(&e1));
+    float best[2] = {1e30f, 1e30f};
+    int pick[2] = {0, 0};
+    for (int axis = 0; axis < s->dims; axis++) {
+        int n = axis == 0 ? vg::kNumXCfg : vg::kNumYCfg;
+        for (int c = 0; c < n; c++) {
+            const vg::SweepFn fn = axis == 0 ? s->ops->x[c] : s->ops->y[c];
+            cudaError_t e = fn(a, st);  // warm-up (module load, caches)
+            if (e != cudaSuccess) {
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                return cuda_fail(e, "autotune launch");
+            }
+            VG_CUDA(cudaEventRecord(e0, st));
+            for (int r = 0; r < reps; r++) fn(a, st);
+            VG_CUDA(cudaEventRecord(e1, st));
+            VG_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.0f;
+            VG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            ms /= reps;
+            if (times_ms) times_ms[axis * vg::kNumXCfg + c] = ms;
+            if (ms < best[axis]) {
+                best[axis] = ms;
+                pick[axis] = c;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    VG_CUDA(cudaGetLastError());
+    tune_cache_store(key, pick[0], pick[1]);
+    return vg_set_launch_config(s, pick[0], pick[1]);
+}
 
 }  // extern "C"

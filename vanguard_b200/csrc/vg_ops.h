@@ -5,6 +5,7 @@
 
 #include <string>
 
+#include "sweep_table.cuh"
 #include "vg_common.cuh"
 
 namespace vg {
@@ -20,8 +21,9 @@ enum Variant : int {
 
 struct Ops {
     int nw;  // carried primitive planes
-    // One sweep (axis 0 = X, 1 = Y).  a.in / a.out must not alias.
-    cudaError_t (*sweep)(int axis, const SweepArgs& a, cudaStream_t st);
+    // One sweep per launch configuration (see sweep_table.cuh).  a.in / a.out must not alias.
+    const SweepFn* x;
+    const SweepFn* y;
     // Maximum wave speed of a.in folded into ctrl->smax_next (caller zeroes it first).
     cudaError_t (*max_wave)(const SweepArgs& a, cudaStream_t st);
     // dt for the next step from ctrl->smax_next (and corner ghosts in 2D); zeroes smax_next.
@@ -37,8 +39,5 @@ const Ops* ops_mixed(int variant);
 
 // Record the text returned by vg_last_error_string() on this thread.
 void set_last_error(const std::string& msg);
-
-// Kernels launched by one sweep / max_wave / step_begin call (for launch accounting).
-inline int launches_per_sweep() { return 1; }
 
 }  // namespace vg
