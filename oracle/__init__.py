@@ -77,6 +77,8 @@ def lib():
                                    _c_int, _D, _D]
         L.vo_nvar.restype = _c_int
         L.vo_nparams.restype = _c_int
+        L.vo_forcing.argtypes = [_c_int, _D, _c_int, _c_int, _c_double, _c_double, _c_double, _c_int, _D, _c_int]
+        L.vo_hpr_cell.argtypes = [_D, _D, _D, _D, _D, _D, _D]
         _lib = L
     return _lib
 
@@ -111,6 +113,8 @@ def ref():
         R.vgref_mhd2d_run.restype = _c_double
         R.vgref_mhd2d_run.argtypes = [_D, _c_int, _c_int, _c_double, _c_double, _c_double, _c_int,
                                       _c_double, _c_int, _D, _c_int, _c_int, _I]
+        if hasattr(R, "vgref_hpr_cell"):
+            R.vgref_hpr_cell.argtypes = [_D, _D, _D, _D, _D, _D, _D]
         if hasattr(R, "vgref_hpr2d_run"):
             R.vgref_hpr2d_run.restype = _c_double
             R.vgref_hpr2d_run.argtypes = [_D, _c_int, _c_int, _c_double, _c_double, _c_double, _c_int,
@@ -156,6 +160,25 @@ def max_wave(model, planes, params):
     if planes.ndim == 2:
         return lib().vo_max_wave1d(model, _ptr(planes), planes.shape[1], _ptr(prm))
     return lib().vo_max_wave2d(model, _ptr(planes), planes.shape[2], planes.shape[1], _ptr(prm))
+
+
+def forcing(planes, dx, dt, bias=0.0, limiter=SUPERBEE, params=None, bc=TRANSMISSIVE):
+    """One HPR RK4 relaxation-source sub-cycle over the grid (restatement), in place."""
+    _check(planes, NVAR[HPR])
+    prm = np.ascontiguousarray(params, dtype=np.float64)
+    nx, ny = (planes.shape[2], planes.shape[1]) if planes.ndim == 3 else (planes.shape[1], 1)
+    lib().vo_forcing(HPR, _ptr(planes), nx, ny, dx, dt, bias, limiter, _ptr(prm), bc)
+
+
+def hpr_cell(w, params, reference=False):
+    """(U, F_x, F_y, S, (speed_x, speed_y)) of one HPR primitive state, from the restatement or the reference."""
+    w = np.ascontiguousarray(w, dtype=np.float64)
+    prm = np.ascontiguousarray(params, dtype=np.float64)
+    outs = [np.zeros(17) for _ in range(4)]
+    sp = np.zeros(2)
+    fn = ref().vgref_hpr_cell if reference else lib().vo_hpr_cell
+    fn(_ptr(w), _ptr(prm), *[_ptr(o) for o in outs], _ptr(sp))
+    return (*outs, sp)
 
 
 # ------------------------------------------------------------------------------------ reference

@@ -130,6 +130,38 @@ MHDMaterialParameters mhdParams(const double* prm) {
     return mp;
 }
 
+// ------------------------------------------------------------------------------------------------ HPR
+// Plane order = HPRStateVector primitive order (HPR/hprstatevector.cpp:50-73):
+// rho, p, A(9, row-major), u, v, w, Jx, Jy, Jz.
+// prm = {gamma, p_inf, c_v, rho0, T0, c_s, alpha, tau1, tau2, T_ref, p_ref, is_thermal}; StiffenedGas,
+// non-plastic (HPR/hprmaterialparameters.cpp:34-69 argument order).
+HPRMaterialParameters hprParams(const double* prm) {
+    return HPRMaterialParameters("StiffenedGas", prm[11] != 0.0, false, 8.31445985, prm[3], prm[10], prm[9], prm[4], prm[2],
+                                 prm[0], prm[1], 0.0, 0.0, 0.0, 0.0, prm[5], prm[7], prm[8], 1.0e-2, 0.75, 0.0, 1.0, prm[6],
+                                 0.0, 0.0, 0.0);
+}
+
+HPRStateVector hprCell(const double* planes, long plane, long k) {
+    vector<vector<double> > A(3, vector<double>(3));
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) A[i][j] = planes[(2 + 3 * i + j) * plane + k];
+    return HPRStateVector(planes[k], planes[plane + k], A, planes[11 * plane + k], planes[12 * plane + k],
+                          planes[13 * plane + k], planes[14 * plane + k], planes[15 * plane + k], planes[16 * plane + k]);
+}
+
+void hprStore(HPRStateVector& c, double* planes, long plane, long k) {
+    planes[k] = c.getDensity();
+    planes[plane + k] = c.getPressure();
+    vector<vector<double> > A = c.getDistortionTensor();
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) planes[(2 + 3 * i + j) * plane + k] = A[i][j];
+    planes[11 * plane + k] = c.getXVelocity();
+    planes[12 * plane + k] = c.getYVelocity();
+    planes[13 * plane + k] = c.getZVelocity();
+    planes[14 * plane + k] = c.getXThermalImpulse();
+    planes[15 * plane + k] = c.getYThermalImpulse();
+    planes[16 * plane + k] = c.getZThermalImpulse();
+}
 }  // namespace
 
 extern "C" {
@@ -330,3 +362,113 @@ double vgref_mhd2d_run(double* planes, int nx, int ny, double dx, double cfl, do
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------- HPR 1D/2D
+// planes: 17 x cells.  subcycles > 0 runs HPRForcingSolver's RK4 relaxation source around the sweeps as
+// solve()/solve2D() do (Solvers/hprsecondordersolver.cpp:323-341, :514-541).
+extern "C" double vgref_hpr1d_run(double* planes, int n, double dx, double cfl, double t_end, int max_steps,
+                                  double bias, int limiter, const double* prm, int bc, int subcycles, int* steps_out) {
+    QuietCout quiet;
+    HPRMaterialParameters mp = hprParams(prm);
+    vector<HPRStateVector> cells(n);
+    for (int i = 0; i < n; i++) cells[i] = hprCell(planes, n, i);
+    double t = 0.0;
+    int it = 0;
+    if (max_steps <= 0 && bc == 0) {
+        cells = HPRSecondOrderSolver::solve(cells, dx, cfl, t_end, bias, limiter, subcycles, mp);
+        t = -1.0;
+        it = -1;
+    } else {
+        double tEnd = t_end > 0.0 ? t_end : kNoEnd;
+        int limit = max_steps > 0 ? max_steps : 0x7fffffff;
+        auto ghosts = [&](vector<HPRStateVector>& c, int b) {
+            return bc == 1 ? periodicGhosts1D(c, b) : HPRSolvers::insertBoundaryCells(c, b);
+        };
+        while (t < tEnd && it < limit) {
+            vector<HPRStateVector> withB = ghosts(cells, 2);
+            double dt = HPRSolvers::computeStableTimeStep(withB, dx, cfl, t, tEnd, it, mp);
+            for (int s = 0; s < subcycles; s++) {
+                withB = ghosts(cells, 1);
+                HPRForcingSolver::computeRungeKuttaTimeStep(cells, withB, dx, 0.5 * (dt / subcycles), bias, limiter, mp);
+            }
+            withB = ghosts(cells, 2);
+            HPRSecondOrderSolver::computeSLICTimeStep(cells, withB, dx, dt, bias, limiter, mp);
+            for (int s = 0; s < subcycles; s++) {
+                withB = ghosts(cells, 1);
+                HPRForcingSolver::computeRungeKuttaTimeStep(cells, withB, dx, 0.5 * (dt / subcycles), bias, limiter, mp);
+            }
+            t += dt;
+            it += 1;
+        }
+    }
+    for (int i = 0; i < n; i++) hprStore(cells[i], planes, n, i);
+    if (steps_out) *steps_out = it;
+    return t;
+}
+
+extern "C" double vgref_hpr2d_run(double* planes, int nx, int ny, double dx, double cfl, double t_end, int max_steps,
+                                  double bias, int limiter, const double* prm, int bc, int subcycles, int* steps_out) {
+    QuietCout quiet;
+    HPRMaterialParameters mp = hprParams(prm);
+    long plane = (long)nx * ny;
+    vector<vector<HPRStateVector> > cells(ny, vector<HPRStateVector>(nx));
+    for (int i = 0; i < ny; i++)
+        for (int j = 0; j < nx; j++) cells[i][j] = hprCell(planes, plane, (long)i * nx + j);
+    double t = 0.0;
+    int it = 0;
+    if (max_steps <= 0 && bc == 0) {
+        cells = HPRSecondOrderSolver::solve2D(cells, dx, cfl, t_end, bias, limiter, subcycles, mp);
+        t = -1.0;
+        it = -1;
+    } else {
+        double tEnd = t_end > 0.0 ? t_end : kNoEnd;
+        int limit = max_steps > 0 ? max_steps : 0x7fffffff;
+        auto ghosts = [&](vector<vector<HPRStateVector> >& c, int b) {
+            return bc == 1 ? periodicGhosts2D(c, b) : HPRSolvers::insertBoundaryCells2D(c, b);
+        };
+        while (t < tEnd && it < limit) {
+            vector<vector<HPRStateVector> > withB = ghosts(cells, 2);
+            double dt = HPRSolvers::computeStableTimeStep2D(withB, dx, cfl, t, tEnd, it, mp);
+            for (int s = 0; s < subcycles; s++) {
+                withB = ghosts(cells, 1);
+                HPRForcingSolver::computeRungeKuttaTimeStep2D(cells, withB, dx, 0.5 * (dt / subcycles), bias, limiter, mp);
+            }
+            withB = ghosts(cells, 2);
+            HPRSecondOrderSolver::computeXSLICTimeStep2D(cells, withB, dx, 0.5 * dt, bias, limiter, mp);
+            withB = ghosts(cells, 2);
+            HPRSecondOrderSolver::computeYSLICTimeStep2D(cells, withB, dx, dt, bias, limiter, mp);
+            withB = ghosts(cells, 2);
+            HPRSecondOrderSolver::computeXSLICTimeStep2D(cells, withB, dx, 0.5 * dt, bias, limiter, mp);
+            for (int s = 0; s < subcycles; s++) {
+                withB = ghosts(cells, 1);
+                HPRForcingSolver::computeRungeKuttaTimeStep2D(cells, withB, dx, 0.5 * (dt / subcycles), bias, limiter, mp);
+            }
+            t += dt;
+            it += 1;
+        }
+    }
+    for (int i = 0; i < ny; i++)
+        for (int j = 0; j < nx; j++) hprStore(cells[i][j], planes, plane, (long)i * nx + j);
+    if (steps_out) *steps_out = it;
+    return t;
+}
+
+// Single-cell probes of the HPR model for unit tests: cons (U[17]), x/y flux of a conserved vector,
+// source term of a conserved vector, and the acoustic-tensor wave speed in a direction.
+extern "C" void vgref_hpr_cell(const double* w, const double* prm, double* u, double* fx, double* fy, double* src,
+                               double* speed_xy) {
+    HPRMaterialParameters mp = hprParams(prm);
+    HPRStateVector s = hprCell(w, 1, 0);
+    vector<double> U = s.computeConservedVariableVector(mp);
+    vector<double> Fx = HPRStateVector::computeXFluxVector(U, mp);
+    vector<double> Fy = HPRStateVector::computeYFluxVector(U, mp);
+    vector<double> S = HPRStateVector::computeSourceTermVector(U, mp);
+    for (int i = 0; i < 17; i++) {
+        u[i] = U[i];
+        fx[i] = Fx[i];
+        fy[i] = Fy[i];
+        src[i] = S[i];
+    }
+    speed_xy[0] = HPRAcousticTensor::computeMaximumWaveSpeed(s, mp, 0);
+    speed_xy[1] = HPRAcousticTensor::computeMaximumWaveSpeed(s, mp, 1);
+}

@@ -234,19 +234,345 @@ static void mhd_default(const double* prm, double* W) {
     W[0] = 1.0; W[4] = 1.0;
 }
 
+
+/* ---- HPR / GPR with the StiffenedGas Mie-Grueneisen branch, non-plastic.
+ * prm = {gamma, p_inf, c_v, rho0, T0, c_s, alpha, tau1, tau2, T_ref, p_ref, is_thermal}.
+ * W = rho, p, A(9 row-major), u, v, w, Jx, Jy, Jz;  U = rho, rho E, A(9), rho v(3), rho J(3).
+ * Matrix products sum from 0.0 in index order (MatrixAlgebra::multiplyMatrices,
+ * Mathematics/matrixalgebra.cpp:62-81). */
+
+typedef struct { double m[3][3]; } mat3;
+
+/* MatrixAlgebra::multiplyMatrices of two 3x3 matrices */
+static mat3 mm3(const mat3* a, const mat3* b) {
+    mat3 r;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+            double s = 0.0;
+            for (int k = 0; k < 3; k++) s += a->m[i][k] * b->m[k][j];
+            r.m[i][j] = s;
+        }
+    return r;
+}
+static mat3 tr3(const mat3* a) {
+    mat3 r;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) r.m[j][i] = a->m[i][j];
+    return r;
+}
+static mat3 load_A(const double* a9) {
+    mat3 r;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) r.m[i][j] = a9[3 * i + j];
+    return r;
+}
+/* TensorAlgebra::computeDeviator (Mathematics/tensoralgebra.cpp:27-30): G + (-1 * ((tr/3) * I)) */
+static mat3 deviator3(const mat3* g) {
+    double tr = ((0.0 + g->m[0][0]) + g->m[1][1]) + g->m[2][2];
+    double c = tr / 3.0;
+    mat3 r;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) r.m[i][j] = g->m[i][j] + (-1.0 * (c * (i == j ? 1.0 : 0.0)));
+    return r;
+}
+/* MatrixAlgebra::computeDeterminant (Mathematics/matrixalgebra.cpp:131-135) */
+static double det3(const mat3* a) {
+    const double(*m)[3] = a->m;
+    return ((m[0][0] * ((m[1][1] * m[2][2]) - (m[2][1] * m[1][2]))) - (m[0][1] * ((m[1][0] * m[2][2]) - (m[1][2] * m[2][0])))) +
+           (m[0][2] * ((m[1][0] * m[2][1]) - (m[1][1] * m[2][0])));
+}
+static double hpr_gm1(const double* prm) { return prm[0] - 1.0; }           /* HPR/hprmiegruneisen.cpp:11-16 */
+static double hpr_pref(const double* prm) { return -prm[1]; }               /* :34-39 */
+static double hpr_eref(double rho, const double* prm) { return prm[1] / rho; } /* :72-77 */
+/* HPRMieGruneisen::computeInternalEnergy / computePressure / computeTemperature (:194-221) */
+static double mg_energy(double rho, double p, const double* prm) {
+    return hpr_eref(rho, prm) + ((p - hpr_pref(prm)) / (rho * hpr_gm1(prm)));
+}
+static double mg_pressure(double rho, double e, const double* prm) {
+    return (((e - hpr_eref(rho, prm)) * rho) * hpr_gm1(prm)) + hpr_pref(prm);
+}
+static double mg_temperature(double rho, double p, const double* prm) {
+    return prm[9] + ((p - hpr_pref(prm)) / ((rho * hpr_gm1(prm)) * prm[2]));
+}
+/* HPRMieGruneisen::computeInternalEnergyDerivativeDensity (:223-234) for StiffenedGas */
+static double mg_dedrho(double rho, double p, const double* prm) {
+    double G = hpr_gm1(prm), dG = 0.0, pr = hpr_pref(prm), dpr = 0.0, der = -(prm[1] / (rho * rho));
+    return der - ((((dpr * rho) * G) + ((G + (rho * dG)) * (p - pr))) / ((rho * G) * (rho * G)));
+}
+static double mg_dedp(double rho, const double* prm) { return 1.0 / (rho * hpr_gm1(prm)); } /* :236-241 */
+static double mg_dTdrho(double rho, double p, const double* prm) {                          /* :243-255 */
+    double G = hpr_gm1(prm), dG = 0.0, pr = hpr_pref(prm), dpr = 0.0;
+    return (-(((dpr * rho) * G) + ((G + (rho * dG)) * (p - pr)))) / (((rho * G) * (rho * G)) / prm[2]);
+}
+static double mg_dTdp(double rho, const double* prm) { return mg_dedp(rho, prm) / prm[2]; } /* :257-262 */
+
+/* HPREquationOfState::computeMesoscaleDistortionEnergy (HPR/hprequationofstate.cpp:12-19) */
+static double meso_distortion(const mat3* A, const double* prm) {
+    mat3 At = tr3(A), G = mm3(&At, A), D = deviator3(&G);
+    double sum = 0.0;
+    for (int i = 0; i < 3; i++) {
+        double row = 0.0;
+        for (int j = 0; j < 3; j++) row += D.m[i][j] * D.m[i][j];
+        sum += row;
+    }
+    return (0.25 * (prm[5] * prm[5])) * sum;
+}
+static double meso_thermal(double jx, double jy, double jz, const double* prm) {   /* :21-27 */
+    return (0.5 * (prm[6] * prm[6])) * (((jx * jx) + (jy * jy)) + (jz * jz));
+}
+static double macro_energy(double u, double v, double w) { return 0.5 * (((u * u) + (v * v)) + (w * w)); } /* :29-34 */
+static int hpr_thermal(const double* prm) { return prm[11] != 0.0; }
+/* HPREquationOfState::computeTotalEnergy / computePressure (:36-62) */
+static double hpr_total_energy(double rho, double p, double u, double v, double w, const mat3* A, double jx, double jy,
+                               double jz, const double* prm) {
+    double E = (mg_energy(rho, p, prm) + meso_distortion(A, prm)) + macro_energy(u, v, w);
+    if (hpr_thermal(prm)) E += meso_thermal(jx, jy, jz, prm);
+    return E;
+}
+static double hpr_pressure(double rho, double E, double u, double v, double w, const mat3* A, double jx, double jy, double jz,
+                           const double* prm) {
+    double e = E - (macro_energy(u, v, w) + meso_distortion(A, prm));
+    if (hpr_thermal(prm)) e -= meso_thermal(jx, jy, jz, prm);
+    return mg_pressure(rho, e, prm);
+}
+/* HPRDerivatives::computeTotalEnergyDerivativeDistortionTensor (HPR/hprderivatives.cpp:17-25): c_s^2 (A dev(A^T A)) */
+static mat3 dE_dA(const mat3* A, const double* prm) {
+    mat3 At = tr3(A), G = mm3(&At, A), D = deviator3(&G), AD = mm3(A, &D), r;
+    double cs2 = prm[5] * prm[5];
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) r.m[i][j] = cs2 * AD.m[i][j];
+    return r;
+}
+/* HPREquationOfState::computeShearStressTensor (:76-81): -rho A^T dE/dA */
+static mat3 shear_stress(double rho, const mat3* A, const double* prm) {
+    mat3 d = dE_dA(A, prm), At = tr3(A), P = mm3(&At, &d), r;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) r.m[i][j] = (-rho) * P.m[i][j];
+    return r;
+}
+
+/* HPRStateVector::computeConservedVariableVector (HPR/hprstatevector.cpp:134-162) */
+static void hpr_cons(const double* W, const double* prm, double* U) {
+    mat3 A = load_A(W + 2);
+    double rho = W[0];
+    for (int i = 0; i < 17; i++) U[i] = 0.0;
+    U[0] = rho;
+    U[1] = rho * hpr_total_energy(rho, W[1], W[11], W[12], W[13], &A, W[14], W[15], W[16], prm);
+    for (int i = 0; i < 9; i++) U[2 + i] = W[2 + i];
+    U[11] = rho * W[11];
+    U[12] = rho * W[12];
+    U[13] = rho * W[13];
+    if (hpr_thermal(prm)) {
+        U[14] = rho * W[14];
+        U[15] = rho * W[15];
+        U[16] = rho * W[16];
+    }
+}
+/* HPRStateVector::setConservedVariableVector (HPR/hprstatevector.cpp:78-103); J kept when not thermal */
+static void hpr_setcons(const double* U, const double* prm, double* W) {
+    double rho = U[0];
+    W[0] = rho;
+    for (int i = 0; i < 9; i++) W[2 + i] = U[2 + i];
+    W[11] = U[11] / rho;
+    W[12] = U[12] / rho;
+    W[13] = U[13] / rho;
+    if (hpr_thermal(prm)) {
+        W[14] = U[14] / rho;
+        W[15] = U[15] / rho;
+        W[16] = U[16] / rho;
+    }
+    mat3 A = load_A(W + 2);
+    W[1] = hpr_pressure(rho, U[1] / rho, W[11], W[12], W[13], &A, W[14], W[15], W[16], prm);
+}
+/* HPRStateVector::compute{X,Y}FluxVector (HPR/hprstatevector.cpp:164-228, :235-298) */
+static void hpr_flux(const double* U, int axis, const double* prm, double* F) {
+    double rho = U[0];
+    mat3 A = load_A(U + 2);
+    mat3 sig = shear_stress(rho, &A, prm);
+    double u = U[11] / rho, v = U[12] / rho, w = U[13] / rho;
+    double jx = U[14] / rho, jy = U[15] / rho, jz = U[16] / rho;
+    double E = U[1] / rho;
+    double p = hpr_pressure(rho, E, u, v, w, &A, jx, jy, jz, prm);
+    double vel[3] = {u, v, w};
+    double un = axis == 0 ? u : v;
+    for (int i = 0; i < 17; i++) F[i] = 0.0;
+    F[0] = rho * un;
+    F[1] = (rho * (un * E)) + (p * un);
+    if (axis == 0) {
+        F[11] = (rho * (u * u)) + p;
+        F[12] = rho * (u * v);
+        F[13] = rho * (u * w);
+    } else {
+        F[11] = rho * (v * u);
+        F[12] = (rho * (v * v)) + p;
+        F[13] = rho * (v * w);
+    }
+    /* MatrixAlgebra::multiplyMatrixByVector (Mathematics/matrixalgebra.cpp:97-106): sums from 0.0 */
+    double Av[3];
+    for (int i = 0; i < 3; i++) Av[i] = ((0.0 + (A.m[i][0] * u)) + (A.m[i][1] * v)) + (A.m[i][2] * w);
+    F[1] -= ((0.0 + (sig.m[axis][0] * vel[0])) + (sig.m[axis][1] * vel[1])) + (sig.m[axis][2] * vel[2]);
+    for (int i = 0; i < 3; i++) F[11 + i] -= sig.m[axis][i];
+    for (int i = 0; i < 3; i++) F[2 + (i * 3) + axis] = Av[i];
+    if (hpr_thermal(prm)) {
+        double T = mg_temperature(rho, p, prm);
+        double a2 = prm[6] * prm[6];
+        double q[3] = {T * (a2 * jx), T * (a2 * jy), T * (a2 * jz)};
+        F[1] += q[axis];
+        if (axis == 0) {
+            F[14] = (rho * (u * jx)) + T;
+            F[15] = rho * (u * jy);
+            F[16] = rho * (u * jz);
+        } else {
+            F[14] = rho * (v * jx);
+            F[15] = (rho * (v * jy)) + T;
+            F[16] = rho * (v * jz);
+        }
+    }
+}
+/* HPRStateVector::computeSourceTermVector (HPR/hprstatevector.cpp:312-366) with HPRSourceTerms
+ * (HPR/hprsourceterms.cpp:7-39), non-plastic branch */
+static void hpr_source(const double* U, const double* prm, double* S) {
+    double rho = U[0];
+    mat3 A = load_A(U + 2);
+    mat3 d = dE_dA(&A, prm);
+    double cs2 = prm[5] * prm[5];
+    double th1 = 3.0 * (pow(det3(&A), (5.0 / 3.0)) / (cs2 * prm[7]));
+    for (int i = 0; i < 17; i++) S[i] = 0.0;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) S[2 + (i * 3) + j] = -d.m[i][j] * th1;
+    if (hpr_thermal(prm)) {
+        double E = U[1] / rho;
+        double u = U[11] / rho, v = U[12] / rho, w = U[13] / rho;
+        double jx = U[14] / rho, jy = U[15] / rho, jz = U[16] / rho;
+        double p = hpr_pressure(rho, E, u, v, w, &A, jx, jy, jz, prm);
+        double T = mg_temperature(rho, p, prm);
+        double a2 = prm[6] * prm[6];
+        double dj[3] = {a2 * jx, a2 * jy, a2 * jz};
+        double th2 = 1.0 / ((a2 * prm[8]) * ((rho / prm[3]) * (prm[4] / T)));
+        for (int i = 0; i < 3; i++) S[14 + i] = ((-rho) * th2) * dj[i];
+    }
+}
+
+/* HPRAcousticTensor::computeMaximumWaveSpeed (HPR/hpracoustictensor.cpp:7-97) with the 10-step power
+ * iteration of MatrixAlgebra::computeLargestEigenvalue (Mathematics/matrixalgebra.cpp:182-199).
+ * Only the entries dsigma/dA[d][i][j][d] of HPREquationOfState::computeShearStressTensorDerivativeDistortionTensor
+ * (HPR/hprequationofstate.cpp:83-113) enter; they are rebuilt here with the same sums and the same order of
+ * the two += updates (the i == d entries receive the update twice, in the same loop iteration). */
+static double hpr_acoustic_speed(const double* W, int d, const double* prm) {
+    double rho = W[0], p = W[1];
+    mat3 A = load_A(W + 2);
+    mat3 At = tr3(&A), G = mm3(&At, &A), D = deviator3(&G);
+    mat3 AD = mm3(&A, &D), M = tr3(&AD);
+    double cs2 = prm[5] * prm[5];
+    double dsdA[3][3];
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+            /* P[a][b][c][e] = 0 + G[a][b] A[c][e]; T[a][b][c][e] = (P[e][b][c][a] + P[a][e][c][b]) + (-1 ((2/3) P[a][b][c][e]))
+             * at a = d, b = i, c = j, e = d */
+            double s1 = 0.0 + (G.m[d][i] * A.m[j][d]);
+            double s2 = 0.0 + (G.m[d][d] * A.m[j][i]);
+            double pp = 0.0 + (G.m[d][i] * A.m[j][d]);
+            double t = (s1 + s2) + (-1.0 * ((2.0 / 3.0) * pp));
+            t += M.m[i][j];
+            if (i == d) t += M.m[d][j];
+            dsdA[i][j] = (-(rho * cs2)) * t;
+        }
+    mat3 dEdA = dE_dA(&A, prm), Pd = mm3(&At, &dEdA), dsdrho, sig;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+            dsdrho.m[i][j] = -1.0 * Pd.m[i][j];
+            sig.m[i][j] = (-rho) * Pd.m[i][j];
+        }
+    double c1[4][5], c2[5][4];
+    memset(c1, 0, sizeof(c1));
+    memset(c2, 0, sizeof(c2));
+    c1[0][1] = 1.0 / rho;
+    for (int i = 0; i < 3; i++) c1[i][0] = -(1.0 / rho) * dsdrho.m[d][i];
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) c1[i][2 + j] = -(1.0 / rho) * dsdA[i][j];
+    if (hpr_thermal(prm)) {
+        c1[3][0] = mg_dTdrho(rho, p, prm) / rho;
+        c1[3][1] = mg_dTdp(rho, prm) / rho;
+    }
+    /* HPRWaveSpeeds::computeAdiabaticSoundSpeed (HPR/hprwavespeeds.cpp:7-13) */
+    double cad = sqrt(((p / (rho * rho)) - mg_dedrho(rho, p, prm)) / mg_dedp(rho, prm));
+    c2[0][0] = rho;
+    c2[1][d] = rho * (cad * cad);
+    for (int i = 0; i < 3; i++) c2[1][i] += sig.m[d][i] - (rho * dsdrho.m[d][i]);
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) c2[2 + i][j] = A.m[i][j];
+    if (hpr_thermal(prm)) {
+        double T = mg_temperature(rho, p, prm);
+        double dTdp = mg_dTdp(rho, prm);
+        double ch = (sqrt((prm[6] * prm[6]) * (T / prm[2]))) / rho;  /* HPR/hprwavespeeds.cpp:15-21 */
+        c2[1][3] = rho * ((ch * ch) / dTdp);
+    }
+    double om[4][4];
+    for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 4; j++) {
+            double s = 0.0;
+            for (int k = 0; k < 5; k++) s += c1[i][k] * c2[k][j];
+            om[i][j] = s;
+        }
+    double x[4] = {1.0, 1.0, 1.0, 1.0}, y[4];
+    for (int it = 0; it < 10; it++) {
+        for (int i = 0; i < 4; i++) {
+            double s = 0.0;
+            for (int k = 0; k < 4; k++) s += om[i][k] * x[k];
+            y[i] = s;
+        }
+        double n2 = 0.0;
+        for (int i = 0; i < 4; i++) n2 += y[i] * y[i];
+        double inv = 1.0 / sqrt(n2);
+        for (int i = 0; i < 4; i++) x[i] = inv * y[i];
+    }
+    for (int i = 0; i < 4; i++) {
+        double s = 0.0;
+        for (int k = 0; k < 4; k++) s += om[i][k] * x[k];
+        y[i] = s;
+    }
+    double n2 = 0.0;
+    for (int i = 0; i < 4; i++) n2 += y[i] * y[i];
+    return sqrt(sqrt(n2));
+}
+/* HPRSolvers::computeMaximumWaveSpeed{,2D} per-cell terms (Solvers/hprsolvers.cpp:286-303, :362-385) */
+static double hpr_wave1d(const double* W, const double* prm) { return fabs(W[11]) + hpr_acoustic_speed(W, 0, prm); }
+static double hpr_wave2d(const double* W, const double* prm) {
+    return smax(fabs(W[11]), fabs(W[12])) + smax(hpr_acoustic_speed(W, 0, prm), hpr_acoustic_speed(W, 1, prm));
+}
+/* HPRStateVector() (HPR/hprstatevector.cpp:3-16): rho 1, p 1/1.4, A = 1^(1/3) I */
+static void hpr_default(const double* prm, double* W) {
+    (void)prm;
+    for (int i = 0; i < 17; i++) W[i] = 0.0;
+    double c = pow(1.0, (1.0 / 3.0));
+    W[0] = 1.0;
+    W[1] = 1.0 / 1.4;
+    W[2] = c * 1.0;
+    W[3] = c * 0.0;
+    W[4] = c * 0.0;
+    W[5] = c * 0.0;
+    W[6] = c * 1.0;
+    W[7] = c * 0.0;
+    W[8] = c * 0.0;
+    W[9] = c * 0.0;
+    W[10] = c * 1.0;
+}
+
 static const model M_EULER = {6, euler_cons, euler_setcons, euler_flux, euler_wave1d, euler_wave2d, euler_default};
 static const model M_MHD = {9, mhd_cons, mhd_setcons, mhd_flux, mhd_wave1d, mhd_wave2d, mhd_default};
+static const model M_HPR = {17, hpr_cons, hpr_setcons, hpr_flux, hpr_wave1d, hpr_wave2d, hpr_default};
 
 static const model* model_of(int id) {
     switch (id) {
         case VO_EULER: return &M_EULER;
         case VO_MHD: return &M_MHD;
+        case VO_HPR: return &M_HPR;
         default: return NULL;
     }
 }
 
 int vo_nvar(int id) { const model* m = model_of(id); return m ? m->nv : 0; }
-int vo_nparams(int id) { return id == VO_EULER ? 6 : id == VO_MHD ? 3 : 0; }
+int vo_nparams(int id) { return id == VO_EULER ? 6 : id == VO_MHD ? 3 : id == VO_HPR ? 12 : 0; }
 
 /* ------------------------------------------------------------------------------- SLIC building blocks */
 
@@ -399,6 +725,128 @@ double vo_max_wave2d(int id, const double* planes, int nx, int ny, const double*
     return m ? max_wave(m, planes, (long)nx * ny, 2, prm) : 0.0;
 }
 
+/* ------------------------------------------------------------------------- HPR relaxation source (RK4) */
+
+/* HPRSolvers::evolveStateByFractional{X,Y}TimeStep (Solvers/hprsolvers.cpp:606-620, :673-687) with
+ * evolveStateByFractionalTimeStep (:791-797): the middle state advanced by frac * dt of the flux difference of
+ * its own slope-limited edge values; returns primitives (default-constructed target). */
+static void frac_evolve(const model* m, double frac, const double* wl, const double* wm, const double* wr, int axis,
+                        double dx, double dt, double w, int lim, const double* prm, double* out) {
+    double uL[MAXV], uM[MAXV], uR[MAXV], s[MAXV], xl[MAXV], xr[MAXV], fl[MAXV], fr[MAXV], sum[MAXV];
+    int nv = m->nv;
+    m->cons(wl, prm, uL);
+    m->cons(wm, prm, uM);
+    m->cons(wr, prm, uR);
+    slope_vector(nv, uL, uM, uR, w, lim, s);
+    for (int i = 0; i < nv; i++) {
+        xl[i] = uM[i] + (-1.0 * (0.5 * s[i]));
+        xr[i] = uM[i] + (0.5 * s[i]);
+    }
+    m->flux(xl, axis, prm, fl);
+    m->flux(xr, axis, prm, fr);
+    double c = frac * (dt / dx);   /* Solvers::computeFractionalEvolutionVector (Solvers/solvers.cpp:606-609) */
+    for (int i = 0; i < nv; i++) sum[i] = uM[i] + (c * (fl[i] + (-1.0 * fr[i])));
+    m->default_state(prm, out);
+    m->setcons(sum, prm, out);
+}
+
+static void prim_of(const model* m, const double* u, const double* prm, double* w) {
+    m->default_state(prm, w);
+    m->setcons(u, prm, w);
+}
+
+/* HPRForcingSolver::evolveConservedVariableVector{,2D} (Solvers/hprforcingsolver.cpp:7-44, :134-194) and
+ * computeEvolvedConservedVariableVector (:332-339).  dims == 1 uses the X predictor alone with fractions
+ * (1/2, 1/2, 1); dims == 2 the X(f/2) Y(f) X(f/2) predictor with f = 1/2, 1/2, 1. */
+static void rk4_source(const model* m, const double* uLf, const double* uM, const double* uRf, const double* uTf,
+                       const double* uBf, int dims, double dx, double dt, double w, int lim, const double* prm,
+                       double* result) {
+    int nv = m->nv;
+    double wl[MAXV], wr[MAXV], wt[MAXV], wb[MAXV], wm[MAXV], e1[MAXV], e2[MAXV], e[MAXV], ue[MAXV], S[MAXV];
+    double k[4][MAXV], ut[MAXV];
+    prim_of(m, uLf, prm, wl);
+    prim_of(m, uRf, prm, wr);
+    if (dims == 2) {
+        prim_of(m, uTf, prm, wt);
+        prim_of(m, uBf, prm, wb);
+    }
+    m->default_state(prm, wm);
+    hpr_source(uM, prm, S);
+    for (int i = 0; i < nv; i++) k[0][i] = dt * S[i];
+    static const double stage[3] = {0.5, 0.5, 1.0};
+    for (int s = 0; s < 3; s++) {
+        for (int i = 0; i < nv; i++) ut[i] = uM[i] + (s < 2 ? (0.5 * k[s][i]) : k[s][i]);
+        m->setcons(ut, prm, wm);
+        double f = stage[s];
+        if (dims == 1) {
+            frac_evolve(m, f, wl, wm, wr, 0, dx, dt, w, lim, prm, e);
+        } else {
+            frac_evolve(m, 0.5 * f, wl, wm, wr, 0, dx, dt, w, lim, prm, e1);
+            frac_evolve(m, f, wt, e1, wb, 1, dx, dt, w, lim, prm, e2);
+            frac_evolve(m, 0.5 * f, wl, e2, wr, 0, dx, dt, w, lim, prm, e);
+        }
+        m->cons(e, prm, ue);
+        hpr_source(ue, prm, S);
+        for (int i = 0; i < nv; i++) k[s + 1][i] = dt * S[i];
+    }
+    for (int i = 0; i < nv; i++)
+        result[i] = uM[i] + ((1.0 / 6.0) * (k[0][i] + ((2.0 * k[1][i]) + ((2.0 * k[2][i]) + k[3][i]))));
+}
+
+/* 1-ghost boundary of insertBoundaryCells{,2D}(cells, 1): transmissive copies g[-1] = c[0], g[n] = c[n-1]
+ * (Solvers/hprsolvers.cpp, same layout as Solvers/solvers.cpp:11-15) or wrap-around. */
+static int ghost1(int k, int n, int bc) {
+    if (k >= 0 && k < n) return k;
+    if (bc == VO_BC_PERIODIC) return k < 0 ? k + n : k - n;
+    return k < 0 ? 0 : n - 1;
+}
+
+/* HPRForcingSolver::computeRungeKuttaTimeStep{,2D} (Solvers/hprforcingsolver.cpp:341-357, :394-418) */
+static void forcing_grid(const model* m, double* planes, int nx, int ny, int dims, double dx, double dt, double w,
+                         int lim, const double* prm, int bc) {
+    long plane = (long)nx * ny;
+    int nv = m->nv;
+    double* out = (double*)malloc(sizeof(double) * nv * plane);
+#pragma omp parallel for schedule(static)
+    for (long idx = 0; idx < plane; idx++) {
+        int i = (int)(idx / nx), j = (int)(idx - (long)i * nx);
+        double W[MAXV], uL[MAXV], uM[MAXV], uR[MAXV], uT[MAXV], uB[MAXV], res[MAXV];
+        load_cell(planes, plane, (long)i * nx + ghost1(j - 1, nx, bc), nv, W);
+        m->cons(W, prm, uL);
+        load_cell(planes, plane, (long)i * nx + ghost1(j + 1, nx, bc), nv, W);
+        m->cons(W, prm, uR);
+        if (dims == 2) {
+            load_cell(planes, plane, (long)ghost1(i - 1, ny, bc) * nx + j, nv, W);
+            m->cons(W, prm, uT);
+            load_cell(planes, plane, (long)ghost1(i + 1, ny, bc) * nx + j, nv, W);
+            m->cons(W, prm, uB);
+        }
+        load_cell(planes, plane, idx, nv, W);
+        m->cons(W, prm, uM);
+        rk4_source(m, uL, uM, uR, uT, uB, dims, dx, dt, w, lim, prm, res);
+        m->setcons(res, prm, W);
+        for (int v = 0; v < nv; v++) out[v * plane + idx] = W[v];
+    }
+    memcpy(planes, out, sizeof(double) * nv * plane);
+    free(out);
+}
+
+void vo_forcing(int id, double* planes, int nx, int ny, double dx, double dt, double w, int lim, const double* prm,
+                int bc) {
+    const model* m = model_of(id);
+    if (!m || id != VO_HPR) return;
+    forcing_grid(m, planes, nx, ny, ny > 1 ? 2 : 1, dx, dt, w, lim, prm, bc);
+}
+
+void vo_hpr_cell(const double* w, const double* prm, double* u, double* fx, double* fy, double* src, double* speed_xy) {
+    hpr_cons(w, prm, u);
+    hpr_flux(u, 0, prm, fx);
+    hpr_flux(u, 1, prm, fy);
+    hpr_source(u, prm, src);
+    speed_xy[0] = hpr_acoustic_speed(w, 0, prm);
+    speed_xy[1] = hpr_acoustic_speed(w, 1, prm);
+}
+
 /* Solvers::computeStableTimeStep(dt, t, tEnd, it), Solvers/solvers.cpp:437-452 */
 static double stable_dt(double dt, double t, double t_end, int it) {
     double d = dt;
@@ -411,22 +859,26 @@ static double stable_dt(double dt, double t, double t_end, int it) {
  * c_h = padded-grid maximum wave speed before the sweeps (Solvers/mhdsecondordersolver.cpp:330-332,
  * :513-515). */
 static double run(int id, double* planes, int nx, int ny, int dims, double dx, double cfl, double t_end,
-                  int max_steps, double w, int lim, const double* prm_in, int bc, int* steps_out,
+                  int max_steps, double w, int lim, const double* prm_in, int bc, int subcycles, int* steps_out,
                   double* dt_log) {
     const model* m = model_of(id);
     if (!m) return -1.0;
-    double prm[8];
+    double prm[16];
     memcpy(prm, prm_in, sizeof(double) * vo_nparams(id));
     double tEnd = t_end > 0.0 ? t_end : 1.0e300;
     int limit = max_steps > 0 ? max_steps : 0x7fffffff;
     long plane = (long)nx * ny;
     double t = 0.0;
     int it = 0;
+    int sub = id == VO_HPR ? subcycles : 0;
     while (t < tEnd && it < limit) {
         double smax_ = max_wave(m, planes, plane, dims, prm);
         double dt = stable_dt(cfl * (dx / smax_), t, tEnd, it);
         if (id == VO_MHD) prm[2] = smax_;
         if (dt_log) dt_log[it] = dt;
+        /* HPR: sub-cycled RK4 relaxation source before and after the sweeps
+         * (Solvers/hprsecondordersolver.cpp:323-341, :514-541) */
+        for (int s = 0; s < sub; s++) forcing_grid(m, planes, nx, ny, dims, dx, 0.5 * (dt / sub), w, lim, prm, bc);
         if (dims == 1) {
             sweep_grid(m, planes, nx, 1, 0, dx, dt, w, lim, prm, bc);
         } else {
@@ -434,6 +886,7 @@ static double run(int id, double* planes, int nx, int ny, int dims, double dx, d
             sweep_grid(m, planes, nx, ny, 1, dx, dt, w, lim, prm, bc);
             sweep_grid(m, planes, nx, ny, 0, dx, 0.5 * dt, w, lim, prm, bc);
         }
+        for (int s = 0; s < sub; s++) forcing_grid(m, planes, nx, ny, dims, dx, 0.5 * (dt / sub), w, lim, prm, bc);
         t += dt;
         it += 1;
     }
@@ -443,14 +896,12 @@ static double run(int id, double* planes, int nx, int ny, int dims, double dx, d
 
 double vo_run1d(int id, double* planes, int n, double dx, double cfl, double t_end, int max_steps, double w,
                 int lim, const double* prm, int bc, int subcycles, int* steps_out, double* dt_log) {
-    (void)subcycles;
-    return run(id, planes, n, 1, 1, dx, cfl, t_end, max_steps, w, lim, prm, bc, steps_out, dt_log);
+    return run(id, planes, n, 1, 1, dx, cfl, t_end, max_steps, w, lim, prm, bc, subcycles, steps_out, dt_log);
 }
 
 double vo_run2d(int id, double* planes, int nx, int ny, double dx, double cfl, double t_end, int max_steps,
                 double w, int lim, const double* prm, int bc, int subcycles, int* steps_out, double* dt_log) {
-    (void)subcycles;
-    return run(id, planes, nx, ny, 2, dx, cfl, t_end, max_steps, w, lim, prm, bc, steps_out, dt_log);
+    return run(id, planes, nx, ny, 2, dx, cfl, t_end, max_steps, w, lim, prm, bc, subcycles, steps_out, dt_log);
 }
 
 /* ------------------------------------------------------------------------- unit-test building blocks */

@@ -53,6 +53,14 @@ void vo_sweep2d(int model, double* planes, int nx, int ny, int axis, double dx, 
 double vo_max_wave1d(int model, const double* planes, int n, const double* prm);
 double vo_max_wave2d(int model, const double* planes, int nx, int ny, const double* prm);
 
+/* One sub-cycle of the HPR RK4 relaxation-source solver over the grid (HPRForcingSolver::
+ * computeRungeKuttaTimeStep{,2D}, Solvers/hprforcingsolver.cpp:341-357, :394-418), in place. */
+void vo_forcing(int model, double* planes, int nx, int ny, double dx, double dt, double bias, int limiter,
+                const double* prm, int bc);
+
+/* HPR single-cell probe: conserved vector, x/y fluxes, source and acoustic-tensor speeds of primitives w. */
+void vo_hpr_cell(const double* w, const double* prm, double* u, double* fx, double* fy, double* src, double* speed_xy);
+
 /* Single-interface building blocks, exposed for unit tests of the device functions. */
 double vo_slope_limiter(double r, double bias, int limiter);
 void vo_prim_to_cons(int model, const double* w, const double* prm, double* u);

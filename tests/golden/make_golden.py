@@ -43,6 +43,16 @@ CASES = {
     "mhd1d_briowu200_superbee_t01": (O.MHD, lambda: wl.brio_wu_1d(200),
                                      dict(dx=1 / 200, cfl=0.8, t_end=0.1, steps=0, limiter=O.SUPERBEE,
                                           params=wl.mhd_params(2.0))),
+    # HPR, thermal, StiffenedGas ideal gas: sweeps only, then with the RK4 relaxation source sub-cycled
+    "hpr2d_smooth24x20_superbee_10": (O.HPR, lambda: wl.hpr_smooth_2d(24, 20, seed=3),
+                                      dict(dx=1 / 24, cfl=0.8, steps=10, limiter=O.SUPERBEE,
+                                           params=wl.hpr_params(tau1=1e-2, tau2=1e-2))),
+    "hpr2d_smooth16_rk4sub1_4": (O.HPR, lambda: wl.hpr_smooth_2d(16, 16, seed=4),
+                                 dict(dx=1 / 16, cfl=0.8, steps=4, limiter=O.SUPERBEE, subcycles=1,
+                                      params=wl.hpr_params(tau1=1e-2, tau2=1e-2))),
+    "hpr1d_heat100_rk4sub2_20": (O.HPR, lambda: wl.hpr_heat_conduction_1d(100),
+                                 dict(dx=1 / 100, cfl=0.8, steps=20, limiter=O.SUPERBEE, subcycles=2,
+                                      params=wl.hpr_params(tau1=1e-1, tau2=1e-1))),
 }
 
 

@@ -114,3 +114,31 @@ def test_reference_solve_matches_step_loop():
     O.ref_run(O.EULER, a, 1 / 200, 0.9, t_end=0.1, steps=0, limiter=2, params=prm)      # solve() itself
     O.ref_run(O.EULER, b, 1 / 200, 0.9, t_end=0.1, steps=100000, limiter=2, params=prm)  # step loop
     assert np.array_equal(a, b)
+
+
+@needs_ref
+@pytest.mark.parametrize("thermal", [True, False])
+def test_oracle_vs_reference_hpr_cell(thermal):
+    """Conserved vector, x/y fluxes, relaxation source and both acoustic-tensor speeds of random states."""
+    rng = np.random.default_rng(7 if thermal else 8)
+    for trial in range(6):
+        prm = wl.hpr_params(tau1=10 ** rng.uniform(-3, -1), tau2=10 ** rng.uniform(-3, -1), thermal=thermal,
+                            p_inf=0.25 * trial)
+        w = np.zeros(17)
+        w[0], w[1] = rng.uniform(0.5, 2.0), rng.uniform(0.5, 2.0)
+        w[2:11] = (np.eye(3) + 0.1 * rng.standard_normal((3, 3))).ravel()
+        w[11:14] = 0.3 * rng.standard_normal(3)
+        w[14:17] = 0.2 * rng.standard_normal(3)
+        for a, b in zip(O.hpr_cell(w, prm), O.hpr_cell(w, prm, reference=True)):
+            assert np.array_equal(a, b)
+
+
+@needs_ref
+@pytest.mark.parametrize("sub,bc", [(0, 1), (1, 0)])
+def test_oracle_vs_reference_hpr2d(sub, bc):
+    W = wl.hpr_smooth_2d(14, 12, seed=10 + sub)
+    a, b = W.copy(), W.copy()
+    prm = wl.hpr_params(tau1=2e-2, tau2=3e-2)
+    O.run(O.HPR, a, 1 / 14, 0.8, steps=3, limiter=1, params=prm, bc=bc, subcycles=sub)
+    O.ref_run(O.HPR, b, 1 / 14, 0.8, steps=3, limiter=1, params=prm, bc=bc, subcycles=sub)
+    assert np.array_equal(a, b)

@@ -85,6 +85,56 @@ def mhd_vortex_2d(nx=2048, ny=None, seed=0, gamma=5.0 / 3.0, amplitude=1e-3):
     return W
 
 
+HPR_NVAR = 17  # rho, p, A(9 row-major), u, v, w, Jx, Jy, Jz
+
+
+def hpr_params(gamma=1.4, p_inf=0.0, c_v=2.5, rho0=1.0, T0=1.0, c_s=1.0, alpha=1.0, tau1=1e-2, tau2=1e-2,
+               T_ref=0.0, p_ref=1.0, thermal=True):
+    """HPRMaterialParameters for the StiffenedGas equation of state (ideal gas when p_inf = 0), non-plastic:
+    {gamma, p_inf, c_v, rho0, T0, c_s, alpha, tau1, tau2, T_ref, p_ref, is_thermal}.  Defaults follow the
+    reference's heat-conduction scenario (HPR/hprtests.cpp:33-57): rho0 = 1, p_ref = 1, T_ref = 0, T0 = 1,
+    c_v = 2.5."""
+    return np.array([gamma, p_inf, c_v, rho0, T0, c_s, alpha, tau1, tau2, T_ref, p_ref, 1.0 if thermal else 0.0])
+
+
+def hpr_relaxation_times(seed):
+    """tau1, tau2 log-uniform on [1e-6, 1e-2] from `seed`."""
+    rng = np.random.default_rng(seed)
+    return 10.0 ** rng.uniform(-6.0, -2.0, 2)
+
+
+def hpr_smooth_2d(nx=1024, ny=None, seed=0):
+    """Seeded smooth field: rho = 1 + 0.2 sin(2 pi (k.x) + phi), velocity of magnitude <= 0.1 from seeded
+    Fourier phases, p = 1, A = I, J = 0 (A = I with rho != rho0 is not rho0 det A; the reference does not
+    enforce that relation)."""
+    ny = nx if ny is None else ny
+    x = (np.arange(nx) + 0.5) / nx
+    y = (np.arange(ny) + 0.5) / ny
+    X, Y = np.meshgrid(x, y)
+    rng = np.random.default_rng(seed)
+    kx, ky = rng.integers(1, 4, 2)
+    phi = rng.uniform(0, 2 * np.pi, 5)
+    W = np.zeros((HPR_NVAR, ny, nx))
+    W[0] = 1.0 + 0.2 * np.sin(2 * np.pi * (kx * X + ky * Y) + phi[0])
+    W[1] = 1.0
+    W[2] = W[6] = W[10] = 1.0
+    W[11] = 0.05 * (np.sin(2 * np.pi * Y + phi[1]) + np.cos(2 * np.pi * X + phi[2]))
+    W[12] = 0.05 * (np.sin(2 * np.pi * X + phi[3]) + np.cos(2 * np.pi * Y + phi[4]))
+    return W
+
+
+def hpr_heat_conduction_1d(n=200):
+    """HPRTests::solveHeatConductionProblem initial data (HPR/hprtests.cpp:42-53): rho = 2 | 0.5, p = 1,
+    A = rho^(1/3) I, split at i <= n/2."""
+    W = np.zeros((HPR_NVAR, n))
+    left = np.arange(n) <= 0.5 * n
+    W[0] = np.where(left, 2.0, 0.5)
+    W[1] = 1.0
+    a = np.where(left, 2.0 ** (1.0 / 3.0), 0.5 ** (1.0 / 3.0))
+    W[2] = W[6] = W[10] = a
+    return W
+
+
 def brio_wu_1d(n=400, gamma=2.0):
     """Brio-Wu-type MHD shock tube (MHDTests' first Dumbser test family): left (1, 0, 0, 0, 1, 0.75, 1, 0),
     right (0.125, 0, 0, 0, 0.1, 0.75, -1, 0), split at i <= n/2."""
