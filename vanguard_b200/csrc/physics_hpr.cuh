@@ -1,0 +1,338 @@
+// Exact-FP64 device restatement of the HPR / GPR model (StiffenedGas Mie-Grueneisen branch, non-plastic).
+//
+// Compiled with -fmad=false and IEEE division / square root; every expression keeps the reference's
+// association order (matrix products summed from 0.0 in index order, Mathematics/matrixalgebra.cpp:62-81),
+// so the sweeps and the CFL reproduce the reference bit for bit.  The relaxation source uses pow(det A, 5/3)
+// (HPR/hprsourceterms.cpp:21-26); CUDA's pow and glibc's may differ in the last place, so runs with the source
+// switched on agree with the reference to ~1e-15 relative rather than bitwise.
+//
+// W = (rho, p, A00..A22, u, v, w, Jx, Jy, Jz)   (HPR/hprstatevector.cpp:50-73)
+// U = (rho, rho E, A00..A22, rho u, rho v, rho w, rho Jx, rho Jy, rho Jz)   (HPR/hprstatevector.cpp:134-162)
+// params = {gamma, p_inf, c_v, rho0, T0, c_s, alpha, tau1, tau2, T_ref, p_ref, is_thermal}
+#pragma once
+
+#include "vg_common.cuh"
+
+namespace vg {
+
+struct HPRF64 {
+    static constexpr int NW = 17;
+    static constexpr int NU = 17;
+    static constexpr bool HAS_Y = true;
+    struct P {
+        double g, pinf, cv, rho0, T0, cs, alpha, tau1, tau2, Tref;
+        int thermal;
+        double ch2;
+    };
+    __device__ static P params(const double* prm, double /*ch*/) {
+        return P{prm[0], prm[1], prm[2], prm[3], prm[4], prm[5], prm[6], prm[7], prm[8], prm[9], prm[11] != 0.0, 0.0};
+    }
+
+    // ---- 3x3 algebra in the reference's order
+    struct M3 {
+        double m[3][3];
+    };
+    __device__ static M3 load(const double* a9) {
+        M3 r;
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) r.m[i][j] = a9[3 * i + j];
+        return r;
+    }
+    __device__ static M3 mul(const M3& a, const M3& b) {
+        M3 r;
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) r.m[i][j] = ((0.0 + (a.m[i][0] * b.m[0][j])) + (a.m[i][1] * b.m[1][j])) + (a.m[i][2] * b.m[2][j]);
+        return r;
+    }
+    __device__ static M3 tmul(const M3& a, const M3& b) {  // a^T b
+        M3 r;
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) r.m[i][j] = ((0.0 + (a.m[0][i] * b.m[0][j])) + (a.m[1][i] * b.m[1][j])) + (a.m[2][i] * b.m[2][j]);
+        return r;
+    }
+    // TensorAlgebra::computeDeviator (Mathematics/tensoralgebra.cpp:27-30)
+    __device__ static M3 dev(const M3& g) {
+        double c = (((0.0 + g.m[0][0]) + g.m[1][1]) + g.m[2][2]) / 3.0;
+        M3 r;
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) r.m[i][j] = g.m[i][j] + (-1.0 * (c * (i == j ? 1.0 : 0.0)));
+        return r;
+    }
+    __device__ static double det(const M3& a) {  // Mathematics/matrixalgebra.cpp:131-135
+        return ((a.m[0][0] * ((a.m[1][1] * a.m[2][2]) - (a.m[2][1] * a.m[1][2]))) -
+                (a.m[0][1] * ((a.m[1][0] * a.m[2][2]) - (a.m[1][2] * a.m[2][0])))) +
+               (a.m[0][2] * ((a.m[1][0] * a.m[2][1]) - (a.m[1][1] * a.m[2][0])));
+    }
+
+    // ---- StiffenedGas Mie-Grueneisen (HPR/hprmiegruneisen.cpp:7-262)
+    __device__ static double gm1(const P& q) { return q.g - 1.0; }
+    __device__ static double pref(const P& q) { return -q.pinf; }
+    __device__ static double eref(double rho, const P& q) { return q.pinf / rho; }
+    __device__ static double mg_energy(double rho, double p, const P& q) { return eref(rho, q) + ((p - pref(q)) / (rho * gm1(q))); }
+    __device__ static double mg_pressure(double rho, double e, const P& q) {
+        return (((e - eref(rho, q)) * rho) * gm1(q)) + pref(q);
+    }
+    __device__ static double mg_temperature(double rho, double p, const P& q) {
+        return q.Tref + ((p - pref(q)) / ((rho * gm1(q)) * q.cv));
+    }
+    __device__ static double mg_dedrho(double rho, double p, const P& q) {
+        double G = gm1(q), dG = 0.0, pr = pref(q), dpr = 0.0, der = -(q.pinf / (rho * rho));
+        return der - ((((dpr * rho) * G) + ((G + (rho * dG)) * (p - pr))) / ((rho * G) * (rho * G)));
+    }
+    __device__ static double mg_dedp(double rho, const P& q) { return 1.0 / (rho * gm1(q)); }
+    __device__ static double mg_dTdrho(double rho, double p, const P& q) {
+        double G = gm1(q), dG = 0.0, pr = pref(q), dpr = 0.0;
+        return (-(((dpr * rho) * G) + ((G + (rho * dG)) * (p - pr)))) / (((rho * G) * (rho * G)) / q.cv);
+    }
+    __device__ static double mg_dTdp(double rho, const P& q) { return mg_dedp(rho, q) / q.cv; }
+
+    // ---- HPREquationOfState (HPR/hprequationofstate.cpp:7-81)
+    __device__ static double meso_distortion(const M3& A, const P& q) {
+        M3 D = dev(tmul(A, A));
+        double sum = 0.0;
+#pragma unroll
+        for (int i = 0; i < 3; i++) sum += ((0.0 + (D.m[i][0] * D.m[i][0])) + (D.m[i][1] * D.m[i][1])) + (D.m[i][2] * D.m[i][2]);
+        return (0.25 * (q.cs * q.cs)) * sum;
+    }
+    __device__ static double meso_thermal(double jx, double jy, double jz, const P& q) {
+        return (0.5 * (q.alpha * q.alpha)) * (((jx * jx) + (jy * jy)) + (jz * jz));
+    }
+    __device__ static double macro(double u, double v, double w) { return 0.5 * (((u * u) + (v * v)) + (w * w)); }
+    __device__ static double total_energy(double rho, double p, double u, double v, double w, const M3& A, double jx, double jy,
+                                          double jz, const P& q) {
+        double E = (mg_energy(rho, p, q) + meso_distortion(A, q)) + macro(u, v, w);
+        if (q.thermal) E += meso_thermal(jx, jy, jz, q);
+        return E;
+    }
+    __device__ static double pressure_of(double rho, double E, double u, double v, double w, const M3& A, double jx, double jy,
+                                         double jz, const P& q) {
+        double e = E - (macro(u, v, w) + meso_distortion(A, q));
+        if (q.thermal) e -= meso_thermal(jx, jy, jz, q);
+        return mg_pressure(rho, e, q);
+    }
+    // c_s^2 A dev(A^T A)   (HPR/hprderivatives.cpp:17-25)
+    __device__ static M3 dEdA(const M3& A, const P& q) {
+        M3 AD = mul(A, dev(tmul(A, A)));
+        double cs2 = q.cs * q.cs;
+        M3 r;
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) r.m[i][j] = cs2 * AD.m[i][j];
+        return r;
+    }
+
+    // HPRStateVector::computeConservedVariableVector (HPR/hprstatevector.cpp:134-162)
+    __device__ static void cons(const double* W, const P& q, double* U) {
+        M3 A = load(W + 2);
+        double rho = W[0];
+        U[0] = rho;
+        U[1] = rho * total_energy(rho, W[1], W[11], W[12], W[13], A, W[14], W[15], W[16], q);
+#pragma unroll
+        for (int i = 0; i < 9; i++) U[2 + i] = W[2 + i];
+        U[11] = rho * W[11];
+        U[12] = rho * W[12];
+        U[13] = rho * W[13];
+        U[14] = q.thermal ? rho * W[14] : 0.0;
+        U[15] = q.thermal ? rho * W[15] : 0.0;
+        U[16] = q.thermal ? rho * W[16] : 0.0;
+    }
+    // HPRStateVector::setConservedVariableVector (HPR/hprstatevector.cpp:78-103); J kept when not thermal
+    __device__ static void setcons(const double* U, const P& q, double* W) {
+        double rho = U[0];
+        W[0] = rho;
+#pragma unroll
+        for (int i = 0; i < 9; i++) W[2 + i] = U[2 + i];
+        W[11] = U[11] / rho;
+        W[12] = U[12] / rho;
+        W[13] = U[13] / rho;
+        if (q.thermal) {
+            W[14] = U[14] / rho;
+            W[15] = U[15] / rho;
+            W[16] = U[16] / rho;
+        }
+        M3 A = load(W + 2);
+        W[1] = pressure_of(rho, U[1] / rho, W[11], W[12], W[13], A, W[14], W[15], W[16], q);
+    }
+    // HPRStateVector::compute{X,Y}FluxVector (HPR/hprstatevector.cpp:164-298)
+    template <int AXIS>
+    __device__ static void flux(const double* U, const P& q, double* F) {
+        double rho = U[0];
+        M3 A = load(U + 2);
+        M3 d = dEdA(A, q);
+        M3 Pm = tmul(A, d);
+        double sig[3];
+#pragma unroll
+        for (int i = 0; i < 3; i++) sig[i] = (-rho) * Pm.m[AXIS][i];
+        double u = U[11] / rho, v = U[12] / rho, w = U[13] / rho;
+        double jx = U[14] / rho, jy = U[15] / rho, jz = U[16] / rho;
+        double E = U[1] / rho;
+        double p = pressure_of(rho, E, u, v, w, A, jx, jy, jz, q);
+        double un = AXIS == 0 ? u : v;
+#pragma unroll
+        for (int i = 0; i < 17; i++) F[i] = 0.0;
+        F[0] = rho * un;
+        F[1] = (rho * (un * E)) + (p * un);
+        if (AXIS == 0) {
+            F[11] = (rho * (u * u)) + p;
+            F[12] = rho * (u * v);
+            F[13] = rho * (u * w);
+        } else {
+            F[11] = rho * (v * u);
+            F[12] = (rho * (v * v)) + p;
+            F[13] = rho * (v * w);
+        }
+        F[1] -= ((0.0 + (sig[0] * u)) + (sig[1] * v)) + (sig[2] * w);
+#pragma unroll
+        for (int i = 0; i < 3; i++) F[11 + i] -= sig[i];
+#pragma unroll
+        for (int i = 0; i < 3; i++) F[2 + (i * 3) + AXIS] = ((0.0 + (A.m[i][0] * u)) + (A.m[i][1] * v)) + (A.m[i][2] * w);
+        if (q.thermal) {
+            double T = mg_temperature(rho, p, q);
+            double a2 = q.alpha * q.alpha;
+            F[1] += T * (a2 * (AXIS == 0 ? jx : jy));
+            if (AXIS == 0) {
+                F[14] = (rho * (u * jx)) + T;
+                F[15] = rho * (u * jy);
+                F[16] = rho * (u * jz);
+            } else {
+                F[14] = rho * (v * jx);
+                F[15] = (rho * (v * jy)) + T;
+                F[16] = rho * (v * jz);
+            }
+        }
+    }
+    // HPRStateVector::computeSourceTermVector (HPR/hprstatevector.cpp:312-366), HPRSourceTerms (HPR/hprsourceterms.cpp:7-39)
+    __device__ static void source(const double* U, const P& q, double* S) {
+        double rho = U[0];
+        M3 A = load(U + 2);
+        M3 d = dEdA(A, q);
+        double cs2 = q.cs * q.cs;
+        double th1 = 3.0 * (pow(det(A), (5.0 / 3.0)) / (cs2 * q.tau1));
+#pragma unroll
+        for (int i = 0; i < 17; i++) S[i] = 0.0;
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) S[2 + (i * 3) + j] = -d.m[i][j] * th1;
+        if (q.thermal) {
+            double E = U[1] / rho;
+            double u = U[11] / rho, v = U[12] / rho, w = U[13] / rho;
+            double jx = U[14] / rho, jy = U[15] / rho, jz = U[16] / rho;
+            double p = pressure_of(rho, E, u, v, w, A, jx, jy, jz, q);
+            double T = mg_temperature(rho, p, q);
+            double a2 = q.alpha * q.alpha;
+            double th2 = 1.0 / ((a2 * q.tau2) * ((rho / q.rho0) * (q.T0 / T)));
+            S[14] = ((-rho) * th2) * (a2 * jx);
+            S[15] = ((-rho) * th2) * (a2 * jy);
+            S[16] = ((-rho) * th2) * (a2 * jz);
+        }
+    }
+
+    // HPRAcousticTensor::computeMaximumWaveSpeed (HPR/hpracoustictensor.cpp:7-97) with the 10-step power iteration of
+    // MatrixAlgebra::computeLargestEigenvalue (Mathematics/matrixalgebra.cpp:182-199).  Only the entries
+    // d sigma / d A [d][i][j][d] of HPREquationOfState::computeShearStressTensorDerivativeDistortionTensor
+    // (HPR/hprequationofstate.cpp:83-113) enter; the i == d entries receive its += update twice.
+    __device__ static double acoustic_speed(const double* W, int d, const P& q) {
+        double rho = W[0], p = W[1];
+        M3 A = load(W + 2);
+        M3 G = tmul(A, A), D = dev(G), AD = mul(A, D);
+        double cs2 = q.cs * q.cs;
+        double c1[4][5], c2[5][4];
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 5; j++) c1[i][j] = 0.0;
+#pragma unroll
+        for (int i = 0; i < 5; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) c2[i][j] = 0.0;
+        double ir = 1.0 / rho;
+        c1[0][1] = ir;
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                double s1 = 0.0 + (G.m[d][i] * A.m[j][d]);
+                double s2 = 0.0 + (G.m[d][d] * A.m[j][i]);
+                double pp = 0.0 + (G.m[d][i] * A.m[j][d]);
+                double t = (s1 + s2) + (-1.0 * ((2.0 / 3.0) * pp));
+                t += AD.m[j][i];
+                if (i == d) t += AD.m[j][d];
+                c1[i][2 + j] = -ir * ((-(rho * cs2)) * t);
+            }
+        M3 dd = dEdA(A, q);
+        M3 Pm = tmul(A, dd);
+#pragma unroll
+        for (int i = 0; i < 3; i++) c1[i][0] = -ir * (-1.0 * Pm.m[d][i]);
+        if (q.thermal) {
+            c1[3][0] = mg_dTdrho(rho, p, q) / rho;
+            c1[3][1] = mg_dTdp(rho, q) / rho;
+        }
+        double cad = sqrt(((p / (rho * rho)) - mg_dedrho(rho, p, q)) / mg_dedp(rho, q));
+        c2[0][0] = rho;
+        c2[1][d] = rho * (cad * cad);
+#pragma unroll
+        for (int i = 0; i < 3; i++) c2[1][i] += ((-rho) * Pm.m[d][i]) - (rho * (-1.0 * Pm.m[d][i]));
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) c2[2 + i][j] = A.m[i][j];
+        if (q.thermal) {
+            double T = mg_temperature(rho, p, q);
+            double dTdp = mg_dTdp(rho, q);
+            double ch = (sqrt((q.alpha * q.alpha) * (T / q.cv))) / rho;
+            c2[1][3] = rho * ((ch * ch) / dTdp);
+        }
+        double om[4][4];
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                double s = 0.0;
+#pragma unroll
+                for (int k = 0; k < 5; k++) s += c1[i][k] * c2[k][j];
+                om[i][j] = s;
+            }
+        double x[4] = {1.0, 1.0, 1.0, 1.0}, y[4];
+        for (int it = 0; it < 10; it++) {
+#pragma unroll
+            for (int i = 0; i < 4; i++) y[i] = (((0.0 + (om[i][0] * x[0])) + (om[i][1] * x[1])) + (om[i][2] * x[2])) + (om[i][3] * x[3]);
+            double n2 = (((0.0 + (y[0] * y[0])) + (y[1] * y[1])) + (y[2] * y[2])) + (y[3] * y[3]);
+            double inv = 1.0 / sqrt(n2);
+#pragma unroll
+            for (int i = 0; i < 4; i++) x[i] = inv * y[i];
+        }
+#pragma unroll
+        for (int i = 0; i < 4; i++) y[i] = (((0.0 + (om[i][0] * x[0])) + (om[i][1] * x[1])) + (om[i][2] * x[2])) + (om[i][3] * x[3]);
+        double n2 = (((0.0 + (y[0] * y[0])) + (y[1] * y[1])) + (y[2] * y[2])) + (y[3] * y[3]);
+        return sqrt(sqrt(n2));
+    }
+    // HPRSolvers::computeMaximumWaveSpeed{,2D} per-cell terms (Solvers/hprsolvers.cpp:286-303, :362-385)
+    __device__ static double wave(const double* W, const P& q, int dims) {
+        if (dims == 1) return fabs(W[11]) + acoustic_speed(W, 0, q);
+        return std_max(fabs(W[11]), fabs(W[12])) + std_max(acoustic_speed(W, 0, q), acoustic_speed(W, 1, q));
+    }
+    // HPRStateVector() (HPR/hprstatevector.cpp:3-16): rho 1, p 1/1.4, A = 1^(1/3) I = I
+    __device__ static void default_state(double* W) {
+#pragma unroll
+        for (int i = 0; i < 17; i++) W[i] = 0.0;
+        W[0] = 1.0;
+        W[1] = 1.0 / 1.4;
+        W[2] = 1.0;
+        W[6] = 1.0;
+        W[10] = 1.0;
+    }
+    __device__ static double density(const double* W) { return W[0]; }
+    __device__ static double pressure(const double* W) { return W[1]; }
+};
+
+}  // namespace vg

@@ -1,7 +1,9 @@
 // Exact-FP64 SLIC kernels.  This translation unit MUST be compiled with -fmad=false: the reference's
 // x86-64 build forms no fused multiply-adds, and bitwise parity depends on every product being rounded
 // before it is added.
+#include "forcing_kernels.cuh"
 #include "physics_fp64.cuh"
+#include "physics_hpr.cuh"
 #include "slic_kernels.cuh"
 #include "sweep_table.cuh"
 #include "vg_ops.h"
@@ -44,9 +46,29 @@ cudaError_t finish_impl(const SweepArgs& a, double* out, cudaStream_t st) {
 }
 
 template <class M>
-constexpr Ops make_ops() {
-    return Ops{M::NW, SweepTable<Fp64Kernels, M>::x, SweepTable<Fp64Kernels, M>::y, &max_wave_impl<M>,
-               &step_begin_impl<M>, &finish_impl<M>};
+cudaError_t forcing_impl(const SweepArgs& a, int subcycles, cudaStream_t st) {
+    long n = (long)a.nx * a.ny;
+    forcing_kernel<M><<<(unsigned)((n + 127) / 128), 128, 0, st>>>(a, subcycles);
+    return cudaGetLastError();
+}
+
+template <class M>
+constexpr Ops make_ops(bool with_source = false) {
+    return Ops{M::NW,
+               SweepTable<Fp64Kernels, M>::x,
+               SweepTable<Fp64Kernels, M>::y,
+               &max_wave_impl<M>,
+               &step_begin_impl<M>,
+               &finish_impl<M>,
+               nullptr,
+               (M::NU > 9)};
+}
+
+template <>
+constexpr Ops make_ops<HPRF64>(bool) {
+    return Ops{HPRF64::NW,        SweepTable<Fp64Kernels, HPRF64>::x, SweepTable<Fp64Kernels, HPRF64>::y,
+               &max_wave_impl<HPRF64>, &step_begin_impl<HPRF64>,         &finish_impl<HPRF64>,
+               &forcing_impl<HPRF64>,  true};
 }
 
 const Ops kOps[V_COUNT] = {
@@ -54,6 +76,7 @@ const Ops kOps[V_COUNT] = {
     make_ops<EulerF64<2>>(),
     make_ops<MHDF64<false>>(),
     make_ops<MHDF64<true>>(),
+    make_ops<HPRF64>(),
 };
 
 }  // namespace

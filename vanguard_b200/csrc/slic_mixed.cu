@@ -45,10 +45,10 @@ cudaError_t finish_impl(const SweepArgs& a, double* out, cudaStream_t st) {
 template <class M>
 constexpr Ops make_ops() {
     return Ops{M::NW, SweepTable<MixedKernels, M>::x, SweepTable<MixedKernels, M>::y, &max_wave_impl<M>,
-               &step_begin_impl<M>, &finish_impl<M>};
+               &step_begin_impl<M>, &finish_impl<M>, nullptr, false};
 }
 
-const Ops kOps[V_COUNT] = {
+const Ops kOps[V_HPR17] = {
     make_ops<EulerMixed<1>>(),
     make_ops<EulerMixed<2>>(),
     make_ops<MHDMixed<false>>(),
@@ -57,6 +57,6 @@ const Ops kOps[V_COUNT] = {
 
 }  // namespace
 
-const Ops* ops_mixed(int variant) { return (variant >= 0 && variant < V_COUNT) ? &kOps[variant] : nullptr; }
+const Ops* ops_mixed(int variant) { return (variant >= 0 && variant < V_HPR17) ? &kOps[variant] : nullptr; }
 
 }  // namespace vg

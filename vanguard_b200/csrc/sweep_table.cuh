@@ -37,8 +37,25 @@ cudaError_t launch_y(const SweepArgs& a, cudaStream_t st) {
     }
 }
 
+// Models with more than 9 conserved components (HPR, 17) use shorter X segments so that the three FP64
+// shared-memory tiles stay inside the 48 KB static limit.
+template <class K, class M, bool BIG = (M::NU > 9)>
+struct SweepTable;
+
 template <class K, class M>
-struct SweepTable {
+struct SweepTable<K, M, true> {
+    static constexpr SweepFn x[kNumXCfg] = {
+        launch_x<K, M, 64, 1, 1>, launch_x<K, M, 32, 2, 1>, launch_x<K, M, 96, 1, 1>,
+        launch_x<K, M, 64, 1, 2>, launch_x<K, M, 32, 1, 1>,
+    };
+    static constexpr SweepFn y[kNumYCfg] = {
+        launch_y<K, M, 64, 64, 1>, launch_y<K, M, 64, 32, 1>, launch_y<K, M, 32, 32, 1>,
+        launch_y<K, M, 32, 64, 1>, launch_y<K, M, 128, 32, 1>, launch_y<K, M, 64, 16, 1>,
+    };
+};
+
+template <class K, class M>
+struct SweepTable<K, M, false> {
     static constexpr SweepFn x[kNumXCfg] = {
         launch_x<K, M, 128, 1, 1>, launch_x<K, M, 64, 2, 1>, launch_x<K, M, 192, 1, 1>,
         launch_x<K, M, 128, 1, 6>, launch_x<K, M, 128, 1, 8>,
@@ -49,14 +66,16 @@ struct SweepTable {
     };
 };
 
-inline const char* x_cfg_name(int i) {
+inline const char* x_cfg_name(int i, bool big = false) {
     static const char* n[kNumXCfg] = {"P128xL1", "P64xL2", "P192xL1", "P128xL1/min6", "P128xL1/min8"};
-    return (i >= 0 && i < kNumXCfg) ? n[i] : "?";
+    static const char* nb[kNumXCfg] = {"P64xL1", "P32xL2", "P96xL1", "P64xL1/min2", "P32xL1"};
+    return (i >= 0 && i < kNumXCfg) ? (big ? nb[i] : n[i]) : "?";
 }
-inline const char* y_cfg_name(int i) {
+inline const char* y_cfg_name(int i, bool big = false) {
     static const char* n[kNumYCfg] = {"TX64xTY64", "TX64xTY32", "TX64xTY64/min12", "TX64xTY64/min16",
                                       "TX128xTY32/min5", "TX32xTY64"};
-    return (i >= 0 && i < kNumYCfg) ? n[i] : "?";
+    static const char* nb[kNumYCfg] = {"TX64xTY64", "TX64xTY32", "TX32xTY32", "TX32xTY64", "TX128xTY32", "TX64xTY16"};
+    return (i >= 0 && i < kNumYCfg) ? (big ? nb[i] : n[i]) : "?";
 }
 
 }  // namespace vg

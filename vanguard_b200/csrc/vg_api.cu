@@ -41,11 +41,12 @@ vg_status cuda_fail(cudaError_t e, const char* what) {
 int ref_nvar(int model) { return model == VG_MODEL_EULER ? 6 : model == VG_MODEL_MHD ? 9 : model == VG_MODEL_HPR ? 17 : 0; }
 
 // Reference plane carried in device plane k, per variant.
-const int kPlanes[vg::V_COUNT][9] = {
+const int kPlanes[vg::V_COUNT][17] = {
     {0, 1, 4},                      // V_EULER1: rho, u, p
     {0, 1, 2, 4},                   // V_EULER2: rho, u, v, p
     {0, 1, 2, 4, 5, 6, 8},          // V_MHD7:   rho, u, v, p, Bx, By, psi
     {0, 1, 2, 3, 4, 5, 6, 7, 8},    // V_MHD9
+    {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16},  // V_HPR17
 };
 
 }  // namespace
@@ -154,7 +155,22 @@ SweepArgs base_args(const vg_solver* s) {
     return a;
 }
 
-// Enqueue one time step reading from buffer `from`; returns the number of kernels.
+// HPR relaxation source: `sub` out-of-place sub-cycles starting in buffer `from`; returns the buffer holding the
+// result (Solvers/hprsecondordersolver.cpp:514-519, :532-537).
+int enqueue_forcing(vg_solver* s, SweepArgs a, int sub, int from, cudaStream_t st, cudaError_t* e, int* n) {
+    int b = from;
+    for (int i = 0; i < sub && *e == cudaSuccess; i++) {
+        a.in = s->buf[b];
+        a.out = s->buf[1 - b];
+        *e = s->ops->forcing(a, sub, st);
+        (*n)++;
+        b = 1 - b;
+    }
+    return b;
+}
+
+// Enqueue one time step reading from buffer `from`; returns the number of kernels.  Every step makes an odd
+// number of out-of-place passes (1 or 3 sweeps plus 2 * subcycles source passes), so it ends in buffer 1 - from.
 int enqueue_step(vg_solver* s, const vg_run_config& c, int from, cudaStream_t st, cudaError_t* err) {
     SweepArgs a = base_args(s);
     a.dx = c.dx;
@@ -163,13 +179,19 @@ int enqueue_step(vg_solver* s, const vg_run_config& c, int from, cudaStream_t st
     int n = 0;
     cudaError_t e = s->ops->step_begin(a, st);
     n++;
+    const int sub = (s->ops->forcing && c.subcycles > 0) ? c.subcycles : 0;
+    from = enqueue_forcing(s, a, sub, from, st, &e, &n);
+    // Without a trailing source pass the last sweep folds the next step's CFL maximum into its epilogue;
+    // with one, a separate reduction runs after it.
+    const int fuse_wave = sub == 0;
     if (s->dims == 1) {
         a.in = s->buf[from];
         a.out = s->buf[1 - from];
-        a.accumulate_wave = 1;
+        a.accumulate_wave = fuse_wave;
         a.advance_time = 1;
         if (e == cudaSuccess) e = run_sweep(s, 0, a, st);
         n++;
+        from = 1 - from;
     } else {
         // Solvers/secondordersolver.cpp:403-410: X(dt/2), Y(dt), X(dt/2)
         a.in = s->buf[from];
@@ -183,16 +205,30 @@ int enqueue_step(vg_solver* s, const vg_run_config& c, int from, cudaStream_t st
         a.in = s->buf[from];
         a.out = s->buf[1 - from];
         a.dt_scale = 0.5;
-        a.accumulate_wave = 1;
+        a.accumulate_wave = fuse_wave;
         a.advance_time = 1;
         if (e == cudaSuccess) e = run_sweep(s, 0, a, st);
         n += 3;
+        from = 1 - from;
+    }
+    a.dt_scale = 1.0;
+    a.accumulate_wave = 0;
+    a.advance_time = 0;
+    from = enqueue_forcing(s, a, sub, from, st, &e, &n);
+    if (!fuse_wave) {
+        a.in = s->buf[from];
+        if (e == cudaSuccess) e = s->ops->max_wave(a, st);
+        n++;
     }
     *err = e;
     return n;
 }
 
-int kernels_per_step(const vg_solver* s) { return s->dims == 1 ? 2 : 4; }
+int kernels_per_step(const vg_solver* s, int sub) {
+    int n = s->dims == 1 ? 2 : 4;
+    if (s->ops->forcing && sub > 0) n += 2 * sub + 1;
+    return n;
+}
 
 void destroy_graphs(vg_solver* s) {
     if (s->g.chunk) cudaGraphExecDestroy(s->g.chunk);
@@ -223,7 +259,7 @@ vg_status capture(vg_solver* s, const vg_run_config& c, int steps, int from, cud
 }
 
 bool same_cfg(const vg_run_config& a, const vg_run_config& b) {
-    return a.dx == b.dx && a.bias == b.bias && a.limiter == b.limiter;
+    return a.dx == b.dx && a.bias == b.bias && a.limiter == b.limiter && a.subcycles == b.subcycles;
 }
 
 vg_status ensure_graphs(vg_solver* s, const vg_run_config& c) {
@@ -263,7 +299,7 @@ const char* vg_status_string(vg_status st) {
 vg_status vg_create(const vg_grid_desc* desc, vg_solver** out) {
     if (!desc || !out) return fail(VG_EINVAL, "null argument");
     *out = nullptr;
-    if (desc->model != VG_MODEL_EULER && desc->model != VG_MODEL_MHD)
+    if (desc->model != VG_MODEL_EULER && desc->model != VG_MODEL_MHD && desc->model != VG_MODEL_HPR)
         return fail(VG_EUNSUPPORTED, "model not available in this build");
     if (desc->nx < 2 || desc->ny < 1 || (desc->ny > 1 && desc->ny < 2))
         return fail(VG_EINVAL, "grid needs at least 2 cells along every swept axis");
@@ -276,7 +312,7 @@ vg_status vg_create(const vg_grid_desc* desc, vg_solver** out) {
     if (!s) return fail(VG_ENOMEM, "host allocation");
     s->d = *desc;
     s->dims = desc->ny > 1 ? 2 : 1;
-    s->max_nw = desc->model == VG_MODEL_EULER ? 4 : 9;
+    s->max_nw = desc->model == VG_MODEL_EULER ? 4 : desc->model == VG_MODEL_MHD ? 9 : 17;
     s->pitch = ((long)desc->nx + 31) / 32 * 32;  // 256-byte aligned rows
     s->plane = s->pitch * desc->ny;
     s->floor5 = std::pow(10.0, -5.0);  // SlopeLimiters::computeSlopeVector's floor (Solvers/slopelimiters.cpp:232-239)
@@ -329,6 +365,8 @@ vg_status vg_upload_primitive(vg_solver* s, const double* planes, int is_device,
             }
             variant = (s->dims == 1 && zero_v) ? vg::V_EULER1 : vg::V_EULER2;
         }
+    } else if (s->d.model == VG_MODEL_HPR) {
+        variant = vg::V_HPR17;
     } else {
         bool reduced = true;
         if (!is_device) {
@@ -390,7 +428,9 @@ vg_status vg_run(vg_solver* s, const vg_run_config* cfg, int* steps_taken, doubl
     if (!s->ops) return fail(VG_EINVAL, "no state uploaded");
     if (!(cfg->dx > 0.0) || !(cfg->cfl > 0.0)) return fail(VG_EINVAL, "dx and cfl must be positive");
     if (cfg->max_steps <= 0 && !(cfg->t_end > 0.0)) return fail(VG_EINVAL, "need t_end > 0 or max_steps > 0");
-    if (cfg->subcycles != 0) return fail(VG_EUNSUPPORTED, "source sub-cycling is not available for this model");
+    if (cfg->subcycles < 0) return fail(VG_EINVAL, "subcycles must be >= 0");
+    if (cfg->subcycles > 0 && !s->ops->forcing)
+        return fail(VG_EUNSUPPORTED, "source sub-cycling is only available for the HPR model");
     cudaStream_t st = (cudaStream_t)stream;
     VG_CUDA(cudaSetDevice(s->d.device));
 
@@ -441,7 +481,7 @@ vg_status vg_run(vg_solver* s, const vg_run_config* cfg, int* steps_taken, doubl
             if (!(h->t < h->t_end) || h->it >= h->max_steps) break;
         }
     }
-    launches += launched_steps * kernels_per_step(s);
+    launches += launched_steps * kernels_per_step(s, cfg->subcycles);
     // every step is an odd number of sweeps in 2D (3) and 1 in 1D: the state ends in buffer (steps & 1)
     s->cur = (int)(launched_steps & 1);
     VG_CUDA(cudaMemcpyAsync(h, s->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
@@ -528,8 +568,9 @@ vg_status vg_get_launch_config(vg_solver* s, int* xcfg, int* ycfg, const char** 
     if (!s) return fail(VG_EINVAL, "null solver");
     if (xcfg) *xcfg = s->xcfg;
     if (ycfg) *ycfg = s->ycfg;
-    if (xname) *xname = vg::x_cfg_name(s->xcfg);
-    if (yname) *yname = vg::y_cfg_name(s->ycfg);
+    const bool big = s->ops && s->ops->big_tiles;
+    if (xname) *xname = vg::x_cfg_name(s->xcfg, big);
+    if (yname) *yname = vg::y_cfg_name(s->ycfg, big);
     return VG_OK;
 }
 

@@ -16,7 +16,8 @@ enum Variant : int {
     V_EULER2 = 1,  // Euler, 2 velocities:                 rho, u, v, p
     V_MHD7 = 2,    // MHD with w == Bz == 0:               rho, u, v, p, Bx, By, psi
     V_MHD9 = 3,    // MHD, all components:                 rho, u, v, w, p, Bx, By, Bz, psi
-    V_COUNT = 4
+    V_HPR17 = 4,   // HPR, all 17 components:              rho, p, A(9), u, v, w, Jx, Jy, Jz
+    V_COUNT = 5
 };
 
 struct Ops {
@@ -30,6 +31,9 @@ struct Ops {
     cudaError_t (*step_begin)(const SweepArgs& a, cudaStream_t st);
     // *out = maximum wave speed including corner ghosts (reads ctrl->smax_next).
     cudaError_t (*max_wave_finish)(const SweepArgs& a, double* out, cudaStream_t st);
+    // One relaxation-source sub-cycle of length 0.5 dt / subcycles, a.in -> a.out (null: model has no source).
+    cudaError_t (*forcing)(const SweepArgs& a, int subcycles, cudaStream_t st);
+    bool big_tiles;  // SweepTable<.., BIG = true> (names of the launch configurations)
 };
 
 // Exact-FP64 kernels (compiled with -fmad=false; bitwise parity with the reference).
