@@ -1,0 +1,103 @@
+// A Vanguard-style caller of the drop-in C++ surface: it uses only the reference's class names and
+// signatures (as EulerTests::solveToroTest1 and RGFM's per-sweep calls do) and writes the resulting primitive
+// planes to a binary file for tests/test_shim_gpu.py to compare with the oracle.
+//   shim_driver <out.bin>
+// Output, in order (float64): Euler 1D solve (6 x 200), Euler 2D per-sweep loop (6 x 24 x 20),
+// MHD solve2D (9 x 16 x 16), HPR solve (17 x 50), then the number of 2D steps the per-sweep loop took.
+#include <cmath>
+#include <cstdio>
+#include <vector>
+
+#include "Solvers/secondordersolver.h"
+
+using std::vector;
+
+static void put(FILE* f, const vector<double>& v) { std::fwrite(v.data(), sizeof(double), v.size(), f); }
+
+int main(int argc, char** argv) {
+    if (argc < 2) return 2;
+    FILE* f = std::fopen(argv[1], "wb");
+    if (!f) return 3;
+
+    // 1) SecondOrderSolver::solve on a shock tube (minbee, CFL 0.9, to t = 0.1)
+    {
+        int n = 200;
+        vector<EulerStateVector> cells(n);
+        EulerMaterialParameters mp(1.4);
+        for (int i = 0; i < n; i++)
+            cells[i] = i <= 0.5 * n ? EulerStateVector(1.0, 0.0, 0.0, 0.0, 1.0) : EulerStateVector(0.125, 0.0, 0.0, 0.0, 0.1);
+        vector<EulerStateVector> out = SecondOrderSolver::solve(cells, 1.0 / n, 0.9, 0.1, 0.0, 2, 0, mp);
+        vector<double> v;
+        for (int k = 0; k < 6; k++)
+            for (auto& c : out) v.push_back(c.computePrimitiveVariableVector()[k]);
+        put(f, v);
+    }
+    // 2) the per-step functions, as solve2D is built from them (Solvers/secondordersolver.cpp:399-410)
+    int steps = 0;
+    {
+        int nx = 24, ny = 20;
+        vector<vector<EulerStateVector> > cells(ny, vector<EulerStateVector>(nx));
+        EulerMaterialParameters mp(1.4);
+        for (int i = 0; i < ny; i++)
+            for (int j = 0; j < nx; j++)
+                cells[i][j] = (i < ny / 2) == (j < nx / 2) ? EulerStateVector(1.0, 0.1, -0.2, 0.0, 1.0)
+                                                           : EulerStateVector(0.3, -0.1, 0.3, 0.0, 0.4);
+        double t = 0.0, dx = 1.0 / nx;
+        for (steps = 0; steps < 6; steps++) {
+            vector<vector<EulerStateVector> > withB = Solvers::insertBoundaryCells2D(cells, 2);
+            double dt = Solvers::computeStableTimeStep2D(withB, dx, 0.8, t, 1.0, steps, mp);
+            SecondOrderSolver::computeXSLICTimeStep2D(cells, withB, dx, 0.5 * dt, 0.0, 0, mp);
+            withB = Solvers::insertBoundaryCells2D(cells, 2);
+            SecondOrderSolver::computeYSLICTimeStep2D(cells, withB, dx, dt, 0.0, 0, mp);
+            withB = Solvers::insertBoundaryCells2D(cells, 2);
+            SecondOrderSolver::computeXSLICTimeStep2D(cells, withB, dx, 0.5 * dt, 0.0, 0, mp);
+            t += dt;
+        }
+        vector<double> v;
+        for (int k = 0; k < 6; k++)
+            for (auto& row : cells)
+                for (auto& c : row) v.push_back(c.computePrimitiveVariableVector()[k]);
+        put(f, v);
+    }
+    // 3) MHDSecondOrderSolver::solve2D (to t = 0.02)
+    {
+        int n = 16;
+        const double pi = 3.14159265358979323846, g = 5.0 / 3.0, s = 1.0 / std::sqrt(4.0 * pi);
+        vector<vector<MHDStateVector> > cells(n, vector<MHDStateVector>(n));
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) {
+                double x = (j + 0.5) / n, y = (i + 0.5) / n;
+                cells[i][j] = MHDStateVector(g * g, -std::sin(2 * pi * y), std::sin(2 * pi * x), 0.0, g, -std::sin(2 * pi * y) * s,
+                                             std::sin(4 * pi * x) * s, 0.0, 0.0);
+            }
+        vector<vector<MHDStateVector> > out = MHDSecondOrderSolver::solve2D(cells, 1.0 / n, 0.8, 0.02, 0.0, 0, 0, MHDMaterialParameters(g));
+        vector<double> v;
+        for (int k = 0; k < 9; k++)
+            for (auto& row : out)
+                for (auto& c : row) v.push_back(c.computePrimitiveVariableVector()[k]);
+        put(f, v);
+    }
+    // 4) HPRSecondOrderSolver::solve with the heat-conduction material (HPR/hprtests.cpp:33-57), 1 sub-cycle, t = 0.02
+    {
+        int n = 50;
+        HPRMaterialParameters mp("StiffenedGas", true, false, 8.31445985, 1.0, 1.0, 0.0, 1.0, 2.5, 1.4, 0.0, 0.0, 0.0, 0.0, 0.0,
+                                 1.0, 0.0, 0.0, std::pow(10.0, -2.0), 0.75, 0.0, 1.0, 2.0, 0.0, 0.0, 0.0);
+        mp.configureStrainDissipationTime();
+        mp.configureThermalImpulseRelaxationTime(std::pow(10.0, -2.0));
+        vector<HPRStateVector> cells(n);
+        for (int i = 0; i < n; i++) {
+            double r = i <= 0.5 * n ? 2.0 : 0.5, a = std::pow(r, 1.0 / 3.0);
+            vector<vector<double> > A = {{a, 0.0, 0.0}, {0.0, a, 0.0}, {0.0, 0.0, a}};
+            cells[i] = HPRStateVector(r, 1.0, A, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0);
+        }
+        vector<HPRStateVector> out = HPRSecondOrderSolver::solve(cells, 1.0 / n, 0.8, 0.02, 0.0, 0, 1, mp);
+        vector<double> v;
+        for (int k = 0; k < 17; k++)
+            for (auto& c : out) v.push_back(c.data()[k]);
+        put(f, v);
+    }
+    double st = steps;
+    std::fwrite(&st, sizeof(double), 1, f);
+    std::fclose(f);
+    return 0;
+}

@@ -73,7 +73,36 @@ def build(verbose: bool = False, force: bool = False) -> str:
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True, env=env)
+    build_shim(verbose=verbose, force=force)
     return OUT
+
+
+SHIM_DIR = os.path.join(HERE, "shim")
+SHIM_OUT = os.path.join(HERE, "libvanguard_shim.so")
+DRIVER_SRC = os.path.join(os.path.dirname(HERE), "tests", "shim", "shim_driver.cpp")
+DRIVER_OUT = os.path.join(os.path.dirname(HERE), "tests", "shim", "shim_driver")
+
+
+def build_shim(verbose: bool = False, force: bool = False) -> str:
+    """The drop-in C++ surface (libvanguard_shim.so, the reference's class names over the C ABI) and the
+    Vanguard-style test caller tests/shim/shim_driver, both with g++ and an $ORIGIN-relative rpath."""
+    env = dict(os.environ)
+    env.pop("CXX", None)
+    src = os.path.join(SHIM_DIR, "vanguard_shim.cpp")
+    hdrs = [os.path.join(SHIM_DIR, "vanguard_shim.h"), os.path.join(os.path.dirname(HERE), "include", "vanguard_slic.h")]
+    if force or _stale(SHIM_OUT, [src, OUT] + hdrs):
+        cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-Wall", "-o", SHIM_OUT, src, "-L" + HERE,
+               "-lvanguard_slic", "-Wl,-rpath,$ORIGIN"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True, env=env)
+    if os.path.exists(DRIVER_SRC) and (force or _stale(DRIVER_OUT, [DRIVER_SRC, SHIM_OUT] + hdrs)):
+        cmd = ["g++", "-O2", "-std=c++17", "-Wall", "-I" + SHIM_DIR, "-o", DRIVER_OUT, DRIVER_SRC, "-L" + HERE,
+               "-lvanguard_shim", "-lvanguard_slic", "-Wl,-rpath," + "$ORIGIN/../../vanguard_b200"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True, env=env)
+    return SHIM_OUT
 
 
 if __name__ == "__main__":

@@ -1,0 +1,561 @@
+// Implementation of the drop-in C++ surface (vanguard_shim.h) over the C ABI of libvanguard_slic.so.
+//
+// Model classes hold primitives exactly as the reference's do and implement the closed-form conversions callers
+// use on the host; everything grid-sized (solve, solve2D, the per-sweep updates, the CFL maximum) runs through the
+// C ABI on the GPU.  Defaults of every constructor follow the reference's: Euler/eulermaterialparameters.cpp:3-34,
+// Euler/eulerstatevector.cpp:3-34, MHD/mhdmaterialparameters.cpp:3-19, MHD/mhdstatevector.cpp:3-33,
+// HPR/hprmaterialparameters.cpp:3-69, HPR/hprstatevector.cpp:3-33.
+#include "vanguard_shim.h"
+
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <tuple>
+
+#include "../../include/vanguard_slic.h"
+
+namespace {
+
+[[noreturn]] void raise(vg_status st, const char* where) {
+    throw std::runtime_error(std::string(where) + ": " + vg_status_string(st) + ": " + vg_last_error_string());
+}
+
+void check(vg_status st, const char* where) {
+    if (st != VG_OK) raise(st, where);
+}
+
+int device() {
+    const char* d = std::getenv("VG_DEVICE");
+    return d ? std::atoi(d) : 0;
+}
+
+int precision() {
+    const char* p = std::getenv("VG_PRECISION");
+    return (p && std::strcmp(p, "mixed") == 0) ? VG_MIXED : VG_FP64;
+}
+
+struct SolverDeleter {
+    void operator()(vg_solver* s) const { vg_destroy(s); }
+};
+using SolverPtr = std::unique_ptr<vg_solver, SolverDeleter>;
+
+SolverPtr make_solver(int model, int nx, int ny, int boundary, const double* params, int nparams) {
+    vg_grid_desc d{};
+    d.model = model;
+    d.nx = nx;
+    d.ny = ny;
+    d.precision = precision();
+    d.boundary = boundary;
+    d.device = device();
+    for (int i = 0; i < nparams && i < VG_MAX_PARAMS; i++) d.params[i] = params[i];
+    vg_solver* s = nullptr;
+    check(vg_create(&d, &s), "vg_create");
+    return SolverPtr(s);
+}
+
+// One cached solver per thread for the per-sweep entry points (a sweep per call would otherwise reallocate).
+vg_solver* cached_solver(int model, int nx, int ny, int boundary, const double* params, int nparams) {
+    thread_local std::map<std::tuple<int, int, int, int, int, std::string>, SolverPtr> cache;
+    std::string key(reinterpret_cast<const char*>(params), sizeof(double) * nparams);
+    auto k = std::make_tuple(model, nx, ny, boundary, precision(), key);
+    auto it = cache.find(k);
+    if (it == cache.end()) it = cache.emplace(k, make_solver(model, nx, ny, boundary, params, nparams)).first;
+    return it->second.get();
+}
+
+// Runs solve()/solve2D()'s time loop (finalTime-driven) on reference-order primitive planes, in place.
+void run_planes(int model, std::vector<double>& planes, int nx, int ny, const double* params, int nparams, double dx,
+                double cfl, double tEnd, double bias, int limiter, int subcycles) {
+    SolverPtr s = make_solver(model, nx, ny, VG_TRANSMISSIVE, params, nparams);
+    vg_run_config c{};
+    c.dx = dx;
+    c.cfl = cfl;
+    c.t_end = tEnd;
+    c.max_steps = 0;
+    c.bias = bias;
+    c.limiter = limiter;
+    c.subcycles = subcycles;
+    vg_status st = vg_solve(s.get(), planes.data(), planes.data(), &c, nullptr, nullptr, nullptr);
+    if (st != VG_OK && st != VG_ENAN) raise(st, "vg_solve");  // non-finite results are returned, as the reference does
+}
+
+// ---- packing between reference-style cells and SoA primitive planes
+template <class S, class Get>
+std::vector<double> pack(const std::vector<S>& cells, int nvar, Get get) {
+    long n = cells.size();
+    std::vector<double> p(nvar * n);
+    for (long i = 0; i < n; i++) {
+        double w[17];
+        get(cells[i], w);
+        for (int v = 0; v < nvar; v++) p[v * n + i] = w[v];
+    }
+    return p;
+}
+template <class S, class Get>
+std::vector<double> pack2(const std::vector<std::vector<S> >& cells, int nvar, Get get) {
+    long ny = cells.size(), nx = cells[0].size(), n = nx * ny;
+    std::vector<double> p(nvar * n);
+    for (long i = 0; i < ny; i++)
+        for (long j = 0; j < nx; j++) {
+            double w[17];
+            get(cells[i][j], w);
+            for (int v = 0; v < nvar; v++) p[v * n + i * nx + j] = w[v];
+        }
+    return p;
+}
+
+void euler_get(const EulerStateVector& c, double* w) {
+    w[0] = c.getDensity(), w[1] = c.getXVelocity(), w[2] = c.getYVelocity(), w[3] = c.getZVelocity();
+    w[4] = c.getPressure(), w[5] = c.getReactionProgress();
+}
+EulerStateVector euler_make(const double* w) { return EulerStateVector(w[0], w[1], w[2], w[3], w[4], w[5]); }
+void mhd_get(const MHDStateVector& c, double* w) {
+    std::vector<double> v = c.computePrimitiveVariableVector();
+    for (int i = 0; i < 9; i++) w[i] = v[i];
+}
+MHDStateVector mhd_make(const double* w) { return MHDStateVector(w[0], w[1], w[2], w[3], w[4], w[5], w[6], w[7], w[8]); }
+void hpr_get(const HPRStateVector& c, double* w) { std::memcpy(w, c.data(), sizeof(double) * 17); }
+HPRStateVector hpr_make(const double* w) {
+    HPRStateVector s;
+    std::memcpy(s.data(), w, sizeof(double) * 17);
+    return s;
+}
+
+template <class S, class Make>
+std::vector<S> unpack(const std::vector<double>& p, long n, int nvar, Make make) {
+    std::vector<S> out;
+    out.reserve(n);
+    for (long i = 0; i < n; i++) {
+        double w[17];
+        for (int v = 0; v < nvar; v++) w[v] = p[v * n + i];
+        out.push_back(make(w));
+    }
+    return out;
+}
+template <class S, class Make>
+std::vector<std::vector<S> > unpack2(const std::vector<double>& p, long nx, long ny, int nvar, Make make) {
+    std::vector<std::vector<S> > out(ny);
+    long n = nx * ny;
+    for (long i = 0; i < ny; i++) {
+        out[i].reserve(nx);
+        for (long j = 0; j < nx; j++) {
+            double w[17];
+            for (int v = 0; v < nvar; v++) w[v] = p[v * n + i * nx + j];
+            out[i].push_back(make(w));
+        }
+    }
+    return out;
+}
+
+void euler_params(const EulerMaterialParameters& mp, double* prm) {
+    prm[0] = mp.getAdiabaticIndex(), prm[1] = mp.getStiffeningParameter(), prm[2] = mp.getSpecificHeatCapacity();
+    prm[3] = mp.getEnergyOfFormation(), prm[4] = mp.getIgnitionTemperature(), prm[5] = mp.getReactionRate();
+}
+void mhd_params(const MHDMaterialParameters& mp, double* prm) {
+    prm[0] = mp.getAdiabaticIndex(), prm[1] = mp.getStiffeningParameter(), prm[2] = mp.getHyperbolicWaveSpeed();
+}
+void hpr_params(const HPRMaterialParameters& mp, double* prm) {
+    if (mp.getEquationOfState() != "StiffenedGas" || mp.getIsPlastic())
+        throw std::runtime_error("HPR: only the StiffenedGas equation of state without plasticity runs on the GPU path");
+    prm[0] = mp.getAdiabaticIndex(), prm[1] = mp.getStiffeningParameter(), prm[2] = mp.getSpecificHeatCapacity();
+    prm[3] = mp.getReferenceDensity(), prm[4] = mp.getInitialTemperature(), prm[5] = mp.getTransverseWaveSpeed();
+    prm[6] = mp.getHeatWaveSpeed(), prm[7] = mp.getStrainDissipationTime(), prm[8] = mp.getThermalImpulseRelaxationTime();
+    prm[9] = mp.getReferenceTemperature(), prm[10] = mp.getReferencePressure(), prm[11] = mp.getIsThermal() ? 1.0 : 0.0;
+}
+
+// Boundary kind of a caller-built ghosted array along one line: the reference's transmissive mirror
+// (Solvers/solvers.cpp:17-23) or wrap-around; anything else cannot be expressed by the GPU path.
+template <class Eq>
+int boundary_kind(long n, Eq same) {
+    // same(g, c): ghost slot g (0..n+3) holds interior cell c
+    if (same(0, 1) && same(1, 0) && same(n + 2, n - 1) && same(n + 3, n - 2)) return VG_TRANSMISSIVE;
+    if (same(0, n - 2) && same(1, n - 1) && same(n + 2, 0) && same(n + 3, 1)) return VG_PERIODIC;
+    return -1;
+}
+
+template <class S, class Get>
+bool equal_cells(const S& a, const S& b, int nvar, Get get) {
+    double wa[17], wb[17];
+    get(a, wa);
+    get(b, wb);
+    return std::memcmp(wa, wb, sizeof(double) * nvar) == 0;
+}
+
+template <class S, class Get, class Make>
+void sweep2d(int model, int nvar, std::vector<std::vector<S> >& cells, std::vector<std::vector<S> >& withB, int axis,
+             double dx, double dt, double bias, int limiter, const double* prm, int nprm, Get get, Make make) {
+    long ny = cells.size(), nx = cells[0].size();
+    if ((long)withB.size() != ny + 4 || (long)withB[0].size() != nx + 4)
+        throw std::runtime_error("sweep: the ghosted array must have 2 ghost cells on every side");
+    int bc = -1;
+    for (long line = 0; line < (axis == 0 ? ny : nx); line++) {
+        int k = axis == 0 ? boundary_kind(nx, [&](long g, long c) { return equal_cells(withB[line + 2][g], cells[line][c], nvar, get); })
+                          : boundary_kind(ny, [&](long g, long c) { return equal_cells(withB[g][line + 2], cells[c][line], nvar, get); });
+        if (k < 0 || (bc >= 0 && k != bc))
+            throw std::runtime_error("sweep: ghost cells other than transmissive or periodic copies are not supported");
+        bc = k;
+    }
+    vg_solver* s = cached_solver(model, (int)nx, (int)ny, bc, prm, nprm);
+    std::vector<double> planes = pack2(cells, nvar, get);
+    check(vg_upload_primitive(s, planes.data(), 0, nullptr), "vg_upload_primitive");
+    check(vg_sweep(s, axis, dx, dt, bias, limiter, nullptr), "vg_sweep");
+    check(vg_download_primitive(s, planes.data(), 0, nullptr), "vg_download_primitive");
+    cells = unpack2<S>(planes, nx, ny, nvar, make);
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------- Euler model
+EulerMaterialParameters::EulerMaterialParameters() : EulerMaterialParameters(1.0, 0.0) {}
+EulerMaterialParameters::EulerMaterialParameters(double g) : EulerMaterialParameters(g, 0.0) {}
+EulerMaterialParameters::EulerMaterialParameters(double g, double pinf) : EulerMaterialParameters(g, pinf, 25.0, 0.0, 0.25, 250.0) {}
+EulerMaterialParameters::EulerMaterialParameters(double g, double pinf, double cv, double e0, double tign, double rate)
+    : adiabaticIndex(g), stiffeningParameter(pinf), specificHeatCapacity(cv), energyOfFormation(e0), ignitionTemperature(tign),
+      reactionRate(rate) {}
+
+double EulerEquationOfState::computeSpecificInternalEnergy(double rho, double p, EulerMaterialParameters mp) {
+    double g = mp.getAdiabaticIndex();
+    return (p + (g * mp.getStiffeningParameter())) / ((g - 1) * rho);
+}
+double EulerEquationOfState::computePressure(double rho, double e, EulerMaterialParameters mp) {
+    double g = mp.getAdiabaticIndex();
+    return ((e * (g - 1)) * rho) - (g * mp.getStiffeningParameter());
+}
+double EulerEquationOfState::computeSoundSpeed(double rho, double p, EulerMaterialParameters mp) {
+    return std::sqrt((mp.getAdiabaticIndex() * (p + mp.getStiffeningParameter())) / rho);
+}
+
+EulerStateVector::EulerStateVector() : EulerStateVector(1.0, 0.0, 0.0, 0.0, 1.0, 1.0) {}
+EulerStateVector::EulerStateVector(double r, double u, double v, double w, double p) : EulerStateVector(r, u, v, w, p, 1.0) {}
+EulerStateVector::EulerStateVector(double r, double u, double v, double w, double p, double lam)
+    : density(r), xVelocity(u), yVelocity(v), zVelocity(w), pressure(p), reactionProgress(lam) {}
+
+void EulerStateVector::setPrimitiveVariableVector(vector<double> w) {
+    density = w[0], xVelocity = w[1], yVelocity = w[2], zVelocity = w[3], pressure = w[4], reactionProgress = w[5];
+}
+vector<double> EulerStateVector::computePrimitiveVariableVector() const {
+    return {density, xVelocity, yVelocity, zVelocity, pressure, reactionProgress};
+}
+double EulerStateVector::computeSpecificInternalEnergy(EulerMaterialParameters mp) const {
+    return EulerEquationOfState::computeSpecificInternalEnergy(density, pressure, mp);
+}
+double EulerStateVector::computeTotalEnergy(EulerMaterialParameters mp) const {
+    double v2 = ((xVelocity * xVelocity) + (yVelocity * yVelocity)) + (zVelocity * zVelocity);
+    return density * (((0.5 * v2) + computeSpecificInternalEnergy(mp)) + (mp.getEnergyOfFormation() * (reactionProgress - 1.0)));
+}
+double EulerStateVector::computeSoundSpeed(EulerMaterialParameters mp) const {
+    return EulerEquationOfState::computeSoundSpeed(density, pressure, mp);
+}
+vector<double> EulerStateVector::computeConservedVariableVector(EulerMaterialParameters mp) const {
+    return {density, density * xVelocity, density * yVelocity, density * zVelocity, computeTotalEnergy(mp), density * reactionProgress};
+}
+void EulerStateVector::setConservedVariableVector(vector<double> u, EulerMaterialParameters mp) {
+    density = u[0];
+    xVelocity = u[1] / density, yVelocity = u[2] / density, zVelocity = u[3] / density;
+    reactionProgress = u[5] / density;
+    double v2 = ((xVelocity * xVelocity) + (yVelocity * yVelocity)) + (zVelocity * zVelocity);
+    double e = ((u[4] / density) - (0.5 * v2)) - (mp.getEnergyOfFormation() * (reactionProgress - 1.0));
+    pressure = EulerEquationOfState::computePressure(density, e, mp);
+}
+static vector<double> euler_flux(const vector<double>& u, EulerMaterialParameters mp, int axis) {
+    double rho = u[0], vx = u[1] / rho, vy = u[2] / rho, vz = u[3] / rho, lam = u[5] / rho;
+    double v2 = ((vx * vx) + (vy * vy)) + (vz * vz);
+    double E = u[4] / rho;
+    double p = EulerEquationOfState::computePressure(rho, (E - (0.5 * v2)) - (mp.getEnergyOfFormation() * (lam - 1.0)), mp);
+    double un = axis == 0 ? vx : vy;
+    vector<double> f = {rho * un, rho * (un * vx), rho * (un * vy), rho * (un * vz), (rho * (un * E)) + (un * p), rho * (un * lam)};
+    f[1 + axis] += p;
+    return f;
+}
+vector<double> EulerStateVector::computeXFluxVector(vector<double> u, EulerMaterialParameters mp) { return euler_flux(u, mp, 0); }
+vector<double> EulerStateVector::computeYFluxVector(vector<double> u, EulerMaterialParameters mp) { return euler_flux(u, mp, 1); }
+vector<double> EulerStateVector::computeXFluxVector(EulerMaterialParameters mp) const {
+    return computeXFluxVector(computeConservedVariableVector(mp), mp);
+}
+vector<double> EulerStateVector::computeYFluxVector(EulerMaterialParameters mp) const {
+    return computeYFluxVector(computeConservedVariableVector(mp), mp);
+}
+
+// --------------------------------------------------------------------------------------------- MHD model
+MHDMaterialParameters::MHDMaterialParameters() : adiabaticIndex(1.0), stiffeningParameter(0.0), hyperbolicWaveSpeed(2.0),
+                                                 parabolicDamping(std::sqrt(0.36)) {}
+MHDMaterialParameters::MHDMaterialParameters(double g) : adiabaticIndex(g), stiffeningParameter(0.0), hyperbolicWaveSpeed(0.0),
+                                                         parabolicDamping(0.0) {}
+void MHDMaterialParameters::configureParabolicDamping() { parabolicDamping = std::sqrt(hyperbolicWaveSpeed * 0.18); }
+
+MHDStateVector::MHDStateVector() : MHDStateVector(1.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0, 0.0) {}
+MHDStateVector::MHDStateVector(double r, double u, double v, double w, double p, double bx, double by, double bz, double psi)
+    : w_{r, u, v, w, p, bx, by, bz, psi} {}
+void MHDStateVector::setPrimitiveVariableVector(vector<double> w) {
+    for (int i = 0; i < 9; i++) w_[i] = w[i];
+}
+vector<double> MHDStateVector::computePrimitiveVariableVector() const { return vector<double>(w_, w_ + 9); }
+vector<double> MHDStateVector::computeConservedVariableVector(MHDMaterialParameters mp) const {
+    double r = w_[0], u = w_[1], v = w_[2], w = w_[3], p = w_[4], g = mp.getAdiabaticIndex();
+    double e = (p + (g * mp.getStiffeningParameter())) / ((g - 1) * r);
+    double hydro = r * ((0.5 * (((u * u) + (v * v)) + (w * w))) + e);
+    double b2 = ((w_[5] * w_[5]) + (w_[6] * w_[6])) + (w_[7] * w_[7]);
+    return {r, r * u, r * v, r * w, hydro + (0.5 * b2), w_[5], w_[6], w_[7], w_[8]};
+}
+void MHDStateVector::setConservedVariableVector(vector<double> U, MHDMaterialParameters mp) {
+    double r = U[0], g = mp.getAdiabaticIndex();
+    double u = U[1] / r, v = U[2] / r, w = U[3] / r;
+    double b2 = ((U[5] * U[5]) + (U[6] * U[6])) + (U[7] * U[7]);
+    double e = ((U[4] - (0.5 * b2)) / r) - (0.5 * (((u * u) + (v * v)) + (w * w)));
+    double p = ((e * (g - 1)) * r) - (g * mp.getStiffeningParameter());
+    double nw[9] = {r, u, v, w, p, U[5], U[6], U[7], U[8]};
+    std::memcpy(w_, nw, sizeof(nw));
+}
+
+// --------------------------------------------------------------------------------------------- HPR model
+HPRMaterialParameters::HPRMaterialParameters()
+    : HPRMaterialParameters("StiffenedGas", false, false, 8.31445985, 1.0, 1.0 / 1.4, 0.0, 0.0, 1.0, 1.4, 0.0, 0.0, 0.0, 0.0,
+                            0.0, 1.0, 0.0, 0.0, std::pow(10.0, -2.0), 0.75, 0.0, 1.0, std::pow(10.0, -16.0), 0.0, 0.0, 0.0) {}
+HPRMaterialParameters::HPRMaterialParameters(string eos, bool thermal, bool plastic, double R, double rho0, double pref,
+                                             double tref, double t0, double cv, double g, double pinf, double c0, double gr0,
+                                             double s, double e0, double cs, double tau1, double tau2, double mu, double pr,
+                                             double sy, double n, double alpha, double a, double b, double c)
+    : equationOfState(eos), isThermal(thermal), isPlastic(plastic), idealGasConstant(R), referenceDensity(rho0),
+      referencePressure(pref), referenceTemperature(tref), initialTemperature(t0), specificHeatCapacity(cv), adiabaticIndex(g),
+      stiffeningParameter(pinf), referenceSoundSpeed(c0), referenceGruneisenCoefficient(gr0), hugoniotSlopeCoefficient(s),
+      referenceInternalEnergy(e0), transverseWaveSpeed(cs), strainDissipationTime(tau1), thermalImpulseRelaxationTime(tau2),
+      dynamicViscosityCoefficient(mu), prandtlNumber(pr), elasticPlasticTransitionParameter(sy), powerLawIndex(n),
+      heatWaveSpeed(alpha), alphaParameter(a), betaParameter(b), gammaParameter(c) {}
+// HPR/hprmaterialparameters.cpp:71-119
+double HPRMaterialParameters::computeStrainDissipationTime() const {
+    return 6.0 * (dynamicViscosityCoefficient / (referencePressure * (transverseWaveSpeed * transverseWaveSpeed)));
+}
+double HPRMaterialParameters::computeHeatConductionCoefficient() const {
+    return dynamicViscosityCoefficient * adiabaticIndex * (specificHeatCapacity / prandtlNumber);
+}
+double HPRMaterialParameters::computeThermalImpulseRelaxationTime(double kappa) const {
+    return kappa * (referenceDensity / (initialTemperature * (heatWaveSpeed * heatWaveSpeed)));
+}
+double HPRMaterialParameters::computeThermalImpulseRelaxationTime() const {
+    return computeThermalImpulseRelaxationTime(computeHeatConductionCoefficient());
+}
+void HPRMaterialParameters::configureStrainDissipationTime() { strainDissipationTime = computeStrainDissipationTime(); }
+void HPRMaterialParameters::configureThermalImpulseRelaxationTime() {
+    thermalImpulseRelaxationTime = computeThermalImpulseRelaxationTime();
+}
+void HPRMaterialParameters::configureThermalImpulseRelaxationTime(double kappa) {
+    thermalImpulseRelaxationTime = computeThermalImpulseRelaxationTime(kappa);
+}
+
+HPRStateVector::HPRStateVector() {
+    std::memset(w_, 0, sizeof(w_));
+    double c = std::pow(1.0, 1.0 / 3.0);
+    w_[0] = 1.0;
+    w_[1] = 1.0 / 1.4;
+    w_[2] = w_[6] = w_[10] = c;
+}
+HPRStateVector::HPRStateVector(double rho, double p, vector<vector<double> > A, double u, double v, double w, double jx,
+                               double jy, double jz) {
+    w_[0] = rho, w_[1] = p;
+    setDistortionTensor(A);
+    w_[11] = u, w_[12] = v, w_[13] = w, w_[14] = jx, w_[15] = jy, w_[16] = jz;
+}
+vector<vector<double> > HPRStateVector::getDistortionTensor() const {
+    vector<vector<double> > A(3, vector<double>(3));
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) A[i][j] = w_[2 + 3 * i + j];
+    return A;
+}
+void HPRStateVector::setDistortionTensor(vector<vector<double> > A) {
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) w_[2 + 3 * i + j] = A[i][j];
+}
+
+// ----------------------------------------------------------------------------------------- slope limiters
+double SlopeLimiters::computeRCoefficient(double r, double w) { return 2.0 / ((1.0 - w) + ((1.0 + w) * r)); }
+double SlopeLimiters::computeSuperBeeSlopeLimiter(double r, double w) {
+    if (r < 0.0) return 0.0;
+    if (r < 0.5) return 2.0 * r;
+    if (r < 1.0) return 1.0;
+    double xi = computeRCoefficient(r, w), m = (xi < r) ? xi : r;
+    return (2.0 < m) ? 2.0 : m;
+}
+double SlopeLimiters::computeVanLeerSlopeLimiter(double r, double w) {
+    if (r < 0.0) return 0.0;
+    double a = (2.0 * r) / (1.0 + r), b = computeRCoefficient(r, w);
+    return (b < a) ? b : a;
+}
+double SlopeLimiters::computeMinBeeSlopeLimiter(double r, double w) {
+    if (r < 0.0) return 0.0;
+    if (r < 1.0) return r;
+    double b = computeRCoefficient(r, w);
+    return (b < 1.0) ? b : 1.0;
+}
+double SlopeLimiters::computeSlopeLimiter(double r, double w, int id) {
+    return id == 0 ? computeSuperBeeSlopeLimiter(r, w) : id == 1 ? computeVanLeerSlopeLimiter(r, w) : computeMinBeeSlopeLimiter(r, w);
+}
+
+// ------------------------------------------------------------------------------------------ solver helpers
+vector<EulerStateVector> Solvers::insertBoundaryCells(vector<EulerStateVector>& c, int b) {
+    long n = c.size();
+    vector<EulerStateVector> g(n + 2 * b);
+    for (long i = 0; i < n; i++) g[i + b] = c[i];
+    for (int k = 0; k < b; k++) {
+        g[b - 1 - k] = c[k < n ? k : n - 1];
+        g[n + b + k] = c[n - 1 - k >= 0 ? n - 1 - k : 0];
+    }
+    return g;
+}
+vector<vector<EulerStateVector> > Solvers::insertBoundaryCells2D(vector<vector<EulerStateVector> >& c, int b) {
+    long ny = c.size(), nx = c[0].size();
+    vector<vector<EulerStateVector> > g(ny + 2 * b, vector<EulerStateVector>(nx + 2 * b));
+    for (long i = 0; i < ny; i++)
+        for (long j = 0; j < nx; j++) g[i + b][j + b] = c[i][j];
+    for (long i = 0; i < ny; i++)
+        for (int k = 0; k < b; k++) {
+            g[i + b][b - 1 - k] = c[i][k];
+            g[i + b][nx + b + k] = c[i][nx - 1 - k];
+        }
+    for (long j = 0; j < nx; j++)
+        for (int k = 0; k < b; k++) {
+            g[b - 1 - k][j + b] = c[k][j];
+            g[ny + b + k][j + b] = c[ny - 1 - k][j];
+        }
+    return g;  // corner blocks keep the default state, as the reference's do
+}
+double Solvers::computeMaximumWaveSpeed(vector<EulerStateVector>& cells, EulerMaterialParameters mp) {
+    double prm[6];
+    euler_params(mp, prm);
+    std::vector<double> p = pack(cells, 6, euler_get);
+    vg_solver* s = cached_solver(VG_MODEL_EULER, (int)cells.size(), 1, VG_TRANSMISSIVE, prm, 6);
+    check(vg_upload_primitive(s, p.data(), 0, nullptr), "vg_upload_primitive");
+    double out = 0.0;
+    check(vg_max_wave_speed(s, &out, nullptr), "vg_max_wave_speed");
+    return out;
+}
+double Solvers::computeMaximumWaveSpeed2D(vector<vector<EulerStateVector> >& cells, EulerMaterialParameters mp) {
+    // the ghosted array the reference passes here contains its default-constructed corners; vg_max_wave_speed adds
+    // the default state's speed for a 2D grid, which is the same set of values
+    double prm[6];
+    euler_params(mp, prm);
+    std::vector<double> p = pack2(cells, 6, euler_get);
+    vg_solver* s = cached_solver(VG_MODEL_EULER, (int)cells[0].size(), (int)cells.size(), VG_TRANSMISSIVE, prm, 6);
+    check(vg_upload_primitive(s, p.data(), 0, nullptr), "vg_upload_primitive");
+    double out = 0.0;
+    check(vg_max_wave_speed(s, &out, nullptr), "vg_max_wave_speed");
+    return out;
+}
+double Solvers::computeStableTimeStep(double dt, double t, double tEnd, int it) {
+    double d = dt;
+    if (it <= 5) d *= 0.2;
+    if ((t + d) > tEnd) d = tEnd - t;
+    return d;
+}
+double Solvers::computeStableTimeStep(vector<EulerStateVector>& cells, double dx, double cfl, double t, double tEnd, int it,
+                                      EulerMaterialParameters mp) {
+    return computeStableTimeStep(cfl * (dx / computeMaximumWaveSpeed(cells, mp)), t, tEnd, it);
+}
+double Solvers::computeStableTimeStep2D(vector<vector<EulerStateVector> >& cells, double dx, double cfl, double t, double tEnd,
+                                        int it, EulerMaterialParameters mp) {
+    return computeStableTimeStep(cfl * (dx / computeMaximumWaveSpeed2D(cells, mp)), t, tEnd, it);
+}
+
+// ------------------------------------------------------------------------------------------- Euler solver
+void SecondOrderSolver::computeSLICTimeStep(vector<EulerStateVector>& cells, vector<EulerStateVector>& withB, double dx,
+                                            double dt, double bias, int limiter, EulerMaterialParameters mp) {
+    long n = cells.size();
+    if ((long)withB.size() != n + 4) throw std::runtime_error("computeSLICTimeStep: need 2 ghost cells per side");
+    int bc = boundary_kind(n, [&](long g, long c) { return equal_cells(withB[g], cells[c], 6, euler_get); });
+    if (bc < 0) throw std::runtime_error("computeSLICTimeStep: ghost cells other than transmissive or periodic copies");
+    double prm[6];
+    euler_params(mp, prm);
+    vg_solver* s = cached_solver(VG_MODEL_EULER, (int)n, 1, bc, prm, 6);
+    std::vector<double> p = pack(cells, 6, euler_get);
+    check(vg_upload_primitive(s, p.data(), 0, nullptr), "vg_upload_primitive");
+    check(vg_sweep(s, 0, dx, dt, bias, limiter, nullptr), "vg_sweep");
+    check(vg_download_primitive(s, p.data(), 0, nullptr), "vg_download_primitive");
+    cells = unpack<EulerStateVector>(p, n, 6, euler_make);
+}
+void SecondOrderSolver::computeXSLICTimeStep2D(vector<vector<EulerStateVector> >& cells, vector<vector<EulerStateVector> >& withB,
+                                               double dx, double dt, double bias, int limiter, EulerMaterialParameters mp) {
+    double prm[6];
+    euler_params(mp, prm);
+    sweep2d(VG_MODEL_EULER, 6, cells, withB, 0, dx, dt, bias, limiter, prm, 6, euler_get, euler_make);
+}
+void SecondOrderSolver::computeYSLICTimeStep2D(vector<vector<EulerStateVector> >& cells, vector<vector<EulerStateVector> >& withB,
+                                               double dx, double dt, double bias, int limiter, EulerMaterialParameters mp) {
+    double prm[6];
+    euler_params(mp, prm);
+    sweep2d(VG_MODEL_EULER, 6, cells, withB, 1, dx, dt, bias, limiter, prm, 6, euler_get, euler_make);
+}
+vector<EulerStateVector> SecondOrderSolver::solve(vector<EulerStateVector>& initialCells, double dx, double cfl, double tEnd,
+                                                  double bias, int limiter, int /*subcycles: no source in the Euler model*/,
+                                                  EulerMaterialParameters mp) {
+    double prm[6];
+    euler_params(mp, prm);
+    std::vector<double> p = pack(initialCells, 6, euler_get);
+    run_planes(VG_MODEL_EULER, p, (int)initialCells.size(), 1, prm, 6, dx, cfl, tEnd, bias, limiter, 0);
+    return unpack<EulerStateVector>(p, initialCells.size(), 6, euler_make);
+}
+vector<vector<EulerStateVector> > SecondOrderSolver::solve2D(vector<vector<EulerStateVector> >& initialCells, double dx,
+                                                             double cfl, double tEnd, double bias, int limiter, int,
+                                                             EulerMaterialParameters mp) {
+    double prm[6];
+    euler_params(mp, prm);
+    std::vector<double> p = pack2(initialCells, 6, euler_get);
+    long ny = initialCells.size(), nx = initialCells[0].size();
+    run_planes(VG_MODEL_EULER, p, (int)nx, (int)ny, prm, 6, dx, cfl, tEnd, bias, limiter, 0);
+    return unpack2<EulerStateVector>(p, nx, ny, 6, euler_make);
+}
+
+// --------------------------------------------------------------------------------------------- MHD solver
+void MHDSecondOrderSolver::computeXSLICTimeStep2D(vector<vector<MHDStateVector> >& cells, vector<vector<MHDStateVector> >& withB,
+                                                  double dx, double dt, double bias, int limiter, MHDMaterialParameters mp) {
+    double prm[3];
+    mhd_params(mp, prm);
+    sweep2d(VG_MODEL_MHD, 9, cells, withB, 0, dx, dt, bias, limiter, prm, 3, mhd_get, mhd_make);
+}
+void MHDSecondOrderSolver::computeYSLICTimeStep2D(vector<vector<MHDStateVector> >& cells, vector<vector<MHDStateVector> >& withB,
+                                                  double dx, double dt, double bias, int limiter, MHDMaterialParameters mp) {
+    double prm[3];
+    mhd_params(mp, prm);
+    sweep2d(VG_MODEL_MHD, 9, cells, withB, 1, dx, dt, bias, limiter, prm, 3, mhd_get, mhd_make);
+}
+vector<MHDStateVector> MHDSecondOrderSolver::solve(vector<MHDStateVector>& initialCells, double dx, double cfl, double tEnd,
+                                                   double bias, int limiter, int subcycles, MHDMaterialParameters mp) {
+    if (subcycles != 0) throw std::runtime_error("MHD GLM damping sub-cycles are not available on the GPU path");
+    double prm[3];
+    mhd_params(mp, prm);
+    std::vector<double> p = pack(initialCells, 9, mhd_get);
+    run_planes(VG_MODEL_MHD, p, (int)initialCells.size(), 1, prm, 3, dx, cfl, tEnd, bias, limiter, 0);
+    return unpack<MHDStateVector>(p, initialCells.size(), 9, mhd_make);
+}
+vector<vector<MHDStateVector> > MHDSecondOrderSolver::solve2D(vector<vector<MHDStateVector> >& initialCells, double dx, double cfl,
+                                                              double tEnd, double bias, int limiter, int subcycles,
+                                                              MHDMaterialParameters mp) {
+    if (subcycles != 0) throw std::runtime_error("MHD GLM damping sub-cycles are not available on the GPU path");
+    double prm[3];
+    mhd_params(mp, prm);
+    std::vector<double> p = pack2(initialCells, 9, mhd_get);
+    long ny = initialCells.size(), nx = initialCells[0].size();
+    run_planes(VG_MODEL_MHD, p, (int)nx, (int)ny, prm, 3, dx, cfl, tEnd, bias, limiter, 0);
+    return unpack2<MHDStateVector>(p, nx, ny, 9, mhd_make);
+}
+
+// --------------------------------------------------------------------------------------------- HPR solver
+vector<HPRStateVector> HPRSecondOrderSolver::solve(vector<HPRStateVector>& initialCells, double dx, double cfl, double tEnd,
+                                                   double bias, int limiter, int subcycles, HPRMaterialParameters mp) {
+    double prm[12];
+    hpr_params(mp, prm);
+    std::vector<double> p = pack(initialCells, 17, hpr_get);
+    run_planes(VG_MODEL_HPR, p, (int)initialCells.size(), 1, prm, 12, dx, cfl, tEnd, bias, limiter, subcycles);
+    return unpack<HPRStateVector>(p, initialCells.size(), 17, hpr_make);
+}
+vector<vector<HPRStateVector> > HPRSecondOrderSolver::solve2D(vector<vector<HPRStateVector> >& initialCells, double dx, double cfl,
+                                                              double tEnd, double bias, int limiter, int subcycles,
+                                                              HPRMaterialParameters mp) {
+    double prm[12];
+    hpr_params(mp, prm);
+    std::vector<double> p = pack2(initialCells, 17, hpr_get);
+    long ny = initialCells.size(), nx = initialCells[0].size();
+    run_planes(VG_MODEL_HPR, p, (int)nx, (int)ny, prm, 12, dx, cfl, tEnd, bias, limiter, subcycles);
+    return unpack2<HPRStateVector>(p, nx, ny, 17, hpr_make);
+}

@@ -1,0 +1,287 @@
+// Drop-in C++ surface of Vanguard's single-material SLIC path, backed by the B200 C ABI (include/vanguard_slic.h).
+//
+// Same class names, static-method signatures and value semantics as the reference's Solvers/ entry points
+// (Solvers/secondordersolver.h:7-72, Solvers/mhdsecondordersolver.h:12-70, Solvers/hprsecondordersolver.h:12-67,
+// Solvers/slopelimiters.h:23-70, Solvers/solvers.h:8-76) and of the model types they take, so existing callers
+// recompile against vanguard_b200/shim and link libvanguard_shim.so instead of the OpenMP sources:
+//   * solve / solve2D copy the input, run the whole time loop on the GPU and return the result by value;
+//   * the per-sweep functions update `cells` in place from the caller's ghosted array;
+//   * errors (no GPU, unsupported input) throw std::runtime_error with the C ABI's message -- the reference has
+//     no error reporting, and this layer never falls back to a CPU path.
+// Environment: VG_DEVICE selects the CUDA device (default 0); VG_PRECISION=mixed selects the mixed FP32/FP64 form
+// (default: the plain FP64 form, bitwise equal to the reference).
+#pragma once
+
+#include <string>
+#include <vector>
+
+using std::string;
+using std::vector;
+
+// ------------------------------------------------------------------------------------------------- Euler
+class EulerMaterialParameters {
+public:
+    EulerMaterialParameters();
+    explicit EulerMaterialParameters(double newAdiabaticIndex);
+    EulerMaterialParameters(double newAdiabaticIndex, double newStiffeningParameter);
+    EulerMaterialParameters(double newAdiabaticIndex, double newStiffeningParameter, double newSpecificHeatCapacity,
+                            double newEnergyOfFormation, double newIgnitionTemperature, double newReactionRate);
+    void setAdiabaticIndex(double v) { adiabaticIndex = v; }
+    void setStiffeningParameter(double v) { stiffeningParameter = v; }
+    void setSpecificHeatCapacity(double v) { specificHeatCapacity = v; }
+    void setEnergyOfFormation(double v) { energyOfFormation = v; }
+    void setIgnitionTemperature(double v) { ignitionTemperature = v; }
+    void setReactionRate(double v) { reactionRate = v; }
+    double getAdiabaticIndex() const { return adiabaticIndex; }
+    double getStiffeningParameter() const { return stiffeningParameter; }
+    double getSpecificHeatCapacity() const { return specificHeatCapacity; }
+    double getEnergyOfFormation() const { return energyOfFormation; }
+    double getIgnitionTemperature() const { return ignitionTemperature; }
+    double getReactionRate() const { return reactionRate; }
+
+private:
+    double adiabaticIndex, stiffeningParameter, specificHeatCapacity, energyOfFormation, ignitionTemperature, reactionRate;
+};
+
+class EulerEquationOfState {
+public:
+    static double computeSpecificInternalEnergy(double density, double pressure, EulerMaterialParameters mp);
+    static double computePressure(double density, double specificInternalEnergy, EulerMaterialParameters mp);
+    static double computeSoundSpeed(double density, double pressure, EulerMaterialParameters mp);
+};
+
+class EulerStateVector {
+public:
+    EulerStateVector();
+    EulerStateVector(double newDensity, double newXVelocity, double newYVelocity, double newZVelocity, double newPressure);
+    EulerStateVector(double newDensity, double newXVelocity, double newYVelocity, double newZVelocity, double newPressure,
+                     double newReactionProgress);
+    void setPrimitiveVariableVector(vector<double> w);
+    void setConservedVariableVector(vector<double> u, EulerMaterialParameters mp);
+    vector<double> computePrimitiveVariableVector() const;
+    vector<double> computeConservedVariableVector(EulerMaterialParameters mp) const;
+    static vector<double> computeXFluxVector(vector<double> u, EulerMaterialParameters mp);
+    vector<double> computeXFluxVector(EulerMaterialParameters mp) const;
+    static vector<double> computeYFluxVector(vector<double> u, EulerMaterialParameters mp);
+    vector<double> computeYFluxVector(EulerMaterialParameters mp) const;
+    double computeSpecificInternalEnergy(EulerMaterialParameters mp) const;
+    double computeTotalEnergy(EulerMaterialParameters mp) const;
+    double computeSoundSpeed(EulerMaterialParameters mp) const;
+    void setDensity(double v) { density = v; }
+    void setXVelocity(double v) { xVelocity = v; }
+    void setYVelocity(double v) { yVelocity = v; }
+    void setZVelocity(double v) { zVelocity = v; }
+    void setPressure(double v) { pressure = v; }
+    void setReactionProgress(double v) { reactionProgress = v; }
+    double getDensity() const { return density; }
+    double getXVelocity() const { return xVelocity; }
+    double getYVelocity() const { return yVelocity; }
+    double getZVelocity() const { return zVelocity; }
+    double getPressure() const { return pressure; }
+    double getReactionProgress() const { return reactionProgress; }
+
+private:
+    double density, xVelocity, yVelocity, zVelocity, pressure, reactionProgress;
+};
+
+// --------------------------------------------------------------------------------------------------- MHD
+class MHDMaterialParameters {
+public:
+    MHDMaterialParameters();
+    explicit MHDMaterialParameters(double newAdiabaticIndex);
+    double computeHyperbolicWaveSpeedSquared() const { return hyperbolicWaveSpeed * hyperbolicWaveSpeed; }
+    double computeParabolicDampingSquared() const { return parabolicDamping * parabolicDamping; }
+    void configureParabolicDamping();
+    void setAdiabaticIndex(double v) { adiabaticIndex = v; }
+    void setStiffeningParameter(double v) { stiffeningParameter = v; }
+    void setHyperbolicWaveSpeed(double v) { hyperbolicWaveSpeed = v; }
+    void setParabolicDamping(double v) { parabolicDamping = v; }
+    double getAdiabaticIndex() const { return adiabaticIndex; }
+    double getStiffeningParameter() const { return stiffeningParameter; }
+    double getHyperbolicWaveSpeed() const { return hyperbolicWaveSpeed; }
+    double getParabolicDamping() const { return parabolicDamping; }
+
+private:
+    double adiabaticIndex, stiffeningParameter, hyperbolicWaveSpeed, parabolicDamping;
+};
+
+class MHDStateVector {
+public:
+    MHDStateVector();
+    MHDStateVector(double newDensity, double newXVelocity, double newYVelocity, double newZVelocity, double newPressure,
+                   double newXMagneticField, double newYMagneticField, double newZMagneticField, double newAuxiliaryField);
+    void setPrimitiveVariableVector(vector<double> w);
+    vector<double> computePrimitiveVariableVector() const;
+    vector<double> computeConservedVariableVector(MHDMaterialParameters mp) const;
+    void setConservedVariableVector(vector<double> u, MHDMaterialParameters mp);
+    double getDensity() const { return w_[0]; }
+    double getXVelocity() const { return w_[1]; }
+    double getYVelocity() const { return w_[2]; }
+    double getZVelocity() const { return w_[3]; }
+    double getPressure() const { return w_[4]; }
+    double getXMagneticField() const { return w_[5]; }
+    double getYMagneticField() const { return w_[6]; }
+    double getZMagneticField() const { return w_[7]; }
+    double getAuxiliaryField() const { return w_[8]; }
+    void setDensity(double v) { w_[0] = v; }
+    void setXVelocity(double v) { w_[1] = v; }
+    void setYVelocity(double v) { w_[2] = v; }
+    void setZVelocity(double v) { w_[3] = v; }
+    void setPressure(double v) { w_[4] = v; }
+    void setXMagneticField(double v) { w_[5] = v; }
+    void setYMagneticField(double v) { w_[6] = v; }
+    void setZMagneticField(double v) { w_[7] = v; }
+    void setAuxiliaryField(double v) { w_[8] = v; }
+
+private:
+    double w_[9];
+};
+
+// --------------------------------------------------------------------------------------------------- HPR
+class HPRMaterialParameters {
+public:
+    HPRMaterialParameters();
+    HPRMaterialParameters(string newEquationOfState, bool newIsThermal, bool newIsPlastic, double newIdealGasConstant,
+                          double newReferenceDensity, double newReferencePressure, double newReferenceTemperature,
+                          double newInitialTemperature, double newSpecificHeatCapacity, double newAdiabaticIndex,
+                          double newStiffeningParameter, double newReferenceSoundSpeed, double newReferenceGruneisenCoefficient,
+                          double newHugoniotSlopeCoefficient, double newReferenceInternalEnergy, double newTransverseWaveSpeed,
+                          double newStrainDissipationTime, double newThermalImpulseRelaxationTime,
+                          double newDynamicViscosityCoefficient, double newPrandtlNumber,
+                          double newElasticPlasticTransitionParameter, double newPowerLawIndex, double newHeatWaveSpeed,
+                          double newAlphaParameter, double newBetaParameter, double newGammaParameter);
+    void configureStrainDissipationTime();
+    void configureThermalImpulseRelaxationTime();
+    void configureThermalImpulseRelaxationTime(double heatConductionCoefficient);
+    double computeStrainDissipationTime() const;
+    double computeHeatConductionCoefficient() const;
+    double computeThermalImpulseRelaxationTime() const;
+    double computeThermalImpulseRelaxationTime(double heatConductionCoefficient) const;
+    string getEquationOfState() const { return equationOfState; }
+    bool getIsThermal() const { return isThermal; }
+    bool getIsPlastic() const { return isPlastic; }
+    double getReferenceDensity() const { return referenceDensity; }
+    double getReferencePressure() const { return referencePressure; }
+    double getReferenceTemperature() const { return referenceTemperature; }
+    double getInitialTemperature() const { return initialTemperature; }
+    double getSpecificHeatCapacity() const { return specificHeatCapacity; }
+    double getAdiabaticIndex() const { return adiabaticIndex; }
+    double getStiffeningParameter() const { return stiffeningParameter; }
+    double getTransverseWaveSpeed() const { return transverseWaveSpeed; }
+    double getStrainDissipationTime() const { return strainDissipationTime; }
+    double getThermalImpulseRelaxationTime() const { return thermalImpulseRelaxationTime; }
+    double getHeatWaveSpeed() const { return heatWaveSpeed; }
+    void setIsThermal(bool v) { isThermal = v; }
+    void setStrainDissipationTime(double v) { strainDissipationTime = v; }
+    void setThermalImpulseRelaxationTime(double v) { thermalImpulseRelaxationTime = v; }
+
+private:
+    string equationOfState;
+    bool isThermal, isPlastic;
+    double idealGasConstant, referenceDensity, referencePressure, referenceTemperature, initialTemperature,
+        specificHeatCapacity, adiabaticIndex, stiffeningParameter, referenceSoundSpeed, referenceGruneisenCoefficient,
+        hugoniotSlopeCoefficient, referenceInternalEnergy, transverseWaveSpeed, strainDissipationTime,
+        thermalImpulseRelaxationTime, dynamicViscosityCoefficient, prandtlNumber, elasticPlasticTransitionParameter,
+        powerLawIndex, heatWaveSpeed, alphaParameter, betaParameter, gammaParameter;
+};
+
+class HPRStateVector {
+public:
+    HPRStateVector();
+    HPRStateVector(double newDensity, double newPressure, vector<vector<double> > newDistortionTensor, double newXVelocity,
+                   double newYVelocity, double newZVelocity, double newXThermalImpulse, double newYThermalImpulse,
+                   double newZThermalImpulse);
+    double getDensity() const { return w_[0]; }
+    double getPressure() const { return w_[1]; }
+    vector<vector<double> > getDistortionTensor() const;
+    double getXVelocity() const { return w_[11]; }
+    double getYVelocity() const { return w_[12]; }
+    double getZVelocity() const { return w_[13]; }
+    double getXThermalImpulse() const { return w_[14]; }
+    double getYThermalImpulse() const { return w_[15]; }
+    double getZThermalImpulse() const { return w_[16]; }
+    void setDensity(double v) { w_[0] = v; }
+    void setPressure(double v) { w_[1] = v; }
+    void setDistortionTensor(vector<vector<double> > a);
+    void setXVelocity(double v) { w_[11] = v; }
+    void setYVelocity(double v) { w_[12] = v; }
+    void setZVelocity(double v) { w_[13] = v; }
+    void setXThermalImpulse(double v) { w_[14] = v; }
+    void setYThermalImpulse(double v) { w_[15] = v; }
+    void setZThermalImpulse(double v) { w_[16] = v; }
+    const double* data() const { return w_; }
+    double* data() { return w_; }
+
+private:
+    double w_[17];
+};
+
+// ------------------------------------------------------------------------------------------- slope limiters
+class SlopeLimiters {
+public:
+    static double computeRCoefficient(double steepness, double bias);
+    static double computeSuperBeeSlopeLimiter(double steepness, double bias);
+    static double computeVanLeerSlopeLimiter(double steepness, double bias);
+    static double computeMinBeeSlopeLimiter(double steepness, double bias);
+    static double computeSlopeLimiter(double steepness, double bias, int slopeLimiter);
+};
+
+// ------------------------------------------------------------------------------------------- solver helpers
+class Solvers {
+public:
+    static vector<EulerStateVector> insertBoundaryCells(vector<EulerStateVector>& currentCells, int boundarySize);
+    static vector<vector<EulerStateVector> > insertBoundaryCells2D(vector<vector<EulerStateVector> >& currentCells, int boundarySize);
+    static double computeMaximumWaveSpeed(vector<EulerStateVector>& currentCells, EulerMaterialParameters mp);
+    static double computeMaximumWaveSpeed2D(vector<vector<EulerStateVector> >& currentCells, EulerMaterialParameters mp);
+    static double computeStableTimeStep(vector<EulerStateVector>& currentCells, double cellSpacing, double CFLCoefficient,
+                                        double currentTime, double finalTime, int currentIteration, EulerMaterialParameters mp);
+    static double computeStableTimeStep2D(vector<vector<EulerStateVector> >& currentCells, double cellSpacing,
+                                          double CFLCoefficient, double currentTime, double finalTime, int currentIteration,
+                                          EulerMaterialParameters mp);
+    static double computeStableTimeStep(double timeStep, double currentTime, double finalTime, int currentIteration);
+};
+
+// ------------------------------------------------------------------------------------------------ solvers
+class SecondOrderSolver {
+public:
+    static void computeSLICTimeStep(vector<EulerStateVector>& currentCells, vector<EulerStateVector>& currentCellsWithBoundary,
+                                    double cellSpacing, double timeStep, double bias, int slopeLimiter, EulerMaterialParameters mp);
+    static void computeXSLICTimeStep2D(vector<vector<EulerStateVector> >& currentCells,
+                                       vector<vector<EulerStateVector> >& currentCellsWithBoundary, double cellSpacing,
+                                       double timeStep, double bias, int slopeLimiter, EulerMaterialParameters mp);
+    static void computeYSLICTimeStep2D(vector<vector<EulerStateVector> >& currentCells,
+                                       vector<vector<EulerStateVector> >& currentCellsWithBoundary, double cellSpacing,
+                                       double timeStep, double bias, int slopeLimiter, EulerMaterialParameters mp);
+    static vector<EulerStateVector> solve(vector<EulerStateVector>& initialCells, double cellSpacing, double CFLCoefficient,
+                                          double finalTime, double bias, int slopeLimiter, int subcyclingIterations,
+                                          EulerMaterialParameters mp);
+    static vector<vector<EulerStateVector> > solve2D(vector<vector<EulerStateVector> >& initialCells, double cellSpacing,
+                                                     double CFLCofficient, double finalTime, double bias, int slopeLimiter,
+                                                     int subcyclingIterations, EulerMaterialParameters mp);
+};
+
+class MHDSecondOrderSolver {
+public:
+    static void computeXSLICTimeStep2D(vector<vector<MHDStateVector> >& currentCells,
+                                       vector<vector<MHDStateVector> >& currentCellsWithBoundary, double cellSpacing,
+                                       double timeStep, double bias, int slopeLimiter, MHDMaterialParameters mp);
+    static void computeYSLICTimeStep2D(vector<vector<MHDStateVector> >& currentCells,
+                                       vector<vector<MHDStateVector> >& currentCellsWithBoundary, double cellSpacing,
+                                       double timeStep, double bias, int slopeLimiter, MHDMaterialParameters mp);
+    static vector<MHDStateVector> solve(vector<MHDStateVector>& initialCells, double cellSpacing, double CFLCoefficient,
+                                        double finalTime, double bias, int slopeLimiter, int subcyclingIterations,
+                                        MHDMaterialParameters mp);
+    static vector<vector<MHDStateVector> > solve2D(vector<vector<MHDStateVector> >& initialCells, double cellSpacing,
+                                                   double CFLCoefficient, double finalTime, double bias, int slopeLimiter,
+                                                   int subcyclingIterations, MHDMaterialParameters mp);
+};
+
+class HPRSecondOrderSolver {
+public:
+    static vector<HPRStateVector> solve(vector<HPRStateVector>& initialCells, double cellSpacing, double CFLCoefficient,
+                                        double finalTime, double bias, int slopeLimiter, int subcyclingIterations,
+                                        HPRMaterialParameters mp);
+    static vector<vector<HPRStateVector> > solve2D(vector<vector<HPRStateVector> >& initialCells, double cellSpacing,
+                                                   double CFLCoefficient, double finalTime, double bias, int slopeLimiter,
+                                                   int subcyclingIterations, HPRMaterialParameters mp);
+};
