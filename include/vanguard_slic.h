@@ -142,6 +142,25 @@ vg_status vg_autotune(vg_solver* s, const vg_run_config* cfg, int reps, float* t
 vg_status vg_set_launch_config(vg_solver* s, int xcfg, int ycfg);
 vg_status vg_get_launch_config(vg_solver* s, int* xcfg, int* ycfg, const char** xname, const char** yname);
 
+/* ---- Ragged batches of independent 1D Euler problems.  No counterpart in the reference, whose scenario drivers
+ * call SecondOrderSolver::solve (Solvers/secondordersolver.cpp:288-314) once per problem; a batch runs that same
+ * per-problem loop for many problems at once, each instance bit-equal to its own solve().
+ * Instance k has ncell[k] >= 2 cells of width dx[k], adiabatic index gamma[k] and stiffening p_inf[k] (p_inf may be
+ * NULL: 0), transmissive boundaries.  State planes at this boundary are the 6 Euler primitive planes of all
+ * instances concatenated in instance order (total = sum of ncell), with v == w == 0 and lambda == 1.
+ * vg_batch_run advances every instance by `steps` steps, each with its own dt_k = CFL dx_k / S_k (x0.2 for the
+ * first six steps) computed on the device; the whole loop is one captured CUDA graph of one persistent kernel
+ * per step.  dt_last (nullable, ninst entries) receives each instance's last time step. */
+typedef struct vg_batch vg_batch;
+vg_status vg_batch_create(int ninst, const int* ncell, const double* dx, const double* gamma, const double* p_inf,
+                          int device, vg_batch** out);
+vg_status vg_batch_destroy(vg_batch* b);
+long vg_batch_total_cells(vg_batch* b);
+vg_status vg_batch_upload(vg_batch* b, const double* planes, int is_device, void* stream);
+vg_status vg_batch_download(vg_batch* b, double* planes, int is_device, void* stream);
+vg_status vg_batch_run(vg_batch* b, double cfl, int steps, double bias, int limiter, double* dt_last, void* stream);
+long vg_batch_last_launch_count(vg_batch* b);
+
 /* Rows accepted by vg_max_wave_speed_noalloc: the size of its static scratch array (8 bytes per row,
  * 512 KiB, held on every GPU that loads the library until the process exits). */
 #define VG_NOALLOC_MAX_ROWS 65536

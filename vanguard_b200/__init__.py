@@ -50,7 +50,9 @@ class RunConfig(ctypes.Structure):
 EXPORTS = ["vg_create", "vg_destroy", "vg_model_nvar", "vg_upload_primitive", "vg_download_primitive",
            "vg_run", "vg_solve", "vg_sweep", "vg_max_wave_speed", "vg_state_device", "vg_last_launch_count",
            "vg_last_error_string", "vg_status_string", "vg_max_wave_speed_noalloc", "vg_autotune",
-           "vg_set_launch_config", "vg_get_launch_config"]
+           "vg_set_launch_config", "vg_get_launch_config", "vg_batch_create", "vg_batch_destroy",
+           "vg_batch_total_cells", "vg_batch_upload", "vg_batch_download", "vg_batch_run",
+           "vg_batch_last_launch_count"]
 NUM_XCFG, NUM_YCFG = 5, 6
 
 NOALLOC_MAX_ROWS = 65536
@@ -94,6 +96,16 @@ def lib():
                                            ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_char_p)]
         L.vg_last_launch_count.argtypes = [vp]
         L.vg_last_launch_count.restype = ctypes.c_long
+        I = ctypes.POINTER(ctypes.c_int)
+        L.vg_batch_create.argtypes = [ctypes.c_int, I, D, D, D, ctypes.c_int, ctypes.POINTER(vp)]
+        L.vg_batch_destroy.argtypes = [vp]
+        L.vg_batch_total_cells.argtypes = [vp]
+        L.vg_batch_total_cells.restype = ctypes.c_long
+        L.vg_batch_upload.argtypes = [vp, vp, ctypes.c_int, vp]
+        L.vg_batch_download.argtypes = [vp, vp, ctypes.c_int, vp]
+        L.vg_batch_run.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_int, D, vp]
+        L.vg_batch_last_launch_count.argtypes = [vp]
+        L.vg_batch_last_launch_count.restype = ctypes.c_long
         L.vg_last_error_string.restype = ctypes.c_char_p
         L.vg_status_string.restype = ctypes.c_char_p
         L.vg_status_string.argtypes = [ctypes.c_int]
@@ -212,3 +224,60 @@ class Solver:
 
     def set_launch_config(self, xcfg, ycfg):
         return _check(lib().vg_set_launch_config(self._h, xcfg, ycfg))
+
+
+class Batch:
+    """Ragged batch of independent 1D Euler problems (vg_batch_*): one persistent kernel per step, the whole
+    time loop replayed from one CUDA graph, per-instance dt on the device."""
+
+    def __init__(self, ncell, dx, gamma, p_inf=None, device=0):
+        self.ncell = np.ascontiguousarray(ncell, dtype=np.int32)
+        self.dx = np.ascontiguousarray(dx, dtype=np.float64)
+        self.gamma = np.ascontiguousarray(gamma, dtype=np.float64)
+        self.p_inf = None if p_inf is None else np.ascontiguousarray(p_inf, dtype=np.float64)
+        self.ninst = len(self.ncell)
+        self.total = int(self.ncell.sum())
+        self._h = ctypes.c_void_p()
+        D = ctypes.POINTER(ctypes.c_double)
+        _check(lib().vg_batch_create(self.ninst, self.ncell.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                     self.dx.ctypes.data_as(D), self.gamma.ctypes.data_as(D),
+                                     None if self.p_inf is None else self.p_inf.ctypes.data_as(D), device,
+                                     ctypes.byref(self._h)))
+
+    def close(self):
+        if self._h:
+            lib().vg_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def upload(self, planes, stream=None):
+        """planes: (6, total) float64 Euler primitives of all instances concatenated."""
+        if hasattr(planes, "data_ptr"):
+            return _check(lib().vg_batch_upload(self._h, ctypes.c_void_p(planes.data_ptr()), 1, stream))
+        a = np.ascontiguousarray(planes, dtype=np.float64)
+        return _check(lib().vg_batch_upload(self._h, a.ctypes.data_as(ctypes.c_void_p), 0, stream))
+
+    def download(self, stream=None):
+        a = np.empty((6, self.total))
+        _check(lib().vg_batch_download(self._h, a.ctypes.data_as(ctypes.c_void_p), 0, stream))
+        return a
+
+    def run(self, cfl, steps, bias=0.0, limiter=SUPERBEE, stream=None):
+        dts = np.empty(self.ninst)
+        _check(lib().vg_batch_run(self._h, cfl, steps, bias, limiter,
+                                  dts.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), stream))
+        return dts
+
+    def last_launch_count(self):
+        return lib().vg_batch_last_launch_count(self._h)

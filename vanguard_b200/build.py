@@ -27,6 +27,7 @@ UNITS = [
     ("slic_mixed.cu", ["-fmad=true"]),
     ("vg_api.cu", []),
     ("vg_noalloc.cu", ["-fmad=false"]),
+    ("batch.cu", ["-fmad=false"]),
 ]
 
 

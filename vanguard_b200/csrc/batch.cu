@@ -1,0 +1,436 @@
+// Ragged batches of independent 1D Euler problems in one persistent launch per time step.
+//
+// Instances k = 0..K-1 have n_k cells (any sizes), their own gamma / p_inf and cell width dx_k, and are
+// concatenated into structure-of-arrays planes (rho, u, p) with a cell-offset table.  The work is cut into
+// tiles of P - 2 consecutive cells of one instance; a persistent grid strides over the tile table, so no block
+// straddles two instances and the transmissive ghosts of each instance are synthesised by the loader exactly as
+// Solvers::insertBoundaryCells builds them (Solvers/solvers.cpp:7-32).  Every instance takes its own time step
+// dt_k = CFL * dx_k / S_k (x0.2 for the first six steps, Solvers/solvers.cpp:437-452) from its own maximum wave
+// speed S_k, kept on the device in a three-slot ring: step s reads slot s % 3, accumulates the next maximum into
+// (s + 1) % 3 in the update epilogue and clears (s + 2) % 3.  The last block to finish a step advances the step
+// counter, so one kernel per step and a captured CUDA graph of many steps run the whole time loop with no host
+// involvement.  Each instance reproduces SecondOrderSolver::solve's step (Solvers/secondordersolver.cpp:288-314)
+// bit for bit.  Compiled with -fmad=false.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/vanguard_slic.h"
+#include "physics_fp64.cuh"
+#include "slic_kernels.cuh"
+#include "vg_ops.h"
+
+namespace vg {
+namespace {
+
+using M1 = EulerF64<1>;
+constexpr int BP = 128;  // cells per tile segment (BP - 2 outputs)
+
+struct Tile {
+    int inst;   // instance
+    int s0;     // first output cell within the instance
+};
+
+struct BatchArgs {
+    const double* in;
+    double* out;
+    long plane;                 // plane stride (total cells)
+    const long* offset;         // first cell of each instance
+    const int* ncell;           // cells of each instance
+    const double* dx;           // cell width of each instance
+    const double* gam;          // gamma, p_inf of each instance (2 per instance)
+    const Tile* tiles;
+    int ntiles;
+    int ninst;
+    unsigned long long* smax;   // 3 x ninst ring of wave-speed maxima (bit patterns)
+    double* dt_out;             // dt of the current step per instance (diagnostics / adjoint)
+    int* step;                  // device step counter
+    unsigned int* done;         // blocks finished in this step
+    unsigned int* err;
+    double cfl, bias, floor5;
+    int limiter;
+    int max_steps;
+};
+
+__device__ __forceinline__ double instance_dt(const BatchArgs& a, int k, int s) {
+    double S = __longlong_as_double((long long)a.smax[(s % 3) * a.ninst + k]);
+    double dt = a.cfl * (a.dx[k] / S);
+    if (s <= 5) dt *= 0.2;
+    return dt;
+}
+
+__global__ void __launch_bounds__(BP) batch_step_kernel(BatchArgs a) {
+    constexpr int NU = M1::NU, NW = M1::NW;
+    __shared__ double Us[NU][BP + 2];
+    __shared__ double Es[NU][BP];
+    __shared__ double Fs[NU][BP];
+    __shared__ double red[BP / 32];
+    const int p = threadIdx.x;
+    const int s = *a.step;
+    const bool active = s < a.max_steps;
+    const int slot_next = ((s + 1) % 3) * a.ninst;
+
+    for (int t = blockIdx.x; t < a.ntiles && active; t += gridDim.x) {
+        const Tile tile = a.tiles[t];
+        const int k = tile.inst, len = a.ncell[k], s0 = tile.s0;
+        const long base = a.offset[k];
+        const int cell = s0 - 1 + p;
+        const bool out_ok = p >= 1 && p <= BP - 2 && cell < len;
+        const double dt = instance_dt(a, k, s);
+        SweepConst kc;
+        kc.r = dt / a.dx[k];
+        kc.rinv = a.dx[k] / dt;
+        kc.half_r = 0.5 * (dt / a.dx[k]);
+        kc.cm = 0.5 * (1.0 + a.bias);
+        kc.cp = 0.5 * (1.0 - a.bias);
+        kc.bias = a.bias;
+        kc.floor5 = a.floor5;
+        kc.limiter = a.limiter;
+        M1::P q{a.gam[2 * k], a.gam[2 * k + 1], 0.0};
+        if (p == 0 && s0 == 0) a.dt_out[k] = dt;
+
+        auto conserve = [&](int slot) {
+            int c = ghost_index(s0 - 2 + slot, len, 0);
+            double W[NW], U[NU];
+            for (int v = 0; v < NW; v++) W[v] = a.in[v * a.plane + base + c];
+            M1::cons(W, q, U);
+            for (int v = 0; v < NU; v++) Us[v][slot] = U[v];
+        };
+        conserve(p + 1);
+        if (p == 0) conserve(0);
+        if (p == BP - 1) conserve(BP + 1);
+        __syncthreads();
+        double ub[NU];
+        {
+            double uL[NU], u[NU], uR[NU], ua[NU];
+            for (int v = 0; v < NU; v++) {
+                uL[v] = Us[v][p];
+                u[v] = Us[v][p + 1];
+                uR[v] = Us[v][p + 2];
+            }
+            evolve_edges<M1, 0>(uL, u, uR, kc, q, ub, ua, p >= 1, p <= BP - 2);
+            for (int v = 0; v < NU; v++) Es[v][p] = ua[v];
+        }
+        __syncthreads();
+        if (p >= 1) {
+            double ua[NU], F[NU];
+            for (int v = 0; v < NU; v++) ua[v] = Es[v][p - 1];
+            force_flux<M1, 0>(ua, ub, kc, q, F);
+            for (int v = 0; v < NU; v++) Fs[v][p] = F[v];
+        }
+        __syncthreads();
+        double wave = 0.0;
+        if (out_ok) {
+            double Un[NU], W[NW];
+            for (int v = 0; v < NU; v++) Un[v] = Us[v][p + 1] + (kc.r * (Fs[v][p] - Fs[v][p + 1]));
+            M1::setcons(Un, q, W);
+            for (int v = 0; v < NW; v++) a.out[v * a.plane + base + cell] = W[v];
+            if (bad_state<M1>(W)) atomicOr(a.err, ERR_STATE);
+            double sw = M1::wave(W, q, 1);
+            if (sw > wave) wave = sw;
+        }
+        // per-tile maximum into the instance's next slot
+        for (int o = 16; o > 0; o >>= 1) {
+            double w = __shfl_xor_sync(0xffffffffu, wave, o);
+            wave = (w > wave) ? w : wave;
+        }
+        if ((p & 31) == 0) red[p >> 5] = wave;
+        __syncthreads();
+        if (p == 0) {
+            double m = 0.0;
+            for (int w = 0; w < BP / 32; w++) m = (red[w] > m) ? red[w] : m;
+            if (m > 0.0) atomic_max_nonneg(&a.smax[slot_next + k], m);
+        }
+        __syncthreads();
+    }
+    if (!active) {  // past the last step: carry the state over so the buffer parity stays fixed
+        for (long i = blockIdx.x * (long)BP + threadIdx.x; i < a.plane; i += (long)gridDim.x * BP)
+            for (int v = 0; v < NW; v++) a.out[v * a.plane + i] = a.in[v * a.plane + i];
+    }
+    // the last block to finish advances the step and clears the slot the step after next will fill
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        unsigned int prev = atomicAdd(a.done, 1u);
+        if (prev == gridDim.x - 1) {
+            __threadfence();
+            const int clear = ((s + 2) % 3) * a.ninst;
+            for (int k = 0; k < a.ninst; k++) a.smax[clear + k] = 0ull;
+            if (active) *a.step = s + 1;
+            *a.done = 0u;
+            __threadfence();
+        }
+    }
+}
+
+// Initial maxima: slot 0 <- max over each instance (grid-stride over cells; instance by binary search).
+__global__ void __launch_bounds__(256) batch_max_wave_kernel(BatchArgs a) {
+    for (long i = blockIdx.x * 256L + threadIdx.x; i < a.plane; i += (long)gridDim.x * 256) {
+        int lo = 0, hi = a.ninst - 1;
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (a.offset[mid] <= i) lo = mid;
+            else hi = mid - 1;
+        }
+        double W[M1::NW];
+        for (int v = 0; v < M1::NW; v++) W[v] = a.in[v * a.plane + i];
+        M1::P q{a.gam[2 * lo], a.gam[2 * lo + 1], 0.0};
+        double sw = M1::wave(W, q, 1);
+        if (sw > 0.0) atomic_max_nonneg(&a.smax[lo], sw);
+    }
+}
+
+}  // namespace
+}  // namespace vg
+
+using vg::BatchArgs;
+using vg::Tile;
+
+struct vg_batch {
+    int ninst = 0, device = 0;
+    long total = 0;
+    std::vector<int> ncell;
+    std::vector<long> offset;
+    double* buf[2] = {nullptr, nullptr};
+    long* d_offset = nullptr;
+    int* d_ncell = nullptr;
+    double* d_dx = nullptr;
+    double* d_gam = nullptr;
+    Tile* d_tiles = nullptr;
+    int ntiles = 0;
+    unsigned long long* d_smax = nullptr;
+    double* d_dt = nullptr;
+    int* d_step = nullptr;
+    unsigned int* d_done = nullptr;
+    unsigned int* d_err = nullptr;
+    int cur = 0;
+    int grid = 0;
+    cudaStream_t cap = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = 0, graph_from = -1;
+    double graph_cfl = 0, graph_bias = 0;
+    int graph_limiter = -1, graph_max = -1;
+    long last_launches = 0;
+};
+
+namespace {
+
+vg_status bfail(vg_status st, const std::string& m) {
+    vg::set_last_error(m);
+    return st;
+}
+
+#define VB_CUDA(call)                                                                               \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess) return bfail(e_ == cudaErrorMemoryAllocation ? VG_ENOMEM : VG_ECUDA,  \
+                                            std::string(#call) + ": " + cudaGetErrorString(e_));    \
+    } while (0)
+
+BatchArgs batch_args(vg_batch* b, int from, double cfl, double bias, int limiter, int max_steps) {
+    BatchArgs a{};
+    a.in = b->buf[from];
+    a.out = b->buf[1 - from];
+    a.plane = b->total;
+    a.offset = b->d_offset;
+    a.ncell = b->d_ncell;
+    a.dx = b->d_dx;
+    a.gam = b->d_gam;
+    a.tiles = b->d_tiles;
+    a.ntiles = b->ntiles;
+    a.ninst = b->ninst;
+    a.smax = b->d_smax;
+    a.dt_out = b->d_dt;
+    a.step = b->d_step;
+    a.done = b->d_done;
+    a.err = b->d_err;
+    a.cfl = cfl;
+    a.bias = bias;
+    a.floor5 = std::pow(10.0, -5.0);
+    a.limiter = limiter;
+    a.max_steps = max_steps;
+    return a;
+}
+
+}  // namespace
+
+extern "C" {
+
+vg_status vg_batch_create(int ninst, const int* ncell, const double* dx, const double* gamma, const double* p_inf, int device,
+                          vg_batch** out) {
+    if (!out || !ncell || !dx || !gamma || ninst < 1) return bfail(VG_EINVAL, "bad vg_batch_create argument");
+    *out = nullptr;
+    for (int k = 0; k < ninst; k++)
+        if (ncell[k] < 2 || !(dx[k] > 0.0)) return bfail(VG_EINVAL, "every instance needs >= 2 cells and dx > 0");
+    VB_CUDA(cudaSetDevice(device));
+    vg_batch* b = new (std::nothrow) vg_batch();
+    if (!b) return bfail(VG_ENOMEM, "host allocation");
+    b->ninst = ninst;
+    b->device = device;
+    b->ncell.assign(ncell, ncell + ninst);
+    b->offset.resize(ninst);
+    std::vector<Tile> tiles;
+    long total = 0;
+    for (int k = 0; k < ninst; k++) {
+        b->offset[k] = total;
+        total += ncell[k];
+    }
+    // tiles in decreasing instance size so the persistent grid ends on short work (longest-first balance)
+    std::vector<int> order(ninst);
+    for (int k = 0; k < ninst; k++) order[k] = k;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return ncell[x] > ncell[y]; });
+    for (int k : order)
+        for (int s0 = 0; s0 < ncell[k]; s0 += vg::BP - 2) tiles.push_back({k, s0});
+    b->total = total;
+    b->ntiles = (int)tiles.size();
+    int sms = 148, per_sm = 1;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, vg::batch_step_kernel, vg::BP, 0);
+    b->grid = std::max(1, std::min(b->ntiles, sms * std::max(per_sm, 1)));
+    std::vector<double> gam(2 * ninst);
+    for (int k = 0; k < ninst; k++) {
+        gam[2 * k] = gamma[k];
+        gam[2 * k + 1] = p_inf ? p_inf[k] : 0.0;
+    }
+    cudaError_t e = cudaSuccess;
+    for (int i = 0; i < 2 && e == cudaSuccess; i++) e = cudaMalloc(&b->buf[i], sizeof(double) * 3 * total);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_offset, sizeof(long) * ninst);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_ncell, sizeof(int) * ninst);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_dx, sizeof(double) * ninst);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_gam, sizeof(double) * 2 * ninst);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_tiles, sizeof(Tile) * tiles.size());
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_smax, sizeof(unsigned long long) * 3 * ninst);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_dt, sizeof(double) * ninst);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_step, sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_done, sizeof(unsigned int));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_err, sizeof(unsigned int));
+    if (e == cudaSuccess) e = cudaMemcpy(b->d_offset, b->offset.data(), sizeof(long) * ninst, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(b->d_ncell, ncell, sizeof(int) * ninst, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(b->d_dx, dx, sizeof(double) * ninst, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(b->d_gam, gam.data(), sizeof(double) * 2 * ninst, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(b->d_tiles, tiles.data(), sizeof(Tile) * tiles.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        vg_batch_destroy(b);
+        return bfail(VG_ECUDA, std::string("vg_batch_create: ") + cudaGetErrorString(e));
+    }
+    *out = b;
+    return VG_OK;
+}
+
+vg_status vg_batch_destroy(vg_batch* b) {
+    if (!b) return VG_OK;
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    for (auto p : b->buf)
+        if (p) cudaFree(p);
+    for (void* p : {(void*)b->d_offset, (void*)b->d_ncell, (void*)b->d_dx, (void*)b->d_gam, (void*)b->d_tiles,
+                    (void*)b->d_smax, (void*)b->d_dt, (void*)b->d_step, (void*)b->d_done, (void*)b->d_err})
+        if (p) cudaFree(p);
+    if (b->cap) cudaStreamDestroy(b->cap);
+    delete b;
+    return VG_OK;
+}
+
+long vg_batch_total_cells(vg_batch* b) { return b ? b->total : 0; }
+
+vg_status vg_batch_upload(vg_batch* b, const double* planes, int is_device, void* stream) {
+    if (!b || !planes) return bfail(VG_EINVAL, "null argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    const long n = b->total;
+    if (!is_device) {
+        for (long i = 0; i < n; i++)
+            if (planes[2 * n + i] != 0.0 || planes[3 * n + i] != 0.0 || planes[5 * n + i] != 1.0)
+                return bfail(VG_EUNSUPPORTED, "batched 1D Euler needs v == w == 0 and lambda == 1");
+    }
+    const int ref[3] = {0, 1, 4};
+    for (int k = 0; k < 3; k++)
+        VB_CUDA(cudaMemcpyAsync(b->buf[0] + k * n, planes + ref[k] * n, sizeof(double) * n,
+                                is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+    VB_CUDA(cudaStreamSynchronize(st));
+    b->cur = 0;
+    return VG_OK;
+}
+
+vg_status vg_batch_download(vg_batch* b, double* planes, int is_device, void* stream) {
+    if (!b || !planes) return bfail(VG_EINVAL, "null argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    const long n = b->total;
+    const int ref[3] = {0, 1, 4};
+    for (int k = 0; k < 3; k++)
+        VB_CUDA(cudaMemcpyAsync(planes + ref[k] * n, b->buf[b->cur] + k * n, sizeof(double) * n,
+                                is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
+    VB_CUDA(cudaStreamSynchronize(st));
+    if (!is_device) {
+        for (long i = 0; i < n; i++) {
+            planes[2 * n + i] = 0.0;
+            planes[3 * n + i] = 0.0;
+            planes[5 * n + i] = 1.0;
+        }
+    } else {
+        std::vector<double> z(n, 0.0), o(n, 1.0);
+        VB_CUDA(cudaMemcpy(planes + 2 * n, z.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+        VB_CUDA(cudaMemcpy(planes + 3 * n, z.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+        VB_CUDA(cudaMemcpy(planes + 5 * n, o.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+    }
+    return VG_OK;
+}
+
+vg_status vg_batch_run(vg_batch* b, double cfl, int steps, double bias, int limiter, double* dt_last, void* stream) {
+    if (!b || steps < 1 || !(cfl > 0.0)) return bfail(VG_EINVAL, "bad vg_batch_run argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    VB_CUDA(cudaSetDevice(b->device));
+    // state to buffer 0 so the captured graph always starts there
+    if (b->cur != 0) {
+        VB_CUDA(cudaMemcpyAsync(b->buf[0], b->buf[1], sizeof(double) * 3 * b->total, cudaMemcpyDeviceToDevice, st));
+        b->cur = 0;
+    }
+    VB_CUDA(cudaMemsetAsync(b->d_smax, 0, sizeof(unsigned long long) * 3 * b->ninst, st));
+    VB_CUDA(cudaMemsetAsync(b->d_step, 0, sizeof(int), st));
+    VB_CUDA(cudaMemsetAsync(b->d_done, 0, sizeof(unsigned int), st));
+    VB_CUDA(cudaMemsetAsync(b->d_err, 0, sizeof(unsigned int), st));
+    BatchArgs a0 = batch_args(b, 0, cfl, bias, limiter, steps);
+    int mw = (int)std::min<long>((b->total + 255) / 256, 148L * 8);
+    vg::batch_max_wave_kernel<<<mw, 256, 0, st>>>(a0);
+    VB_CUDA(cudaGetLastError());
+    // one graph per (steps, cfl, bias, limiter): the whole time loop, one persistent kernel per step
+    if (!b->graph || b->graph_steps != steps || b->graph_cfl != cfl || b->graph_bias != bias || b->graph_limiter != limiter) {
+        if (b->graph) cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+        cudaGraph_t g = nullptr;
+        VB_CUDA(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal));
+        for (int i = 0; i < steps; i++) {
+            BatchArgs a = batch_args(b, i & 1, cfl, bias, limiter, steps);
+            vg::batch_step_kernel<<<b->grid, vg::BP, 0, b->cap>>>(a);
+        }
+        cudaError_t e1 = cudaGetLastError();
+        cudaError_t e2 = cudaStreamEndCapture(b->cap, &g);
+        if (e1 != cudaSuccess || e2 != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return bfail(VG_ECUDA, "batch graph capture failed");
+        }
+        cudaError_t e3 = cudaGraphInstantiate(&b->graph, g, 0);
+        cudaGraphDestroy(g);
+        VB_CUDA(e3);
+        b->graph_steps = steps;
+        b->graph_cfl = cfl;
+        b->graph_bias = bias;
+        b->graph_limiter = limiter;
+    }
+    VB_CUDA(cudaGraphLaunch(b->graph, st));
+    b->cur = steps & 1;
+    b->last_launches = 1 + steps;
+    unsigned int err = 0;
+    VB_CUDA(cudaMemcpyAsync(&err, b->d_err, sizeof(err), cudaMemcpyDeviceToHost, st));
+    if (dt_last) VB_CUDA(cudaMemcpyAsync(dt_last, b->d_dt, sizeof(double) * b->ninst, cudaMemcpyDeviceToHost, st));
+    VB_CUDA(cudaStreamSynchronize(st));
+    if (err) return bfail(VG_ENAN, "non-finite or non-positive density/pressure produced");
+    return VG_OK;
+}
+
+long vg_batch_last_launch_count(vg_batch* b) { return b ? b->last_launches : 0; }
+
+}  // extern "C"

@@ -145,3 +145,31 @@ def brio_wu_1d(n=400, gamma=2.0):
     W[5] = 0.75
     W[6] = np.where(is_left, 1.0, -1.0)
     return W
+
+
+def ragged_riemann_batch(ninst=4096, seed=0, nmin=200, nmax=4000):
+    """Independent 1D Riemann problems on [0, 1]: cells ~ U{nmin..nmax}, gamma ~ U[1.2, 1.67], left/right
+    rho ~ U[0.1, 2], u ~ U[-1, 1], p ~ U[0.1, 10], interface at the middle (cell i is left when i <= n/2).
+    Returns (ncell, dx, gamma, theta, planes) with theta the (ninst, 6) initial states
+    (rho_L, u_L, p_L, rho_R, u_R, p_R) and planes the (6, total) concatenated Euler primitives."""
+    rng = np.random.default_rng(seed)
+    ncell = rng.integers(nmin, nmax + 1, ninst)
+    gamma = rng.uniform(1.2, 1.67, ninst)
+    theta = np.stack([rng.uniform(0.1, 2.0, ninst), rng.uniform(-1.0, 1.0, ninst), rng.uniform(0.1, 10.0, ninst),
+                      rng.uniform(0.1, 2.0, ninst), rng.uniform(-1.0, 1.0, ninst), rng.uniform(0.1, 10.0, ninst)], 1)
+    return ncell, 1.0 / ncell, gamma, theta, batch_planes(ncell, theta)
+
+
+def batch_planes(ncell, theta):
+    """Concatenated (6, total) Euler primitive planes of Riemann problems with states theta (ninst, 6)."""
+    total = int(np.sum(ncell))
+    W = np.zeros((EULER_NVAR, total))
+    W[5] = 1.0
+    off = 0
+    for k, n in enumerate(ncell):
+        left = np.arange(n) <= 0.5 * n
+        W[0, off:off + n] = np.where(left, theta[k, 0], theta[k, 3])
+        W[1, off:off + n] = np.where(left, theta[k, 1], theta[k, 4])
+        W[4, off:off + n] = np.where(left, theta[k, 2], theta[k, 5])
+        off += n
+    return W
