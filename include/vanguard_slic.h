@@ -161,6 +161,21 @@ vg_status vg_batch_download(vg_batch* b, double* planes, int is_device, void* st
 vg_status vg_batch_run(vg_batch* b, double cfl, int steps, double bias, int limiter, double* dt_last, void* stream);
 long vg_batch_last_launch_count(vg_batch* b);
 
+/* No counterpart in the reference (it has no derivatives): the discrete adjoint of vg_batch_run.
+ * Loss L = sum over all cells of all instances of (rho(T) - target_rho)^2 after `steps` steps of vg_batch_run
+ * (same cfl, bias, limiter) from the batch's current state.  Returns L, dL/d(initial primitives) in the 6-plane
+ * layout (rho, u, p planes filled; v, w, lambda planes 0: held fixed) and dL/dgamma per instance.  The dt of
+ * every step depends on the state through the CFL maximum and that dependence is differentiated (the first cell
+ * attaining the maximum carries it).  Non-smooth points take the derivative of the branch the forward step took.
+ * `checkpoints` >= 1 state slots on the device (slot 0 holds the initial state; capped at `steps`) bound the
+ * memory to (checkpoints + 3) states; steps are recomputed on Griewank's binomial schedule, so checkpoints ==
+ * steps stores every state and recomputes nothing.  forward_steps / adjoint_steps (nullable) receive the number
+ * of forward steps advanced (recomputation and the final step included) and of reversed steps.  The batch keeps
+ * its initial state.  target_rho, grad_planes (6 x total) and grad_gamma (ninst) are host arrays. */
+vg_status vg_batch_gradient(vg_batch* b, const double* target_rho, double cfl, int steps, double bias, int limiter,
+                            int checkpoints, double* loss, double* grad_planes, double* grad_gamma, long* forward_steps,
+                            long* adjoint_steps, void* stream);
+
 /* Rows accepted by vg_max_wave_speed_noalloc: the size of its static scratch array (8 bytes per row,
  * 512 KiB, held on every GPU that loads the library until the process exits). */
 #define VG_NOALLOC_MAX_ROWS 65536

@@ -52,7 +52,7 @@ EXPORTS = ["vg_create", "vg_destroy", "vg_model_nvar", "vg_upload_primitive", "v
            "vg_last_error_string", "vg_status_string", "vg_max_wave_speed_noalloc", "vg_autotune",
            "vg_set_launch_config", "vg_get_launch_config", "vg_batch_create", "vg_batch_destroy",
            "vg_batch_total_cells", "vg_batch_upload", "vg_batch_download", "vg_batch_run",
-           "vg_batch_last_launch_count"]
+           "vg_batch_last_launch_count", "vg_batch_gradient"]
 NUM_XCFG, NUM_YCFG = 5, 6
 
 NOALLOC_MAX_ROWS = 65536
@@ -106,6 +106,9 @@ def lib():
         L.vg_batch_run.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_int, D, vp]
         L.vg_batch_last_launch_count.argtypes = [vp]
         L.vg_batch_last_launch_count.restype = ctypes.c_long
+        Lp = ctypes.POINTER(ctypes.c_long)
+        L.vg_batch_gradient.argtypes = [vp, D, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                        ctypes.c_int, D, D, D, Lp, Lp, vp]
         L.vg_last_error_string.restype = ctypes.c_char_p
         L.vg_status_string.restype = ctypes.c_char_p
         L.vg_status_string.argtypes = [ctypes.c_int]
@@ -281,3 +284,21 @@ class Batch:
 
     def last_launch_count(self):
         return lib().vg_batch_last_launch_count(self._h)
+
+    def gradient(self, target_rho, cfl, steps, bias=0.0, limiter=SUPERBEE, checkpoints=None, stream=None):
+        """Discrete adjoint of run(cfl, steps) from the current state for L = sum (rho(T) - target_rho)^2.
+        Returns (L, dL/dW0 as (6, total) planes, dL/dgamma (ninst,), forward steps, reversed steps).
+        checkpoints defaults to every state (no recomputation)."""
+        t = np.ascontiguousarray(target_rho, dtype=np.float64)
+        if t.shape != (self.total,):
+            raise ValueError(f"target_rho must have shape ({self.total},)")
+        D = ctypes.POINTER(ctypes.c_double)
+        L = ctypes.c_double()
+        g = np.empty((6, self.total))
+        gg = np.empty(self.ninst)
+        fw, aw = ctypes.c_long(), ctypes.c_long()
+        _check(lib().vg_batch_gradient(self._h, t.ctypes.data_as(D), cfl, steps, bias, limiter,
+                                       steps if checkpoints is None else checkpoints, ctypes.byref(L),
+                                       g.ctypes.data_as(D), gg.ctypes.data_as(D), ctypes.byref(fw), ctypes.byref(aw),
+                                       stream))
+        return L.value, g, gg, fw.value, aw.value

@@ -28,6 +28,7 @@ UNITS = [
     ("vg_api.cu", []),
     ("vg_noalloc.cu", ["-fmad=false"]),
     ("batch.cu", ["-fmad=false"]),
+    ("adjoint.cu", ["-fmad=false"]),
 ]
 
 

@@ -2,7 +2,7 @@
 //
 // Instances k = 0..K-1 have n_k cells (any sizes), their own gamma / p_inf and cell width dx_k, and are
 // concatenated into structure-of-arrays planes (rho, u, p) with a cell-offset table.  The work is cut into
-// tiles of P - 2 consecutive cells of one instance; a persistent grid strides over the tile table, so no block
+// tiles of BP - 2 consecutive cells of one instance; a persistent grid strides over the tile table, so no block
 // straddles two instances and the transmissive ghosts of each instance are synthesised by the loader exactly as
 // Solvers::insertBoundaryCells builds them (Solvers/solvers.cpp:7-32).  Every instance takes its own time step
 // dt_k = CFL * dx_k / S_k (x0.2 for the first six steps, Solvers/solvers.cpp:437-452) from its own maximum wave
@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "../../include/vanguard_slic.h"
+#include "batch_internal.cuh"
 #include "physics_fp64.cuh"
 #include "slic_kernels.cuh"
 #include "vg_ops.h"
@@ -28,33 +29,6 @@ namespace vg {
 namespace {
 
 using M1 = EulerF64<1>;
-constexpr int BP = 128;  // cells per tile segment (BP - 2 outputs)
-
-struct Tile {
-    int inst;   // instance
-    int s0;     // first output cell within the instance
-};
-
-struct BatchArgs {
-    const double* in;
-    double* out;
-    long plane;                 // plane stride (total cells)
-    const long* offset;         // first cell of each instance
-    const int* ncell;           // cells of each instance
-    const double* dx;           // cell width of each instance
-    const double* gam;          // gamma, p_inf of each instance (2 per instance)
-    const Tile* tiles;
-    int ntiles;
-    int ninst;
-    unsigned long long* smax;   // 3 x ninst ring of wave-speed maxima (bit patterns)
-    double* dt_out;             // dt of the current step per instance (diagnostics / adjoint)
-    int* step;                  // device step counter
-    unsigned int* done;         // blocks finished in this step
-    unsigned int* err;
-    double cfl, bias, floor5;
-    int limiter;
-    int max_steps;
-};
 
 __device__ __forceinline__ double instance_dt(const BatchArgs& a, int k, int s) {
     double S = __longlong_as_double((long long)a.smax[(s % 3) * a.ninst + k]);
@@ -167,8 +141,13 @@ __global__ void __launch_bounds__(BP) batch_step_kernel(BatchArgs a) {
     }
 }
 
-// Initial maxima: slot 0 <- max over each instance (grid-stride over cells; instance by binary search).
+// Initial maxima: slot a.wave_slot <- max over each instance (grid-stride over cells; instance by binary search).
+// Also resets the step counter to a.step_init and the finished-block counter.
 __global__ void __launch_bounds__(256) batch_max_wave_kernel(BatchArgs a) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *a.step = a.step_init;
+        *a.done = 0u;
+    }
     for (long i = blockIdx.x * 256L + threadIdx.x; i < a.plane; i += (long)gridDim.x * 256) {
         int lo = 0, hi = a.ninst - 1;
         while (lo < hi) {
@@ -180,61 +159,14 @@ __global__ void __launch_bounds__(256) batch_max_wave_kernel(BatchArgs a) {
         for (int v = 0; v < M1::NW; v++) W[v] = a.in[v * a.plane + i];
         M1::P q{a.gam[2 * lo], a.gam[2 * lo + 1], 0.0};
         double sw = M1::wave(W, q, 1);
-        if (sw > 0.0) atomic_max_nonneg(&a.smax[lo], sw);
+        if (sw > 0.0) atomic_max_nonneg(&a.smax[a.wave_slot * a.ninst + lo], sw);
     }
 }
 
-}  // namespace
-}  // namespace vg
-
-using vg::BatchArgs;
-using vg::Tile;
-
-struct vg_batch {
-    int ninst = 0, device = 0;
-    long total = 0;
-    std::vector<int> ncell;
-    std::vector<long> offset;
-    double* buf[2] = {nullptr, nullptr};
-    long* d_offset = nullptr;
-    int* d_ncell = nullptr;
-    double* d_dx = nullptr;
-    double* d_gam = nullptr;
-    Tile* d_tiles = nullptr;
-    int ntiles = 0;
-    unsigned long long* d_smax = nullptr;
-    double* d_dt = nullptr;
-    int* d_step = nullptr;
-    unsigned int* d_done = nullptr;
-    unsigned int* d_err = nullptr;
-    int cur = 0;
-    int grid = 0;
-    cudaStream_t cap = nullptr;
-    cudaGraphExec_t graph = nullptr;
-    int graph_steps = 0, graph_from = -1;
-    double graph_cfl = 0, graph_bias = 0;
-    int graph_limiter = -1, graph_max = -1;
-    long last_launches = 0;
-};
-
-namespace {
-
-vg_status bfail(vg_status st, const std::string& m) {
-    vg::set_last_error(m);
-    return st;
-}
-
-#define VB_CUDA(call)                                                                               \
-    do {                                                                                            \
-        cudaError_t e_ = (call);                                                                    \
-        if (e_ != cudaSuccess) return bfail(e_ == cudaErrorMemoryAllocation ? VG_ENOMEM : VG_ECUDA,  \
-                                            std::string(#call) + ": " + cudaGetErrorString(e_));    \
-    } while (0)
-
-BatchArgs batch_args(vg_batch* b, int from, double cfl, double bias, int limiter, int max_steps) {
+BatchArgs batch_args(vg_batch* b, const double* in, double* out, double cfl, double bias, int limiter, int max_steps) {
     BatchArgs a{};
-    a.in = b->buf[from];
-    a.out = b->buf[1 - from];
+    a.in = in;
+    a.out = out;
     a.plane = b->total;
     a.offset = b->d_offset;
     a.ncell = b->d_ncell;
@@ -253,8 +185,60 @@ BatchArgs batch_args(vg_batch* b, int from, double cfl, double bias, int limiter
     a.floor5 = std::pow(10.0, -5.0);
     a.limiter = limiter;
     a.max_steps = max_steps;
+    a.wave_slot = 0;
     return a;
 }
+
+cudaError_t start_steps(vg_batch* b, const double* state, int s_start, double cfl, double bias, int limiter, int max_steps,
+                        cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(b->d_smax, 0, sizeof(unsigned long long) * 3 * b->ninst, st);
+    if (e != cudaSuccess) return e;
+    BatchArgs a0 = batch_args(b, state, nullptr, cfl, bias, limiter, max_steps);
+    a0.wave_slot = s_start % 3;
+    a0.step_init = s_start;
+    int mw = (int)std::min<long>((b->total + 255) / 256, 148L * 8);
+    batch_max_wave_kernel<<<mw, 256, 0, st>>>(a0);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t batch_advance(vg_batch* b, const double* src, double* dst, int s_start, int nsteps, double cfl, double bias,
+                          int limiter, cudaStream_t st) {
+    const size_t bytes = sizeof(double) * 3 * b->total;
+    cudaError_t e = cudaSuccess;
+    if (nsteps <= 0) return src == dst ? cudaSuccess : cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, st);
+    if (src != b->buf[0]) e = cudaMemcpyAsync(b->buf[0], src, bytes, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = start_steps(b, b->buf[0], s_start, cfl, bias, limiter, s_start + nsteps, st);
+    for (int i = 0; i < nsteps && e == cudaSuccess; i++) {
+        BatchArgs a = batch_args(b, b->buf[i & 1], b->buf[1 - (i & 1)], cfl, bias, limiter, s_start + nsteps);
+        batch_step_kernel<<<b->grid, BP, 0, st>>>(a);
+        e = cudaGetLastError();
+    }
+    b->last_forward_steps += nsteps;
+    double* res = b->buf[nsteps & 1];
+    if (e == cudaSuccess && dst != res) e = cudaMemcpyAsync(dst, res, bytes, cudaMemcpyDeviceToDevice, st);
+    return e;
+}
+
+}  // namespace vg
+
+using vg::BatchArgs;
+using vg::Tile;
+
+namespace {
+
+vg_status bfail(vg_status st, const std::string& m) {
+    vg::set_last_error(m);
+    return st;
+}
+
+#define VB_CUDA(call)                                                                               \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess) return bfail(e_ == cudaErrorMemoryAllocation ? VG_ENOMEM : VG_ECUDA,  \
+                                            std::string(#call) + ": " + cudaGetErrorString(e_));    \
+    } while (0)
 
 }  // namespace
 
@@ -279,7 +263,7 @@ vg_status vg_batch_create(int ninst, const int* ncell, const double* dx, const d
         b->offset[k] = total;
         total += ncell[k];
     }
-    // tiles in decreasing instance size so the persistent grid ends on short work (longest-first balance)
+    // tiles in decreasing instance size so the persistent grid ends on short work (longest first)
     std::vector<int> order(ninst);
     for (int k = 0; k < ninst; k++) order[k] = k;
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return ncell[x] > ncell[y]; });
@@ -313,6 +297,7 @@ vg_status vg_batch_create(int ninst, const int* ncell, const double* dx, const d
     if (e == cudaSuccess) e = cudaMemcpy(b->d_dx, dx, sizeof(double) * ninst, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(b->d_gam, gam.data(), sizeof(double) * 2 * ninst, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(b->d_tiles, tiles.data(), sizeof(Tile) * tiles.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(b->d_err, 0, sizeof(unsigned int));
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
         vg_batch_destroy(b);
@@ -327,8 +312,12 @@ vg_status vg_batch_destroy(vg_batch* b) {
     if (b->graph) cudaGraphExecDestroy(b->graph);
     for (auto p : b->buf)
         if (p) cudaFree(p);
+    for (auto p : b->lam)
+        if (p) cudaFree(p);
     for (void* p : {(void*)b->d_offset, (void*)b->d_ncell, (void*)b->d_dx, (void*)b->d_gam, (void*)b->d_tiles,
-                    (void*)b->d_smax, (void*)b->d_dt, (void*)b->d_step, (void*)b->d_done, (void*)b->d_err})
+                    (void*)b->d_smax, (void*)b->d_dt, (void*)b->d_step, (void*)b->d_done, (void*)b->d_err, (void*)b->ckpt,
+                    (void*)b->d_target, (void*)b->d_atiles, (void*)b->d_tile_part, (void*)b->d_tile_first,
+                    (void*)b->d_tile_count, (void*)b->d_ggam, (void*)b->d_stepdt, (void*)b->d_arg, (void*)b->d_loss})
         if (p) cudaFree(p);
     if (b->cap) cudaStreamDestroy(b->cap);
     delete b;
@@ -388,14 +377,8 @@ vg_status vg_batch_run(vg_batch* b, double cfl, int steps, double bias, int limi
         VB_CUDA(cudaMemcpyAsync(b->buf[0], b->buf[1], sizeof(double) * 3 * b->total, cudaMemcpyDeviceToDevice, st));
         b->cur = 0;
     }
-    VB_CUDA(cudaMemsetAsync(b->d_smax, 0, sizeof(unsigned long long) * 3 * b->ninst, st));
-    VB_CUDA(cudaMemsetAsync(b->d_step, 0, sizeof(int), st));
-    VB_CUDA(cudaMemsetAsync(b->d_done, 0, sizeof(unsigned int), st));
     VB_CUDA(cudaMemsetAsync(b->d_err, 0, sizeof(unsigned int), st));
-    BatchArgs a0 = batch_args(b, 0, cfl, bias, limiter, steps);
-    int mw = (int)std::min<long>((b->total + 255) / 256, 148L * 8);
-    vg::batch_max_wave_kernel<<<mw, 256, 0, st>>>(a0);
-    VB_CUDA(cudaGetLastError());
+    VB_CUDA(vg::start_steps(b, b->buf[0], 0, cfl, bias, limiter, steps, st));
     // one graph per (steps, cfl, bias, limiter): the whole time loop, one persistent kernel per step
     if (!b->graph || b->graph_steps != steps || b->graph_cfl != cfl || b->graph_bias != bias || b->graph_limiter != limiter) {
         if (b->graph) cudaGraphExecDestroy(b->graph);
@@ -403,7 +386,7 @@ vg_status vg_batch_run(vg_batch* b, double cfl, int steps, double bias, int limi
         cudaGraph_t g = nullptr;
         VB_CUDA(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal));
         for (int i = 0; i < steps; i++) {
-            BatchArgs a = batch_args(b, i & 1, cfl, bias, limiter, steps);
+            BatchArgs a = vg::batch_args(b, b->buf[i & 1], b->buf[1 - (i & 1)], cfl, bias, limiter, steps);
             vg::batch_step_kernel<<<b->grid, vg::BP, 0, b->cap>>>(a);
         }
         cudaError_t e1 = cudaGetLastError();
