@@ -4,26 +4,29 @@
 // Loss  L = sum_k sum_i (rho_k,i(T) - target_k,i)^2  after `steps` steps of every instance's own solve() loop.
 // Output dL/dW^0 (primitive planes rho, u, p of every cell) and dL/dgamma_k.
 //
-// One reverse step s maps lambda^{s+1} = dL/dW^{s+1} to lambda^s through the exact-FP64 forward step of
-// batch.cu, recomputed from W^s with the same device functions (so the limiter takes the same branches):
+// One reverse step s maps lambda^{s+1} = dL/dW^{s+1} to lambda^s through the forward step of batch.cu:
 //   W^{s+1}_i = setcons(U_i + r (F_{i-1/2} - F_{i+1/2})),  U_i = cons(W^s_i),  r = dt / dx,
 //   F_{j+1/2} = FORCE(evolve_R(W_{j-1}, W_j, W_{j+1}), evolve_L(W_j, W_{j+1}, W_{j+2})),
 //   dt = CFL dx / S (x0.2 for s <= 5),  S = max_i (|u_i| + c_i).
-// Vector-Jacobian products are written by hand for cons / setcons / the x flux (exact identities of the ideal
-// stiffened gas, the primitive round trips of the reference are identities), the slope limiter, the half-step
-// evolution, the Lax-Friedrichs / Richtmyer / FORCE combination and the update.  Subgradients:
-//   * limiter: the derivative of the branch the forward pass took (one-sided at r = 0, 1/2, 1 and where the
-//     minimum switches between r, xi_R and 2), computed with the forward's own comparisons;
+// Vector-Jacobian products are written by hand for cons / setcons / the x flux (the primitive round trips of the
+// reference are identities and drop out), the slope limiter, the half-step evolution, the Lax-Friedrichs /
+// Richtmyer / FORCE combination and the update.  Subgradients:
+//   * limiter: the derivative of the branch the forward step took (one-sided at r = 0, 1/2, 1 and where the
+//     minimum switches between r, xi_R and 2), decided by the forward's own comparisons on bit-equal operands;
 //   * the |delta| < 1e-5 floor: zero derivative of the floored ratio operand;
 //   * the CFL maximum: only the first cell attaining the maximum receives dS; |u| has derivative sign(u), 0 at 0.
-// The dt dependence is propagated (dt -> S -> that cell's state and gamma), so the gradient is that of the
-// scheme that adapts its step, which is what central finite differences measure.
+// The dt dependence is propagated (dt -> S -> that cell's state and gamma), so the result is the gradient of the
+// scheme that adapts its step, which is what central finite differences measure where the loss is smooth.
 //
-// Tiles: AP = 128 positions per block, AH = 5 halo cells each side, AP - 2 AH outputs.  Every contribution to r-bar
-// and gamma-bar is owned by exactly one tile (interfaces by their right cell, or the last cell at the right end;
-// ghost-cell edges by the instance's end cells), so the per-instance sums are deterministic.  Ghost cells
+// Arithmetic: the values that select a branch (cons, the slope ratio and xi_R, the wave speed) are recomputed
+// with uncontracted IEEE operations (__dmul_rn & co.) exactly as the forward step forms them, so every branch
+// matches it; everything else (edge states, fluxes, the derivative formulas) uses reciprocals refined to full
+// double precision and FMA contraction, which moves the gradient by round-off only.
+//
+// Tiles: AP = 128 positions per block, AH = 5 halo cells each side, AP - 2 AH outputs.  Every contribution to
+// r-bar and gamma-bar is owned by exactly one tile (interfaces by their right cell, or the last cell at the right
+// end; ghost-cell edges by the instance's end cells), so the per-instance sums are deterministic.  Ghost cells
 // (transmissive mirror copies, Solvers/solvers.cpp:17-23) fold their adjoints into the cells they copy.
-// Compiled with -fmad=false so the recomputed forward matches the stored one bit for bit.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -33,145 +36,130 @@
 
 #include "../../include/vanguard_slic.h"
 #include "batch_internal.cuh"
-#include "physics_fp64.cuh"
-#include "slic_kernels.cuh"
+#include "physics_mixed.cuh"
 #include "vg_ops.h"
 
 namespace vg {
 namespace {
 
-using M1 = EulerF64<1>;
 constexpr int AP = 128;
 constexpr int AH = 5;
 constexpr int AOUT = AP - 2 * AH;
 
-struct Q1 {
-    double g, pinf;
+__device__ __forceinline__ double xmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double xadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double xsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double xdiv(double a, double b) { return __ddiv_rn(a, b); }
+
+struct Gas {
+    double g, pinf, gm1, igm1, gpinf;
 };
 
-// ---------------------------------------------------------------------------- vector-Jacobian products
-// U = (rho, rho u, rho u^2 / 2 + (p + g pinf) / (g - 1))
-__device__ __forceinline__ void cons_vjp(const double* W, const Q1& q, const double* Ub, double* Wb, double& gb) {
-    double rho = W[0], u = W[1], p = W[2], gm1 = q.g - 1.0;
-    Wb[0] += Ub[0] + u * Ub[1] + 0.5 * u * u * Ub[2];
-    Wb[1] += rho * Ub[1] + rho * u * Ub[2];
-    Wb[2] += Ub[2] / gm1;
-    gb += (-(p + q.pinf) / (gm1 * gm1)) * Ub[2];
+// EulerStateVector::computeConservedVariableVector (Euler/eulerstatevector.cpp:78-91), operation for operation
+__device__ __forceinline__ void cons_exact(const double* W, const Gas& q, double* U) {
+    const double rho = W[0], u = W[1], p = W[2];
+    const double e = xdiv(xadd(p, xmul(q.g, q.pinf)), xmul(xsub(q.g, 1.0), rho));
+    U[0] = rho;
+    U[1] = xmul(rho, u);
+    U[2] = xmul(rho, xadd(xmul(0.5, xmul(u, u)), e));
 }
-// p = (g - 1)(U2 - U1 u / 2) - g pinf with u = U1 / U0
-__device__ __forceinline__ void pressure_vjp(const double* U, const Q1& q, double u, double pb, double* Ub, double& gb) {
-    double gm1 = q.g - 1.0;
-    Ub[0] += gm1 * 0.5 * u * u * pb;
-    Ub[1] += -gm1 * u * pb;
-    Ub[2] += gm1 * pb;
-    gb += ((U[2] - 0.5 * U[1] * u) - q.pinf) * pb;
-}
-__device__ __forceinline__ void setcons_vjp(const double* U, const Q1& q, const double* Wb, double* Ub, double& gb) {
-    double rho = U[0], u = U[1] / rho;
-    Ub[0] += Wb[0] - (u / rho) * Wb[1];
-    Ub[1] += Wb[1] / rho;
-    pressure_vjp(U, q, u, Wb[2], Ub, gb);
-}
-// F = (U1, U1 u + p, u (U2 + p))
-__device__ __forceinline__ void flux_vjp(const double* U, const Q1& q, const double* Fb, double* Ub, double& gb) {
-    double rho = U[0], u = U[1] / rho;
-    double p = (q.g - 1.0) * (U[2] - 0.5 * U[1] * u) - q.g * q.pinf;
-    double ub = U[1] * Fb[1] + (U[2] + p) * Fb[2];
-    double pb = Fb[1] + u * Fb[2];
-    Ub[1] += Fb[0] + u * Fb[1];
-    Ub[2] += u * Fb[2];
-    Ub[0] += -(u / rho) * ub;
-    Ub[1] += ub / rho;
-    pressure_vjp(U, q, u, pb, Ub, gb);
-}
-// d xi / d r of the branch SlopeLimiters::computeSlopeLimiter takes (Solvers/slopelimiters.cpp:7-74), with the
-// forward's own comparisons and std::min tie rule
-__device__ __forceinline__ double limiter_deriv(double r, double w, int id) {
-    double den = (1.0 - w) + ((1.0 + w) * r);
-    double xr = 2.0 / den, dxr = -2.0 * (1.0 + w) / (den * den);
-    if (id == 0) {
-        if (r < 0.0) return 0.0;
-        if (r < 0.5) return 2.0;
-        if (r < 1.0) return 0.0;
-        double m1 = (xr < r) ? xr : r, dm1 = (xr < r) ? dxr : 1.0;
-        return (2.0 < m1) ? 0.0 : dm1;
-    } else if (id == 1) {
-        if (r < 0.0) return 0.0;
-        double a = (2.0 * r) / (1.0 + r);
-        return (xr < a) ? dxr : 2.0 / ((1.0 + r) * (1.0 + r));
-    }
-    if (r < 0.0) return 0.0;
-    if (r < 1.0) return 1.0;
-    return (xr < 1.0) ? dxr : 0.0;
-}
-__device__ __forceinline__ void slope_vjp(double uL, double u, double uR, const SweepConst& k, double sb, double& uLb,
-                                          double& ub, double& uRb) {
-    double dm = u - uL, dp = uR - u;
-    double base = (k.cm * dm) + (k.cp * dp);
-    bool nf = fabs(dm) < k.floor5, df = fabs(dp) < k.floor5;
-    double num = nf ? k.floor5 : dm, den = df ? k.floor5 : dp;
-    double r = num / den;
-    double xi = limiter_f64(r, k.bias, k.limiter), dxi = limiter_deriv(r, k.bias, k.limiter);
-    double dmb = sb * (k.cm * xi) + (nf ? 0.0 : sb * base * dxi / den);
-    double dpb = sb * (k.cp * xi) + (df ? 0.0 : -sb * base * dxi * num / (den * den));
-    uLb -= dmb;
-    ub += dmb - dpb;
-    uRb += dpb;
-}
-// adjoint of evolve_edges for one cell: ab / bb adjoints of its left-side / right-side evolved states
-__device__ void evolve_vjp(const double* uL, const double* u, const double* uR, const SweepConst& k, const Q1& q1,
-                           const M1::P& q, const double* ab, const double* bb, double* uLb, double* ub, double* uRb,
-                           double& halfrb, double& gb) {
-    double xl[3], xr[3], fl[3], fr[3];
-    for (int i = 0; i < 3; i++) {
-        double s = slope_f64(uL[i], u[i], uR[i], k);
-        xl[i] = u[i] - (0.5 * s);
-        xr[i] = u[i] + (0.5 * s);
-    }
-    M1::flux<0>(xl, q, fl);
-    M1::flux<0>(xr, q, fr);
-    double xlb[3], xrb[3], flb[3], frb[3];
-    for (int i = 0; i < 3; i++) {
-        double evb = ab[i] + bb[i];
-        xlb[i] = ab[i];
-        xrb[i] = bb[i];
-        flb[i] = k.half_r * evb;
-        frb[i] = -k.half_r * evb;
-        halfrb += evb * (fl[i] - fr[i]);
-    }
-    flux_vjp(xl, q1, flb, xlb, gb);
-    flux_vjp(xr, q1, frb, xrb, gb);
-    for (int i = 0; i < 3; i++) {
-        ub[i] += xlb[i] + xrb[i];
-        slope_vjp(uL[i], u[i], uR[i], k, 0.5 * (xrb[i] - xlb[i]), uLb[i], ub[i], uRb[i]);
-    }
-}
-// adjoint of force_flux(ua, ub)
-__device__ void force_vjp(const double* ua, const double* ubv, const SweepConst& k, const Q1& q1, const M1::P& q,
-                          const double* Fb, double* uab, double* ubb, double& rb, double& rinvb, double& gb) {
-    double fa[3], fb[3], uri[3];
-    M1::flux<0>(ua, q, fa);
-    M1::flux<0>(ubv, q, fb);
-    for (int i = 0; i < 3; i++) uri[i] = 0.5 * ((ua[i] + ubv[i]) + (k.r * (fa[i] - fb[i])));
-    double urib[3] = {0.0, 0.0, 0.0}, frib[3], lfb[3], fab[3], fbb[3];
-    for (int i = 0; i < 3; i++) {
-        lfb[i] = 0.5 * Fb[i];
-        frib[i] = 0.5 * Fb[i];
-    }
-    flux_vjp(uri, q1, frib, urib, gb);
-    for (int i = 0; i < 3; i++) {
-        fab[i] = 0.5 * lfb[i] + 0.5 * k.r * urib[i];
-        fbb[i] = 0.5 * lfb[i] - 0.5 * k.r * urib[i];
-        uab[i] += 0.5 * k.rinv * lfb[i] + 0.5 * urib[i];
-        ubb[i] += -0.5 * k.rinv * lfb[i] + 0.5 * urib[i];
-        rb += 0.5 * urib[i] * (fa[i] - fb[i]);
-        rinvb += 0.5 * lfb[i] * (ua[i] - ubv[i]);
-    }
-    flux_vjp(ua, q1, fab, uab, gb);
-    flux_vjp(ubv, q1, fbb, ubb, gb);
+// |u| + c of Solvers::computeMaximumWaveSpeed (Solvers/solvers.cpp:259-276), operation for operation
+__device__ __forceinline__ double wave_exact(double rho, double u, double p, double g, double pinf) {
+    return xadd(fabs(u), __dsqrt_rn(xdiv(xmul(g, xadd(p, pinf)), rho)));
 }
 
-// ------------------------------------------------------------------------------------------------ kernels
+// xi(r) of SlopeLimiters::computeSlopeLimiter (Solvers/slopelimiters.cpp:7-74) with the derivative of the branch
+// taken; the comparisons see the forward's operands bit for bit (std::min(a, b) = b < a ? b : a).
+__device__ __forceinline__ void limiter_d(double r, double w, int id, double& xi, double& dxi) {
+    const double xr = xdiv(2.0, xadd(1.0 - w, xmul(1.0 + w, r)));
+    const double dxr = -0.5 * (1.0 + w) * xr * xr;  // d(2 / den)/dr = -2 (1 + w) / den^2
+    xi = 0.0;
+    dxi = 0.0;
+    if (r < 0.0) return;
+    if (id == 0) {
+        if (r < 0.5) {
+            xi = xmul(2.0, r);
+            dxi = 2.0;
+        } else if (r < 1.0) {
+            xi = 1.0;
+        } else {
+            const bool t = xr < r;
+            const double m1 = t ? xr : r;
+            if (!(2.0 < m1)) {
+                xi = m1;
+                dxi = t ? dxr : 1.0;
+            } else {
+                xi = 2.0;
+            }
+        }
+    } else if (id == 1) {
+        const double a = xdiv(xmul(2.0, r), xadd(1.0, r));
+        if (xr < a) {
+            xi = xr;
+            dxi = dxr;
+        } else {
+            const double ip = rcp_nr2(1.0 + r);
+            xi = a;
+            dxi = 2.0 * ip * ip;
+        }
+    } else {
+        if (r < 1.0) {
+            xi = r;
+            dxi = 1.0;
+        } else if (xr < 1.0) {
+            xi = xr;
+            dxi = dxr;
+        } else {
+            xi = 1.0;
+        }
+    }
+}
+
+struct K {
+    double r, rinv, half_r, cm, cp, bias, floor5;
+    int limiter;
+};
+
+// One slope component (SlopeLimiters::computeSlopeVector, Solvers/slopelimiters.cpp:217-246) and its partial
+// derivatives with respect to delta- = u - uL and delta+ = uR - u.
+__device__ __forceinline__ double slope_d(double uL, double u, double uR, const K& k, double& sdm, double& sdp) {
+    const double dm = u - uL, dp = uR - u;
+    const bool nf = fabs(dm) < k.floor5, df = fabs(dp) < k.floor5;
+    const double num = nf ? k.floor5 : dm, den = df ? k.floor5 : dp;
+    const double r = xdiv(num, den);
+    double xi, dxi;
+    limiter_d(r, k.bias, k.limiter, xi, dxi);
+    const double base = k.cm * dm + k.cp * dp;
+    const double t = base * dxi * rcp_nr2(den);  // base * dxi * dr/dnum
+    sdm = k.cm * xi + (nf ? 0.0 : t);
+    sdp = k.cp * xi - (df ? 0.0 : t * r);  // dr/dden = -r / den
+    return base * xi;
+}
+
+// x flux of a conserved state with 1/rho kept for the vector-Jacobian product
+__device__ __forceinline__ void flux_a(const double* U, const Gas& q, double* F, double& ir) {
+    ir = rcp_nr2(U[0]);
+    const double u = U[1] * ir;
+    const double p = q.gm1 * (U[2] - 0.5 * U[1] * u) - q.gpinf;
+    F[0] = U[1];
+    F[1] = U[1] * u + p;
+    F[2] = u * (U[2] + p);
+}
+// Ub += (dF/dU)^T Fb, gb += (dF/dgamma) . Fb, for F = (m, m u + p, u (E + p)), u = m / rho,
+// p = (gamma - 1)(E - m u / 2) - gamma p_inf
+__device__ __forceinline__ void flux_vjp(const double* U, double ir, const Gas& q, const double* Fb, double* Ub,
+                                         double& gb) {
+    const double u = U[1] * ir;
+    const double X = U[2] - 0.5 * U[1] * u;
+    const double p = q.gm1 * X - q.gpinf;
+    const double ub = U[1] * Fb[1] + (U[2] + p) * Fb[2];
+    const double pb = Fb[1] + u * Fb[2];
+    Ub[0] += q.gm1 * 0.5 * u * u * pb - u * ir * ub;
+    Ub[1] += Fb[0] + u * Fb[1] + ir * ub - q.gm1 * u * pb;
+    Ub[2] += u * Fb[2] + q.gm1 * pb;
+    gb += (X - q.pinf) * pb;
+}
+
 struct AdjArgs {
     const double* W;        // state W^s (rho, u, p planes)
     const double* lam_in;   // dL/dW^{s+1}
@@ -183,16 +171,33 @@ struct AdjArgs {
     const double* gam;
     const Tile* tiles;      // adjoint tiles: AOUT outputs each
     int ntiles;
-    const double* dts;      // dt and S of step s, 2 per instance
+    const unsigned long long* S;  // max |u| + c of W^s per instance (double bit patterns)
+    int* arg;               // first cell attaining S per instance (atomicMin; reset by the dt adjoint kernel)
     double* tile_part;      // per tile: r-bar (dL/dr) and gamma-bar
-    double bias, floor5;
+    double cfl, bias, floor5;
     int limiter;
+    int step;               // s
 };
 
-__global__ void __launch_bounds__(AP) adjoint_step_kernel(AdjArgs a) {
-    __shared__ double Us[3][AP], Ea[3][AP], Eb[3][AP], Fs[3][AP + 1], MU[3][AP], AB[3][AP], BB[3][AP], UL[3][AP],
-        US[3][AP], UR[3][AP];
+// dt of step s from S, operation for operation as the forward step forms it (Solvers/solvers.cpp:437-452)
+__device__ __forceinline__ double step_dt(double cfl, double dx, double S, int s) {
+    double d = xmul(cfl, xdiv(dx, S));
+    if (s <= 5) d = xmul(d, 0.2);
+    return d;
+}
+
+__global__ void __launch_bounds__(AP, 4) adjoint_step_kernel(AdjArgs a) {
+    // stage-aliased shared arrays: Us -> UL, Ea -> AB, Eb -> BB, Fs -> US
+    __shared__ double S0[3][AP], S1[3][AP], S2[3][AP], S3[3][AP], MU[3][AP], UR[3][AP];
     __shared__ double red[2][AP / 32];
+    auto& Us = S0;
+    auto& UL = S0;
+    auto& Ea = S1;
+    auto& AB = S1;
+    auto& Eb = S2;
+    auto& BB = S2;
+    auto& Fs = S3;
+    auto& US = S3;
     const int p = threadIdx.x;
     for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
         const Tile tile = a.tiles[t];
@@ -201,117 +206,173 @@ __global__ void __launch_bounds__(AP) adjoint_step_kernel(AdjArgs a) {
         const int c = s0 - AH + p;  // cell of this position (may be a ghost or beyond)
         const bool real = c >= 0 && c < n;
         const bool out = p >= AH && p < AP - AH && real;
-        const bool owns_first = s0 == 0;                       // tile owning cell 0
+        const bool owns_first = s0 == 0;                          // tile owning cell 0
         const bool owns_last = s0 <= n - 1 && n - 1 < s0 + AOUT;  // tile owning cell n-1
-        const double dt = a.dts[2 * k], dxk = a.dx[k];
-        SweepConst kc;
-        kc.r = dt / dxk;
+        const double dxk = a.dx[k];
+        const double Sk = __longlong_as_double((long long)a.S[k]);
+        const double dt = step_dt(a.cfl, dxk, Sk, a.step);
+        K kc;
+        kc.r = xdiv(dt, dxk);
         kc.rinv = dxk / dt;
-        kc.half_r = 0.5 * (dt / dxk);
+        kc.half_r = 0.5 * kc.r;
         kc.cm = 0.5 * (1.0 + a.bias);
         kc.cp = 0.5 * (1.0 - a.bias);
         kc.bias = a.bias;
         kc.floor5 = a.floor5;
         kc.limiter = a.limiter;
-        const M1::P q{a.gam[2 * k], a.gam[2 * k + 1], 0.0};
-        const Q1 q1{a.gam[2 * k], a.gam[2 * k + 1]};
-        double W[3];
+        Gas q;
+        q.g = a.gam[2 * k];
+        q.pinf = a.gam[2 * k + 1];
+        q.gm1 = q.g - 1.0;
+        q.igm1 = 1.0 / q.gm1;
+        q.gpinf = q.g * q.pinf;
+        // stage A: conserved vectors of every position (ghosts by the transmissive mirror); the adjoint input of
+        // the cells reverse 1 needs is loaded here so its latency hides behind stages B and C
+        double W[3], lam[3] = {0.0, 0.0, 0.0};
+        const bool upd = p >= 2 && p < AP - 2 && real;
         {
             const int gi = ghost_index(c, n, 0);
             for (int v = 0; v < 3; v++) W[v] = a.W[v * a.plane + base + gi];
+            if (upd)
+                for (int v = 0; v < 3; v++) lam[v] = a.lam_in[v * a.plane + base + c];
             double U[3];
-            M1::cons(W, q, U);
-            for (int v = 0; v < 3; v++) {
-                Us[v][p] = U[v];
-                MU[v][p] = AB[v][p] = BB[v][p] = UL[v][p] = US[v][p] = UR[v][p] = 0.0;
-            }
+            cons_exact(W, q, U);
+            for (int v = 0; v < 3; v++) Us[v][p] = U[v];
+        }
+        // first cell of the instance attaining S (the CFL maximum's argmax)
+        {
+            const unsigned hit = (out && wave_exact(W[0], W[1], W[2], q.g, q.pinf) == Sk) ? (unsigned)c : 0xffffffffu;
+            const unsigned m = __reduce_min_sync(0xffffffffu, hit);
+            if ((p & 31) == 0 && m != 0xffffffffu) atomicMin(&a.arg[k], (int)m);
         }
         __syncthreads();
-        // forward: evolved edge states of positions [1, AP-1)
+        // stage B: slopes (with their derivatives) and the evolved edge states of positions [1, AP-1)
+        double xl[3], xr[3], dF[3], sdm[3], sdp[3], irl = 1.0, irr = 1.0;
         if (p >= 1 && p < AP - 1) {
-            double uL[3], u[3], uR[3], ea[3], eb[3];
             for (int v = 0; v < 3; v++) {
-                uL[v] = Us[v][p - 1];
-                u[v] = Us[v][p];
-                uR[v] = Us[v][p + 1];
+                const double u = Us[v][p];
+                const double s = slope_d(Us[v][p - 1], u, Us[v][p + 1], kc, sdm[v], sdp[v]);
+                xl[v] = u - 0.5 * s;
+                xr[v] = u + 0.5 * s;
             }
-            evolve_edges<M1, 0>(uL, u, uR, kc, q, ea, eb, true, true);
+            double fl[3], fr[3];
+            flux_a(xl, q, fl, irl);
+            flux_a(xr, q, fr, irr);
             for (int v = 0; v < 3; v++) {
-                Ea[v][p] = ea[v];
-                Eb[v][p] = eb[v];
+                dF[v] = fl[v] - fr[v];
+                const double ev = kc.half_r * dF[v];
+                Ea[v][p] = xl[v] + ev;
+                Eb[v][p] = xr[v] + ev;
             }
         }
         __syncthreads();
-        // forward: FORCE flux at the interface left of positions [2, AP-1)
+        // stage C: FORCE flux at the interface left of positions [2, AP-1)
+        double ua[3], ub[3], uri[3], dfab[3], ira = 1.0, irb = 1.0, iri = 1.0;
         if (p >= 2 && p < AP - 1) {
-            double ua[3], ub[3], F[3];
+            double fa[3], fb[3], fri[3];
             for (int v = 0; v < 3; v++) {
                 ua[v] = Eb[v][p - 1];
                 ub[v] = Ea[v][p];
             }
-            force_flux<M1, 0>(ua, ub, kc, q, F);
-            for (int v = 0; v < 3; v++) Fs[v][p] = F[v];
+            flux_a(ua, q, fa, ira);
+            flux_a(ub, q, fb, irb);
+            for (int v = 0; v < 3; v++) {
+                dfab[v] = fa[v] - fb[v];
+                uri[v] = 0.5 * ((ua[v] + ub[v]) + kc.r * dfab[v]);
+            }
+            flux_a(uri, q, fri, iri);
+            for (int v = 0; v < 3; v++) Fs[v][p] = 0.5 * (0.5 * ((fa[v] + fb[v]) + kc.rinv * (ua[v] - ub[v])) + fri[v]);
         }
         __syncthreads();
         double rb = 0.0, rinvb = 0.0, halfrb = 0.0, gb = 0.0;
-        // reverse 1: update and setcons, mu = dL/dU'_c for real cells of positions [2, AP-2)
-        if (p >= 2 && p < AP - 2 && real) {
-            double Un[3], lam[3], mu[3] = {0.0, 0.0, 0.0}, g0 = 0.0;
-            for (int v = 0; v < 3; v++) {
-                Un[v] = Us[v][p] + (kc.r * (Fs[v][p] - Fs[v][p + 1]));
-                lam[v] = a.lam_in[v * a.plane + base + c];
+        // reverse 1: update and setcons; mu = dL/dU'_c for real cells of positions [2, AP-2)
+        {
+            double mu[3] = {0.0, 0.0, 0.0};
+            if (upd) {
+                double Un[3];
+                for (int v = 0; v < 3; v++) Un[v] = Us[v][p] + kc.r * (Fs[v][p] - Fs[v][p + 1]);
+                // W = (rho, m / rho, (gamma - 1)(E - m u / 2) - gamma p_inf)
+                const double ir = rcp_nr2(Un[0]);
+                const double u = Un[1] * ir;
+                const double X = Un[2] - 0.5 * Un[1] * u;
+                mu[0] = lam[0] - u * ir * lam[1] + q.gm1 * 0.5 * u * u * lam[2];
+                mu[1] = ir * lam[1] - q.gm1 * u * lam[2];
+                mu[2] = q.gm1 * lam[2];
+                if (out) {
+                    gb += (X - q.pinf) * lam[2];
+                    for (int v = 0; v < 3; v++) rb += mu[v] * (Fs[v][p] - Fs[v][p + 1]);
+                }
             }
-            setcons_vjp(Un, q1, lam, mu, g0);
             for (int v = 0; v < 3; v++) MU[v][p] = mu[v];
-            if (out) {
-                gb += g0;
-                for (int v = 0; v < 3; v++) rb += mu[v] * (Fs[v][p] - Fs[v][p + 1]);
-            }
         }
         __syncthreads();
         // reverse 2: interface left of positions [3, AP-2); real for right cell c in [0, n]
-        if (p >= 3 && p < AP - 2 && c >= 0 && c <= n) {
-            double Fb[3], uab[3] = {0.0, 0.0, 0.0}, ubb[3] = {0.0, 0.0, 0.0}, ua[3], ub[3];
-            double lrb = 0.0, lrinvb = 0.0, lgb = 0.0;
-            for (int v = 0; v < 3; v++) {
-                Fb[v] = kc.r * (MU[v][p] - MU[v][p - 1]);
-                ua[v] = Eb[v][p - 1];
-                ub[v] = Ea[v][p];
+        {
+            double uab[3] = {0.0, 0.0, 0.0}, ubb[3] = {0.0, 0.0, 0.0};
+            const bool live = p >= 3 && p < AP - 2 && c >= 0 && c <= n;
+            if (live) {
+                double lf_b[3], urib[3] = {0.0, 0.0, 0.0}, lrb = 0.0, lrinvb = 0.0, lgb = 0.0;
+                for (int v = 0; v < 3; v++) lf_b[v] = 0.5 * kc.r * (MU[v][p] - MU[v][p - 1]);  // lf-bar = fri-bar = F-bar / 2
+                flux_vjp(uri, iri, q, lf_b, urib, lgb);
+                double fab[3], fbb[3];
+                for (int v = 0; v < 3; v++) {
+                    fab[v] = 0.5 * lf_b[v] + 0.5 * kc.r * urib[v];
+                    fbb[v] = 0.5 * lf_b[v] - 0.5 * kc.r * urib[v];
+                    uab[v] = 0.5 * kc.rinv * lf_b[v] + 0.5 * urib[v];
+                    ubb[v] = -0.5 * kc.rinv * lf_b[v] + 0.5 * urib[v];
+                    lrb += 0.5 * urib[v] * dfab[v];
+                    lrinvb += 0.5 * lf_b[v] * (ua[v] - ub[v]);
+                }
+                flux_vjp(ua, ira, q, fab, uab, lgb);
+                flux_vjp(ub, irb, q, fbb, ubb, lgb);
+                const bool own = c < n ? out : (p - 1 >= AH && p - 1 < AP - AH);
+                if (own) {
+                    rb += lrb;
+                    rinvb += lrinvb;
+                    gb += lgb;
+                }
             }
-            force_vjp(ua, ub, kc, q1, q, Fb, uab, ubb, lrb, lrinvb, lgb);
-            for (int v = 0; v < 3; v++) {
-                BB[v][p - 1] = uab[v];
-                AB[v][p] = ubb[v];
-            }
-            const bool own = c < n ? out : (p - 1 >= AH && p - 1 < AP - AH);
-            if (own) {
-                rb += lrb;
-                rinvb += lrinvb;
-                gb += lgb;
+            // edge adjoints of positions [2, AP-3); interfaces outside [0, n] contribute nothing
+            if (p >= 3 && p < AP - 2) {
+                for (int v = 0; v < 3; v++) {
+                    BB[v][p - 1] = uab[v];
+                    AB[v][p] = ubb[v];
+                }
             }
         }
         __syncthreads();
         // reverse 3: edge adjoints of positions [3, AP-3) -> contributions to cells p-1, p, p+1
-        if (p >= 3 && p < AP - 3) {
-            double uL[3], u[3], uR[3], ab[3], bb[3], uLb[3] = {0, 0, 0}, ub[3] = {0, 0, 0}, uRb[3] = {0, 0, 0};
-            double lh = 0.0, lgb = 0.0;
-            for (int v = 0; v < 3; v++) {
-                uL[v] = Us[v][p - 1];
-                u[v] = Us[v][p];
-                uR[v] = Us[v][p + 1];
-                ab[v] = AB[v][p];
-                bb[v] = BB[v][p];
+        {
+            double l[3] = {0.0, 0.0, 0.0}, m[3] = {0.0, 0.0, 0.0}, rr[3] = {0.0, 0.0, 0.0};
+            if (p >= 3 && p < AP - 3) {
+                double xlb[3], xrb[3], flb[3], frb[3], lh = 0.0, lgb = 0.0;
+                for (int v = 0; v < 3; v++) {
+                    const double evb = AB[v][p] + BB[v][p];
+                    xlb[v] = AB[v][p];
+                    xrb[v] = BB[v][p];
+                    flb[v] = kc.half_r * evb;
+                    frb[v] = -kc.half_r * evb;
+                    lh += evb * dF[v];
+                }
+                flux_vjp(xl, irl, q, flb, xlb, lgb);
+                flux_vjp(xr, irr, q, frb, xrb, lgb);
+                for (int v = 0; v < 3; v++) {
+                    const double sb = 0.5 * (xrb[v] - xlb[v]);
+                    const double dmb = sb * sdm[v], dpb = sb * sdp[v];
+                    l[v] = -dmb;
+                    m[v] = xlb[v] + xrb[v] + dmb - dpb;
+                    rr[v] = dpb;
+                }
+                const bool own = real ? out : (c < 0 ? owns_first : owns_last);
+                if (own) {
+                    halfrb += lh;
+                    gb += lgb;
+                }
             }
-            evolve_vjp(uL, u, uR, kc, q1, q, ab, bb, uLb, ub, uRb, lh, lgb);
             for (int v = 0; v < 3; v++) {
-                UL[v][p] = uLb[v];
-                US[v][p] = ub[v];
-                UR[v][p] = uRb[v];
-            }
-            const bool own = real ? out : (c < 0 ? owns_first : owns_last);
-            if (own) {
-                halfrb += lh;
-                gb += lgb;
+                UL[v][p] = l[v];
+                US[v][p] = m[v];
+                UR[v][p] = rr[v];
             }
         }
         __syncthreads();
@@ -321,18 +382,21 @@ __global__ void __launch_bounds__(AP) adjoint_step_kernel(AdjArgs a) {
             for (int v = 0; v < 3; v++) {
                 Ub[v] = MU[v][p] + US[v][p] + UR[v][p - 1] + UL[v][p + 1];
                 // ghost g mirrors cell c when g = -1 - c (c <= 1) or g = 2n - 1 - c (c >= n - 2); its dL/dU is
-                // US[g] + UR[g-1] + UL[g+1], where only edges of the ghosts -1 and n and the real end cells are non-zero
-                if (c == 0) Ub[v] += US[v][p - 1] + UL[v][p];                      // ghost -1: own edge, cell 0's left
-                if (c == 1) Ub[v] += UL[v][p - 2];                                  // ghost -2: ghost -1's left
-                if (c == n - 1) Ub[v] += US[v][p + 1] + UR[v][p];                   // ghost n: own edge, cell n-1's right
-                if (c == n - 2) Ub[v] += UR[v][p + 2];                              // ghost n+1: ghost n's right
+                // US[g] + UR[g-1] + UL[g+1], where only the edges of ghosts -1 and n and of the real cells are live
+                if (c == 0) Ub[v] += US[v][p - 1] + UL[v][p];      // ghost -1: own edges, cell 0's left operand
+                if (c == 1) Ub[v] += UL[v][p - 2];                  // ghost -2: ghost -1's left operand
+                if (c == n - 1) Ub[v] += US[v][p + 1] + UR[v][p];  // ghost n: own edges, cell n-1's right operand
+                if (c == n - 2) Ub[v] += UR[v][p + 2];              // ghost n+1: ghost n's right operand
             }
-            double Wb[3] = {0.0, 0.0, 0.0};
-            cons_vjp(W, q1, Ub, Wb, gb);
-            for (int v = 0; v < 3; v++) a.lam_out[v * a.plane + base + c] = Wb[v];
+            // U = (rho, rho u, rho u^2 / 2 + (p + gamma p_inf) / (gamma - 1))
+            const double rho = W[0], u = W[1], pr = W[2];
+            a.lam_out[base + c] = Ub[0] + u * Ub[1] + 0.5 * u * u * Ub[2];
+            a.lam_out[a.plane + base + c] = rho * Ub[1] + rho * u * Ub[2];
+            a.lam_out[2 * a.plane + base + c] = q.igm1 * Ub[2];
+            gb += -(pr + q.pinf) * q.igm1 * q.igm1 * Ub[2];
         }
         // r-bar of this tile: r, half_r = r / 2 and rinv = 1 / r all depend on dt
-        double tr = rb + 0.5 * halfrb - rinvb / (kc.r * kc.r);
+        double tr = rb + 0.5 * halfrb - rinvb * (kc.rinv * kc.rinv);
         for (int o = 16; o > 0; o >>= 1) {
             tr += __shfl_xor_sync(0xffffffffu, tr, o);
             gb += __shfl_xor_sync(0xffffffffu, gb, o);
@@ -355,54 +419,11 @@ __global__ void __launch_bounds__(AP) adjoint_step_kernel(AdjArgs a) {
     }
 }
 
-// Per instance: S = max (|u| + c) with its first argmax, and dt of step s (one block per instance).
-__global__ void __launch_bounds__(256) instance_dt_kernel(const double* W, long plane, const long* offset, const int* ncell,
-                                                          const double* dx, const double* gam, double cfl, int s,
-                                                          double* dts, int* arg_out) {
-    const int k = blockIdx.x;
-    const long base = offset[k];
-    const int n = ncell[k];
-    const M1::P q{gam[2 * k], gam[2 * k + 1], 0.0};
-    double best = 0.0;
-    int arg = 0x7fffffff;
-    for (int i = threadIdx.x; i < n; i += 256) {
-        double w[3] = {W[base + i], W[plane + base + i], W[2 * plane + base + i]};
-        double sw = M1::wave(w, q, 1);
-        if (sw > best) {  // per thread the indices increase, so the first maximum is kept
-            best = sw;
-            arg = i;
-        }
-    }
-    __shared__ double bv[256];
-    __shared__ int bi[256];
-    bv[threadIdx.x] = best;
-    bi[threadIdx.x] = arg;
-    __syncthreads();
-    for (int o = 128; o > 0; o >>= 1) {
-        if (threadIdx.x < o) {
-            double ov = bv[threadIdx.x + o];
-            int oi = bi[threadIdx.x + o];
-            if (ov > bv[threadIdx.x] || (ov == bv[threadIdx.x] && oi < bi[threadIdx.x])) {
-                bv[threadIdx.x] = ov;
-                bi[threadIdx.x] = oi;
-            }
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        double S = bv[0];
-        double d = cfl * (dx[k] / S);
-        if (s <= 5) d *= 0.2;
-        dts[2 * k] = d;
-        dts[2 * k + 1] = S;
-        arg_out[k] = bi[0];
-    }
-}
-
 // Per instance: sum the tile partials in tile order, propagate dt-bar through the CFL maximum to the argmax cell.
-__global__ void instance_dt_adjoint_kernel(double* lam, const double* W, long plane, const long* offset, const double* dx,
-                                           const double* gam, const int* tile_first, const int* tile_count,
-                                           const double* tile_part, const double* dts, const int* arg, double* ggam,
+__global__ void instance_dt_adjoint_kernel(double* lam, const double* W, long plane, const long* offset, const int* ncell,
+                                           const double* dx, const double* gam, const int* tile_first,
+                                           const int* tile_count, const double* tile_part,
+                                           const unsigned long long* Sbits, double cfl, int s, int* arg, double* ggam,
                                            int ninst) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= ninst) return;
@@ -411,10 +432,17 @@ __global__ void instance_dt_adjoint_kernel(double* lam, const double* W, long pl
         rbar += tile_part[2 * t];
         gbar += tile_part[2 * t + 1];
     }
-    // r = dt / dx, dt = CFL dx / S (x0.2):  dS-bar = -(dt / S) dt-bar
+    const int ai = arg[k];
+    arg[k] = 0x7fffffff;  // ready for the next reversed step
+    if (ai < 0 || ai >= ncell[k]) {  // no cell attains S: cannot happen for a state whose S was taken from it
+        ggam[k] += gbar;
+        return;
+    }
+    // r = dt / dx, dt = CFL dx / S (x0.2):  S-bar = -(dt / S) dt-bar
+    const double S = __longlong_as_double((long long)Sbits[k]);
     const double dtb = rbar / dx[k];
-    const double Sb = -(dts[2 * k] / dts[2 * k + 1]) * dtb;
-    const long i = offset[k] + arg[k];
+    const double Sb = -(step_dt(cfl, dx[k], S, s) / S) * dtb;
+    const long i = offset[k] + ai;
     const double rho = W[i], u = W[plane + i], p = W[2 * plane + i];
     const double g = gam[2 * k], pinf = gam[2 * k + 1];
     const double c = sqrt((g * (p + pinf)) / rho);
@@ -429,7 +457,7 @@ __global__ void __launch_bounds__(256) loss_kernel(const double* W, const double
                                                    double* block_loss) {
     double acc = 0.0;
     for (long i = blockIdx.x * 256L + threadIdx.x; i < plane; i += (long)gridDim.x * 256) {
-        double d = W[i] - target[i];
+        const double d = W[i] - target[i];
         acc += d * d;
         lam[i] = 2.0 * d;
         lam[plane + i] = 0.0;
@@ -477,9 +505,12 @@ cudaError_t ensure_workspace(vg_batch* b, int checkpoints) {
     cudaError_t e = cudaSuccess;
     if (b->ckpt_slots != checkpoints) {
         if (b->ckpt) cudaFree(b->ckpt);
+        if (b->ckptS) cudaFree(b->ckptS);
         b->ckpt = nullptr;
+        b->ckptS = nullptr;
         b->ckpt_slots = 0;
         e = cudaMalloc(&b->ckpt, sbytes * (checkpoints + 1));  // + 1: the recomputation buffer
+        if (e == cudaSuccess) e = cudaMalloc(&b->ckptS, sizeof(unsigned long long) * b->ninst * (checkpoints + 1));
         if (e != cudaSuccess) return e;
         b->ckpt_slots = checkpoints;
     }
@@ -507,14 +538,17 @@ cudaError_t ensure_workspace(vg_batch* b, int checkpoints) {
     if (e == cudaSuccess) e = cudaMalloc(&b->d_tile_first, sizeof(int) * b->ninst);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_tile_count, sizeof(int) * b->ninst);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_ggam, sizeof(double) * b->ninst);
-    if (e == cudaSuccess) e = cudaMalloc(&b->d_stepdt, sizeof(double) * 2 * b->ninst);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_arg, sizeof(int) * b->ninst);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_loss, sizeof(double) * b->loss_blocks);
     if (e == cudaSuccess) e = cudaMemcpy(b->d_atiles, at.data(), sizeof(vg::Tile) * at.size(), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(b->d_tile_first, af.data(), sizeof(int) * b->ninst, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(b->d_tile_count, ac.data(), sizeof(int) * b->ninst, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        std::vector<int> none(b->ninst, 0x7fffffff);
+        e = cudaMemcpy(b->d_arg, none.data(), sizeof(int) * b->ninst, cudaMemcpyHostToDevice);
+    }
     if (e != cudaSuccess) {  // leave the workspace absent so the next call retries
-        for (double** p : {&b->lam[0], &b->lam[1], &b->d_target, &b->d_tile_part, &b->d_ggam, &b->d_stepdt, &b->d_loss}) {
+        for (double** p : {&b->lam[0], &b->lam[1], &b->d_target, &b->d_tile_part, &b->d_ggam, &b->d_loss}) {
             cudaFree(*p);
             *p = nullptr;
         }
@@ -535,8 +569,10 @@ struct Reverser {
     int limiter, steps;
     cudaStream_t st;
     std::vector<double*> slots;  // checkpoint buffers; slot 0 holds W^0 throughout
+    std::vector<unsigned long long*> slotsS;  // their per-instance maxima |u| + c
     std::vector<bool> used;
     double* tmp;                 // recomputed state
+    unsigned long long* tmpS;
     int lam_cur = 0;             // lam[lam_cur] holds dL/dW^{s+1} before reversing step s
     bool started = false;
 
@@ -550,9 +586,9 @@ struct Reverser {
     }
 
     // W^steps from W^{steps-1} (into the idle adjoint buffer), then the loss and dL/dW^steps
-    cudaError_t init_final(const double* Wprev) {
+    cudaError_t init_final(const double* Wprev, const unsigned long long* WprevS) {
         double* Wfin = b->lam[1 - lam_cur];
-        cudaError_t e = vg::batch_advance(b, Wprev, Wfin, steps - 1, 1, cfl, bias, limiter, st);
+        cudaError_t e = vg::batch_advance(b, Wprev, WprevS, Wfin, nullptr, steps - 1, 1, cfl, bias, limiter, st);
         if (e != cudaSuccess) return e;
         vg::loss_kernel<<<b->loss_blocks, 256, 0, st>>>(Wfin, b->d_target, b->total, b->lam[lam_cur], b->d_loss);
         started = true;
@@ -560,13 +596,11 @@ struct Reverser {
     }
 
     // dL/dW^s from dL/dW^{s+1} and W^s
-    cudaError_t adjoint_step(const double* Ws, int s) {
+    cudaError_t adjoint_step(const double* Ws, const unsigned long long* WsS, int s) {
         if (s == steps - 1 && !started) {
-            cudaError_t e = init_final(Ws);
+            cudaError_t e = init_final(Ws, WsS);
             if (e != cudaSuccess) return e;
         }
-        vg::instance_dt_kernel<<<b->ninst, 256, 0, st>>>(Ws, b->total, b->d_offset, b->d_ncell, b->d_dx, b->d_gam, cfl, s,
-                                                          b->d_stepdt, b->d_arg);
         vg::AdjArgs a{};
         a.W = Ws;
         a.lam_in = b->lam[lam_cur];
@@ -578,15 +612,18 @@ struct Reverser {
         a.gam = b->d_gam;
         a.tiles = b->d_atiles;
         a.ntiles = b->natiles;
-        a.dts = b->d_stepdt;
+        a.S = WsS;
+        a.arg = b->d_arg;
         a.tile_part = b->d_tile_part;
+        a.cfl = cfl;
         a.bias = bias;
         a.floor5 = floor5;
         a.limiter = limiter;
+        a.step = s;
         vg::adjoint_step_kernel<<<b->agrid, vg::AP, 0, st>>>(a);
         vg::instance_dt_adjoint_kernel<<<(b->ninst + 127) / 128, 128, 0, st>>>(
-            b->lam[1 - lam_cur], Ws, b->total, b->d_offset, b->d_dx, b->d_gam, b->d_tile_first, b->d_tile_count,
-            b->d_tile_part, b->d_stepdt, b->d_arg, b->d_ggam, b->ninst);
+            b->lam[1 - lam_cur], Ws, b->total, b->d_offset, b->d_ncell, b->d_dx, b->d_gam, b->d_tile_first,
+            b->d_tile_count, b->d_tile_part, WsS, cfl, s, b->d_arg, b->d_ggam, b->ninst);
         lam_cur = 1 - lam_cur;
         b->last_adjoint_steps++;
         return cudaGetLastError();
@@ -599,12 +636,13 @@ struct Reverser {
     cudaError_t reverse(int s0, int s1, int c, int slot) {
         cudaError_t e = cudaSuccess;
         const int n = s1 - s0;
-        if (n == 1) return adjoint_step(slots[slot], s0);
+        if (n == 1) return adjoint_step(slots[slot], slotsS[slot], s0);
         if (c == 0) {  // only the starting state: recompute every step from it
-            for (int s = s1 - 1; s >= s0 && e == cudaSuccess; s--) {
-                e = vg::batch_advance(b, slots[slot], tmp, s0, s - s0, cfl, bias, limiter, st);
-                if (e == cudaSuccess) e = adjoint_step(tmp, s);
+            for (int s = s1 - 1; s > s0 && e == cudaSuccess; s--) {
+                e = vg::batch_advance(b, slots[slot], slotsS[slot], tmp, tmpS, s0, s - s0, cfl, bias, limiter, st);
+                if (e == cudaSuccess) e = adjoint_step(tmp, tmpS, s);
             }
+            if (e == cudaSuccess) e = adjoint_step(slots[slot], slotsS[slot], s0);
             return e;
         }
         int t = 1;
@@ -612,7 +650,7 @@ struct Reverser {
         const int right = (int)std::min<double>(n - 1, beta(c, t));
         const int m = s1 - right;
         const int ns = take();
-        e = vg::batch_advance(b, slots[slot], slots[ns], s0, m - s0, cfl, bias, limiter, st);
+        e = vg::batch_advance(b, slots[slot], slotsS[slot], slots[ns], slotsS[ns], s0, m - s0, cfl, bias, limiter, st);
         if (e == cudaSuccess) e = reverse(m, s1, c - 1, ns);
         used[ns] = false;
         if (e == cudaSuccess) e = reverse(s0, m, c, slot);
@@ -646,12 +684,17 @@ extern "C" vg_status vg_batch_gradient(vg_batch* b, const double* target_rho, do
     R.limiter = limiter;
     R.steps = steps;
     R.st = st;
-    for (int i = 0; i < checkpoints; i++) R.slots.push_back(b->ckpt + (long)i * 3 * n);
+    for (int i = 0; i < checkpoints; i++) {
+        R.slots.push_back(b->ckpt + (long)i * 3 * n);
+        R.slotsS.push_back(b->ckptS + (long)i * b->ninst);
+    }
     R.used.assign(checkpoints, false);
     R.tmp = b->ckpt + (long)checkpoints * 3 * n;
+    R.tmpS = b->ckptS + (long)checkpoints * b->ninst;
     b->last_forward_steps = 0;
     b->last_adjoint_steps = 0;
     VA_CUDA(cudaMemcpyAsync(R.slots[0], b->buf[b->cur], sbytes, cudaMemcpyDeviceToDevice, st));
+    VA_CUDA(vg::batch_wave_max(b, R.slots[0], R.slotsS[0], st));
     R.used[0] = true;
     cudaError_t e = R.reverse(0, steps, checkpoints - 1, 0);
     // the batch keeps its initial state

@@ -141,26 +141,44 @@ __global__ void __launch_bounds__(BP) batch_step_kernel(BatchArgs a) {
     }
 }
 
-// Initial maxima: slot a.wave_slot <- max over each instance (grid-stride over cells; instance by binary search).
+// Initial maxima: slot a.wave_slot <- max over each instance's cells (one block per instance, no atomics).
 // Also resets the step counter to a.step_init and the finished-block counter.
 __global__ void __launch_bounds__(256) batch_max_wave_kernel(BatchArgs a) {
+    const int k = blockIdx.x;
+    if (k == 0 && threadIdx.x == 0) {
+        *a.step = a.step_init;
+        *a.done = 0u;
+    }
+    const long base = a.offset[k];
+    const int n = a.ncell[k];
+    const M1::P q{a.gam[2 * k], a.gam[2 * k + 1], 0.0};
+    double m = 0.0;
+    for (int i = threadIdx.x; i < n; i += 256) {
+        double W[M1::NW];
+        for (int v = 0; v < M1::NW; v++) W[v] = a.in[v * a.plane + base + i];
+        const double sw = M1::wave(W, q, 1);
+        m = (sw > m) ? sw : m;
+    }
+    __shared__ double red[8];
+    for (int o = 16; o > 0; o >>= 1) {
+        const double w = __shfl_xor_sync(0xffffffffu, m, o);
+        m = (w > m) ? w : m;
+    }
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < 8; w++) m = (red[w] > m) ? red[w] : m;
+        a.smax[a.wave_slot * a.ninst + k] = (unsigned long long)__double_as_longlong(m);
+    }
+}
+
+// Known maxima (bit patterns) into slot a.wave_slot, and the counters reset.
+__global__ void __launch_bounds__(256) batch_set_wave_kernel(BatchArgs a, const unsigned long long* S) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         *a.step = a.step_init;
         *a.done = 0u;
     }
-    for (long i = blockIdx.x * 256L + threadIdx.x; i < a.plane; i += (long)gridDim.x * 256) {
-        int lo = 0, hi = a.ninst - 1;
-        while (lo < hi) {
-            int mid = (lo + hi + 1) >> 1;
-            if (a.offset[mid] <= i) lo = mid;
-            else hi = mid - 1;
-        }
-        double W[M1::NW];
-        for (int v = 0; v < M1::NW; v++) W[v] = a.in[v * a.plane + i];
-        M1::P q{a.gam[2 * lo], a.gam[2 * lo + 1], 0.0};
-        double sw = M1::wave(W, q, 1);
-        if (sw > 0.0) atomic_max_nonneg(&a.smax[a.wave_slot * a.ninst + lo], sw);
-    }
+    for (int k = blockIdx.x * 256 + threadIdx.x; k < a.ninst; k += gridDim.x * 256) a.smax[a.wave_slot * a.ninst + k] = S[k];
 }
 
 BatchArgs batch_args(vg_batch* b, const double* in, double* out, double cfl, double bias, int limiter, int max_steps) {
@@ -189,36 +207,64 @@ BatchArgs batch_args(vg_batch* b, const double* in, double* out, double cfl, dou
     return a;
 }
 
-cudaError_t start_steps(vg_batch* b, const double* state, int s_start, double cfl, double bias, int limiter, int max_steps,
-                        cudaStream_t st) {
+// Ring, step counter and the maxima of `state` for a run starting at step s_start; state_S (nullable) holds
+// those maxima already (bit patterns, one per instance).
+cudaError_t start_steps(vg_batch* b, const double* state, const unsigned long long* state_S, int s_start, double cfl,
+                        double bias, int limiter, int max_steps, cudaStream_t st) {
     cudaError_t e = cudaMemsetAsync(b->d_smax, 0, sizeof(unsigned long long) * 3 * b->ninst, st);
     if (e != cudaSuccess) return e;
     BatchArgs a0 = batch_args(b, state, nullptr, cfl, bias, limiter, max_steps);
     a0.wave_slot = s_start % 3;
     a0.step_init = s_start;
-    int mw = (int)std::min<long>((b->total + 255) / 256, 148L * 8);
-    batch_max_wave_kernel<<<mw, 256, 0, st>>>(a0);
+    if (state_S)
+        batch_set_wave_kernel<<<std::max(1, std::min(b->ninst / 256 + 1, 148)), 256, 0, st>>>(a0, state_S);
+    else
+        batch_max_wave_kernel<<<b->ninst, 256, 0, st>>>(a0);
     return cudaGetLastError();
 }
 
 }  // namespace
 
-cudaError_t batch_advance(vg_batch* b, const double* src, double* dst, int s_start, int nsteps, double cfl, double bias,
-                          int limiter, cudaStream_t st) {
+cudaError_t batch_advance(vg_batch* b, const double* src, const unsigned long long* src_S, double* dst,
+                          unsigned long long* dst_S, int s_start, int nsteps, double cfl, double bias, int limiter,
+                          cudaStream_t st) {
     const size_t bytes = sizeof(double) * 3 * b->total;
-    cudaError_t e = cudaSuccess;
-    if (nsteps <= 0) return src == dst ? cudaSuccess : cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, st);
-    if (src != b->buf[0]) e = cudaMemcpyAsync(b->buf[0], src, bytes, cudaMemcpyDeviceToDevice, st);
-    if (e == cudaSuccess) e = start_steps(b, b->buf[0], s_start, cfl, bias, limiter, s_start + nsteps, st);
+    const size_t sbytes = sizeof(unsigned long long) * b->ninst;
+    if (nsteps <= 0) {
+        cudaError_t e = src == dst ? cudaSuccess : cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, st);
+        if (e == cudaSuccess && dst_S && dst_S != src_S) {
+            if (src_S) return cudaMemcpyAsync(dst_S, src_S, sbytes, cudaMemcpyDeviceToDevice, st);
+            return batch_wave_max(b, src, dst_S, st);
+        }
+        return e;
+    }
+    // src is only read; intermediate states alternate between the batch's two buffers and the last step writes
+    // dst directly (dst must not be src or one of the batch's buffers)
+    cudaError_t e = start_steps(b, src, src_S, s_start, cfl, bias, limiter, s_start + nsteps, st);
+    const double* cur = src;
     for (int i = 0; i < nsteps && e == cudaSuccess; i++) {
-        BatchArgs a = batch_args(b, b->buf[i & 1], b->buf[1 - (i & 1)], cfl, bias, limiter, s_start + nsteps);
+        double* nxt = (i == nsteps - 1) ? dst : b->buf[i & 1];
+        BatchArgs a = batch_args(b, cur, nxt, cfl, bias, limiter, s_start + nsteps);
         batch_step_kernel<<<b->grid, BP, 0, st>>>(a);
         e = cudaGetLastError();
+        cur = nxt;
     }
     b->last_forward_steps += nsteps;
-    double* res = b->buf[nsteps & 1];
-    if (e == cudaSuccess && dst != res) e = cudaMemcpyAsync(dst, res, bytes, cudaMemcpyDeviceToDevice, st);
+    // the last step accumulated the maxima of its result into slot (s_start + nsteps) % 3
+    if (e == cudaSuccess && dst_S)
+        e = cudaMemcpyAsync(dst_S, b->d_smax + ((s_start + nsteps) % 3) * b->ninst, sbytes, cudaMemcpyDeviceToDevice, st);
     return e;
+}
+
+cudaError_t batch_wave_max(vg_batch* b, const double* state, unsigned long long* out_S, cudaStream_t st) {
+    BatchArgs a0 = batch_args(b, state, nullptr, 0.0, 0.0, 0, 0);
+    // a private ring slot view: slot 0 of out_S, counters untouched by pointing them at scratch
+    a0.smax = out_S;
+    a0.wave_slot = 0;
+    a0.step = b->d_step;
+    a0.step_init = 0;
+    batch_max_wave_kernel<<<b->ninst, 256, 0, st>>>(a0);
+    return cudaGetLastError();
 }
 
 }  // namespace vg
@@ -317,7 +363,7 @@ vg_status vg_batch_destroy(vg_batch* b) {
     for (void* p : {(void*)b->d_offset, (void*)b->d_ncell, (void*)b->d_dx, (void*)b->d_gam, (void*)b->d_tiles,
                     (void*)b->d_smax, (void*)b->d_dt, (void*)b->d_step, (void*)b->d_done, (void*)b->d_err, (void*)b->ckpt,
                     (void*)b->d_target, (void*)b->d_atiles, (void*)b->d_tile_part, (void*)b->d_tile_first,
-                    (void*)b->d_tile_count, (void*)b->d_ggam, (void*)b->d_stepdt, (void*)b->d_arg, (void*)b->d_loss})
+                    (void*)b->d_tile_count, (void*)b->d_ggam, (void*)b->ckptS, (void*)b->d_arg, (void*)b->d_loss})
         if (p) cudaFree(p);
     if (b->cap) cudaStreamDestroy(b->cap);
     delete b;
@@ -378,7 +424,7 @@ vg_status vg_batch_run(vg_batch* b, double cfl, int steps, double bias, int limi
         b->cur = 0;
     }
     VB_CUDA(cudaMemsetAsync(b->d_err, 0, sizeof(unsigned int), st));
-    VB_CUDA(vg::start_steps(b, b->buf[0], 0, cfl, bias, limiter, steps, st));
+    VB_CUDA(vg::start_steps(b, b->buf[0], nullptr, 0, cfl, bias, limiter, steps, st));
     // one graph per (steps, cfl, bias, limiter): the whole time loop, one persistent kernel per step
     if (!b->graph || b->graph_steps != steps || b->graph_cfl != cfl || b->graph_bias != bias || b->graph_limiter != limiter) {
         if (b->graph) cudaGraphExecDestroy(b->graph);

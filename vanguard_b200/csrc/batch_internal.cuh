@@ -42,9 +42,15 @@ struct BatchArgs {
 
 // Forward-advance nsteps steps from the state in `src` (3 planes of the batch's total cells), with step
 // indices starting at s_start (the x0.2 factor applies to indices <= 5); the result is written to `dst`.
-// src and dst may be the batch's own buffers or any device buffers of the same shape.
-cudaError_t batch_advance(::vg_batch* b, const double* src, double* dst, int s_start, int nsteps, double cfl,
-                          double bias, int limiter, cudaStream_t st);
+// src is left unchanged; dst must be a device buffer of the same shape other than src and the batch's buf[].
+// src_S (nullable) holds the maxima |u| + c of src per instance (double bit patterns) so no pass over src is
+// needed; dst_S (nullable) receives those of dst.
+cudaError_t batch_advance(::vg_batch* b, const double* src, const unsigned long long* src_S, double* dst,
+                          unsigned long long* dst_S, int s_start, int nsteps, double cfl, double bias, int limiter,
+                          cudaStream_t st);
+
+// out_S[k] <- max over instance k's cells of |u| + c of `state` (bit patterns); resets the batch's step counter.
+cudaError_t batch_wave_max(::vg_batch* b, const double* state, unsigned long long* out_S, cudaStream_t st);
 
 }  // namespace vg
 
@@ -76,6 +82,7 @@ struct vg_batch {
     // adjoint workspace (allocated on first use by vg_batch_gradient)
     double* lam[2] = {nullptr, nullptr};  // dL/dW of the step being reversed and of the one before
     double* ckpt = nullptr;               // checkpoint slots + one recomputation buffer
+    unsigned long long* ckptS = nullptr;  // their per-instance maxima |u| + c (double bit patterns)
     int ckpt_slots = 0;
     double* d_target = nullptr;           // target density of the loss
     vg::Tile* d_atiles = nullptr;         // adjoint tiles (contiguous per instance)
@@ -85,8 +92,7 @@ struct vg_batch {
     int* d_tile_first = nullptr;          // first adjoint tile of each instance
     int* d_tile_count = nullptr;
     double* d_ggam = nullptr;             // gamma gradient per instance
-    double* d_stepdt = nullptr;           // dt and S of the step being reversed (2 per instance)
-    int* d_arg = nullptr;                 // first cell attaining S, per instance
+    int* d_arg = nullptr;                 // first cell attaining S, per instance (INT_MAX between steps)
     double* d_loss = nullptr;             // per-block partial losses
     int loss_blocks = 0;
     long last_forward_steps = 0, last_adjoint_steps = 0;
