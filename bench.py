@@ -323,12 +323,129 @@ def run_cuda(args, world, rank, local):
         d = np.abs(finals["mixed"][0] - finals["fp64"][0])
         line["mixed_error_vs_fp64"] = {"rho_L1": float(d.mean()), "rho_Linf": float(d.max()),
                                        "reference": "the FP64 CUDA form, bitwise equal to the oracle"}
+    if not args.headline_only:
+        line["configs"] = {"C5_ragged_batch_adjoint": ragged_adjoint_leg(local, stream, sh),
+                           "C3_mhd_2048": mhd_leg(local, stream, sh),
+                           "C1_sod_1000": sod_leg(local, stream, sh)}
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample()
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
     return 0
+
+
+C5_NINST, C5_STEPS, C5_CKPT = 4096, 500, 32
+
+
+def ragged_adjoint_leg(local, stream, sh, reps=3):
+    """C5: 4096 ragged 1D Euler Riemann problems (cells U{200..4000}), CFL 0.8, superbee, 500 steps per instance
+    in one persistent launch per step (the whole loop one CUDA graph), then the discrete adjoint of
+    L = sum (rho(T) - target)^2 with respect to the initial states and gamma.  Device-timed with CUDA events on the
+    launching stream; the adjoint cost is reported against the forward for a binomial schedule with C5_CKPT state
+    slots (recomputes forward segments) and with every state stored."""
+    import torch
+    import vanguard_b200 as vg
+    from vanguard_b200 import workloads as wl
+
+    ncell, dx, gamma, theta, W0 = wl.ragged_riemann_batch(ninst=C5_NINST, seed=SEED)
+    total = int(W0.shape[1])
+    target = np.random.default_rng(SEED + 1).uniform(0.1, 2.0, total)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    out = {"workload": f"{C5_NINST} ragged 1D Euler Riemann problems, cells U{{200..4000}} ({total} cells), "
+                       f"gamma U[1.2,1.67], CFL 0.8, superbee, {C5_STEPS} steps, per-instance device dt",
+           "cells": total}
+    with vg.Batch(ncell, dx, gamma, device=local) as b:
+        b.upload(W0, stream=sh)
+        b.run(CFL, C5_STEPS, limiter=LIMITER, stream=sh)  # graph capture
+        fwd = []
+        for _ in range(reps):
+            b.upload(W0, stream=sh)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            b.run(CFL, C5_STEPS, limiter=LIMITER, stream=sh)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            fwd.append(e0.elapsed_time(e1))
+        fwd_ms = statistics.median(fwd)
+        out["forward"] = {"ms": fwd_ms, "cell_updates_per_s": total * C5_STEPS / (fwd_ms / 1e3),
+                          "launches": b.last_launch_count()}
+        tgt = torch.from_numpy(target).to(f"cuda:{local}")
+        g = torch.empty((6, total), dtype=torch.float64, device=f"cuda:{local}")
+        gg = torch.empty((C5_NINST,), dtype=torch.float64, device=f"cuda:{local}")
+        for name, ck in (("binomial", C5_CKPT), ("store_all", C5_STEPS)):
+            b.upload(W0, stream=sh)
+            b.gradient(tgt, CFL, C5_STEPS, limiter=LIMITER, checkpoints=ck, out=(g, gg), stream=sh)  # workspace
+            torch.cuda.synchronize()
+            e0.record(stream)
+            L, _, _, fw, aw = b.gradient(tgt, CFL, C5_STEPS, limiter=LIMITER, checkpoints=ck, out=(g, gg), stream=sh)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            out[f"adjoint_{name}"] = {"checkpoints": ck, "ms": ms, "ratio_vs_forward": ms / fwd_ms,
+                                      "forward_steps": fw, "reversed_steps": aw, "loss": L,
+                                      "state_slot_bytes": (ck + 1) * 3 * total * 8}
+        # through the host-buffer API: target up, gradient planes and gamma gradient down, inside the timed region
+        b.upload(W0, stream=sh)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        b.gradient(target, CFL, C5_STEPS, limiter=LIMITER, checkpoints=C5_CKPT, stream=sh)
+        host_s = time.perf_counter() - t0
+        out["adjoint_binomial"]["e2e_ms"] = host_s * 1e3
+        out["adjoint_binomial"]["e2e_ratio_vs_forward"] = host_s * 1e3 / fwd_ms
+    return out
+
+
+def mhd_leg(local, stream, sh, steps=500):
+    """C3: 2D ideal MHD (GLM) 2048^2 periodic smooth vortex, superbee, CFL 0.8, `steps` steps, FP64 and mixed."""
+    import torch
+    import vanguard_b200 as vg
+    from vanguard_b200 import workloads as wl
+
+    n = 2048
+    W = wl.mhd_vortex_2d(n, seed=SEED)
+    prm = wl.mhd_params()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    res, finals = {}, {}
+    for name, prec in (("fp64", vg.FP64), ("mixed", vg.MIXED)):
+        with vg.Solver(vg.MHD, n, n, prm, precision=prec, boundary=vg.PERIODIC, device=local) as s:
+            s.upload(W, stream=sh)
+            s.autotune(1.0 / n, CFL, limiter=LIMITER, stream=sh)
+            s.run(1.0 / n, CFL, steps=3, limiter=LIMITER, stream=sh)
+            s.upload(W, stream=sh)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            s.run(1.0 / n, CFL, steps=steps, limiter=LIMITER, stream=sh)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            finals[name] = s.download(stream=sh)
+            res[name] = {"ms": ms, "cell_updates_per_s": n * n * steps / (ms / 1e3)}
+    d = np.abs(finals["mixed"][0] - finals["fp64"][0])
+    res["mixed_error_vs_fp64"] = {"rho_L1": float(d.mean()), "rho_Linf": float(d.max())}
+    res["mixed_speedup"] = res["fp64"]["ms"] / res["mixed"]["ms"]
+    res["workload"] = f"2D MHD {n}x{n} periodic vortex (seeded noise 1e-3), gamma 5/3, superbee, CFL 0.8, {steps} steps"
+    return res
+
+
+def sod_leg(local, stream, sh):
+    """C1: 1D Sod, 1000 cells, minbee, CFL 0.9, t_end 0.25 (time to solution, FP64)."""
+    import torch
+    import vanguard_b200 as vg
+    from vanguard_b200 import workloads as wl
+
+    W = wl.sod_1d(1000)
+    with vg.Solver(vg.EULER, 1000, 1, wl.euler_params(1.4), device=local) as s:
+        s.upload(W, stream=sh)
+        s.run(1e-3, 0.9, t_end=0.25, limiter=2, stream=sh)
+        s.upload(W, stream=sh)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        t, it = s.run(1e-3, 0.9, t_end=0.25, limiter=2, stream=sh)
+        torch.cuda.synchronize()
+        sec = time.perf_counter() - t0
+    return {"workload": "1D Sod 1000 cells, minbee, CFL 0.9, t_end 0.25", "steps": it, "t": t, "ms": sec * 1e3,
+            "cell_updates_per_s": 1000 * it / sec}
 
 
 def ctypes_stream(stream):
@@ -368,6 +485,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--headline-only", action="store_true", help="skip the C1/C3/C5 measurements")
     ap.add_argument("--nx", type=int, default=4096, help="grid size (smaller grids are for profiling only)")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -171,10 +171,11 @@ long vg_batch_last_launch_count(vg_batch* b);
  * memory to (checkpoints + 3) states; steps are recomputed on Griewank's binomial schedule, so checkpoints ==
  * steps stores every state and recomputes nothing.  forward_steps / adjoint_steps (nullable) receive the number
  * of forward steps advanced (recomputation and the final step included) and of reversed steps.  The batch keeps
- * its initial state.  target_rho, grad_planes (6 x total) and grad_gamma (ninst) are host arrays. */
+ * its initial state.  target_rho (total), grad_planes (6 x total, nullable) and grad_gamma (ninst, nullable) are
+ * host arrays, or device arrays when is_device != 0; loss (nullable) is a host scalar.  Returns when done. */
 vg_status vg_batch_gradient(vg_batch* b, const double* target_rho, double cfl, int steps, double bias, int limiter,
-                            int checkpoints, double* loss, double* grad_planes, double* grad_gamma, long* forward_steps,
-                            long* adjoint_steps, void* stream);
+                            int checkpoints, double* loss, double* grad_planes, double* grad_gamma, int is_device,
+                            long* forward_steps, long* adjoint_steps, void* stream);
 
 /* Rows accepted by vg_max_wave_speed_noalloc: the size of its static scratch array (8 bytes per row,
  * 512 KiB, held on every GPU that loads the library until the process exits). */

@@ -179,3 +179,38 @@ def test_torch_autograd_wrapper_gradcheck(gpu):
     th = torch.tensor(theta, dtype=torch.float64, requires_grad=True)
     ga = torch.tensor(gamma, dtype=torch.float64, requires_grad=True)
     assert torch.autograd.gradcheck(BatchLoss.apply, (th, ga), eps=1e-6, atol=1e-6, rtol=1e-5)
+
+
+def test_device_buffers_match_host_buffers(gpu):
+    torch = pytest.importorskip("torch")
+    ncell = np.array([7, 140])
+    gamma, theta = _theta_batch(ncell, 5)
+    W0 = wl.batch_planes(ncell, theta)
+    target = np.random.default_rng(3).uniform(0.1, 2.0, W0.shape[1])
+    with gpu.Batch(ncell, 1.0 / ncell, gamma) as b:
+        b.upload(W0)
+        L, G, gg, fw, aw = b.gradient(target, CFL, 12, checkpoints=3)
+        td = torch.from_numpy(target).cuda()
+        g = torch.full((6, W0.shape[1]), 7.0, dtype=torch.float64, device="cuda")
+        ggd = torch.empty(len(ncell), dtype=torch.float64, device="cuda")
+        L2, _, _, fw2, aw2 = b.gradient(td, CFL, 12, checkpoints=3, out=(g, ggd))
+    assert L == L2 and (fw, aw) == (fw2, aw2)
+    assert np.array_equal(g.cpu().numpy(), G) and np.array_equal(ggd.cpu().numpy(), gg)
+
+
+def test_adjoint_matches_tangent_linear_long_horizon(gpu):
+    # 300 steps: far past the horizon where central differences stay smooth for superbee (limiter kinks and the
+    # 1e-5 floor are crossed within +-h); the tangent-linear run follows the same branches and stays exact
+    ncell = np.array([60, 131])
+    gamma, theta = _theta_batch(ncell, 21)
+    W0 = wl.batch_planes(ncell, theta)
+    target = np.random.default_rng(9).uniform(0.1, 2.0, W0.shape[1])
+    steps = 300
+    with gpu.Batch(ncell, 1.0 / ncell, gamma) as b:
+        b.upload(W0)
+        L, G, gg, fw, aw = b.gradient(target, CFL, steps, checkpoints=20)
+    Lt, Gt, ggt = tangent.gradient(ncell, 1.0 / ncell, gamma, W0, target, CFL, steps, 0.0, 0)
+    assert abs(L - Lt) <= 1e-12 * Lt
+    scale = np.abs(Gt).max()
+    assert np.abs(G - Gt).max() <= 1e-8 * scale
+    assert np.allclose(gg, ggt, rtol=1e-8, atol=1e-12 * scale)

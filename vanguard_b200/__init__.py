@@ -107,8 +107,8 @@ def lib():
         L.vg_batch_last_launch_count.argtypes = [vp]
         L.vg_batch_last_launch_count.restype = ctypes.c_long
         Lp = ctypes.POINTER(ctypes.c_long)
-        L.vg_batch_gradient.argtypes = [vp, D, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_int,
-                                        ctypes.c_int, D, D, D, Lp, Lp, vp]
+        L.vg_batch_gradient.argtypes = [vp, vp, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                        ctypes.c_int, D, vp, vp, ctypes.c_int, Lp, Lp, vp]
         L.vg_last_error_string.restype = ctypes.c_char_p
         L.vg_status_string.restype = ctypes.c_char_p
         L.vg_status_string.argtypes = [ctypes.c_int]
@@ -285,20 +285,31 @@ class Batch:
     def last_launch_count(self):
         return lib().vg_batch_last_launch_count(self._h)
 
-    def gradient(self, target_rho, cfl, steps, bias=0.0, limiter=SUPERBEE, checkpoints=None, stream=None):
+    def gradient(self, target_rho, cfl, steps, bias=0.0, limiter=SUPERBEE, checkpoints=None, out=None, stream=None):
         """Discrete adjoint of run(cfl, steps) from the current state for L = sum (rho(T) - target_rho)^2.
         Returns (L, dL/dW0 as (6, total) planes, dL/dgamma (ninst,), forward steps, reversed steps).
-        checkpoints defaults to every state (no recomputation)."""
+        checkpoints defaults to every state (no recomputation).  With torch CUDA tensors for target_rho and
+        out = (grad_planes (6, total), grad_gamma (ninst,)) everything stays on the device."""
+        fw, aw = ctypes.c_long(), ctypes.c_long()
+        L = ctypes.c_double()
+        ck = steps if checkpoints is None else checkpoints
+        if hasattr(target_rho, "data_ptr"):
+            g, gg = out
+            for x, shape in ((target_rho, (self.total,)), (g, (6, self.total)), (gg, (self.ninst,))):
+                if tuple(x.shape) != shape or not x.is_contiguous():
+                    raise ValueError(f"expected a contiguous device tensor of shape {shape}")
+            _check(lib().vg_batch_gradient(self._h, ctypes.c_void_p(target_rho.data_ptr()), cfl, steps, bias, limiter,
+                                           ck, ctypes.byref(L), ctypes.c_void_p(g.data_ptr()),
+                                           ctypes.c_void_p(gg.data_ptr()), 1, ctypes.byref(fw), ctypes.byref(aw),
+                                           stream))
+            return L.value, g, gg, fw.value, aw.value
         t = np.ascontiguousarray(target_rho, dtype=np.float64)
         if t.shape != (self.total,):
             raise ValueError(f"target_rho must have shape ({self.total},)")
-        D = ctypes.POINTER(ctypes.c_double)
-        L = ctypes.c_double()
         g = np.empty((6, self.total))
         gg = np.empty(self.ninst)
-        fw, aw = ctypes.c_long(), ctypes.c_long()
-        _check(lib().vg_batch_gradient(self._h, t.ctypes.data_as(D), cfl, steps, bias, limiter,
-                                       steps if checkpoints is None else checkpoints, ctypes.byref(L),
-                                       g.ctypes.data_as(D), gg.ctypes.data_as(D), ctypes.byref(fw), ctypes.byref(aw),
+        _check(lib().vg_batch_gradient(self._h, t.ctypes.data_as(ctypes.c_void_p), cfl, steps, bias, limiter, ck,
+                                       ctypes.byref(L), g.ctypes.data_as(ctypes.c_void_p),
+                                       gg.ctypes.data_as(ctypes.c_void_p), 0, ctypes.byref(fw), ctypes.byref(aw),
                                        stream))
         return L.value, g, gg, fw.value, aw.value

@@ -662,7 +662,8 @@ struct Reverser {
 
 extern "C" vg_status vg_batch_gradient(vg_batch* b, const double* target_rho, double cfl, int steps, double bias,
                                        int limiter, int checkpoints, double* loss, double* grad_planes,
-                                       double* grad_gamma, long* forward_steps, long* adjoint_steps, void* stream) {
+                                       double* grad_gamma, int is_device, long* forward_steps, long* adjoint_steps,
+                                       void* stream) {
     if (!b || !target_rho || steps < 1 || !(cfl > 0.0) || limiter < 0 || limiter > 2)
         return afail(VG_EINVAL, "bad vg_batch_gradient argument");
     if (checkpoints < 1) return afail(VG_EINVAL, "need at least one checkpoint slot (the initial state)");
@@ -672,7 +673,9 @@ extern "C" vg_status vg_batch_gradient(vg_batch* b, const double* target_rho, do
     VA_CUDA(ensure_workspace(b, checkpoints));
     const long n = b->total;
     const size_t sbytes = sizeof(double) * 3 * n;
-    VA_CUDA(cudaMemcpyAsync(b->d_target, target_rho, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+    const cudaMemcpyKind in_kind = is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    const cudaMemcpyKind out_kind = is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    VA_CUDA(cudaMemcpyAsync(b->d_target, target_rho, sizeof(double) * n, in_kind, st));
     VA_CUDA(cudaMemsetAsync(b->d_ggam, 0, sizeof(double) * b->ninst, st));
     VA_CUDA(cudaMemsetAsync(b->d_err, 0, sizeof(unsigned int), st));
 
@@ -708,13 +711,15 @@ extern "C" vg_status vg_batch_gradient(vg_batch* b, const double* target_rho, do
     const double* lam0 = b->lam[R.lam_cur];
     const int ref[3] = {0, 1, 4};
     for (int v = 0; v < 3 && e == cudaSuccess && grad_planes; v++)
-        e = cudaMemcpyAsync(grad_planes + ref[v] * n, lam0 + v * n, sizeof(double) * n, cudaMemcpyDeviceToHost, st);
+        e = cudaMemcpyAsync(grad_planes + ref[v] * n, lam0 + v * n, sizeof(double) * n, out_kind, st);
+    for (int v : {2, 3, 5})
+        if (e == cudaSuccess && grad_planes && is_device) e = cudaMemsetAsync(grad_planes + v * n, 0, sizeof(double) * n, st);
     if (e == cudaSuccess && grad_gamma)
-        e = cudaMemcpyAsync(grad_gamma, b->d_ggam, sizeof(double) * b->ninst, cudaMemcpyDeviceToHost, st);
+        e = cudaMemcpyAsync(grad_gamma, b->d_ggam, sizeof(double) * b->ninst, out_kind, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return afail(VG_ECUDA, std::string("vg_batch_gradient: ") + cudaGetErrorString(e));
     if (err) return afail(VG_ENAN, "non-finite or non-positive density/pressure produced");
-    if (grad_planes)
+    if (grad_planes && !is_device)
         for (long i = 0; i < n; i++) grad_planes[2 * n + i] = grad_planes[3 * n + i] = grad_planes[5 * n + i] = 0.0;
     if (loss) {
         double sum = 0.0;
