@@ -212,15 +212,27 @@ def run_cuda(args, world, rank, local):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    prm = wl.euler_params(1.4)
-    W0 = wl.euler_quadrants_2d(NX, NY, seed=SEED + rank)
     stream = torch.cuda.current_stream()
     sh = ctypes_stream(stream)
+    legs = [x for x in args.legs.split(",") if x]
+    if "headline" not in legs:  # profiling / diagnostic runs of single legs (not a bench line)
+        out = {}
+        for leg in legs:
+            out[leg] = LEGS[leg](local, stream, sh)
+        if rank == 0:
+            print(json.dumps({"legs": out}), flush=True)
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
+
+    prm = wl.euler_params(1.4)
+    W0 = wl.euler_quadrants_2d(NX, NY, seed=SEED + rank)
     dx = 1.0 / NX
 
     results = {}
-    forms = [("fp64", vg.FP64)]
-    if vg_mixed_available(vg):
+    wanted = args.forms.split(",")
+    forms = [("fp64", vg.FP64)] if "fp64" in wanted else []
+    if "mixed" in wanted and vg_mixed_available(vg):
         forms.append(("mixed", vg.MIXED))
     finals = {}
     for name, prec in forms:
@@ -294,7 +306,7 @@ def run_cuda(args, world, rank, local):
     peak, peak_kind = measured_peak()
     x_bytes = cells * BYTES_PER_CELL_SWEEP
     achieved = x_bytes / (r["x_sweep_ms"] / 1000.0) / 1e9
-    traffic = load_traffic()
+    traffic = load_traffic(best)
 
     if rank != 0:
         if dist is not None:
@@ -306,7 +318,8 @@ def run_cuda(args, world, rank, local):
         "vs_baseline": None, "dtype": "f64" if best == "fp64" else "f32+f64", "data": "synthetic",
         "config": dict(workload_config(), form=best),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "kernel": "sweep_x_kernel (X half-sweep)",
+                     "traffic": traffic,
+                     "kernel": ("sweep_x_mixed_kernel" if best == "mixed" else "sweep_x_kernel") + " (X half-sweep)",
                      "algorithmic_bytes_per_launch": x_bytes, "peak_source": peak_kind},
         "e2e": {"value": world * cells * args.steps / e2e_s, "unit": UNIT,
                 "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
@@ -323,10 +336,10 @@ def run_cuda(args, world, rank, local):
         d = np.abs(finals["mixed"][0] - finals["fp64"][0])
         line["mixed_error_vs_fp64"] = {"rho_L1": float(d.mean()), "rho_Linf": float(d.max()),
                                        "reference": "the FP64 CUDA form, bitwise equal to the oracle"}
-    if not args.headline_only:
-        line["configs"] = {"C5_ragged_batch_adjoint": ragged_adjoint_leg(local, stream, sh),
-                           "C3_mhd_2048": mhd_leg(local, stream, sh),
-                           "C1_sod_1000": sod_leg(local, stream, sh)}
+    names = {"c5": "C5_ragged_batch_adjoint", "c3": "C3_mhd_2048", "c1": "C1_sod_1000"}
+    extra = {names[leg]: LEGS[leg](local, stream, sh) for leg in legs if leg in names}
+    if extra:
+        line["configs"] = extra
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample()
     print(json.dumps(line), flush=True)
@@ -448,6 +461,11 @@ def sod_leg(local, stream, sh):
             "cell_updates_per_s": 1000 * it / sec}
 
 
+LEGS = {"c5": lambda l, st, sh: ragged_adjoint_leg(l, st, sh),
+        "c3": lambda l, st, sh: mhd_leg(l, st, sh),
+        "c1": lambda l, st, sh: sod_leg(l, st, sh)}
+
+
 def ctypes_stream(stream):
     import ctypes
     return ctypes.c_void_p(stream.cuda_stream)
@@ -468,12 +486,12 @@ def mixed_ok(finals):
     return float(np.abs(finals["mixed"][0] - finals["fp64"][0]).mean()) <= 1e-6
 
 
-def load_traffic():
-    """DRAM bytes per X-sweep launch from the committed ncu summary, if present."""
+def load_traffic(form):
+    """DRAM bytes per X-sweep launch of `form` at the bench size, from the committed ncu summaries, if present."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     try:
         with open(p) as f:
-            return json.load(f).get("sweep_x_kernel_fp64_bytes_per_launch")
+            return json.load(f).get(f"sweep_x_kernel_{form}_bytes_per_launch")
     except Exception:
         return None
 
@@ -486,12 +504,20 @@ def main():
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--headline-only", action="store_true", help="skip the C1/C3/C5 measurements")
+    ap.add_argument("--legs", default="headline,c5,c3,c1",
+                    help="comma list of headline (C2), c5, c3, c1; without headline only those legs run (profiling)")
+    ap.add_argument("--forms", default="fp64,mixed", help="C2 forms to run (profiling)")
+    ap.add_argument("--c5-ninst", type=int, default=4096, help="C5 instances (smaller is for profiling only)")
+    ap.add_argument("--c5-steps", type=int, default=500, help="C5 steps (smaller is for profiling only)")
     ap.add_argument("--nx", type=int, default=4096, help="grid size (smaller grids are for profiling only)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    global NX, NY
+    global NX, NY, C5_NINST, C5_STEPS
     NX = NY = args.nx
+    C5_NINST, C5_STEPS = args.c5_ninst, args.c5_steps
+    if args.headline_only:
+        args.legs = "headline"
     world, rank, local = dist_setup()
     if args.impl == "reference":
         return run_reference(args, world, rank)

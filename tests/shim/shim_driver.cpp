@@ -3,7 +3,8 @@
 // planes to a binary file for tests/test_shim_gpu.py to compare with the oracle.
 //   shim_driver <out.bin>
 // Output, in order (float64): Euler 1D solve (6 x 200), Euler 2D per-sweep loop (6 x 24 x 20),
-// MHD solve2D (9 x 16 x 16), HPR solve (17 x 50), then the number of 2D steps the per-sweep loop took.
+// MHD solve2D (9 x 16 x 16), HPR solve (17 x 50), Euler 1D step-count solve (6 x 150), then the number of 2D
+// steps the per-sweep loop took.
 #include <cmath>
 #include <cstdio>
 #include <vector>
@@ -94,6 +95,19 @@ int main(int argc, char** argv) {
         vector<double> v;
         for (int k = 0; k < 17; k++)
             for (auto& c : out) v.push_back(c.data()[k]);
+        put(f, v);
+    }
+    // 5) the step-count overload: SecondOrderSolver::solve(..., maxSteps) with no end time, superbee, 37 steps
+    {
+        int n = 150;
+        vector<EulerStateVector> cells(n);
+        EulerMaterialParameters mp(1.4);
+        for (int i = 0; i < n; i++)
+            cells[i] = i <= 0.5 * n ? EulerStateVector(1.0, 0.0, 0.0, 0.0, 1.0) : EulerStateVector(0.125, 0.0, 0.0, 0.0, 0.1);
+        vector<EulerStateVector> out = SecondOrderSolver::solve(cells, 1.0 / n, 0.8, 0.0, 0.0, 0, 0, mp, 37);
+        vector<double> v;
+        for (int k = 0; k < 6; k++)
+            for (auto& c : out) v.push_back(c.computePrimitiveVariableVector()[k]);
         put(f, v);
     }
     double st = steps;

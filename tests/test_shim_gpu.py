@@ -76,5 +76,11 @@ def test_shim_driver_matches_oracle(gpu, oracle_lib, tmp_path):
     O.run(O.HPR, ref, 1 / 50, 0.8, t_end=0.02, limiter=0, params=prm, subcycles=1)
     assert _rel(got, ref) <= 1e-12
 
+    # 5) the step-count overload solve(..., maxSteps = 37) with no end time
+    got = take((6, 150))
+    ref = wl.sod_1d(150)
+    O.run(O.EULER, ref, 1 / 150, 0.8, steps=37, limiter=0, params=wl.euler_params(1.4))
+    assert np.array_equal(got, ref)
+
     assert take((1,))[0] == 6
     assert off == data.size

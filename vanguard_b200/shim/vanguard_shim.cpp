@@ -67,14 +67,15 @@ vg_solver* cached_solver(int model, int nx, int ny, int boundary, const double* 
 }
 
 // Runs solve()/solve2D()'s time loop (finalTime-driven) on reference-order primitive planes, in place.
+// maxSteps > 0 also stops the loop after that many steps (the shim's step-count overloads).
 void run_planes(int model, std::vector<double>& planes, int nx, int ny, const double* params, int nparams, double dx,
-                double cfl, double tEnd, double bias, int limiter, int subcycles) {
+                double cfl, double tEnd, double bias, int limiter, int subcycles, int maxSteps = 0) {
     SolverPtr s = make_solver(model, nx, ny, VG_TRANSMISSIVE, params, nparams);
     vg_run_config c{};
     c.dx = dx;
     c.cfl = cfl;
     c.t_end = tEnd;
-    c.max_steps = 0;
+    c.max_steps = maxSteps;
     c.bias = bias;
     c.limiter = limiter;
     c.subcycles = subcycles;
@@ -487,22 +488,31 @@ void SecondOrderSolver::computeYSLICTimeStep2D(vector<vector<EulerStateVector> >
     sweep2d(VG_MODEL_EULER, 6, cells, withB, 1, dx, dt, bias, limiter, prm, 6, euler_get, euler_make);
 }
 vector<EulerStateVector> SecondOrderSolver::solve(vector<EulerStateVector>& initialCells, double dx, double cfl, double tEnd,
+                                                  double bias, int limiter, int subcycles, EulerMaterialParameters mp) {
+    return solve(initialCells, dx, cfl, tEnd, bias, limiter, subcycles, mp, 0);
+}
+vector<EulerStateVector> SecondOrderSolver::solve(vector<EulerStateVector>& initialCells, double dx, double cfl, double tEnd,
                                                   double bias, int limiter, int /*subcycles: no source in the Euler model*/,
-                                                  EulerMaterialParameters mp) {
+                                                  EulerMaterialParameters mp, int maxSteps) {
     double prm[6];
     euler_params(mp, prm);
     std::vector<double> p = pack(initialCells, 6, euler_get);
-    run_planes(VG_MODEL_EULER, p, (int)initialCells.size(), 1, prm, 6, dx, cfl, tEnd, bias, limiter, 0);
+    run_planes(VG_MODEL_EULER, p, (int)initialCells.size(), 1, prm, 6, dx, cfl, tEnd, bias, limiter, 0, maxSteps);
     return unpack<EulerStateVector>(p, initialCells.size(), 6, euler_make);
 }
 vector<vector<EulerStateVector> > SecondOrderSolver::solve2D(vector<vector<EulerStateVector> >& initialCells, double dx,
-                                                             double cfl, double tEnd, double bias, int limiter, int,
+                                                             double cfl, double tEnd, double bias, int limiter, int subcycles,
                                                              EulerMaterialParameters mp) {
+    return solve2D(initialCells, dx, cfl, tEnd, bias, limiter, subcycles, mp, 0);
+}
+vector<vector<EulerStateVector> > SecondOrderSolver::solve2D(vector<vector<EulerStateVector> >& initialCells, double dx,
+                                                             double cfl, double tEnd, double bias, int limiter, int,
+                                                             EulerMaterialParameters mp, int maxSteps) {
     double prm[6];
     euler_params(mp, prm);
     std::vector<double> p = pack2(initialCells, 6, euler_get);
     long ny = initialCells.size(), nx = initialCells[0].size();
-    run_planes(VG_MODEL_EULER, p, (int)nx, (int)ny, prm, 6, dx, cfl, tEnd, bias, limiter, 0);
+    run_planes(VG_MODEL_EULER, p, (int)nx, (int)ny, prm, 6, dx, cfl, tEnd, bias, limiter, 0, maxSteps);
     return unpack2<EulerStateVector>(p, nx, ny, 6, euler_make);
 }
 
@@ -521,41 +531,61 @@ void MHDSecondOrderSolver::computeYSLICTimeStep2D(vector<vector<MHDStateVector> 
 }
 vector<MHDStateVector> MHDSecondOrderSolver::solve(vector<MHDStateVector>& initialCells, double dx, double cfl, double tEnd,
                                                    double bias, int limiter, int subcycles, MHDMaterialParameters mp) {
+    return solve(initialCells, dx, cfl, tEnd, bias, limiter, subcycles, mp, 0);
+}
+vector<MHDStateVector> MHDSecondOrderSolver::solve(vector<MHDStateVector>& initialCells, double dx, double cfl, double tEnd,
+                                                   double bias, int limiter, int subcycles, MHDMaterialParameters mp,
+                                                   int maxSteps) {
     if (subcycles != 0) throw std::runtime_error("MHD GLM damping sub-cycles are not available on the GPU path");
     double prm[3];
     mhd_params(mp, prm);
     std::vector<double> p = pack(initialCells, 9, mhd_get);
-    run_planes(VG_MODEL_MHD, p, (int)initialCells.size(), 1, prm, 3, dx, cfl, tEnd, bias, limiter, 0);
+    run_planes(VG_MODEL_MHD, p, (int)initialCells.size(), 1, prm, 3, dx, cfl, tEnd, bias, limiter, 0, maxSteps);
     return unpack<MHDStateVector>(p, initialCells.size(), 9, mhd_make);
 }
 vector<vector<MHDStateVector> > MHDSecondOrderSolver::solve2D(vector<vector<MHDStateVector> >& initialCells, double dx, double cfl,
                                                               double tEnd, double bias, int limiter, int subcycles,
                                                               MHDMaterialParameters mp) {
+    return solve2D(initialCells, dx, cfl, tEnd, bias, limiter, subcycles, mp, 0);
+}
+vector<vector<MHDStateVector> > MHDSecondOrderSolver::solve2D(vector<vector<MHDStateVector> >& initialCells, double dx, double cfl,
+                                                              double tEnd, double bias, int limiter, int subcycles,
+                                                              MHDMaterialParameters mp, int maxSteps) {
     if (subcycles != 0) throw std::runtime_error("MHD GLM damping sub-cycles are not available on the GPU path");
     double prm[3];
     mhd_params(mp, prm);
     std::vector<double> p = pack2(initialCells, 9, mhd_get);
     long ny = initialCells.size(), nx = initialCells[0].size();
-    run_planes(VG_MODEL_MHD, p, (int)nx, (int)ny, prm, 3, dx, cfl, tEnd, bias, limiter, 0);
+    run_planes(VG_MODEL_MHD, p, (int)nx, (int)ny, prm, 3, dx, cfl, tEnd, bias, limiter, 0, maxSteps);
     return unpack2<MHDStateVector>(p, nx, ny, 9, mhd_make);
 }
 
 // --------------------------------------------------------------------------------------------- HPR solver
 vector<HPRStateVector> HPRSecondOrderSolver::solve(vector<HPRStateVector>& initialCells, double dx, double cfl, double tEnd,
                                                    double bias, int limiter, int subcycles, HPRMaterialParameters mp) {
+    return solve(initialCells, dx, cfl, tEnd, bias, limiter, subcycles, mp, 0);
+}
+vector<HPRStateVector> HPRSecondOrderSolver::solve(vector<HPRStateVector>& initialCells, double dx, double cfl, double tEnd,
+                                                   double bias, int limiter, int subcycles, HPRMaterialParameters mp,
+                                                   int maxSteps) {
     double prm[12];
     hpr_params(mp, prm);
     std::vector<double> p = pack(initialCells, 17, hpr_get);
-    run_planes(VG_MODEL_HPR, p, (int)initialCells.size(), 1, prm, 12, dx, cfl, tEnd, bias, limiter, subcycles);
+    run_planes(VG_MODEL_HPR, p, (int)initialCells.size(), 1, prm, 12, dx, cfl, tEnd, bias, limiter, subcycles, maxSteps);
     return unpack<HPRStateVector>(p, initialCells.size(), 17, hpr_make);
 }
 vector<vector<HPRStateVector> > HPRSecondOrderSolver::solve2D(vector<vector<HPRStateVector> >& initialCells, double dx, double cfl,
                                                               double tEnd, double bias, int limiter, int subcycles,
                                                               HPRMaterialParameters mp) {
+    return solve2D(initialCells, dx, cfl, tEnd, bias, limiter, subcycles, mp, 0);
+}
+vector<vector<HPRStateVector> > HPRSecondOrderSolver::solve2D(vector<vector<HPRStateVector> >& initialCells, double dx, double cfl,
+                                                              double tEnd, double bias, int limiter, int subcycles,
+                                                              HPRMaterialParameters mp, int maxSteps) {
     double prm[12];
     hpr_params(mp, prm);
     std::vector<double> p = pack2(initialCells, 17, hpr_get);
     long ny = initialCells.size(), nx = initialCells[0].size();
-    run_planes(VG_MODEL_HPR, p, (int)nx, (int)ny, prm, 12, dx, cfl, tEnd, bias, limiter, subcycles);
+    run_planes(VG_MODEL_HPR, p, (int)nx, (int)ny, prm, 12, dx, cfl, tEnd, bias, limiter, subcycles, maxSteps);
     return unpack2<HPRStateVector>(p, nx, ny, 17, hpr_make);
 }

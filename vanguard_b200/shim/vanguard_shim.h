@@ -258,6 +258,13 @@ public:
     static vector<vector<EulerStateVector> > solve2D(vector<vector<EulerStateVector> >& initialCells, double cellSpacing,
                                                      double CFLCofficient, double finalTime, double bias, int slopeLimiter,
                                                      int subcyclingIterations, EulerMaterialParameters mp);
+    // step-count overloads (not in the reference): also stop after maxSteps steps when maxSteps > 0
+    static vector<EulerStateVector> solve(vector<EulerStateVector>& initialCells, double cellSpacing, double CFLCoefficient,
+                                          double finalTime, double bias, int slopeLimiter, int subcyclingIterations,
+                                          EulerMaterialParameters mp, int maxSteps);
+    static vector<vector<EulerStateVector> > solve2D(vector<vector<EulerStateVector> >& initialCells, double cellSpacing,
+                                                     double CFLCofficient, double finalTime, double bias, int slopeLimiter,
+                                                     int subcyclingIterations, EulerMaterialParameters mp, int maxSteps);
 };
 
 class MHDSecondOrderSolver {
@@ -274,6 +281,12 @@ public:
     static vector<vector<MHDStateVector> > solve2D(vector<vector<MHDStateVector> >& initialCells, double cellSpacing,
                                                    double CFLCoefficient, double finalTime, double bias, int slopeLimiter,
                                                    int subcyclingIterations, MHDMaterialParameters mp);
+    static vector<MHDStateVector> solve(vector<MHDStateVector>& initialCells, double cellSpacing, double CFLCoefficient,
+                                        double finalTime, double bias, int slopeLimiter, int subcyclingIterations,
+                                        MHDMaterialParameters mp, int maxSteps);
+    static vector<vector<MHDStateVector> > solve2D(vector<vector<MHDStateVector> >& initialCells, double cellSpacing,
+                                                   double CFLCoefficient, double finalTime, double bias, int slopeLimiter,
+                                                   int subcyclingIterations, MHDMaterialParameters mp, int maxSteps);
 };
 
 class HPRSecondOrderSolver {
@@ -284,4 +297,10 @@ public:
     static vector<vector<HPRStateVector> > solve2D(vector<vector<HPRStateVector> >& initialCells, double cellSpacing,
                                                    double CFLCoefficient, double finalTime, double bias, int slopeLimiter,
                                                    int subcyclingIterations, HPRMaterialParameters mp);
+    static vector<HPRStateVector> solve(vector<HPRStateVector>& initialCells, double cellSpacing, double CFLCoefficient,
+                                        double finalTime, double bias, int slopeLimiter, int subcyclingIterations,
+                                        HPRMaterialParameters mp, int maxSteps);
+    static vector<vector<HPRStateVector> > solve2D(vector<vector<HPRStateVector> >& initialCells, double cellSpacing,
+                                                   double CFLCoefficient, double finalTime, double bias, int slopeLimiter,
+                                                   int subcyclingIterations, HPRMaterialParameters mp, int maxSteps);
 };
