@@ -332,7 +332,7 @@ def run_cuda(args, world, rank, local):
                       "hbm_frac_of_step": world * cells * args.steps * BYTES_PER_CELL_UPDATE / (v["ms"] / 1000.0) / 1e9 / peak}
                   for k, v in results.items()},
     }
-    if "mixed" in finals:
+    if "mixed" in finals and "fp64" in finals:
         d = np.abs(finals["mixed"][0] - finals["fp64"][0])
         line["mixed_error_vs_fp64"] = {"rho_L1": float(d.mean()), "rho_Linf": float(d.max()),
                                        "reference": "the FP64 CUDA form, bitwise equal to the oracle"}
@@ -397,7 +397,7 @@ def ragged_adjoint_leg(local, stream, sh, reps=3):
             ms = e0.elapsed_time(e1)
             out[f"adjoint_{name}"] = {"checkpoints": ck, "ms": ms, "ratio_vs_forward": ms / fwd_ms,
                                       "forward_steps": fw, "reversed_steps": aw, "loss": L,
-                                      "state_slot_bytes": (ck + 1) * 3 * total * 8}
+                                      "state_slot_bytes": (min(ck, C5_STEPS) + 1) * 3 * total * 8}
         # through the host-buffer API: target up, gradient planes and gamma gradient down, inside the timed region
         b.upload(W0, stream=sh)
         torch.cuda.synchronize()
@@ -483,6 +483,8 @@ def vg_mixed_available(vg):
 def mixed_ok(finals):
     if "mixed" not in finals:
         return False
+    if "fp64" not in finals:  # a profiling run of the mixed form alone
+        return True
     return float(np.abs(finals["mixed"][0] - finals["fp64"][0]).mean()) <= 1e-6
 
 
