@@ -108,6 +108,42 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(mhz)}
 
 
+class RankGroup:
+    """One process per GPU (torchrun): the barrier and the max over ranks of the timing protocol.  NCCL on the
+    GPUs; the same code runs with gloo on CPU tensors in the multi-process tests.  world == 1 needs no group."""
+
+    def __init__(self, world, rank, backend, device):
+        self.world, self.rank, self.device, self.dist = world, rank, device, None
+        if world > 1:
+            import datetime
+            import torch.distributed as dist
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+            self.dist = dist
+
+    def barrier(self):
+        if self.dist is not None:
+            self.dist.barrier()
+
+    def max(self, x):
+        """The largest x over all ranks (every rank calls it, in the same order)."""
+        if self.dist is None:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.dist is not None:
+            self.dist.destroy_process_group()
+            self.dist = None
+
+
+def job_value(world, units_per_rank, slowest_seconds):
+    """Whole-job throughput of `world` replicas that each processed units_per_rank, timed by the slowest rank."""
+    return world * units_per_rank / slowest_seconds
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -195,22 +231,8 @@ def run_cuda(args, world, rank, local):
     from vanguard_b200 import workloads as wl
 
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    group = RankGroup(world, rank, "nccl", f"cuda:{local}")
+    barrier, max_over_ranks = group.barrier, group.max
 
     stream = torch.cuda.current_stream()
     sh = ctypes_stream(stream)
@@ -221,8 +243,7 @@ def run_cuda(args, world, rank, local):
             out[leg] = LEGS[leg](local, stream, sh)
         if rank == 0:
             print(json.dumps({"legs": out}), flush=True)
-        if dist is not None:
-            dist.destroy_process_group()
+        group.close()
         return 0
 
     prm = wl.euler_params(1.4)
@@ -302,15 +323,14 @@ def run_cuda(args, world, rank, local):
 
     r = results[best]
     cells = NX * NY
-    value = world * cells * args.steps / (r["ms"] / 1000.0)
+    value = job_value(world, cells * args.steps, r["ms"] / 1000.0)
     peak, peak_kind = measured_peak()
     x_bytes = cells * BYTES_PER_CELL_SWEEP
     achieved = x_bytes / (r["x_sweep_ms"] / 1000.0) / 1e9
     traffic = load_traffic(best)
 
     if rank != 0:
-        if dist is not None:
-            dist.destroy_process_group()
+        group.close()
         return 0
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -321,7 +341,7 @@ def run_cuda(args, world, rank, local):
                      "traffic": traffic,
                      "kernel": ("sweep_x_mixed_kernel" if best == "mixed" else "sweep_x_kernel") + " (X half-sweep)",
                      "algorithmic_bytes_per_launch": x_bytes, "peak_source": peak_kind},
-        "e2e": {"value": world * cells * args.steps / e2e_s, "unit": UNIT,
+        "e2e": {"value": job_value(world, cells * args.steps, e2e_s), "unit": UNIT,
                 "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                 "api": "vg_solve (pinned host buffers; one upload + K steps + one download per call)"},
         "gpu_launches": r["launches"],
@@ -343,8 +363,7 @@ def run_cuda(args, world, rank, local):
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample()
     print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.destroy_process_group()
+    group.close()
     return 0
 
 
