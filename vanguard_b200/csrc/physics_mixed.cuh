@@ -55,7 +55,7 @@ struct EulerMixed {
     };
     __device__ static P params(const double* prm, double /*ch*/) {
         double g = prm[0], pinf = prm[1];
-        return P{g - 1.0, 1.0 / (g - 1.0), g * pinf, g, pinf, 0.0};
+        return P{g - 1.0, prm[15], g * pinf, g, pinf, 0.0};
     }
     // W -> U in FP64: E = rho |v|^2 / 2 + (p + gamma p_inf) / (gamma - 1)
     __device__ static void cons(const double* W, const P& q, double* U) {
@@ -126,7 +126,7 @@ struct MHDMixed {
     };
     __device__ static P params(const double* prm, double ch) {
         double g = prm[0], pinf = prm[1];
-        return P{g - 1.0, 1.0 / (g - 1.0), g * pinf, g, pinf, ch * ch};
+        return P{g - 1.0, prm[15], g * pinf, g, pinf, ch * ch};
     }
     __device__ static double sq3(double a, double b, double c) {
         if constexpr (FULL) return fma(a, a, fma(b, b, c * c));

@@ -99,11 +99,18 @@ __device__ __forceinline__ void force_flux(const double* ua, const double* ub, c
 }
 
 __device__ __forceinline__ SweepConst sweep_const(const SweepArgs& a, double& ts) {
-    ts = (a.ctrl ? a.ctrl->dt : a.dt_host) * a.dt_scale;
     SweepConst k;
-    k.r = ts / a.dx;
-    k.rinv = a.dx / ts;
-    k.half_r = 0.5 * (ts / a.dx);
+    if (a.ctrl) {
+        ts = a.ctrl->dt * a.dt_scale;
+        k.r = a.ctrl->kr[a.kslot];
+        k.rinv = a.ctrl->krinv[a.kslot];
+        k.half_r = a.ctrl->khalf_r[a.kslot];
+    } else {
+        ts = a.dt_host * a.dt_scale;
+        k.r = a.r_host;
+        k.rinv = a.rinv_host;
+        k.half_r = a.half_r_host;
+    }
     k.cm = 0.5 * (1.0 + a.bias);
     k.cp = 0.5 * (1.0 - a.bias);
     k.bias = a.bias;
@@ -329,6 +336,12 @@ __global__ void step_begin_kernel(Ctrl* c, SweepArgs a) {
         if ((c->t + dt) > c->t_end) dt = c->t_end - c->t;
         c->dt = dt;
         c->ch = S;
+        for (int i = 0; i < 2; i++) {
+            sweep_scale(dt * (i == 0 ? 0.5 : 1.0), c->dx, c->kr[i], c->krinv[i], c->khalf_r[i]);
+            c->kr_f[i] = (float)c->kr[i];
+            c->krinv_f[i] = (float)c->krinv[i];
+            c->khalf_r_f[i] = (float)c->khalf_r[i];
+        }
     }
     c->smax_next = 0ull;
 }

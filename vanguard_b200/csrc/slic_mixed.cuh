@@ -31,12 +31,20 @@ struct MixedConst {
 };
 
 __device__ __forceinline__ MixedConst mixed_const(const SweepArgs& a, double& ts) {
-    ts = (a.ctrl ? a.ctrl->dt : a.dt_host) * a.dt_scale;
     MixedConst k;
-    k.r = ts / a.dx;
-    k.r_f = (float)k.r;
-    k.rinv_f = (float)(a.dx / ts);
-    k.half_r = (float)(0.5 * k.r);
+    if (a.ctrl) {
+        ts = a.ctrl->dt * a.dt_scale;
+        k.r = a.ctrl->kr[a.kslot];
+        k.r_f = a.ctrl->kr_f[a.kslot];
+        k.rinv_f = a.ctrl->krinv_f[a.kslot];
+        k.half_r = a.ctrl->khalf_r_f[a.kslot];
+    } else {
+        ts = a.dt_host * a.dt_scale;
+        k.r = a.r_host;
+        k.r_f = a.r_host_f;
+        k.rinv_f = a.rinv_host_f;
+        k.half_r = a.half_r_host_f;
+    }
     k.cm = 0.5 * (1.0 + a.bias);
     k.cp = 0.5 * (1.0 - a.bias);
     k.bias = a.bias;

@@ -85,7 +85,21 @@ namespace {
 
 constexpr int kChunk = 16;  // steps per captured chunk (even: a chunk returns to buffer 0 in 1D and 2D)
 
-cudaError_t run_sweep(const vg_solver* s, int axis, const SweepArgs& a, cudaStream_t st) {
+// Per-launch constants of a sweep: the ctrl slot of its length and, for a host-given dt, r / rinv / half_r.
+SweepArgs prepared(const SweepArgs& a0) {
+    SweepArgs a = a0;
+    a.kslot = a.dt_scale == 0.5 ? 0 : 1;
+    if (!a.ctrl) {
+        vg::sweep_scale(a.dt_host * a.dt_scale, a.dx, a.r_host, a.rinv_host, a.half_r_host);
+        a.r_host_f = (float)a.r_host;
+        a.rinv_host_f = (float)a.rinv_host;
+        a.half_r_host_f = (float)a.half_r_host;
+    }
+    return a;
+}
+
+cudaError_t run_sweep(const vg_solver* s, int axis, const SweepArgs& a0, cudaStream_t st) {
+    const SweepArgs a = prepared(a0);
     return axis == 0 ? s->ops->x[s->xcfg](a, st) : s->ops->y[s->ycfg](a, st);
 }
 
@@ -150,7 +164,8 @@ SweepArgs base_args(const vg_solver* s) {
     a.dims = s->dims;
     a.wave_acc = &s->ctrl->smax_next;
     a.err = &s->ctrl->err;
-    for (int i = 0; i < VG_MAX_PARAMS; i++) a.params[i] = s->d.params[i];
+    for (int i = 0; i < VG_MAX_PARAMS - 1; i++) a.params[i] = s->d.params[i];
+    a.params[VG_MAX_PARAMS - 1] = 1.0 / (s->d.params[0] - 1.0);
     a.ch_host = s->d.params[2];
     return a;
 }
@@ -600,6 +615,7 @@ vg_status vg_autotune(vg_solver* s, const vg_run_config* cfg, int reps, float* t
     a.limiter = cfg->limiter;
     a.in = s->buf[s->cur];
     a.out = s->buf[1 - s->cur];
+    a = prepared(a);
     cudaEvent_t e0, e1;
     VG_CUDA(cudaEventCreate(&e0));
     VG_CUDA(cudaEventCreate(&e1));

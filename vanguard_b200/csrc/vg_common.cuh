@@ -23,6 +23,10 @@ struct Ctrl {
     unsigned int err;                // bit 0: non-finite or non-positive density / pressure written
     int dims;                        // 1 or 2
     int pad;
+    // sweep constants of this step, computed once by step_begin for the two sweep lengths dt/2 (slot 0) and
+    // dt (slot 1): ts / dx, dx / ts, 0.5 * (ts / dx), and their float roundings
+    double kr[2], krinv[2], khalf_r[2];
+    float kr_f[2], krinv_f[2], khalf_r_f[2];
 };
 
 enum : unsigned int { ERR_STATE = 1u };
@@ -68,6 +72,9 @@ struct SweepArgs {
     Ctrl* ctrl;              // device control block, or null for a host-given dt
     double dt_host;          // time step when ctrl == null
     double dt_scale;         // 0.5 for the X half sweeps of a 2D step, else 1
+    int kslot;               // ctrl->kr[] slot of dt_scale (0: 0.5, 1: 1.0)
+    double r_host, rinv_host, half_r_host;  // the same constants for ctrl == null (set by the host)
+    float r_host_f, rinv_host_f, half_r_host_f;
     double ch_host;          // MHD c_h when ctrl == null
     double dx;
     double bias;
@@ -78,8 +85,16 @@ struct SweepArgs {
     int dims;                // 1 or 2 (selects the wave-speed formula)
     unsigned long long* wave_acc;  // running maximum (bit pattern), usually &ctrl->smax_next
     unsigned int* err;             // error word (always valid)
-    double params[16];       // model parameters (model-specific layout)
+    double params[16];       // model parameters (model-specific layout); params[15] = 1 / (params[0] - 1)
 };
+
+// Sweep constants of one sweep of length ts = dt * scale, formed as the reference forms them
+// (Solvers/solvers.cpp:606-609, Solvers/firstordersolver.cpp:79-85): one place for the device and the host.
+__host__ __device__ __forceinline__ void sweep_scale(double ts, double dx, double& r, double& rinv, double& half_r) {
+    r = ts / dx;
+    rinv = dx / ts;
+    half_r = 0.5 * (ts / dx);
+}
 
 __device__ __forceinline__ void atomic_max_nonneg(unsigned long long* addr, double v) {
     atomicMax(addr, (unsigned long long)__double_as_longlong(v));
