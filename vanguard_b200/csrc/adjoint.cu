@@ -190,6 +190,7 @@ __global__ void __launch_bounds__(AP, 4) adjoint_step_kernel(AdjArgs a) {
     // stage-aliased shared arrays: Us -> UL, Ea -> AB, Eb -> BB, Fs -> US
     __shared__ double S0[3][AP], S1[3][AP], S2[3][AP], S3[3][AP], MU[3][AP], UR[3][AP];
     __shared__ double red[2][AP / 32];
+    __shared__ double tile_k[4];  // dt/dx, dx/dt, 1/(gamma - 1) of the tile's instance, formed by one thread
     auto& Us = S0;
     auto& UL = S0;
     auto& Ea = S1;
@@ -210,11 +211,13 @@ __global__ void __launch_bounds__(AP, 4) adjoint_step_kernel(AdjArgs a) {
         const bool owns_last = s0 <= n - 1 && n - 1 < s0 + AOUT;  // tile owning cell n-1
         const double dxk = a.dx[k];
         const double Sk = __longlong_as_double((long long)a.S[k]);
-        const double dt = step_dt(a.cfl, dxk, Sk, a.step);
+        if (p == 0) {
+            const double dt = step_dt(a.cfl, dxk, Sk, a.step);
+            tile_k[0] = xdiv(dt, dxk);
+            tile_k[1] = dxk / dt;
+            tile_k[2] = 1.0 / (a.gam[2 * k] - 1.0);
+        }
         K kc;
-        kc.r = xdiv(dt, dxk);
-        kc.rinv = dxk / dt;
-        kc.half_r = 0.5 * kc.r;
         kc.cm = 0.5 * (1.0 + a.bias);
         kc.cp = 0.5 * (1.0 - a.bias);
         kc.bias = a.bias;
@@ -224,7 +227,6 @@ __global__ void __launch_bounds__(AP, 4) adjoint_step_kernel(AdjArgs a) {
         q.g = a.gam[2 * k];
         q.pinf = a.gam[2 * k + 1];
         q.gm1 = q.g - 1.0;
-        q.igm1 = 1.0 / q.gm1;
         q.gpinf = q.g * q.pinf;
         // stage A: conserved vectors of every position (ghosts by the transmissive mirror); the adjoint input of
         // the cells reverse 1 needs is loaded here so its latency hides behind stages B and C
@@ -246,6 +248,10 @@ __global__ void __launch_bounds__(AP, 4) adjoint_step_kernel(AdjArgs a) {
             if ((p & 31) == 0 && m != 0xffffffffu) atomicMin(&a.arg[k], (int)m);
         }
         __syncthreads();
+        kc.r = tile_k[0];
+        kc.rinv = tile_k[1];
+        kc.half_r = 0.5 * kc.r;
+        q.igm1 = tile_k[2];
         // stage B: slopes (with their derivatives) and the evolved edge states of positions [1, AP-1)
         double xl[3], xr[3], dF[3], sdm[3], sdp[3], irl = 1.0, irr = 1.0;
         if (p >= 1 && p < AP - 1) {

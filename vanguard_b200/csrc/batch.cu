@@ -43,6 +43,7 @@ __global__ void __launch_bounds__(BP) batch_step_kernel(BatchArgs a) {
     __shared__ double Es[NU][BP];
     __shared__ double Fs[NU][BP];
     __shared__ double red[BP / 32];
+    __shared__ double tile_k[4];  // dt, dt/dx, dx/dt, 0.5 (dt/dx) of the tile's instance
     const int p = threadIdx.x;
     const int s = *a.step;
     const bool active = s < a.max_steps;
@@ -54,18 +55,22 @@ __global__ void __launch_bounds__(BP) batch_step_kernel(BatchArgs a) {
         const long base = a.offset[k];
         const int cell = s0 - 1 + p;
         const bool out_ok = p >= 1 && p <= BP - 2 && cell < len;
-        const double dt = instance_dt(a, k, s);
+        // the instance's step constants, formed once per tile by one thread and shared after the first barrier
+        if (p == 0) {
+            const double dt = instance_dt(a, k, s);
+            tile_k[0] = dt;
+            tile_k[1] = dt / a.dx[k];
+            tile_k[2] = a.dx[k] / dt;
+            tile_k[3] = 0.5 * (dt / a.dx[k]);
+            if (s0 == 0) a.dt_out[k] = dt;
+        }
         SweepConst kc;
-        kc.r = dt / a.dx[k];
-        kc.rinv = a.dx[k] / dt;
-        kc.half_r = 0.5 * (dt / a.dx[k]);
         kc.cm = 0.5 * (1.0 + a.bias);
         kc.cp = 0.5 * (1.0 - a.bias);
         kc.bias = a.bias;
         kc.floor5 = a.floor5;
         kc.limiter = a.limiter;
         M1::P q{a.gam[2 * k], a.gam[2 * k + 1], 0.0};
-        if (p == 0 && s0 == 0) a.dt_out[k] = dt;
 
         auto conserve = [&](int slot) {
             int c = ghost_index(s0 - 2 + slot, len, 0);
@@ -78,6 +83,9 @@ __global__ void __launch_bounds__(BP) batch_step_kernel(BatchArgs a) {
         if (p == 0) conserve(0);
         if (p == BP - 1) conserve(BP + 1);
         __syncthreads();
+        kc.r = tile_k[1];
+        kc.rinv = tile_k[2];
+        kc.half_r = tile_k[3];
         double ub[NU];
         {
             double uL[NU], u[NU], uR[NU], ua[NU];
@@ -125,15 +133,21 @@ __global__ void __launch_bounds__(BP) batch_step_kernel(BatchArgs a) {
         for (long i = blockIdx.x * (long)BP + threadIdx.x; i < a.plane; i += (long)gridDim.x * BP)
             for (int v = 0; v < NW; v++) a.out[v * a.plane + i] = a.in[v * a.plane + i];
     }
-    // the last block to finish advances the step and clears the slot the step after next will fill
+    // the last block to finish clears (with all its threads) the slot the step after next will fill and advances
+    // the step
+    __shared__ int last;
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
-        unsigned int prev = atomicAdd(a.done, 1u);
-        if (prev == gridDim.x - 1) {
-            __threadfence();
-            const int clear = ((s + 2) % 3) * a.ninst;
-            for (int k = 0; k < a.ninst; k++) a.smax[clear + k] = 0ull;
+        last = atomicAdd(a.done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last) {
+        const int clear = ((s + 2) % 3) * a.ninst;
+        for (int k = threadIdx.x; k < a.ninst; k += blockDim.x) a.smax[clear + k] = 0ull;
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) {
             if (active) *a.step = s + 1;
             *a.done = 0u;
             __threadfence();
