@@ -356,7 +356,7 @@ def run_cuda(args, world, rank, local):
         d = np.abs(finals["mixed"][0] - finals["fp64"][0])
         line["mixed_error_vs_fp64"] = {"rho_L1": float(d.mean()), "rho_Linf": float(d.max()),
                                        "reference": "the FP64 CUDA form, bitwise equal to the oracle"}
-    names = {"c5": "C5_ragged_batch_adjoint", "c3": "C3_mhd_2048", "c1": "C1_sod_1000"}
+    names = {"c5": "C5_ragged_batch_adjoint", "c4": "C4_hpr_1024", "c3": "C3_mhd_2048", "c1": "C1_sod_1000"}
     extra = {names[leg]: LEGS[leg](local, stream, sh) for leg in legs if leg in names}
     if extra:
         line["configs"] = extra
@@ -417,14 +417,26 @@ def ragged_adjoint_leg(local, stream, sh, reps=3):
             out[f"adjoint_{name}"] = {"checkpoints": ck, "ms": ms, "ratio_vs_forward": ms / fwd_ms,
                                       "forward_steps": fw, "reversed_steps": aw, "loss": L,
                                       "state_slot_bytes": (min(ck, C5_STEPS) + 1) * 3 * total * 8}
-        # through the host-buffer API: target up, gradient planes and gamma gradient down, inside the timed region
-        b.upload(W0, stream=sh)
+        # through the host-buffer API with pinned buffers, copies inside the timed region: the forward uploads the
+        # initial planes and downloads the final ones; the gradient uploads the initial planes and the target and
+        # downloads the gradient planes and the gamma gradient
+        pin = lambda shape: torch.empty(shape, dtype=torch.float64).pin_memory().numpy()
+        h_w0, h_out, h_tgt, h_g, h_gg = pin((6, total)), pin((6, total)), pin((total,)), pin((6, total)), pin((C5_NINST,))
+        h_w0[:] = W0
+        h_tgt[:] = target
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        b.gradient(target, CFL, C5_STEPS, limiter=LIMITER, checkpoints=C5_CKPT, stream=sh)
-        host_s = time.perf_counter() - t0
-        out["adjoint_binomial"]["e2e_ms"] = host_s * 1e3
-        out["adjoint_binomial"]["e2e_ratio_vs_forward"] = host_s * 1e3 / fwd_ms
+        b.upload(h_w0, stream=sh)
+        b.run(CFL, C5_STEPS, limiter=LIMITER, stream=sh)
+        b.download(out=h_out, stream=sh)
+        fwd_host_s = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        b.upload(h_w0, stream=sh)
+        b.gradient(h_tgt, CFL, C5_STEPS, limiter=LIMITER, checkpoints=C5_CKPT, out=(h_g, h_gg), stream=sh)
+        grad_host_s = time.perf_counter() - t0
+        out["forward"]["e2e_ms"] = fwd_host_s * 1e3
+        out["adjoint_binomial"]["e2e_ms"] = grad_host_s * 1e3
+        out["adjoint_binomial"]["e2e_ratio_vs_forward"] = grad_host_s / fwd_host_s
     return out
 
 
@@ -460,6 +472,47 @@ def mhd_leg(local, stream, sh, steps=500):
     return res
 
 
+C4_STEPS = 300
+
+
+def hpr_leg(local, stream, sh):
+    """C4: 2D HPR (GPR) 1024^2 smooth field (seeded), ideal gas via the stiffened-gas branch, thermal, tau1 and tau2
+    log-uniform on [1e-6, 1e-2] from the seed, superbee, CFL 0.8, C4_STEPS steps, exact FP64.  The relaxation source
+    runs as the reference runs it: the RK4 forcing solver with fractional-flux predictors, sub-cycled dt/(2 sub)
+    before and after the sweeps, with sub chosen so each sub-step stays inside the explicit RK4 stability bound
+    (0.5 dt / sub <= 2.5 min(tau1, tau2), dt estimated from the initial CFL speed with a 1.5x margin)."""
+    import math
+    import torch
+    import vanguard_b200 as vg
+    from vanguard_b200 import workloads as wl
+
+    n = 1024
+    tau1, tau2 = wl.hpr_relaxation_times(SEED)
+    prm = wl.hpr_params(tau1=tau1, tau2=tau2)
+    W = wl.hpr_smooth_2d(n, seed=SEED)
+    with vg.Solver(vg.HPR, n, n, prm, device=local) as s:
+        s.upload(W, stream=sh)
+        S0 = s.max_wave_speed(stream=sh)
+        dt_est = 1.5 * CFL * (1.0 / n) / S0
+        sub = max(1, math.ceil(0.5 * dt_est / (2.5 * min(tau1, tau2))))
+        s.autotune(1.0 / n, CFL, limiter=LIMITER, stream=sh)
+        s.run(1.0 / n, CFL, steps=2, limiter=LIMITER, subcycles=sub, stream=sh)
+        s.upload(W, stream=sh)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        t, it = s.run(1.0 / n, CFL, steps=C4_STEPS, limiter=LIMITER, subcycles=sub, stream=sh, allow_nan=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        fin = s.download(stream=sh)
+        launches = s.last_launch_count()
+    return {"workload": f"2D HPR {n}x{n} smooth field (seeded), thermal ideal gas, tau1 {tau1:.3e}, tau2 {tau2:.3e}, "
+                        f"superbee, CFL 0.8, {C4_STEPS} steps, RK4 forcing with {sub} sub-cycles per half step",
+            "subcycles": sub, "steps": it, "t": t, "ms": ms, "cell_updates_per_s": n * n * it / (ms / 1e3),
+            "launches": launches, "finite": bool(np.isfinite(fin).all()), "precision": "fp64"}
+
+
 def sod_leg(local, stream, sh):
     """C1: 1D Sod, 1000 cells, minbee, CFL 0.9, t_end 0.25 (time to solution, FP64)."""
     import torch
@@ -481,6 +534,7 @@ def sod_leg(local, stream, sh):
 
 
 LEGS = {"c5": lambda l, st, sh: ragged_adjoint_leg(l, st, sh),
+        "c4": lambda l, st, sh: hpr_leg(l, st, sh),
         "c3": lambda l, st, sh: mhd_leg(l, st, sh),
         "c1": lambda l, st, sh: sod_leg(l, st, sh)}
 
@@ -530,13 +584,14 @@ def main():
     ap.add_argument("--forms", default="fp64,mixed", help="C2 forms to run (profiling)")
     ap.add_argument("--c5-ninst", type=int, default=4096, help="C5 instances (smaller is for profiling only)")
     ap.add_argument("--c5-steps", type=int, default=500, help="C5 steps (smaller is for profiling only)")
+    ap.add_argument("--c4-steps", type=int, default=300, help="C4 steps (smaller is for profiling only)")
     ap.add_argument("--nx", type=int, default=4096, help="grid size (smaller grids are for profiling only)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    global NX, NY, C5_NINST, C5_STEPS
+    global NX, NY, C5_NINST, C5_STEPS, C4_STEPS
     NX = NY = args.nx
-    C5_NINST, C5_STEPS = args.c5_ninst, args.c5_steps
+    C5_NINST, C5_STEPS, C4_STEPS = args.c5_ninst, args.c5_steps, args.c4_steps
     if args.headline_only:
         args.legs = "headline"
     world, rank, local = dist_setup()

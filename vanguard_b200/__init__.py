@@ -271,8 +271,10 @@ class Batch:
         a = np.ascontiguousarray(planes, dtype=np.float64)
         return _check(lib().vg_batch_upload(self._h, a.ctypes.data_as(ctypes.c_void_p), 0, stream))
 
-    def download(self, stream=None):
-        a = np.empty((6, self.total))
+    def download(self, out=None, stream=None):
+        a = np.empty((6, self.total)) if out is None else out
+        if a.shape != (6, self.total) or a.dtype != np.float64 or not a.flags.c_contiguous:
+            raise ValueError(f"out must be a C-contiguous float64 array of shape (6, {self.total})")
         _check(lib().vg_batch_download(self._h, a.ctypes.data_as(ctypes.c_void_p), 0, stream))
         return a
 
@@ -289,7 +291,8 @@ class Batch:
         """Discrete adjoint of run(cfl, steps) from the current state for L = sum (rho(T) - target_rho)^2.
         Returns (L, dL/dW0 as (6, total) planes, dL/dgamma (ninst,), forward steps, reversed steps).
         checkpoints defaults to every state (no recomputation).  With torch CUDA tensors for target_rho and
-        out = (grad_planes (6, total), grad_gamma (ninst,)) everything stays on the device."""
+        out = (grad_planes (6, total), grad_gamma (ninst,)) everything stays on the device; with numpy arrays
+        (pinned ones for full copy speed) out receives the host result."""
         fw, aw = ctypes.c_long(), ctypes.c_long()
         L = ctypes.c_double()
         ck = steps if checkpoints is None else checkpoints
@@ -306,8 +309,10 @@ class Batch:
         t = np.ascontiguousarray(target_rho, dtype=np.float64)
         if t.shape != (self.total,):
             raise ValueError(f"target_rho must have shape ({self.total},)")
-        g = np.empty((6, self.total))
-        gg = np.empty(self.ninst)
+        g, gg = (np.empty((6, self.total)), np.empty(self.ninst)) if out is None else out
+        for x, shape in ((g, (6, self.total)), (gg, (self.ninst,))):
+            if x.shape != shape or x.dtype != np.float64 or not x.flags.c_contiguous:
+                raise ValueError(f"expected a C-contiguous float64 array of shape {shape}")
         _check(lib().vg_batch_gradient(self._h, t.ctypes.data_as(ctypes.c_void_p), cfl, steps, bias, limiter, ck,
                                        ctypes.byref(L), g.ctypes.data_as(ctypes.c_void_p),
                                        gg.ctypes.data_as(ctypes.c_void_p), 0, ctypes.byref(fw), ctypes.byref(aw),
