@@ -107,3 +107,24 @@ def test_hpr_golden_rk4(gpu):
               subcycles=int(z["subcycles"]))
         out = s.download()
     assert _rel(out, out_ref) <= REL
+
+
+def test_hpr_non_thermal_keeps_heat_flux(gpu, oracle_lib):
+    """A non-thermal material: J is not evolved, and setConservedVariableVector leaves it as the cell had it, so a
+    non-zero initial J must survive every sweep unchanged, bit for bit with the oracle."""
+    nx, ny = 30, 26
+    W = wl.hpr_smooth_2d(nx, ny, seed=17)
+    rng = np.random.default_rng(5)
+    W[14:17] = 0.1 * rng.standard_normal((3, ny, nx))
+    prm = wl.hpr_params(thermal=False)
+    ref = W.copy()
+    O.run(O.HPR, ref, 1.0 / nx, 0.8, steps=6, limiter=0, params=prm)
+    assert np.array_equal(ref[14:17], W[14:17])
+    for prec in (gpu.FP64, gpu.MIXED):
+        with gpu.Solver(gpu.HPR, nx, ny, prm, precision=prec) as s:
+            s.upload(W)
+            s.run(1.0 / nx, 0.8, steps=6, limiter=0)
+            out = s.download()
+        assert np.array_equal(out[14:17], W[14:17])
+        if prec == gpu.FP64:
+            _bitwise(out, ref)

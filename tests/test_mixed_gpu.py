@@ -108,3 +108,42 @@ def test_conservation_periodic(gpu, oracle_lib, precision, model):
     drift = np.abs(after[idx] - before[idx]) / scale
     print(f"model {model} precision {precision}: relative drift {drift}")
     assert drift.max() <= 1e-12
+
+
+@pytest.mark.parametrize("subcycles", [0, 2])
+def test_mixed_hpr_smooth(gpu, oracle_lib, subcycles):
+    """HPR mixed form: FP32 flux combinations, FP64 state, pressure recovery, acoustic-tensor CFL and relaxation
+    source; against the FP64 oracle (with the RK4 source sub-cycled when subcycles > 0)."""
+    nx, ny = 48, 40
+    W = wl.hpr_smooth_2d(nx, ny, seed=31)
+    prm = wl.hpr_params(tau1=1e-2, tau2=1e-2)
+    ref = W.copy()
+    O.run(O.HPR, ref, 1.0 / nx, 0.8, steps=20, limiter=0, params=prm, subcycles=subcycles)
+    with gpu.Solver(gpu.HPR, nx, ny, prm, precision=gpu.MIXED) as s:
+        s.upload(W)
+        s.run(1.0 / nx, 0.8, steps=20, limiter=0, subcycles=subcycles)
+        out = s.download()
+    l1, linf = _errors(out[0], ref[0])
+    print(f"hpr mixed sub{subcycles}: L1(rho) {l1:.3e}  Linf(rho) {linf:.3e}  L1(all) {np.abs(out - ref).mean():.3e}")
+    assert l1 <= L1_RHO
+    assert linf <= 1e-4
+    assert np.abs(out - ref).mean() <= 1e-6
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_hpr_conservation_periodic(gpu, oracle_lib, precision):
+    """Mass, momentum and total energy of HPR change by round-off only (the relaxation source moves only A and J)."""
+    nx, ny = 40, 36
+    W = wl.hpr_smooth_2d(nx, ny, seed=41)
+    prm = wl.hpr_params(tau1=1e-2, tau2=1e-2)
+    before = _totals(O.HPR, W, prm)
+    with gpu.Solver(gpu.HPR, nx, ny, prm, precision=precision, boundary=gpu.PERIODIC) as s:
+        s.upload(W)
+        s.run(1.0 / nx, 0.8, steps=12, limiter=0, subcycles=1)
+        out = s.download()
+    after = _totals(O.HPR, out, prm)
+    idx = [0, 1, 11, 12]
+    scale = np.abs(before[idx]).max()
+    drift = np.abs(after[idx] - before[idx]) / scale
+    print(f"hpr precision {precision}: relative drift {drift}")
+    assert drift.max() <= 1e-12

@@ -19,6 +19,7 @@
 // (half-step evolution increment, Lax-Friedrichs, Richtmyer and FORCE averages) runs in FP32.
 #pragma once
 
+#include "physics_hpr.cuh"
 #include "vg_common.cuh"
 
 namespace vg {
@@ -215,6 +216,32 @@ struct MHDMixed {
     }
     __device__ static double density(const double* W) { return W[0]; }
     __device__ static double pressure(const double* W) { return W[IP]; }
+};
+
+// ---------------------------------------------------------------------------------------------- HPR
+// HPR (GPR) in the mixed form.  The state and its conversions, the pressure recovered from total energy inside the
+// flux, the acoustic-tensor CFL speed and the relaxation source (run by the exact forcing kernel) are the exact
+// model's FP64 formulas (here compiled with FMA contraction); each flux value leaves in FP32 for the FP32
+// half-step and FORCE combinations.
+struct HPRMixed {
+    static constexpr int NW = 17;
+    static constexpr int NU = 17;
+    static constexpr bool HAS_Y = true;
+    using P = HPRF64::P;
+    __device__ static P params(const double* prm, double ch) { return HPRF64::params(prm, ch); }
+    __device__ static void cons(const double* W, const P& q, double* U) { HPRF64::cons(W, q, U); }
+    __device__ static void setcons(const double* U, const P& q, double* W) { HPRF64::setcons(U, q, W); }
+    template <int AXIS>
+    __device__ static void flux(const double* U, const P& q, float* F) {
+        double Fd[17];
+        HPRF64::template flux<AXIS>(U, q, Fd);
+#pragma unroll
+        for (int i = 0; i < 17; i++) F[i] = (float)Fd[i];
+    }
+    __device__ static double wave(const double* W, const P& q, int dims) { return HPRF64::wave(W, q, dims); }
+    __device__ static void default_state(double* W) { HPRF64::default_state(W); }
+    __device__ static double density(const double* W) { return W[0]; }
+    __device__ static double pressure(const double* W) { return W[1]; }
 };
 
 }  // namespace vg

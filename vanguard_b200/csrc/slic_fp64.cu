@@ -83,4 +83,8 @@ const Ops kOps[V_COUNT] = {
 
 const Ops* ops_fp64(int variant) { return (variant >= 0 && variant < V_COUNT) ? &kOps[variant] : nullptr; }
 
+cudaError_t hpr_forcing_fp64(const SweepArgs& a, int subcycles, cudaStream_t st) {
+    return forcing_impl<HPRF64>(a, subcycles, st);
+}
+
 }  // namespace vg

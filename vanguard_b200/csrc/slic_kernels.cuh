@@ -131,6 +131,17 @@ __device__ __forceinline__ void store_w(const SweepArgs& a, long idx, const doub
     for (int v = 0; v < M::NW; v++) a.out[v * a.plane + idx] = W[v];
 }
 
+// Fields setConservedVariableVector leaves alone keep the cell's own values, as when the reference updates the
+// cell object in place (Solvers/firstordersolver.cpp:428-433): HPR's J when the material is not thermal
+// (HPR/hprstatevector.cpp:78-103).
+template <class M>
+__device__ __forceinline__ void keep_fields(const SweepArgs& a, long idx, const typename M::P& q, double* W) {
+    if constexpr (M::NW == 17) {
+        if (!q.thermal)
+            for (int v = 14; v < 17; v++) W[v] = a.in[v * a.plane + idx];
+    }
+}
+
 template <class M>
 __device__ __forceinline__ bool bad_state(const double* W) {
     double rho = M::density(W), p = M::pressure(W);
@@ -211,6 +222,7 @@ __global__ void __launch_bounds__(P* LPB, MINB) sweep_x_kernel(SweepArgs a) {
         double Un[NU], W[NW];
 #pragma unroll
         for (int v = 0; v < NU; v++) Un[v] = Us[v][l][p + 1] + (k.r * (Fs[v][l][p] - Fs[v][l][p + 1]));
+        keep_fields<M>(a, rowbase + cell, q, W);
         M::setcons(Un, q, W);
         store_w<M>(a, rowbase + cell, W);
         if (bad_state<M>(W)) atomicOr(a.err, ERR_STATE);
@@ -270,6 +282,7 @@ __global__ void __launch_bounds__(TX, MINB) sweep_y_kernel(SweepArgs a) {
             double Un[NU], W[NW];
 #pragma unroll
             for (int v = 0; v < NU; v++) Un[v] = um1[v] + (k.r * (f_prev[v] - F[v]));
+            keep_fields<M>(a, (long)(r - 1) * a.pitch + c, q, W);
             M::setcons(Un, q, W);
             store_w<M>(a, (long)(r - 1) * a.pitch + c, W);
             if (bad_state<M>(W)) atomicOr(a.err, ERR_STATE);

@@ -45,18 +45,26 @@ cudaError_t finish_impl(const SweepArgs& a, double* out, cudaStream_t st) {
 template <class M>
 constexpr Ops make_ops() {
     return Ops{M::NW, SweepTable<MixedKernels, M>::x, SweepTable<MixedKernels, M>::y, &max_wave_impl<M>,
-               &step_begin_impl<M>, &finish_impl<M>, nullptr, false};
+               &step_begin_impl<M>, &finish_impl<M>, nullptr, (M::NU > 9)};
 }
 
-const Ops kOps[V_HPR17] = {
+// HPR: the relaxation source keeps FP64 and runs the exact forcing kernel
+template <>
+constexpr Ops make_ops<HPRMixed>() {
+    return Ops{HPRMixed::NW, SweepTable<MixedKernels, HPRMixed>::x, SweepTable<MixedKernels, HPRMixed>::y,
+               &max_wave_impl<HPRMixed>, &step_begin_impl<HPRMixed>, &finish_impl<HPRMixed>, &hpr_forcing_fp64, true};
+}
+
+const Ops kOps[V_COUNT] = {
     make_ops<EulerMixed<1>>(),
     make_ops<EulerMixed<2>>(),
     make_ops<MHDMixed<false>>(),
     make_ops<MHDMixed<true>>(),
+    make_ops<HPRMixed>(),
 };
 
 }  // namespace
 
-const Ops* ops_mixed(int variant) { return (variant >= 0 && variant < V_HPR17) ? &kOps[variant] : nullptr; }
+const Ops* ops_mixed(int variant) { return (variant >= 0 && variant < V_COUNT) ? &kOps[variant] : nullptr; }
 
 }  // namespace vg

@@ -4,6 +4,7 @@
 #pragma once
 
 #include "physics_mixed.cuh"
+#include "slic_kernels.cuh"
 #include "vg_common.cuh"
 
 namespace vg {
@@ -180,6 +181,7 @@ __global__ void __launch_bounds__(P* LPB, MINB) sweep_x_mixed_kernel(SweepArgs a
 #pragma unroll
         for (int v = 0; v < NU; v++)
             Un[v] = fma(k.r, Fs[v][l][p] - Fs[v][l][p + 1], Us[v][l][p + 1]);
+        keep_fields<M>(a, rowbase + cell, q, W);
         M::setcons(Un, q, W);
 #pragma unroll
         for (int v = 0; v < NW; v++) a.out[v * a.plane + rowbase + cell] = W[v];
@@ -244,6 +246,7 @@ __global__ void __launch_bounds__(TX, MINB) sweep_y_mixed_kernel(SweepArgs a) {
             double Un[NU], W[NW];
 #pragma unroll
             for (int v = 0; v < NU; v++) Un[v] = fma(k.r, f_prev[v] - (double)F[v], um1[v]);
+            keep_fields<M>(a, (long)(r - 1) * a.pitch + c, q, W);
             M::setcons(Un, q, W);
 #pragma unroll
             for (int v = 0; v < NW; v++) a.out[v * a.plane + (long)(r - 1) * a.pitch + c] = W[v];
