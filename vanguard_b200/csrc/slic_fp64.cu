@@ -47,8 +47,10 @@ cudaError_t finish_impl(const SweepArgs& a, double* out, cudaStream_t st) {
 
 template <class M>
 cudaError_t forcing_impl(const SweepArgs& a, int subcycles, cudaStream_t st) {
+    if (!a.aux) return cudaErrorInvalidValue;
     long n = (long)a.nx * a.ny;
-    forcing_kernel<M><<<(unsigned)((n + 127) / 128), 128, 0, st>>>(a, subcycles);
+    roundtrip_kernel<M><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a);
+    forcing_kernel<M><<<(unsigned)((n + FT - 1) / FT), FT, sizeof(double) * 3 * M::NU * FT, st>>>(a, subcycles);
     return cudaGetLastError();
 }
 

@@ -63,6 +63,7 @@ struct vg_solver {
     long pitch = 0, plane = 0;
     int max_nw = 0;
     double* buf[2] = {nullptr, nullptr};
+    double* aux = nullptr;    // HPR forcing scratch (conserved planes), allocated with the buffers
     int cur = 0;
     Ctrl* ctrl = nullptr;     // device
     Ctrl* hctrl = nullptr;    // pinned host mirror
@@ -164,6 +165,7 @@ SweepArgs base_args(const vg_solver* s) {
     a.dims = s->dims;
     a.wave_acc = &s->ctrl->smax_next;
     a.err = &s->ctrl->err;
+    a.aux = s->aux;
     for (int i = 0; i < VG_MAX_PARAMS - 1; i++) a.params[i] = s->d.params[i];
     a.params[VG_MAX_PARAMS - 1] = 1.0 / (s->d.params[0] - 1.0);
     a.ch_host = s->d.params[2];
@@ -178,7 +180,7 @@ int enqueue_forcing(vg_solver* s, SweepArgs a, int sub, int from, cudaStream_t s
         a.in = s->buf[b];
         a.out = s->buf[1 - b];
         *e = s->ops->forcing(a, sub, st);
-        (*n)++;
+        *n += vg::kForcingLaunches;
         b = 1 - b;
     }
     return b;
@@ -241,7 +243,7 @@ int enqueue_step(vg_solver* s, const vg_run_config& c, int from, cudaStream_t st
 
 int kernels_per_step(const vg_solver* s, int sub) {
     int n = s->dims == 1 ? 2 : 4;
-    if (s->ops->forcing && sub > 0) n += 2 * sub + 1;
+    if (s->ops->forcing && sub > 0) n += 2 * sub * vg::kForcingLaunches + 1;
     return n;
 }
 
@@ -333,6 +335,7 @@ vg_status vg_create(const vg_grid_desc* desc, vg_solver** out) {
     s->floor5 = std::pow(10.0, -5.0);  // SlopeLimiters::computeSlopeVector's floor (Solvers/slopelimiters.cpp:232-239)
     cudaError_t e = cudaSuccess;
     for (int b = 0; b < 2 && e == cudaSuccess; b++) e = cudaMalloc(&s->buf[b], sizeof(double) * s->plane * s->max_nw);
+    if (e == cudaSuccess && desc->model == VG_MODEL_HPR) e = cudaMalloc(&s->aux, sizeof(double) * s->plane * s->max_nw);
     if (e == cudaSuccess) e = cudaMalloc(&s->ctrl, sizeof(Ctrl));
     if (e == cudaSuccess) e = cudaMalloc(&s->dout, sizeof(double));
     if (e == cudaSuccess) e = cudaMallocHost(&s->hctrl, sizeof(Ctrl));
@@ -352,6 +355,7 @@ vg_status vg_destroy(vg_solver* s) {
     destroy_graphs(s);
     for (auto& b : s->buf)
         if (b) cudaFree(b);
+    if (s->aux) cudaFree(s->aux);
     if (s->ctrl) cudaFree(s->ctrl);
     if (s->dout) cudaFree(s->dout);
     if (s->hctrl) cudaFreeHost(s->hctrl);

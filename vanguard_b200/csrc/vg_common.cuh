@@ -85,6 +85,7 @@ struct SweepArgs {
     int dims;                // 1 or 2 (selects the wave-speed formula)
     unsigned long long* wave_acc;  // running maximum (bit pattern), usually &ctrl->smax_next
     unsigned int* err;             // error word (always valid)
+    double* aux;                   // model scratch planes (HPR forcing neighbours), or null
     double params[16];       // model parameters (model-specific layout); params[15] = 1 / (params[0] - 1)
 };
 

@@ -31,10 +31,13 @@ struct Ops {
     cudaError_t (*step_begin)(const SweepArgs& a, cudaStream_t st);
     // *out = maximum wave speed including corner ghosts (reads ctrl->smax_next).
     cudaError_t (*max_wave_finish)(const SweepArgs& a, double* out, cudaStream_t st);
-    // One relaxation-source sub-cycle of length 0.5 dt / subcycles, a.in -> a.out (null: model has no source).
+    // One relaxation-source sub-cycle of length 0.5 dt / subcycles, a.in -> a.out, with a.aux as scratch
+    // (kForcingLaunches kernels; null: model has no source).
     cudaError_t (*forcing)(const SweepArgs& a, int subcycles, cudaStream_t st);
     bool big_tiles;  // SweepTable<.., BIG = true> (names of the launch configurations)
 };
+
+constexpr int kForcingLaunches = 2;  // kernels per forcing sub-cycle
 
 // Exact-FP64 kernels (compiled with -fmad=false; bitwise parity with the reference).
 const Ops* ops_fp64(int variant);
