@@ -72,6 +72,8 @@ struct model {
     double (*wave1d)(const double* W, const double* prm);
     double (*wave2d)(const double* W, const double* prm);
     void (*default_state)(const double* prm, double* W);
+    /* computeSourceTermVector of the conserved vector (null: the model has no source) */
+    void (*source)(const double* U, const double* prm, double* S);
 };
 
 /* ---- Euler: Euler/eulerstatevector.cpp, Euler/eulerequationofstate.cpp
@@ -175,6 +177,16 @@ static void mhd_setcons(const double* U, const double* prm, double* W) {
     double e = E - (0.5 * v2);
     W[0] = rho; W[1] = u; W[2] = v; W[3] = w; W[4] = mhd_p(rho, e, prm);
     W[5] = bx; W[6] = by; W[7] = bz; W[8] = U[8];
+}
+/* MHDStateVector::computeSourceTermVector (MHD/mhdstatevector.cpp:222-234): GLM damping of psi with
+ * c_h = prm[2] and the parabolic damping of MHDMaterialParameters::configureParabolicDamping,
+ * c_p = sqrt(c_h * 0.18) (MHD/mhdmaterialparameters.cpp:21-36). */
+static void mhd_source(const double* U, const double* prm, double* S) {
+    double ch2 = prm[2] * prm[2];
+    double cp = sqrt(prm[2] * 0.18);
+    double cp2 = cp * cp;
+    for (int i = 0; i < 9; i++) S[i] = 0.0;
+    S[8] = (-(ch2 / cp2)) * U[8];
 }
 /* MHDStateVector::compute{X,Y}FluxVector(vector, params), MHD/mhdstatevector.cpp:108-158, :165-215.
  * v.B is VectorAlgebra::computeDotProduct (Mathematics/vectoralgebra.cpp:38-49), summed from 0.0. */
@@ -558,9 +570,9 @@ static void hpr_default(const double* prm, double* W) {
     W[10] = c * 1.0;
 }
 
-static const model M_EULER = {6, euler_cons, euler_setcons, euler_flux, euler_wave1d, euler_wave2d, euler_default};
-static const model M_MHD = {9, mhd_cons, mhd_setcons, mhd_flux, mhd_wave1d, mhd_wave2d, mhd_default};
-static const model M_HPR = {17, hpr_cons, hpr_setcons, hpr_flux, hpr_wave1d, hpr_wave2d, hpr_default};
+static const model M_EULER = {6, euler_cons, euler_setcons, euler_flux, euler_wave1d, euler_wave2d, euler_default, 0};
+static const model M_MHD = {9, mhd_cons, mhd_setcons, mhd_flux, mhd_wave1d, mhd_wave2d, mhd_default, mhd_source};
+static const model M_HPR = {17, hpr_cons, hpr_setcons, hpr_flux, hpr_wave1d, hpr_wave2d, hpr_default, hpr_source};
 
 static const model* model_of(int id) {
     switch (id) {
@@ -756,7 +768,8 @@ static void prim_of(const model* m, const double* u, const double* prm, double* 
 }
 
 /* HPRForcingSolver::evolveConservedVariableVector{,2D} (Solvers/hprforcingsolver.cpp:7-44, :134-194) and
- * computeEvolvedConservedVariableVector (:332-339).  dims == 1 uses the X predictor alone with fractions
+ * computeEvolvedConservedVariableVector (:332-339); MHDForcingSolver's are the same steps with the MHD model
+ * (Solvers/mhdforcingsolver.cpp:7-44, :134-194).  dims == 1 uses the X predictor alone with fractions
  * (1/2, 1/2, 1); dims == 2 the X(f/2) Y(f) X(f/2) predictor with f = 1/2, 1/2, 1. */
 static void rk4_source(const model* m, const double* uLf, const double* uM, const double* uRf, const double* uTf,
                        const double* uBf, int dims, double dx, double dt, double w, int lim, const double* prm,
@@ -771,7 +784,7 @@ static void rk4_source(const model* m, const double* uLf, const double* uM, cons
         prim_of(m, uBf, prm, wb);
     }
     m->default_state(prm, wm);
-    hpr_source(uM, prm, S);
+    m->source(uM, prm, S);
     for (int i = 0; i < nv; i++) k[0][i] = dt * S[i];
     static const double stage[3] = {0.5, 0.5, 1.0};
     for (int s = 0; s < 3; s++) {
@@ -786,7 +799,7 @@ static void rk4_source(const model* m, const double* uLf, const double* uM, cons
             frac_evolve(m, 0.5 * f, wl, e2, wr, 0, dx, dt, w, lim, prm, e);
         }
         m->cons(e, prm, ue);
-        hpr_source(ue, prm, S);
+        m->source(ue, prm, S);
         for (int i = 0; i < nv; i++) k[s + 1][i] = dt * S[i];
     }
     for (int i = 0; i < nv; i++)
@@ -801,7 +814,8 @@ static int ghost1(int k, int n, int bc) {
     return k < 0 ? 0 : n - 1;
 }
 
-/* HPRForcingSolver::computeRungeKuttaTimeStep{,2D} (Solvers/hprforcingsolver.cpp:341-357, :394-418) */
+/* HPRForcingSolver::computeRungeKuttaTimeStep{,2D} (Solvers/hprforcingsolver.cpp:341-357, :394-418) and
+ * MHDForcingSolver's (Solvers/mhdforcingsolver.cpp:341-357, :394-418) */
 static void forcing_grid(const model* m, double* planes, int nx, int ny, int dims, double dx, double dt, double w,
                          int lim, const double* prm, int bc) {
     long plane = (long)nx * ny;
@@ -834,7 +848,7 @@ static void forcing_grid(const model* m, double* planes, int nx, int ny, int dim
 void vo_forcing(int id, double* planes, int nx, int ny, double dx, double dt, double w, int lim, const double* prm,
                 int bc) {
     const model* m = model_of(id);
-    if (!m || id != VO_HPR) return;
+    if (!m || !m->source) return;
     forcing_grid(m, planes, nx, ny, ny > 1 ? 2 : 1, dx, dt, w, lim, prm, bc);
 }
 
@@ -870,14 +884,14 @@ static double run(int id, double* planes, int nx, int ny, int dims, double dx, d
     long plane = (long)nx * ny;
     double t = 0.0;
     int it = 0;
-    int sub = id == VO_HPR ? subcycles : 0;
+    int sub = m->source ? subcycles : 0;
     while (t < tEnd && it < limit) {
         double smax_ = max_wave(m, planes, plane, dims, prm);
         double dt = stable_dt(cfl * (dx / smax_), t, tEnd, it);
         if (id == VO_MHD) prm[2] = smax_;
         if (dt_log) dt_log[it] = dt;
-        /* HPR: sub-cycled RK4 relaxation source before and after the sweeps
-         * (Solvers/hprsecondordersolver.cpp:323-341, :514-541) */
+        /* HPR relaxation / MHD GLM damping: sub-cycled RK4 source before and after the sweeps
+         * (Solvers/hprsecondordersolver.cpp:323-341, :514-541; Solvers/mhdsecondordersolver.cpp:334-348, :517-540) */
         for (int s = 0; s < sub; s++) forcing_grid(m, planes, nx, ny, dims, dx, 0.5 * (dt / sub), w, lim, prm, bc);
         if (dims == 1) {
             sweep_grid(m, planes, nx, 1, 0, dx, dt, w, lim, prm, bc);

@@ -142,3 +142,22 @@ def test_oracle_vs_reference_hpr2d(sub, bc):
     O.run(O.HPR, a, 1 / 14, 0.8, steps=3, limiter=1, params=prm, bc=bc, subcycles=sub)
     O.ref_run(O.HPR, b, 1 / 14, 0.8, steps=3, limiter=1, params=prm, bc=bc, subcycles=sub)
     assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("bc", [0, 1])
+def test_oracle_vs_reference_mhd_glm_subcycles(bc):
+    """MHD with GLM damping sub-cycles (MHDForcingSolver's RK4 around the sweeps), 1D and 2D, bit for bit."""
+    if not O.ref_available():
+        pytest.skip("compiled reference not built")
+    W = wl.mhd_vortex_2d(20, 16, seed=4)
+    a, b = W.copy(), W.copy()
+    O.run(O.MHD, a, 1 / 20, 0.8, steps=6, limiter=0, params=wl.mhd_params(5 / 3), bc=bc, subcycles=2)
+    O.ref_run(O.MHD, b, 1 / 20, 0.8, steps=6, limiter=0, params=wl.mhd_params(5 / 3), bc=bc, subcycles=2)
+    assert np.array_equal(a, b)
+    assert np.abs(a[8] - W[8]).max() > 1e-4  # psi is damped and transported, not left alone
+    W1 = wl.brio_wu_1d(60)
+    W1[8] = 0.01 * np.sin(np.arange(60))
+    a, b = W1.copy(), W1.copy()
+    O.run(O.MHD, a, 1 / 60, 0.8, steps=8, limiter=1, params=wl.mhd_params(2.0), bc=bc, subcycles=3)
+    O.ref_run(O.MHD, b, 1 / 60, 0.8, steps=8, limiter=1, params=wl.mhd_params(2.0), bc=bc, subcycles=3)
+    assert np.array_equal(a, b)

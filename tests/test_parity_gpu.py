@@ -156,3 +156,40 @@ def test_autotune_picks_and_keeps_results(gpu, oracle_lib):
         s.upload(W)
         s.run(1.0 / nx, 0.8, steps=10, limiter=0)
         _bitwise(s.download(), ref)
+
+
+@pytest.mark.parametrize("bc", [0, 1])
+def test_mhd_glm_subcycles_bitwise(gpu, oracle_lib, bc):
+    """MHD with GLM damping sub-cycles (MHDForcingSolver's RK4 before and after the sweeps), FP64 bit for bit;
+    the mixed form keeps the damping in FP64 and stays within the mixed-form bound."""
+    nx, ny = 40, 36
+    W = wl.mhd_vortex_2d(nx, ny, seed=6)
+    W[8] = 0.01 * np.sin(2 * np.pi * np.arange(nx) / nx)[None, :] * np.ones((ny, 1))
+    prm = wl.mhd_params(5.0 / 3.0)
+    ref = W.copy()
+    O.run(O.MHD, ref, 1.0 / nx, 0.8, steps=12, limiter=0, params=prm, bc=bc, subcycles=2)
+    assert np.abs(ref[8] - W[8]).max() > 1e-4
+    for prec in (gpu.FP64, gpu.MIXED):
+        with gpu.Solver(gpu.MHD, nx, ny, prm, precision=prec, boundary=bc) as s:
+            s.upload(W)
+            s.run(1.0 / nx, 0.8, steps=12, limiter=0, subcycles=2)
+            out = s.download()
+        if prec == gpu.FP64:
+            assert np.array_equal(out, ref)
+        else:
+            assert np.abs(out[0] - ref[0]).mean() <= 1e-6
+            assert np.abs(out[8] - ref[8]).max() <= 1e-5
+
+
+def test_mhd_1d_glm_subcycles_bitwise(gpu, oracle_lib):
+    n = 120
+    W = wl.brio_wu_1d(n)
+    W[8] = 0.01 * np.sin(np.arange(n))
+    prm = wl.mhd_params(2.0)
+    ref = W.copy()
+    O.run(O.MHD, ref, 1.0 / n, 0.8, steps=15, limiter=1, params=prm, subcycles=3)
+    with gpu.Solver(gpu.MHD, n, 1, prm) as s:
+        s.upload(W)
+        s.run(1.0 / n, 0.8, steps=15, limiter=1, subcycles=3)
+        out = s.download()
+    assert np.array_equal(out, ref)

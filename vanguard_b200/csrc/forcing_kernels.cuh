@@ -1,4 +1,5 @@
-// HPR relaxation-source sub-cycle: HPRForcingSolver's RK4 with fractional flux predictors, one thread per cell.
+// Relaxation-source sub-cycle: HPRForcingSolver's RK4 with fractional flux predictors, one thread per cell; the
+// MHD GLM damping of MHDForcingSolver (Solvers/mhdforcingsolver.cpp) is the same scheme with the MHD model.
 //
 // HPRForcingSolver::computeRungeKuttaTimeStep{,2D} (Solvers/hprforcingsolver.cpp:341-357, :394-418) evaluates,
 // for every cell, four source terms S(U) at stage states that are advanced by slope-limited fractional flux steps
@@ -58,7 +59,7 @@ __global__ void __launch_bounds__(256) roundtrip_kernel(SweepArgs a) {
     if (idx >= n || (a.ctrl && !a.ctrl->active)) return;
     const int i = (int)(idx / a.nx), j = (int)(idx - (long)i * a.nx);
     const long self = (long)i * a.pitch + j;
-    const typename M::P q = M::params(a.params, 0.0);
+    const typename M::P q = M::params(a.params, a.ctrl ? a.ctrl->ch : a.ch_host);
     double W[NW], U[NU];
     for (int v = 0; v < NW; v++) W[v] = a.in[v * a.plane + self];
     M::cons(W, q, U);
@@ -91,7 +92,7 @@ __global__ void __launch_bounds__(FT, 6) forcing_kernel(SweepArgs a, int subcycl
     k.bias = a.bias;
     k.floor5 = a.floor5;
     k.limiter = a.limiter;
-    const typename M::P q = M::params(a.params, 0.0);
+    const typename M::P q = M::params(a.params, a.ctrl ? a.ctrl->ch : a.ch_host);
     const int dims = a.ny > 1 ? 2 : 1;
     auto kk = [&](int s, int v) -> double& { return ksh[(s * NU + v) * FT + threadIdx.x]; };
     // neighbours through the 1-ghost boundary: left, right, top, bottom

@@ -20,6 +20,7 @@ struct EulerF64 {
     static constexpr int NU = NW;
     static constexpr int IE = NU - 1;  // energy / pressure slot
     static constexpr bool HAS_Y = NVEL == 2;
+    static constexpr bool HAS_SOURCE = false;
     struct P {
         double g, pinf, ch2;
     };
@@ -107,10 +108,21 @@ struct MHDF64 {
     static constexpr int IBY = IP + 2;
     static constexpr int IPSI = NW - 1;
     static constexpr bool HAS_Y = true;
+    static constexpr bool HAS_SOURCE = true;
     struct P {
-        double g, pinf, ch2;
+        double g, pinf, ch2, ch;
     };
-    __device__ static P params(const double* prm, double ch) { return P{prm[0], prm[1], ch * ch}; }
+    __device__ static P params(const double* prm, double ch) { return P{prm[0], prm[1], ch * ch, ch}; }
+
+    // MHDStateVector::computeSourceTermVector (MHD/mhdstatevector.cpp:222-234): GLM damping of psi with the
+    // parabolic damping c_p = sqrt(c_h * 0.18) of MHDMaterialParameters::configureParabolicDamping
+    // (MHD/mhdmaterialparameters.cpp:21-36), c_h being this step's maximum wave speed
+    __device__ static void source(const double* U, const P& q, double* S) {
+#pragma unroll
+        for (int i = 0; i < NU; i++) S[i] = 0.0;
+        const double cp = sqrt(q.ch * 0.18);
+        S[IPSI] = (-(q.ch2 / (cp * cp))) * U[IPSI];
+    }
 
     __device__ static double e_of(double rho, double p, const P& q) { return (p + (q.g * q.pinf)) / ((q.g - 1) * rho); }
     __device__ static double p_of(double rho, double e, const P& q) { return ((e * (q.g - 1)) * rho) - (q.g * q.pinf); }

@@ -19,6 +19,7 @@ struct HPRF64 {
     static constexpr int NW = 17;
     static constexpr int NU = 17;
     static constexpr bool HAS_Y = true;
+    static constexpr bool HAS_SOURCE = true;
     struct P {
         double g, pinf, cv, rho0, T0, cs, alpha, tau1, tau2, Tref;
         int thermal;

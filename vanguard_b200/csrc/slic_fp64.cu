@@ -54,23 +54,24 @@ cudaError_t forcing_impl(const SweepArgs& a, int subcycles, cudaStream_t st) {
     return cudaGetLastError();
 }
 
+using ForcingFn = cudaError_t (*)(const SweepArgs&, int, cudaStream_t);
+
 template <class M>
-constexpr Ops make_ops(bool with_source = false) {
+constexpr ForcingFn forcing_of() {
+    if constexpr (M::HAS_SOURCE) return &forcing_impl<M>;
+    else return nullptr;
+}
+
+template <class M>
+constexpr Ops make_ops() {
     return Ops{M::NW,
                SweepTable<Fp64Kernels, M>::x,
                SweepTable<Fp64Kernels, M>::y,
                &max_wave_impl<M>,
                &step_begin_impl<M>,
                &finish_impl<M>,
-               nullptr,
+               forcing_of<M>(),
                (M::NU > 9)};
-}
-
-template <>
-constexpr Ops make_ops<HPRF64>(bool) {
-    return Ops{HPRF64::NW,        SweepTable<Fp64Kernels, HPRF64>::x, SweepTable<Fp64Kernels, HPRF64>::y,
-               &max_wave_impl<HPRF64>, &step_begin_impl<HPRF64>,         &finish_impl<HPRF64>,
-               &forcing_impl<HPRF64>,  true};
 }
 
 const Ops kOps[V_COUNT] = {
@@ -87,6 +88,12 @@ const Ops* ops_fp64(int variant) { return (variant >= 0 && variant < V_COUNT) ? 
 
 cudaError_t hpr_forcing_fp64(const SweepArgs& a, int subcycles, cudaStream_t st) {
     return forcing_impl<HPRF64>(a, subcycles, st);
+}
+cudaError_t mhd7_forcing_fp64(const SweepArgs& a, int subcycles, cudaStream_t st) {
+    return forcing_impl<MHDF64<false>>(a, subcycles, st);
+}
+cudaError_t mhd9_forcing_fp64(const SweepArgs& a, int subcycles, cudaStream_t st) {
+    return forcing_impl<MHDF64<true>>(a, subcycles, st);
 }
 
 }  // namespace vg

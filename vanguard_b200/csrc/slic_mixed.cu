@@ -42,25 +42,21 @@ cudaError_t finish_impl(const SweepArgs& a, double* out, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-template <class M>
-constexpr Ops make_ops() {
-    return Ops{M::NW, SweepTable<MixedKernels, M>::x, SweepTable<MixedKernels, M>::y, &max_wave_impl<M>,
-               &step_begin_impl<M>, &finish_impl<M>, nullptr, (M::NU > 9)};
-}
+using ForcingFn = cudaError_t (*)(const SweepArgs&, int, cudaStream_t);
 
-// HPR: the relaxation source keeps FP64 and runs the exact forcing kernel
-template <>
-constexpr Ops make_ops<HPRMixed>() {
-    return Ops{HPRMixed::NW, SweepTable<MixedKernels, HPRMixed>::x, SweepTable<MixedKernels, HPRMixed>::y,
-               &max_wave_impl<HPRMixed>, &step_begin_impl<HPRMixed>, &finish_impl<HPRMixed>, &hpr_forcing_fp64, true};
+// The source sub-cycles keep FP64: the exact forcing kernels of each model
+template <class M>
+constexpr Ops make_ops(ForcingFn forcing = nullptr) {
+    return Ops{M::NW, SweepTable<MixedKernels, M>::x, SweepTable<MixedKernels, M>::y, &max_wave_impl<M>,
+               &step_begin_impl<M>, &finish_impl<M>, forcing, (M::NU > 9)};
 }
 
 const Ops kOps[V_COUNT] = {
     make_ops<EulerMixed<1>>(),
     make_ops<EulerMixed<2>>(),
-    make_ops<MHDMixed<false>>(),
-    make_ops<MHDMixed<true>>(),
-    make_ops<HPRMixed>(),
+    make_ops<MHDMixed<false>>(&mhd7_forcing_fp64),
+    make_ops<MHDMixed<true>>(&mhd9_forcing_fp64),
+    make_ops<HPRMixed>(&hpr_forcing_fp64),
 };
 
 }  // namespace

@@ -335,7 +335,8 @@ vg_status vg_create(const vg_grid_desc* desc, vg_solver** out) {
     s->floor5 = std::pow(10.0, -5.0);  // SlopeLimiters::computeSlopeVector's floor (Solvers/slopelimiters.cpp:232-239)
     cudaError_t e = cudaSuccess;
     for (int b = 0; b < 2 && e == cudaSuccess; b++) e = cudaMalloc(&s->buf[b], sizeof(double) * s->plane * s->max_nw);
-    if (e == cudaSuccess && desc->model == VG_MODEL_HPR) e = cudaMalloc(&s->aux, sizeof(double) * s->plane * s->max_nw);
+    if (e == cudaSuccess && desc->model != VG_MODEL_EULER)  // scratch of the source sub-cycles (HPR, MHD)
+        e = cudaMalloc(&s->aux, sizeof(double) * s->plane * s->max_nw);
     if (e == cudaSuccess) e = cudaMalloc(&s->ctrl, sizeof(Ctrl));
     if (e == cudaSuccess) e = cudaMalloc(&s->dout, sizeof(double));
     if (e == cudaSuccess) e = cudaMallocHost(&s->hctrl, sizeof(Ctrl));
@@ -449,7 +450,7 @@ vg_status vg_run(vg_solver* s, const vg_run_config* cfg, int* steps_taken, doubl
     if (cfg->max_steps <= 0 && !(cfg->t_end > 0.0)) return fail(VG_EINVAL, "need t_end > 0 or max_steps > 0");
     if (cfg->subcycles < 0) return fail(VG_EINVAL, "subcycles must be >= 0");
     if (cfg->subcycles > 0 && !s->ops->forcing)
-        return fail(VG_EUNSUPPORTED, "source sub-cycling is only available for the HPR model");
+        return fail(VG_EUNSUPPORTED, "source sub-cycling needs a model with a source (HPR relaxation, MHD GLM damping)");
     cudaStream_t st = (cudaStream_t)stream;
     VG_CUDA(cudaSetDevice(s->d.device));
 

@@ -43,8 +43,10 @@ constexpr int kForcingLaunches = 2;  // kernels per forcing sub-cycle
 const Ops* ops_fp64(int variant);
 // Mixed FP32/FP64 kernels.
 const Ops* ops_mixed(int variant);
-// The exact HPR relaxation-source sub-cycle (slic_fp64.cu), which the mixed form uses unchanged.
+// The exact source sub-cycles (slic_fp64.cu), which the mixed form uses unchanged: HPR relaxation, MHD GLM damping.
 cudaError_t hpr_forcing_fp64(const SweepArgs& a, int subcycles, cudaStream_t st);
+cudaError_t mhd7_forcing_fp64(const SweepArgs& a, int subcycles, cudaStream_t st);
+cudaError_t mhd9_forcing_fp64(const SweepArgs& a, int subcycles, cudaStream_t st);
 
 // Record the text returned by vg_last_error_string() on this thread.
 void set_last_error(const std::string& msg);

@@ -536,11 +536,10 @@ vector<MHDStateVector> MHDSecondOrderSolver::solve(vector<MHDStateVector>& initi
 vector<MHDStateVector> MHDSecondOrderSolver::solve(vector<MHDStateVector>& initialCells, double dx, double cfl, double tEnd,
                                                    double bias, int limiter, int subcycles, MHDMaterialParameters mp,
                                                    int maxSteps) {
-    if (subcycles != 0) throw std::runtime_error("MHD GLM damping sub-cycles are not available on the GPU path");
     double prm[3];
     mhd_params(mp, prm);
     std::vector<double> p = pack(initialCells, 9, mhd_get);
-    run_planes(VG_MODEL_MHD, p, (int)initialCells.size(), 1, prm, 3, dx, cfl, tEnd, bias, limiter, 0, maxSteps);
+    run_planes(VG_MODEL_MHD, p, (int)initialCells.size(), 1, prm, 3, dx, cfl, tEnd, bias, limiter, subcycles, maxSteps);
     return unpack<MHDStateVector>(p, initialCells.size(), 9, mhd_make);
 }
 vector<vector<MHDStateVector> > MHDSecondOrderSolver::solve2D(vector<vector<MHDStateVector> >& initialCells, double dx, double cfl,
@@ -551,12 +550,11 @@ vector<vector<MHDStateVector> > MHDSecondOrderSolver::solve2D(vector<vector<MHDS
 vector<vector<MHDStateVector> > MHDSecondOrderSolver::solve2D(vector<vector<MHDStateVector> >& initialCells, double dx, double cfl,
                                                               double tEnd, double bias, int limiter, int subcycles,
                                                               MHDMaterialParameters mp, int maxSteps) {
-    if (subcycles != 0) throw std::runtime_error("MHD GLM damping sub-cycles are not available on the GPU path");
     double prm[3];
     mhd_params(mp, prm);
     std::vector<double> p = pack2(initialCells, 9, mhd_get);
     long ny = initialCells.size(), nx = initialCells[0].size();
-    run_planes(VG_MODEL_MHD, p, (int)nx, (int)ny, prm, 3, dx, cfl, tEnd, bias, limiter, 0, maxSteps);
+    run_planes(VG_MODEL_MHD, p, (int)nx, (int)ny, prm, 3, dx, cfl, tEnd, bias, limiter, subcycles, maxSteps);
     return unpack2<MHDStateVector>(p, nx, ny, 9, mhd_make);
 }
 
