@@ -77,7 +77,10 @@ typedef struct vg_run_config {
     int max_steps;      /* > 0: stop after this many steps; <= 0: run until t_end */
     double bias;        /* slope-limiter bias omega */
     int limiter;        /* slopeLimiter id */
-    int subcycles;      /* subcyclingIterations (source integration; HPR and MHD only) */
+    int subcycles;      /* subcyclingIterations (source integration; HPR and MHD only; second order only) */
+    int order;          /* 2 (or 0): SecondOrderSolver's SLIC loop; 1: FirstOrderSolver's FORCE loop
+                         * (Solvers/firstordersolver.cpp:435-553 and the MHD / HPR twins: 1-ghost boundary, FORCE
+                         * of the cells themselves, no source, the MHD c_h kept at params[2]; VG_FP64 only) */
 } vg_run_config;
 
 typedef struct vg_solver vg_solver;

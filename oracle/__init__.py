@@ -79,6 +79,9 @@ def lib():
         L.vo_nparams.restype = _c_int
         L.vo_forcing.argtypes = [_c_int, _D, _c_int, _c_int, _c_double, _c_double, _c_double, _c_int, _D, _c_int]
         L.vo_hpr_cell.argtypes = [_D, _D, _D, _D, _D, _D, _D]
+        L.vo_run_first_order.restype = _c_double
+        L.vo_run_first_order.argtypes = [_c_int, _D, _c_int, _c_int, _c_double, _c_double, _c_double, _c_int, _D,
+                                         _c_int, ctypes.POINTER(_c_int)]
         _lib = L
     return _lib
 
@@ -94,6 +97,9 @@ def ref():
         if not ref_available():
             raise FileNotFoundError(f"{REF_SO} not built (make -C oracle ref needs the reference tree)")
         R = ctypes.CDLL(REF_SO)
+        R.vgref_first_order_run.restype = _c_double
+        R.vgref_first_order_run.argtypes = [_c_int, _D, _c_int, _c_int, _c_double, _c_double, _c_double, _c_int, _D,
+                                            _c_int, ctypes.POINTER(_c_int)]
         R.vgref_set_threads.restype = _c_int
         R.vgref_set_threads.argtypes = [_c_int]
         R.vgref_euler1d_run.restype = _c_double
@@ -142,6 +148,29 @@ def run(model, planes, dx, cfl, t_end=0.0, steps=0, bias=0.0, limiter=SUPERBEE, 
         t = lib().vo_run2d(model, _ptr(planes), planes.shape[2], planes.shape[1], dx, cfl, t_end, steps,
                            bias, limiter, _ptr(prm), bc, subcycles, ctypes.byref(st), _ptr(dts))
     return (t, st.value, dts) if dt_log else (t, st.value)
+
+
+def run_first_order(model, planes, dx, cfl, t_end=0.0, steps=0, params=None, bc=TRANSMISSIVE):
+    """FirstOrderSolver::solve/solve2D's loop (and the MHD / HPR twins) in the C restatement, in place.
+    Returns (t, steps)."""
+    _check(planes, NVAR[model])
+    prm = np.ascontiguousarray(params, dtype=np.float64)
+    st = ctypes.c_int()
+    nx, ny = (planes.shape[2], planes.shape[1]) if planes.ndim == 3 else (planes.shape[1], 1)
+    t = lib().vo_run_first_order(model, _ptr(planes), nx, ny, dx, cfl, t_end, steps, _ptr(prm), bc, ctypes.byref(st))
+    return t, st.value
+
+
+def ref_run_first_order(model, planes, dx, cfl, t_end=0.0, steps=0, params=None, bc=TRANSMISSIVE, threads=1):
+    """The reference's first-order loop from its own per-step functions, in place.  Returns (t, steps)."""
+    _check(planes, NVAR[model])
+    R = ref()
+    R.vgref_set_threads(threads)
+    prm = np.ascontiguousarray(params, dtype=np.float64)
+    st = ctypes.c_int()
+    nx, ny = (planes.shape[2], planes.shape[1]) if planes.ndim == 3 else (planes.shape[1], 1)
+    t = R.vgref_first_order_run(model, _ptr(planes), nx, ny, dx, cfl, t_end, steps, _ptr(prm), bc, ctypes.byref(st))
+    return t, st.value
 
 
 def sweep(model, planes, axis, dx, dt, bias=0.0, limiter=SUPERBEE, params=None, bc=TRANSMISSIVE):

@@ -16,6 +16,8 @@
 //     c_h set from the padded-grid maximum wave speed each step as solve() does (:330-332, :513-515).
 //   * the HPR equivalents (Solvers/hprsecondordersolver.cpp, Solvers/hprsolvers.cpp,
 //     Solvers/hprforcingsolver.cpp).
+//   * the first-order FORCE solvers' loops (FirstOrderSolver::solve{,2D}, Solvers/firstordersolver.cpp:435,521;
+//     MHDFirstOrderSolver, HPRFirstOrderSolver) from their per-step functions compute{,X,Y}FORCETimeStep{,2D}.
 //
 // The reference has no periodic boundary.  For periodic runs this harness builds the ghosted arrays
 // itself (2 ghost cells, wrap-around) and leaves the 2D corner blocks default-constructed, exactly as
@@ -24,6 +26,9 @@
 // Parity runs call vgref_set_threads(1): the reference's CFL maximum is an unsynchronised OpenMP
 // update (Solvers/solvers.cpp:264-273) and is only reproducible on one thread.
 
+#include "Solvers/firstordersolver.h"
+#include "Solvers/hprfirstordersolver.h"
+#include "Solvers/mhdfirstordersolver.h"
 #include "Solvers/secondordersolver.h"
 #include "Solvers/mhdsecondordersolver.h"
 #include "Solvers/mhdforcingsolver.h"
@@ -471,4 +476,91 @@ extern "C" void vgref_hpr_cell(const double* w, const double* prm, double* u, do
     }
     speed_xy[0] = HPRAcousticTensor::computeMaximumWaveSpeed(s, mp, 0);
     speed_xy[1] = HPRAcousticTensor::computeMaximumWaveSpeed(s, mp, 1);
+}
+
+// ---------------------------------------------------------------------------------------- first order
+// FirstOrderSolver / MHDFirstOrderSolver / HPRFirstOrderSolver::solve{,2D} (Solvers/firstordersolver.cpp:435-553,
+// Solvers/mhdfirstordersolver.cpp:457-478, Solvers/hprfirstordersolver.cpp:547-574): 1-ghost boundary, stable
+// time step, one FORCE step in 1D or X(dt/2) Y(dt) X(dt/2) in 2D.  The material parameters are not touched
+// between steps (the MHD c_h stays what the caller gave, prm[2]).
+namespace {
+
+template <class S, class P, class Sol, class FO>
+double firstOrder1D(vector<S>& cells, double dx, double cfl, double t_end, int max_steps, P mp, int bc, int* steps) {
+    QuietCout quiet;
+    double t = 0.0, tEnd = t_end > 0.0 ? t_end : kNoEnd;
+    int it = 0, limit = max_steps > 0 ? max_steps : 0x7fffffff;
+    while (t < tEnd && it < limit) {
+        vector<S> withB = bc == 1 ? periodicGhosts1D(cells, 1) : Sol::insertBoundaryCells(cells, 1);
+        double dt = Sol::computeStableTimeStep(withB, dx, cfl, t, tEnd, it, mp);
+        FO::computeFORCETimeStep(cells, withB, dx, dt, mp);
+        t += dt;
+        it += 1;
+    }
+    if (steps) *steps = it;
+    return t;
+}
+
+template <class S, class P, class Sol, class FO>
+double firstOrder2D(vector<vector<S> >& cells, double dx, double cfl, double t_end, int max_steps, P mp, int bc,
+                    int* steps) {
+    QuietCout quiet;
+    auto ghosts = [&](vector<vector<S> >& c) { return bc == 1 ? periodicGhosts2D(c, 1) : Sol::insertBoundaryCells2D(c, 1); };
+    double t = 0.0, tEnd = t_end > 0.0 ? t_end : kNoEnd;
+    int it = 0, limit = max_steps > 0 ? max_steps : 0x7fffffff;
+    while (t < tEnd && it < limit) {
+        vector<vector<S> > withB = ghosts(cells);
+        double dt = Sol::computeStableTimeStep2D(withB, dx, cfl, t, tEnd, it, mp);
+        FO::computeXFORCETimeStep2D(cells, withB, dx, 0.5 * dt, mp);
+        withB = ghosts(cells);
+        FO::computeYFORCETimeStep2D(cells, withB, dx, dt, mp);
+        withB = ghosts(cells);
+        FO::computeXFORCETimeStep2D(cells, withB, dx, 0.5 * dt, mp);
+        t += dt;
+        it += 1;
+    }
+    if (steps) *steps = it;
+    return t;
+}
+
+}  // namespace
+
+// model 0 Euler (prm as eulerParams), 1 MHD (prm = {gamma, p_inf, c_h}), 2 HPR (prm as hprParams); ny == 1: 1D.
+extern "C" double vgref_first_order_run(int model, double* planes, int nx, int ny, double dx, double cfl,
+                                        double t_end, int max_steps, const double* prm, int bc, int* steps_out) {
+    const long plane = (long)nx * ny;
+    double t = 0.0;
+    if (model == 0) {
+        EulerMaterialParameters mp = eulerParams(prm);
+        vector<vector<EulerStateVector> > g = eulerGrid(planes, nx, ny);
+        if (ny == 1)
+            t = firstOrder1D<EulerStateVector, EulerMaterialParameters, Solvers, FirstOrderSolver>(g[0], dx, cfl, t_end, max_steps, mp, bc, steps_out);
+        else
+            t = firstOrder2D<EulerStateVector, EulerMaterialParameters, Solvers, FirstOrderSolver>(g, dx, cfl, t_end, max_steps, mp, bc, steps_out);
+        eulerUngrid(g, planes, nx, ny);
+    } else if (model == 1) {
+        MHDMaterialParameters mp = mhdParams(prm);
+        mp.setHyperbolicWaveSpeed(prm[2]);
+        vector<vector<MHDStateVector> > g(ny, vector<MHDStateVector>(nx));
+        for (int i = 0; i < ny; i++)
+            for (int j = 0; j < nx; j++) g[i][j] = mhdCell(planes, plane, (long)i * nx + j);
+        if (ny == 1)
+            t = firstOrder1D<MHDStateVector, MHDMaterialParameters, MHDSolvers, MHDFirstOrderSolver>(g[0], dx, cfl, t_end, max_steps, mp, bc, steps_out);
+        else
+            t = firstOrder2D<MHDStateVector, MHDMaterialParameters, MHDSolvers, MHDFirstOrderSolver>(g, dx, cfl, t_end, max_steps, mp, bc, steps_out);
+        for (int i = 0; i < ny; i++)
+            for (int j = 0; j < nx; j++) mhdStore(g[i][j], planes, plane, (long)i * nx + j);
+    } else {
+        HPRMaterialParameters mp = hprParams(prm);
+        vector<vector<HPRStateVector> > g(ny, vector<HPRStateVector>(nx));
+        for (int i = 0; i < ny; i++)
+            for (int j = 0; j < nx; j++) g[i][j] = hprCell(planes, plane, (long)i * nx + j);
+        if (ny == 1)
+            t = firstOrder1D<HPRStateVector, HPRMaterialParameters, HPRSolvers, HPRFirstOrderSolver>(g[0], dx, cfl, t_end, max_steps, mp, bc, steps_out);
+        else
+            t = firstOrder2D<HPRStateVector, HPRMaterialParameters, HPRSolvers, HPRFirstOrderSolver>(g, dx, cfl, t_end, max_steps, mp, bc, steps_out);
+        for (int i = 0; i < ny; i++)
+            for (int j = 0; j < nx; j++) hprStore(g[i][j], planes, plane, (long)i * nx + j);
+    }
+    return t;
 }

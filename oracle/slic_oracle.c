@@ -908,6 +908,72 @@ static double run(int id, double* planes, int nx, int ny, int dims, double dx, d
     return t;
 }
 
+/* One sweep of FirstOrderSolver::computeFORCETimeStep / compute{X,Y}FORCETimeStep2D (Solvers/firstordersolver.cpp:
+ * 232-247, :286-308, :357-379): FORCE fluxes of the cells themselves over the 1-ghost boundary (the ghosts -1 and
+ * n are the 2-ghost mirror's), then computeFORCEUpdate (:428-433). */
+static void sweep1_grid(const model* m, double* planes, int nx, int ny, int axis, double dx, double dt,
+                        const double* prm, int bc) {
+    long plane = (long)nx * ny;
+    int nv = m->nv;
+    int len = axis == 0 ? nx : ny, nlines = axis == 0 ? ny : nx;
+    double r = dt / dx;
+    double* out = (double*)malloc(sizeof(double) * nv * plane);
+#pragma omp parallel for schedule(static)
+    for (int line = 0; line < nlines; line++) {
+        double* fl = (double*)malloc(sizeof(double) * (len + 1) * MAXV);
+        for (int f = 0; f <= len; f++) {
+            double wa[MAXV], wb[MAXV];
+            int ka = ghost_index(f - 1, len, bc), kb = ghost_index(f, len, bc);
+            load_cell(planes, plane, axis == 0 ? (long)line * nx + ka : (long)ka * nx + line, nv, wa);
+            load_cell(planes, plane, axis == 0 ? (long)line * nx + kb : (long)kb * nx + line, nv, wb);
+            force_flux(m, wa, wb, axis, dx, dt, prm, fl + (long)f * MAXV);
+        }
+        for (int c = 0; c < len; c++) {
+            long idx = axis == 0 ? (long)line * nx + c : (long)c * nx + line;
+            double W[MAXV], U[MAXV], Un[MAXV];
+            load_cell(planes, plane, idx, nv, W);
+            m->cons(W, prm, U);
+            for (int v = 0; v < nv; v++)
+                Un[v] = U[v] + (r * (fl[(long)c * MAXV + v] + (-1.0 * fl[(long)(c + 1) * MAXV + v])));
+            m->setcons(Un, prm, W);
+            for (int v = 0; v < nv; v++) out[v * plane + idx] = W[v];
+        }
+        free(fl);
+    }
+    memcpy(planes, out, sizeof(double) * nv * plane);
+    free(out);
+}
+
+/* FirstOrderSolver::solve{,2D} (Solvers/firstordersolver.cpp:435-553) and the MHD / HPR twins
+ * (Solvers/mhdfirstordersolver.cpp:457-478, Solvers/hprfirstordersolver.cpp:547-574): the parameters stay as
+ * given (the MHD c_h = prm[2] is not reset), no source sub-cycles. */
+double vo_run_first_order(int id, double* planes, int nx, int ny, double dx, double cfl, double t_end, int max_steps,
+                          const double* prm, int bc, int* steps_out) {
+    const model* m = model_of(id);
+    if (!m) return -1.0;
+    int dims = ny > 1 ? 2 : 1;
+    double tEnd = t_end > 0.0 ? t_end : 1.0e300;
+    int limit = max_steps > 0 ? max_steps : 0x7fffffff;
+    long plane = (long)nx * ny;
+    double t = 0.0;
+    int it = 0;
+    while (t < tEnd && it < limit) {
+        double smax_ = max_wave(m, planes, plane, dims, prm);
+        double dt = stable_dt(cfl * (dx / smax_), t, tEnd, it);
+        if (dims == 1) {
+            sweep1_grid(m, planes, nx, 1, 0, dx, dt, prm, bc);
+        } else {
+            sweep1_grid(m, planes, nx, ny, 0, dx, 0.5 * dt, prm, bc);
+            sweep1_grid(m, planes, nx, ny, 1, dx, dt, prm, bc);
+            sweep1_grid(m, planes, nx, ny, 0, dx, 0.5 * dt, prm, bc);
+        }
+        t += dt;
+        it += 1;
+    }
+    if (steps_out) *steps_out = it;
+    return t;
+}
+
 double vo_run1d(int id, double* planes, int n, double dx, double cfl, double t_end, int max_steps, double w,
                 int lim, const double* prm, int bc, int subcycles, int* steps_out, double* dt_log) {
     return run(id, planes, n, 1, 1, dx, cfl, t_end, max_steps, w, lim, prm, bc, subcycles, steps_out, dt_log);

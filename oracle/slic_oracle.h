@@ -69,6 +69,10 @@ void vo_flux(int model, const double* u, int axis, const double* prm, double* f)
 void vo_slic_flux(int model, const double* wLL, const double* wL, const double* wR, const double* wRR,
                   int axis, double dx, double dt, double bias, int limiter, const double* prm, double* f);
 
+/* FirstOrderSolver::solve{,2D} and the MHD / HPR twins (ny == 1: 1D); the MHD c_h stays prm[2]. */
+double vo_run_first_order(int model, double* planes, int nx, int ny, double dx, double cfl, double t_end,
+                          int max_steps, const double* prm, int bc, int* steps_out);
+
 #ifdef __cplusplus
 }
 #endif

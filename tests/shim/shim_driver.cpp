@@ -3,12 +3,13 @@
 // planes to a binary file for tests/test_shim_gpu.py to compare with the oracle.
 //   shim_driver <out.bin>
 // Output, in order (float64): Euler 1D solve (6 x 200), Euler 2D per-sweep loop (6 x 24 x 20),
-// MHD solve2D (9 x 16 x 16), HPR solve (17 x 50), Euler 1D step-count solve (6 x 150), then the number of 2D
-// steps the per-sweep loop took.
+// MHD solve2D (9 x 16 x 16), HPR solve (17 x 50), Euler 1D step-count solve (6 x 150), Euler 1D first-order solve
+// (6 x 150), then the number of 2D steps the per-sweep loop took.
 #include <cmath>
 #include <cstdio>
 #include <vector>
 
+#include "Solvers/firstordersolver.h"
 #include "Solvers/secondordersolver.h"
 
 using std::vector;
@@ -105,6 +106,19 @@ int main(int argc, char** argv) {
         for (int i = 0; i < n; i++)
             cells[i] = i <= 0.5 * n ? EulerStateVector(1.0, 0.0, 0.0, 0.0, 1.0) : EulerStateVector(0.125, 0.0, 0.0, 0.0, 0.1);
         vector<EulerStateVector> out = SecondOrderSolver::solve(cells, 1.0 / n, 0.8, 0.0, 0.0, 0, 0, mp, 37);
+        vector<double> v;
+        for (int k = 0; k < 6; k++)
+            for (auto& c : out) v.push_back(c.computePrimitiveVariableVector()[k]);
+        put(f, v);
+    }
+    // 6) FirstOrderSolver::solve on the same shock tube, to t = 0.05
+    {
+        int n = 150;
+        vector<EulerStateVector> cells(n);
+        EulerMaterialParameters mp(1.4);
+        for (int i = 0; i < n; i++)
+            cells[i] = i <= 0.5 * n ? EulerStateVector(1.0, 0.0, 0.0, 0.0, 1.0) : EulerStateVector(0.125, 0.0, 0.0, 0.0, 0.1);
+        vector<EulerStateVector> out = FirstOrderSolver::solve(cells, 1.0 / n, 0.8, 0.05, 0, mp);
         vector<double> v;
         for (int k = 0; k < 6; k++)
             for (auto& c : out) v.push_back(c.computePrimitiveVariableVector()[k]);

@@ -161,3 +161,28 @@ def test_oracle_vs_reference_mhd_glm_subcycles(bc):
     O.run(O.MHD, a, 1 / 60, 0.8, steps=8, limiter=1, params=wl.mhd_params(2.0), bc=bc, subcycles=3)
     O.ref_run(O.MHD, b, 1 / 60, 0.8, steps=8, limiter=1, params=wl.mhd_params(2.0), bc=bc, subcycles=3)
     assert np.array_equal(a, b)
+
+
+def _first_order_cases():
+    return [
+        ("euler1d", O.EULER, wl.sod_1d(100), wl.euler_params(1.4), 1 / 100, 0),
+        ("euler2d", O.EULER, wl.euler_quadrants_2d(24, 20, seed=3), wl.euler_params(1.4), 1 / 24, 0),
+        ("euler2d_periodic", O.EULER, wl.euler_quadrants_2d(24, 20, seed=3), wl.euler_params(1.4), 1 / 24, 1),
+        ("mhd2d_periodic", O.MHD, wl.mhd_vortex_2d(20, 16, seed=2), wl.mhd_params(5 / 3, c_h=1.3), 1 / 20, 1),
+        ("mhd1d", O.MHD, wl.brio_wu_1d(80), wl.mhd_params(2.0, c_h=0.7), 1 / 80, 0),
+        ("hpr2d", O.HPR, wl.hpr_smooth_2d(16, 14, seed=5), wl.hpr_params(), 1 / 16, 0),
+        ("hpr1d_periodic", O.HPR, wl.hpr_heat_conduction_1d(40), wl.hpr_params(), 1 / 40, 1),
+    ]
+
+
+@pytest.mark.parametrize("case", _first_order_cases(), ids=lambda c: c[0])
+def test_oracle_vs_reference_first_order(case):
+    """FirstOrderSolver / MHDFirstOrderSolver / HPRFirstOrderSolver loops, bit for bit (the MHD c_h is not reset)."""
+    if not O.ref_available():
+        pytest.skip("compiled reference not built")
+    _, model, W, prm, dx, bc = case
+    a, b = W.copy(), W.copy()
+    ta = O.run_first_order(model, a, dx, 0.8, steps=7, params=prm, bc=bc)
+    tb = O.ref_run_first_order(model, b, dx, 0.8, steps=7, params=prm, bc=bc)
+    assert ta == tb
+    assert np.array_equal(a, b)

@@ -82,5 +82,11 @@ def test_shim_driver_matches_oracle(gpu, oracle_lib, tmp_path):
     O.run(O.EULER, ref, 1 / 150, 0.8, steps=37, limiter=0, params=wl.euler_params(1.4))
     assert np.array_equal(got, ref)
 
+    # 6) FirstOrderSolver::solve, to t = 0.05
+    got = take((6, 150))
+    ref = wl.sod_1d(150)
+    O.run_first_order(O.EULER, ref, 1 / 150, 0.8, t_end=0.05, params=wl.euler_params(1.4))
+    assert np.array_equal(got, ref)
+
     assert take((1,))[0] == 6
     assert off == data.size

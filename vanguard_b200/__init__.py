@@ -43,7 +43,7 @@ class GridDesc(ctypes.Structure):
 class RunConfig(ctypes.Structure):
     _fields_ = [("dx", ctypes.c_double), ("cfl", ctypes.c_double), ("t_end", ctypes.c_double),
                 ("max_steps", ctypes.c_int), ("bias", ctypes.c_double), ("limiter", ctypes.c_int),
-                ("subcycles", ctypes.c_int)]
+                ("subcycles", ctypes.c_int), ("order", ctypes.c_int)]
 
 
 # Every function the C ABI header declares (tests check the library exports them all).
@@ -173,8 +173,9 @@ class Solver:
         return a
 
     def run(self, dx, cfl, t_end=0.0, steps=0, bias=0.0, limiter=SUPERBEE, subcycles=0, stream=None,
-            allow_nan=False):
-        c = RunConfig(dx, cfl, t_end, steps, bias, limiter, subcycles)
+            allow_nan=False, order=2):
+        """The solve() time loop on the device; order=1 runs FirstOrderSolver's FORCE loop instead."""
+        c = RunConfig(dx, cfl, t_end, steps, bias, limiter, subcycles, order)
         it = ctypes.c_int()
         t = ctypes.c_double()
         _check(lib().vg_run(self._h, ctypes.byref(c), ctypes.byref(it), ctypes.byref(t), stream),
@@ -186,7 +187,7 @@ class Solver:
         """Host-buffer round trip through vg_solve (upload, run, download)."""
         a = np.ascontiguousarray(planes_in, dtype=np.float64)
         o = np.empty_like(a) if out is None else out
-        c = RunConfig(dx, cfl, t_end, steps, bias, limiter, subcycles)
+        c = RunConfig(dx, cfl, t_end, steps, bias, limiter, subcycles, 2)
         it = ctypes.c_int()
         t = ctypes.c_double()
         _check(lib().vg_solve(self._h, a.ctypes.data_as(ctypes.c_void_p), o.ctypes.data_as(ctypes.c_void_p),
@@ -212,7 +213,7 @@ class Solver:
 
     def autotune(self, dx, cfl, bias=0.0, limiter=SUPERBEE, reps=3, measure=True, stream=None):
         """Pick the fastest sweep tile shapes on the uploaded state; returns (x_times, y_times) in ms."""
-        c = RunConfig(dx, cfl, 0.0, 1, bias, limiter, 0)
+        c = RunConfig(dx, cfl, 0.0, 1, bias, limiter, 0, 2)
         times = (ctypes.c_float * (NUM_XCFG + NUM_YCFG))() if measure else None
         _check(lib().vg_autotune(self._h, ctypes.byref(c), reps, times, stream))
         if times is None:

@@ -1,6 +1,7 @@
 // Exact-FP64 SLIC kernels.  This translation unit MUST be compiled with -fmad=false: the reference's
 // x86-64 build forms no fused multiply-adds, and bitwise parity depends on every product being rounded
 // before it is added.
+#include "first_order_kernels.cuh"
 #include "forcing_kernels.cuh"
 #include "physics_fp64.cuh"
 #include "physics_hpr.cuh"
@@ -54,6 +55,24 @@ cudaError_t forcing_impl(const SweepArgs& a, int subcycles, cudaStream_t st) {
     return cudaGetLastError();
 }
 
+template <class M>
+cudaError_t force1_x(const SweepArgs& a, cudaStream_t st) {
+    constexpr int P = 128;
+    force1_x_kernel<M, P><<<dim3((a.nx + P - 1) / P, a.ny), P, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+template <class M>
+cudaError_t force1_y(const SweepArgs& a, cudaStream_t st) {
+    if constexpr (!M::HAS_Y) {
+        return cudaErrorInvalidValue;
+    } else {
+        constexpr int TX = 64, TY = 64;
+        force1_y_kernel<M, TX, TY><<<dim3((a.nx + TX - 1) / TX, (a.ny + TY - 1) / TY), TX, 0, st>>>(a);
+        return cudaGetLastError();
+    }
+}
+
 using ForcingFn = cudaError_t (*)(const SweepArgs&, int, cudaStream_t);
 
 template <class M>
@@ -71,7 +90,9 @@ constexpr Ops make_ops() {
                &step_begin_impl<M>,
                &finish_impl<M>,
                forcing_of<M>(),
-               (M::NU > 9)};
+               (M::NU > 9),
+               &force1_x<M>,
+               &force1_y<M>};
 }
 
 const Ops kOps[V_COUNT] = {

@@ -348,7 +348,7 @@ __global__ void step_begin_kernel(Ctrl* c, SweepArgs a) {
         if (it <= 5) dt *= 0.2;
         if ((c->t + dt) > c->t_end) dt = c->t_end - c->t;
         c->dt = dt;
-        c->ch = S;
+        c->ch = a.ch_fixed ? a.ch_host : S;
         for (int i = 0; i < 2; i++) {
             sweep_scale(dt * (i == 0 ? 0.5 : 1.0), c->dx, c->kr[i], c->krinv[i], c->khalf_r[i]);
             c->kr_f[i] = (float)c->kr[i];

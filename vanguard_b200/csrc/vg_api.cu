@@ -193,10 +193,17 @@ int enqueue_step(vg_solver* s, const vg_run_config& c, int from, cudaStream_t st
     a.dx = c.dx;
     a.bias = c.bias;
     a.limiter = c.limiter;
+    // FirstOrderSolver's loop: FORCE sweeps, no source (its sub-cycle loop is empty), c_h as given
+    const bool first = c.order == 1;
+    a.ch_fixed = first;
+    auto sweep = [&](int axis, const SweepArgs& sa) {
+        if (!first) return run_sweep(s, axis, sa, st);
+        return (axis == 0 ? s->ops->x1 : s->ops->y1)(prepared(sa), st);
+    };
     int n = 0;
     cudaError_t e = s->ops->step_begin(a, st);
     n++;
-    const int sub = (s->ops->forcing && c.subcycles > 0) ? c.subcycles : 0;
+    const int sub = (!first && s->ops->forcing && c.subcycles > 0) ? c.subcycles : 0;
     from = enqueue_forcing(s, a, sub, from, st, &e, &n);
     // Without a trailing source pass the last sweep folds the next step's CFL maximum into its epilogue;
     // with one, a separate reduction runs after it.
@@ -206,7 +213,7 @@ int enqueue_step(vg_solver* s, const vg_run_config& c, int from, cudaStream_t st
         a.out = s->buf[1 - from];
         a.accumulate_wave = fuse_wave;
         a.advance_time = 1;
-        if (e == cudaSuccess) e = run_sweep(s, 0, a, st);
+        if (e == cudaSuccess) e = sweep(0, a);
         n++;
         from = 1 - from;
     } else {
@@ -214,17 +221,17 @@ int enqueue_step(vg_solver* s, const vg_run_config& c, int from, cudaStream_t st
         a.in = s->buf[from];
         a.out = s->buf[1 - from];
         a.dt_scale = 0.5;
-        if (e == cudaSuccess) e = run_sweep(s, 0, a, st);
+        if (e == cudaSuccess) e = sweep(0, a);
         a.in = s->buf[1 - from];
         a.out = s->buf[from];
         a.dt_scale = 1.0;
-        if (e == cudaSuccess) e = run_sweep(s, 1, a, st);
+        if (e == cudaSuccess) e = sweep(1, a);
         a.in = s->buf[from];
         a.out = s->buf[1 - from];
         a.dt_scale = 0.5;
         a.accumulate_wave = fuse_wave;
         a.advance_time = 1;
-        if (e == cudaSuccess) e = run_sweep(s, 0, a, st);
+        if (e == cudaSuccess) e = sweep(0, a);
         n += 3;
         from = 1 - from;
     }
@@ -275,8 +282,11 @@ vg_status capture(vg_solver* s, const vg_run_config& c, int steps, int from, cud
     return VG_OK;
 }
 
+int order_of(const vg_run_config& c) { return c.order == 1 ? 1 : 2; }
+
 bool same_cfg(const vg_run_config& a, const vg_run_config& b) {
-    return a.dx == b.dx && a.bias == b.bias && a.limiter == b.limiter && a.subcycles == b.subcycles;
+    return a.dx == b.dx && a.bias == b.bias && a.limiter == b.limiter && a.subcycles == b.subcycles &&
+           order_of(a) == order_of(b);
 }
 
 vg_status ensure_graphs(vg_solver* s, const vg_run_config& c) {
@@ -451,6 +461,8 @@ vg_status vg_run(vg_solver* s, const vg_run_config* cfg, int* steps_taken, doubl
     if (cfg->subcycles < 0) return fail(VG_EINVAL, "subcycles must be >= 0");
     if (cfg->subcycles > 0 && !s->ops->forcing)
         return fail(VG_EUNSUPPORTED, "source sub-cycling needs a model with a source (HPR relaxation, MHD GLM damping)");
+    if (cfg->order != 0 && cfg->order != 1 && cfg->order != 2) return fail(VG_EINVAL, "order must be 1 or 2");
+    if (cfg->order == 1 && !s->ops->x1) return fail(VG_EUNSUPPORTED, "the first-order loop runs in VG_FP64 only");
     cudaStream_t st = (cudaStream_t)stream;
     VG_CUDA(cudaSetDevice(s->d.device));
 
@@ -501,7 +513,7 @@ vg_status vg_run(vg_solver* s, const vg_run_config* cfg, int* steps_taken, doubl
             if (!(h->t < h->t_end) || h->it >= h->max_steps) break;
         }
     }
-    launches += launched_steps * kernels_per_step(s, cfg->subcycles);
+    launches += launched_steps * kernels_per_step(s, cfg->order == 1 ? 0 : cfg->subcycles);
     // every step is an odd number of sweeps in 2D (3) and 1 in 1D: the state ends in buffer (steps & 1)
     s->cur = (int)(launched_steps & 1);
     VG_CUDA(cudaMemcpyAsync(h, s->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));

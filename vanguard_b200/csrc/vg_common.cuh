@@ -83,6 +83,7 @@ struct SweepArgs {
     int accumulate_wave;     // fold max wave speed of the output into *wave_acc
     int advance_time;        // last sweep of a step: ctrl->t += dt, ctrl->it += 1
     int dims;                // 1 or 2 (selects the wave-speed formula)
+    int ch_fixed;            // step_begin keeps ctrl->ch = ch_host instead of this step's maximum (first order)
     unsigned long long* wave_acc;  // running maximum (bit pattern), usually &ctrl->smax_next
     unsigned int* err;             // error word (always valid)
     double* aux;                   // model scratch planes (HPR forcing neighbours), or null

@@ -35,6 +35,9 @@ struct Ops {
     // (kForcingLaunches kernels; null: model has no source).
     cudaError_t (*forcing)(const SweepArgs& a, int subcycles, cudaStream_t st);
     bool big_tiles;  // SweepTable<.., BIG = true> (names of the launch configurations)
+    // First-order FORCE sweeps (FirstOrderSolver), null where the form has none.
+    SweepFn x1 = nullptr;
+    SweepFn y1 = nullptr;
 };
 
 constexpr int kForcingLaunches = 2;  // kernels per forcing sub-cycle

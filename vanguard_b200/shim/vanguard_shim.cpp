@@ -42,12 +42,13 @@ struct SolverDeleter {
 };
 using SolverPtr = std::unique_ptr<vg_solver, SolverDeleter>;
 
-SolverPtr make_solver(int model, int nx, int ny, int boundary, const double* params, int nparams) {
+// prec < 0: the form VG_PRECISION selects
+SolverPtr make_solver(int model, int nx, int ny, int boundary, const double* params, int nparams, int prec = -1) {
     vg_grid_desc d{};
     d.model = model;
     d.nx = nx;
     d.ny = ny;
-    d.precision = precision();
+    d.precision = prec < 0 ? precision() : prec;
     d.boundary = boundary;
     d.device = device();
     for (int i = 0; i < nparams && i < VG_MAX_PARAMS; i++) d.params[i] = params[i];
@@ -69,8 +70,9 @@ vg_solver* cached_solver(int model, int nx, int ny, int boundary, const double* 
 // Runs solve()/solve2D()'s time loop (finalTime-driven) on reference-order primitive planes, in place.
 // maxSteps > 0 also stops the loop after that many steps (the shim's step-count overloads).
 void run_planes(int model, std::vector<double>& planes, int nx, int ny, const double* params, int nparams, double dx,
-                double cfl, double tEnd, double bias, int limiter, int subcycles, int maxSteps = 0) {
-    SolverPtr s = make_solver(model, nx, ny, VG_TRANSMISSIVE, params, nparams);
+                double cfl, double tEnd, double bias, int limiter, int subcycles, int maxSteps = 0, int order = 2) {
+    // the first-order loop exists in the plain FP64 form only
+    SolverPtr s = make_solver(model, nx, ny, VG_TRANSMISSIVE, params, nparams, order == 1 ? VG_FP64 : -1);
     vg_run_config c{};
     c.dx = dx;
     c.cfl = cfl;
@@ -79,6 +81,7 @@ void run_planes(int model, std::vector<double>& planes, int nx, int ny, const do
     c.bias = bias;
     c.limiter = limiter;
     c.subcycles = subcycles;
+    c.order = order;
     vg_status st = vg_solve(s.get(), planes.data(), planes.data(), &c, nullptr, nullptr, nullptr);
     if (st != VG_OK && st != VG_ENAN) raise(st, "vg_solve");  // non-finite results are returned, as the reference does
 }
@@ -585,5 +588,87 @@ vector<vector<HPRStateVector> > HPRSecondOrderSolver::solve2D(vector<vector<HPRS
     std::vector<double> p = pack2(initialCells, 17, hpr_get);
     long ny = initialCells.size(), nx = initialCells[0].size();
     run_planes(VG_MODEL_HPR, p, (int)nx, (int)ny, prm, 12, dx, cfl, tEnd, bias, limiter, subcycles, maxSteps);
+    return unpack2<HPRStateVector>(p, nx, ny, 17, hpr_make);
+}
+
+// ------------------------------------------------------------------------------------------- first order
+vector<EulerStateVector> FirstOrderSolver::solve(vector<EulerStateVector>& initialCells, double dx, double cfl, double tEnd,
+                                                 int subcycles, EulerMaterialParameters mp) {
+    return solve(initialCells, dx, cfl, tEnd, subcycles, mp, 0);
+}
+vector<EulerStateVector> FirstOrderSolver::solve(vector<EulerStateVector>& initialCells, double dx, double cfl, double tEnd,
+                                                 int, EulerMaterialParameters mp, int maxSteps) {
+    double prm[6];
+    euler_params(mp, prm);
+    std::vector<double> p = pack(initialCells, 6, euler_get);
+    run_planes(VG_MODEL_EULER, p, (int)initialCells.size(), 1, prm, 6, dx, cfl, tEnd, 0.0, 0, 0, maxSteps, 1);
+    return unpack<EulerStateVector>(p, initialCells.size(), 6, euler_make);
+}
+vector<vector<EulerStateVector> > FirstOrderSolver::solve2D(vector<vector<EulerStateVector> >& initialCells, double dx,
+                                                            double cfl, double tEnd, int subcycles, EulerMaterialParameters mp) {
+    return solve2D(initialCells, dx, cfl, tEnd, subcycles, mp, 0);
+}
+vector<vector<EulerStateVector> > FirstOrderSolver::solve2D(vector<vector<EulerStateVector> >& initialCells, double dx,
+                                                            double cfl, double tEnd, int, EulerMaterialParameters mp,
+                                                            int maxSteps) {
+    double prm[6];
+    euler_params(mp, prm);
+    std::vector<double> p = pack2(initialCells, 6, euler_get);
+    long ny = initialCells.size(), nx = initialCells[0].size();
+    run_planes(VG_MODEL_EULER, p, (int)nx, (int)ny, prm, 6, dx, cfl, tEnd, 0.0, 0, 0, maxSteps, 1);
+    return unpack2<EulerStateVector>(p, nx, ny, 6, euler_make);
+}
+
+vector<MHDStateVector> MHDFirstOrderSolver::solve(vector<MHDStateVector>& initialCells, double dx, double cfl, double tEnd,
+                                                  int subcycles, MHDMaterialParameters mp) {
+    return solve(initialCells, dx, cfl, tEnd, subcycles, mp, 0);
+}
+vector<MHDStateVector> MHDFirstOrderSolver::solve(vector<MHDStateVector>& initialCells, double dx, double cfl, double tEnd,
+                                                  int, MHDMaterialParameters mp, int maxSteps) {
+    double prm[3];
+    mhd_params(mp, prm);
+    std::vector<double> p = pack(initialCells, 9, mhd_get);
+    run_planes(VG_MODEL_MHD, p, (int)initialCells.size(), 1, prm, 3, dx, cfl, tEnd, 0.0, 0, 0, maxSteps, 1);
+    return unpack<MHDStateVector>(p, initialCells.size(), 9, mhd_make);
+}
+vector<vector<MHDStateVector> > MHDFirstOrderSolver::solve2D(vector<vector<MHDStateVector> >& initialCells, double dx,
+                                                             double cfl, double tEnd, int subcycles, MHDMaterialParameters mp) {
+    return solve2D(initialCells, dx, cfl, tEnd, subcycles, mp, 0);
+}
+vector<vector<MHDStateVector> > MHDFirstOrderSolver::solve2D(vector<vector<MHDStateVector> >& initialCells, double dx,
+                                                             double cfl, double tEnd, int, MHDMaterialParameters mp,
+                                                             int maxSteps) {
+    double prm[3];
+    mhd_params(mp, prm);
+    std::vector<double> p = pack2(initialCells, 9, mhd_get);
+    long ny = initialCells.size(), nx = initialCells[0].size();
+    run_planes(VG_MODEL_MHD, p, (int)nx, (int)ny, prm, 3, dx, cfl, tEnd, 0.0, 0, 0, maxSteps, 1);
+    return unpack2<MHDStateVector>(p, nx, ny, 9, mhd_make);
+}
+
+vector<HPRStateVector> HPRFirstOrderSolver::solve(vector<HPRStateVector>& initialCells, double dx, double cfl, double tEnd,
+                                                  int subcycles, HPRMaterialParameters mp) {
+    return solve(initialCells, dx, cfl, tEnd, subcycles, mp, 0);
+}
+vector<HPRStateVector> HPRFirstOrderSolver::solve(vector<HPRStateVector>& initialCells, double dx, double cfl, double tEnd,
+                                                  int, HPRMaterialParameters mp, int maxSteps) {
+    double prm[12];
+    hpr_params(mp, prm);
+    std::vector<double> p = pack(initialCells, 17, hpr_get);
+    run_planes(VG_MODEL_HPR, p, (int)initialCells.size(), 1, prm, 12, dx, cfl, tEnd, 0.0, 0, 0, maxSteps, 1);
+    return unpack<HPRStateVector>(p, initialCells.size(), 17, hpr_make);
+}
+vector<vector<HPRStateVector> > HPRFirstOrderSolver::solve2D(vector<vector<HPRStateVector> >& initialCells, double dx,
+                                                             double cfl, double tEnd, int subcycles, HPRMaterialParameters mp) {
+    return solve2D(initialCells, dx, cfl, tEnd, subcycles, mp, 0);
+}
+vector<vector<HPRStateVector> > HPRFirstOrderSolver::solve2D(vector<vector<HPRStateVector> >& initialCells, double dx,
+                                                             double cfl, double tEnd, int, HPRMaterialParameters mp,
+                                                             int maxSteps) {
+    double prm[12];
+    hpr_params(mp, prm);
+    std::vector<double> p = pack2(initialCells, 17, hpr_get);
+    long ny = initialCells.size(), nx = initialCells[0].size();
+    run_planes(VG_MODEL_HPR, p, (int)nx, (int)ny, prm, 12, dx, cfl, tEnd, 0.0, 0, 0, maxSteps, 1);
     return unpack2<HPRStateVector>(p, nx, ny, 17, hpr_make);
 }

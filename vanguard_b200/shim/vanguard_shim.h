@@ -289,6 +289,52 @@ public:
                                                    int subcyclingIterations, MHDMaterialParameters mp, int maxSteps);
 };
 
+// FirstOrderSolver / MHDFirstOrderSolver / HPRFirstOrderSolver::solve{,2D} (Solvers/firstordersolver.h:86-97,
+// Solvers/mhdfirstordersolver.h:77-90, Solvers/hprfirstordersolver.h:77-90): FORCE of the cells themselves over a
+// 1-ghost boundary; subcyclingIterations is accepted and, as in the reference, does nothing.  The maxSteps
+// overloads (not in the reference) also stop after that many steps.
+class FirstOrderSolver {
+public:
+    static vector<EulerStateVector> solve(vector<EulerStateVector>& initialCells, double cellSpacing, double CFLCoefficient,
+                                          double finalTime, int subcyclingIterations, EulerMaterialParameters mp);
+    static vector<vector<EulerStateVector> > solve2D(vector<vector<EulerStateVector> >& initialCells, double cellSpacing,
+                                                     double CFLCoefficient, double finalTime, int subcyclingIterations,
+                                                     EulerMaterialParameters mp);
+    static vector<EulerStateVector> solve(vector<EulerStateVector>& initialCells, double cellSpacing, double CFLCoefficient,
+                                          double finalTime, int subcyclingIterations, EulerMaterialParameters mp, int maxSteps);
+    static vector<vector<EulerStateVector> > solve2D(vector<vector<EulerStateVector> >& initialCells, double cellSpacing,
+                                                     double CFLCoefficient, double finalTime, int subcyclingIterations,
+                                                     EulerMaterialParameters mp, int maxSteps);
+};
+
+class MHDFirstOrderSolver {
+public:
+    static vector<MHDStateVector> solve(vector<MHDStateVector>& initialCells, double cellSpacing, double CFLCoefficient,
+                                        double finalTime, int subcyclingIterations, MHDMaterialParameters mp);
+    static vector<vector<MHDStateVector> > solve2D(vector<vector<MHDStateVector> >& initialCells, double cellSpacing,
+                                                   double CFLCoefficient, double finalTime, int subcyclingIterations,
+                                                   MHDMaterialParameters mp);
+    static vector<MHDStateVector> solve(vector<MHDStateVector>& initialCells, double cellSpacing, double CFLCoefficient,
+                                        double finalTime, int subcyclingIterations, MHDMaterialParameters mp, int maxSteps);
+    static vector<vector<MHDStateVector> > solve2D(vector<vector<MHDStateVector> >& initialCells, double cellSpacing,
+                                                   double CFLCoefficient, double finalTime, int subcyclingIterations,
+                                                   MHDMaterialParameters mp, int maxSteps);
+};
+
+class HPRFirstOrderSolver {
+public:
+    static vector<HPRStateVector> solve(vector<HPRStateVector>& initialCells, double cellSpacing, double CFLCoefficient,
+                                        double finalTime, int subcyclingIterations, HPRMaterialParameters mp);
+    static vector<vector<HPRStateVector> > solve2D(vector<vector<HPRStateVector> >& initialCells, double cellSpacing,
+                                                   double CFLCoefficient, double finalTime, int subcyclingIterations,
+                                                   HPRMaterialParameters mp);
+    static vector<HPRStateVector> solve(vector<HPRStateVector>& initialCells, double cellSpacing, double CFLCoefficient,
+                                        double finalTime, int subcyclingIterations, HPRMaterialParameters mp, int maxSteps);
+    static vector<vector<HPRStateVector> > solve2D(vector<vector<HPRStateVector> >& initialCells, double cellSpacing,
+                                                   double CFLCoefficient, double finalTime, int subcyclingIterations,
+                                                   HPRMaterialParameters mp, int maxSteps);
+};
+
 class HPRSecondOrderSolver {
 public:
     static vector<HPRStateVector> solve(vector<HPRStateVector>& initialCells, double cellSpacing, double CFLCoefficient,
