@@ -490,27 +490,36 @@ def hpr_leg(local, stream, sh):
     tau1, tau2 = wl.hpr_relaxation_times(SEED)
     prm = wl.hpr_params(tau1=tau1, tau2=tau2)
     W = wl.hpr_smooth_2d(n, seed=SEED)
-    with vg.Solver(vg.HPR, n, n, prm, device=local) as s:
-        s.upload(W, stream=sh)
-        S0 = s.max_wave_speed(stream=sh)
-        dt_est = 1.5 * CFL * (1.0 / n) / S0
-        sub = max(1, math.ceil(0.5 * dt_est / (2.5 * min(tau1, tau2))))
-        s.autotune(1.0 / n, CFL, limiter=LIMITER, stream=sh)
-        s.run(1.0 / n, CFL, steps=2, limiter=LIMITER, subcycles=sub, stream=sh)
-        s.upload(W, stream=sh)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        e0.record(stream)
-        t, it = s.run(1.0 / n, CFL, steps=C4_STEPS, limiter=LIMITER, subcycles=sub, stream=sh, allow_nan=True)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1)
-        fin = s.download(stream=sh)
-        launches = s.last_launch_count()
-    return {"workload": f"2D HPR {n}x{n} smooth field (seeded), thermal ideal gas, tau1 {tau1:.3e}, tau2 {tau2:.3e}, "
-                        f"superbee, CFL 0.8, {C4_STEPS} steps, RK4 forcing with {sub} sub-cycles per half step",
-            "subcycles": sub, "steps": it, "t": t, "ms": ms, "cell_updates_per_s": n * n * it / (ms / 1e3),
-            "launches": launches, "finite": bool(np.isfinite(fin).all()), "precision": "fp64"}
+    res, finals, sub = {}, {}, 1
+    for name, prec in (("fp64", vg.FP64), ("mixed", vg.MIXED)):
+        with vg.Solver(vg.HPR, n, n, prm, precision=prec, device=local) as s:
+            s.upload(W, stream=sh)
+            if name == "fp64":
+                S0 = s.max_wave_speed(stream=sh)
+                dt_est = 1.5 * CFL * (1.0 / n) / S0
+                sub = max(1, math.ceil(0.5 * dt_est / (2.5 * min(tau1, tau2))))
+            s.autotune(1.0 / n, CFL, limiter=LIMITER, stream=sh)
+            s.run(1.0 / n, CFL, steps=2, limiter=LIMITER, subcycles=sub, stream=sh)
+            s.upload(W, stream=sh)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            t, it = s.run(1.0 / n, CFL, steps=C4_STEPS, limiter=LIMITER, subcycles=sub, stream=sh, allow_nan=True)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            finals[name] = s.download(stream=sh)
+            res[name] = {"ms": ms, "steps": it, "t": t, "cell_updates_per_s": n * n * it / (ms / 1e3),
+                         "launches": s.last_launch_count(), "finite": bool(np.isfinite(finals[name]).all())}
+    d = np.abs(finals["mixed"] - finals["fp64"])
+    res["mixed_error_vs_fp64"] = {"rho_L1": float(d[0].mean()), "rho_Linf": float(d[0].max()),
+                                  "all_L1": float(d.mean())}
+    res["mixed_speedup"] = res["fp64"]["ms"] / res["mixed"]["ms"]
+    res["subcycles"] = sub
+    res["workload"] = (f"2D HPR {n}x{n} smooth field (seeded), thermal ideal gas, tau1 {tau1:.3e}, tau2 {tau2:.3e}, "
+                       f"superbee, CFL 0.8, {C4_STEPS} steps, RK4 forcing (FP64 in both forms) with {sub} sub-cycles "
+                       f"per half step")
+    return res
 
 
 def sod_leg(local, stream, sh):
@@ -579,8 +588,8 @@ def main():
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--headline-only", action="store_true", help="skip the C1/C3/C5 measurements")
-    ap.add_argument("--legs", default="headline,c5,c3,c1",
-                    help="comma list of headline (C2), c5, c3, c1; without headline only those legs run (profiling)")
+    ap.add_argument("--legs", default="headline,c5,c4,c3,c1",
+                    help="comma list of headline (C2), c5, c4, c3, c1; without headline only those legs run (profiling)")
     ap.add_argument("--forms", default="fp64,mixed", help="C2 forms to run (profiling)")
     ap.add_argument("--c5-ninst", type=int, default=4096, help="C5 instances (smaller is for profiling only)")
     ap.add_argument("--c5-steps", type=int, default=500, help="C5 steps (smaller is for profiling only)")
