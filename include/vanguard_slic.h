@@ -81,6 +81,11 @@ typedef struct vg_run_config {
     int order;          /* 2 (or 0): SecondOrderSolver's SLIC loop; 1: FirstOrderSolver's FORCE loop
                          * (Solvers/firstordersolver.cpp:435-553 and the MHD / HPR twins: 1-ghost boundary, FORCE
                          * of the cells themselves, no source, the MHD c_h kept at params[2]; VG_FP64 only) */
+    int stiff_source;   /* HPR only, no counterpart in the reference: 1 replaces the RK4 forcing sub-cycles by a
+                         * stiff relaxation of dt/2 before and after the sweeps, cell by cell (distortion by implicit
+                         * Euler on the eigenvalues of A^T A, heat flux by exponential sub-steps), stable at any tau;
+                         * subcycles is then ignored.  Results approach the forcing's as its sub-cycles grow, not bit
+                         * for bit. */
 } vg_run_config;
 
 typedef struct vg_solver vg_solver;

@@ -465,6 +465,136 @@ static void hpr_source(const double* U, const double* prm, double* S) {
     }
 }
 
+/* ---- Stiff relaxation of the HPR source over a time h, cell by cell.  No counterpart in the reference, whose
+ * only source integrator is the explicit RK4 forcing solver (stable for sub-steps up to ~2.8 tau).
+ * Distortion: S_A = -c A dev(A^T A), c = 3 det(A)^(5/3) / tau1 (the non-plastic source above with dE/dA =
+ * c_s^2 A dev(A^T A)).  det A is conserved (dev is traceless), so c is constant; G = A^T A keeps its eigenvectors
+ * and its eigenvalues obey d(ln l_i)/dt = -2 c (l_i - mean(l)).  That system is integrated by implicit Euler
+ * (L-stable; Newton on three unknowns), then A <- A V diag(sqrt(l_i' / l_i)) V^T.
+ * Heat flux: d(rho J)/dt = -(rho0 T / (tau2 T0 rho)) rho J, integrated by exponential sub-steps with T from the
+ * current state.  rho, rho v and rho E do not change. */
+
+/* cyclic Jacobi eigen-decomposition of a symmetric 3x3 matrix: g = V diag(l) V^T (published method) */
+static void sym_eig3(const mat3* g, double l[3], double V[3][3]) {
+    double a[3][3];
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+            a[i][j] = g->m[i][j];
+            V[i][j] = i == j ? 1.0 : 0.0;
+        }
+    for (int sweep = 0; sweep < 16; sweep++) {
+        double off = a[0][1] * a[0][1] + a[0][2] * a[0][2] + a[1][2] * a[1][2];
+        double dia = a[0][0] * a[0][0] + a[1][1] * a[1][1] + a[2][2] * a[2][2];
+        if (off <= 1e-32 * dia) break;
+        for (int pq = 0; pq < 3; pq++) {
+            int p = pq == 2 ? 1 : 0, q = pq == 0 ? 1 : 2;
+            if (a[p][q] == 0.0) continue;
+            double theta = (a[q][q] - a[p][p]) / (2.0 * a[p][q]);
+            double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+            double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
+            double apq = a[p][q];
+            a[p][p] -= t * apq;
+            a[q][q] += t * apq;
+            a[p][q] = a[q][p] = 0.0;
+            for (int r = 0; r < 3; r++) {
+                if (r != p && r != q) {
+                    double arp = a[r][p], arq = a[r][q];
+                    a[r][p] = a[p][r] = c * arp - s * arq;
+                    a[r][q] = a[q][r] = s * arp + c * arq;
+                }
+                double vrp = V[r][p], vrq = V[r][q];
+                V[r][p] = c * vrp - s * vrq;
+                V[r][q] = s * vrp + c * vrq;
+            }
+        }
+    }
+    for (int i = 0; i < 3; i++) l[i] = a[i][i];
+}
+
+/* n implicit-Euler steps of d(mu_i)/dt = -2 c (exp(mu_i) - mean(exp(mu))) with k = 2 c h / n per step */
+static void relax_log_eigs(double mu[3], double k, int n) {
+    for (int s = 0; s < n; s++) {
+        double m0[3] = {mu[0], mu[1], mu[2]}, x[3] = {mu[0], mu[1], mu[2]};
+        for (int it = 0; it < 100; it++) {
+            double e[3] = {exp(x[0]), exp(x[1]), exp(x[2])};
+            double mean = (e[0] + e[1] + e[2]) / 3.0;
+            double F[3], J[3][3];
+            for (int i = 0; i < 3; i++) {
+                F[i] = (x[i] - m0[i]) + k * (e[i] - mean);
+                for (int j = 0; j < 3; j++) J[i][j] = (i == j ? 1.0 + k * e[i] : 0.0) - k * e[j] / 3.0;
+            }
+            /* J dx = -F by Cramer's rule */
+            double det = J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) - J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
+                         J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
+            double dx[3], big = 0.0;
+            for (int c = 0; c < 3; c++) {
+                double M[3][3];
+                for (int i = 0; i < 3; i++)
+                    for (int j = 0; j < 3; j++) M[i][j] = j == c ? -F[i] : J[i][j];
+                double dc = M[0][0] * (M[1][1] * M[2][2] - M[1][2] * M[2][1]) - M[0][1] * (M[1][0] * M[2][2] - M[1][2] * M[2][0]) +
+                            M[0][2] * (M[1][0] * M[2][1] - M[1][1] * M[2][0]);
+                dx[c] = dc / det;
+                if (fabs(dx[c]) > big) big = fabs(dx[c]);
+            }
+            double damp = big > 0.5 ? 0.5 / big : 1.0;
+            for (int i = 0; i < 3; i++) x[i] += damp * dx[i];
+            if (big < 1e-15) break;
+        }
+        for (int i = 0; i < 3; i++) mu[i] = x[i];
+    }
+}
+
+static int clampi(double v, int lo, int hi) {
+    if (!(v > lo)) return lo;
+    if (v > hi) return hi;
+    return (int)ceil(v);
+}
+
+static void hpr_relax_cell(double* U, double h, const double* prm) {
+    double rho = U[0];
+    mat3 A = load_A(U + 2);
+    double d = det3(&A);
+    if (!(d > 0.0) || !(h > 0.0)) return;
+    mat3 At = tr3(&A), G = mm3(&At, &A);
+    double l[3], V[3][3], mu[3];
+    sym_eig3(&G, l, V);
+    if (!(l[0] > 0.0 && l[1] > 0.0 && l[2] > 0.0)) return;
+    double c = 3.0 * (pow(d, 5.0 / 3.0) / prm[7]);
+    double lmax = fmax(l[0], fmax(l[1], l[2]));
+    int nA = clampi((2.0 * c * lmax * h) / 0.25, 1, 256);
+    for (int i = 0; i < 3; i++) mu[i] = log(l[i]);
+    relax_log_eigs(mu, 2.0 * c * (h / nA), nA);
+    /* A' = A V diag(sqrt(l'/l)) V^T */
+    double f[3], M[3][3];
+    for (int i = 0; i < 3; i++) f[i] = exp(0.5 * (mu[i] - log(l[i])));
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+            double sum = 0.0;
+            for (int k = 0; k < 3; k++) sum += V[i][k] * f[k] * V[j][k];
+            M[i][j] = sum;
+        }
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+            double sum = 0.0;
+            for (int k = 0; k < 3; k++) sum += A.m[i][k] * M[k][j];
+            U[2 + 3 * i + j] = sum;
+        }
+    if (!hpr_thermal(prm)) return;
+    mat3 An = load_A(U + 2);
+    double E = U[1] / rho, u = U[11] / rho, v = U[12] / rho, w = U[13] / rho;
+    double p0 = hpr_pressure(rho, E, u, v, w, &An, U[14] / rho, U[15] / rho, U[16] / rho, prm);
+    double k0 = (prm[3] * mg_temperature(rho, p0, prm)) / (prm[8] * prm[4] * rho);
+    int nJ = clampi(k0 * h, 1, 32);
+    double hs = h / nJ;
+    for (int s = 0; s < nJ; s++) {
+        double p = hpr_pressure(rho, E, u, v, w, &An, U[14] / rho, U[15] / rho, U[16] / rho, prm);
+        double T = mg_temperature(rho, p, prm);
+        double k = T > 0.0 ? (prm[3] * T) / (prm[8] * prm[4] * rho) : 0.0;
+        double fac = exp(-k * hs);
+        for (int i = 14; i < 17; i++) U[i] *= fac;
+    }
+}
+
 /* HPRAcousticTensor::computeMaximumWaveSpeed (HPR/hpracoustictensor.cpp:7-97) with the 10-step power
  * iteration of MatrixAlgebra::computeLargestEigenvalue (Mathematics/matrixalgebra.cpp:182-199).
  * Only the entries dsigma/dA[d][i][j][d] of HPREquationOfState::computeShearStressTensorDerivativeDistortionTensor
@@ -861,6 +991,20 @@ void vo_hpr_cell(const double* w, const double* prm, double* u, double* fx, doub
     speed_xy[1] = hpr_acoustic_speed(w, 1, prm);
 }
 
+/* the stiff relaxation of every cell of the grid (see hpr_relax_cell) */
+static void relax_grid(const model* m, double* planes, long plane, double h, const double* prm) {
+    int nv = m->nv;
+#pragma omp parallel for schedule(static)
+    for (long idx = 0; idx < plane; idx++) {
+        double W[MAXV], U[MAXV];
+        load_cell(planes, plane, idx, nv, W);
+        m->cons(W, prm, U);
+        hpr_relax_cell(U, h, prm);
+        m->setcons(U, prm, W);
+        for (int v = 0; v < nv; v++) planes[v * plane + idx] = W[v];
+    }
+}
+
 /* Solvers::computeStableTimeStep(dt, t, tEnd, it), Solvers/solvers.cpp:437-452 */
 static double stable_dt(double dt, double t, double t_end, int it) {
     double d = dt;
@@ -884,7 +1028,9 @@ static double run(int id, double* planes, int nx, int ny, int dims, double dx, d
     long plane = (long)nx * ny;
     double t = 0.0;
     int it = 0;
-    int sub = m->source ? subcycles : 0;
+    /* subcycles < 0 (HPR): the stiff relaxation of dt/2 before and after the sweeps instead of the RK4 forcing */
+    int stiff = id == VO_HPR && subcycles < 0;
+    int sub = (m->source && subcycles > 0) ? subcycles : 0;
     while (t < tEnd && it < limit) {
         double smax_ = max_wave(m, planes, plane, dims, prm);
         double dt = stable_dt(cfl * (dx / smax_), t, tEnd, it);
@@ -893,6 +1039,7 @@ static double run(int id, double* planes, int nx, int ny, int dims, double dx, d
         /* HPR relaxation / MHD GLM damping: sub-cycled RK4 source before and after the sweeps
          * (Solvers/hprsecondordersolver.cpp:323-341, :514-541; Solvers/mhdsecondordersolver.cpp:334-348, :517-540) */
         for (int s = 0; s < sub; s++) forcing_grid(m, planes, nx, ny, dims, dx, 0.5 * (dt / sub), w, lim, prm, bc);
+        if (stiff) relax_grid(m, planes, plane, 0.5 * dt, prm);
         if (dims == 1) {
             sweep_grid(m, planes, nx, 1, 0, dx, dt, w, lim, prm, bc);
         } else {
@@ -901,6 +1048,7 @@ static double run(int id, double* planes, int nx, int ny, int dims, double dx, d
             sweep_grid(m, planes, nx, ny, 0, dx, 0.5 * dt, w, lim, prm, bc);
         }
         for (int s = 0; s < sub; s++) forcing_grid(m, planes, nx, ny, dims, dx, 0.5 * (dt / sub), w, lim, prm, bc);
+        if (stiff) relax_grid(m, planes, plane, 0.5 * dt, prm);
         t += dt;
         it += 1;
     }

@@ -43,7 +43,7 @@ class GridDesc(ctypes.Structure):
 class RunConfig(ctypes.Structure):
     _fields_ = [("dx", ctypes.c_double), ("cfl", ctypes.c_double), ("t_end", ctypes.c_double),
                 ("max_steps", ctypes.c_int), ("bias", ctypes.c_double), ("limiter", ctypes.c_int),
-                ("subcycles", ctypes.c_int), ("order", ctypes.c_int)]
+                ("subcycles", ctypes.c_int), ("order", ctypes.c_int), ("stiff_source", ctypes.c_int)]
 
 
 # Every function the C ABI header declares (tests check the library exports them all).
@@ -173,9 +173,10 @@ class Solver:
         return a
 
     def run(self, dx, cfl, t_end=0.0, steps=0, bias=0.0, limiter=SUPERBEE, subcycles=0, stream=None,
-            allow_nan=False, order=2):
-        """The solve() time loop on the device; order=1 runs FirstOrderSolver's FORCE loop instead."""
-        c = RunConfig(dx, cfl, t_end, steps, bias, limiter, subcycles, order)
+            allow_nan=False, order=2, stiff=False):
+        """The solve() time loop on the device; order=1 runs FirstOrderSolver's FORCE loop instead; stiff=True
+        (HPR) relaxes the source over dt/2 before and after the sweeps instead of the RK4 forcing sub-cycles."""
+        c = RunConfig(dx, cfl, t_end, steps, bias, limiter, subcycles, order, 1 if stiff else 0)
         it = ctypes.c_int()
         t = ctypes.c_double()
         _check(lib().vg_run(self._h, ctypes.byref(c), ctypes.byref(it), ctypes.byref(t), stream),

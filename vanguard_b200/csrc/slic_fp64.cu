@@ -3,6 +3,7 @@
 // before it is added.
 #include "first_order_kernels.cuh"
 #include "forcing_kernels.cuh"
+#include "relax_kernels.cuh"
 #include "physics_fp64.cuh"
 #include "physics_hpr.cuh"
 #include "slic_kernels.cuh"
@@ -82,6 +83,19 @@ constexpr ForcingFn forcing_of() {
 }
 
 template <class M>
+cudaError_t relax_impl(const SweepArgs& a, cudaStream_t st) {
+    long n = (long)a.nx * a.ny;
+    relax_kernel<M><<<(unsigned)((n + 127) / 128), 128, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+template <class M>
+constexpr SweepFn relax_of() {
+    if constexpr (M::NW == 17) return &relax_impl<M>;
+    else return nullptr;
+}
+
+template <class M>
 constexpr Ops make_ops() {
     return Ops{M::NW,
                SweepTable<Fp64Kernels, M>::x,
@@ -92,7 +106,8 @@ constexpr Ops make_ops() {
                forcing_of<M>(),
                (M::NU > 9),
                &force1_x<M>,
-               &force1_y<M>};
+               &force1_y<M>,
+               relax_of<M>()};
 }
 
 const Ops kOps[V_COUNT] = {
@@ -110,6 +125,7 @@ const Ops* ops_fp64(int variant) { return (variant >= 0 && variant < V_COUNT) ? 
 cudaError_t hpr_forcing_fp64(const SweepArgs& a, int subcycles, cudaStream_t st) {
     return forcing_impl<HPRF64>(a, subcycles, st);
 }
+cudaError_t hpr_relax_fp64(const SweepArgs& a, cudaStream_t st) { return relax_impl<HPRF64>(a, st); }
 cudaError_t mhd7_forcing_fp64(const SweepArgs& a, int subcycles, cudaStream_t st) {
     return forcing_impl<MHDF64<false>>(a, subcycles, st);
 }

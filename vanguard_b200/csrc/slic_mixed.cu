@@ -46,9 +46,9 @@ using ForcingFn = cudaError_t (*)(const SweepArgs&, int, cudaStream_t);
 
 // The source sub-cycles keep FP64: the exact forcing kernels of each model
 template <class M>
-constexpr Ops make_ops(ForcingFn forcing = nullptr) {
+constexpr Ops make_ops(ForcingFn forcing = nullptr, SweepFn relax = nullptr) {
     return Ops{M::NW, SweepTable<MixedKernels, M>::x, SweepTable<MixedKernels, M>::y, &max_wave_impl<M>,
-               &step_begin_impl<M>, &finish_impl<M>, forcing, (M::NU > 9)};
+               &step_begin_impl<M>, &finish_impl<M>, forcing, (M::NU > 9), nullptr, nullptr, relax};
 }
 
 const Ops kOps[V_COUNT] = {
@@ -56,7 +56,7 @@ const Ops kOps[V_COUNT] = {
     make_ops<EulerMixed<2>>(),
     make_ops<MHDMixed<false>>(&mhd7_forcing_fp64),
     make_ops<MHDMixed<true>>(&mhd9_forcing_fp64),
-    make_ops<HPRMixed>(&hpr_forcing_fp64),
+    make_ops<HPRMixed>(&hpr_forcing_fp64, &hpr_relax_fp64),
 };
 
 }  // namespace

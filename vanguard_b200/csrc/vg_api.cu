@@ -203,11 +203,21 @@ int enqueue_step(vg_solver* s, const vg_run_config& c, int from, cudaStream_t st
     int n = 0;
     cudaError_t e = s->ops->step_begin(a, st);
     n++;
-    const int sub = (!first && s->ops->forcing && c.subcycles > 0) ? c.subcycles : 0;
+    const bool stiff = !first && c.stiff_source && s->ops->relax;
+    const int sub = (!first && !stiff && s->ops->forcing && c.subcycles > 0) ? c.subcycles : 0;
     from = enqueue_forcing(s, a, sub, from, st, &e, &n);
+    // stiff source: relaxation over dt/2 in place before and after the sweeps
+    auto relax = [&]() {
+        SweepArgs r = a;
+        r.in = r.out = s->buf[from];
+        r.dt_scale = 0.5;
+        if (e == cudaSuccess) e = s->ops->relax(r, st);
+        n++;
+    };
+    if (stiff) relax();
     // Without a trailing source pass the last sweep folds the next step's CFL maximum into its epilogue;
     // with one, a separate reduction runs after it.
-    const int fuse_wave = sub == 0;
+    const int fuse_wave = sub == 0 && !stiff;
     if (s->dims == 1) {
         a.in = s->buf[from];
         a.out = s->buf[1 - from];
@@ -239,6 +249,7 @@ int enqueue_step(vg_solver* s, const vg_run_config& c, int from, cudaStream_t st
     a.accumulate_wave = 0;
     a.advance_time = 0;
     from = enqueue_forcing(s, a, sub, from, st, &e, &n);
+    if (stiff) relax();
     if (!fuse_wave) {
         a.in = s->buf[from];
         if (e == cudaSuccess) e = s->ops->max_wave(a, st);
@@ -248,8 +259,9 @@ int enqueue_step(vg_solver* s, const vg_run_config& c, int from, cudaStream_t st
     return n;
 }
 
-int kernels_per_step(const vg_solver* s, int sub) {
+int kernels_per_step(const vg_solver* s, int sub, bool stiff = false) {
     int n = s->dims == 1 ? 2 : 4;
+    if (stiff) return n + 3;  // two relaxations and the separate CFL maximum
     if (s->ops->forcing && sub > 0) n += 2 * sub * vg::kForcingLaunches + 1;
     return n;
 }
@@ -286,7 +298,7 @@ int order_of(const vg_run_config& c) { return c.order == 1 ? 1 : 2; }
 
 bool same_cfg(const vg_run_config& a, const vg_run_config& b) {
     return a.dx == b.dx && a.bias == b.bias && a.limiter == b.limiter && a.subcycles == b.subcycles &&
-           order_of(a) == order_of(b);
+           order_of(a) == order_of(b) && (a.stiff_source != 0) == (b.stiff_source != 0);
 }
 
 vg_status ensure_graphs(vg_solver* s, const vg_run_config& c) {
@@ -463,6 +475,8 @@ vg_status vg_run(vg_solver* s, const vg_run_config* cfg, int* steps_taken, doubl
         return fail(VG_EUNSUPPORTED, "source sub-cycling needs a model with a source (HPR relaxation, MHD GLM damping)");
     if (cfg->order != 0 && cfg->order != 1 && cfg->order != 2) return fail(VG_EINVAL, "order must be 1 or 2");
     if (cfg->order == 1 && !s->ops->x1) return fail(VG_EUNSUPPORTED, "the first-order loop runs in VG_FP64 only");
+    if (cfg->stiff_source && cfg->order != 1 && !s->ops->relax)
+        return fail(VG_EUNSUPPORTED, "the stiff source relaxation exists for the HPR model only");
     cudaStream_t st = (cudaStream_t)stream;
     VG_CUDA(cudaSetDevice(s->d.device));
 
@@ -513,7 +527,8 @@ vg_status vg_run(vg_solver* s, const vg_run_config* cfg, int* steps_taken, doubl
             if (!(h->t < h->t_end) || h->it >= h->max_steps) break;
         }
     }
-    launches += launched_steps * kernels_per_step(s, cfg->order == 1 ? 0 : cfg->subcycles);
+    const bool stiff = cfg->order != 1 && cfg->stiff_source && s->ops->relax;
+    launches += launched_steps * kernels_per_step(s, cfg->order == 1 || stiff ? 0 : cfg->subcycles, stiff);
     // every step is an odd number of sweeps in 2D (3) and 1 in 1D: the state ends in buffer (steps & 1)
     s->cur = (int)(launched_steps & 1);
     VG_CUDA(cudaMemcpyAsync(h, s->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));

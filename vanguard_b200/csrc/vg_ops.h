@@ -38,6 +38,8 @@ struct Ops {
     // First-order FORCE sweeps (FirstOrderSolver), null where the form has none.
     SweepFn x1 = nullptr;
     SweepFn y1 = nullptr;
+    // Stiff relaxation of the source over dt * a.dt_scale, in place on a.out (HPR), null where the model has none.
+    SweepFn relax = nullptr;
 };
 
 constexpr int kForcingLaunches = 2;  // kernels per forcing sub-cycle
@@ -50,6 +52,8 @@ const Ops* ops_mixed(int variant);
 cudaError_t hpr_forcing_fp64(const SweepArgs& a, int subcycles, cudaStream_t st);
 cudaError_t mhd7_forcing_fp64(const SweepArgs& a, int subcycles, cudaStream_t st);
 cudaError_t mhd9_forcing_fp64(const SweepArgs& a, int subcycles, cudaStream_t st);
+// The stiff HPR relaxation (slic_fp64.cu), FP64 in both forms.
+cudaError_t hpr_relax_fp64(const SweepArgs& a, cudaStream_t st);
 
 // Record the text returned by vg_last_error_string() on this thread.
 void set_last_error(const std::string& msg);
