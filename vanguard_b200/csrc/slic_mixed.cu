@@ -52,8 +52,8 @@ constexpr Ops make_ops(ForcingFn forcing = nullptr, SweepFn relax = nullptr) {
 }
 
 const Ops kOps[V_COUNT] = {
-    make_ops<EulerMixed<1>>(),
-    make_ops<EulerMixed<2>>(),
+    make_ops<EulerF32<1>>(),
+    make_ops<EulerF32<2>>(),
     make_ops<MHDMixed<false>>(&mhd7_forcing_fp64),
     make_ops<MHDMixed<true>>(&mhd9_forcing_fp64),
     make_ops<HPRMixed>(&hpr_forcing_fp64, &hpr_relax_fp64),

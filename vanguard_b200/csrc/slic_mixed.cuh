@@ -25,11 +25,64 @@ __device__ __forceinline__ double limiter_approx(double r, double w, int id) {
     return fmin(1.0, xi_r);
 }
 
+// FP32 twin of limiter_approx for models whose reconstruction is FP32.
+__device__ __forceinline__ float limiter_approx(float r, float w, int id) {
+    if (r < 0.0f) return 0.0f;
+    float xi_r = 2.0f * rcp_approx_f((1.0f - w) + (1.0f + w) * r);
+    if (id == 0) {
+        if (r < 0.5f) return 2.0f * r;
+        if (r < 1.0f) return 1.0f;
+        return fminf(fminf(r, xi_r), 2.0f);
+    } else if (id == 1) {
+        return fminf(2.0f * r * rcp_approx_f(1.0f + r), xi_r);
+    }
+    if (r < 1.0f) return r;
+    return fminf(1.0f, xi_r);
+}
+
 struct MixedConst {
     float half_r, r_f, rinv_f;
     double r, cm, cp, bias, floor5;
+    float cm_f, cp_f, bias_f, floor5_f;
     int limiter;
+    bool one_rcp;  // superbee or minbee with |bias| <= 1: half_slope_mixed needs one reciprocal
 };
+
+// Half the limited slope, (Delta / 2) xi(r), of SlopeLimiters::computeSlopeVector (Solvers/slopelimiters.cpp:217-246)
+// and computeSlopeLimiter (:7-74) in the mixed form.  For |w| <= 1 and r >= 1, xi_R = 2 / ((1 - w) + (1 + w) r) is
+// at most 1, hence at most r and 2, so superbee's min(r, xi_R, 2) and minbee's min(1, xi_R) are xi_R, and
+// xi_R / 2 = den / ((1 - w) den + (1 + w) num).  The branch tests r < 0, 1/2, 1 are sign tests of (num - t den) den,
+// so one reciprocal (of den, or of that denominator) serves every branch.  Van Leer and |w| > 1 use limiter_approx.
+__device__ __forceinline__ double half_slope_mixed(double dm, double dp, const MixedConst& k) {
+    const double num = fabs(dm) < k.floor5 ? k.floor5 : dm;
+    const double den = fabs(dp) < k.floor5 ? k.floor5 : dp;
+    const double base = fma(k.cm, dm, k.cp * dp);
+    if (!k.one_rcp) return 0.5 * base * limiter_approx(num * rcp_approx(den), k.bias, k.limiter);
+    const bool ge1 = (num - den) * den >= 0.0;
+    const double f = (ge1 ? den : num) * rcp_approx(ge1 ? fma(1.0 + k.bias, num, (1.0 - k.bias) * den) : den);
+    double half_xi;
+    if (k.limiter == 0)
+        half_xi = (ge1 || (num - 0.5 * den) * den < 0.0) ? f : 0.5;
+    else
+        half_xi = ge1 ? f : 0.5 * f;
+    return num * den < 0.0 ? 0.0 : base * half_xi;
+}
+
+// FP32 twin of half_slope_mixed (same branches, FP32 operands) for FP32 reconstruction.
+__device__ __forceinline__ float half_slope_mixed(float dm, float dp, const MixedConst& k) {
+    const float num = fabsf(dm) < k.floor5_f ? k.floor5_f : dm;
+    const float den = fabsf(dp) < k.floor5_f ? k.floor5_f : dp;
+    const float base = fmaf(k.cm_f, dm, k.cp_f * dp);
+    if (!k.one_rcp) return 0.5f * base * limiter_approx(num * rcp_approx_f(den), k.bias_f, k.limiter);
+    const bool ge1 = (num - den) * den >= 0.0f;
+    const float f = (ge1 ? den : num) * rcp_approx_f(ge1 ? fmaf(1.0f + k.bias_f, num, (1.0f - k.bias_f) * den) : den);
+    float half_xi;
+    if (k.limiter == 0)
+        half_xi = (ge1 || (num - 0.5f * den) * den < 0.0f) ? f : 0.5f;
+    else
+        half_xi = ge1 ? f : 0.5f * f;
+    return num * den < 0.0f ? 0.0f : base * half_xi;
+}
 
 __device__ __forceinline__ MixedConst mixed_const(const SweepArgs& a, double& ts) {
     MixedConst k;
@@ -50,50 +103,55 @@ __device__ __forceinline__ MixedConst mixed_const(const SweepArgs& a, double& ts
     k.cp = 0.5 * (1.0 - a.bias);
     k.bias = a.bias;
     k.floor5 = a.floor5;
+    k.cm_f = (float)k.cm;
+    k.cp_f = (float)k.cp;
+    k.bias_f = (float)a.bias;
+    k.floor5_f = (float)a.floor5;
     k.limiter = a.limiter;
+    k.one_rcp = a.limiter != 1 && fabs(a.bias) <= 1.0;
     return k;
 }
 
-// Both evolved edge states of one cell (FP64), from the FP64 conserved vectors of the cell and its
-// neighbours.  ua_left_side: x_L + dt/2 evolution; ua_right_side: x_R + dt/2 evolution.
+// Both evolved edge states of one cell (type M::R), from the FP64 conserved vectors of the cell and its
+// neighbours; the slope differences are formed in FP64.  ua_left_side: x_L + dt/2 evolution; ua_right_side:
+// x_R + dt/2 evolution.
 template <class M, int AXIS>
 __device__ __forceinline__ void evolve_edges_mixed(const double* uL, const double* u, const double* uR,
                                                    const MixedConst& k, const typename M::P& q,
-                                                   double* ua_left_side, double* ua_right_side) {
+                                                   typename M::R* ua_left_side, typename M::R* ua_right_side) {
+    using R = typename M::R;
     constexpr int NU = M::NU;
-    double xl[NU], xr[NU];
+    R xl[NU], xr[NU];
 #pragma unroll
     for (int i = 0; i < NU; i++) {
-        double dm = u[i] - uL[i];
-        double dp = uR[i] - u[i];
-        double num = fabs(dm) < k.floor5 ? k.floor5 : dm;
-        double den = fabs(dp) < k.floor5 ? k.floor5 : dp;
-        double hs = 0.5 * fma(k.cm, dm, k.cp * dp) * limiter_approx(num * rcp_approx(den), k.bias, k.limiter);
-        xl[i] = u[i] - hs;
-        xr[i] = u[i] + hs;
+        R hs = half_slope_mixed((R)(u[i] - uL[i]), (R)(uR[i] - u[i]), k);
+        R uc = (R)u[i];
+        xl[i] = uc - hs;
+        xr[i] = uc + hs;
     }
     float fl[NU], fr[NU];
     M::template flux<AXIS>(xl, q, fl);
     M::template flux<AXIS>(xr, q, fr);
 #pragma unroll
     for (int i = 0; i < NU; i++) {
-        double ev = (double)(k.half_r * (fl[i] - fr[i]));
+        R ev = (R)(k.half_r * (fl[i] - fr[i]));
         ua_left_side[i] = xl[i] + ev;
         ua_right_side[i] = xr[i] + ev;
     }
 }
 
-// FORCE flux of FP64 states ua (left) and ub (right), FP32 result.
+// FORCE flux of the evolved states ua (left) and ub (right), FP32 result.
 template <class M, int AXIS>
-__device__ __forceinline__ void force_flux_mixed(const double* ua, const double* ub, const MixedConst& k,
-                                                 const typename M::P& q, float* F) {
+__device__ __forceinline__ void force_flux_mixed(const typename M::R* ua, const typename M::R* ub,
+                                                 const MixedConst& k, const typename M::P& q, float* F) {
+    using R = typename M::R;
     constexpr int NU = M::NU;
     float fa[NU], fb[NU], fri[NU];
-    double uri[NU];
+    R uri[NU];
     M::template flux<AXIS>(ua, q, fa);
     M::template flux<AXIS>(ub, q, fb);
 #pragma unroll
-    for (int i = 0; i < NU; i++) uri[i] = 0.5 * (ua[i] + ub[i]) + (double)(0.5f * k.r_f * (fa[i] - fb[i]));
+    for (int i = 0; i < NU; i++) uri[i] = (R)0.5 * (ua[i] + ub[i]) + (R)(0.5f * k.r_f * (fa[i] - fb[i]));
     M::template flux<AXIS>(uri, q, fri);
 #pragma unroll
     for (int i = 0; i < NU; i++) {
@@ -111,10 +169,11 @@ __device__ __forceinline__ bool bad_state_mixed(const double* W) {
 // ----------------------------------------------------------------------------------------- X sweep
 template <class M, int P, int LPB, int MINB>
 __global__ void __launch_bounds__(P* LPB, MINB) sweep_x_mixed_kernel(SweepArgs a) {
+    using R = typename M::R;
     constexpr int NU = M::NU, NW = M::NW;
     constexpr int NT = P * LPB;
     __shared__ double Us[NU][LPB][P + 2];
-    __shared__ double Es[NU][LPB][P];
+    __shared__ R Es[NU][LPB][P];
     __shared__ double Fs[NU][LPB][P];  // interface fluxes, widened once to FP64 for the update
 
     const int p = threadIdx.x % P, l = threadIdx.x / P;
@@ -149,9 +208,10 @@ __global__ void __launch_bounds__(P* LPB, MINB) sweep_x_mixed_kernel(SweepArgs a
     if (p == P - 1) conserve(P + 1);
     __syncthreads();
 
-    double ub[NU];
+    R ub[NU];
     {
-        double uL[NU], u[NU], uR[NU], ua[NU];
+        double uL[NU], u[NU], uR[NU];
+        R ua[NU];
 #pragma unroll
         for (int v = 0; v < NU; v++) {
             uL[v] = Us[v][l][p];
@@ -165,7 +225,7 @@ __global__ void __launch_bounds__(P* LPB, MINB) sweep_x_mixed_kernel(SweepArgs a
     __syncthreads();
 
     if (p >= 1) {
-        double ua[NU];
+        R ua[NU];
         float F[NU];
 #pragma unroll
         for (int v = 0; v < NU; v++) ua[v] = Es[v][l][p - 1];
@@ -225,7 +285,9 @@ __global__ void __launch_bounds__(TX, MINB) sweep_y_mixed_kernel(SweepArgs a) {
         for (int v = 0; v < NW; v++) W[v] = a.in[v * a.plane + (long)rr * a.pitch + c];
     };
 
-    double um1[NU], u0[NU], up1[NU], ua_prev[NU], dummy[NU], f_prev[NU], wnext[NW];
+    using R = typename M::R;
+    double um1[NU], u0[NU], up1[NU], f_prev[NU], wnext[NW];
+    R ua_prev[NU], dummy[NU];
     double wave = 0.0;
     load(r0 - 2, wnext);
     M::cons(wnext, q, up1);
@@ -238,7 +300,7 @@ __global__ void __launch_bounds__(TX, MINB) sweep_y_mixed_kernel(SweepArgs a) {
     for (int r = r0; r <= r1; r++) {
         M::cons(wnext, q, up1);
         if (r < r1) load(r + 2, wnext);
-        double ub[NU], ua_next[NU];
+        R ub[NU], ua_next[NU];
         evolve_edges_mixed<M, 1>(um1, u0, up1, k, q, ub, ua_next);
         float F[NU];
         force_flux_mixed<M, 1>(ua_prev, ub, k, q, F);
