@@ -38,6 +38,23 @@ __device__ __forceinline__ float rcp_approx_f(float a) {
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
     return r;
 }
+// Two FP32 lanes processed by one packed Blackwell instruction (FADD2/FMUL2/FFMA2): the X sweep of the
+// Euler mixed form carries two grid rows through its FP32 arithmetic this way, lane x = first row.  Each lane
+// is rounded exactly as the scalar operation would be (a - b is fma(b, -1, a), which rounds once).
+struct f2 {
+    float2 v;
+};
+__device__ __forceinline__ f2 mk2(float a, float b) { return {make_float2(a, b)}; }
+__device__ __forceinline__ f2 splat2(float s) { return {make_float2(s, s)}; }
+__device__ __forceinline__ f2 operator+(f2 a, f2 b) { return {__fadd2_rn(a.v, b.v)}; }
+__device__ __forceinline__ f2 operator*(f2 a, f2 b) { return {__fmul2_rn(a.v, b.v)}; }
+__device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c) { return {__ffma2_rn(a.v, b.v, c.v)}; }
+__device__ __forceinline__ f2 operator-(f2 a, f2 b) { return fma2(b, splat2(-1.0f), a); }
+__device__ __forceinline__ f2 sel2(bool cx, bool cy, f2 a, f2 b) {
+    return mk2(cx ? a.v.x : b.v.x, cy ? a.v.y : b.v.y);
+}
+__device__ __forceinline__ f2 rcp2(f2 a) { return mk2(rcp_approx_f(a.v.x), rcp_approx_f(a.v.y)); }
+
 // 1/a refined by one Newton step: relative error ~2^-44, far below the FP32 rounding of a flux value.
 __device__ __forceinline__ double rcp_nr1(double a) {
     double x = rcp_approx(a);
@@ -61,6 +78,7 @@ struct EulerMixed {
     static constexpr int IE = NU - 1;
     static constexpr bool HAS_Y = NVEL == 2;
     using R = double;  // type of the reconstructed, evolved and Richtmyer states
+    static constexpr bool PAIR_X = false;  // X sweep carries two rows per thread in packed FP32 lanes
     struct P {
         double gm1, inv_gm1, gpinf, g, pinf, ch2;
     };
@@ -132,6 +150,7 @@ struct EulerF32 : EulerMixed<NVEL> {
     using Base = EulerMixed<NVEL>;
     using Base::IE;
     using R = float;
+    static constexpr bool PAIR_X = true;
     struct P : Base::P {
         float gm1_f, gpinf_f;
     };
@@ -160,6 +179,25 @@ struct EulerF32 : EulerMixed<NVEL> {
         }
         F[IE] = (U[IE] + p) * un;
     }
+    // flux of two states at once, one per lane, with the same operations as flux()
+    template <int AXIS>
+    __device__ static void flux2(const f2* U, const P& q, f2* F) {
+        f2 inv = rcp2(U[0]);
+        f2 mx = U[1], my = (NVEL == 2) ? U[2] : splat2(0.0f);
+        f2 un = (AXIS == 0 ? mx : my) * inv;
+        f2 ke2 = ((NVEL == 2) ? fma2(mx, mx, my * my) : mx * mx) * inv;
+        f2 p = fma2(splat2(q.gm1_f), fma2(splat2(-0.5f), ke2, U[IE]), splat2(-q.gpinf_f));
+        if constexpr (AXIS == 0) {
+            F[0] = mx;
+            F[1] = fma2(mx, un, p);
+            if constexpr (NVEL == 2) F[2] = my * un;
+        } else {
+            F[0] = my;
+            F[1] = mx * un;
+            F[2] = fma2(my, un, p);
+        }
+        F[IE] = (U[IE] + p) * un;
+    }
 };
 
 // --------------------------------------------------------------------------------------------- MHD
@@ -173,6 +211,7 @@ struct MHDMixed {
     static constexpr int IPSI = NW - 1;
     static constexpr bool HAS_Y = true;
     using R = double;
+    static constexpr bool PAIR_X = false;
     struct P {
         double gm1, inv_gm1, gpinf, g, pinf, ch2;
     };
@@ -279,6 +318,7 @@ struct HPRMixed {
     static constexpr int NU = 17;
     static constexpr bool HAS_Y = true;
     using R = double;
+    static constexpr bool PAIR_X = false;
     using P = HPRF64::P;
     __device__ static P params(const double* prm, double ch) { return HPRF64::params(prm, ch); }
     __device__ static void cons(const double* W, const P& q, double* U) { HPRF64::cons(W, q, U); }

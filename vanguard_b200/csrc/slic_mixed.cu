@@ -13,7 +13,12 @@ constexpr int MW_NT = 256;
 struct MixedKernels {
     template <class M, int P, int LPB, int MINB>
     static void x(dim3 grid, int nt, cudaStream_t st, const SweepArgs& a) {
-        sweep_x_mixed_kernel<M, P, LPB, MINB><<<grid, nt, 0, st>>>(a);
+        if constexpr (M::PAIR_X) {
+            dim3 g(grid.x, (a.ny + 2 * LPB - 1) / (2 * LPB));
+            sweep_x_pair_kernel<M, P, LPB, MINB><<<g, nt, 0, st>>>(a);
+        } else {
+            sweep_x_mixed_kernel<M, P, LPB, MINB><<<grid, nt, 0, st>>>(a);
+        }
     }
     template <class M, int TX, int TY, int MINB>
     static void y(dim3 grid, int nt, cudaStream_t st, const SweepArgs& a) {

@@ -333,4 +333,153 @@ __global__ void __launch_bounds__(TX, MINB) sweep_y_mixed_kernel(SweepArgs a) {
     }
 }
 
+// ------------------------------------------------------------------------------ X sweep, two rows per thread
+// Models with PAIR_X (FP32 reconstruction) run the X sweep with each thread carrying the same column of two
+// adjacent rows.  Every stencil neighbour of the sweep lies along x, so the two rows never exchange data and all
+// FP32 arithmetic runs as packed two-lane instructions (lane x = the even row); the FP64 parts (conserved
+// variables, slope differences, update, primitive recovery) stay scalar per row.  The per-cell operations are
+// those of evolve_edges_mixed / force_flux_mixed with R = float.
+
+__device__ __forceinline__ f2 half_slope2(f2 dm, f2 dp, const MixedConst& k) {
+    const f2 fl = splat2(k.floor5_f);
+    const f2 num = sel2(fabsf(dm.v.x) < k.floor5_f, fabsf(dm.v.y) < k.floor5_f, fl, dm);
+    const f2 den = sel2(fabsf(dp.v.x) < k.floor5_f, fabsf(dp.v.y) < k.floor5_f, fl, dp);
+    const f2 base = fma2(splat2(k.cm_f), dm, splat2(k.cp_f) * dp);
+    if (!k.one_rcp) {
+        const f2 r = num * rcp2(den);
+        return splat2(0.5f) * base *
+               mk2(limiter_approx(r.v.x, k.bias_f, k.limiter), limiter_approx(r.v.y, k.bias_f, k.limiter));
+    }
+    const f2 t = (num - den) * den;
+    const bool gx = t.v.x >= 0.0f, gy = t.v.y >= 0.0f;
+    const f2 q = fma2(splat2(1.0f + k.bias_f), num, splat2(1.0f - k.bias_f) * den);
+    const f2 f = sel2(gx, gy, den, num) * rcp2(sel2(gx, gy, q, den));
+    f2 half_xi;
+    if (k.limiter == 0) {
+        const f2 t2 = fma2(splat2(-0.5f), den, num) * den;
+        half_xi = sel2(gx || t2.v.x < 0.0f, gy || t2.v.y < 0.0f, f, splat2(0.5f));
+    } else {
+        half_xi = sel2(gx, gy, f, splat2(0.5f) * f);
+    }
+    const f2 nd = num * den;
+    return sel2(nd.v.x < 0.0f, nd.v.y < 0.0f, splat2(0.0f), base * half_xi);
+}
+
+template <class M, int P, int LPB, int MINB>
+__global__ void __launch_bounds__(P* LPB, MINB) sweep_x_pair_kernel(SweepArgs a) {
+    constexpr int NU = M::NU, NW = M::NW;
+    constexpr int NT = P * LPB;
+    __shared__ double2 Us[NU][LPB][P + 2];
+    __shared__ float2 Es[NU][LPB][P];
+    __shared__ double2 Fs[NU][LPB][P];  // interface fluxes, widened once to FP64 for the update
+
+    const int p = threadIdx.x % P, l = threadIdx.x / P;
+    const int row0 = (blockIdx.y * LPB + l) * 2;
+    const int len = a.nx;
+    const int s0 = blockIdx.x * (P - 2);
+    const int cell = s0 - 1 + p;
+    const bool ok0 = row0 < a.ny, ok1 = row0 + 1 < a.ny;
+    const bool col_ok = p >= 1 && p <= P - 2 && cell < len;
+    // a missing second row (odd ny) repeats the first; it is computed but never stored
+    const long base[2] = {(long)(ok0 ? row0 : 0) * a.pitch, (long)(ok1 ? row0 + 1 : (ok0 ? row0 : 0)) * a.pitch};
+
+    if (a.ctrl && !a.ctrl->active) {
+        if (col_ok)
+            for (int h = 0; h < (ok1 ? 2 : ok0 ? 1 : 0); h++)
+                for (int v = 0; v < NW; v++) a.out[v * a.plane + base[h] + cell] = a.in[v * a.plane + base[h] + cell];
+        return;
+    }
+    double ts;
+    const MixedConst k = mixed_const(a, ts);
+    const typename M::P q = M::params(a.params, a.ctrl ? a.ctrl->ch : a.ch_host);
+
+    auto conserve = [&](int slot) {
+        int c = ghost_index(s0 - 2 + slot, len, a.periodic);
+        double W0[NW], W1[NW], U0[NU], U1[NU];
+#pragma unroll
+        for (int v = 0; v < NW; v++) {
+            W0[v] = a.in[v * a.plane + base[0] + c];
+            W1[v] = a.in[v * a.plane + base[1] + c];
+        }
+        M::cons(W0, q, U0);
+        M::cons(W1, q, U1);
+#pragma unroll
+        for (int v = 0; v < NU; v++) Us[v][l][slot] = make_double2(U0[v], U1[v]);
+    };
+    conserve(p + 1);
+    if (p == 0) conserve(0);
+    if (p == P - 1) conserve(P + 1);
+    __syncthreads();
+
+    f2 ub[NU];
+    {
+        f2 xl[NU], xr[NU], fl[NU], fr[NU];
+#pragma unroll
+        for (int i = 0; i < NU; i++) {
+            const double2 L = Us[i][l][p], C = Us[i][l][p + 1], R = Us[i][l][p + 2];
+            const f2 hs = half_slope2(mk2((float)(C.x - L.x), (float)(C.y - L.y)),
+                                      mk2((float)(R.x - C.x), (float)(R.y - C.y)), k);
+            const f2 uc = mk2((float)C.x, (float)C.y);
+            xl[i] = uc - hs;
+            xr[i] = uc + hs;
+        }
+        M::template flux2<0>(xl, q, fl);
+        M::template flux2<0>(xr, q, fr);
+#pragma unroll
+        for (int i = 0; i < NU; i++) {
+            const f2 ev = splat2(k.half_r) * (fl[i] - fr[i]);
+            ub[i] = xl[i] + ev;
+            Es[i][l][p] = (xr[i] + ev).v;
+        }
+    }
+    __syncthreads();
+
+    if (p >= 1) {
+        f2 ua[NU], fa[NU], fb[NU], uri[NU], fri[NU];
+#pragma unroll
+        for (int v = 0; v < NU; v++) ua[v].v = Es[v][l][p - 1];
+        M::template flux2<0>(ua, q, fa);
+        M::template flux2<0>(ub, q, fb);
+#pragma unroll
+        for (int i = 0; i < NU; i++)
+            uri[i] = fma2(splat2(0.5f), ua[i] + ub[i], splat2(0.5f * k.r_f) * (fa[i] - fb[i]));
+        M::template flux2<0>(uri, q, fri);
+#pragma unroll
+        for (int i = 0; i < NU; i++) {
+            const f2 lf = fma2(splat2(0.5f), fa[i] + fb[i], splat2(0.5f * k.rinv_f) * (ua[i] - ub[i]));
+            const f2 F = splat2(0.5f) * (lf + fri[i]);
+            Fs[i][l][p] = make_double2((double)F.v.x, (double)F.v.y);
+        }
+    }
+    __syncthreads();
+
+    double wave = 0.0;
+    if (col_ok) {
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            if (!(h == 0 ? ok0 : ok1)) continue;
+            double Un[NU], W[NW];
+#pragma unroll
+            for (int v = 0; v < NU; v++) {
+                const double2 fl = Fs[v][l][p], fr = Fs[v][l][p + 1], c = Us[v][l][p + 1];
+                Un[v] = h == 0 ? fma(k.r, fl.x - fr.x, c.x) : fma(k.r, fl.y - fr.y, c.y);
+            }
+            keep_fields<M>(a, base[h] + cell, q, W);
+            M::setcons(Un, q, W);
+#pragma unroll
+            for (int v = 0; v < NW; v++) a.out[v * a.plane + base[h] + cell] = W[v];
+            if (bad_state_mixed<M>(W)) atomicOr(a.err, ERR_STATE);
+            if (a.accumulate_wave) {
+                double s = M::wave(W, q, a.dims);
+                if (s > wave) wave = s;
+            }
+        }
+    }
+    if (a.accumulate_wave) block_max_to<NT>(wave, a.wave_acc);
+    if (a.advance_time && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
+        a.ctrl->t += a.ctrl->dt;
+        a.ctrl->it += 1;
+    }
+}
+
 }  // namespace vg
