@@ -339,7 +339,7 @@ def run_cuda(args, world, rank, local):
         "config": dict(workload_config(), form=best),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic,
-                     "kernel": ("sweep_x_mixed_kernel" if best == "mixed" else "sweep_x_kernel") + " (X half-sweep)",
+                     "kernel": ("sweep_x_pair_kernel" if best == "mixed" else "sweep_x_kernel") + " (X half-sweep)",
                      "algorithmic_bytes_per_launch": x_bytes, "peak_source": peak_kind},
         "e2e": {"value": job_value(world, cells * args.steps, e2e_s), "unit": UNIT,
                 "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
