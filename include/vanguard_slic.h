@@ -52,14 +52,21 @@ typedef enum vg_boundary { VG_TRANSMISSIVE = 0, VG_PERIODIC = 1 } vg_boundary;
  * any other value minbee. */
 enum { VG_SUPERBEE = 0, VG_VANLEER = 1, VG_MINBEE = 2 };
 
-#define VG_MAX_PARAMS 16
+#define VG_MAX_PARAMS 24
 
 /* Material parameter blocks (params[] below):
  *   Euler: {gamma, p_inf, c_v, E0, T_ign, rate}   EulerMaterialParameters (Euler/eulermaterialparameters.h)
  *   MHD:   {gamma, p_inf, c_h}                    MHDMaterialParameters; c_h is recomputed every step by
  *                                                 vg_run as solve() does, and read from here by vg_sweep
- *   HPR:   {gamma, p_inf, c_v, rho0, T0, c_s, alpha, tau1, tau2, T_ref, p_ref, is_thermal}
- *                                                 HPRMaterialParameters, StiffenedGas equation of state */
+ *   HPR:   {gamma, p_inf, c_v, rho0, T0, c_s, alpha, tau1, tau2, T_ref, p_ref, is_thermal,
+ *           eos, Gamma0, c0, s, alpha_eos, is_plastic, sigma0, n}
+ *                                                 HPRMaterialParameters (HPR/hprmaterialparameters.cpp:34-69):
+ *                                                 eos 0 StiffenedGas, 1 ShockMieGruneisen (reference Grueneisen
+ *                                                 coefficient Gamma0, reference sound speed c0, Hugoniot slope s,
+ *                                                 with p_ref the reference pressure), 2 GodunovRomenski (c0 and
+ *                                                 the exponent alpha_eos); is_plastic selects the plastic strain
+ *                                                 relaxation with transition stress sigma0 and power-law index n
+ *                                                 (HPR/hprsourceterms.cpp:12-23).  The last slot is reserved. */
 typedef struct vg_grid_desc {
     int model;                        /* vg_model */
     int nx;                           /* cells along X (columns) */

@@ -134,11 +134,29 @@ def ref():
 
 # ------------------------------------------------------------------------------------ restatement
 
+NPARAMS = 24  # size of every parameter block handed to the C libraries (VG_MAX_PARAMS)
+
+
+def _params(params):
+    """The model's parameter block zero-padded to NPARAMS (zero = StiffenedGas, non-plastic for HPR)."""
+    p = np.zeros(NPARAMS)
+    v = np.asarray(params, dtype=np.float64).ravel()
+    p[:len(v)] = v
+    return p
+
+
+def _ref_runnable(model, prm):
+    """The compiled reference cannot run a GodunovRomenski HPR material: its computeGruneisenCoefficientDerivative
+    (HPR/hprmiegruneisen.cpp:104-119) has no return for that branch and, compiled with -O2, does not return."""
+    if model == HPR and int(prm[12]) == 2:
+        raise ValueError("the reference's GodunovRomenski wave speed does not return; use the oracle (run)")
+
+
 def run(model, planes, dx, cfl, t_end=0.0, steps=0, bias=0.0, limiter=SUPERBEE, params=None,
         bc=TRANSMISSIVE, subcycles=0, dt_log=False):
     """Run solve()/solve2D()'s loop in the C restatement, in place.  Returns (t, steps[, dts])."""
     _check(planes, NVAR[model])
-    prm = np.ascontiguousarray(params, dtype=np.float64)
+    prm = _params(params)
     st = ctypes.c_int()
     dts = np.zeros(max(steps, 1), dtype=np.float64) if dt_log else None
     if planes.ndim == 2:
@@ -154,7 +172,7 @@ def run_first_order(model, planes, dx, cfl, t_end=0.0, steps=0, params=None, bc=
     """FirstOrderSolver::solve/solve2D's loop (and the MHD / HPR twins) in the C restatement, in place.
     Returns (t, steps)."""
     _check(planes, NVAR[model])
-    prm = np.ascontiguousarray(params, dtype=np.float64)
+    prm = _params(params)
     st = ctypes.c_int()
     nx, ny = (planes.shape[2], planes.shape[1]) if planes.ndim == 3 else (planes.shape[1], 1)
     t = lib().vo_run_first_order(model, _ptr(planes), nx, ny, dx, cfl, t_end, steps, _ptr(prm), bc, ctypes.byref(st))
@@ -166,7 +184,8 @@ def ref_run_first_order(model, planes, dx, cfl, t_end=0.0, steps=0, params=None,
     _check(planes, NVAR[model])
     R = ref()
     R.vgref_set_threads(threads)
-    prm = np.ascontiguousarray(params, dtype=np.float64)
+    prm = _params(params)
+    _ref_runnable(model, prm)
     st = ctypes.c_int()
     nx, ny = (planes.shape[2], planes.shape[1]) if planes.ndim == 3 else (planes.shape[1], 1)
     t = R.vgref_first_order_run(model, _ptr(planes), nx, ny, dx, cfl, t_end, steps, _ptr(prm), bc, ctypes.byref(st))
@@ -175,7 +194,7 @@ def ref_run_first_order(model, planes, dx, cfl, t_end=0.0, steps=0, params=None,
 
 def sweep(model, planes, axis, dx, dt, bias=0.0, limiter=SUPERBEE, params=None, bc=TRANSMISSIVE):
     _check(planes, NVAR[model])
-    prm = np.ascontiguousarray(params, dtype=np.float64)
+    prm = _params(params)
     if planes.ndim == 2:
         lib().vo_sweep1d(model, _ptr(planes), planes.shape[1], dx, dt, bias, limiter, _ptr(prm), bc)
     else:
@@ -185,7 +204,7 @@ def sweep(model, planes, axis, dx, dt, bias=0.0, limiter=SUPERBEE, params=None, 
 
 def max_wave(model, planes, params):
     _check(planes, NVAR[model])
-    prm = np.ascontiguousarray(params, dtype=np.float64)
+    prm = _params(params)
     if planes.ndim == 2:
         return lib().vo_max_wave1d(model, _ptr(planes), planes.shape[1], _ptr(prm))
     return lib().vo_max_wave2d(model, _ptr(planes), planes.shape[2], planes.shape[1], _ptr(prm))
@@ -194,7 +213,7 @@ def max_wave(model, planes, params):
 def forcing(planes, dx, dt, bias=0.0, limiter=SUPERBEE, params=None, bc=TRANSMISSIVE):
     """One HPR RK4 relaxation-source sub-cycle over the grid (restatement), in place."""
     _check(planes, NVAR[HPR])
-    prm = np.ascontiguousarray(params, dtype=np.float64)
+    prm = _params(params)
     nx, ny = (planes.shape[2], planes.shape[1]) if planes.ndim == 3 else (planes.shape[1], 1)
     lib().vo_forcing(HPR, _ptr(planes), nx, ny, dx, dt, bias, limiter, _ptr(prm), bc)
 
@@ -202,12 +221,32 @@ def forcing(planes, dx, dt, bias=0.0, limiter=SUPERBEE, params=None, bc=TRANSMIS
 def hpr_cell(w, params, reference=False):
     """(U, F_x, F_y, S, (speed_x, speed_y)) of one HPR primitive state, from the restatement or the reference."""
     w = np.ascontiguousarray(w, dtype=np.float64)
-    prm = np.ascontiguousarray(params, dtype=np.float64)
+    prm = _params(params)
     outs = [np.zeros(17) for _ in range(4)]
     sp = np.zeros(2)
     fn = ref().vgref_hpr_cell if reference else lib().vo_hpr_cell
     fn(_ptr(w), _ptr(prm), *[_ptr(o) for o in outs], _ptr(sp))
     return (*outs, sp)
+
+
+def hpr_eos(params, rho, p, e, reference=False):
+    """(n, 13) HPR Mie-Grueneisen values at densities rho (see vo_hpr_eos), from the restatement or the
+    reference's own functions (NaN where the reference's GodunovRomenski derivative does not return)."""
+    rho, p, e = (np.ascontiguousarray(x, dtype=np.float64) for x in (rho, p, e))
+    out = np.zeros((len(rho), 13))
+    fn = ref().vgref_hpr_eos if reference else lib().vo_hpr_eos
+    fn(_ptr(_params(params)), _ptr(rho), _ptr(p), _ptr(e), len(rho), _ptr(out))
+    return out
+
+
+def hpr_theta1(params, rho, A, reference=False):
+    """HPRSourceTerms::computeTheta1Reciprocal of densities rho (n,) and distortions A (n, 3, 3)."""
+    rho = np.ascontiguousarray(rho, dtype=np.float64)
+    A = np.ascontiguousarray(A, dtype=np.float64)
+    out = np.zeros(len(rho))
+    fn = ref().vgref_hpr_theta1 if reference else lib().vo_hpr_theta1
+    fn(_ptr(_params(params)), _ptr(rho), _ptr(A), len(rho), _ptr(out))
+    return out
 
 
 # ------------------------------------------------------------------------------------ reference
@@ -219,7 +258,8 @@ def ref_run(model, planes, dx, cfl, t_end=0.0, steps=0, bias=0.0, limiter=SUPERB
     _check(planes, NVAR[model])
     R = ref()
     R.vgref_set_threads(threads)
-    prm = np.ascontiguousarray(params, dtype=np.float64)
+    prm = _params(params)
+    _ref_runnable(model, prm)
     st = ctypes.c_int()
     if model == EULER and planes.ndim == 2:
         t = R.vgref_euler1d_run(_ptr(planes), planes.shape[1], dx, cfl, t_end, steps, bias, limiter,

@@ -37,6 +37,7 @@
 
 #include <omp.h>
 #include <iostream>
+#include <limits>
 #include <vector>
 
 using std::vector;
@@ -138,12 +139,15 @@ MHDMaterialParameters mhdParams(const double* prm) {
 // ------------------------------------------------------------------------------------------------ HPR
 // Plane order = HPRStateVector primitive order (HPR/hprstatevector.cpp:50-73):
 // rho, p, A(9, row-major), u, v, w, Jx, Jy, Jz.
-// prm = {gamma, p_inf, c_v, rho0, T0, c_s, alpha, tau1, tau2, T_ref, p_ref, is_thermal}; StiffenedGas,
-// non-plastic (HPR/hprmaterialparameters.cpp:34-69 argument order).
+// prm = {gamma, p_inf, c_v, rho0, T0, c_s, alpha, tau1, tau2, T_ref, p_ref, is_thermal, eos, Gamma0, c0, s,
+// alpha_eos, is_plastic, sigma0, n} (HPR/hprmaterialparameters.cpp:34-69 argument order); eos 0 StiffenedGas,
+// 1 ShockMieGruneisen, 2 GodunovRomenski.
 HPRMaterialParameters hprParams(const double* prm) {
-    return HPRMaterialParameters("StiffenedGas", prm[11] != 0.0, false, 8.31445985, prm[3], prm[10], prm[9], prm[4], prm[2],
-                                 prm[0], prm[1], 0.0, 0.0, 0.0, 0.0, prm[5], prm[7], prm[8], 1.0e-2, 0.75, 0.0, 1.0, prm[6],
-                                 0.0, 0.0, 0.0);
+    static const char* eos[3] = {"StiffenedGas", "ShockMieGruneisen", "GodunovRomenski"};
+    int id = (int)prm[12];
+    return HPRMaterialParameters(eos[id >= 0 && id < 3 ? id : 0], prm[11] != 0.0, prm[17] != 0.0, 8.31445985, prm[3],
+                                 prm[10], prm[9], prm[4], prm[2], prm[0], prm[1], prm[14], prm[13], prm[15], 0.0, prm[5],
+                                 prm[7], prm[8], 1.0e-2, 0.75, prm[18], prm[19], prm[6], prm[16], 0.0, 0.0);
 }
 
 HPRStateVector hprCell(const double* planes, long plane, long k) {
@@ -563,4 +567,41 @@ extern "C" double vgref_first_order_run(int model, double* planes, int nx, int n
             for (int j = 0; j < nx; j++) hprStore(g[i][j], planes, plane, (long)i * nx + j);
     }
     return t;
+}
+
+// ------------------------------------------------------------------------------------ HPR EOS / source probes
+// The 13 values of vo_hpr_eos from HPRMieGruneisen's own functions.  For GodunovRomenski the three values that go
+// through computeGruneisenCoefficientDerivative (dGamma, de/drho, dT/drho) are NaN: that function has no
+// GodunovRomenski return (HPR/hprmiegruneisen.cpp:104-119), and compiled with -O2 a call to it does not return.
+extern "C" void vgref_hpr_eos(const double* prm, const double* rho, const double* p, const double* e, int n, double* out) {
+    HPRMaterialParameters mp = hprParams(prm);
+    const bool gr = (int)prm[12] == 2;
+    const double nan = std::numeric_limits<double>::quiet_NaN();
+    for (int k = 0; k < n; k++) {
+        double r = rho[k], *o = out + 13 * k;
+        o[0] = HPRMieGruneisen::computeGruneisenCoefficient(r, mp);
+        o[1] = HPRMieGruneisen::computeReferencePressure(r, mp);
+        o[2] = HPRMieGruneisen::computeReferenceInternalEnergy(r, mp);
+        o[3] = gr ? nan : HPRMieGruneisen::computeGruneisenCoefficientDerivative(r, mp);
+        o[4] = HPRMieGruneisen::computeReferencePressureDerivative(r, mp);
+        o[5] = HPRMieGruneisen::computeReferenceInternalEnergyDerivative(r, mp);
+        o[6] = HPRMieGruneisen::computeInternalEnergy(r, p[k], mp);
+        o[7] = HPRMieGruneisen::computePressure(r, e[k], mp);
+        o[8] = HPRMieGruneisen::computeTemperature(r, p[k], mp);
+        o[9] = gr ? nan : HPRMieGruneisen::computeInternalEnergyDerivativeDensity(r, p[k], mp);
+        o[10] = HPRMieGruneisen::computeInternalEnergyDerivativePressure(r, mp);
+        o[11] = gr ? nan : HPRMieGruneisen::computeTemperatureDerivativeDensity(r, p[k], mp);
+        o[12] = HPRMieGruneisen::computeTemperatureDerivativePressure(r, mp);
+    }
+}
+
+// HPRSourceTerms::computeTheta1Reciprocal of (rho[k], A = a9[9k..9k+8] row-major).
+extern "C" void vgref_hpr_theta1(const double* prm, const double* rho, const double* a9, int n, double* out) {
+    HPRMaterialParameters mp = hprParams(prm);
+    for (int k = 0; k < n; k++) {
+        vector<vector<double> > A(3, vector<double>(3));
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) A[i][j] = a9[9 * k + 3 * i + j];
+        out[k] = HPRSourceTerms::computeTheta1Reciprocal(rho[k], A, mp);
+    }
 }

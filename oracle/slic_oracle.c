@@ -247,8 +247,9 @@ static void mhd_default(const double* prm, double* W) {
 }
 
 
-/* ---- HPR / GPR with the StiffenedGas Mie-Grueneisen branch, non-plastic.
- * prm = {gamma, p_inf, c_v, rho0, T0, c_s, alpha, tau1, tau2, T_ref, p_ref, is_thermal}.
+/* ---- HPR / GPR.
+ * prm = {gamma, p_inf, c_v, rho0, T0, c_s, alpha, tau1, tau2, T_ref, p_ref, is_thermal,
+ *        eos, Gamma0, c0, s, alpha_eos, is_plastic, sigma0, n}.
  * W = rho, p, A(9 row-major), u, v, w, Jx, Jy, Jz;  U = rho, rho E, A(9), rho v(3), rho J(3).
  * Matrix products sum from 0.0 in index order (MatrixAlgebra::multiplyMatrices,
  * Mathematics/matrixalgebra.cpp:62-81). */
@@ -293,27 +294,106 @@ static double det3(const mat3* a) {
     return ((m[0][0] * ((m[1][1] * m[2][2]) - (m[2][1] * m[1][2]))) - (m[0][1] * ((m[1][0] * m[2][2]) - (m[1][2] * m[2][0])))) +
            (m[0][2] * ((m[1][0] * m[2][1]) - (m[1][1] * m[2][0])));
 }
-static double hpr_gm1(const double* prm) { return prm[0] - 1.0; }           /* HPR/hprmiegruneisen.cpp:11-16 */
-static double hpr_pref(const double* prm) { return -prm[1]; }               /* :34-39 */
-static double hpr_eref(double rho, const double* prm) { return prm[1] / rho; } /* :72-77 */
-/* HPRMieGruneisen::computeInternalEnergy / computePressure / computeTemperature (:194-221) */
+/* ---- HPRMieGruneisen (HPR/hprmiegruneisen.cpp) for the three equations of state, selected by prm[12]:
+ * 0 StiffenedGas, 1 ShockMieGruneisen, 2 GodunovRomenski.  prm[13] Gamma0, prm[14] c0, prm[15] Hugoniot slope s,
+ * prm[16] GodunovRomenski alpha, prm[10] the reference pressure of the shock branch's reference energy.
+ * computeGruneisenCoefficientDerivative (:104-119) has no GodunovRomenski return; the Grueneisen coefficient
+ * of that branch is the constant gamma (:23-26), so its derivative is taken as 0 here. */
+static int hpr_eos(const double* prm) { return (int)prm[12]; }
+/* computeGruneisenCoefficient (:7-28) */
+static double mg_G(double rho, const double* prm) {
+    switch (hpr_eos(prm)) {
+        case 1: return prm[13] * (prm[3] / rho);
+        case 2: return prm[0];
+        default: return prm[0] - 1.0;
+    }
+}
+/* the GodunovRomenski coefficient (rho / rho0)^alpha (:57-58, :94-95, :150-151, :187-188) */
+static double gr_coef(double rho, const double* prm) { return pow((rho / prm[3]), prm[16]); }
+/* computeReferencePressure (:30-66) */
+static double mg_pref(double rho, const double* prm) {
+    switch (hpr_eos(prm)) {
+        case 1: {
+            double c0sq = prm[14] * prm[14], rho0 = prm[3], s = prm[15];
+            if (rho > rho0)
+                return c0sq * (((1.0 / rho0) - (1.0 / rho)) / pow(((1.0 / rho0) - (s * ((1.0 / rho0) - (1.0 / rho)))), 2.0));
+            return c0sq * (rho - rho0);
+        }
+        case 2: {
+            double c = gr_coef(rho, prm);
+            return (((prm[14] * prm[14]) * (rho / prm[16])) * (c - 1.0)) * c;
+        }
+        default: return -prm[1];
+    }
+}
+/* computeReferenceInternalEnergy (:68-102) */
+static double mg_eref(double rho, const double* prm) {
+    switch (hpr_eos(prm)) {
+        case 1:
+            if (rho > prm[3]) return 0.5 * prm[10] * ((1.0 / prm[3]) - (1.0 / rho));
+            return 0.0;
+        case 2: {
+            double c = gr_coef(rho, prm);
+            return ((prm[14] * prm[14]) / (2.0 * (prm[16] * prm[16]))) * ((c - 1.0) * (c - 1.0));
+        }
+        default: return prm[1] / rho;
+    }
+}
+/* computeGruneisenCoefficientDerivative (:104-119); 0 for GodunovRomenski, see above */
+static double mg_dG(double rho, const double* prm) {
+    if (hpr_eos(prm) == 1) return -prm[13] * (prm[3] / (rho * rho));
+    return 0.0;
+}
+/* computeReferencePressureDerivative (:121-155) */
+static double mg_dpref(double rho, const double* prm) {
+    switch (hpr_eos(prm)) {
+        case 1: {
+            double c0sq = prm[14] * prm[14], rho0 = prm[3], s = prm[15];
+            if (rho > rho0)
+                return c0sq * (rho0 * rho0) * (((s * (rho0 - rho)) - rho) / pow((s * (rho - rho0)) - rho, 3.0));
+            return c0sq;
+        }
+        case 2: {
+            double c = gr_coef(rho, prm), a = prm[16];
+            return ((prm[14] * prm[14]) / a) * c * (((1.0 + a) * (c - 1.0)) + (a * c));
+        }
+        default: return 0.0;
+    }
+}
+/* computeReferenceInternalEnergyDerivative (:157-192) */
+static double mg_deref(double rho, const double* prm) {
+    switch (hpr_eos(prm)) {
+        case 1: {
+            double c0sq = prm[14] * prm[14], rho0 = prm[3], s = prm[15];
+            if (rho > rho0) return -((rho - rho0) * rho0 * c0sq) / pow(((s * (rho - rho0)) - rho), 3.0);
+            return 0.0;
+        }
+        case 2: {
+            double c = gr_coef(rho, prm);
+            return ((prm[14] * prm[14]) / (rho * prm[16])) * (c - 1.0) * c;
+        }
+        default: return -(prm[1] / (rho * rho));
+    }
+}
+/* computeInternalEnergy / computePressure / computeTemperature (:194-221) */
 static double mg_energy(double rho, double p, const double* prm) {
-    return hpr_eref(rho, prm) + ((p - hpr_pref(prm)) / (rho * hpr_gm1(prm)));
+    return mg_eref(rho, prm) + ((p - mg_pref(rho, prm)) / (rho * mg_G(rho, prm)));
 }
 static double mg_pressure(double rho, double e, const double* prm) {
-    return (((e - hpr_eref(rho, prm)) * rho) * hpr_gm1(prm)) + hpr_pref(prm);
+    return (((e - mg_eref(rho, prm)) * rho) * mg_G(rho, prm)) + mg_pref(rho, prm);
 }
 static double mg_temperature(double rho, double p, const double* prm) {
-    return prm[9] + ((p - hpr_pref(prm)) / ((rho * hpr_gm1(prm)) * prm[2]));
+    return prm[9] + ((p - mg_pref(rho, prm)) / ((rho * mg_G(rho, prm)) * prm[2]));
 }
-/* HPRMieGruneisen::computeInternalEnergyDerivativeDensity (:223-234) for StiffenedGas */
+/* computeInternalEnergyDerivativeDensity (:223-234) */
 static double mg_dedrho(double rho, double p, const double* prm) {
-    double G = hpr_gm1(prm), dG = 0.0, pr = hpr_pref(prm), dpr = 0.0, der = -(prm[1] / (rho * rho));
+    double G = mg_G(rho, prm), dG = mg_dG(rho, prm), pr = mg_pref(rho, prm), dpr = mg_dpref(rho, prm);
+    double der = mg_deref(rho, prm);
     return der - ((((dpr * rho) * G) + ((G + (rho * dG)) * (p - pr))) / ((rho * G) * (rho * G)));
 }
-static double mg_dedp(double rho, const double* prm) { return 1.0 / (rho * hpr_gm1(prm)); } /* :236-241 */
-static double mg_dTdrho(double rho, double p, const double* prm) {                          /* :243-255 */
-    double G = hpr_gm1(prm), dG = 0.0, pr = hpr_pref(prm), dpr = 0.0;
+static double mg_dedp(double rho, const double* prm) { return 1.0 / (rho * mg_G(rho, prm)); } /* :236-241 */
+static double mg_dTdrho(double rho, double p, const double* prm) {                            /* :243-255 */
+    double G = mg_G(rho, prm), dG = mg_dG(rho, prm), pr = mg_pref(rho, prm), dpr = mg_dpref(rho, prm);
     return (-(((dpr * rho) * G) + ((G + (rho * dG)) * (p - pr)))) / (((rho * G) * (rho * G)) / prm[2]);
 }
 static double mg_dTdp(double rho, const double* prm) { return mg_dedp(rho, prm) / prm[2]; } /* :257-262 */
@@ -361,6 +441,28 @@ static mat3 shear_stress(double rho, const mat3* A, const double* prm) {
     for (int i = 0; i < 3; i++)
         for (int j = 0; j < 3; j++) r.m[i][j] = (-rho) * P.m[i][j];
     return r;
+}
+
+/* TensorAlgebra::computeSigmaNorm (Mathematics/tensoralgebra.cpp:276-283) */
+static double sigma_norm(const mat3* s) {
+    const double(*t)[3] = s->m;
+    double c1 = (((t[0][0] - t[1][1]) * (t[0][0] - t[1][1])) + ((t[1][1] - t[2][2]) * (t[1][1] - t[2][2]))) +
+                ((t[2][2] - t[0][0]) * (t[2][2] - t[0][0]));
+    double c2 = ((t[0][1] * t[0][1]) + (t[1][2] * t[1][2])) + (t[2][0] * t[2][0]);
+    return sqrt((0.5 * c1) + (3.0 * c2));
+}
+/* HPRSourceTerms::computeTheta1Reciprocal (HPR/hprsourceterms.cpp:7-27); prm[17] selects the plastic branch,
+ * prm[18] its transition stress sigma0, prm[19] its power-law index; the stress norm is capped at 1e8 with
+ * std::min's tie rule */
+static double hpr_theta1(double rho, const mat3* A, const double* prm) {
+    double cs2 = prm[5] * prm[5];
+    if (prm[17] != 0.0) {
+        mat3 sig = shear_stress(rho, A, prm);
+        double nrm = sigma_norm(&sig), cap = pow(10.0, 8.0);
+        nrm = cap < nrm ? cap : nrm;
+        return 3.0 * (pow(det3(A), (5.0 / 3.0)) / (cs2 * prm[7])) * pow(nrm / prm[18], prm[19]);
+    }
+    return 3.0 * (pow(det3(A), (5.0 / 3.0)) / (cs2 * prm[7]));
 }
 
 /* HPRStateVector::computeConservedVariableVector (HPR/hprstatevector.cpp:134-162) */
@@ -442,13 +544,12 @@ static void hpr_flux(const double* U, int axis, const double* prm, double* F) {
     }
 }
 /* HPRStateVector::computeSourceTermVector (HPR/hprstatevector.cpp:312-366) with HPRSourceTerms
- * (HPR/hprsourceterms.cpp:7-39), non-plastic branch */
+ * (HPR/hprsourceterms.cpp:7-39) */
 static void hpr_source(const double* U, const double* prm, double* S) {
     double rho = U[0];
     mat3 A = load_A(U + 2);
     mat3 d = dE_dA(&A, prm);
-    double cs2 = prm[5] * prm[5];
-    double th1 = 3.0 * (pow(det3(&A), (5.0 / 3.0)) / (cs2 * prm[7]));
+    double th1 = hpr_theta1(rho, &A, prm);
     for (int i = 0; i < 17; i++) S[i] = 0.0;
     for (int i = 0; i < 3; i++)
         for (int j = 0; j < 3; j++) S[2 + (i * 3) + j] = -d.m[i][j] * th1;
@@ -714,7 +815,7 @@ static const model* model_of(int id) {
 }
 
 int vo_nvar(int id) { const model* m = model_of(id); return m ? m->nv : 0; }
-int vo_nparams(int id) { return id == VO_EULER ? 6 : id == VO_MHD ? 3 : id == VO_HPR ? 12 : 0; }
+int vo_nparams(int id) { return id == VO_EULER ? 6 : id == VO_MHD ? 3 : id == VO_HPR ? 20 : 0; }
 
 /* ------------------------------------------------------------------------------- SLIC building blocks */
 
@@ -991,6 +1092,32 @@ void vo_hpr_cell(const double* w, const double* prm, double* u, double* fx, doub
     speed_xy[1] = hpr_acoustic_speed(w, 1, prm);
 }
 
+void vo_hpr_eos(const double* prm, const double* rho, const double* p, const double* e, int n, double* out) {
+    for (int k = 0; k < n; k++) {
+        double r = rho[k], *o = out + 13 * k;
+        o[0] = mg_G(r, prm);
+        o[1] = mg_pref(r, prm);
+        o[2] = mg_eref(r, prm);
+        o[3] = mg_dG(r, prm);
+        o[4] = mg_dpref(r, prm);
+        o[5] = mg_deref(r, prm);
+        o[6] = mg_energy(r, p[k], prm);
+        o[7] = mg_pressure(r, e[k], prm);
+        o[8] = mg_temperature(r, p[k], prm);
+        o[9] = mg_dedrho(r, p[k], prm);
+        o[10] = mg_dedp(r, prm);
+        o[11] = mg_dTdrho(r, p[k], prm);
+        o[12] = mg_dTdp(r, prm);
+    }
+}
+
+void vo_hpr_theta1(const double* prm, const double* rho, const double* a9, int n, double* out) {
+    for (int k = 0; k < n; k++) {
+        mat3 A = load_A(a9 + 9 * k);
+        out[k] = hpr_theta1(rho[k], &A, prm);
+    }
+}
+
 /* the stiff relaxation of every cell of the grid (see hpr_relax_cell) */
 static void relax_grid(const model* m, double* planes, long plane, double h, const double* prm) {
     int nv = m->nv;
@@ -1021,7 +1148,7 @@ static double run(int id, double* planes, int nx, int ny, int dims, double dx, d
                   double* dt_log) {
     const model* m = model_of(id);
     if (!m) return -1.0;
-    double prm[16];
+    double prm[24];
     memcpy(prm, prm_in, sizeof(double) * vo_nparams(id));
     double tEnd = t_end > 0.0 ? t_end : 1.0e300;
     int limit = max_steps > 0 ? max_steps : 0x7fffffff;

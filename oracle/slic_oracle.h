@@ -29,7 +29,7 @@ int vo_nvar(int model);
 /* Length of the parameter block each model takes:
  *   Euler: {gamma, p_inf, c_v, E0, T_ign, reaction_rate}     (Euler/eulermaterialparameters.cpp:36-46)
  *   MHD:   {gamma, p_inf, c_h}   c_h is only read by vo_sweep*; vo_run* sets it every step
- *   HPR:   see slic_oracle.c (hpr_params).                                                       */
+ *   HPR:   20 values, see slic_oracle.c; trailing zeros select StiffenedGas, non-plastic      */
 int vo_nparams(int model);
 
 /* Fixed-step or time-driven run of solve()/solve2D()'s loop (max_steps <= 0: run until t_end;
@@ -57,6 +57,13 @@ double vo_max_wave2d(int model, const double* planes, int nx, int ny, const doub
  * computeRungeKuttaTimeStep{,2D}, Solvers/hprforcingsolver.cpp:341-357, :394-418), in place. */
 void vo_forcing(int model, double* planes, int nx, int ny, double dx, double dt, double bias, int limiter,
                 const double* prm, int bc);
+
+/* HPR Mie-Grueneisen probe (HPR/hprmiegruneisen.cpp), 13 values per point k:
+ *   Gamma, p_ref(rho), e_ref(rho), dGamma, dp_ref, de_ref, e(rho, p), p(rho, e), T(rho, p), de/drho(rho, p),
+ *   de/dp, dT/drho(rho, p), dT/dp. */
+void vo_hpr_eos(const double* prm, const double* rho, const double* p, const double* e, int n, double* out);
+/* HPRSourceTerms::computeTheta1Reciprocal of density rho[k] and distortion a9[9k..9k+8] (row-major). */
+void vo_hpr_theta1(const double* prm, const double* rho, const double* a9, int n, double* out);
 
 /* HPR single-cell probe: conserved vector, x/y fluxes, source and acoustic-tensor speeds of primitives w. */
 void vo_hpr_cell(const double* w, const double* prm, double* u, double* fx, double* fy, double* src, double* speed_xy);

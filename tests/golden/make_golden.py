@@ -53,6 +53,18 @@ CASES = {
     "hpr1d_heat100_rk4sub2_20": (O.HPR, lambda: wl.hpr_heat_conduction_1d(100),
                                  dict(dx=1 / 100, cfl=0.8, steps=20, limiter=O.SUPERBEE, subcycles=2,
                                       params=wl.hpr_params(tau1=1e-1, tau2=1e-1))),
+    # HPR solids: the ShockMieGruneisen equation of state, thermal with the RK4 source, and 2D sweeps only
+    "hpr1d_shockmg60_thermal_rk4sub2_12": (O.HPR, lambda: wl.hpr_shock_riemann(60, 1, wl.hpr_shock_mg_params(thermal=True, tau1=0.1)),
+                                           dict(dx=1 / 60, cfl=0.8, steps=12, limiter=O.SUPERBEE, subcycles=2,
+                                                params=wl.hpr_shock_mg_params(thermal=True, tau1=0.1))),
+    "hpr2d_shockmg20x16_minbee_8": (O.HPR, lambda: wl.hpr_shock_riemann(20, 16, wl.hpr_shock_mg_params(), seed=2),
+                                    dict(dx=1 / 20, cfl=0.8, steps=8, limiter=O.MINBEE,
+                                         params=wl.hpr_shock_mg_params())),
+    # HPR plastic strain relaxation (StiffenedGas gas, theta1 scaled by (|sigma| / sigma0)^n), RK4 source
+    "hpr1d_heat80_plastic_rk4sub2_16": (O.HPR, lambda: wl.hpr_heat_conduction_1d(80),
+                                        dict(dx=1 / 80, cfl=0.8, steps=16, limiter=O.SUPERBEE, subcycles=2,
+                                             params=wl.hpr_params(tau1=1e-2, tau2=1e-1, plastic=True, sigma0=0.05,
+                                                                  n=2.0))),
 }
 
 

@@ -21,7 +21,7 @@ FP64, MIXED = 0, 1
 TRANSMISSIVE, PERIODIC = 0, 1
 SUPERBEE, VANLEER, MINBEE = 0, 1, 2
 NVAR = {EULER: 6, MHD: 9, HPR: 17}
-MAX_PARAMS = 16
+MAX_PARAMS = 24
 
 
 class VgError(RuntimeError):

@@ -111,7 +111,7 @@ __global__ void __launch_bounds__(BP) batch_step_kernel(BatchArgs a) {
             for (int v = 0; v < NU; v++) Un[v] = Us[v][p + 1] + (kc.r * (Fs[v][p] - Fs[v][p + 1]));
             M1::setcons(Un, q, W);
             for (int v = 0; v < NW; v++) a.out[v * a.plane + base + cell] = W[v];
-            if (bad_state<M1>(W)) atomicOr(a.err, ERR_STATE);
+            if (bad_state<M1>(W, q)) atomicOr(a.err, ERR_STATE);
             double sw = M1::wave(W, q, 1);
             if (sw > wave) wave = sw;
         }

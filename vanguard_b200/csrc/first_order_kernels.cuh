@@ -63,7 +63,7 @@ __global__ void __launch_bounds__(P) force1_x_kernel(SweepArgs a) {
         keep_fields<M>(a, rowbase + cell, q, W);
         M::setcons(Un, q, W);
         store_w<M>(a, rowbase + cell, W);
-        if (bad_state<M>(W)) atomicOr(a.err, ERR_STATE);
+        if (bad_state<M>(W, q)) atomicOr(a.err, ERR_STATE);
         if (a.accumulate_wave) {
             const double s = M::wave(W, q, a.dims);
             if (s > wave) wave = s;
@@ -115,7 +115,7 @@ __global__ void __launch_bounds__(TX) force1_y_kernel(SweepArgs a) {
             keep_fields<M>(a, idx, q, W);
             M::setcons(Un, q, W);
             store_w<M>(a, idx, W);
-            if (bad_state<M>(W)) atomicOr(a.err, ERR_STATE);
+            if (bad_state<M>(W, q)) atomicOr(a.err, ERR_STATE);
             if (a.accumulate_wave) {
                 const double s = M::wave(W, q, 2);
                 if (s > wave) wave = s;

@@ -143,7 +143,7 @@ __global__ void __launch_bounds__(FT, 6) forcing_kernel(SweepArgs a, int subcycl
     }
     M::setcons(uM, q, W);  // the cell keeps its own primitives for fields setConservedVariableVector leaves alone
     for (int v = 0; v < NW; v++) a.out[v * a.plane + self] = W[v];
-    if (bad_state<M>(W)) atomicOr(a.err, ERR_STATE);
+    if (bad_state<M>(W, q)) atomicOr(a.err, ERR_STATE);
 }
 
 }  // namespace vg

@@ -1,21 +1,33 @@
-// Exact-FP64 device restatement of the HPR / GPR model (StiffenedGas Mie-Grueneisen branch, non-plastic).
+// Exact-FP64 device restatement of the HPR / GPR model: the StiffenedGas, ShockMieGruneisen and GodunovRomenski
+// branches of HPRMieGruneisen and the elastic and plastic strain relaxation of HPRSourceTerms.
 //
 // Compiled with -fmad=false and IEEE division / square root; every expression keeps the reference's
 // association order (matrix products summed from 0.0 in index order, Mathematics/matrixalgebra.cpp:62-81),
 // so the sweeps and the CFL reproduce the reference bit for bit.  The relaxation source uses pow(det A, 5/3)
-// (HPR/hprsourceterms.cpp:21-26); CUDA's pow and glibc's may differ in the last place, so runs with the source
-// switched on agree with the reference to ~1e-15 relative rather than bitwise.
+// (HPR/hprsourceterms.cpp:21-26), and the ShockMieGruneisen and GodunovRomenski branches pow of the density
+// ratio; CUDA's pow and glibc's may differ in the last place, so runs with the source switched on or a solid
+// equation of state agree with the reference to ~1e-15 relative rather than bitwise.
+//
+// computeGruneisenCoefficientDerivative (HPR/hprmiegruneisen.cpp:104-119) has no GodunovRomenski return, and
+// compiled with -O2 a call to it does not return; the Grueneisen coefficient of that branch is the constant
+// gamma (:23-26), so its derivative is 0 here.
 //
 // W = (rho, p, A00..A22, u, v, w, Jx, Jy, Jz)   (HPR/hprstatevector.cpp:50-73)
 // U = (rho, rho E, A00..A22, rho u, rho v, rho w, rho Jx, rho Jy, rho Jz)   (HPR/hprstatevector.cpp:134-162)
-// params = {gamma, p_inf, c_v, rho0, T0, c_s, alpha, tau1, tau2, T_ref, p_ref, is_thermal}
+// params = {gamma, p_inf, c_v, rho0, T0, c_s, alpha, tau1, tau2, T_ref, p_ref, is_thermal,
+//           eos (0 StiffenedGas, 1 ShockMieGruneisen, 2 GodunovRomenski), Gamma0, c0, s, alpha_eos, is_plastic,
+//           sigma0, n}
 #pragma once
 
 #include "vg_common.cuh"
 
 namespace vg {
 
-struct HPRF64 {
+// SOLID = false: the StiffenedGas gas with elastic strain relaxation only (the thermal-gas configurations);
+// SOLID = true: every equation-of-state branch (params[12]) and the plastic relaxation (params[17]).  The gas
+// instantiation compiles the StiffenedGas formulas alone, so it carries no branch or register cost for solids.
+template <bool SOLID>
+struct HPRModel {
     static constexpr int NW = 17;
     static constexpr int NU = 17;
     static constexpr bool HAS_Y = true;
@@ -24,10 +36,15 @@ struct HPRF64 {
         double g, pinf, cv, rho0, T0, cs, alpha, tau1, tau2, Tref;
         int thermal;
         double ch2;
+        int eos, plastic;
+        double pref_mat, G0, c0, s, aeos, sigma0, npl;
     };
     __device__ static P params(const double* prm, double /*ch*/) {
-        return P{prm[0], prm[1], prm[2], prm[3], prm[4], prm[5], prm[6], prm[7], prm[8], prm[9], prm[11] != 0.0, 0.0};
+        return P{prm[0], prm[1], prm[2], prm[3], prm[4], prm[5], prm[6], prm[7], prm[8], prm[9], prm[11] != 0.0, 0.0,
+                 (int)prm[12], prm[17] != 0.0, prm[10], prm[13], prm[14], prm[15], prm[16], prm[18], prm[19]};
     }
+    // gases need a positive pressure; the solid equations of state admit zero and tension
+    __device__ static bool positive_pressure(const P& q) { return !SOLID || q.eos == 0; }
 
     // ---- 3x3 algebra in the reference's order
     struct M3 {
@@ -73,24 +90,84 @@ struct HPRF64 {
                (a.m[0][2] * ((a.m[1][0] * a.m[2][1]) - (a.m[1][1] * a.m[2][0])));
     }
 
-    // ---- StiffenedGas Mie-Grueneisen (HPR/hprmiegruneisen.cpp:7-262)
-    __device__ static double gm1(const P& q) { return q.g - 1.0; }
-    __device__ static double pref(const P& q) { return -q.pinf; }
-    __device__ static double eref(double rho, const P& q) { return q.pinf / rho; }
-    __device__ static double mg_energy(double rho, double p, const P& q) { return eref(rho, q) + ((p - pref(q)) / (rho * gm1(q))); }
+    // ---- HPRMieGruneisen (HPR/hprmiegruneisen.cpp), branch q.eos
+    __device__ static double mg_G(double rho, const P& q) {  // computeGruneisenCoefficient (:7-28)
+        if constexpr (!SOLID) return q.g - 1.0;
+        if (q.eos == 1) return q.G0 * (q.rho0 / rho);
+        if (q.eos == 2) return q.g;
+        return q.g - 1.0;
+    }
+    __device__ static double gr_coef(double rho, const P& q) { return pow((rho / q.rho0), q.aeos); }
+    __device__ static double mg_pref(double rho, const P& q) {  // computeReferencePressure (:30-66)
+        if constexpr (!SOLID) return -q.pinf;
+        if (q.eos == 1) {
+            double c0sq = q.c0 * q.c0;
+            if (rho > q.rho0)
+                return c0sq * (((1.0 / q.rho0) - (1.0 / rho)) / pow(((1.0 / q.rho0) - (q.s * ((1.0 / q.rho0) - (1.0 / rho)))), 2.0));
+            return c0sq * (rho - q.rho0);
+        }
+        if (q.eos == 2) {
+            double c = gr_coef(rho, q);
+            return (((q.c0 * q.c0) * (rho / q.aeos)) * (c - 1.0)) * c;
+        }
+        return -q.pinf;
+    }
+    __device__ static double mg_eref(double rho, const P& q) {  // computeReferenceInternalEnergy (:68-102)
+        if constexpr (!SOLID) return q.pinf / rho;
+        if (q.eos == 1) return rho > q.rho0 ? (0.5 * q.pref_mat) * ((1.0 / q.rho0) - (1.0 / rho)) : 0.0;
+        if (q.eos == 2) {
+            double c = gr_coef(rho, q);
+            return ((q.c0 * q.c0) / (2.0 * (q.aeos * q.aeos))) * ((c - 1.0) * (c - 1.0));
+        }
+        return q.pinf / rho;
+    }
+    __device__ static double mg_dG(double rho, const P& q) {  // computeGruneisenCoefficientDerivative (:104-119)
+        return (SOLID && q.eos == 1) ? (-q.G0) * (q.rho0 / (rho * rho)) : 0.0;
+    }
+    __device__ static double mg_dpref(double rho, const P& q) {  // computeReferencePressureDerivative (:121-155)
+        if constexpr (!SOLID) return 0.0;
+        if (q.eos == 1) {
+            double c0sq = q.c0 * q.c0;
+            if (rho > q.rho0)
+                return (c0sq * (q.rho0 * q.rho0)) * (((q.s * (q.rho0 - rho)) - rho) / pow((q.s * (rho - q.rho0)) - rho, 3.0));
+            return c0sq;
+        }
+        if (q.eos == 2) {
+            double c = gr_coef(rho, q);
+            return (((q.c0 * q.c0) / q.aeos) * c) * (((1.0 + q.aeos) * (c - 1.0)) + (q.aeos * c));
+        }
+        return 0.0;
+    }
+    __device__ static double mg_deref(double rho, const P& q) {  // computeReferenceInternalEnergyDerivative (:157-192)
+        if constexpr (!SOLID) return -(q.pinf / (rho * rho));
+        if (q.eos == 1) {
+            if (rho > q.rho0) return (-(((rho - q.rho0) * q.rho0) * (q.c0 * q.c0))) / pow(((q.s * (rho - q.rho0)) - rho), 3.0);
+            return 0.0;
+        }
+        if (q.eos == 2) {
+            double c = gr_coef(rho, q);
+            return (((q.c0 * q.c0) / (rho * q.aeos)) * (c - 1.0)) * c;
+        }
+        return -(q.pinf / (rho * rho));
+    }
+    // computeInternalEnergy / computePressure / computeTemperature (:194-221)
+    __device__ static double mg_energy(double rho, double p, const P& q) {
+        return mg_eref(rho, q) + ((p - mg_pref(rho, q)) / (rho * mg_G(rho, q)));
+    }
     __device__ static double mg_pressure(double rho, double e, const P& q) {
-        return (((e - eref(rho, q)) * rho) * gm1(q)) + pref(q);
+        return (((e - mg_eref(rho, q)) * rho) * mg_G(rho, q)) + mg_pref(rho, q);
     }
     __device__ static double mg_temperature(double rho, double p, const P& q) {
-        return q.Tref + ((p - pref(q)) / ((rho * gm1(q)) * q.cv));
+        return q.Tref + ((p - mg_pref(rho, q)) / ((rho * mg_G(rho, q)) * q.cv));
     }
+    // computeInternalEnergyDerivativeDensity / Pressure, computeTemperatureDerivativeDensity / Pressure (:223-262)
     __device__ static double mg_dedrho(double rho, double p, const P& q) {
-        double G = gm1(q), dG = 0.0, pr = pref(q), dpr = 0.0, der = -(q.pinf / (rho * rho));
+        double G = mg_G(rho, q), dG = mg_dG(rho, q), pr = mg_pref(rho, q), dpr = mg_dpref(rho, q), der = mg_deref(rho, q);
         return der - ((((dpr * rho) * G) + ((G + (rho * dG)) * (p - pr))) / ((rho * G) * (rho * G)));
     }
-    __device__ static double mg_dedp(double rho, const P& q) { return 1.0 / (rho * gm1(q)); }
+    __device__ static double mg_dedp(double rho, const P& q) { return 1.0 / (rho * mg_G(rho, q)); }
     __device__ static double mg_dTdrho(double rho, double p, const P& q) {
-        double G = gm1(q), dG = 0.0, pr = pref(q), dpr = 0.0;
+        double G = mg_G(rho, q), dG = mg_dG(rho, q), pr = mg_pref(rho, q), dpr = mg_dpref(rho, q);
         return (-(((dpr * rho) * G) + ((G + (rho * dG)) * (p - pr)))) / (((rho * G) * (rho * G)) / q.cv);
     }
     __device__ static double mg_dTdp(double rho, const P& q) { return mg_dedp(rho, q) / q.cv; }
@@ -211,13 +288,33 @@ struct HPRF64 {
             }
         }
     }
+    // HPRSourceTerms::computeTheta1Reciprocal (HPR/hprsourceterms.cpp:7-27) given d = dE/dA; the plastic branch
+    // scales it by (min(|sigma|, 1e8) / sigma0)^n, |sigma| = TensorAlgebra::computeSigmaNorm
+    // (Mathematics/tensoralgebra.cpp:276-283) of sigma = -rho A^T dE/dA, with std::min's tie rule
+    __device__ static double theta1(double rho, const M3& A, const M3& d, const P& q) {
+        const double cs2 = q.cs * q.cs;
+        const double th = 3.0 * (pow(det(A), (5.0 / 3.0)) / (cs2 * q.tau1));
+        if (!SOLID || !q.plastic) return th;
+        M3 Pm = tmul(A, d);
+        double t[3][3];
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) t[i][j] = (-rho) * Pm.m[i][j];
+        double c1 = (((t[0][0] - t[1][1]) * (t[0][0] - t[1][1])) + ((t[1][1] - t[2][2]) * (t[1][1] - t[2][2]))) +
+                    ((t[2][2] - t[0][0]) * (t[2][2] - t[0][0]));
+        double c2 = ((t[0][1] * t[0][1]) + (t[1][2] * t[1][2])) + (t[2][0] * t[2][0]);
+        double nrm = sqrt((0.5 * c1) + (3.0 * c2));
+        const double cap = 1.0e8;  // pow(10.0, 8.0), exact
+        nrm = cap < nrm ? cap : nrm;
+        return th * pow(nrm / q.sigma0, q.npl);
+    }
     // HPRStateVector::computeSourceTermVector (HPR/hprstatevector.cpp:312-366), HPRSourceTerms (HPR/hprsourceterms.cpp:7-39)
     __device__ static void source(const double* U, const P& q, double* S) {
         double rho = U[0];
         M3 A = load(U + 2);
         M3 d = dEdA(A, q);
-        double cs2 = q.cs * q.cs;
-        double th1 = 3.0 * (pow(det(A), (5.0 / 3.0)) / (cs2 * q.tau1));
+        double th1 = theta1(rho, A, d, q);
 #pragma unroll
         for (int i = 0; i < 17; i++) S[i] = 0.0;
 #pragma unroll
@@ -335,5 +432,8 @@ struct HPRF64 {
     __device__ static double density(const double* W) { return W[0]; }
     __device__ static double pressure(const double* W) { return W[1]; }
 };
+
+using HPRF64 = HPRModel<false>;
+using HPRSolidF64 = HPRModel<true>;
 
 }  // namespace vg

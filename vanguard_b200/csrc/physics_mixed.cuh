@@ -84,7 +84,7 @@ struct EulerMixed {
     };
     __device__ static P params(const double* prm, double /*ch*/) {
         double g = prm[0], pinf = prm[1];
-        return P{g - 1.0, prm[15], g * pinf, g, pinf, 0.0};
+        return P{g - 1.0, prm[kInvGm1], g * pinf, g, pinf, 0.0};
     }
     // W -> U in FP64: E = rho |v|^2 / 2 + (p + gamma p_inf) / (gamma - 1)
     __device__ static void cons(const double* W, const P& q, double* U) {
@@ -217,7 +217,7 @@ struct MHDMixed {
     };
     __device__ static P params(const double* prm, double ch) {
         double g = prm[0], pinf = prm[1];
-        return P{g - 1.0, prm[15], g * pinf, g, pinf, ch * ch};
+        return P{g - 1.0, prm[kInvGm1], g * pinf, g, pinf, ch * ch};
     }
     __device__ static double sq3(double a, double b, double c) {
         if constexpr (FULL) return fma(a, a, fma(b, b, c * c));
@@ -313,27 +313,31 @@ struct MHDMixed {
 // flux, the acoustic-tensor CFL speed and the relaxation source (run by the exact forcing kernel) are the exact
 // model's FP64 formulas (here compiled with FMA contraction); each flux value leaves in FP32 for the FP32
 // half-step and FORCE combinations.
-struct HPRMixed {
+template <bool SOLID>
+struct HPRMixedT {
     static constexpr int NW = 17;
     static constexpr int NU = 17;
     static constexpr bool HAS_Y = true;
     using R = double;
     static constexpr bool PAIR_X = false;
-    using P = HPRF64::P;
-    __device__ static P params(const double* prm, double ch) { return HPRF64::params(prm, ch); }
-    __device__ static void cons(const double* W, const P& q, double* U) { HPRF64::cons(W, q, U); }
-    __device__ static void setcons(const double* U, const P& q, double* W) { HPRF64::setcons(U, q, W); }
+    using P = typename HPRModel<SOLID>::P;
+    __device__ static P params(const double* prm, double ch) { return HPRModel<SOLID>::params(prm, ch); }
+    __device__ static bool positive_pressure(const P& q) { return HPRModel<SOLID>::positive_pressure(q); }
+    __device__ static void cons(const double* W, const P& q, double* U) { HPRModel<SOLID>::cons(W, q, U); }
+    __device__ static void setcons(const double* U, const P& q, double* W) { HPRModel<SOLID>::setcons(U, q, W); }
     template <int AXIS>
     __device__ static void flux(const double* U, const P& q, float* F) {
         double Fd[17];
-        HPRF64::template flux<AXIS>(U, q, Fd);
+        HPRModel<SOLID>::template flux<AXIS>(U, q, Fd);
 #pragma unroll
         for (int i = 0; i < 17; i++) F[i] = (float)Fd[i];
     }
-    __device__ static double wave(const double* W, const P& q, int dims) { return HPRF64::wave(W, q, dims); }
-    __device__ static void default_state(double* W) { HPRF64::default_state(W); }
+    __device__ static double wave(const double* W, const P& q, int dims) { return HPRModel<SOLID>::wave(W, q, dims); }
+    __device__ static void default_state(double* W) { HPRModel<SOLID>::default_state(W); }
     __device__ static double density(const double* W) { return W[0]; }
     __device__ static double pressure(const double* W) { return W[1]; }
 };
+using HPRMixed = HPRMixedT<false>;
+using HPRSolidMixed = HPRMixedT<true>;
 
 }  // namespace vg

@@ -94,13 +94,13 @@ __device__ inline int clamp_steps(double v, int lo, int hi) {
 }
 
 // Relax the conserved vector U of one cell over a time h (see the file comment).
-__device__ inline void hpr_relax_cell(double* U, double h, const HPRF64::P& q) {
-    using M = HPRF64;
+template <class M>
+__device__ inline void hpr_relax_cell(double* U, double h, const typename M::P& q) {
     const double rho = U[0];
-    const M::M3 A = M::load(U + 2);
+    const typename M::M3 A = M::load(U + 2);
     const double d = M::det(A);
     if (!(d > 0.0) || !(h > 0.0)) return;
-    const M::M3 G = M::tmul(A, A);
+    const typename M::M3 G = M::tmul(A, A);
     double l[3], V[3][3], mu[3];
     sym_eig3(G.m, l, V);
     if (!(l[0] > 0.0 && l[1] > 0.0 && l[2] > 0.0)) return;
@@ -124,7 +124,7 @@ __device__ inline void hpr_relax_cell(double* U, double h, const HPRF64::P& q) {
             U[2 + 3 * i + j] = sum;
         }
     if (!q.thermal) return;
-    const M::M3 An = M::load(U + 2);
+    const typename M::M3 An = M::load(U + 2);
     const double E = U[1] / rho, u = U[11] / rho, v = U[12] / rho, w = U[13] / rho;
     const double p0 = M::pressure_of(rho, E, u, v, w, An, U[14] / rho, U[15] / rho, U[16] / rho, q);
     const double k0 = (q.rho0 * M::mg_temperature(rho, p0, q)) / (q.tau2 * q.T0 * rho);
@@ -153,10 +153,10 @@ __global__ void __launch_bounds__(128) relax_kernel(SweepArgs a) {
     double W[NW], U[NU];
     for (int v = 0; v < NW; v++) W[v] = a.in[v * a.plane + self];
     M::cons(W, q, U);
-    hpr_relax_cell(U, h, q);
+    hpr_relax_cell<M>(U, h, q);
     M::setcons(U, q, W);  // the cell keeps its own J when the material is not thermal
     for (int v = 0; v < NW; v++) a.out[v * a.plane + self] = W[v];
-    if (bad_state<M>(W)) atomicOr(a.err, ERR_STATE);
+    if (bad_state<M>(W, q)) atomicOr(a.err, ERR_STATE);
 }
 
 }  // namespace vg

@@ -116,6 +116,7 @@ const Ops kOps[V_COUNT] = {
     make_ops<MHDF64<false>>(),
     make_ops<MHDF64<true>>(),
     make_ops<HPRF64>(),
+    make_ops<HPRSolidF64>(),
 };
 
 }  // namespace
@@ -126,6 +127,10 @@ cudaError_t hpr_forcing_fp64(const SweepArgs& a, int subcycles, cudaStream_t st)
     return forcing_impl<HPRF64>(a, subcycles, st);
 }
 cudaError_t hpr_relax_fp64(const SweepArgs& a, cudaStream_t st) { return relax_impl<HPRF64>(a, st); }
+cudaError_t hpr_solid_forcing_fp64(const SweepArgs& a, int subcycles, cudaStream_t st) {
+    return forcing_impl<HPRSolidF64>(a, subcycles, st);
+}
+cudaError_t hpr_solid_relax_fp64(const SweepArgs& a, cudaStream_t st) { return relax_impl<HPRSolidF64>(a, st); }
 cudaError_t mhd7_forcing_fp64(const SweepArgs& a, int subcycles, cudaStream_t st) {
     return forcing_impl<MHDF64<false>>(a, subcycles, st);
 }

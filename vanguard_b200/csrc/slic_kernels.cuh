@@ -142,9 +142,21 @@ __device__ __forceinline__ void keep_fields(const SweepArgs& a, long idx, const 
     }
 }
 
+// Whether a state of model M must have a positive pressure: models with a positive_pressure(q) member decide
+// (HPR: only its gas equation of state); every other model requires it.
+template <class M, class = void>
+struct pressure_rule {
+    __device__ static bool positive(const typename M::P&) { return true; }
+};
 template <class M>
-__device__ __forceinline__ bool bad_state(const double* W) {
+struct pressure_rule<M, decltype((void)&M::positive_pressure)> {
+    __device__ static bool positive(const typename M::P& q) { return M::positive_pressure(q); }
+};
+
+template <class M>
+__device__ __forceinline__ bool bad_state(const double* W, const typename M::P& q) {
     double rho = M::density(W), p = M::pressure(W);
+    if (!pressure_rule<M>::positive(q)) return !(rho > 0.0) || !isfinite(rho) || !isfinite(p);
     return !(rho > 0.0) || !(p > 0.0) || !isfinite(rho) || !isfinite(p);
 }
 
@@ -225,7 +237,7 @@ __global__ void __launch_bounds__(P* LPB, MINB) sweep_x_kernel(SweepArgs a) {
         keep_fields<M>(a, rowbase + cell, q, W);
         M::setcons(Un, q, W);
         store_w<M>(a, rowbase + cell, W);
-        if (bad_state<M>(W)) atomicOr(a.err, ERR_STATE);
+        if (bad_state<M>(W, q)) atomicOr(a.err, ERR_STATE);
         if (a.accumulate_wave) {
             double s = M::wave(W, q, a.dims);
             if (s > wave) wave = s;
@@ -285,7 +297,7 @@ __global__ void __launch_bounds__(TX, MINB) sweep_y_kernel(SweepArgs a) {
             keep_fields<M>(a, (long)(r - 1) * a.pitch + c, q, W);
             M::setcons(Un, q, W);
             store_w<M>(a, (long)(r - 1) * a.pitch + c, W);
-            if (bad_state<M>(W)) atomicOr(a.err, ERR_STATE);
+            if (bad_state<M>(W, q)) atomicOr(a.err, ERR_STATE);
             if (a.accumulate_wave) {
                 double s = M::wave(W, q, 2);
                 if (s > wave) wave = s;

@@ -62,6 +62,7 @@ const Ops kOps[V_COUNT] = {
     make_ops<MHDMixed<false>>(&mhd7_forcing_fp64),
     make_ops<MHDMixed<true>>(&mhd9_forcing_fp64),
     make_ops<HPRMixed>(&hpr_forcing_fp64, &hpr_relax_fp64),
+    make_ops<HPRSolidMixed>(&hpr_solid_forcing_fp64, &hpr_solid_relax_fp64),
 };
 
 }  // namespace

@@ -161,8 +161,9 @@ __device__ __forceinline__ void force_flux_mixed(const typename M::R* ua, const 
 }
 
 template <class M>
-__device__ __forceinline__ bool bad_state_mixed(const double* W) {
+__device__ __forceinline__ bool bad_state_mixed(const double* W, const typename M::P& q) {
     double rho = M::density(W), p = M::pressure(W);
+    if (!pressure_rule<M>::positive(q)) return !(rho > 0.0) || !isfinite(rho) || !isfinite(p);
     return !(rho > 0.0) || !(p > 0.0) || !isfinite(rho) || !isfinite(p);
 }
 
@@ -245,7 +246,7 @@ __global__ void __launch_bounds__(P* LPB, MINB) sweep_x_mixed_kernel(SweepArgs a
         M::setcons(Un, q, W);
 #pragma unroll
         for (int v = 0; v < NW; v++) a.out[v * a.plane + rowbase + cell] = W[v];
-        if (bad_state_mixed<M>(W)) atomicOr(a.err, ERR_STATE);
+        if (bad_state_mixed<M>(W, q)) atomicOr(a.err, ERR_STATE);
         if (a.accumulate_wave) {
             double s = M::wave(W, q, a.dims);
             if (s > wave) wave = s;
@@ -312,7 +313,7 @@ __global__ void __launch_bounds__(TX, MINB) sweep_y_mixed_kernel(SweepArgs a) {
             M::setcons(Un, q, W);
 #pragma unroll
             for (int v = 0; v < NW; v++) a.out[v * a.plane + (long)(r - 1) * a.pitch + c] = W[v];
-            if (bad_state_mixed<M>(W)) atomicOr(a.err, ERR_STATE);
+            if (bad_state_mixed<M>(W, q)) atomicOr(a.err, ERR_STATE);
             if (a.accumulate_wave) {
                 double s = M::wave(W, q, 2);
                 if (s > wave) wave = s;
@@ -468,7 +469,7 @@ __global__ void __launch_bounds__(P* LPB, MINB) sweep_x_pair_kernel(SweepArgs a)
             M::setcons(Un, q, W);
 #pragma unroll
             for (int v = 0; v < NW; v++) a.out[v * a.plane + base[h] + cell] = W[v];
-            if (bad_state_mixed<M>(W)) atomicOr(a.err, ERR_STATE);
+            if (bad_state_mixed<M>(W, q)) atomicOr(a.err, ERR_STATE);
             if (a.accumulate_wave) {
                 double s = M::wave(W, q, a.dims);
                 if (s > wave) wave = s;

@@ -47,6 +47,7 @@ const int kPlanes[vg::V_COUNT][17] = {
     {0, 1, 2, 4, 5, 6, 8},          // V_MHD7:   rho, u, v, p, Bx, By, psi
     {0, 1, 2, 3, 4, 5, 6, 7, 8},    // V_MHD9
     {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16},  // V_HPR17
+    {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16},  // V_HPR17S
 };
 
 }  // namespace
@@ -168,6 +169,7 @@ SweepArgs base_args(const vg_solver* s) {
     a.aux = s->aux;
     for (int i = 0; i < VG_MAX_PARAMS - 1; i++) a.params[i] = s->d.params[i];
     a.params[VG_MAX_PARAMS - 1] = 1.0 / (s->d.params[0] - 1.0);
+    static_assert(vg::kParams == VG_MAX_PARAMS, "device parameter block must match VG_MAX_PARAMS");
     a.ch_host = s->d.params[2];
     return a;
 }
@@ -346,6 +348,12 @@ vg_status vg_create(const vg_grid_desc* desc, vg_solver** out) {
     if (desc->boundary != VG_TRANSMISSIVE && desc->boundary != VG_PERIODIC) return fail(VG_EINVAL, "bad boundary");
     if (desc->precision == VG_MIXED && !vg::ops_mixed(vg::V_EULER2))
         return fail(VG_EUNSUPPORTED, "mixed precision not available in this build");
+    if (desc->model == VG_MODEL_HPR) {
+        const double eos = desc->params[12];
+        if (eos != 0.0 && eos != 1.0 && eos != 2.0)
+            return fail(VG_EINVAL, "HPR params[12] (equation of state) must be 0 StiffenedGas, 1 ShockMieGruneisen or 2 "
+                                   "GodunovRomenski");
+    }
     VG_CUDA(cudaSetDevice(desc->device));
     vg_solver* s = new (std::nothrow) vg_solver();
     if (!s) return fail(VG_ENOMEM, "host allocation");
@@ -408,7 +416,8 @@ vg_status vg_upload_primitive(vg_solver* s, const double* planes, int is_device,
             variant = (s->dims == 1 && zero_v) ? vg::V_EULER1 : vg::V_EULER2;
         }
     } else if (s->d.model == VG_MODEL_HPR) {
-        variant = vg::V_HPR17;
+        // a solid equation of state or plasticity selects the instantiation that carries them
+        variant = (s->d.params[12] != 0.0 || s->d.params[17] != 0.0) ? vg::V_HPR17S : vg::V_HPR17;
     } else {
         bool reduced = true;
         if (!is_device) {
@@ -477,6 +486,9 @@ vg_status vg_run(vg_solver* s, const vg_run_config* cfg, int* steps_taken, doubl
     if (cfg->order == 1 && !s->ops->x1) return fail(VG_EUNSUPPORTED, "the first-order loop runs in VG_FP64 only");
     if (cfg->stiff_source && cfg->order != 1 && !s->ops->relax)
         return fail(VG_EUNSUPPORTED, "the stiff source relaxation exists for the HPR model only");
+    if (cfg->stiff_source && cfg->order != 1 && s->d.params[17] != 0.0)
+        return fail(VG_EUNSUPPORTED, "the stiff source relaxation integrates the elastic strain relaxation only; plastic "
+                                     "materials run the RK4 source sub-cycles");
     cudaStream_t st = (cudaStream_t)stream;
     VG_CUDA(cudaSetDevice(s->d.device));
 

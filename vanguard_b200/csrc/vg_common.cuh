@@ -61,6 +61,9 @@ struct SweepConst {
     int limiter;
 };
 
+constexpr int kParams = 24;           // VG_MAX_PARAMS
+constexpr int kInvGm1 = kParams - 1;  // slot the host fills with 1 / (gamma - 1)
+
 // Launch-independent description of one sweep.
 struct SweepArgs {
     const double* in;        // plane 0 of the input state
@@ -87,7 +90,7 @@ struct SweepArgs {
     unsigned long long* wave_acc;  // running maximum (bit pattern), usually &ctrl->smax_next
     unsigned int* err;             // error word (always valid)
     double* aux;                   // model scratch planes (HPR forcing neighbours), or null
-    double params[16];       // model parameters (model-specific layout); params[15] = 1 / (params[0] - 1)
+    double params[kParams];  // model parameters (model-specific layout); params[kInvGm1] = 1 / (params[0] - 1)
 };
 
 // Sweep constants of one sweep of length ts = dt * scale, formed as the reference forms them

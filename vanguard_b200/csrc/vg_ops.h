@@ -17,7 +17,8 @@ enum Variant : int {
     V_MHD7 = 2,    // MHD with w == Bz == 0:               rho, u, v, p, Bx, By, psi
     V_MHD9 = 3,    // MHD, all components:                 rho, u, v, w, p, Bx, By, Bz, psi
     V_HPR17 = 4,   // HPR, all 17 components:              rho, p, A(9), u, v, w, Jx, Jy, Jz
-    V_COUNT = 5
+    V_HPR17S = 5,  // HPR solid (ShockMieGruneisen / GodunovRomenski) or plastic material, same planes
+    V_COUNT = 6
 };
 
 struct Ops {
@@ -54,6 +55,8 @@ cudaError_t mhd7_forcing_fp64(const SweepArgs& a, int subcycles, cudaStream_t st
 cudaError_t mhd9_forcing_fp64(const SweepArgs& a, int subcycles, cudaStream_t st);
 // The stiff HPR relaxation (slic_fp64.cu), FP64 in both forms.
 cudaError_t hpr_relax_fp64(const SweepArgs& a, cudaStream_t st);
+cudaError_t hpr_solid_forcing_fp64(const SweepArgs& a, int subcycles, cudaStream_t st);
+cudaError_t hpr_solid_relax_fp64(const SweepArgs& a, cudaStream_t st);
 
 // Record the text returned by vg_last_error_string() on this thread.
 void set_last_error(const std::string& msg);

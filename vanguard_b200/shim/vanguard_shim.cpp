@@ -162,8 +162,14 @@ void mhd_params(const MHDMaterialParameters& mp, double* prm) {
     prm[0] = mp.getAdiabaticIndex(), prm[1] = mp.getStiffeningParameter(), prm[2] = mp.getHyperbolicWaveSpeed();
 }
 void hpr_params(const HPRMaterialParameters& mp, double* prm) {
-    if (mp.getEquationOfState() != "StiffenedGas" || mp.getIsPlastic())
-        throw std::runtime_error("HPR: only the StiffenedGas equation of state without plasticity runs on the GPU path");
+    const string& eos = mp.getEquationOfState();
+    if (eos != "StiffenedGas" && eos != "ShockMieGruneisen" && eos != "GodunovRomenski")
+        throw std::runtime_error("HPR: unknown equation of state '" + eos + "'");
+    prm[12] = eos == "StiffenedGas" ? 0.0 : eos == "ShockMieGruneisen" ? 1.0 : 2.0;
+    prm[13] = mp.getReferenceGruneisenCoefficient(), prm[14] = mp.getReferenceSoundSpeed();
+    prm[15] = mp.getHugoniotSlopeCoefficient(), prm[16] = mp.getAlphaParameter();
+    prm[17] = mp.getIsPlastic() ? 1.0 : 0.0, prm[18] = mp.getElasticPlasticTransitionParameter();
+    prm[19] = mp.getPowerLawIndex();
     prm[0] = mp.getAdiabaticIndex(), prm[1] = mp.getStiffeningParameter(), prm[2] = mp.getSpecificHeatCapacity();
     prm[3] = mp.getReferenceDensity(), prm[4] = mp.getInitialTemperature(), prm[5] = mp.getTransverseWaveSpeed();
     prm[6] = mp.getHeatWaveSpeed(), prm[7] = mp.getStrainDissipationTime(), prm[8] = mp.getThermalImpulseRelaxationTime();
@@ -569,10 +575,10 @@ vector<HPRStateVector> HPRSecondOrderSolver::solve(vector<HPRStateVector>& initi
 vector<HPRStateVector> HPRSecondOrderSolver::solve(vector<HPRStateVector>& initialCells, double dx, double cfl, double tEnd,
                                                    double bias, int limiter, int subcycles, HPRMaterialParameters mp,
                                                    int maxSteps) {
-    double prm[12];
+    double prm[20];
     hpr_params(mp, prm);
     std::vector<double> p = pack(initialCells, 17, hpr_get);
-    run_planes(VG_MODEL_HPR, p, (int)initialCells.size(), 1, prm, 12, dx, cfl, tEnd, bias, limiter, subcycles, maxSteps);
+    run_planes(VG_MODEL_HPR, p, (int)initialCells.size(), 1, prm, 20, dx, cfl, tEnd, bias, limiter, subcycles, maxSteps);
     return unpack<HPRStateVector>(p, initialCells.size(), 17, hpr_make);
 }
 vector<vector<HPRStateVector> > HPRSecondOrderSolver::solve2D(vector<vector<HPRStateVector> >& initialCells, double dx, double cfl,
@@ -583,11 +589,11 @@ vector<vector<HPRStateVector> > HPRSecondOrderSolver::solve2D(vector<vector<HPRS
 vector<vector<HPRStateVector> > HPRSecondOrderSolver::solve2D(vector<vector<HPRStateVector> >& initialCells, double dx, double cfl,
                                                               double tEnd, double bias, int limiter, int subcycles,
                                                               HPRMaterialParameters mp, int maxSteps) {
-    double prm[12];
+    double prm[20];
     hpr_params(mp, prm);
     std::vector<double> p = pack2(initialCells, 17, hpr_get);
     long ny = initialCells.size(), nx = initialCells[0].size();
-    run_planes(VG_MODEL_HPR, p, (int)nx, (int)ny, prm, 12, dx, cfl, tEnd, bias, limiter, subcycles, maxSteps);
+    run_planes(VG_MODEL_HPR, p, (int)nx, (int)ny, prm, 20, dx, cfl, tEnd, bias, limiter, subcycles, maxSteps);
     return unpack2<HPRStateVector>(p, nx, ny, 17, hpr_make);
 }
 
@@ -652,10 +658,10 @@ vector<HPRStateVector> HPRFirstOrderSolver::solve(vector<HPRStateVector>& initia
 }
 vector<HPRStateVector> HPRFirstOrderSolver::solve(vector<HPRStateVector>& initialCells, double dx, double cfl, double tEnd,
                                                   int, HPRMaterialParameters mp, int maxSteps) {
-    double prm[12];
+    double prm[20];
     hpr_params(mp, prm);
     std::vector<double> p = pack(initialCells, 17, hpr_get);
-    run_planes(VG_MODEL_HPR, p, (int)initialCells.size(), 1, prm, 12, dx, cfl, tEnd, 0.0, 0, 0, maxSteps, 1);
+    run_planes(VG_MODEL_HPR, p, (int)initialCells.size(), 1, prm, 20, dx, cfl, tEnd, 0.0, 0, 0, maxSteps, 1);
     return unpack<HPRStateVector>(p, initialCells.size(), 17, hpr_make);
 }
 vector<vector<HPRStateVector> > HPRFirstOrderSolver::solve2D(vector<vector<HPRStateVector> >& initialCells, double dx,
@@ -665,10 +671,10 @@ vector<vector<HPRStateVector> > HPRFirstOrderSolver::solve2D(vector<vector<HPRSt
 vector<vector<HPRStateVector> > HPRFirstOrderSolver::solve2D(vector<vector<HPRStateVector> >& initialCells, double dx,
                                                              double cfl, double tEnd, int, HPRMaterialParameters mp,
                                                              int maxSteps) {
-    double prm[12];
+    double prm[20];
     hpr_params(mp, prm);
     std::vector<double> p = pack2(initialCells, 17, hpr_get);
     long ny = initialCells.size(), nx = initialCells[0].size();
-    run_planes(VG_MODEL_HPR, p, (int)nx, (int)ny, prm, 12, dx, cfl, tEnd, 0.0, 0, 0, maxSteps, 1);
+    run_planes(VG_MODEL_HPR, p, (int)nx, (int)ny, prm, 20, dx, cfl, tEnd, 0.0, 0, 0, maxSteps, 1);
     return unpack2<HPRStateVector>(p, nx, ny, 17, hpr_make);
 }

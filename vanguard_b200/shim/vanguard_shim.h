@@ -171,6 +171,12 @@ public:
     double getStrainDissipationTime() const { return strainDissipationTime; }
     double getThermalImpulseRelaxationTime() const { return thermalImpulseRelaxationTime; }
     double getHeatWaveSpeed() const { return heatWaveSpeed; }
+    double getReferenceSoundSpeed() const { return referenceSoundSpeed; }
+    double getReferenceGruneisenCoefficient() const { return referenceGruneisenCoefficient; }
+    double getHugoniotSlopeCoefficient() const { return hugoniotSlopeCoefficient; }
+    double getElasticPlasticTransitionParameter() const { return elasticPlasticTransitionParameter; }
+    double getPowerLawIndex() const { return powerLawIndex; }
+    double getAlphaParameter() const { return alphaParameter; }
     void setIsThermal(bool v) { isThermal = v; }
     void setStrainDissipationTime(double v) { strainDissipationTime = v; }
     void setThermalImpulseRelaxationTime(double v) { thermalImpulseRelaxationTime = v; }

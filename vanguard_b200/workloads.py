@@ -88,13 +88,104 @@ def mhd_vortex_2d(nx=2048, ny=None, seed=0, gamma=5.0 / 3.0, amplitude=1e-3):
 HPR_NVAR = 17  # rho, p, A(9 row-major), u, v, w, Jx, Jy, Jz
 
 
+HPR_EOS = {"StiffenedGas": 0, "ShockMieGruneisen": 1, "GodunovRomenski": 2}
+
+
 def hpr_params(gamma=1.4, p_inf=0.0, c_v=2.5, rho0=1.0, T0=1.0, c_s=1.0, alpha=1.0, tau1=1e-2, tau2=1e-2,
-               T_ref=0.0, p_ref=1.0, thermal=True):
-    """HPRMaterialParameters for the StiffenedGas equation of state (ideal gas when p_inf = 0), non-plastic:
-    {gamma, p_inf, c_v, rho0, T0, c_s, alpha, tau1, tau2, T_ref, p_ref, is_thermal}.  Defaults follow the
-    reference's heat-conduction scenario (HPR/hprtests.cpp:33-57): rho0 = 1, p_ref = 1, T_ref = 0, T0 = 1,
-    c_v = 2.5."""
-    return np.array([gamma, p_inf, c_v, rho0, T0, c_s, alpha, tau1, tau2, T_ref, p_ref, 1.0 if thermal else 0.0])
+               T_ref=0.0, p_ref=1.0, thermal=True, eos="StiffenedGas", Gamma0=0.0, c0=0.0, s=0.0, alpha_eos=0.0,
+               plastic=False, sigma0=0.0, n=0.0):
+    """HPRMaterialParameters (HPR/hprmaterialparameters.cpp:34-69) as the 20-value block
+    {gamma, p_inf, c_v, rho0, T0, c_s, alpha, tau1, tau2, T_ref, p_ref, is_thermal,
+     eos, Gamma0, c0, s, alpha_eos, is_plastic, sigma0, n}.
+    eos: StiffenedGas (gamma, p_inf; an ideal gas when p_inf = 0), ShockMieGruneisen (Gamma0, c0, Hugoniot slope
+    s, reference pressure p_ref) or GodunovRomenski (c0, exponent alpha_eos, Grueneisen coefficient gamma).
+    plastic: the plastic strain relaxation theta1 * (min(|sigma|, 1e8) / sigma0)^n (HPR/hprsourceterms.cpp:12-23).
+    Defaults follow the reference's heat-conduction scenario (HPR/hprtests.cpp:33-57): a non-plastic ideal gas,
+    rho0 = 1, p_ref = 1, T_ref = 0, T0 = 1, c_v = 2.5."""
+    return np.array([gamma, p_inf, c_v, rho0, T0, c_s, alpha, tau1, tau2, T_ref, p_ref, 1.0 if thermal else 0.0,
+                     float(HPR_EOS[eos]), Gamma0, c0, s, alpha_eos, 1.0 if plastic else 0.0, sigma0, n])
+
+
+def hpr_barton_params():
+    """The copper of the reference's Barton test (HPR/hprtests.cpp:59-66): GodunovRomenski, rho0 8.9, c0 3.909,
+    exponent 1, Grueneisen coefficient gamma 1 (its adiabatic index), c_s 2.1, c_v 3.94e-4, T_ref = T0 = 300,
+    tau1 1e8 (elastic), tau2 4e-8, not thermal, not plastic."""
+    return hpr_params(gamma=1.0, p_inf=0.0, c_v=3.94e-4, rho0=8.9, T0=300.0, c_s=2.1,
+                      alpha=8.9 * 3.909 * np.sqrt(4.0e-4 / 300.0), tau1=1e8, tau2=4.0e-8, T_ref=300.0, p_ref=0.0,
+                      thermal=False, eos="GodunovRomenski", c0=3.909, alpha_eos=1.0)
+
+
+def hpr_zhang_params():
+    """The aluminium of the reference's Zhang elastic-plastic test (HPR/hprtests.cpp:109-115): GodunovRomenski,
+    rho0 2.71, c0 5.037, exponent 1, gamma 1, c_s 3.16, c_v 9e-4, p_ref 73, T_ref = T0 = 300, tau1 1e-9, plastic
+    with sigma0 0.2976e9 and n 1.338, not thermal."""
+    return hpr_params(gamma=1.0, p_inf=0.0, c_v=9.0e-4, rho0=2.71, T0=300.0, c_s=3.16, alpha=2.0, tau1=1e-9,
+                      tau2=0.0, T_ref=300.0, p_ref=73.0, thermal=False, eos="GodunovRomenski", Gamma0=1.0, c0=5.037,
+                      s=1.338, alpha_eos=1.0, plastic=True, sigma0=0.2976e9, n=1.338)
+
+
+def hpr_shock_mg_params(thermal=False, plastic=False, sigma0=0.05, n=2.0, tau1=1e-3):
+    """A ShockMieGruneisen solid (copper-like: rho0 8.93, c0 3.94, Gamma0 2.0, Hugoniot slope 1.49, p_ref 1e-4,
+    c_s 2.2, c_v 3.9e-4, T_ref = T0 = 300)."""
+    return hpr_params(gamma=2.0, p_inf=0.0, c_v=3.9e-4, rho0=8.93, T0=300.0, c_s=2.2, alpha=1.0, tau1=tau1,
+                      tau2=1e-3, T_ref=300.0, p_ref=1e-4, thermal=thermal, eos="ShockMieGruneisen", Gamma0=2.0,
+                      c0=3.94, s=1.49, plastic=plastic, sigma0=sigma0, n=n)
+
+
+def gr_reference_pressure(rho, prm):
+    """GodunovRomenski cold pressure c0^2 (rho / alpha) (c - 1) c, c = (rho / rho0)^alpha
+    (HPR/hprmiegruneisen.cpp:55-63)."""
+    c = (rho / prm[3]) ** prm[16]
+    return prm[14] ** 2 * (rho / prm[16]) * (c - 1.0) * c
+
+
+def hpr_solid_riemann_1d(n, prm, F_left, F_right, v_left, v_right, p_offset=0.0):
+    """A 1D solid Riemann problem in the shape of the reference's Barton and Zhang tests (HPR/hprtests.cpp:68-104,
+    :119-131): A = F^-1 on each side of i <= n/2, rho = rho0 det A, velocities v_left / v_right, and the cold state
+    p = p_ref(rho) + p_offset of a GodunovRomenski solid.  The reference's own set-up takes p from the hyperelastic
+    equation of state of its Elasticity module, which this package does not carry."""
+    W = np.zeros((HPR_NVAR, n))
+    left = np.arange(n) <= 0.5 * n
+    for side, F, v in ((left, F_left, v_left), (~left, F_right, v_right)):
+        A = np.linalg.inv(np.asarray(F, dtype=np.float64))
+        rho = prm[3] * np.linalg.det(A)
+        W[0, side] = rho
+        W[1, side] = gr_reference_pressure(rho, prm) + p_offset
+        W[2:11, side] = A.reshape(9)[:, None]
+        W[11:14, side] = np.asarray(v, dtype=np.float64)[:, None]
+    return W
+
+
+def smg_reference_pressure(rho, prm):
+    """ShockMieGruneisen cold pressure (HPR/hprmiegruneisen.cpp:41-54): compressed c0^2 (1/rho0 - 1/rho) /
+    (1/rho0 - s (1/rho0 - 1/rho))^2, expanded c0^2 (rho - rho0)."""
+    rho = np.asarray(rho, dtype=np.float64)
+    v0, c0sq, s = 1.0 / prm[3], prm[14] ** 2, prm[15]
+    comp = c0sq * ((v0 - 1.0 / rho) / (v0 - s * (v0 - 1.0 / rho)) ** 2)
+    return np.where(rho > prm[3], comp, c0sq * (rho - prm[3]))
+
+
+def hpr_shock_riemann(nx, ny, prm, seed=0):
+    """A ShockMieGruneisen solid with a compressed left state (rho 9.4 | 8.93 for the copper-like set) on the cold
+    curve plus a small thermal pressure, A = (rho / rho0)^(1/3) I, and a seeded shear velocity jump; ny == 1 gives
+    planes (17, nx), else (17, ny, nx) with the split along x."""
+    rng = np.random.default_rng(seed)
+    shape = (nx,) if ny == 1 else (ny, nx)
+    W = np.zeros((HPR_NVAR,) + shape)
+    x = np.arange(nx) if ny == 1 else np.meshgrid(np.arange(nx), np.arange(ny))[0]
+    left = x <= 0.5 * nx
+    rho = np.where(left, 1.0526 * prm[3], prm[3])
+    W[0] = rho
+    W[1] = smg_reference_pressure(rho, prm) + np.where(left, 0.02, 1e-3)
+    a = (rho / prm[3]) ** (1.0 / 3.0)
+    W[2] = W[6] = W[10] = a
+    W[11] = np.where(left, 0.0, -0.1)
+    W[12] = np.where(left, rng.uniform(0.02, 0.08), 0.0)
+    return W
+
+
+BARTON_F = ([[0.98, 0.0, 0.0], [0.02, 1.0, 0.1], [0.0, 0.0, 1.0]],
+            [[1.0, 0.0, 0.0], [0.0, 1.0, 0.1], [0.0, 0.0, 1.0]])
 
 
 def hpr_relaxation_times(seed):
