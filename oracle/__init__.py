@@ -251,6 +251,27 @@ def hpr_theta1(params, rho, A, reference=False):
 
 # ------------------------------------------------------------------------------------ reference
 
+def ref_write(model, planes, directory, params=None):
+    """The reference scenarios' own .dat writers (EulerTests / MHDTests / HPRTests::outputSolution{,2D}) on
+    primitive planes, into `directory` (they write into the working directory, which is switched around the
+    call)."""
+    planes = np.ascontiguousarray(planes, dtype=np.float64)
+    nx = planes.shape[-1]
+    ny = 1 if planes.ndim == 2 else planes.shape[1]
+    R = ref()
+    cwd = os.getcwd()
+    os.chdir(directory)
+    try:
+        if model == EULER:
+            R.vgref_write_euler(_ptr(planes), nx)
+        elif model == MHD:
+            R.vgref_write_mhd(_ptr(planes), nx, ny)
+        else:
+            R.vgref_write_hpr(_ptr(planes), nx, ny, _ptr(_params(params)))
+    finally:
+        os.chdir(cwd)
+
+
 def ref_run(model, planes, dx, cfl, t_end=0.0, steps=0, bias=0.0, limiter=SUPERBEE, params=None,
             bc=TRANSMISSIVE, subcycles=0, threads=1):
     """Run the reference's own code on the same planes, in place.  steps <= 0 calls solve()/solve2D()

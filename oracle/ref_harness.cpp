@@ -34,6 +34,9 @@
 #include "Solvers/mhdforcingsolver.h"
 #include "Solvers/hprsecondordersolver.h"
 #include "Solvers/hprforcingsolver.h"
+#include "Euler/eulertests.h"
+#include "MHD/mhdtests.h"
+#include "HPR/hprtests.h"
 
 #include <omp.h>
 #include <iostream>
@@ -605,3 +608,43 @@ extern "C" void vgref_hpr_theta1(const double* prm, const double* rho, const dou
         out[k] = HPRSourceTerms::computeTheta1Reciprocal(rho[k], A, mp);
     }
 }
+
+// ------------------------------------------------------------------------------------ .dat writers
+// The reference scenarios' solution writers, writing density.dat etc. into the current working directory:
+// EulerTests::outputSolution (Euler/eulertests.cpp:54-80), MHDTests::outputSolution{,2D} (MHD/mhdtests.cpp:123-161),
+// HPRTests::outputSolution{,2D} (HPR/hprtests.cpp:219-269).  planes: the model's primitive planes, nx x ny cells.
+extern "C" void vgref_write_euler(const double* planes, int n) {
+    vector<EulerStateVector> cells(n);
+    for (int i = 0; i < n; i++) cells[i] = eulerCell(planes, n, i);
+    EulerTests::outputSolution(cells);
+}
+
+extern "C" void vgref_write_mhd(const double* planes, int nx, int ny) {
+    const long plane = (long)nx * ny;
+    if (ny == 1) {
+        vector<MHDStateVector> cells(nx);
+        for (int i = 0; i < nx; i++) cells[i] = mhdCell(planes, plane, i);
+        MHDTests::outputSolution(cells);
+        return;
+    }
+    vector<vector<MHDStateVector> > g(ny, vector<MHDStateVector>(nx));
+    for (int i = 0; i < ny; i++)
+        for (int j = 0; j < nx; j++) g[i][j] = mhdCell(planes, plane, (long)i * nx + j);
+    MHDTests::outputSolution2D(g);
+}
+
+extern "C" void vgref_write_hpr(const double* planes, int nx, int ny, const double* prm) {
+    HPRMaterialParameters mp = hprParams(prm);
+    const long plane = (long)nx * ny;
+    if (ny == 1) {
+        vector<HPRStateVector> cells(nx);
+        for (int i = 0; i < nx; i++) cells[i] = hprCell(planes, plane, i);
+        HPRTests::outputSolution(cells, mp);
+        return;
+    }
+    vector<vector<HPRStateVector> > g(ny, vector<HPRStateVector>(nx));
+    for (int i = 0; i < ny; i++)
+        for (int j = 0; j < nx; j++) g[i][j] = hprCell(planes, plane, (long)i * nx + j);
+    HPRTests::outputSolution2D(g, mp);
+}
+

@@ -4,7 +4,7 @@
 //   shim_driver <out.bin>
 // Output, in order (float64): Euler 1D solve (6 x 200), Euler 2D per-sweep loop (6 x 24 x 20),
 // MHD solve2D (9 x 16 x 16), HPR solve (17 x 50), Euler 1D step-count solve (6 x 150), Euler 1D first-order solve
-// (6 x 150), then the number of 2D steps the per-sweep loop took.
+// (6 x 150), HPR GodunovRomenski plastic solve (17 x 60), then the number of 2D steps the per-sweep loop took.
 #include <cmath>
 #include <cstdio>
 #include <vector>
@@ -122,6 +122,23 @@ int main(int argc, char** argv) {
         vector<double> v;
         for (int k = 0; k < 6; k++)
             for (auto& c : out) v.push_back(c.computePrimitiveVariableVector()[k]);
+        put(f, v);
+    }
+    // 7) HPRSecondOrderSolver::solve, step-count overload, with the reference's Zhang elastic-plastic material
+    //    (GodunovRomenski, plastic; HPR/hprtests.cpp:109-115), A = I, rho = rho0, u = +-0.75, p = 0, 2 sub-cycles
+    {
+        int n = 60;
+        HPRMaterialParameters mp("GodunovRomenski", false, true, 8.31445985, 2.71, 73.0, 300.0, 300.0, 9.0 * std::pow(10.0, -4.0),
+                                 1.0, 0.0, 5.037, 1.0, 1.338, 0.0, 3.16, std::pow(10.0, -9.0), 0.0, 24.8 * std::pow(10.0, 9.0),
+                                 0.75, 0.2976 * std::pow(10.0, 9.0), 1.338, 2.0, 1.0, 3.577, 2.088);
+        vector<vector<double> > I = {{1.0, 0.0, 0.0}, {0.0, 1.0, 0.0}, {0.0, 0.0, 1.0}};
+        vector<HPRStateVector> cells(n);
+        for (int i = 0; i < n; i++)
+            cells[i] = HPRStateVector(2.71, 0.0, I, i <= 0.5 * n ? 0.75 : -0.75, 0.0, 0.0, 0.0, 0.0, 0.0);
+        vector<HPRStateVector> out = HPRSecondOrderSolver::solve(cells, 10.0 / n, 0.8, 0.0, 0.0, 0, 2, mp, 20);
+        vector<double> v;
+        for (int k = 0; k < 17; k++)
+            for (auto& c : out) v.push_back(c.data()[k]);
         put(f, v);
     }
     double st = steps;

@@ -88,5 +88,14 @@ def test_shim_driver_matches_oracle(gpu, oracle_lib, tmp_path):
     O.run_first_order(O.EULER, ref, 1 / 150, 0.8, t_end=0.05, params=wl.euler_params(1.4))
     assert np.array_equal(got, ref)
 
+    # 7) HPRSecondOrderSolver::solve(..., maxSteps = 20), the Zhang GodunovRomenski plastic material, 2 sub-cycles;
+    #    a solid equation of state calls pow in every pressure recovery: per-plane normwise bound (test_hpr_solids_gpu)
+    got = take((17, 60))
+    zp = wl.hpr_zhang_params()
+    ref = wl.hpr_solid_riemann_1d(60, zp, np.eye(3), np.eye(3), (0.75, 0.0, 0.0), (-0.75, 0.0, 0.0))
+    O.run(O.HPR, ref, 10.0 / 60, 0.8, steps=20, limiter=0, params=zp, subcycles=2)
+    d = np.abs(got - ref).max(axis=1) / np.maximum(np.abs(ref).max(axis=1), 1e-300)
+    assert np.isfinite(got).all() and d.max() <= 1e-10
+
     assert take((1,))[0] == 6
     assert off == data.size
