@@ -104,7 +104,7 @@ constexpr Ops make_ops() {
                &step_begin_impl<M>,
                &finish_impl<M>,
                forcing_of<M>(),
-               (M::NU > 9),
+               tile_kind<M>(),
                &force1_x<M>,
                &force1_y<M>,
                relax_of<M>()};

@@ -2,6 +2,7 @@
 #include "physics_mixed.cuh"
 #include "slic_kernels.cuh"
 #include "slic_mixed.cuh"
+#include "slic_tma.cuh"
 #include "sweep_table.cuh"
 #include "vg_ops.h"
 
@@ -19,6 +20,21 @@ struct MixedKernels {
         } else {
             sweep_x_mixed_kernel<M, P, LPB, MINB><<<grid, nt, 0, st>>>(a);
         }
+    }
+    // persistent: as many blocks as fit on the device at once, or one per tile
+    template <class M, int P, int MINB>
+    static void x_tma(cudaStream_t st, const SweepArgs& a) {
+        static int resident = 0;
+        if (resident == 0) {
+            int per_sm = 0, sms = 0, dev = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_x_tma_kernel<M, P, MINB>, P, 0);
+            resident = (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
+        }
+        const long tiles = (long)((a.nx + P - 3) / (P - 2)) * ((a.ny + 1) / 2);
+        const int grid = (int)(tiles < resident ? tiles : resident);
+        sweep_x_tma_kernel<M, P, MINB><<<grid, P, 0, st>>>(a);
     }
     template <class M, int TX, int TY, int MINB>
     static void y(dim3 grid, int nt, cudaStream_t st, const SweepArgs& a) {
@@ -53,7 +69,8 @@ using ForcingFn = cudaError_t (*)(const SweepArgs&, int, cudaStream_t);
 template <class M>
 constexpr Ops make_ops(ForcingFn forcing = nullptr, SweepFn relax = nullptr) {
     return Ops{M::NW, SweepTable<MixedKernels, M>::x, SweepTable<MixedKernels, M>::y, &max_wave_impl<M>,
-               &step_begin_impl<M>, &finish_impl<M>, forcing, (M::NU > 9), nullptr, nullptr, relax};
+               &step_begin_impl<M>, &finish_impl<M>, forcing, tile_kind<M>(), nullptr, nullptr, relax,
+               tile_kind<M>() == 2 ? M::NW : 0};
 }
 
 const Ops kOps[V_COUNT] = {

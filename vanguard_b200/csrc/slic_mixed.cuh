@@ -366,6 +366,52 @@ __device__ __forceinline__ f2 half_slope2(f2 dm, f2 dp, const MixedConst& k) {
     return sel2(nd.v.x < 0.0f, nd.v.y < 0.0f, splat2(0.0f), base * half_xi);
 }
 
+// evolve_edges_mixed for two lanes: get(i, o) returns component i of the FP64 conserved vector of the left
+// neighbour (o = 0), the cell (1) and the right neighbour (2), one lane each in the double2's x and y.  Same
+// operations as the inline stages of sweep_x_pair_kernel (used by the TMA-staged sweep, whose shared tiles keep the
+// two rows apart).
+template <class M, int AXIS, class Get>
+__device__ __forceinline__ void evolve_edges_pair(Get get, const MixedConst& k, const typename M::P& q,
+                                                  f2* ua_left_side, f2* ua_right_side) {
+    constexpr int NU = M::NU;
+    f2 xl[NU], xr[NU], fl[NU], fr[NU];
+#pragma unroll
+    for (int i = 0; i < NU; i++) {
+        const double2 L = get(i, 0), C = get(i, 1), R = get(i, 2);
+        const f2 hs = half_slope2(mk2((float)(C.x - L.x), (float)(C.y - L.y)),
+                                  mk2((float)(R.x - C.x), (float)(R.y - C.y)), k);
+        const f2 uc = mk2((float)C.x, (float)C.y);
+        xl[i] = uc - hs;
+        xr[i] = uc + hs;
+    }
+    M::template flux2<AXIS>(xl, q, fl);
+    M::template flux2<AXIS>(xr, q, fr);
+#pragma unroll
+    for (int i = 0; i < NU; i++) {
+        const f2 ev = splat2(k.half_r) * (fl[i] - fr[i]);
+        ua_left_side[i] = xl[i] + ev;
+        ua_right_side[i] = xr[i] + ev;
+    }
+}
+
+// force_flux_mixed for two lanes
+template <class M, int AXIS>
+__device__ __forceinline__ void force_flux_pair(const f2* ua, const f2* ub, const MixedConst& k,
+                                                const typename M::P& q, f2* F) {
+    constexpr int NU = M::NU;
+    f2 fa[NU], fb[NU], uri[NU], fri[NU];
+    M::template flux2<AXIS>(ua, q, fa);
+    M::template flux2<AXIS>(ub, q, fb);
+#pragma unroll
+    for (int i = 0; i < NU; i++) uri[i] = fma2(splat2(0.5f), ua[i] + ub[i], splat2(0.5f * k.r_f) * (fa[i] - fb[i]));
+    M::template flux2<AXIS>(uri, q, fri);
+#pragma unroll
+    for (int i = 0; i < NU; i++) {
+        const f2 lf = fma2(splat2(0.5f), fa[i] + fb[i], splat2(0.5f * k.rinv_f) * (ua[i] - ub[i]));
+        F[i] = splat2(0.5f) * (lf + fri[i]);
+    }
+}
+
 template <class M, int P, int LPB, int MINB>
 __global__ void __launch_bounds__(P* LPB, MINB) sweep_x_pair_kernel(SweepArgs a) {
     constexpr int NU = M::NU, NW = M::NW;

@@ -37,13 +37,38 @@ cudaError_t launch_y(const SweepArgs& a, cudaStream_t st) {
     }
 }
 
+// X sweep staged by TMA (persistent, two rows per thread; see slic_tma.cuh) when the solver holds a tensor map over
+// a.in, else the plain two-row kernel of the same shape.
+template <class K, class M, int P, int MINB>
+cudaError_t launch_x_tma(const SweepArgs& a, cudaStream_t st) {
+    static_assert(P == kTmaTile, "the solver's tensor maps have a box of kTmaTile + 2 cells");
+    if (!a.tmap) return launch_x<K, M, P, 1, MINB>(a, st);
+    K::template x_tma<M, P, MINB>(st, a);
+    return cudaGetLastError();
+}
+
+template <class M, class = void>
+struct pair_sweeps {
+    static constexpr bool value = false;
+};
+template <class M>
+struct pair_sweeps<M, decltype((void)M::PAIR_X)> {
+    static constexpr bool value = M::PAIR_X;
+};
+
 // Models with more than 9 conserved components (HPR, 17) use shorter X segments so that the three FP64
-// shared-memory tiles stay inside the 48 KB static limit.
-template <class K, class M, bool BIG = (M::NU > 9)>
+// shared-memory tiles stay inside the 48 KB static limit (kind 1).  The PAIR_X models (two rows per thread in the
+// X sweep) add the TMA-staged X shapes (kind 2).
+template <class M>
+constexpr int tile_kind() {
+    return (M::NU > 9) ? 1 : pair_sweeps<M>::value ? 2 : 0;
+}
+
+template <class K, class M, int KIND = tile_kind<M>()>
 struct SweepTable;
 
 template <class K, class M>
-struct SweepTable<K, M, true> {
+struct SweepTable<K, M, 1> {
     static constexpr SweepFn x[kNumXCfg] = {
         launch_x<K, M, 64, 1, 1>, launch_x<K, M, 32, 2, 1>, launch_x<K, M, 96, 1, 1>,
         launch_x<K, M, 64, 1, 2>, launch_x<K, M, 32, 1, 1>,
@@ -55,7 +80,7 @@ struct SweepTable<K, M, true> {
 };
 
 template <class K, class M>
-struct SweepTable<K, M, false> {
+struct SweepTable<K, M, 0> {
     static constexpr SweepFn x[kNumXCfg] = {
         launch_x<K, M, 128, 1, 1>, launch_x<K, M, 64, 2, 1>, launch_x<K, M, 192, 1, 1>,
         launch_x<K, M, 128, 1, 6>, launch_x<K, M, 128, 1, 8>,
@@ -66,16 +91,30 @@ struct SweepTable<K, M, false> {
     };
 };
 
-inline const char* x_cfg_name(int i, bool big = false) {
+template <class K, class M>
+struct SweepTable<K, M, 2> {
+    static constexpr SweepFn x[kNumXCfg] = {
+        launch_x<K, M, 128, 1, 1>, launch_x_tma<K, M, 128, 7>, launch_x_tma<K, M, 128, 8>,
+        launch_x<K, M, 128, 1, 6>, launch_x<K, M, 128, 1, 8>,
+    };
+    static constexpr SweepFn y[kNumYCfg] = {
+        launch_y<K, M, 64, 64, 1>, launch_y<K, M, 64, 32, 1>, launch_y<K, M, 64, 64, 12>,
+        launch_y<K, M, 64, 64, 16>, launch_y<K, M, 128, 32, 5>, launch_y<K, M, 32, 64, 1>,
+    };
+};
+
+// Names of the shapes of SweepTable<K, M, kind>.
+inline const char* x_cfg_name(int i, int kind = 0) {
     static const char* n[kNumXCfg] = {"P128xL1", "P64xL2", "P192xL1", "P128xL1/min6", "P128xL1/min8"};
     static const char* nb[kNumXCfg] = {"P64xL1", "P32xL2", "P96xL1", "P64xL1/min2", "P32xL1"};
-    return (i >= 0 && i < kNumXCfg) ? (big ? nb[i] : n[i]) : "?";
+    static const char* np[kNumXCfg] = {"P128x2", "TMA P128x2/min7", "TMA P128x2/min8", "P128x2/min6", "P128x2/min8"};
+    return (i >= 0 && i < kNumXCfg) ? (kind == 1 ? nb[i] : kind == 2 ? np[i] : n[i]) : "?";
 }
-inline const char* y_cfg_name(int i, bool big = false) {
+inline const char* y_cfg_name(int i, int kind = 0) {
     static const char* n[kNumYCfg] = {"TX64xTY64", "TX64xTY32", "TX64xTY64/min12", "TX64xTY64/min16",
                                       "TX128xTY32/min5", "TX32xTY64"};
     static const char* nb[kNumYCfg] = {"TX64xTY64", "TX64xTY32", "TX32xTY32", "TX32xTY64", "TX128xTY32", "TX64xTY16"};
-    return (i >= 0 && i < kNumYCfg) ? (big ? nb[i] : n[i]) : "?";
+    return (i >= 0 && i < kNumYCfg) ? (kind == 1 ? nb[i] : n[i]) : "?";
 }
 
 }  // namespace vg

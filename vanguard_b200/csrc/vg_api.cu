@@ -1,5 +1,7 @@
 // C ABI of the SLIC/FORCE solver (include/vanguard_slic.h): solver objects, state upload/download, the
 // device-resident time loop replayed from captured CUDA graphs, and the per-sweep entry points.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <climits>
@@ -81,6 +83,9 @@ struct vg_solver {
     } g;
     long last_launches = 0;
     int xcfg = 0, ycfg = 0;   // launch configuration of each sweep (sweep_table.cuh)
+    // TMA tensor maps over buf[0] and buf[1] for the TMA-staged X sweep (device memory; null: none)
+    CUtensorMap* d_tmaps = nullptr;
+    int tmap_planes = 0;
 };
 
 namespace {
@@ -100,9 +105,47 @@ SweepArgs prepared(const SweepArgs& a0) {
     return a;
 }
 
+// The tensor map over a.in for the TMA-staged X sweep, where the solver holds one for that buffer.
+const void* tmap_for(const vg_solver* s, const double* in) {
+    if (!s->d_tmaps || s->tmap_planes != s->ops->tma_planes) return nullptr;
+    return in == s->buf[0] ? (const void*)&s->d_tmaps[0] : in == s->buf[1] ? (const void*)&s->d_tmaps[1] : nullptr;
+}
+
 cudaError_t run_sweep(const vg_solver* s, int axis, const SweepArgs& a0, cudaStream_t st) {
-    const SweepArgs a = prepared(a0);
+    SweepArgs a = prepared(a0);
+    a.tmap = axis == 0 ? tmap_for(s, a.in) : nullptr;
     return axis == 0 ? s->ops->x[s->xcfg](a, st) : s->ops->y[s->ycfg](a, st);
+}
+
+// Tensor maps of the TMA-staged X sweep over both state buffers: dims {nx, ny, planes}, row and plane strides in
+// bytes, box {kTmaTile + 2, 2, planes} of FP64 with zero fill outside the grid.  The driver's encoder is reached
+// through the runtime's entry-point query, so the library needs no link to libcuda.  On any failure the solver
+// keeps no maps and the sweep shapes fall back to the plain two-row kernel.
+void build_tmaps(vg_solver* s, int planes) {
+    if (s->d_tmaps && s->tmap_planes == planes) return;
+    s->tmap_planes = 0;
+    PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    cudaDriverEntryPointQueryResult qr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", (void**)&encode, cudaEnableDefault, &qr) != cudaSuccess ||
+        qr != cudaDriverEntryPointSuccess || !encode)
+        return;
+    CUtensorMap maps[2];
+    for (int b = 0; b < 2; b++) {
+        const cuuint64_t dims[3] = {(cuuint64_t)s->d.nx, (cuuint64_t)s->d.ny, (cuuint64_t)planes};
+        const cuuint64_t strides[2] = {(cuuint64_t)(s->pitch * sizeof(double)), (cuuint64_t)(s->plane * sizeof(double))};
+        const cuuint32_t box[3] = {(cuuint32_t)(vg::kTmaTile + 2), 2u, (cuuint32_t)planes};
+        const cuuint32_t estr[3] = {1u, 1u, 1u};
+        if (encode(&maps[b], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, s->buf[b], dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return;
+    }
+    if (!s->d_tmaps && cudaMalloc(&s->d_tmaps, sizeof(maps)) != cudaSuccess) {
+        s->d_tmaps = nullptr;
+        return;
+    }
+    if (cudaMemcpy(s->d_tmaps, maps, sizeof(maps), cudaMemcpyHostToDevice) != cudaSuccess) return;
+    s->tmap_planes = planes;
 }
 
 // In-process cache of tuned launch configurations keyed by variant, precision, grid and SM count;
@@ -387,6 +430,7 @@ vg_status vg_destroy(vg_solver* s) {
     for (auto& b : s->buf)
         if (b) cudaFree(b);
     if (s->aux) cudaFree(s->aux);
+    if (s->d_tmaps) cudaFree(s->d_tmaps);
     if (s->ctrl) cudaFree(s->ctrl);
     if (s->dout) cudaFree(s->dout);
     if (s->hctrl) cudaFreeHost(s->hctrl);
@@ -434,6 +478,7 @@ vg_status vg_upload_primitive(vg_solver* s, const double* planes, int is_device,
     s->variant = variant;
     s->ops = ops;
     s->cur = 0;
+    if (ops->tma_planes > 0) build_tmaps(s, ops->tma_planes);
     for (int k = 0; k < ops->nw; k++) {
         const double* src = planes + (long)kPlanes[variant][k] * n;
         VG_CUDA(cudaMemcpy2DAsync(s->buf[0] + k * s->plane, sizeof(double) * s->pitch, src, sizeof(double) * s->d.nx,
@@ -548,6 +593,7 @@ vg_status vg_run(vg_solver* s, const vg_run_config* cfg, int* steps_taken, doubl
     s->last_launches = launches;
     if (steps_taken) *steps_taken = h->it;
     if (t_reached) *t_reached = h->t;
+    if (h->err & vg::ERR_TIMEOUT) return fail(VG_ETIMEOUT, "a bounded wait of the TMA-staged sweep gave up");
     if (h->err) return fail(VG_ENAN, "non-finite or non-positive density/pressure produced");
     return VG_OK;
 }
@@ -627,9 +673,9 @@ vg_status vg_get_launch_config(vg_solver* s, int* xcfg, int* ycfg, const char** 
     if (!s) return fail(VG_EINVAL, "null solver");
     if (xcfg) *xcfg = s->xcfg;
     if (ycfg) *ycfg = s->ycfg;
-    const bool big = s->ops && s->ops->big_tiles;
-    if (xname) *xname = vg::x_cfg_name(s->xcfg, big);
-    if (yname) *yname = vg::y_cfg_name(s->ycfg, big);
+    const int kind = s->ops ? s->ops->tile_kind : 0;
+    if (xname) *xname = vg::x_cfg_name(s->xcfg, kind);
+    if (yname) *yname = vg::y_cfg_name(s->ycfg, kind);
     return VG_OK;
 }
 
@@ -669,6 +715,7 @@ vg_status vg_autotune(vg_solver* s, const vg_run_config* cfg, int reps, float* t
         int n = axis == 0 ? vg::kNumXCfg : vg::kNumYCfg;
         for (int c = 0; c < n; c++) {
             const vg::SweepFn fn = axis == 0 ? s->ops->x[c] : s->ops->y[c];
+            a.tmap = axis == 0 ? tmap_for(s, a.in) : nullptr;
             cudaError_t e = fn(a, st);  // warm-up (module load, caches)
             if (e != cudaSuccess) {
                 cudaEventDestroy(e0);

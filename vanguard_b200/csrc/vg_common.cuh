@@ -29,7 +29,7 @@ struct Ctrl {
     float kr_f[2], krinv_f[2], khalf_r_f[2];
 };
 
-enum : unsigned int { ERR_STATE = 1u };
+enum : unsigned int { ERR_STATE = 1u, ERR_TIMEOUT = 2u };  // bits of Ctrl::err
 
 // Ghost-cell index along one axis of length n with 2 ghost cells per side (k in [-2, n+1]):
 // transmissive mirror g[-1] = c[0], g[-2] = c[1], g[n] = c[n-1], g[n+1] = c[n-2] (Solvers/solvers.cpp:17-23)
@@ -62,6 +62,7 @@ struct SweepConst {
 };
 
 constexpr int kParams = 24;           // VG_MAX_PARAMS
+constexpr int kTmaTile = 128;         // threads (cells per row, halo included: kTmaTile + 2) of the TMA X sweep
 constexpr int kInvGm1 = kParams - 1;  // slot the host fills with 1 / (gamma - 1)
 
 // Launch-independent description of one sweep.
@@ -91,6 +92,9 @@ struct SweepArgs {
     unsigned int* err;             // error word (always valid)
     double* aux;                   // model scratch planes (HPR forcing neighbours), or null
     double params[kParams];  // model parameters (model-specific layout); params[kInvGm1] = 1 / (params[0] - 1)
+    // device CUtensorMap over `in` for the TMA-staged X sweep (null: none); kept last, since a field ahead of
+    // params[] changed the register allocation of the two-row X sweep (56 -> 60)
+    const void* tmap;
 };
 
 // Sweep constants of one sweep of length ts = dt * scale, formed as the reference forms them

@@ -35,12 +35,14 @@ struct Ops {
     // One relaxation-source sub-cycle of length 0.5 dt / subcycles, a.in -> a.out, with a.aux as scratch
     // (kForcingLaunches kernels; null: model has no source).
     cudaError_t (*forcing)(const SweepArgs& a, int subcycles, cudaStream_t st);
-    bool big_tiles;  // SweepTable<.., BIG = true> (names of the launch configurations)
+    int tile_kind;  // SweepTable kind: 0 default, 1 big models, 2 PAIR_X models (names of the launch configurations)
     // First-order FORCE sweeps (FirstOrderSolver), null where the form has none.
     SweepFn x1 = nullptr;
     SweepFn y1 = nullptr;
     // Stiff relaxation of the source over dt * a.dt_scale, in place on a.out (HPR), null where the model has none.
     SweepFn relax = nullptr;
+    // Planes of the box of the TMA-staged X sweep (its tensor maps: box {130, 2, tma_planes}); 0: no TMA sweep.
+    int tma_planes = 0;
 };
 
 constexpr int kForcingLaunches = 2;  // kernels per forcing sub-cycle
