@@ -87,7 +87,7 @@ typedef struct vg_run_config {
     int subcycles;      /* subcyclingIterations (source integration; HPR and MHD only; second order only) */
     int order;          /* 2 (or 0): SecondOrderSolver's SLIC loop; 1: FirstOrderSolver's FORCE loop
                          * (Solvers/firstordersolver.cpp:435-553 and the MHD / HPR twins: 1-ghost boundary, FORCE
-                         * of the cells themselves, no source, the MHD c_h kept at params[2]; VG_FP64 only) */
+                         * of the cells themselves, no source, the MHD c_h kept at params[2]; both forms) */
     int stiff_source;   /* HPR only, no counterpart in the reference: 1 replaces the RK4 forcing sub-cycles by a
                          * stiff relaxation of dt/2 before and after the sweeps, cell by cell (distortion by implicit
                          * Euler on the eigenvalues of A^T A, heat flux by exponential sub-steps), stable at any tau;

@@ -3,6 +3,7 @@
 #include "slic_kernels.cuh"
 #include "slic_mixed.cuh"
 #include "slic_tma.cuh"
+#include "first_order_mixed.cuh"
 #include "sweep_table.cuh"
 #include "vg_ops.h"
 
@@ -63,13 +64,31 @@ cudaError_t finish_impl(const SweepArgs& a, double* out, cudaStream_t st) {
     return cudaGetLastError();
 }
 
+template <class M>
+cudaError_t force1_x(const SweepArgs& a, cudaStream_t st) {
+    constexpr int P = 128;
+    force1_x_mixed_kernel<M, P><<<dim3((a.nx + P - 1) / P, a.ny), P, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+template <class M>
+cudaError_t force1_y(const SweepArgs& a, cudaStream_t st) {
+    if constexpr (!M::HAS_Y) {
+        return cudaErrorInvalidValue;
+    } else {
+        constexpr int TX = 64, TY = 64;
+        force1_y_mixed_kernel<M, TX, TY><<<dim3((a.nx + TX - 1) / TX, (a.ny + TY - 1) / TY), TX, 0, st>>>(a);
+        return cudaGetLastError();
+    }
+}
+
 using ForcingFn = cudaError_t (*)(const SweepArgs&, int, cudaStream_t);
 
 // The source sub-cycles keep FP64: the exact forcing kernels of each model
 template <class M>
 constexpr Ops make_ops(ForcingFn forcing = nullptr, SweepFn relax = nullptr) {
     return Ops{M::NW, SweepTable<MixedKernels, M>::x, SweepTable<MixedKernels, M>::y, &max_wave_impl<M>,
-               &step_begin_impl<M>, &finish_impl<M>, forcing, tile_kind<M>(), nullptr, nullptr, relax,
+               &step_begin_impl<M>, &finish_impl<M>, forcing, tile_kind<M>(), &force1_x<M>, &force1_y<M>, relax,
                tile_kind<M>() == 2 ? M::NW : 0};
 }
 

@@ -528,7 +528,7 @@ vg_status vg_run(vg_solver* s, const vg_run_config* cfg, int* steps_taken, doubl
     if (cfg->subcycles > 0 && !s->ops->forcing)
         return fail(VG_EUNSUPPORTED, "source sub-cycling needs a model with a source (HPR relaxation, MHD GLM damping)");
     if (cfg->order != 0 && cfg->order != 1 && cfg->order != 2) return fail(VG_EINVAL, "order must be 1 or 2");
-    if (cfg->order == 1 && !s->ops->x1) return fail(VG_EUNSUPPORTED, "the first-order loop runs in VG_FP64 only");
+    if (cfg->order == 1 && !s->ops->x1) return fail(VG_EUNSUPPORTED, "this kernel form has no first-order loop");
     if (cfg->stiff_source && cfg->order != 1 && !s->ops->relax)
         return fail(VG_EUNSUPPORTED, "the stiff source relaxation exists for the HPR model only");
     if (cfg->stiff_source && cfg->order != 1 && s->d.params[17] != 0.0)
