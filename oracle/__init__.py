@@ -23,7 +23,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libvgref.so")
 
-EULER, MHD, HPR = 0, 1, 2
+EULER, MHD, HPR, EULER_REDUCED = 0, 1, 2, 3
 NVAR = {EULER: 6, MHD: 9, HPR: 17}
 TRANSMISSIVE, PERIODIC = 0, 1
 SUPERBEE, VANLEER, MINBEE = 0, 1, 2
@@ -227,6 +227,34 @@ def hpr_cell(w, params, reference=False):
     fn = ref().vgref_hpr_cell if reference else lib().vo_hpr_cell
     fn(_ptr(w), _ptr(prm), *[_ptr(o) for o in outs], _ptr(sp))
     return (*outs, sp)
+
+
+def run_reduced(planes, dx, cfl, t_end=0.0, steps=0, bias=0.0, limiter=SUPERBEE, params=None, reinit=0,
+                reference=False, threads=1):
+    """SecondOrderSolver::solve{,2D} of the Euler reduced two-material model on its 7 primitive planes (alpha1, u, v,
+    w, rho1, rho2, p) x (n) or (ny, nx), in place, from the restatement or (reference=True) the reference; params =
+    (gamma1, p_inf1, gamma2, p_inf2); reinit > 0 reinitialises the volume fraction every `reinit` steps.  Returns
+    (t, steps)."""
+    assert planes.shape[0] == 7 and planes.dtype == np.float64 and planes.flags.c_contiguous
+    nx = planes.shape[-1]
+    ny = 1 if planes.ndim == 2 else planes.shape[1]
+    prm = _params(params)
+    st = ctypes.c_int()
+    if reference:
+        R = ref()
+        R.vgref_set_threads(threads)
+        R.vgref_reduced_run.restype = _c_double
+        t = R.vgref_reduced_run(_ptr(planes), nx, ny, _c_double(dx), _c_double(cfl), _c_double(t_end), steps,
+                                _c_double(bias), limiter, _ptr(prm), reinit, ctypes.byref(st))
+        return t, st.value
+    padded = np.zeros((8,) + planes.shape[1:])
+    padded[:7] = planes
+    L = lib()
+    L.vo_run_reduced.restype = _c_double
+    t = L.vo_run_reduced(_ptr(padded), nx, ny, _c_double(dx), _c_double(cfl), _c_double(t_end), steps,
+                         _c_double(bias), limiter, _ptr(prm), 0, reinit, ctypes.byref(st))
+    planes[:] = padded[:7]
+    return t, st.value
 
 
 def hpr_eos(params, rho, p, e, reference=False):

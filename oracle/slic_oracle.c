@@ -801,21 +801,141 @@ static void hpr_default(const double* prm, double* W) {
     W[10] = c * 1.0;
 }
 
+/* ---- Euler reduced two-material model: Euler/Multiphysics/eulerreducedstatevector.cpp, prm = {gamma1, p_inf1,
+ * gamma2, p_inf2}.  W = alpha1, u, v, w, rho1, rho2, p (the reference's primitive order) and an unused eighth plane;
+ * U = rho, rho alpha1, rho u, rho v, rho w, alpha1 rho1, alpha2 rho2, rho E.  Every volume fraction the model derives
+ * or uses is clamped to [0.001, 0.999] (:47-58, :99-108, :131-147). */
+static double red_clamp(double a) {
+    if (a < 0.001) return 0.001;
+    if (a > 0.999) return 0.999;
+    return a;
+}
+/* EulerReducedStateVector::computeConservedVariableVector (:96-129) */
+static void red_cons(const double* W, const double* prm, double* U) {
+    double a1 = red_clamp(W[0]), a2 = 1.0 - a1;
+    double u = W[1], v = W[2], w = W[3], r1 = W[4], r2 = W[5], p = W[6];
+    double rho = (a1 * r1) + (a2 * r2);
+    U[0] = rho;
+    U[1] = rho * a1;
+    U[2] = rho * u;
+    U[3] = rho * v;
+    U[4] = rho * w;
+    U[5] = a1 * r1;
+    U[6] = a2 * r2;
+    double v2 = ((u * u) + (v * v)) + (w * w);
+    double e1 = euler_e(rho, p, prm) + (0.5 * v2), e2 = euler_e(rho, p, prm + 2) + (0.5 * v2);
+    U[7] = rho * ((a1 * e1) + (a2 * e2));
+}
+/* EulerReducedStateVector::setConservedVariableVector (:43-73) */
+static void red_setcons(const double* U, const double* prm, double* W) {
+    double rho = U[0];
+    double a1 = red_clamp(U[1] / rho), a2 = 1.0 - a1;
+    double u = U[2] / rho, v = U[3] / rho, w = U[4] / rho;
+    double v2 = ((u * u) + (v * v)) + (w * w);
+    double e = (U[7] / rho) - (0.5 * v2);
+    W[0] = a1; W[1] = u; W[2] = v; W[3] = w;
+    W[4] = U[5] / a1;
+    W[5] = U[6] / a2;
+    W[6] = (a1 * euler_p(rho, e, prm)) + (a2 * euler_p(rho, e, prm + 2));
+    W[7] = 0.0;
+}
+/* EulerReducedStateVector::compute{X,Y}FluxVector(vector, params, params) (:131-180, :187-236) */
+static void red_flux(const double* U, int axis, const double* prm, double* F) {
+    double rho = U[0];
+    double a1 = red_clamp(U[1] / rho), a2 = 1.0 - a1;
+    double u = U[2] / rho, v = U[3] / rho, w = U[4] / rho;
+    double r1 = U[5] / a1, r2 = U[6] / a2;
+    double E = U[7] / rho;
+    double v2 = ((u * u) + (v * v)) + (w * w);
+    double e = E - (0.5 * v2);
+    double p = (a1 * euler_p(rho, e, prm)) + (a2 * euler_p(rho, e, prm + 2));
+    double un = axis == 0 ? u : v;
+    F[0] = rho * un;
+    F[1] = rho * (un * a1);
+    F[2] = rho * (un * u);
+    F[3] = rho * (un * v);
+    F[4] = rho * (un * w);
+    F[axis == 0 ? 2 : 3] += p;
+    F[5] = a1 * (r1 * un);
+    F[6] = a2 * (r2 * un);
+    F[7] = (rho * (un * E)) + (un * p);
+}
+/* EulerEquationOfState::computeSoundSpeed (Euler/eulerequationofstate.cpp:23-29) of material k */
+static double red_c(double rho_k, double p, const double* mk) { return sqrt((mk[0] * (p + mk[1])) / rho_k); }
+/* Solvers::computeMaximumWaveSpeed{,2D} for the reduced model (Solvers/solvers.cpp:298-316, :365-387) */
+static double red_wave1d(const double* W, const double* prm) {
+    return fabs(W[1]) + smax(red_c(W[4], W[6], prm), red_c(W[5], W[6], prm + 2));
+}
+static double red_wave2d(const double* W, const double* prm) {
+    return smax(fabs(W[1]), fabs(W[2])) + smax(red_c(W[4], W[6], prm), red_c(W[5], W[6], prm + 2));
+}
+/* EulerReducedStateVector() (:3-14) */
+static void red_default(const double* prm, double* W) {
+    (void)prm;
+    W[0] = 0.999; W[1] = 0.0; W[2] = 0.0; W[3] = 0.0; W[4] = 1.0; W[5] = 1.0; W[6] = 1.0; W[7] = 0.0;
+}
+
+/* relaxTotalDensity (:281-287) and the volume fraction of a cell of a reinitialisation window */
+static void red_reset_cell(double* planes, long plane, long idx, double alpha) {
+    double a1 = planes[idx];
+    double rho = (a1 * planes[4 * plane + idx]) + ((1.0 - a1) * planes[5 * plane + idx]);
+    planes[4 * plane + idx] = rho;
+    planes[5 * plane + idx] = rho;
+    planes[idx] = alpha;
+}
+/* MultiphysicsSolvers::reinitialiseVolumeFraction for the reduced model (Solvers/multiphysicssolvers.cpp:164-191 in
+ * 1D, :193-... in 2D).  1D: the last cell i >= 1 with alpha_i < 0.5 <= alpha_{i-1} (the loop's single-thread
+ * outcome; i = 0 would read cell -1), or 0, and the window i-2 .. i+1.  2D: per row, then per column, every such
+ * descending crossing (window set to 0.999 | 0.001) and every ascending one (alpha_j > 0.5 >= alpha_{j-1}; 0.001 |
+ * 0.999), at most 100 of each kind per line.  Window cells outside the grid, which the reference writes out of
+ * bounds, are skipped. */
+static void red_reinit_line(double* planes, long plane, long start, long stride, int len) {
+    int loc1[100], loc2[100], n1 = 0, n2 = 0;
+    for (int j = 1; j < len; j++) {
+        double a = planes[start + j * stride], b = planes[start + (j - 1) * stride];
+        if (a < 0.5 && b >= 0.5 && n1 < 100) loc1[n1++] = j;
+        if (a > 0.5 && b <= 0.5 && n2 < 100) loc2[n2++] = j;
+    }
+    for (int k = 0; k < n1; k++)
+        for (int j = loc1[k] - 2; j < loc1[k] + 2; j++)
+            if (j >= 0 && j < len) red_reset_cell(planes, plane, start + j * stride, j < loc1[k] ? 0.999 : 0.001);
+    for (int k = 0; k < n2; k++)
+        for (int j = loc2[k] - 2; j < loc2[k] + 2; j++)
+            if (j >= 0 && j < len) red_reset_cell(planes, plane, start + j * stride, j < loc2[k] ? 0.001 : 0.999);
+}
+static void red_reinit(double* planes, int nx, int ny) {
+    long plane = (long)nx * ny;
+    if (ny == 1) {
+        int loc = 0;
+        for (int i = 1; i < nx; i++)
+            if (planes[i] < 0.5 && planes[i - 1] >= 0.5) loc = i;
+        for (int i = loc - 2; i < loc + 2; i++)
+            if (i >= 0 && i < nx) red_reset_cell(planes, plane, i, i < loc ? 0.999 : 0.001);
+        return;
+    }
+    for (int i = 0; i < ny; i++) red_reinit_line(planes, plane, (long)i * nx, 1, nx);
+    for (int j = 0; j < nx; j++) red_reinit_line(planes, plane, j, nx, ny);
+}
+
 static const model M_EULER = {6, euler_cons, euler_setcons, euler_flux, euler_wave1d, euler_wave2d, euler_default, 0};
 static const model M_MHD = {9, mhd_cons, mhd_setcons, mhd_flux, mhd_wave1d, mhd_wave2d, mhd_default, mhd_source};
 static const model M_HPR = {17, hpr_cons, hpr_setcons, hpr_flux, hpr_wave1d, hpr_wave2d, hpr_default, hpr_source};
+static const model M_RED = {8, red_cons, red_setcons, red_flux, red_wave1d, red_wave2d, red_default, 0};
 
 static const model* model_of(int id) {
     switch (id) {
         case VO_EULER: return &M_EULER;
         case VO_MHD: return &M_MHD;
         case VO_HPR: return &M_HPR;
+        case VO_EULER_REDUCED: return &M_RED;
         default: return NULL;
     }
 }
 
 int vo_nvar(int id) { const model* m = model_of(id); return m ? m->nv : 0; }
-int vo_nparams(int id) { return id == VO_EULER ? 6 : id == VO_MHD ? 3 : id == VO_HPR ? 20 : 0; }
+int vo_nparams(int id) {
+    return id == VO_EULER ? 6 : id == VO_MHD ? 3 : id == VO_HPR ? 20 : id == VO_EULER_REDUCED ? 4 : 0;
+}
 
 /* ------------------------------------------------------------------------------- SLIC building blocks */
 
@@ -1145,7 +1265,7 @@ static double stable_dt(double dt, double t, double t_end, int it) {
  * :513-515). */
 static double run(int id, double* planes, int nx, int ny, int dims, double dx, double cfl, double t_end,
                   int max_steps, double w, int lim, const double* prm_in, int bc, int subcycles, int* steps_out,
-                  double* dt_log) {
+                  double* dt_log, int reinit_freq) {
     const model* m = model_of(id);
     if (!m) return -1.0;
     double prm[24];
@@ -1178,6 +1298,8 @@ static double run(int id, double* planes, int nx, int ny, int dims, double dx, d
         if (stiff) relax_grid(m, planes, plane, 0.5 * dt, prm);
         t += dt;
         it += 1;
+        /* the reduced model's solve{,2D}: reinitialisation every reinit_freq steps (Solvers/secondordersolver.cpp) */
+        if (id == VO_EULER_REDUCED && reinit_freq != 0 && (it % reinit_freq) == 0) red_reinit(planes, nx, dims == 1 ? 1 : ny);
     }
     if (steps_out) *steps_out = it;
     return t;
@@ -1251,12 +1373,18 @@ double vo_run_first_order(int id, double* planes, int nx, int ny, double dx, dou
 
 double vo_run1d(int id, double* planes, int n, double dx, double cfl, double t_end, int max_steps, double w,
                 int lim, const double* prm, int bc, int subcycles, int* steps_out, double* dt_log) {
-    return run(id, planes, n, 1, 1, dx, cfl, t_end, max_steps, w, lim, prm, bc, subcycles, steps_out, dt_log);
+    return run(id, planes, n, 1, 1, dx, cfl, t_end, max_steps, w, lim, prm, bc, subcycles, steps_out, dt_log, 0);
 }
 
 double vo_run2d(int id, double* planes, int nx, int ny, double dx, double cfl, double t_end, int max_steps,
                 double w, int lim, const double* prm, int bc, int subcycles, int* steps_out, double* dt_log) {
-    return run(id, planes, nx, ny, 2, dx, cfl, t_end, max_steps, w, lim, prm, bc, subcycles, steps_out, dt_log);
+    return run(id, planes, nx, ny, 2, dx, cfl, t_end, max_steps, w, lim, prm, bc, subcycles, steps_out, dt_log, 0);
+}
+
+double vo_run_reduced(double* planes, int nx, int ny, double dx, double cfl, double t_end, int max_steps, double w,
+                      int lim, const double* prm, int bc, int reinit_freq, int* steps_out) {
+    return run(VO_EULER_REDUCED, planes, nx, ny, ny > 1 ? 2 : 1, dx, cfl, t_end, max_steps, w, lim, prm, bc, 0,
+               steps_out, NULL, reinit_freq);
 }
 
 /* ------------------------------------------------------------------------- unit-test building blocks */

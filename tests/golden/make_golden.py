@@ -68,7 +68,35 @@ CASES = {
 }
 
 
+# The Euler reduced two-material model (model id O.EULER_REDUCED): run by oracle.run_reduced's reference arm.
+REDUCED_CASES = {
+    "reduced1d_toro100_superbee_30": (lambda: wl.reduced_shock_tube(100),
+                                      dict(dx=1 / 100, cfl=0.8, steps=30, limiter=O.SUPERBEE, reinit=0,
+                                           params=wl.reduced_params(1.4, 0.0, 1.4, 0.0))),
+    "reduced1d_twogamma120_minbee_reinit4_40": (lambda: wl.reduced_shock_tube(120, rho=(1.0, 0.1379), p=(2.0, 1.0)),
+                                                 dict(dx=1 / 120, cfl=0.8, steps=40, limiter=O.MINBEE, reinit=4,
+                                                      params=wl.reduced_params(1.4, 0.0, 1.67, 0.0))),
+    "reduced2d_bubble32_superbee_reinit3_9": (lambda: wl.reduced_bubble_2d(32),
+                                              dict(dx=1 / 32, cfl=0.8, steps=9, limiter=O.SUPERBEE, reinit=3,
+                                                   params=wl.reduced_params(1.4, 0.0, 1.67, 0.0))),
+}
+
+
+def make_reduced(name):
+    init, kw = REDUCED_CASES[name]
+    w0 = np.ascontiguousarray(init())
+    out = w0.copy()
+    kw = dict(kw)
+    O.run_reduced(out, kw.pop("dx"), kw.pop("cfl"), reference=True, **kw)
+    _, kw2 = REDUCED_CASES[name]
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), model=O.EULER_REDUCED, w0=w0, out=out,
+                        **{k: np.asarray(v) for k, v in kw2.items()})
+    print("wrote", name)
+
+
 def make(name):
+    if name in REDUCED_CASES:
+        return make_reduced(name)
     model, init, kw = CASES[name]
     w0 = np.ascontiguousarray(init())
     out = w0.copy()
@@ -81,5 +109,5 @@ def make(name):
 
 
 if __name__ == "__main__":
-    for n in (sys.argv[1:] or CASES):
+    for n in (sys.argv[1:] or list(CASES) + list(REDUCED_CASES)):
         make(n)

@@ -264,3 +264,39 @@ def batch_planes(ncell, theta):
         W[4, off:off + n] = np.where(left, theta[k, 2], theta[k, 5])
         off += n
     return W
+
+
+REDUCED_NVAR = 7  # alpha1, u, v, w, rho1, rho2, p (EulerReducedStateVector, Euler/Multiphysics/eulerreducedstatevector.cpp:30-41)
+
+
+def reduced_params(gamma1=1.4, p_inf1=0.0, gamma2=1.4, p_inf2=0.0):
+    """The two EulerMaterialParameters of the reduced model: (gamma1, p_inf1, gamma2, p_inf2)."""
+    return np.array([gamma1, p_inf1, gamma2, p_inf2])
+
+
+def reduced_shock_tube(n, rho=(1.0, 0.125), p=(1.0, 0.1), u=(0.0, 0.0)):
+    """EulerReducedTests::solveToroTest1's layout (Euler/Multiphysics/eulerreducedtests.cpp:7-26): material 1
+    (alpha1 = 0.999) at i <= n/2, material 2 (0.001) to the right, rho1 = rho[0] and rho2 = rho[1] everywhere."""
+    W = np.zeros((REDUCED_NVAR, n))
+    left = np.arange(n) <= 0.5 * n
+    W[0] = np.where(left, 0.999, 0.001)
+    W[1] = np.where(left, u[0], u[1])
+    W[4] = rho[0]
+    W[5] = rho[1]
+    W[6] = np.where(left, p[0], p[1])
+    return W
+
+
+def reduced_bubble_2d(nx, ny=None, rho=(1.0, 0.125), p=(1.0, 0.1), radius=0.2):
+    """EulerReducedTests::solve2DToroTest1's layout (:58-80): material 1 inside the disc of radius 0.2 n about the
+    grid centre (row index i, column j), material 2 outside."""
+    ny = nx if ny is None else ny
+    I, J = np.meshgrid(np.arange(ny), np.arange(nx), indexing="ij")
+    inside = np.sqrt((I - 0.5 * ny) ** 2 + (J - 0.5 * nx) ** 2) <= radius * nx
+    W = np.zeros((REDUCED_NVAR, ny, nx))
+    W[0] = np.where(inside, 0.999, 0.001)
+    W[4] = rho[0]
+    W[5] = rho[1]
+    W[6] = np.where(inside, p[0], p[1])
+    return W
+
