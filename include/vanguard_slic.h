@@ -12,6 +12,8 @@
  *   VG_MODEL_EULER (6 planes): rho, u, v, w, p, lambda           Euler/eulerstatevector.cpp:36-45
  *   VG_MODEL_MHD   (9 planes): rho, u, v, w, p, Bx, By, Bz, psi  MHD/mhdstatevector.cpp:35-47
  *   VG_MODEL_HPR  (17 planes): rho, p, A(9, row-major), u, v, w, Jx, Jy, Jz
+ *   VG_MODEL_EULER_REDUCED (7 planes): alpha1, u, v, w, rho1, rho2, p     the reduced two-material model,
+ *                                      Euler/Multiphysics/eulerreducedstatevector.cpp:30-41 (w must be 0)
  *                                                                HPR/hprstatevector.cpp:50-73
  * Ownership: a vg_solver owns all device memory it allocates; the caller owns every host buffer.
  * Threading: calls on different solvers are independent and re-entrant; one solver must not be used
@@ -37,7 +39,7 @@ typedef enum vg_status {
     VG_EUNSUPPORTED = 6  /* the input needs a variant this build does not provide (see below) */
 } vg_status;
 
-typedef enum vg_model { VG_MODEL_EULER = 0, VG_MODEL_MHD = 1, VG_MODEL_HPR = 2 } vg_model;
+typedef enum vg_model { VG_MODEL_EULER = 0, VG_MODEL_MHD = 1, VG_MODEL_HPR = 2, VG_MODEL_EULER_REDUCED = 3 } vg_model;
 
 /* VG_FP64: every operation in float64, in the reference's order, no FMA: matches the reference.
  * VG_MIXED: reconstruction, half-step evolution and FORCE flux in float32; pressure recovery, the CFL
@@ -58,6 +60,7 @@ enum { VG_SUPERBEE = 0, VG_VANLEER = 1, VG_MINBEE = 2 };
  *   Euler: {gamma, p_inf, c_v, E0, T_ign, rate}   EulerMaterialParameters (Euler/eulermaterialparameters.h)
  *   MHD:   {gamma, p_inf, c_h}                    MHDMaterialParameters; c_h is recomputed every step by
  *                                                 vg_run as solve() does, and read from here by vg_sweep
+ *   Euler reduced: {gamma1, p_inf1, gamma2, p_inf2}   the two EulerMaterialParameters of the materials
  *   HPR:   {gamma, p_inf, c_v, rho0, T0, c_s, alpha, tau1, tau2, T_ref, p_ref, is_thermal,
  *           eos, Gamma0, c0, s, alpha_eos, is_plastic, sigma0, n}
  *                                                 HPRMaterialParameters (HPR/hprmaterialparameters.cpp:34-69):
@@ -93,6 +96,9 @@ typedef struct vg_run_config {
                          * Euler on the eigenvalues of A^T A, heat flux by exponential sub-steps), stable at any tau;
                          * subcycles is then ignored.  Results approach the forcing's as its sub-cycles grow, not bit
                          * for bit. */
+    int reinit_frequency;  /* Euler reduced model: reinitialisationFrequency of SecondOrderSolver::solve{,2D}
+                            * (Solvers/secondordersolver.cpp:354-385): MultiphysicsSolvers::reinitialiseVolumeFraction
+                            * after every reinit_frequency-th step; 0: never */
 } vg_run_config;
 
 typedef struct vg_solver vg_solver;

@@ -171,10 +171,18 @@ def run(model, planes, dx, cfl, t_end=0.0, steps=0, bias=0.0, limiter=SUPERBEE, 
 def run_first_order(model, planes, dx, cfl, t_end=0.0, steps=0, params=None, bc=TRANSMISSIVE):
     """FirstOrderSolver::solve/solve2D's loop (and the MHD / HPR twins) in the C restatement, in place.
     Returns (t, steps)."""
-    _check(planes, NVAR[model])
     prm = _params(params)
     st = ctypes.c_int()
     nx, ny = (planes.shape[2], planes.shape[1]) if planes.ndim == 3 else (planes.shape[1], 1)
+    if model == EULER_REDUCED:  # the restatement carries an unused eighth plane
+        assert planes.shape[0] == 7 and planes.dtype == np.float64 and planes.flags.c_contiguous
+        padded = np.zeros((8,) + planes.shape[1:])
+        padded[:7] = planes
+        t = lib().vo_run_first_order(model, _ptr(padded), nx, ny, dx, cfl, t_end, steps, _ptr(prm), bc,
+                                     ctypes.byref(st))
+        planes[:] = padded[:7]
+        return t, st.value
+    _check(planes, NVAR[model])
     t = lib().vo_run_first_order(model, _ptr(planes), nx, ny, dx, cfl, t_end, steps, _ptr(prm), bc, ctypes.byref(st))
     return t, st.value
 
@@ -230,7 +238,7 @@ def hpr_cell(w, params, reference=False):
 
 
 def run_reduced(planes, dx, cfl, t_end=0.0, steps=0, bias=0.0, limiter=SUPERBEE, params=None, reinit=0,
-                reference=False, threads=1):
+                reference=False, threads=1, bc=TRANSMISSIVE):
     """SecondOrderSolver::solve{,2D} of the Euler reduced two-material model on its 7 primitive planes (alpha1, u, v,
     w, rho1, rho2, p) x (n) or (ny, nx), in place, from the restatement or (reference=True) the reference; params =
     (gamma1, p_inf1, gamma2, p_inf2); reinit > 0 reinitialises the volume fraction every `reinit` steps.  Returns
@@ -241,6 +249,7 @@ def run_reduced(planes, dx, cfl, t_end=0.0, steps=0, bias=0.0, limiter=SUPERBEE,
     prm = _params(params)
     st = ctypes.c_int()
     if reference:
+        assert bc == TRANSMISSIVE, "the reference's reduced model has transmissive boundaries only"
         R = ref()
         R.vgref_set_threads(threads)
         R.vgref_reduced_run.restype = _c_double
@@ -252,7 +261,7 @@ def run_reduced(planes, dx, cfl, t_end=0.0, steps=0, bias=0.0, limiter=SUPERBEE,
     L = lib()
     L.vo_run_reduced.restype = _c_double
     t = L.vo_run_reduced(_ptr(padded), nx, ny, _c_double(dx), _c_double(cfl), _c_double(t_end), steps,
-                         _c_double(bias), limiter, _ptr(prm), 0, reinit, ctypes.byref(st))
+                         _c_double(bias), limiter, _ptr(prm), bc, reinit, ctypes.byref(st))
     planes[:] = padded[:7]
     return t, st.value
 

@@ -16,11 +16,11 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libvanguard_slic.so")
 
 VG_OK, VG_EINVAL, VG_ENAN, VG_ETIMEOUT, VG_ECUDA, VG_ENOMEM, VG_EUNSUPPORTED = range(7)
-EULER, MHD, HPR = 0, 1, 2
+EULER, MHD, HPR, EULER_REDUCED = 0, 1, 2, 3
 FP64, MIXED = 0, 1
 TRANSMISSIVE, PERIODIC = 0, 1
 SUPERBEE, VANLEER, MINBEE = 0, 1, 2
-NVAR = {EULER: 6, MHD: 9, HPR: 17}
+NVAR = {EULER: 6, MHD: 9, HPR: 17, EULER_REDUCED: 7}
 MAX_PARAMS = 24
 
 
@@ -43,7 +43,8 @@ class GridDesc(ctypes.Structure):
 class RunConfig(ctypes.Structure):
     _fields_ = [("dx", ctypes.c_double), ("cfl", ctypes.c_double), ("t_end", ctypes.c_double),
                 ("max_steps", ctypes.c_int), ("bias", ctypes.c_double), ("limiter", ctypes.c_int),
-                ("subcycles", ctypes.c_int), ("order", ctypes.c_int), ("stiff_source", ctypes.c_int)]
+                ("subcycles", ctypes.c_int), ("order", ctypes.c_int), ("stiff_source", ctypes.c_int),
+                ("reinit_frequency", ctypes.c_int)]
 
 
 # Every function the C ABI header declares (tests check the library exports them all).
@@ -173,10 +174,10 @@ class Solver:
         return a
 
     def run(self, dx, cfl, t_end=0.0, steps=0, bias=0.0, limiter=SUPERBEE, subcycles=0, stream=None,
-            allow_nan=False, order=2, stiff=False):
+            allow_nan=False, order=2, stiff=False, reinit=0):
         """The solve() time loop on the device; order=1 runs FirstOrderSolver's FORCE loop instead; stiff=True
         (HPR) relaxes the source over dt/2 before and after the sweeps instead of the RK4 forcing sub-cycles."""
-        c = RunConfig(dx, cfl, t_end, steps, bias, limiter, subcycles, order, 1 if stiff else 0)
+        c = RunConfig(dx, cfl, t_end, steps, bias, limiter, subcycles, order, 1 if stiff else 0, reinit)
         it = ctypes.c_int()
         t = ctypes.c_double()
         _check(lib().vg_run(self._h, ctypes.byref(c), ctypes.byref(it), ctypes.byref(t), stream),

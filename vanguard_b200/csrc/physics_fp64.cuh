@@ -228,4 +228,100 @@ struct MHDF64 {
     __device__ static double pressure(const double* W) { return W[IP]; }
 };
 
+// ------------------------------------------------------------------------------- Euler reduced two-material
+// EulerReducedStateVector (Euler/Multiphysics/eulerreducedstatevector.cpp) with w == 0 (the host checks it; every w
+// term is an exact additive zero):
+// W = (alpha1, u, v, rho1, rho2, p), U = (rho, rho alpha1, rho u, rho v, alpha1 rho1, alpha2 rho2, rho E).
+// Params: {gamma1, p_inf1, gamma2, p_inf2}.  Every volume fraction the model derives or uses is clamped to
+// [0.001, 0.999] (:47-58, :99-108, :131-147).
+struct EulerReducedF64 {
+    static constexpr int NW = 6;
+    static constexpr int NU = 7;
+    static constexpr bool HAS_Y = true;
+    static constexpr bool HAS_SOURCE = false;
+    struct P {
+        double g1, pinf1, g2, pinf2, ch2;
+    };
+    __device__ static P params(const double* prm, double /*ch*/) { return P{prm[0], prm[1], prm[2], prm[3], 0.0}; }
+
+    __device__ static double clamp_alpha(double a) {
+        if (a < 0.001) return 0.001;
+        if (a > 0.999) return 0.999;
+        return a;
+    }
+    // EulerEquationOfState::computeSpecificInternalEnergy / computePressure / computeSoundSpeed
+    // (Euler/eulerequationofstate.cpp:7-29) of material (g, pinf)
+    __device__ static double e_of(double rho, double p, double g, double pinf) { return (p + (g * pinf)) / ((g - 1) * rho); }
+    __device__ static double p_of(double rho, double e, double g, double pinf) { return ((e * (g - 1)) * rho) - (g * pinf); }
+    __device__ static double c_of(double rho, double p, double g, double pinf) { return sqrt((g * (p + pinf)) / rho); }
+
+    // EulerReducedStateVector::computeConservedVariableVector (:96-129)
+    __device__ static void cons(const double* W, const P& q, double* U) {
+        const double a1 = clamp_alpha(W[0]), a2 = 1.0 - a1;
+        const double u = W[1], v = W[2], r1 = W[3], r2 = W[4], p = W[5];
+        const double rho = (a1 * r1) + (a2 * r2);
+        U[0] = rho;
+        U[1] = rho * a1;
+        U[2] = rho * u;
+        U[3] = rho * v;
+        U[4] = a1 * r1;
+        U[5] = a2 * r2;
+        const double v2 = (u * u) + (v * v);
+        const double E1 = e_of(rho, p, q.g1, q.pinf1) + (0.5 * v2), E2 = e_of(rho, p, q.g2, q.pinf2) + (0.5 * v2);
+        U[6] = rho * ((a1 * E1) + (a2 * E2));
+    }
+    // EulerReducedStateVector::setConservedVariableVector (:43-73)
+    __device__ static void setcons(const double* U, const P& q, double* W) {
+        const double rho = U[0];
+        const double a1 = clamp_alpha(U[1] / rho), a2 = 1.0 - a1;
+        const double u = U[2] / rho, v = U[3] / rho;
+        const double e = (U[6] / rho) - (0.5 * ((u * u) + (v * v)));
+        W[0] = a1;
+        W[1] = u;
+        W[2] = v;
+        W[3] = U[4] / a1;
+        W[4] = U[5] / a2;
+        W[5] = (a1 * p_of(rho, e, q.g1, q.pinf1)) + (a2 * p_of(rho, e, q.g2, q.pinf2));
+    }
+    // EulerReducedStateVector::compute{X,Y}FluxVector(vector, params, params) (:131-180, :187-236)
+    template <int AXIS>
+    __device__ static void flux(const double* U, const P& q, double* F) {
+        const double rho = U[0];
+        const double a1 = clamp_alpha(U[1] / rho), a2 = 1.0 - a1;
+        const double u = U[2] / rho, v = U[3] / rho;
+        const double r1 = U[4] / a1, r2 = U[5] / a2;
+        const double E = U[6] / rho;
+        const double e = E - (0.5 * ((u * u) + (v * v)));
+        const double p = (a1 * p_of(rho, e, q.g1, q.pinf1)) + (a2 * p_of(rho, e, q.g2, q.pinf2));
+        const double un = AXIS == 0 ? u : v;
+        F[0] = rho * un;
+        F[1] = rho * (un * a1);
+        F[2] = rho * (un * u);
+        F[3] = rho * (un * v);
+        if constexpr (AXIS == 0) F[2] = F[2] + p;
+        else F[3] = F[3] + p;
+        F[4] = a1 * (r1 * un);
+        F[5] = a2 * (r2 * un);
+        F[6] = (rho * (un * E)) + (un * p);
+    }
+    // Solvers::computeMaximumWaveSpeed{,2D} of the reduced model (Solvers/solvers.cpp:298-316, :365-387)
+    __device__ static double wave(const double* W, const P& q, int dims) {
+        const double c = std_max(c_of(W[3], W[5], q.g1, q.pinf1), c_of(W[4], W[5], q.g2, q.pinf2));
+        if (dims == 1) return fabs(W[1]) + c;
+        return std_max(fabs(W[1]), fabs(W[2])) + c;
+    }
+    // EulerReducedStateVector() (:3-14)
+    __device__ static void default_state(double* W) {
+        W[0] = 0.999;
+        W[1] = 0.0;
+        W[2] = 0.0;
+        W[3] = 1.0;
+        W[4] = 1.0;
+        W[5] = 1.0;
+    }
+    // the smaller material density (bad-state check: both must stay positive) and the interface pressure
+    __device__ static double density(const double* W) { return W[3] < W[4] ? W[3] : W[4]; }
+    __device__ static double pressure(const double* W) { return W[5]; }
+};
+
 }  // namespace vg

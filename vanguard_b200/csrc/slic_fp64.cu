@@ -7,8 +7,11 @@
 #include "physics_fp64.cuh"
 #include "physics_hpr.cuh"
 #include "slic_kernels.cuh"
+#include "reduced_kernels.cuh"
 #include "sweep_table.cuh"
 #include "vg_ops.h"
+
+#include <type_traits>
 
 namespace vg {
 namespace {
@@ -107,7 +110,9 @@ constexpr Ops make_ops() {
                tile_kind<M>(),
                &force1_x<M>,
                &force1_y<M>,
-               relax_of<M>()};
+               relax_of<M>(),
+               0,
+               std::is_same<M, EulerReducedF64>::value ? &reduced_reinit_fp64 : nullptr};
 }
 
 const Ops kOps[V_COUNT] = {
@@ -117,6 +122,7 @@ const Ops kOps[V_COUNT] = {
     make_ops<MHDF64<true>>(),
     make_ops<HPRF64>(),
     make_ops<HPRSolidF64>(),
+    make_ops<EulerReducedF64>(),
 };
 
 }  // namespace
@@ -131,6 +137,7 @@ cudaError_t hpr_solid_forcing_fp64(const SweepArgs& a, int subcycles, cudaStream
     return forcing_impl<HPRSolidF64>(a, subcycles, st);
 }
 cudaError_t hpr_solid_relax_fp64(const SweepArgs& a, cudaStream_t st) { return relax_impl<HPRSolidF64>(a, st); }
+cudaError_t reduced_reinit_fp64(const SweepArgs& a, cudaStream_t st) { return reduced_reinit(a, st); }
 cudaError_t mhd7_forcing_fp64(const SweepArgs& a, int subcycles, cudaStream_t st) {
     return forcing_impl<MHDF64<false>>(a, subcycles, st);
 }

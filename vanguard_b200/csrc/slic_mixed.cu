@@ -86,10 +86,10 @@ using ForcingFn = cudaError_t (*)(const SweepArgs&, int, cudaStream_t);
 
 // The source sub-cycles keep FP64: the exact forcing kernels of each model
 template <class M>
-constexpr Ops make_ops(ForcingFn forcing = nullptr, SweepFn relax = nullptr) {
+constexpr Ops make_ops(ForcingFn forcing = nullptr, SweepFn relax = nullptr, SweepFn reinit = nullptr) {
     return Ops{M::NW, SweepTable<MixedKernels, M>::x, SweepTable<MixedKernels, M>::y, &max_wave_impl<M>,
                &step_begin_impl<M>, &finish_impl<M>, forcing, tile_kind<M>(), &force1_x<M>, &force1_y<M>, relax,
-               tile_kind<M>() == 2 ? M::NW : 0};
+               tile_kind<M>() == 2 ? M::NW : 0, reinit};
 }
 
 const Ops kOps[V_COUNT] = {
@@ -99,6 +99,7 @@ const Ops kOps[V_COUNT] = {
     make_ops<MHDMixed<true>>(&mhd9_forcing_fp64),
     make_ops<HPRMixed>(&hpr_forcing_fp64, &hpr_relax_fp64),
     make_ops<HPRSolidMixed>(&hpr_solid_forcing_fp64, &hpr_solid_relax_fp64),
+    make_ops<ReducedMixed>(nullptr, nullptr, &reduced_reinit_fp64),
 };
 
 }  // namespace

@@ -112,6 +112,17 @@ __device__ __forceinline__ MixedConst mixed_const(const SweepArgs& a, double& ts
     return k;
 }
 
+// Models whose evolved states must pass through the stored primitive form, as the reference's do, declare
+// ROUNDTRIP_EVOLVED (for the others that trip only rounds, and the mixed form skips it).
+template <class M, class = void>
+struct roundtrip_evolved {
+    static constexpr bool value = false;
+};
+template <class M>
+struct roundtrip_evolved<M, decltype((void)M::ROUNDTRIP_EVOLVED)> {
+    static constexpr bool value = M::ROUNDTRIP_EVOLVED;
+};
+
 // Both evolved edge states of one cell (type M::R), from the FP64 conserved vectors of the cell and its
 // neighbours; the slope differences are formed in FP64.  ua_left_side: x_L + dt/2 evolution; ua_right_side:
 // x_R + dt/2 evolution.
@@ -137,6 +148,15 @@ __device__ __forceinline__ void evolve_edges_mixed(const double* uL, const doubl
         R ev = (R)(k.half_r * (fl[i] - fr[i]));
         ua_left_side[i] = xl[i] + ev;
         ua_right_side[i] = xr[i] + ev;
+    }
+    if constexpr (roundtrip_evolved<M>::value) {
+        // the reference stores each evolved state in a state vector (Solvers/solvers.cpp:584-599): for models where
+        // that is a projection (the reduced model's clamped volume fraction and mixture density), do the same
+        double w[M::NW];
+        M::setcons(ua_left_side, q, w);
+        M::cons(w, q, ua_left_side);
+        M::setcons(ua_right_side, q, w);
+        M::cons(w, q, ua_right_side);
     }
 }
 

@@ -40,7 +40,9 @@ vg_status cuda_fail(cudaError_t e, const char* what) {
         if (e_ != cudaSuccess) return cuda_fail(e_, #call);  \
     } while (0)
 
-int ref_nvar(int model) { return model == VG_MODEL_EULER ? 6 : model == VG_MODEL_MHD ? 9 : model == VG_MODEL_HPR ? 17 : 0; }
+int ref_nvar(int model) {
+    return model == VG_MODEL_EULER ? 6 : model == VG_MODEL_MHD ? 9 : model == VG_MODEL_HPR ? 17 : model == VG_MODEL_EULER_REDUCED ? 7 : 0;
+}
 
 // Reference plane carried in device plane k, per variant.
 const int kPlanes[vg::V_COUNT][17] = {
@@ -50,6 +52,7 @@ const int kPlanes[vg::V_COUNT][17] = {
     {0, 1, 2, 3, 4, 5, 6, 7, 8},    // V_MHD9
     {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16},  // V_HPR17
     {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16},  // V_HPR17S
+    {0, 1, 2, 4, 5, 6},             // V_RED6: alpha1, u, v, rho1, rho2, p
 };
 
 }  // namespace
@@ -249,6 +252,8 @@ int enqueue_step(vg_solver* s, const vg_run_config& c, int from, cudaStream_t st
     cudaError_t e = s->ops->step_begin(a, st);
     n++;
     const bool stiff = !first && c.stiff_source && s->ops->relax;
+    const bool reinit = c.reinit_frequency > 0 && s->ops->reinit;
+    a.reinit_freq = c.reinit_frequency;
     const int sub = (!first && !stiff && s->ops->forcing && c.subcycles > 0) ? c.subcycles : 0;
     from = enqueue_forcing(s, a, sub, from, st, &e, &n);
     // stiff source: relaxation over dt/2 in place before and after the sweeps
@@ -262,7 +267,7 @@ int enqueue_step(vg_solver* s, const vg_run_config& c, int from, cudaStream_t st
     if (stiff) relax();
     // Without a trailing source pass the last sweep folds the next step's CFL maximum into its epilogue;
     // with one, a separate reduction runs after it.
-    const int fuse_wave = sub == 0 && !stiff;
+    const int fuse_wave = sub == 0 && !stiff && !reinit;
     if (s->dims == 1) {
         a.in = s->buf[from];
         a.out = s->buf[1 - from];
@@ -295,6 +300,12 @@ int enqueue_step(vg_solver* s, const vg_run_config& c, int from, cudaStream_t st
     a.advance_time = 0;
     from = enqueue_forcing(s, a, sub, from, st, &e, &n);
     if (stiff) relax();
+    if (reinit) {  // in place on the step's result, before the next step's CFL maximum reads it
+        SweepArgs r = a;
+        r.in = r.out = s->buf[from];
+        if (e == cudaSuccess) e = s->ops->reinit(r, st);
+        n += s->dims == 1 ? 1 : 2;
+    }
     if (!fuse_wave) {
         a.in = s->buf[from];
         if (e == cudaSuccess) e = s->ops->max_wave(a, st);
@@ -304,8 +315,9 @@ int enqueue_step(vg_solver* s, const vg_run_config& c, int from, cudaStream_t st
     return n;
 }
 
-int kernels_per_step(const vg_solver* s, int sub, bool stiff = false) {
+int kernels_per_step(const vg_solver* s, int sub, bool stiff = false, bool reinit = false) {
     int n = s->dims == 1 ? 2 : 4;
+    if (reinit) return n + (s->dims == 1 ? 1 : 2) + 1;  // the reinitialisation and the separate CFL maximum
     if (stiff) return n + 3;  // two relaxations and the separate CFL maximum
     if (s->ops->forcing && sub > 0) n += 2 * sub * vg::kForcingLaunches + 1;
     return n;
@@ -343,7 +355,8 @@ int order_of(const vg_run_config& c) { return c.order == 1 ? 1 : 2; }
 
 bool same_cfg(const vg_run_config& a, const vg_run_config& b) {
     return a.dx == b.dx && a.bias == b.bias && a.limiter == b.limiter && a.subcycles == b.subcycles &&
-           order_of(a) == order_of(b) && (a.stiff_source != 0) == (b.stiff_source != 0);
+           order_of(a) == order_of(b) && (a.stiff_source != 0) == (b.stiff_source != 0) &&
+           a.reinit_frequency == b.reinit_frequency;
 }
 
 vg_status ensure_graphs(vg_solver* s, const vg_run_config& c) {
@@ -383,7 +396,8 @@ const char* vg_status_string(vg_status st) {
 vg_status vg_create(const vg_grid_desc* desc, vg_solver** out) {
     if (!desc || !out) return fail(VG_EINVAL, "null argument");
     *out = nullptr;
-    if (desc->model != VG_MODEL_EULER && desc->model != VG_MODEL_MHD && desc->model != VG_MODEL_HPR)
+    if (desc->model != VG_MODEL_EULER && desc->model != VG_MODEL_MHD && desc->model != VG_MODEL_HPR &&
+        desc->model != VG_MODEL_EULER_REDUCED)
         return fail(VG_EUNSUPPORTED, "model not available in this build");
     if (desc->nx < 2 || desc->ny < 1 || (desc->ny > 1 && desc->ny < 2))
         return fail(VG_EINVAL, "grid needs at least 2 cells along every swept axis");
@@ -402,7 +416,7 @@ vg_status vg_create(const vg_grid_desc* desc, vg_solver** out) {
     if (!s) return fail(VG_ENOMEM, "host allocation");
     s->d = *desc;
     s->dims = desc->ny > 1 ? 2 : 1;
-    s->max_nw = desc->model == VG_MODEL_EULER ? 4 : desc->model == VG_MODEL_MHD ? 9 : 17;
+    s->max_nw = desc->model == VG_MODEL_EULER ? 4 : desc->model == VG_MODEL_MHD ? 9 : desc->model == VG_MODEL_EULER_REDUCED ? 6 : 17;
     s->pitch = ((long)desc->nx + 31) / 32 * 32;  // 256-byte aligned rows
     s->plane = s->pitch * desc->ny;
     s->floor5 = std::pow(10.0, -5.0);  // SlopeLimiters::computeSlopeVector's floor (Solvers/slopelimiters.cpp:232-239)
@@ -459,6 +473,14 @@ vg_status vg_upload_primitive(vg_solver* s, const double* planes, int is_device,
             }
             variant = (s->dims == 1 && zero_v) ? vg::V_EULER1 : vg::V_EULER2;
         }
+    } else if (s->d.model == VG_MODEL_EULER_REDUCED) {
+        // the reduced model carries alpha1, u, v, rho1, rho2, p: w must be 0
+        if (!is_device) {
+            const double* w = planes + 3 * n;
+            for (long i = 0; i < n; i++)
+                if (w[i] != 0.0) return fail(VG_EUNSUPPORTED, "reduced two-material state with w != 0");
+        }
+        variant = vg::V_RED6;
     } else if (s->d.model == VG_MODEL_HPR) {
         // a solid equation of state or plasticity selects the instantiation that carries them
         variant = (s->d.params[12] != 0.0 || s->d.params[17] != 0.0) ? vg::V_HPR17S : vg::V_HPR17;
@@ -531,6 +553,10 @@ vg_status vg_run(vg_solver* s, const vg_run_config* cfg, int* steps_taken, doubl
     if (cfg->order == 1 && !s->ops->x1) return fail(VG_EUNSUPPORTED, "this kernel form has no first-order loop");
     if (cfg->stiff_source && cfg->order != 1 && !s->ops->relax)
         return fail(VG_EUNSUPPORTED, "the stiff source relaxation exists for the HPR model only");
+    if (cfg->reinit_frequency < 0) return fail(VG_EINVAL, "reinit_frequency must be >= 0");
+    if (cfg->reinit_frequency > 0 && (!s->ops->reinit || cfg->order == 1))
+        return fail(VG_EUNSUPPORTED, "volume-fraction reinitialisation belongs to the reduced two-material model's "
+                                     "second-order loop");
     if (cfg->stiff_source && cfg->order != 1 && s->d.params[17] != 0.0)
         return fail(VG_EUNSUPPORTED, "the stiff source relaxation integrates the elastic strain relaxation only; plastic "
                                      "materials run the RK4 source sub-cycles");
@@ -585,7 +611,8 @@ vg_status vg_run(vg_solver* s, const vg_run_config* cfg, int* steps_taken, doubl
         }
     }
     const bool stiff = cfg->order != 1 && cfg->stiff_source && s->ops->relax;
-    launches += launched_steps * kernels_per_step(s, cfg->order == 1 || stiff ? 0 : cfg->subcycles, stiff);
+    launches += launched_steps * kernels_per_step(s, cfg->order == 1 || stiff ? 0 : cfg->subcycles, stiff,
+                                                  cfg->order != 1 && cfg->reinit_frequency > 0 && s->ops->reinit);
     // every step is an odd number of sweeps in 2D (3) and 1 in 1D: the state ends in buffer (steps & 1)
     s->cur = (int)(launched_steps & 1);
     VG_CUDA(cudaMemcpyAsync(h, s->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));

@@ -95,6 +95,7 @@ struct SweepArgs {
     // device CUtensorMap over `in` for the TMA-staged X sweep (null: none); kept last, since a field ahead of
     // params[] changed the register allocation of the two-row X sweep (56 -> 60)
     const void* tmap;
+    int reinit_freq;  // volume-fraction reinitialisation every reinit_freq steps (Euler reduced model; 0: none)
 };
 
 // Sweep constants of one sweep of length ts = dt * scale, formed as the reference forms them

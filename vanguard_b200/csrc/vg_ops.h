@@ -18,7 +18,8 @@ enum Variant : int {
     V_MHD9 = 3,    // MHD, all components:                 rho, u, v, w, p, Bx, By, Bz, psi
     V_HPR17 = 4,   // HPR, all 17 components:              rho, p, A(9), u, v, w, Jx, Jy, Jz
     V_HPR17S = 5,  // HPR solid (ShockMieGruneisen / GodunovRomenski) or plastic material, same planes
-    V_COUNT = 6
+    V_RED6 = 6,    // Euler reduced two-material, w == 0:    alpha1, u, v, rho1, rho2, p
+    V_COUNT = 7
 };
 
 struct Ops {
@@ -43,6 +44,8 @@ struct Ops {
     SweepFn relax = nullptr;
     // Planes of the box of the TMA-staged X sweep (its tensor maps: box {130, 2, tma_planes}); 0: no TMA sweep.
     int tma_planes = 0;
+    // Volume-fraction reinitialisation of one step, in place on a.out (Euler reduced model), null for the others.
+    SweepFn reinit = nullptr;
 };
 
 constexpr int kForcingLaunches = 2;  // kernels per forcing sub-cycle
@@ -59,6 +62,8 @@ cudaError_t mhd9_forcing_fp64(const SweepArgs& a, int subcycles, cudaStream_t st
 cudaError_t hpr_relax_fp64(const SweepArgs& a, cudaStream_t st);
 cudaError_t hpr_solid_forcing_fp64(const SweepArgs& a, int subcycles, cudaStream_t st);
 cudaError_t hpr_solid_relax_fp64(const SweepArgs& a, cudaStream_t st);
+// The reduced model's volume-fraction reinitialisation (slic_fp64.cu), shared by both forms.
+cudaError_t reduced_reinit_fp64(const SweepArgs& a, cudaStream_t st);
 
 // Record the text returned by vg_last_error_string() on this thread.
 void set_last_error(const std::string& msg);
