@@ -4,7 +4,8 @@
 //   shim_driver <out.bin>
 // Output, in order (float64): Euler 1D solve (6 x 200), Euler 2D per-sweep loop (6 x 24 x 20),
 // MHD solve2D (9 x 16 x 16), HPR solve (17 x 50), Euler 1D step-count solve (6 x 150), Euler 1D first-order solve
-// (6 x 150), HPR GodunovRomenski plastic solve (17 x 60), then the number of 2D steps the per-sweep loop took.
+// (6 x 150), HPR GodunovRomenski plastic solve (17 x 60), reduced two-material solve (7 x 120), then the number of 2D
+// steps the per-sweep loop took.
 #include <cmath>
 #include <cstdio>
 #include <vector>
@@ -139,6 +140,22 @@ int main(int argc, char** argv) {
         vector<double> v;
         for (int k = 0; k < 17; k++)
             for (auto& c : out) v.push_back(c.data()[k]);
+        put(f, v);
+    }
+    // 8) SecondOrderSolver::solve of the reduced two-material model (EulerReducedTests::solveToroTest1's layout),
+    //    gamma 1.4 | 1.67, reinitialisation every 5 steps, to t = 0.05
+    {
+        int n = 120;
+        vector<EulerReducedStateVector> cells(n);
+        for (int i = 0; i < n; i++)
+            cells[i] = i <= 0.5 * n ? EulerReducedStateVector(0.999, 0.0, 0.0, 0.0, 1.0, 0.125, 1.0)
+                                    : EulerReducedStateVector(0.001, 0.0, 0.0, 0.0, 1.0, 0.125, 0.1);
+        vector<EulerReducedStateVector> out = SecondOrderSolver::solve(cells, 1.0 / n, 0.8, 0.05, 0.0, 0, 0, 5,
+                                                                       EulerMaterialParameters(1.4),
+                                                                       EulerMaterialParameters(1.67));
+        vector<double> v;
+        for (int k = 0; k < 7; k++)
+            for (auto& c : out) v.push_back(c.computePrimitiveVariableVector()[k]);
         put(f, v);
     }
     double st = steps;

@@ -97,5 +97,11 @@ def test_shim_driver_matches_oracle(gpu, oracle_lib, tmp_path):
     d = np.abs(got - ref).max(axis=1) / np.maximum(np.abs(ref).max(axis=1), 1e-300)
     assert np.isfinite(got).all() and d.max() <= 1e-10
 
+    # 8) SecondOrderSolver::solve of the reduced two-material model, reinitialisation every 5 steps, t = 0.05
+    got = take((7, 120))
+    ref = wl.reduced_shock_tube(120)
+    O.run_reduced(ref, 1 / 120, 0.8, t_end=0.05, limiter=0, params=wl.reduced_params(1.4, 0.0, 1.67, 0.0), reinit=5)
+    assert np.array_equal(got, ref)
+
     assert take((1,))[0] == 6
     assert off == data.size

@@ -70,8 +70,9 @@ vg_solver* cached_solver(int model, int nx, int ny, int boundary, const double* 
 // Runs solve()/solve2D()'s time loop (finalTime-driven) on reference-order primitive planes, in place.
 // maxSteps > 0 also stops the loop after that many steps (the shim's step-count overloads).
 void run_planes(int model, std::vector<double>& planes, int nx, int ny, const double* params, int nparams, double dx,
-                double cfl, double tEnd, double bias, int limiter, int subcycles, int maxSteps = 0, int order = 2) {
-    // the first-order loop exists in the plain FP64 form only
+                double cfl, double tEnd, double bias, int limiter, int subcycles, int maxSteps = 0, int order = 2,
+                int reinit = 0) {
+    // the first-order loop runs in the exact form, bit for bit with the reference
     SolverPtr s = make_solver(model, nx, ny, VG_TRANSMISSIVE, params, nparams, order == 1 ? VG_FP64 : -1);
     vg_run_config c{};
     c.dx = dx;
@@ -82,6 +83,7 @@ void run_planes(int model, std::vector<double>& planes, int nx, int ny, const do
     c.limiter = limiter;
     c.subcycles = subcycles;
     c.order = order;
+    c.reinit_frequency = reinit;
     vg_status st = vg_solve(s.get(), planes.data(), planes.data(), &c, nullptr, nullptr, nullptr);
     if (st != VG_OK && st != VG_ENAN) raise(st, "vg_solve");  // non-finite results are returned, as the reference does
 }
@@ -122,6 +124,13 @@ void mhd_get(const MHDStateVector& c, double* w) {
 }
 MHDStateVector mhd_make(const double* w) { return MHDStateVector(w[0], w[1], w[2], w[3], w[4], w[5], w[6], w[7], w[8]); }
 void hpr_get(const HPRStateVector& c, double* w) { std::memcpy(w, c.data(), sizeof(double) * 17); }
+void reduced_get(const EulerReducedStateVector& c, double* w) { std::memcpy(w, c.data(), sizeof(double) * 7); }
+EulerReducedStateVector reduced_make(const double* w) {
+    EulerReducedStateVector s;
+    std::memcpy(s.data(), w, sizeof(double) * 7);
+    return s;
+}
+
 HPRStateVector hpr_make(const double* w) {
     HPRStateVector s;
     std::memcpy(s.data(), w, sizeof(double) * 17);
@@ -523,6 +532,57 @@ vector<vector<EulerStateVector> > SecondOrderSolver::solve2D(vector<vector<Euler
     long ny = initialCells.size(), nx = initialCells[0].size();
     run_planes(VG_MODEL_EULER, p, (int)nx, (int)ny, prm, 6, dx, cfl, tEnd, bias, limiter, 0, maxSteps);
     return unpack2<EulerStateVector>(p, nx, ny, 6, euler_make);
+}
+
+// ----------------------------------------------------------------------------------- reduced two-material
+EulerReducedStateVector::EulerReducedStateVector() : EulerReducedStateVector(0.999, 0.0, 0.0, 0.0, 1.0, 1.0, 1.0) {}
+EulerReducedStateVector::EulerReducedStateVector(double a1, double u, double v, double w, double r1, double r2, double p)
+    : w_{a1, u, v, w, r1, r2, p} {}
+void EulerReducedStateVector::setPrimitiveVariableVector(vector<double> w) {
+    for (int i = 0; i < 7; i++) w_[i] = w[i];
+}
+vector<double> EulerReducedStateVector::computePrimitiveVariableVector() const { return vector<double>(w_, w_ + 7); }
+
+namespace {
+void reduced_params(const EulerMaterialParameters& m1, const EulerMaterialParameters& m2, double* prm) {
+    prm[0] = m1.getAdiabaticIndex(), prm[1] = m1.getStiffeningParameter();
+    prm[2] = m2.getAdiabaticIndex(), prm[3] = m2.getStiffeningParameter();
+}
+}  // namespace
+
+vector<EulerReducedStateVector> SecondOrderSolver::solve(vector<EulerReducedStateVector>& initialCells, double dx, double cfl,
+                                                         double tEnd, double bias, int limiter, int subcycles, int reinit,
+                                                         EulerMaterialParameters m1, EulerMaterialParameters m2) {
+    return solve(initialCells, dx, cfl, tEnd, bias, limiter, subcycles, reinit, m1, m2, 0);
+}
+vector<EulerReducedStateVector> SecondOrderSolver::solve(vector<EulerReducedStateVector>& initialCells, double dx, double cfl,
+                                                         double tEnd, double bias, int limiter,
+                                                         int /*subcycles: the reference's loop body is empty*/, int reinit,
+                                                         EulerMaterialParameters m1, EulerMaterialParameters m2,
+                                                         int maxSteps) {
+    double prm[4];
+    reduced_params(m1, m2, prm);
+    std::vector<double> p = pack(initialCells, 7, reduced_get);
+    run_planes(VG_MODEL_EULER_REDUCED, p, (int)initialCells.size(), 1, prm, 4, dx, cfl, tEnd, bias, limiter, 0, maxSteps,
+               2, reinit);
+    return unpack<EulerReducedStateVector>(p, initialCells.size(), 7, reduced_make);
+}
+vector<vector<EulerReducedStateVector> > SecondOrderSolver::solve2D(vector<vector<EulerReducedStateVector> >& initialCells,
+                                                                    double dx, double cfl, double tEnd, double bias,
+                                                                    int limiter, int subcycles, int reinit,
+                                                                    EulerMaterialParameters m1, EulerMaterialParameters m2) {
+    return solve2D(initialCells, dx, cfl, tEnd, bias, limiter, subcycles, reinit, m1, m2, 0);
+}
+vector<vector<EulerReducedStateVector> > SecondOrderSolver::solve2D(vector<vector<EulerReducedStateVector> >& initialCells,
+                                                                    double dx, double cfl, double tEnd, double bias,
+                                                                    int limiter, int, int reinit, EulerMaterialParameters m1,
+                                                                    EulerMaterialParameters m2, int maxSteps) {
+    double prm[4];
+    reduced_params(m1, m2, prm);
+    std::vector<double> p = pack2(initialCells, 7, reduced_get);
+    long ny = initialCells.size(), nx = initialCells[0].size();
+    run_planes(VG_MODEL_EULER_REDUCED, p, (int)nx, (int)ny, prm, 4, dx, cfl, tEnd, bias, limiter, 0, maxSteps, 2, reinit);
+    return unpack2<EulerReducedStateVector>(p, nx, ny, 7, reduced_make);
 }
 
 // --------------------------------------------------------------------------------------------- MHD solver

@@ -85,6 +85,37 @@ private:
 };
 
 // --------------------------------------------------------------------------------------------------- MHD
+// EulerReducedStateVector (Euler/Multiphysics/eulerreducedstatevector.h): the reduced two-material state,
+// primitives alpha1, u, v, w, rho1, rho2, p.
+class EulerReducedStateVector {
+public:
+    EulerReducedStateVector();
+    EulerReducedStateVector(double newMaterial1VolumeFraction, double newInterfaceXVelocity, double newInterfaceYVelocity,
+                            double newInterfaceZVelocity, double newMaterial1Density, double newMaterial2Density,
+                            double newInterfacePressure);
+    void setPrimitiveVariableVector(vector<double> w);
+    vector<double> computePrimitiveVariableVector() const;
+    double getMaterial1VolumeFraction() const { return w_[0]; }
+    double getInterfaceXVelocity() const { return w_[1]; }
+    double getInterfaceYVelocity() const { return w_[2]; }
+    double getInterfaceZVelocity() const { return w_[3]; }
+    double getMaterial1Density() const { return w_[4]; }
+    double getMaterial2Density() const { return w_[5]; }
+    double getInterfacePressure() const { return w_[6]; }
+    void setMaterial1VolumeFraction(double v) { w_[0] = v; }
+    void setInterfaceXVelocity(double v) { w_[1] = v; }
+    void setInterfaceYVelocity(double v) { w_[2] = v; }
+    void setInterfaceZVelocity(double v) { w_[3] = v; }
+    void setMaterial1Density(double v) { w_[4] = v; }
+    void setMaterial2Density(double v) { w_[5] = v; }
+    void setInterfacePressure(double v) { w_[6] = v; }
+    double* data() { return w_; }
+    const double* data() const { return w_; }
+
+private:
+    double w_[7];
+};
+
 class MHDMaterialParameters {
 public:
     MHDMaterialParameters();
@@ -264,7 +295,31 @@ public:
     static vector<vector<EulerStateVector> > solve2D(vector<vector<EulerStateVector> >& initialCells, double cellSpacing,
                                                      double CFLCofficient, double finalTime, double bias, int slopeLimiter,
                                                      int subcyclingIterations, EulerMaterialParameters mp);
+    // the reduced two-material model (Solvers/secondordersolver.cpp:354-385, :470-...): reinitialisationFrequency > 0
+    // reinitialises the volume fraction every that many steps
+    static vector<EulerReducedStateVector> solve(vector<EulerReducedStateVector>& initialCells, double cellSpacing,
+                                                 double CFLCoefficient, double finalTime, double bias, int slopeLimiter,
+                                                 int subcyclingIterations, int reinitialisationFrequency,
+                                                 EulerMaterialParameters material1Parameters,
+                                                 EulerMaterialParameters material2Parameters);
+    static vector<vector<EulerReducedStateVector> > solve2D(vector<vector<EulerReducedStateVector> >& initialCells,
+                                                            double cellSpacing, double CFLCoefficient, double finalTime,
+                                                            double bias, int slopeLimiter, int subcyclingIterations,
+                                                            int reinitialisationFrequency,
+                                                            EulerMaterialParameters material1Parameters,
+                                                            EulerMaterialParameters material2Parameters);
     // step-count overloads (not in the reference): also stop after maxSteps steps when maxSteps > 0
+    static vector<EulerReducedStateVector> solve(vector<EulerReducedStateVector>& initialCells, double cellSpacing,
+                                                 double CFLCoefficient, double finalTime, double bias, int slopeLimiter,
+                                                 int subcyclingIterations, int reinitialisationFrequency,
+                                                 EulerMaterialParameters material1Parameters,
+                                                 EulerMaterialParameters material2Parameters, int maxSteps);
+    static vector<vector<EulerReducedStateVector> > solve2D(vector<vector<EulerReducedStateVector> >& initialCells,
+                                                            double cellSpacing, double CFLCoefficient, double finalTime,
+                                                            double bias, int slopeLimiter, int subcyclingIterations,
+                                                            int reinitialisationFrequency,
+                                                            EulerMaterialParameters material1Parameters,
+                                                            EulerMaterialParameters material2Parameters, int maxSteps);
     static vector<EulerStateVector> solve(vector<EulerStateVector>& initialCells, double cellSpacing, double CFLCoefficient,
                                           double finalTime, double bias, int slopeLimiter, int subcyclingIterations,
                                           EulerMaterialParameters mp, int maxSteps);
