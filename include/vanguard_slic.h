@@ -14,6 +14,8 @@
  *   VG_MODEL_HPR  (17 planes): rho, p, A(9, row-major), u, v, w, Jx, Jy, Jz
  *   VG_MODEL_EULER_REDUCED (7 planes): alpha1, u, v, w, rho1, rho2, p     the reduced two-material model,
  *                                      Euler/Multiphysics/eulerreducedstatevector.cpp:30-41 (w must be 0)
+ *   VG_MODEL_EULER_MULTIPHYSICS (8 planes): alpha1, u, v, w, rho1, p1, rho2, p2   the multiphysics two-material
+ *                                      model, Euler/Multiphysics/eulermultiphysicsstatevector.cpp:32-44 (w = 0)
  *                                                                HPR/hprstatevector.cpp:50-73
  * Ownership: a vg_solver owns all device memory it allocates; the caller owns every host buffer.
  * Threading: calls on different solvers are independent and re-entrant; one solver must not be used
@@ -39,7 +41,13 @@ typedef enum vg_status {
     VG_EUNSUPPORTED = 6  /* the input needs a variant this build does not provide (see below) */
 } vg_status;
 
-typedef enum vg_model { VG_MODEL_EULER = 0, VG_MODEL_MHD = 1, VG_MODEL_HPR = 2, VG_MODEL_EULER_REDUCED = 3 } vg_model;
+typedef enum vg_model {
+    VG_MODEL_EULER = 0,
+    VG_MODEL_MHD = 1,
+    VG_MODEL_HPR = 2,
+    VG_MODEL_EULER_REDUCED = 3,
+    VG_MODEL_EULER_MULTIPHYSICS = 4
+} vg_model;
 
 /* VG_FP64: every operation in float64, in the reference's order, no FMA: matches the reference.
  * VG_MIXED: reconstruction, half-step evolution and FORCE flux in float32; pressure recovery, the CFL
@@ -60,7 +68,7 @@ enum { VG_SUPERBEE = 0, VG_VANLEER = 1, VG_MINBEE = 2 };
  *   Euler: {gamma, p_inf, c_v, E0, T_ign, rate}   EulerMaterialParameters (Euler/eulermaterialparameters.h)
  *   MHD:   {gamma, p_inf, c_h}                    MHDMaterialParameters; c_h is recomputed every step by
  *                                                 vg_run as solve() does, and read from here by vg_sweep
- *   Euler reduced: {gamma1, p_inf1, gamma2, p_inf2}   the two EulerMaterialParameters of the materials
+ *   Euler reduced, multiphysics: {gamma1, p_inf1, gamma2, p_inf2}   the two materials' EulerMaterialParameters
  *   HPR:   {gamma, p_inf, c_v, rho0, T0, c_s, alpha, tau1, tau2, T_ref, p_ref, is_thermal,
  *           eos, Gamma0, c0, s, alpha_eos, is_plastic, sigma0, n}
  *                                                 HPRMaterialParameters (HPR/hprmaterialparameters.cpp:34-69):
@@ -96,8 +104,9 @@ typedef struct vg_run_config {
                          * Euler on the eigenvalues of A^T A, heat flux by exponential sub-steps), stable at any tau;
                          * subcycles is then ignored.  Results approach the forcing's as its sub-cycles grow, not bit
                          * for bit. */
-    int reinit_frequency;  /* Euler reduced model: reinitialisationFrequency of SecondOrderSolver::solve{,2D}
-                            * (Solvers/secondordersolver.cpp:354-385): MultiphysicsSolvers::reinitialiseVolumeFraction
+    int reinit_frequency;  /* Euler two-material models: reinitialisationFrequency of SecondOrderSolver::solve{,2D}
+                            * (Solvers/secondordersolver.cpp:314-350, :354-385): MultiphysicsSolvers::
+                            * reinitialiseVolumeFraction
                             * after every reinit_frequency-th step; 0: never */
 } vg_run_config;
 

@@ -23,7 +23,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libvgref.so")
 
-EULER, MHD, HPR, EULER_REDUCED = 0, 1, 2, 3
+EULER, MHD, HPR, EULER_REDUCED, EULER_MULTIPHYSICS = 0, 1, 2, 3, 4
 NVAR = {EULER: 6, MHD: 9, HPR: 17}
 TRANSMISSIVE, PERIODIC = 0, 1
 SUPERBEE, VANLEER, MINBEE = 0, 1, 2
@@ -174,13 +174,14 @@ def run_first_order(model, planes, dx, cfl, t_end=0.0, steps=0, params=None, bc=
     prm = _params(params)
     st = ctypes.c_int()
     nx, ny = (planes.shape[2], planes.shape[1]) if planes.ndim == 3 else (planes.shape[1], 1)
-    if model == EULER_REDUCED:  # the restatement carries an unused eighth plane
-        assert planes.shape[0] == 7 and planes.dtype == np.float64 and planes.flags.c_contiguous
-        padded = np.zeros((8,) + planes.shape[1:])
-        padded[:7] = planes
+    if model in (EULER_REDUCED, EULER_MULTIPHYSICS):  # the restatement carries one unused plane
+        nw = 7 if model == EULER_REDUCED else 8
+        assert planes.shape[0] == nw and planes.dtype == np.float64 and planes.flags.c_contiguous
+        padded = np.zeros((nw + 1,) + planes.shape[1:])
+        padded[:nw] = planes
         t = lib().vo_run_first_order(model, _ptr(padded), nx, ny, dx, cfl, t_end, steps, _ptr(prm), bc,
                                      ctypes.byref(st))
-        planes[:] = padded[:7]
+        planes[:] = padded[:nw]
         return t, st.value
     _check(planes, NVAR[model])
     t = lib().vo_run_first_order(model, _ptr(planes), nx, ny, dx, cfl, t_end, steps, _ptr(prm), bc, ctypes.byref(st))
@@ -237,33 +238,40 @@ def hpr_cell(w, params, reference=False):
     return (*outs, sp)
 
 
-def run_reduced(planes, dx, cfl, t_end=0.0, steps=0, bias=0.0, limiter=SUPERBEE, params=None, reinit=0,
-                reference=False, threads=1, bc=TRANSMISSIVE):
-    """SecondOrderSolver::solve{,2D} of the Euler reduced two-material model on its 7 primitive planes (alpha1, u, v,
-    w, rho1, rho2, p) x (n) or (ny, nx), in place, from the restatement or (reference=True) the reference; params =
-    (gamma1, p_inf1, gamma2, p_inf2); reinit > 0 reinitialises the volume fraction every `reinit` steps.  Returns
-    (t, steps)."""
-    assert planes.shape[0] == 7 and planes.dtype == np.float64 and planes.flags.c_contiguous
+def run_two_material(model, planes, dx, cfl, t_end=0.0, steps=0, bias=0.0, limiter=SUPERBEE, params=None, reinit=0,
+                     reference=False, threads=1, bc=TRANSMISSIVE):
+    """SecondOrderSolver::solve{,2D} of an Euler two-material model on its primitive planes, in place: EULER_REDUCED
+    (7 planes: alpha1, u, v, w, rho1, rho2, p) or EULER_MULTIPHYSICS (8: alpha1, u, v, w, rho1, p1, rho2, p2), x (n)
+    or (ny, nx); from the restatement or (reference=True) the reference.  params = (gamma1, p_inf1, gamma2, p_inf2);
+    reinit > 0 reinitialises the volume fraction every `reinit` steps.  Returns (t, steps)."""
+    nw = 7 if model == EULER_REDUCED else 8
+    assert planes.shape[0] == nw and planes.dtype == np.float64 and planes.flags.c_contiguous
     nx = planes.shape[-1]
     ny = 1 if planes.ndim == 2 else planes.shape[1]
     prm = _params(params)
     st = ctypes.c_int()
     if reference:
-        assert bc == TRANSMISSIVE, "the reference's reduced model has transmissive boundaries only"
+        assert bc == TRANSMISSIVE, "the reference's two-material models have transmissive boundaries only"
         R = ref()
         R.vgref_set_threads(threads)
-        R.vgref_reduced_run.restype = _c_double
-        t = R.vgref_reduced_run(_ptr(planes), nx, ny, _c_double(dx), _c_double(cfl), _c_double(t_end), steps,
-                                _c_double(bias), limiter, _ptr(prm), reinit, ctypes.byref(st))
+        fn = R.vgref_reduced_run if model == EULER_REDUCED else R.vgref_multiphysics_run
+        fn.restype = _c_double
+        t = fn(_ptr(planes), nx, ny, _c_double(dx), _c_double(cfl), _c_double(t_end), steps, _c_double(bias), limiter,
+               _ptr(prm), reinit, ctypes.byref(st))
         return t, st.value
-    padded = np.zeros((8,) + planes.shape[1:])
-    padded[:7] = planes
+    padded = np.zeros((nw + 1,) + planes.shape[1:])  # the restatement carries one unused plane
+    padded[:nw] = planes
     L = lib()
-    L.vo_run_reduced.restype = _c_double
-    t = L.vo_run_reduced(_ptr(padded), nx, ny, _c_double(dx), _c_double(cfl), _c_double(t_end), steps,
-                         _c_double(bias), limiter, _ptr(prm), bc, reinit, ctypes.byref(st))
-    planes[:] = padded[:7]
+    L.vo_run_two_material.restype = _c_double
+    t = L.vo_run_two_material(model, _ptr(padded), nx, ny, _c_double(dx), _c_double(cfl), _c_double(t_end), steps,
+                              _c_double(bias), limiter, _ptr(prm), bc, reinit, ctypes.byref(st))
+    planes[:] = padded[:nw]
     return t, st.value
+
+
+def run_reduced(planes, dx, cfl, **kw):
+    """run_two_material of the reduced model (7 planes)."""
+    return run_two_material(EULER_REDUCED, planes, dx, cfl, **kw)
 
 
 def hpr_eos(params, rho, p, e, reference=False):

@@ -714,3 +714,70 @@ extern "C" double vgref_reduced_run(double* planes, int nx, int ny, double dx, d
     return t;
 }
 
+// ------------------------------------------------------------------------- Euler multiphysics two-material model
+// planes: the 8 primitive planes of EulerMultiphysicsStateVector (alpha1, u, v, w, rho1, p1, rho2, p2; :32-44);
+// prm = {gamma1, p_inf1, gamma2, p_inf2}.  max_steps <= 0: the reference's own SecondOrderSolver::solve{,2D} to t_end;
+// else its per-step functions for max_steps steps, in solve's order (Solvers/secondordersolver.cpp:354-385, :470-...),
+// with the volume-fraction reinitialisation every reinit_freq steps.
+static EulerMultiphysicsStateVector mphCell(const double* planes, long plane, long k) {
+    return EulerMultiphysicsStateVector(planes[k], planes[plane + k], planes[2 * plane + k], planes[3 * plane + k],
+                                        planes[4 * plane + k], planes[5 * plane + k], planes[6 * plane + k],
+                                        planes[7 * plane + k]);
+}
+static void mphStore(EulerMultiphysicsStateVector& c, double* planes, long plane, long k) {
+    vector<double> w = c.computePrimitiveVariableVector();
+    for (int v = 0; v < 8; v++) planes[v * plane + k] = w[v];
+}
+
+extern "C" double vgref_multiphysics_run(double* planes, int nx, int ny, double dx, double cfl, double t_end, int max_steps,
+                                    double bias, int limiter, const double* prm, int reinit_freq, int* steps_out) {
+    EulerMaterialParameters m1(prm[0], prm[1]), m2(prm[2], prm[3]);
+    const long plane = (long)nx * ny;
+    double t = 0.0;
+    int it = 0;
+    if (ny == 1) {
+        vector<EulerMultiphysicsStateVector> cells(nx);
+        for (int i = 0; i < nx; i++) cells[i] = mphCell(planes, plane, i);
+        if (max_steps <= 0) {
+            cells = SecondOrderSolver::solve(cells, dx, cfl, t_end, bias, limiter, 0, reinit_freq, m1, m2);
+            t = t_end;
+        } else {
+            for (; it < max_steps; it++) {
+                vector<EulerMultiphysicsStateVector> withB = Solvers::insertBoundaryCells(cells, 2);
+                double dt = Solvers::computeStableTimeStep(withB, dx, cfl, t, 1.0e300, it, m1, m2);
+                SecondOrderSolver::computeSLICTimeStep(cells, withB, dx, dt, bias, limiter, m1, m2);
+                t += dt;
+                if (reinit_freq != 0 && ((it + 1) % reinit_freq) == 0)
+                    MultiphysicsSolvers::reinitialiseVolumeFraction(cells, m1, m2);
+            }
+        }
+        for (int i = 0; i < nx; i++) mphStore(cells[i], planes, plane, i);
+    } else {
+        vector<vector<EulerMultiphysicsStateVector> > g(ny, vector<EulerMultiphysicsStateVector>(nx));
+        for (int i = 0; i < ny; i++)
+            for (int j = 0; j < nx; j++) g[i][j] = mphCell(planes, plane, (long)i * nx + j);
+        if (max_steps <= 0) {
+            g = SecondOrderSolver::solve2D(g, dx, cfl, t_end, bias, limiter, 0, reinit_freq, m1, m2);
+            t = t_end;
+        } else {
+            for (; it < max_steps; it++) {
+                vector<vector<EulerMultiphysicsStateVector> > withB = Solvers::insertBoundaryCells2D(g, 2);
+                double dt = Solvers::computeStableTimeStep2D(withB, dx, cfl, t, 1.0e300, it, m1, m2);
+                SecondOrderSolver::computeXSLICTimeStep2D(g, withB, dx, 0.5 * dt, bias, limiter, m1, m2);
+                withB = Solvers::insertBoundaryCells2D(g, 2);
+                SecondOrderSolver::computeYSLICTimeStep2D(g, withB, dx, dt, bias, limiter, m1, m2);
+                withB = Solvers::insertBoundaryCells2D(g, 2);
+                SecondOrderSolver::computeXSLICTimeStep2D(g, withB, dx, 0.5 * dt, bias, limiter, m1, m2);
+                t += dt;
+                if (reinit_freq != 0 && ((it + 1) % reinit_freq) == 0)
+                    MultiphysicsSolvers::reinitialiseVolumeFraction(g, m1, m2);
+            }
+        }
+        for (int i = 0; i < ny; i++)
+            for (int j = 0; j < nx; j++) mphStore(g[i][j], planes, plane, (long)i * nx + j);
+    }
+    if (steps_out) *steps_out = it;
+    return t;
+}
+
+

@@ -875,12 +875,93 @@ static void red_default(const double* prm, double* W) {
     W[0] = 0.999; W[1] = 0.0; W[2] = 0.0; W[3] = 0.0; W[4] = 1.0; W[5] = 1.0; W[6] = 1.0; W[7] = 0.0;
 }
 
-/* relaxTotalDensity (:281-287) and the volume fraction of a cell of a reinitialisation window */
+/* ---- Euler multiphysics two-material model: Euler/Multiphysics/eulermultiphysicsstatevector.cpp, prm as the reduced
+ * model's.  W = alpha1, u, v, w, rho1, p1, rho2, p2 (the reference's primitive order) and an unused ninth plane;
+ * U = rho, rho alpha1, rho u, rho v, rho w, alpha1 rho1, alpha1 rho1 E1, alpha2 rho2, alpha2 rho2 E2. */
+/* computeConservedVariableVector (:99-128) with computeMaterial{1,2}TotalEnergy (:255-260, :277-282) */
+static void mph_cons(const double* W, const double* prm, double* U) {
+    double a1 = red_clamp(W[0]), a2 = 1.0 - a1;
+    double u = W[1], v = W[2], w = W[3], r1 = W[4], p1 = W[5], r2 = W[6], p2 = W[7];
+    double rho = (a1 * r1) + (a2 * r2);
+    double v2 = ((u * u) + (v * v)) + (w * w);
+    U[0] = rho;
+    U[1] = rho * a1;
+    U[2] = rho * u;
+    U[3] = rho * v;
+    U[4] = rho * w;
+    U[5] = a1 * r1;
+    U[6] = a1 * (r1 * ((0.5 * v2) + euler_e(r1, p1, prm)));
+    U[7] = a2 * r2;
+    U[8] = a2 * (r2 * ((0.5 * v2) + euler_e(r2, p2, prm + 2)));
+}
+/* setConservedVariableVector (:46-79); its |v|^2 adds w + w where w * w is meant, as the reference does */
+static void mph_setcons(const double* U, const double* prm, double* W) {
+    double rho = U[0];
+    double a1 = red_clamp(U[1] / rho), a2 = 1.0 - a1;
+    double u = U[2] / rho, v = U[3] / rho, w = U[4] / rho;
+    double r1 = U[5] / a1;
+    double v2 = ((u * u) + (v * v)) + (w + w);
+    double e1 = (U[6] / (r1 * a1)) - (0.5 * v2);
+    double r2 = U[7] / a2;
+    double e2 = (U[8] / (r2 * a2)) - (0.5 * v2);
+    W[0] = a1; W[1] = u; W[2] = v; W[3] = w;
+    W[4] = r1; W[5] = euler_p(r1, e1, prm);
+    W[6] = r2; W[7] = euler_p(r2, e2, prm + 2);
+    W[8] = 0.0;
+}
+/* compute{X,Y}FluxVector(vector, params, params) (:130-183, :190-243) */
+static void mph_flux(const double* U, int axis, const double* prm, double* F) {
+    double rho = U[0];
+    double a1 = red_clamp(U[1] / rho), a2 = 1.0 - a1;
+    double u = U[2] / rho, v = U[3] / rho, w = U[4] / rho;
+    double r1 = U[5] / a1;
+    double v2 = ((u * u) + (v * v)) + (w * w);
+    double E1 = U[6] / (a1 * r1);
+    double p1 = euler_p(r1, E1 - (0.5 * v2), prm);
+    double r2 = U[7] / a2;
+    double E2 = U[8] / (a2 * r2);
+    double p2 = euler_p(r2, E2 - (0.5 * v2), prm + 2);
+    double un = axis == 0 ? u : v;
+    double pm = (a1 * p1) + (a2 * p2);
+    F[0] = rho * un;
+    F[1] = rho * (un * a1);
+    F[2] = rho * (un * u);
+    F[3] = rho * (un * v);
+    F[4] = rho * (un * w);
+    F[axis == 0 ? 2 : 3] += pm;
+    F[5] = a1 * (r1 * un);
+    F[6] = a1 * ((r1 * (un * E1)) + (un * p1));
+    F[7] = a2 * (r2 * un);
+    F[8] = a2 * ((r2 * (un * E2)) + (un * p2));
+}
+/* Solvers::computeMaximumWaveSpeed{,2D} (Solvers/solvers.cpp:278-296, :345-363) */
+static double mph_wave1d(const double* W, const double* prm) {
+    return fabs(W[1]) + smax(red_c(W[4], W[5], prm), red_c(W[6], W[7], prm + 2));
+}
+static double mph_wave2d(const double* W, const double* prm) {
+    return smax(fabs(W[1]), fabs(W[2])) + smax(red_c(W[4], W[5], prm), red_c(W[6], W[7], prm + 2));
+}
+/* EulerMultiphysicsStateVector() (:3-15) */
+static void mph_default(const double* prm, double* W) {
+    (void)prm;
+    W[0] = 0.999; W[1] = 0.0; W[2] = 0.0; W[3] = 0.0; W[4] = 1.0; W[5] = 1.0; W[6] = 1.0; W[7] = 1.0; W[8] = 0.0;
+}
+
+/* A cell of a reinitialisation window: relaxTotalDensity (reduced :281-287, multiphysics :308-314), for the
+ * multiphysics model relaxTotalPressure (:316-329, which sets both pressures to the volume-fraction mean), then the
+ * volume fraction.  Planes: reduced rho1 4, rho2 5; multiphysics rho1 4, p1 5, rho2 6, p2 7. */
+static int g_reinit_mph = 0;
 static void red_reset_cell(double* planes, long plane, long idx, double alpha) {
     double a1 = planes[idx];
-    double rho = (a1 * planes[4 * plane + idx]) + ((1.0 - a1) * planes[5 * plane + idx]);
-    planes[4 * plane + idx] = rho;
-    planes[5 * plane + idx] = rho;
+    int i1 = 4, i2 = g_reinit_mph ? 6 : 5;
+    double rho = (a1 * planes[i1 * plane + idx]) + ((1.0 - a1) * planes[i2 * plane + idx]);
+    planes[i1 * plane + idx] = rho;
+    planes[i2 * plane + idx] = rho;
+    if (g_reinit_mph) {
+        double p = (a1 * planes[5 * plane + idx]) + ((1.0 - a1) * planes[7 * plane + idx]);
+        planes[5 * plane + idx] = p;
+        planes[7 * plane + idx] = p;
+    }
     planes[idx] = alpha;
 }
 /* MultiphysicsSolvers::reinitialiseVolumeFraction for the reduced model (Solvers/multiphysicssolvers.cpp:164-191 in
@@ -921,6 +1002,7 @@ static const model M_EULER = {6, euler_cons, euler_setcons, euler_flux, euler_wa
 static const model M_MHD = {9, mhd_cons, mhd_setcons, mhd_flux, mhd_wave1d, mhd_wave2d, mhd_default, mhd_source};
 static const model M_HPR = {17, hpr_cons, hpr_setcons, hpr_flux, hpr_wave1d, hpr_wave2d, hpr_default, hpr_source};
 static const model M_RED = {8, red_cons, red_setcons, red_flux, red_wave1d, red_wave2d, red_default, 0};
+static const model M_MPH = {9, mph_cons, mph_setcons, mph_flux, mph_wave1d, mph_wave2d, mph_default, 0};
 
 static const model* model_of(int id) {
     switch (id) {
@@ -928,13 +1010,14 @@ static const model* model_of(int id) {
         case VO_MHD: return &M_MHD;
         case VO_HPR: return &M_HPR;
         case VO_EULER_REDUCED: return &M_RED;
+        case VO_EULER_MULTIPHYSICS: return &M_MPH;
         default: return NULL;
     }
 }
 
 int vo_nvar(int id) { const model* m = model_of(id); return m ? m->nv : 0; }
 int vo_nparams(int id) {
-    return id == VO_EULER ? 6 : id == VO_MHD ? 3 : id == VO_HPR ? 20 : id == VO_EULER_REDUCED ? 4 : 0;
+    return id == VO_EULER ? 6 : id == VO_MHD ? 3 : id == VO_HPR ? 20 : (id == VO_EULER_REDUCED || id == VO_EULER_MULTIPHYSICS) ? 4 : 0;
 }
 
 /* ------------------------------------------------------------------------------- SLIC building blocks */
@@ -1299,7 +1382,10 @@ static double run(int id, double* planes, int nx, int ny, int dims, double dx, d
         t += dt;
         it += 1;
         /* the reduced model's solve{,2D}: reinitialisation every reinit_freq steps (Solvers/secondordersolver.cpp) */
-        if (id == VO_EULER_REDUCED && reinit_freq != 0 && (it % reinit_freq) == 0) red_reinit(planes, nx, dims == 1 ? 1 : ny);
+        if ((id == VO_EULER_REDUCED || id == VO_EULER_MULTIPHYSICS) && reinit_freq != 0 && (it % reinit_freq) == 0) {
+            g_reinit_mph = id == VO_EULER_MULTIPHYSICS;
+            red_reinit(planes, nx, dims == 1 ? 1 : ny);
+        }
     }
     if (steps_out) *steps_out = it;
     return t;
@@ -1381,9 +1467,10 @@ double vo_run2d(int id, double* planes, int nx, int ny, double dx, double cfl, d
     return run(id, planes, nx, ny, 2, dx, cfl, t_end, max_steps, w, lim, prm, bc, subcycles, steps_out, dt_log, 0);
 }
 
-double vo_run_reduced(double* planes, int nx, int ny, double dx, double cfl, double t_end, int max_steps, double w,
-                      int lim, const double* prm, int bc, int reinit_freq, int* steps_out) {
-    return run(VO_EULER_REDUCED, planes, nx, ny, ny > 1 ? 2 : 1, dx, cfl, t_end, max_steps, w, lim, prm, bc, 0,
+double vo_run_two_material(int id, double* planes, int nx, int ny, double dx, double cfl, double t_end, int max_steps,
+                           double w, int lim, const double* prm, int bc, int reinit_freq, int* steps_out) {
+    if (id != VO_EULER_REDUCED && id != VO_EULER_MULTIPHYSICS) return -1.0;
+    return run(id, planes, nx, ny, ny > 1 ? 2 : 1, dx, cfl, t_end, max_steps, w, lim, prm, bc, 0,
                steps_out, NULL, reinit_freq);
 }
 

@@ -13,6 +13,7 @@
  *   MHD   (9):  rho, u, v, w, p, Bx, By, Bz, psi        MHD/mhdstatevector.cpp:35-47
  *   HPR  (17):  rho, p, A(9 row-major), u, v, w, Jx, Jy, Jz   HPR/hprstatevector.cpp:50-73
  *   Euler reduced (8): alpha1, u, v, w, rho1, rho2, p, unused  Euler/Multiphysics/eulerreducedstatevector.cpp:30-41
+ *   Euler multiphysics (9): alpha1, u, v, w, rho1, p1, rho2, p2, unused  .../eulermultiphysicsstatevector.cpp:32-44
  */
 #ifndef VANGUARD_SLIC_ORACLE_H
 #define VANGUARD_SLIC_ORACLE_H
@@ -21,7 +22,7 @@
 extern "C" {
 #endif
 
-enum { VO_EULER = 0, VO_MHD = 1, VO_HPR = 2, VO_EULER_REDUCED = 3 };
+enum { VO_EULER = 0, VO_MHD = 1, VO_HPR = 2, VO_EULER_REDUCED = 3, VO_EULER_MULTIPHYSICS = 4 };
 enum { VO_BC_TRANSMISSIVE = 0, VO_BC_PERIODIC = 1 };
 
 /* Number of primitive planes of a model (6, 9, 17). */
@@ -59,11 +60,12 @@ double vo_max_wave2d(int model, const double* planes, int nx, int ny, const doub
 void vo_forcing(int model, double* planes, int nx, int ny, double dx, double dt, double bias, int limiter,
                 const double* prm, int bc);
 
-/* SecondOrderSolver::solve{,2D} of the Euler reduced two-material model (8 planes: alpha1, u, v, w, rho1, rho2, p,
- * unused), prm = {gamma1, p_inf1, gamma2, p_inf2}; reinit_freq > 0 reinitialises the volume fraction every
- * reinit_freq steps (MultiphysicsSolvers::reinitialiseVolumeFraction). */
-double vo_run_reduced(double* planes, int nx, int ny, double dx, double cfl, double t_end, int max_steps, double w,
-                      int lim, const double* prm, int bc, int reinit_freq, int* steps_out);
+/* SecondOrderSolver::solve{,2D} of the Euler two-material models, id VO_EULER_REDUCED (8 planes: alpha1, u, v, w, rho1,
+ * rho2, p, unused) or VO_EULER_MULTIPHYSICS (9 planes: alpha1, u, v, w, rho1, p1, rho2, p2, unused), prm = {gamma1,
+ * p_inf1, gamma2, p_inf2}; reinit_freq > 0 reinitialises the volume fraction every reinit_freq steps
+ * (MultiphysicsSolvers::reinitialiseVolumeFraction). */
+double vo_run_two_material(int id, double* planes, int nx, int ny, double dx, double cfl, double t_end, int max_steps,
+                           double w, int lim, const double* prm, int bc, int reinit_freq, int* steps_out);
 
 /* HPR Mie-Grueneisen probe (HPR/hprmiegruneisen.cpp), 13 values per point k:
  *   Gamma, p_ref(rho), e_ref(rho), dGamma, dp_ref, de_ref, e(rho, p), p(rho, e), T(rho, p), de/drho(rho, p),

@@ -80,23 +80,33 @@ REDUCED_CASES = {
                                               dict(dx=1 / 32, cfl=0.8, steps=9, limiter=O.SUPERBEE, reinit=3,
                                                    params=wl.reduced_params(1.4, 0.0, 1.67, 0.0))),
 }
+# The Euler multiphysics two-material model (model id O.EULER_MULTIPHYSICS), same layouts, per-material pressures.
+MULTIPHYSICS_CASES = {
+    "multiphysics1d_twogamma120_superbee_reinit4_40": (
+        lambda: wl.multiphysics_from_reduced(wl.reduced_shock_tube(120, rho=(1.0, 0.1379), p=(2.0, 1.0))),
+        dict(dx=1 / 120, cfl=0.8, steps=40, limiter=O.SUPERBEE, reinit=4,
+             params=wl.reduced_params(1.4, 0.0, 1.67, 0.0))),
+    "multiphysics2d_bubble30x26_minbee_reinit3_9": (
+        lambda: wl.multiphysics_from_reduced(wl.reduced_bubble_2d(30, 26)),
+        dict(dx=1 / 30, cfl=0.8, steps=9, limiter=O.MINBEE, reinit=3, params=wl.reduced_params(1.4, 0.0, 1.67, 0.0))),
+}
 
 
-def make_reduced(name):
-    init, kw = REDUCED_CASES[name]
+def make_two_material(name):
+    model = O.EULER_REDUCED if name in REDUCED_CASES else O.EULER_MULTIPHYSICS
+    init, kw = (REDUCED_CASES if model == O.EULER_REDUCED else MULTIPHYSICS_CASES)[name]
     w0 = np.ascontiguousarray(init())
     out = w0.copy()
-    kw = dict(kw)
-    O.run_reduced(out, kw.pop("dx"), kw.pop("cfl"), reference=True, **kw)
-    _, kw2 = REDUCED_CASES[name]
-    np.savez_compressed(os.path.join(HERE, name + ".npz"), model=O.EULER_REDUCED, w0=w0, out=out,
-                        **{k: np.asarray(v) for k, v in kw2.items()})
+    kw2 = dict(kw)
+    O.run_two_material(model, out, kw2.pop("dx"), kw2.pop("cfl"), reference=True, **kw2)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), model=model, w0=w0, out=out,
+                        **{k: np.asarray(v) for k, v in kw.items()})
     print("wrote", name)
 
 
 def make(name):
-    if name in REDUCED_CASES:
-        return make_reduced(name)
+    if name in REDUCED_CASES or name in MULTIPHYSICS_CASES:
+        return make_two_material(name)
     model, init, kw = CASES[name]
     w0 = np.ascontiguousarray(init())
     out = w0.copy()
@@ -109,5 +119,5 @@ def make(name):
 
 
 if __name__ == "__main__":
-    for n in (sys.argv[1:] or list(CASES) + list(REDUCED_CASES)):
+    for n in (sys.argv[1:] or list(CASES) + list(REDUCED_CASES) + list(MULTIPHYSICS_CASES)):
         make(n)

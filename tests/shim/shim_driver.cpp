@@ -4,8 +4,8 @@
 //   shim_driver <out.bin>
 // Output, in order (float64): Euler 1D solve (6 x 200), Euler 2D per-sweep loop (6 x 24 x 20),
 // MHD solve2D (9 x 16 x 16), HPR solve (17 x 50), Euler 1D step-count solve (6 x 150), Euler 1D first-order solve
-// (6 x 150), HPR GodunovRomenski plastic solve (17 x 60), reduced two-material solve (7 x 120), then the number of 2D
-// steps the per-sweep loop took.
+// (6 x 150), HPR GodunovRomenski plastic solve (17 x 60), reduced two-material solve (7 x 120), multiphysics
+// two-material solve (8 x 100), then the number of 2D steps the per-sweep loop took.
 #include <cmath>
 #include <cstdio>
 #include <vector>
@@ -155,6 +155,21 @@ int main(int argc, char** argv) {
                                                                        EulerMaterialParameters(1.67));
         vector<double> v;
         for (int k = 0; k < 7; k++)
+            for (auto& c : out) v.push_back(c.computePrimitiveVariableVector()[k]);
+        put(f, v);
+    }
+    // 9) SecondOrderSolver::solve of the multiphysics two-material model, reinitialisation every 4 steps, t = 0.04
+    {
+        int n = 100;
+        vector<EulerMultiphysicsStateVector> cells(n);
+        for (int i = 0; i < n; i++)
+            cells[i] = i <= 0.5 * n ? EulerMultiphysicsStateVector(0.999, 0.0, 0.0, 0.0, 1.0, 2.0, 0.1379, 2.0)
+                                    : EulerMultiphysicsStateVector(0.001, 0.0, 0.0, 0.0, 1.0, 1.0, 0.1379, 1.0);
+        vector<EulerMultiphysicsStateVector> out = SecondOrderSolver::solve(cells, 1.0 / n, 0.8, 0.04, 0.0, 0, 0, 4,
+                                                                            EulerMaterialParameters(1.4),
+                                                                            EulerMaterialParameters(1.67));
+        vector<double> v;
+        for (int k = 0; k < 8; k++)
             for (auto& c : out) v.push_back(c.computePrimitiveVariableVector()[k]);
         put(f, v);
     }

@@ -103,5 +103,12 @@ def test_shim_driver_matches_oracle(gpu, oracle_lib, tmp_path):
     O.run_reduced(ref, 1 / 120, 0.8, t_end=0.05, limiter=0, params=wl.reduced_params(1.4, 0.0, 1.67, 0.0), reinit=5)
     assert np.array_equal(got, ref)
 
+    # 9) SecondOrderSolver::solve of the multiphysics two-material model, reinitialisation every 4 steps, t = 0.04
+    got = take((8, 100))
+    ref = wl.multiphysics_from_reduced(wl.reduced_shock_tube(100, rho=(1.0, 0.1379), p=(2.0, 1.0)))
+    O.run_two_material(O.EULER_MULTIPHYSICS, ref, 1 / 100, 0.8, t_end=0.04, limiter=0,
+                       params=wl.reduced_params(1.4, 0.0, 1.67, 0.0), reinit=4)
+    assert np.array_equal(got, ref)
+
     assert take((1,))[0] == 6
     assert off == data.size

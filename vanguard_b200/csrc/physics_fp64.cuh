@@ -324,4 +324,97 @@ struct EulerReducedF64 {
     __device__ static double pressure(const double* W) { return W[5]; }
 };
 
+// ------------------------------------------------------------------------- Euler multiphysics two-material
+// EulerMultiphysicsStateVector (Euler/Multiphysics/eulermultiphysicsstatevector.cpp) with w == 0 (host-checked):
+// W = (alpha1, u, v, rho1, p1, rho2, p2), U = (rho, rho alpha1, rho u, rho v, alpha1 rho1, alpha1 rho1 E1,
+// alpha2 rho2, alpha2 rho2 E2).  Params as EulerReducedF64's; its volume fractions are clamped the same way.
+struct EulerMultiphysicsF64 {
+    static constexpr int NW = 7;
+    static constexpr int NU = 8;
+    static constexpr bool HAS_Y = true;
+    static constexpr bool HAS_SOURCE = false;
+    using P = EulerReducedF64::P;
+    using R2 = EulerReducedF64;
+    __device__ static P params(const double* prm, double ch) { return R2::params(prm, ch); }
+
+    // computeConservedVariableVector (:99-128) with computeMaterial{1,2}TotalEnergy (:255-260, :277-282)
+    __device__ static void cons(const double* W, const P& q, double* U) {
+        const double a1 = R2::clamp_alpha(W[0]), a2 = 1.0 - a1;
+        const double u = W[1], v = W[2], r1 = W[3], p1 = W[4], r2 = W[5], p2 = W[6];
+        const double rho = (a1 * r1) + (a2 * r2);
+        const double v2 = (u * u) + (v * v);
+        U[0] = rho;
+        U[1] = rho * a1;
+        U[2] = rho * u;
+        U[3] = rho * v;
+        U[4] = a1 * r1;
+        U[5] = a1 * (r1 * ((0.5 * v2) + R2::e_of(r1, p1, q.g1, q.pinf1)));
+        U[6] = a2 * r2;
+        U[7] = a2 * (r2 * ((0.5 * v2) + R2::e_of(r2, p2, q.g2, q.pinf2)));
+    }
+    // setConservedVariableVector (:46-79); its |v|^2 term w + w (meant w * w) is an exact zero here
+    __device__ static void setcons(const double* U, const P& q, double* W) {
+        const double rho = U[0];
+        const double a1 = R2::clamp_alpha(U[1] / rho), a2 = 1.0 - a1;
+        const double u = U[2] / rho, v = U[3] / rho;
+        const double r1 = U[4] / a1;
+        const double v2 = (u * u) + (v * v);
+        const double e1 = (U[5] / (r1 * a1)) - (0.5 * v2);
+        const double r2 = U[6] / a2;
+        const double e2 = (U[7] / (r2 * a2)) - (0.5 * v2);
+        W[0] = a1;
+        W[1] = u;
+        W[2] = v;
+        W[3] = r1;
+        W[4] = R2::p_of(r1, e1, q.g1, q.pinf1);
+        W[5] = r2;
+        W[6] = R2::p_of(r2, e2, q.g2, q.pinf2);
+    }
+    // compute{X,Y}FluxVector(vector, params, params) (:130-183, :190-243)
+    template <int AXIS>
+    __device__ static void flux(const double* U, const P& q, double* F) {
+        const double rho = U[0];
+        const double a1 = R2::clamp_alpha(U[1] / rho), a2 = 1.0 - a1;
+        const double u = U[2] / rho, v = U[3] / rho;
+        const double r1 = U[4] / a1;
+        const double v2 = (u * u) + (v * v);
+        const double E1 = U[5] / (a1 * r1);
+        const double p1 = R2::p_of(r1, E1 - (0.5 * v2), q.g1, q.pinf1);
+        const double r2 = U[6] / a2;
+        const double E2 = U[7] / (a2 * r2);
+        const double p2 = R2::p_of(r2, E2 - (0.5 * v2), q.g2, q.pinf2);
+        const double un = AXIS == 0 ? u : v;
+        const double pm = (a1 * p1) + (a2 * p2);
+        F[0] = rho * un;
+        F[1] = rho * (un * a1);
+        F[2] = rho * (un * u);
+        F[3] = rho * (un * v);
+        if constexpr (AXIS == 0) F[2] = F[2] + pm;
+        else F[3] = F[3] + pm;
+        F[4] = a1 * (r1 * un);
+        F[5] = a1 * ((r1 * (un * E1)) + (un * p1));
+        F[6] = a2 * (r2 * un);
+        F[7] = a2 * ((r2 * (un * E2)) + (un * p2));
+    }
+    // Solvers::computeMaximumWaveSpeed{,2D} (Solvers/solvers.cpp:278-296, :345-363)
+    __device__ static double wave(const double* W, const P& q, int dims) {
+        const double c = std_max(R2::c_of(W[3], W[4], q.g1, q.pinf1), R2::c_of(W[5], W[6], q.g2, q.pinf2));
+        if (dims == 1) return fabs(W[1]) + c;
+        return std_max(fabs(W[1]), fabs(W[2])) + c;
+    }
+    // EulerMultiphysicsStateVector() (:3-15)
+    __device__ static void default_state(double* W) {
+        W[0] = 0.999;
+        W[1] = 0.0;
+        W[2] = 0.0;
+        W[3] = 1.0;
+        W[4] = 1.0;
+        W[5] = 1.0;
+        W[6] = 1.0;
+    }
+    // the smaller material density and the smaller material pressure (bad-state check)
+    __device__ static double density(const double* W) { return W[3] < W[5] ? W[3] : W[5]; }
+    __device__ static double pressure(const double* W) { return W[4] < W[6] ? W[4] : W[6]; }
+};
+
 }  // namespace vg

@@ -340,32 +340,35 @@ struct HPRMixedT {
 };
 using HPRMixed = HPRMixedT<false>;
 
-// The Euler reduced two-material model in the mixed form: FP64 states and flux function (its pressure
+// The Euler two-material models in the mixed form: FP64 states and flux function (its pressure
 // recovery from total energy), flux values rounded to FP32, FP32 flux combinations (EulerMixed's split for MHD
 // and HPR).
-struct ReducedMixed {
+template <class F64>
+struct TwoMaterialMixed {
     static constexpr bool ROUNDTRIP_EVOLVED = true;  // the stored form clamps alpha1 and rebuilds rho
-    static constexpr int NW = EulerReducedF64::NW;
-    static constexpr int NU = EulerReducedF64::NU;
+    static constexpr int NW = F64::NW;
+    static constexpr int NU = F64::NU;
     static constexpr bool HAS_Y = true;
     using R = double;
     static constexpr bool PAIR_X = false;
-    using P = EulerReducedF64::P;
-    __device__ static P params(const double* prm, double ch) { return EulerReducedF64::params(prm, ch); }
-    __device__ static void cons(const double* W, const P& q, double* U) { EulerReducedF64::cons(W, q, U); }
-    __device__ static void setcons(const double* U, const P& q, double* W) { EulerReducedF64::setcons(U, q, W); }
+    using P = typename F64::P;
+    __device__ static P params(const double* prm, double ch) { return F64::params(prm, ch); }
+    __device__ static void cons(const double* W, const P& q, double* U) { F64::cons(W, q, U); }
+    __device__ static void setcons(const double* U, const P& q, double* W) { F64::setcons(U, q, W); }
     template <int AXIS>
     __device__ static void flux(const double* U, const P& q, float* F) {
         double Fd[NU];
-        EulerReducedF64::template flux<AXIS>(U, q, Fd);
+        F64::template flux<AXIS>(U, q, Fd);
 #pragma unroll
         for (int i = 0; i < NU; i++) F[i] = (float)Fd[i];
     }
-    __device__ static double wave(const double* W, const P& q, int dims) { return EulerReducedF64::wave(W, q, dims); }
-    __device__ static void default_state(double* W) { EulerReducedF64::default_state(W); }
-    __device__ static double density(const double* W) { return EulerReducedF64::density(W); }
-    __device__ static double pressure(const double* W) { return EulerReducedF64::pressure(W); }
+    __device__ static double wave(const double* W, const P& q, int dims) { return F64::wave(W, q, dims); }
+    __device__ static void default_state(double* W) { F64::default_state(W); }
+    __device__ static double density(const double* W) { return F64::density(W); }
+    __device__ static double pressure(const double* W) { return F64::pressure(W); }
 };
+using ReducedMixed = TwoMaterialMixed<EulerReducedF64>;
+
 using HPRSolidMixed = HPRMixedT<true>;
 
 }  // namespace vg

@@ -2,7 +2,9 @@
 // MultiphysicsSolvers::reinitialiseVolumeFraction (Solvers/multiphysicssolvers.cpp:164-191 in 1D, :193-... in 2D),
 // which solve{,2D} call after every reinitialisationFrequency-th step.  In place on a.out (the step's result);
 // the device step counter decides (ctrl->it, already advanced by the step), so the whole time loop stays in one
-// CUDA graph.  Planes: alpha1 = 0, rho1 = 3, rho2 = 4.
+// CUDA graph.  MPH selects the multiphysics model: planes alpha1 0, rho1 3, p1 4, rho2 5, p2 6, and its cells also
+// relax both pressures to their volume-fraction mean (relaxTotalPressure); the reduced model's planes are alpha1 0,
+// rho1 3, rho2 4.
 //
 // A crossing is a cell j >= 1 with alpha_j < 0.5 <= alpha_{j-1} (descending) or, in 2D, alpha_j > 0.5 >= alpha_{j-1}
 // (ascending).  The four cells j-2 .. j+1 take the mixture density in both materials (relaxTotalDensity) and the
@@ -16,12 +18,20 @@
 
 namespace vg {
 
-// relaxTotalDensity (Euler/Multiphysics/eulerreducedstatevector.cpp:281-287), then the cell's volume fraction
+// relaxTotalDensity (Euler/Multiphysics/eulerreducedstatevector.cpp:281-287, eulermultiphysicsstatevector.cpp:308-314),
+// for the multiphysics model relaxTotalPressure (:316-329), then the cell's volume fraction
+template <bool MPH>
 __device__ inline void reduced_reset_cell(const SweepArgs& a, long idx, double alpha) {
+    constexpr int I1 = 3, I2 = MPH ? 5 : 4;
     const double a1 = a.out[idx];
-    const double rho = (a1 * a.out[3 * a.plane + idx]) + ((1.0 - a1) * a.out[4 * a.plane + idx]);
-    a.out[3 * a.plane + idx] = rho;
-    a.out[4 * a.plane + idx] = rho;
+    const double rho = (a1 * a.out[I1 * a.plane + idx]) + ((1.0 - a1) * a.out[I2 * a.plane + idx]);
+    a.out[I1 * a.plane + idx] = rho;
+    a.out[I2 * a.plane + idx] = rho;
+    if constexpr (MPH) {
+        const double p = (a1 * a.out[4 * a.plane + idx]) + ((1.0 - a1) * a.out[6 * a.plane + idx]);
+        a.out[4 * a.plane + idx] = p;
+        a.out[6 * a.plane + idx] = p;
+    }
     a.out[idx] = alpha;
 }
 
@@ -29,7 +39,7 @@ __device__ inline bool reduced_reinit_due(const SweepArgs& a) {
     return !a.ctrl || (a.ctrl->active && a.reinit_freq > 0 && (a.ctrl->it % a.reinit_freq) == 0);
 }
 
-template <int NT>
+template <bool MPH, int NT>
 __global__ void __launch_bounds__(NT) reduced_reinit1d_kernel(SweepArgs a) {
     if (!reduced_reinit_due(a)) return;
     __shared__ int part[NT / 32];
@@ -43,11 +53,12 @@ __global__ void __launch_bounds__(NT) reduced_reinit1d_kernel(SweepArgs a) {
         loc = 0;
         for (int w = 0; w < NT / 32; w++) loc = max(loc, part[w]);
         const int i = loc - 2 + (int)threadIdx.x;
-        if (i >= 0 && i < a.nx) reduced_reset_cell(a, i, i < loc ? 0.999 : 0.001);
+        if (i >= 0 && i < a.nx) reduced_reset_cell<MPH>(a, i, i < loc ? 0.999 : 0.001);
     }
 }
 
 // one line (row: stride 1, or column: stride pitch) of the 2D reinitialisation, by one thread
+template <bool MPH>
 __device__ inline void reduced_reinit_line(const SweepArgs& a, long start, long stride, int len) {
     int loc1[100], loc2[100], n1 = 0, n2 = 0;
     for (int j = 1; j < len; j++) {
@@ -57,32 +68,35 @@ __device__ inline void reduced_reinit_line(const SweepArgs& a, long start, long 
     }
     for (int k = 0; k < n1; k++)
         for (int j = loc1[k] - 2; j < loc1[k] + 2; j++)
-            if (j >= 0 && j < len) reduced_reset_cell(a, start + j * stride, j < loc1[k] ? 0.999 : 0.001);
+            if (j >= 0 && j < len) reduced_reset_cell<MPH>(a, start + j * stride, j < loc1[k] ? 0.999 : 0.001);
     for (int k = 0; k < n2; k++)
         for (int j = loc2[k] - 2; j < loc2[k] + 2; j++)
-            if (j >= 0 && j < len) reduced_reset_cell(a, start + j * stride, j < loc2[k] ? 0.001 : 0.999);
+            if (j >= 0 && j < len) reduced_reset_cell<MPH>(a, start + j * stride, j < loc2[k] ? 0.001 : 0.999);
 }
 
+template <bool MPH>
 __global__ void reduced_reinit_rows_kernel(SweepArgs a) {
     const int row = blockIdx.x * blockDim.x + threadIdx.x;
     if (row >= a.ny || !reduced_reinit_due(a)) return;
-    reduced_reinit_line(a, (long)row * a.pitch, 1, a.nx);
+    reduced_reinit_line<MPH>(a, (long)row * a.pitch, 1, a.nx);
 }
 
+template <bool MPH>
 __global__ void reduced_reinit_cols_kernel(SweepArgs a) {
     const int col = blockIdx.x * blockDim.x + threadIdx.x;
     if (col >= a.nx || !reduced_reinit_due(a)) return;
-    reduced_reinit_line(a, col, a.pitch, a.ny);
+    reduced_reinit_line<MPH>(a, col, a.pitch, a.ny);
 }
 
 // The reinitialisation of one step (kernels: 1 in 1D, 2 in 2D), in place on a.out.
+template <bool MPH>
 inline cudaError_t reduced_reinit(const SweepArgs& a, cudaStream_t st) {
     if (a.ny == 1) {
-        reduced_reinit1d_kernel<256><<<1, 256, 0, st>>>(a);
+        reduced_reinit1d_kernel<MPH, 256><<<1, 256, 0, st>>>(a);
     } else {
         constexpr int T = 64;
-        reduced_reinit_rows_kernel<<<(a.ny + T - 1) / T, T, 0, st>>>(a);
-        reduced_reinit_cols_kernel<<<(a.nx + T - 1) / T, T, 0, st>>>(a);
+        reduced_reinit_rows_kernel<MPH><<<(a.ny + T - 1) / T, T, 0, st>>>(a);
+        reduced_reinit_cols_kernel<MPH><<<(a.nx + T - 1) / T, T, 0, st>>>(a);
     }
     return cudaGetLastError();
 }

@@ -112,7 +112,9 @@ constexpr Ops make_ops() {
                &force1_y<M>,
                relax_of<M>(),
                0,
-               std::is_same<M, EulerReducedF64>::value ? &reduced_reinit_fp64 : nullptr};
+               std::is_same<M, EulerReducedF64>::value        ? &reduced_reinit_fp64
+               : std::is_same<M, EulerMultiphysicsF64>::value ? &multiphysics_reinit_fp64
+                                                              : nullptr};
 }
 
 const Ops kOps[V_COUNT] = {
@@ -123,6 +125,7 @@ const Ops kOps[V_COUNT] = {
     make_ops<HPRF64>(),
     make_ops<HPRSolidF64>(),
     make_ops<EulerReducedF64>(),
+    make_ops<EulerMultiphysicsF64>(),
 };
 
 }  // namespace
@@ -137,7 +140,8 @@ cudaError_t hpr_solid_forcing_fp64(const SweepArgs& a, int subcycles, cudaStream
     return forcing_impl<HPRSolidF64>(a, subcycles, st);
 }
 cudaError_t hpr_solid_relax_fp64(const SweepArgs& a, cudaStream_t st) { return relax_impl<HPRSolidF64>(a, st); }
-cudaError_t reduced_reinit_fp64(const SweepArgs& a, cudaStream_t st) { return reduced_reinit(a, st); }
+cudaError_t reduced_reinit_fp64(const SweepArgs& a, cudaStream_t st) { return reduced_reinit<false>(a, st); }
+cudaError_t multiphysics_reinit_fp64(const SweepArgs& a, cudaStream_t st) { return reduced_reinit<true>(a, st); }
 cudaError_t mhd7_forcing_fp64(const SweepArgs& a, int subcycles, cudaStream_t st) {
     return forcing_impl<MHDF64<false>>(a, subcycles, st);
 }

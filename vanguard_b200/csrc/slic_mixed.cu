@@ -100,10 +100,16 @@ const Ops kOps[V_COUNT] = {
     make_ops<HPRMixed>(&hpr_forcing_fp64, &hpr_relax_fp64),
     make_ops<HPRSolidMixed>(&hpr_solid_forcing_fp64, &hpr_solid_relax_fp64),
     make_ops<ReducedMixed>(nullptr, nullptr, &reduced_reinit_fp64),
+    Ops{},  // V_MPH7: no mixed form (see ops_mixed)
 };
 
 }  // namespace
 
-const Ops* ops_mixed(int variant) { return (variant >= 0 && variant < V_COUNT) ? &kOps[variant] : nullptr; }
+// The multiphysics two-material model has no mixed form: its trace material (volume fraction clamped at 0.001)
+// recovers its energy from the ratio of two tiny conserved components, which FP32 flux values perturb enough to
+// give negative pressures where FP64 does not.
+const Ops* ops_mixed(int variant) {
+    return (variant >= 0 && variant < V_COUNT && kOps[variant].nw > 0) ? &kOps[variant] : nullptr;
+}
 
 }  // namespace vg

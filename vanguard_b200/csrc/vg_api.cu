@@ -41,7 +41,8 @@ vg_status cuda_fail(cudaError_t e, const char* what) {
     } while (0)
 
 int ref_nvar(int model) {
-    return model == VG_MODEL_EULER ? 6 : model == VG_MODEL_MHD ? 9 : model == VG_MODEL_HPR ? 17 : model == VG_MODEL_EULER_REDUCED ? 7 : 0;
+    return model == VG_MODEL_EULER ? 6 : model == VG_MODEL_MHD ? 9 : model == VG_MODEL_HPR ? 17 : model == VG_MODEL_EULER_REDUCED ? 7
+           : model == VG_MODEL_EULER_MULTIPHYSICS ? 8 : 0;
 }
 
 // Reference plane carried in device plane k, per variant.
@@ -53,6 +54,7 @@ const int kPlanes[vg::V_COUNT][17] = {
     {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16},  // V_HPR17
     {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16},  // V_HPR17S
     {0, 1, 2, 4, 5, 6},             // V_RED6: alpha1, u, v, rho1, rho2, p
+    {0, 1, 2, 4, 5, 6, 7},          // V_MPH7: alpha1, u, v, rho1, p1, rho2, p2
 };
 
 }  // namespace
@@ -397,7 +399,7 @@ vg_status vg_create(const vg_grid_desc* desc, vg_solver** out) {
     if (!desc || !out) return fail(VG_EINVAL, "null argument");
     *out = nullptr;
     if (desc->model != VG_MODEL_EULER && desc->model != VG_MODEL_MHD && desc->model != VG_MODEL_HPR &&
-        desc->model != VG_MODEL_EULER_REDUCED)
+        desc->model != VG_MODEL_EULER_REDUCED && desc->model != VG_MODEL_EULER_MULTIPHYSICS)
         return fail(VG_EUNSUPPORTED, "model not available in this build");
     if (desc->nx < 2 || desc->ny < 1 || (desc->ny > 1 && desc->ny < 2))
         return fail(VG_EINVAL, "grid needs at least 2 cells along every swept axis");
@@ -405,6 +407,9 @@ vg_status vg_create(const vg_grid_desc* desc, vg_solver** out) {
     if (desc->boundary != VG_TRANSMISSIVE && desc->boundary != VG_PERIODIC) return fail(VG_EINVAL, "bad boundary");
     if (desc->precision == VG_MIXED && !vg::ops_mixed(vg::V_EULER2))
         return fail(VG_EUNSUPPORTED, "mixed precision not available in this build");
+    if (desc->precision == VG_MIXED && desc->model == VG_MODEL_EULER_MULTIPHYSICS)
+        return fail(VG_EUNSUPPORTED, "the multiphysics two-material model runs in VG_FP64 only (its trace material's "
+                                     "energy is not stable under FP32 flux values)");
     if (desc->model == VG_MODEL_HPR) {
         const double eos = desc->params[12];
         if (eos != 0.0 && eos != 1.0 && eos != 2.0)
@@ -416,7 +421,8 @@ vg_status vg_create(const vg_grid_desc* desc, vg_solver** out) {
     if (!s) return fail(VG_ENOMEM, "host allocation");
     s->d = *desc;
     s->dims = desc->ny > 1 ? 2 : 1;
-    s->max_nw = desc->model == VG_MODEL_EULER ? 4 : desc->model == VG_MODEL_MHD ? 9 : desc->model == VG_MODEL_EULER_REDUCED ? 6 : 17;
+    s->max_nw = desc->model == VG_MODEL_EULER ? 4 : desc->model == VG_MODEL_MHD ? 9 : desc->model == VG_MODEL_EULER_REDUCED ? 6
+                : desc->model == VG_MODEL_EULER_MULTIPHYSICS ? 7 : 17;
     s->pitch = ((long)desc->nx + 31) / 32 * 32;  // 256-byte aligned rows
     s->plane = s->pitch * desc->ny;
     s->floor5 = std::pow(10.0, -5.0);  // SlopeLimiters::computeSlopeVector's floor (Solvers/slopelimiters.cpp:232-239)
@@ -473,14 +479,14 @@ vg_status vg_upload_primitive(vg_solver* s, const double* planes, int is_device,
             }
             variant = (s->dims == 1 && zero_v) ? vg::V_EULER1 : vg::V_EULER2;
         }
-    } else if (s->d.model == VG_MODEL_EULER_REDUCED) {
-        // the reduced model carries alpha1, u, v, rho1, rho2, p: w must be 0
+    } else if (s->d.model == VG_MODEL_EULER_REDUCED || s->d.model == VG_MODEL_EULER_MULTIPHYSICS) {
+        // the two-material models carry every plane but w, which must be 0
         if (!is_device) {
             const double* w = planes + 3 * n;
             for (long i = 0; i < n; i++)
-                if (w[i] != 0.0) return fail(VG_EUNSUPPORTED, "reduced two-material state with w != 0");
+                if (w[i] != 0.0) return fail(VG_EUNSUPPORTED, "two-material state with w != 0");
         }
-        variant = vg::V_RED6;
+        variant = s->d.model == VG_MODEL_EULER_REDUCED ? vg::V_RED6 : vg::V_MPH7;
     } else if (s->d.model == VG_MODEL_HPR) {
         // a solid equation of state or plasticity selects the instantiation that carries them
         variant = (s->d.params[12] != 0.0 || s->d.params[17] != 0.0) ? vg::V_HPR17S : vg::V_HPR17;

@@ -19,7 +19,8 @@ enum Variant : int {
     V_HPR17 = 4,   // HPR, all 17 components:              rho, p, A(9), u, v, w, Jx, Jy, Jz
     V_HPR17S = 5,  // HPR solid (ShockMieGruneisen / GodunovRomenski) or plastic material, same planes
     V_RED6 = 6,    // Euler reduced two-material, w == 0:    alpha1, u, v, rho1, rho2, p
-    V_COUNT = 7
+    V_MPH7 = 7,    // Euler multiphysics two-material, w == 0: alpha1, u, v, rho1, p1, rho2, p2
+    V_COUNT = 8
 };
 
 struct Ops {
@@ -64,6 +65,7 @@ cudaError_t hpr_solid_forcing_fp64(const SweepArgs& a, int subcycles, cudaStream
 cudaError_t hpr_solid_relax_fp64(const SweepArgs& a, cudaStream_t st);
 // The reduced model's volume-fraction reinitialisation (slic_fp64.cu), shared by both forms.
 cudaError_t reduced_reinit_fp64(const SweepArgs& a, cudaStream_t st);
+cudaError_t multiphysics_reinit_fp64(const SweepArgs& a, cudaStream_t st);
 
 // Record the text returned by vg_last_error_string() on this thread.
 void set_last_error(const std::string& msg);

@@ -72,8 +72,10 @@ vg_solver* cached_solver(int model, int nx, int ny, int boundary, const double* 
 void run_planes(int model, std::vector<double>& planes, int nx, int ny, const double* params, int nparams, double dx,
                 double cfl, double tEnd, double bias, int limiter, int subcycles, int maxSteps = 0, int order = 2,
                 int reinit = 0) {
-    // the first-order loop runs in the exact form, bit for bit with the reference
-    SolverPtr s = make_solver(model, nx, ny, VG_TRANSMISSIVE, params, nparams, order == 1 ? VG_FP64 : -1);
+    // the first-order loop runs in the exact form, bit for bit with the reference; the multiphysics two-material model
+    // has no mixed form
+    const bool exact = order == 1 || model == VG_MODEL_EULER_MULTIPHYSICS;
+    SolverPtr s = make_solver(model, nx, ny, VG_TRANSMISSIVE, params, nparams, exact ? VG_FP64 : -1);
     vg_run_config c{};
     c.dx = dx;
     c.cfl = cfl;
@@ -543,7 +545,23 @@ void EulerReducedStateVector::setPrimitiveVariableVector(vector<double> w) {
 }
 vector<double> EulerReducedStateVector::computePrimitiveVariableVector() const { return vector<double>(w_, w_ + 7); }
 
+EulerMultiphysicsStateVector::EulerMultiphysicsStateVector()
+    : EulerMultiphysicsStateVector(0.999, 0.0, 0.0, 0.0, 1.0, 1.0, 1.0, 1.0) {}
+EulerMultiphysicsStateVector::EulerMultiphysicsStateVector(double a1, double u, double v, double w, double r1, double p1,
+                                                           double r2, double p2)
+    : w_{a1, u, v, w, r1, p1, r2, p2} {}
+void EulerMultiphysicsStateVector::setPrimitiveVariableVector(vector<double> w) {
+    for (int i = 0; i < 8; i++) w_[i] = w[i];
+}
+vector<double> EulerMultiphysicsStateVector::computePrimitiveVariableVector() const { return vector<double>(w_, w_ + 8); }
+
 namespace {
+void mph_get(const EulerMultiphysicsStateVector& c, double* w) { std::memcpy(w, c.data(), sizeof(double) * 8); }
+EulerMultiphysicsStateVector mph_make(const double* w) {
+    EulerMultiphysicsStateVector s;
+    std::memcpy(s.data(), w, sizeof(double) * 8);
+    return s;
+}
 void reduced_params(const EulerMaterialParameters& m1, const EulerMaterialParameters& m2, double* prm) {
     prm[0] = m1.getAdiabaticIndex(), prm[1] = m1.getStiffeningParameter();
     prm[2] = m2.getAdiabaticIndex(), prm[3] = m2.getStiffeningParameter();
@@ -583,6 +601,28 @@ vector<vector<EulerReducedStateVector> > SecondOrderSolver::solve2D(vector<vecto
     long ny = initialCells.size(), nx = initialCells[0].size();
     run_planes(VG_MODEL_EULER_REDUCED, p, (int)nx, (int)ny, prm, 4, dx, cfl, tEnd, bias, limiter, 0, maxSteps, 2, reinit);
     return unpack2<EulerReducedStateVector>(p, nx, ny, 7, reduced_make);
+}
+
+vector<EulerMultiphysicsStateVector> SecondOrderSolver::solve(vector<EulerMultiphysicsStateVector>& initialCells, double dx,
+                                                              double cfl, double tEnd, double bias, int limiter, int,
+                                                              int reinit, EulerMaterialParameters m1,
+                                                              EulerMaterialParameters m2) {
+    double prm[4];
+    reduced_params(m1, m2, prm);
+    std::vector<double> p = pack(initialCells, 8, mph_get);
+    run_planes(VG_MODEL_EULER_MULTIPHYSICS, p, (int)initialCells.size(), 1, prm, 4, dx, cfl, tEnd, bias, limiter, 0, 0, 2,
+               reinit);
+    return unpack<EulerMultiphysicsStateVector>(p, initialCells.size(), 8, mph_make);
+}
+vector<vector<EulerMultiphysicsStateVector> > SecondOrderSolver::solve2D(
+    vector<vector<EulerMultiphysicsStateVector> >& initialCells, double dx, double cfl, double tEnd, double bias,
+    int limiter, int, int reinit, EulerMaterialParameters m1, EulerMaterialParameters m2) {
+    double prm[4];
+    reduced_params(m1, m2, prm);
+    std::vector<double> p = pack2(initialCells, 8, mph_get);
+    long ny = initialCells.size(), nx = initialCells[0].size();
+    run_planes(VG_MODEL_EULER_MULTIPHYSICS, p, (int)nx, (int)ny, prm, 4, dx, cfl, tEnd, bias, limiter, 0, 0, 2, reinit);
+    return unpack2<EulerMultiphysicsStateVector>(p, nx, ny, 8, mph_make);
 }
 
 // --------------------------------------------------------------------------------------------- MHD solver

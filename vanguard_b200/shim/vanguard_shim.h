@@ -116,6 +116,31 @@ private:
     double w_[7];
 };
 
+// EulerMultiphysicsStateVector (Euler/Multiphysics/eulermultiphysicsstatevector.h): the multiphysics two-material
+// state, primitives alpha1, u, v, w, rho1, p1, rho2, p2.
+class EulerMultiphysicsStateVector {
+public:
+    EulerMultiphysicsStateVector();
+    EulerMultiphysicsStateVector(double newMaterial1VolumeFraction, double newInterfaceXVelocity, double newInterfaceYVelocity,
+                                 double newInterfaceZVelocity, double newMaterial1Density, double newMaterial1Pressure,
+                                 double newMaterial2Density, double newMaterial2Pressure);
+    void setPrimitiveVariableVector(vector<double> w);
+    vector<double> computePrimitiveVariableVector() const;
+    double getMaterial1VolumeFraction() const { return w_[0]; }
+    double getInterfaceXVelocity() const { return w_[1]; }
+    double getInterfaceYVelocity() const { return w_[2]; }
+    double getInterfaceZVelocity() const { return w_[3]; }
+    double getMaterial1Density() const { return w_[4]; }
+    double getMaterial1Pressure() const { return w_[5]; }
+    double getMaterial2Density() const { return w_[6]; }
+    double getMaterial2Pressure() const { return w_[7]; }
+    double* data() { return w_; }
+    const double* data() const { return w_; }
+
+private:
+    double w_[8];
+};
+
 class MHDMaterialParameters {
 public:
     MHDMaterialParameters();
@@ -308,6 +333,18 @@ public:
                                                             int reinitialisationFrequency,
                                                             EulerMaterialParameters material1Parameters,
                                                             EulerMaterialParameters material2Parameters);
+    // the multiphysics two-material model (Solvers/secondordersolver.cpp:314-350, :430-468), exact form
+    static vector<EulerMultiphysicsStateVector> solve(vector<EulerMultiphysicsStateVector>& initialCells, double cellSpacing,
+                                                      double CFLCoefficient, double finalTime, double bias, int slopeLimiter,
+                                                      int subcyclingIterations, int reinitialisationFrequency,
+                                                      EulerMaterialParameters material1Parameters,
+                                                      EulerMaterialParameters material2Parameters);
+    static vector<vector<EulerMultiphysicsStateVector> > solve2D(vector<vector<EulerMultiphysicsStateVector> >& initialCells,
+                                                                 double cellSpacing, double CFLCoefficient, double finalTime,
+                                                                 double bias, int slopeLimiter, int subcyclingIterations,
+                                                                 int reinitialisationFrequency,
+                                                                 EulerMaterialParameters material1Parameters,
+                                                                 EulerMaterialParameters material2Parameters);
     // step-count overloads (not in the reference): also stop after maxSteps steps when maxSteps > 0
     static vector<EulerReducedStateVector> solve(vector<EulerReducedStateVector>& initialCells, double cellSpacing,
                                                  double CFLCoefficient, double finalTime, double bias, int slopeLimiter,

@@ -300,3 +300,16 @@ def reduced_bubble_2d(nx, ny=None, rho=(1.0, 0.125), p=(1.0, 0.1), radius=0.2):
     W[6] = np.where(inside, p[0], p[1])
     return W
 
+
+MULTIPHYSICS_NVAR = 8  # alpha1, u, v, w, rho1, p1, rho2, p2 (Euler/Multiphysics/eulermultiphysicsstatevector.cpp:32-44)
+
+
+def multiphysics_from_reduced(W):
+    """The multiphysics model's planes of a reduced-model state: both materials at the interface pressure."""
+    out = np.zeros((MULTIPHYSICS_NVAR,) + W.shape[1:])
+    out[:5] = W[:5]
+    out[5] = W[6]
+    out[6] = W[5]
+    out[7] = W[6]
+    return out
+
