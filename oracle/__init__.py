@@ -23,7 +23,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libvgref.so")
 
-EULER, MHD, HPR, EULER_REDUCED, EULER_MULTIPHYSICS = 0, 1, 2, 3, 4
+EULER, MHD, HPR, EULER_REDUCED, EULER_MULTIPHYSICS, MHD_REDUCED = 0, 1, 2, 3, 4, 5
 NVAR = {EULER: 6, MHD: 9, HPR: 17}
 TRANSMISSIVE, PERIODIC = 0, 1
 SUPERBEE, VANLEER, MINBEE = 0, 1, 2
@@ -174,8 +174,8 @@ def run_first_order(model, planes, dx, cfl, t_end=0.0, steps=0, params=None, bc=
     prm = _params(params)
     st = ctypes.c_int()
     nx, ny = (planes.shape[2], planes.shape[1]) if planes.ndim == 3 else (planes.shape[1], 1)
-    if model in (EULER_REDUCED, EULER_MULTIPHYSICS):  # the restatement carries one unused plane
-        nw = 7 if model == EULER_REDUCED else 8
+    if model in _TWO_MATERIAL_NW:  # the restatement carries one unused plane
+        nw = _TWO_MATERIAL_NW[model]
         assert planes.shape[0] == nw and planes.dtype == np.float64 and planes.flags.c_contiguous
         padded = np.zeros((nw + 1,) + planes.shape[1:])
         padded[:nw] = planes
@@ -238,13 +238,19 @@ def hpr_cell(w, params, reference=False):
     return (*outs, sp)
 
 
+_TWO_MATERIAL_NW = {EULER_REDUCED: 7, EULER_MULTIPHYSICS: 8, MHD_REDUCED: 11}
+
+
 def run_two_material(model, planes, dx, cfl, t_end=0.0, steps=0, bias=0.0, limiter=SUPERBEE, params=None, reinit=0,
-                     reference=False, threads=1, bc=TRANSMISSIVE):
-    """SecondOrderSolver::solve{,2D} of an Euler two-material model on its primitive planes, in place: EULER_REDUCED
-    (7 planes: alpha1, u, v, w, rho1, rho2, p) or EULER_MULTIPHYSICS (8: alpha1, u, v, w, rho1, p1, rho2, p2), x (n)
-    or (ny, nx); from the restatement or (reference=True) the reference.  params = (gamma1, p_inf1, gamma2, p_inf2);
-    reinit > 0 reinitialises the volume fraction every `reinit` steps.  Returns (t, steps)."""
-    nw = 7 if model == EULER_REDUCED else 8
+                     reference=False, threads=1, bc=TRANSMISSIVE, subcycles=0):
+    """(MHD)SecondOrderSolver::solve{,2D} of a two-material model on its primitive planes, in place: EULER_REDUCED
+    (7 planes: alpha1, u, v, w, rho1, rho2, p), EULER_MULTIPHYSICS (8: alpha1, u, v, w, rho1, p1, rho2, p2) or
+    MHD_REDUCED (11: alpha1, u, v, w, rho1, rho2, p, Bx, By, Bz, psi), x (n) or (ny, nx); from the restatement or
+    (reference=True) the reference.  params = (gamma1, p_inf1, gamma2, p_inf2); reinit > 0 reinitialises the volume
+    fraction every `reinit` steps; subcycles > 0 (MHD_REDUCED) adds the RK4 GLM damping sub-cycles.
+    Returns (t, steps)."""
+    nw = _TWO_MATERIAL_NW[model]
+    assert subcycles == 0 or model == MHD_REDUCED, "only the MHD reduced model has a source"
     assert planes.shape[0] == nw and planes.dtype == np.float64 and planes.flags.c_contiguous
     nx = planes.shape[-1]
     ny = 1 if planes.ndim == 2 else planes.shape[1]
@@ -254,6 +260,12 @@ def run_two_material(model, planes, dx, cfl, t_end=0.0, steps=0, bias=0.0, limit
         assert bc == TRANSMISSIVE, "the reference's two-material models have transmissive boundaries only"
         R = ref()
         R.vgref_set_threads(threads)
+        if model == MHD_REDUCED:
+            fn = R.vgref_mhd_reduced_run
+            fn.restype = _c_double
+            t = fn(_ptr(planes), nx, ny, _c_double(dx), _c_double(cfl), _c_double(t_end), steps, _c_double(bias),
+                   limiter, _ptr(prm), subcycles, reinit, ctypes.byref(st))
+            return t, st.value
         fn = R.vgref_reduced_run if model == EULER_REDUCED else R.vgref_multiphysics_run
         fn.restype = _c_double
         t = fn(_ptr(planes), nx, ny, _c_double(dx), _c_double(cfl), _c_double(t_end), steps, _c_double(bias), limiter,
@@ -262,9 +274,14 @@ def run_two_material(model, planes, dx, cfl, t_end=0.0, steps=0, bias=0.0, limit
     padded = np.zeros((nw + 1,) + planes.shape[1:])  # the restatement carries one unused plane
     padded[:nw] = planes
     L = lib()
-    L.vo_run_two_material.restype = _c_double
-    t = L.vo_run_two_material(model, _ptr(padded), nx, ny, _c_double(dx), _c_double(cfl), _c_double(t_end), steps,
-                              _c_double(bias), limiter, _ptr(prm), bc, reinit, ctypes.byref(st))
+    if model == MHD_REDUCED:
+        L.vo_run_mhd_reduced.restype = _c_double
+        t = L.vo_run_mhd_reduced(_ptr(padded), nx, ny, _c_double(dx), _c_double(cfl), _c_double(t_end), steps,
+                                 _c_double(bias), limiter, _ptr(prm), bc, subcycles, reinit, ctypes.byref(st))
+    else:
+        L.vo_run_two_material.restype = _c_double
+        t = L.vo_run_two_material(model, _ptr(padded), nx, ny, _c_double(dx), _c_double(cfl), _c_double(t_end),
+                                  steps, _c_double(bias), limiter, _ptr(prm), bc, reinit, ctypes.byref(st))
     planes[:] = padded[:nw]
     return t, st.value
 

@@ -781,3 +781,99 @@ extern "C" double vgref_multiphysics_run(double* planes, int nx, int ny, double 
 }
 
 
+
+// ------------------------------------------------------------------------------- MHD reduced two-material model
+// planes: the 11 primitive planes of MHDReducedStateVector (alpha1, u, v, w, rho1, rho2, p, Bx, By, Bz, psi;
+// MHD/Multiphysics/mhdreducedstatevector.cpp:91-111); prm = {gamma1, p_inf1, gamma2, p_inf2}.  max_steps <= 0: the
+// reference's own MHDSecondOrderSolver::solve{,2D} to t_end (Solvers/mhdsecondordersolver.cpp:445-495, :615-675);
+// else its per-step functions for max_steps steps in solve's order: c_h of both materials = the padded grid's maximum
+// wave speed, RK4 GLM damping sub-cycles around the sweeps, reinitialisation every reinit_freq steps.
+static MHDReducedStateVector mredCell(const double* planes, long plane, long k) {
+    return MHDReducedStateVector(planes[k], planes[plane + k], planes[2 * plane + k], planes[3 * plane + k],
+                                 planes[4 * plane + k], planes[5 * plane + k], planes[6 * plane + k],
+                                 planes[7 * plane + k], planes[8 * plane + k], planes[9 * plane + k],
+                                 planes[10 * plane + k]);
+}
+static void mredStore(MHDReducedStateVector& c, double* planes, long plane, long k) {
+    vector<double> w = c.computePrimitiveVariableVector();
+    for (int v = 0; v < 11; v++) planes[v * plane + k] = w[v];
+}
+
+extern "C" double vgref_mhd_reduced_run(double* planes, int nx, int ny, double dx, double cfl, double t_end,
+                                        int max_steps, double bias, int limiter, const double* prm, int subcycles,
+                                        int reinit_freq, int* steps_out) {
+    QuietCout quiet;
+    MHDMaterialParameters m1 = mhdParams(prm), m2 = mhdParams(prm + 2);
+    const long plane = (long)nx * ny;
+    double t = 0.0;
+    int it = 0;
+    auto glm = [&](double smax) {
+        m1.setHyperbolicWaveSpeed(smax);
+        m2.setHyperbolicWaveSpeed(smax);
+        m1.configureParabolicDamping();
+        m2.configureParabolicDamping();
+    };
+    if (ny == 1) {
+        vector<MHDReducedStateVector> cells(nx);
+        for (int i = 0; i < nx; i++) cells[i] = mredCell(planes, plane, i);
+        if (max_steps <= 0) {
+            cells = MHDSecondOrderSolver::solve(cells, dx, cfl, t_end, bias, limiter, subcycles, reinit_freq, m1, m2);
+            t = t_end;
+        } else {
+            for (; it < max_steps; it++) {
+                vector<MHDReducedStateVector> withB = MHDSolvers::insertBoundaryCells(cells, 2);
+                double dt = MHDSolvers::computeStableTimeStep(withB, dx, cfl, t, 1.0e300, it, m1, m2);
+                glm(MHDSolvers::computeMaximumWaveSpeed(withB, m1, m2));
+                for (int s = 0; s < subcycles; s++) {
+                    withB = MHDSolvers::insertBoundaryCells(cells, 1);
+                    MHDForcingSolver::computeRungeKuttaTimeStep(cells, withB, dx, 0.5 * (dt / subcycles), bias, limiter, m1, m2);
+                }
+                withB = MHDSolvers::insertBoundaryCells(cells, 2);
+                MHDSecondOrderSolver::computeSLICTimeStep(cells, withB, dx, dt, bias, limiter, m1, m2);
+                for (int s = 0; s < subcycles; s++) {
+                    withB = MHDSolvers::insertBoundaryCells(cells, 1);
+                    MHDForcingSolver::computeRungeKuttaTimeStep(cells, withB, dx, 0.5 * (dt / subcycles), bias, limiter, m1, m2);
+                }
+                t += dt;
+                if (reinit_freq != 0 && ((it + 1) % reinit_freq) == 0)
+                    MultiphysicsSolvers::reinitialiseVolumeFraction(cells, m1, m2);
+            }
+        }
+        for (int i = 0; i < nx; i++) mredStore(cells[i], planes, plane, i);
+    } else {
+        vector<vector<MHDReducedStateVector> > g(ny, vector<MHDReducedStateVector>(nx));
+        for (int i = 0; i < ny; i++)
+            for (int j = 0; j < nx; j++) g[i][j] = mredCell(planes, plane, (long)i * nx + j);
+        if (max_steps <= 0) {
+            g = MHDSecondOrderSolver::solve2D(g, dx, cfl, t_end, bias, limiter, subcycles, reinit_freq, m1, m2);
+            t = t_end;
+        } else {
+            for (; it < max_steps; it++) {
+                vector<vector<MHDReducedStateVector> > withB = MHDSolvers::insertBoundaryCells2D(g, 2);
+                double dt = MHDSolvers::computeStableTimeStep2D(withB, dx, cfl, t, 1.0e300, it, m1, m2);
+                glm(MHDSolvers::computeMaximumWaveSpeed2D(withB, m1, m2));
+                for (int s = 0; s < subcycles; s++) {
+                    withB = MHDSolvers::insertBoundaryCells2D(g, 1);
+                    MHDForcingSolver::computeRungeKuttaTimeStep2D(g, withB, dx, 0.5 * (dt / subcycles), bias, limiter, m1, m2);
+                }
+                withB = MHDSolvers::insertBoundaryCells2D(g, 2);
+                MHDSecondOrderSolver::computeXSLICTimeStep2D(g, withB, dx, 0.5 * dt, bias, limiter, m1, m2);
+                withB = MHDSolvers::insertBoundaryCells2D(g, 2);
+                MHDSecondOrderSolver::computeYSLICTimeStep2D(g, withB, dx, dt, bias, limiter, m1, m2);
+                withB = MHDSolvers::insertBoundaryCells2D(g, 2);
+                MHDSecondOrderSolver::computeXSLICTimeStep2D(g, withB, dx, 0.5 * dt, bias, limiter, m1, m2);
+                for (int s = 0; s < subcycles; s++) {
+                    withB = MHDSolvers::insertBoundaryCells2D(g, 1);
+                    MHDForcingSolver::computeRungeKuttaTimeStep2D(g, withB, dx, 0.5 * (dt / subcycles), bias, limiter, m1, m2);
+                }
+                t += dt;
+                if (reinit_freq != 0 && ((it + 1) % reinit_freq) == 0)
+                    MultiphysicsSolvers::reinitialiseVolumeFraction(g, m1, m2);
+            }
+        }
+        for (int i = 0; i < ny; i++)
+            for (int j = 0; j < nx; j++) mredStore(g[i][j], planes, plane, (long)i * nx + j);
+    }
+    if (steps_out) *steps_out = it;
+    return t;
+}

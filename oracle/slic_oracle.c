@@ -947,6 +947,123 @@ static void mph_default(const double* prm, double* W) {
     W[0] = 0.999; W[1] = 0.0; W[2] = 0.0; W[3] = 0.0; W[4] = 1.0; W[5] = 1.0; W[6] = 1.0; W[7] = 1.0; W[8] = 0.0;
 }
 
+/* ---- MHD reduced two-material model: MHD/Multiphysics/mhdreducedstatevector.cpp, prm = {gamma1, p_inf1, gamma2, p_inf2,
+ * c_h}; c_h is both materials' hyperbolic wave speed (MHDMaterialParameters::setHyperbolicWaveSpeed, which solve{,2D}
+ * sets to the padded grid's maximum wave speed every step).  W = alpha1, u, v, w, rho1, rho2, p, Bx, By, Bz, psi (the
+ * reference's primitive order) and an unused twelfth plane; U = rho, rho alpha1, rho u, rho v, rho w, alpha1 rho1,
+ * alpha2 rho2, E, Bx, By, Bz, psi.  Volume fractions are clamped to [0.001, 0.999] as in the Euler reduced model. */
+/* the mixture c_h^2 (computeHyperbolicWaveSpeedSquared of both materials weighted by the volume fractions) */
+static double mred_ch2(double a1, double a2, const double* prm) {
+    double ch2 = prm[4] * prm[4];
+    return (a1 * ch2) + (a2 * ch2);
+}
+/* computeConservedVariableVector (:113-153) */
+static void mred_cons(const double* W, const double* prm, double* U) {
+    double a1 = red_clamp(W[0]), a2 = 1.0 - a1;
+    double u = W[1], v = W[2], w = W[3], r1 = W[4], r2 = W[5], p = W[6], bx = W[7], by = W[8], bz = W[9];
+    double rho = (a1 * r1) + (a2 * r2);
+    U[0] = rho;
+    U[1] = rho * a1;
+    U[2] = rho * u;
+    U[3] = rho * v;
+    U[4] = rho * w;
+    U[5] = a1 * r1;
+    U[6] = a2 * r2;
+    double v2 = ((u * u) + (v * v)) + (w * w);
+    double b2 = ((bx * bx) + (by * by)) + (bz * bz);
+    double h1 = rho * ((0.5 * v2) + mhd_e(rho, p, prm)), h2 = rho * ((0.5 * v2) + mhd_e(rho, p, prm + 2));
+    U[7] = (a1 * (h1 + (0.5 * b2))) + (a2 * (h2 + (0.5 * b2)));
+    U[8] = bx;
+    U[9] = by;
+    U[10] = bz;
+    U[11] = W[10];
+}
+/* setConservedVariableVector (:58-89) */
+static void mred_setcons(const double* U, const double* prm, double* W) {
+    double rho = U[0];
+    double a1 = red_clamp(U[1] / rho), a2 = 1.0 - a1;
+    double u = U[2] / rho, v = U[3] / rho, w = U[4] / rho;
+    double bx = U[8], by = U[9], bz = U[10];
+    double b2 = ((bx * bx) + (by * by)) + (bz * bz);
+    double E = (U[7] - (0.5 * b2)) / rho;
+    double v2 = ((u * u) + (v * v)) + (w * w);
+    double e = E - (0.5 * v2);
+    W[0] = a1; W[1] = u; W[2] = v; W[3] = w;
+    W[4] = U[5] / a1;
+    W[5] = U[6] / a2;
+    W[6] = (a1 * mhd_p(rho, e, prm)) + (a2 * mhd_p(rho, e, prm + 2));
+    W[7] = bx; W[8] = by; W[9] = bz; W[10] = U[11];
+    W[11] = 0.0;
+}
+/* compute{X,Y}FluxVector(vector, params, params) (:155-232, :239-316); v.B summed from 0.0 as computeDotProduct */
+static void mred_flux(const double* U, int axis, const double* prm, double* F) {
+    double rho = U[0];
+    double a1 = red_clamp(U[1] / rho), a2 = 1.0 - a1;
+    double u = U[2] / rho, v = U[3] / rho, w = U[4] / rho;
+    double r1 = U[5] / a1, r2 = U[6] / a2;
+    double bx = U[8], by = U[9], bz = U[10], psi = U[11];
+    double v2 = ((u * u) + (v * v)) + (w * w);
+    double b2 = ((bx * bx) + (by * by)) + (bz * bz);
+    double E = U[7];
+    double e = ((E - (0.5 * b2)) / rho) - (0.5 * v2);
+    double p = (a1 * mhd_p(rho, e, prm)) + (a2 * mhd_p(rho, e, prm + 2));
+    double ch2 = mred_ch2(a1, a2, prm);
+    double vb = ((0.0 + (u * bx)) + (v * by)) + (w * bz);
+    double un = axis == 0 ? u : v, bn = axis == 0 ? bx : by;
+    F[0] = rho * un;
+    F[1] = rho * (un * a1);
+    F[2] = (rho * (un * u)) - (bn * bx);
+    F[3] = (rho * (un * v)) - (bn * by);
+    F[4] = (rho * (un * w)) - (bn * bz);
+    if (axis == 0) F[2] = (((rho * (u * u)) + p) + (0.5 * b2)) - (bx * bx);
+    else F[3] = (((rho * (v * v)) + p) + (0.5 * b2)) - (by * by);
+    F[5] = a1 * (r1 * un);
+    F[6] = a2 * (r2 * un);
+    F[7] = (((E + p) + (0.5 * b2)) * un) - (vb * bn);
+    if (axis == 0) {
+        F[8] = psi;
+        F[9] = (by * u) - (bx * v);
+    } else {
+        F[8] = (bx * v) - (by * u);
+        F[9] = psi;
+    }
+    F[10] = (bz * un) - (bn * w);
+    F[11] = ch2 * bn;
+}
+/* computeSourceTermVector (:323-347): GLM damping of psi with the mixtures of c_h^2 and of the parabolic damping
+ * c_p^2, c_p = sqrt(c_h * 0.18) (MHDMaterialParameters::configureParabolicDamping, MHD/mhdmaterialparameters.cpp:31-34) */
+static void mred_source(const double* U, const double* prm, double* S) {
+    double rho = U[0];
+    double a1 = red_clamp(U[1] / rho), a2 = 1.0 - a1;
+    double cp = sqrt(prm[4] * 0.18);
+    double cp2 = cp * cp;
+    double ch2 = mred_ch2(a1, a2, prm);
+    double cpm = (a1 * cp2) + (a2 * cp2);
+    for (int i = 0; i < 12; i++) S[i] = 0.0;
+    S[11] = (-(ch2 / cpm)) * U[11];
+}
+/* MHDWaveSpeeds::compute{X,Y}FastMagnetoAcousticSpeed (MHD/mhdwavespeeds.cpp:7-17, :43-63) of material k; the
+ * reference's computeMaterial{1,2}{X,Y}FastMagnetoAcousticSpeed (:393-401, :433-441) both pass material 2's density */
+static double mred_fast(const double* W, const double* mk, double bn) {
+    double V[9] = {W[5], 0.0, 0.0, 0.0, W[6], W[7], W[8], W[9], 0.0};
+    return mhd_fast(V, mk, bn);
+}
+/* MHDSolvers::computeMaximumWaveSpeed{,2D} of the reduced model (Solvers/mhdsolvers.cpp:345-363, :416-440) */
+static double mred_wave1d(const double* W, const double* prm) {
+    return fabs(W[1]) + smax(fabs(mred_fast(W, prm, W[7])), fabs(mred_fast(W, prm + 2, W[7])));
+}
+static double mred_wave2d(const double* W, const double* prm) {
+    return smax(fabs(W[1]), fabs(W[2])) +
+           smax(smax(fabs(mred_fast(W, prm, W[7])), fabs(mred_fast(W, prm, W[8]))),
+                smax(fabs(mred_fast(W, prm + 2, W[7])), fabs(mred_fast(W, prm + 2, W[8]))));
+}
+/* MHDReducedStateVector() (:3-16) */
+static void mred_default(const double* prm, double* W) {
+    (void)prm;
+    for (int i = 0; i < 12; i++) W[i] = 0.0;
+    W[0] = 0.999; W[4] = 1.0; W[5] = 1.0; W[6] = 1.0;
+}
+
 /* A cell of a reinitialisation window: relaxTotalDensity (reduced :281-287, multiphysics :308-314), for the
  * multiphysics model relaxTotalPressure (:316-329, which sets both pressures to the volume-fraction mean), then the
  * volume fraction.  Planes: reduced rho1 4, rho2 5; multiphysics rho1 4, p1 5, rho2 6, p2 7. */
@@ -1003,6 +1120,7 @@ static const model M_MHD = {9, mhd_cons, mhd_setcons, mhd_flux, mhd_wave1d, mhd_
 static const model M_HPR = {17, hpr_cons, hpr_setcons, hpr_flux, hpr_wave1d, hpr_wave2d, hpr_default, hpr_source};
 static const model M_RED = {8, red_cons, red_setcons, red_flux, red_wave1d, red_wave2d, red_default, 0};
 static const model M_MPH = {9, mph_cons, mph_setcons, mph_flux, mph_wave1d, mph_wave2d, mph_default, 0};
+static const model M_MRED = {12, mred_cons, mred_setcons, mred_flux, mred_wave1d, mred_wave2d, mred_default, mred_source};
 
 static const model* model_of(int id) {
     switch (id) {
@@ -1011,13 +1129,14 @@ static const model* model_of(int id) {
         case VO_HPR: return &M_HPR;
         case VO_EULER_REDUCED: return &M_RED;
         case VO_EULER_MULTIPHYSICS: return &M_MPH;
+        case VO_MHD_REDUCED: return &M_MRED;
         default: return NULL;
     }
 }
 
 int vo_nvar(int id) { const model* m = model_of(id); return m ? m->nv : 0; }
 int vo_nparams(int id) {
-    return id == VO_EULER ? 6 : id == VO_MHD ? 3 : id == VO_HPR ? 20 : (id == VO_EULER_REDUCED || id == VO_EULER_MULTIPHYSICS) ? 4 : 0;
+    return id == VO_EULER ? 6 : id == VO_MHD ? 3 : id == VO_HPR ? 20 : (id == VO_EULER_REDUCED || id == VO_EULER_MULTIPHYSICS) ? 4 : id == VO_MHD_REDUCED ? 5 : 0;
 }
 
 /* ------------------------------------------------------------------------------- SLIC building blocks */
@@ -1365,6 +1484,7 @@ static double run(int id, double* planes, int nx, int ny, int dims, double dx, d
         double smax_ = max_wave(m, planes, plane, dims, prm);
         double dt = stable_dt(cfl * (dx / smax_), t, tEnd, it);
         if (id == VO_MHD) prm[2] = smax_;
+        if (id == VO_MHD_REDUCED) prm[4] = smax_;
         if (dt_log) dt_log[it] = dt;
         /* HPR relaxation / MHD GLM damping: sub-cycled RK4 source before and after the sweeps
          * (Solvers/hprsecondordersolver.cpp:323-341, :514-541; Solvers/mhdsecondordersolver.cpp:334-348, :517-540) */
@@ -1382,7 +1502,8 @@ static double run(int id, double* planes, int nx, int ny, int dims, double dx, d
         t += dt;
         it += 1;
         /* the reduced model's solve{,2D}: reinitialisation every reinit_freq steps (Solvers/secondordersolver.cpp) */
-        if ((id == VO_EULER_REDUCED || id == VO_EULER_MULTIPHYSICS) && reinit_freq != 0 && (it % reinit_freq) == 0) {
+        if ((id == VO_EULER_REDUCED || id == VO_EULER_MULTIPHYSICS || id == VO_MHD_REDUCED) && reinit_freq != 0 &&
+            (it % reinit_freq) == 0) {
             g_reinit_mph = id == VO_EULER_MULTIPHYSICS;
             red_reinit(planes, nx, dims == 1 ? 1 : ny);
         }
@@ -1471,6 +1592,12 @@ double vo_run_two_material(int id, double* planes, int nx, int ny, double dx, do
                            double w, int lim, const double* prm, int bc, int reinit_freq, int* steps_out) {
     if (id != VO_EULER_REDUCED && id != VO_EULER_MULTIPHYSICS) return -1.0;
     return run(id, planes, nx, ny, ny > 1 ? 2 : 1, dx, cfl, t_end, max_steps, w, lim, prm, bc, 0,
+               steps_out, NULL, reinit_freq);
+}
+
+double vo_run_mhd_reduced(double* planes, int nx, int ny, double dx, double cfl, double t_end, int max_steps, double w,
+                          int lim, const double* prm, int bc, int subcycles, int reinit_freq, int* steps_out) {
+    return run(VO_MHD_REDUCED, planes, nx, ny, ny > 1 ? 2 : 1, dx, cfl, t_end, max_steps, w, lim, prm, bc, subcycles,
                steps_out, NULL, reinit_freq);
 }
 

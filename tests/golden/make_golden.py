@@ -90,11 +90,32 @@ MULTIPHYSICS_CASES = {
         lambda: wl.multiphysics_from_reduced(wl.reduced_bubble_2d(30, 26)),
         dict(dx=1 / 30, cfl=0.8, steps=9, limiter=O.MINBEE, reinit=3, params=wl.reduced_params(1.4, 0.0, 1.67, 0.0))),
 }
+# The MHD reduced two-material model (model id O.MHD_REDUCED) on MHDReducedTests' Dumbser layouts: one material
+# (gamma 2) and two (1.4, 1.67), RK4 GLM damping sub-cycles, reinitialisation, and one run of the reference's own
+# MHDSecondOrderSolver::solve to t_end (steps = 0).
+MHD_REDUCED_CASES = {
+    "mhdreduced1d_dumbser100_superbee_30": (lambda: wl.mhd_reduced_dumbser_1d(100),
+                                            dict(dx=1 / 100, cfl=0.8, steps=30, limiter=O.SUPERBEE, reinit=0,
+                                                 subcycles=0, params=wl.mhd_reduced_params())),
+    "mhdreduced1d_dumbsermm100_minbee_glm2_reinit4_30": (lambda: wl.mhd_reduced_dumbser_1d(100),
+                                                         dict(dx=1 / 100, cfl=0.8, steps=30, limiter=O.MINBEE,
+                                                              reinit=4, subcycles=2,
+                                                              params=wl.mhd_reduced_params(1.4, 0.0, 1.67, 0.0))),
+    "mhdreduced1d_dumbser60_solve_t01_glm1_reinit5": (lambda: wl.mhd_reduced_dumbser_1d(60),
+                                                      dict(dx=1 / 60, cfl=0.8, t_end=0.1, steps=0, limiter=0,
+                                                           reinit=5, subcycles=1, params=wl.mhd_reduced_params())),
+    "mhdreduced2d_dumbsermm24x20_superbee_glm1_reinit3_6": (lambda: wl.mhd_reduced_dumbser_2d(24, 20),
+                                                            dict(dx=1 / 24, cfl=0.8, steps=6, limiter=O.SUPERBEE,
+                                                                 reinit=3, subcycles=1,
+                                                                 params=wl.mhd_reduced_params(1.4, 0.0, 1.67, 0.0))),
+}
 
 
 def make_two_material(name):
-    model = O.EULER_REDUCED if name in REDUCED_CASES else O.EULER_MULTIPHYSICS
-    init, kw = (REDUCED_CASES if model == O.EULER_REDUCED else MULTIPHYSICS_CASES)[name]
+    model = (O.EULER_REDUCED if name in REDUCED_CASES else O.EULER_MULTIPHYSICS if name in MULTIPHYSICS_CASES
+             else O.MHD_REDUCED)
+    init, kw = {O.EULER_REDUCED: REDUCED_CASES, O.EULER_MULTIPHYSICS: MULTIPHYSICS_CASES,
+                O.MHD_REDUCED: MHD_REDUCED_CASES}[model][name]
     w0 = np.ascontiguousarray(init())
     out = w0.copy()
     kw2 = dict(kw)
@@ -105,7 +126,7 @@ def make_two_material(name):
 
 
 def make(name):
-    if name in REDUCED_CASES or name in MULTIPHYSICS_CASES:
+    if name in REDUCED_CASES or name in MULTIPHYSICS_CASES or name in MHD_REDUCED_CASES:
         return make_two_material(name)
     model, init, kw = CASES[name]
     w0 = np.ascontiguousarray(init())
@@ -119,5 +140,5 @@ def make(name):
 
 
 if __name__ == "__main__":
-    for n in (sys.argv[1:] or list(CASES) + list(REDUCED_CASES) + list(MULTIPHYSICS_CASES)):
+    for n in (sys.argv[1:] or list(CASES) + list(REDUCED_CASES) + list(MULTIPHYSICS_CASES) + list(MHD_REDUCED_CASES)):
         make(n)

@@ -5,13 +5,16 @@
 // Output, in order (float64): Euler 1D solve (6 x 200), Euler 2D per-sweep loop (6 x 24 x 20),
 // MHD solve2D (9 x 16 x 16), HPR solve (17 x 50), Euler 1D step-count solve (6 x 150), Euler 1D first-order solve
 // (6 x 150), HPR GodunovRomenski plastic solve (17 x 60), reduced two-material solve (7 x 120), multiphysics
-// two-material solve (8 x 100), then the number of 2D steps the per-sweep loop took.
+// two-material solve (8 x 100), MHD reduced two-material solve2D (11 x 24 x 24), then the number of 2D steps the
+// per-sweep loop took.
 #include <cmath>
 #include <cstdio>
 #include <vector>
 
 #include "Solvers/firstordersolver.h"
 #include "Solvers/secondordersolver.h"
+#include "Solvers/mhdsecondordersolver.h"
+#include "MHD/Multiphysics/mhdreducedstatevector.h"
 
 using std::vector;
 
@@ -171,6 +174,26 @@ int main(int argc, char** argv) {
         vector<double> v;
         for (int k = 0; k < 8; k++)
             for (auto& c : out) v.push_back(c.computePrimitiveVariableVector()[k]);
+        put(f, v);
+    }
+    // 10) MHDSecondOrderSolver::solve2D of the MHD reduced two-material model (MHDReducedTests::
+    //     solve2DDumbserMultimaterialTest1's layout), gamma 1.4 | 1.67, one GLM sub-cycle, reinitialisation every 3
+    //     steps, 6 steps
+    {
+        int n = 24;
+        vector<vector<MHDReducedStateVector> > cells(n, vector<MHDReducedStateVector>(n));
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) {
+                double r = std::sqrt(((i - (0.5 * n)) * (i - (0.5 * n))) + ((j - (0.5 * n)) * (j - (0.5 * n))));
+                cells[i][j] = r <= 0.2 * n ? MHDReducedStateVector(0.999, 0.0, 0.0, 0.0, 1.0, 0.125, 1.0, 0.75, 1.0, 0.0, 0.0)
+                                           : MHDReducedStateVector(0.001, 0.0, 0.0, 0.0, 1.0, 0.125, 0.1, 0.75, -1.0, 0.0, 0.0);
+            }
+        vector<vector<MHDReducedStateVector> > out = MHDSecondOrderSolver::solve2D(
+            cells, 1.0 / n, 0.8, 1.0, 0.0, 0, 1, 3, MHDMaterialParameters(1.4), MHDMaterialParameters(1.67), 6);
+        vector<double> v;
+        for (int k = 0; k < 11; k++)
+            for (auto& row : out)
+                for (auto& c : row) v.push_back(c.computePrimitiveVariableVector()[k]);
         put(f, v);
     }
     double st = steps;

@@ -110,5 +110,12 @@ def test_shim_driver_matches_oracle(gpu, oracle_lib, tmp_path):
                        params=wl.reduced_params(1.4, 0.0, 1.67, 0.0), reinit=4)
     assert np.array_equal(got, ref)
 
+    # 10) MHDSecondOrderSolver::solve2D of the MHD reduced two-material model, one GLM sub-cycle, reinit every 3 steps
+    got = take((11, 24, 24))
+    ref = wl.mhd_reduced_dumbser_2d(24)
+    O.run_two_material(O.MHD_REDUCED, ref, 1 / 24, 0.8, steps=6, limiter=0, params=wl.mhd_reduced_params(1.4, 0.0, 1.67, 0.0),
+                       reinit=3, subcycles=1)
+    assert np.array_equal(got, ref)
+
     assert take((1,))[0] == 6
     assert off == data.size

@@ -417,4 +417,153 @@ struct EulerMultiphysicsF64 {
     __device__ static double pressure(const double* W) { return W[4] < W[6] ? W[4] : W[6]; }
 };
 
+// ------------------------------------------------------------------------------- MHD reduced two-material
+// MHDReducedStateVector (MHD/Multiphysics/mhdreducedstatevector.cpp) with every plane carried:
+// W = (alpha1, u, v, w, rho1, rho2, p, Bx, By, Bz, psi), U = (rho, rho alpha1, rho u, rho v, rho w, alpha1 rho1,
+// alpha2 rho2, E, Bx, By, Bz, psi).  Params: {gamma1, p_inf1, gamma2, p_inf2}; c_h, the hyperbolic wave speed of both
+// materials, is this step's maximum wave speed as MHDSecondOrderSolver::solve{,2D} sets it (Solvers/
+// mhdsecondordersolver.cpp:454-460), with the parabolic damping c_p = sqrt(c_h * 0.18) (MHD/mhdmaterialparameters.cpp:
+// 31-34).  The GLM coefficients enter as the volume-fraction mixtures of c_h^2 and c_p^2, as the reference forms them.
+struct MHDReducedF64 {
+    static constexpr int NW = 11;
+    static constexpr int NU = 12;
+    static constexpr bool HAS_Y = true;
+    static constexpr bool HAS_SOURCE = true;
+    struct P {
+        double g1, pinf1, g2, pinf2, ch2, cp2;
+    };
+    __device__ static P params(const double* prm, double ch) {
+        const double cp = sqrt(ch * 0.18);
+        return P{prm[0], prm[1], prm[2], prm[3], ch * ch, cp * cp};
+    }
+    // clamp_alpha and the stiffened-gas e(rho, p) / p(rho, e) of MHDEquationOfState (MHD/mhdequationofstate.cpp:7-21),
+    // which are EulerEquationOfState's
+    using R2 = EulerReducedF64;
+
+    __device__ static double b2_of(double bx, double by, double bz) { return ((bx * bx) + (by * by)) + (bz * bz); }
+
+    // computeConservedVariableVector (:113-153)
+    __device__ static void cons(const double* W, const P& q, double* U) {
+        const double a1 = R2::clamp_alpha(W[0]), a2 = 1.0 - a1;
+        const double u = W[1], v = W[2], w = W[3], r1 = W[4], r2 = W[5], p = W[6], bx = W[7], by = W[8], bz = W[9];
+        const double rho = (a1 * r1) + (a2 * r2);
+        U[0] = rho;
+        U[1] = rho * a1;
+        U[2] = rho * u;
+        U[3] = rho * v;
+        U[4] = rho * w;
+        U[5] = a1 * r1;
+        U[6] = a2 * r2;
+        const double v2 = ((u * u) + (v * v)) + (w * w);
+        const double b2 = b2_of(bx, by, bz);
+        const double h1 = rho * ((0.5 * v2) + R2::e_of(rho, p, q.g1, q.pinf1));
+        const double h2 = rho * ((0.5 * v2) + R2::e_of(rho, p, q.g2, q.pinf2));
+        U[7] = (a1 * (h1 + (0.5 * b2))) + (a2 * (h2 + (0.5 * b2)));
+        U[8] = bx;
+        U[9] = by;
+        U[10] = bz;
+        U[11] = W[10];
+    }
+    // setConservedVariableVector (:58-89)
+    __device__ static void setcons(const double* U, const P& q, double* W) {
+        const double rho = U[0];
+        const double a1 = R2::clamp_alpha(U[1] / rho), a2 = 1.0 - a1;
+        const double u = U[2] / rho, v = U[3] / rho, w = U[4] / rho;
+        const double bx = U[8], by = U[9], bz = U[10];
+        const double E = (U[7] - (0.5 * b2_of(bx, by, bz))) / rho;
+        const double e = E - (0.5 * (((u * u) + (v * v)) + (w * w)));
+        W[0] = a1;
+        W[1] = u;
+        W[2] = v;
+        W[3] = w;
+        W[4] = U[5] / a1;
+        W[5] = U[6] / a2;
+        W[6] = (a1 * R2::p_of(rho, e, q.g1, q.pinf1)) + (a2 * R2::p_of(rho, e, q.g2, q.pinf2));
+        W[7] = bx;
+        W[8] = by;
+        W[9] = bz;
+        W[10] = U[11];
+    }
+    // compute{X,Y}FluxVector(vector, params, params) (:155-232, :239-316); v.B summed from 0.0 as
+    // VectorAlgebra::computeDotProduct (Mathematics/vectoralgebra.cpp:38-49)
+    template <int AXIS>
+    __device__ static void flux(const double* U, const P& q, double* F) {
+        const double rho = U[0];
+        const double a1 = R2::clamp_alpha(U[1] / rho), a2 = 1.0 - a1;
+        const double u = U[2] / rho, v = U[3] / rho, w = U[4] / rho;
+        const double r1 = U[5] / a1, r2 = U[6] / a2;
+        const double bx = U[8], by = U[9], bz = U[10], psi = U[11];
+        const double v2 = ((u * u) + (v * v)) + (w * w);
+        const double b2 = b2_of(bx, by, bz);
+        const double E = U[7];
+        const double e = ((E - (0.5 * b2)) / rho) - (0.5 * v2);
+        const double p = (a1 * R2::p_of(rho, e, q.g1, q.pinf1)) + (a2 * R2::p_of(rho, e, q.g2, q.pinf2));
+        const double ch2 = (a1 * q.ch2) + (a2 * q.ch2);
+        const double vb = ((0.0 + (u * bx)) + (v * by)) + (w * bz);
+        const double un = AXIS == 0 ? u : v, bn = AXIS == 0 ? bx : by;
+        F[0] = rho * un;
+        F[1] = rho * (un * a1);
+        if constexpr (AXIS == 0) {
+            F[2] = (((rho * (u * u)) + p) + (0.5 * b2)) - (bx * bx);
+            F[3] = (rho * (u * v)) - (bx * by);
+        } else {
+            F[2] = (rho * (v * u)) - (by * bx);
+            F[3] = (((rho * (v * v)) + p) + (0.5 * b2)) - (by * by);
+        }
+        F[4] = (rho * (un * w)) - (bn * bz);
+        F[5] = a1 * (r1 * un);
+        F[6] = a2 * (r2 * un);
+        F[7] = (((E + p) + (0.5 * b2)) * un) - (vb * bn);
+        if constexpr (AXIS == 0) {
+            F[8] = psi;
+            F[9] = (by * u) - (bx * v);
+        } else {
+            F[8] = (bx * v) - (by * u);
+            F[9] = psi;
+        }
+        F[10] = (bz * un) - (bn * w);
+        F[11] = ch2 * bn;
+    }
+    // computeSourceTermVector (:323-347): GLM damping of psi
+    __device__ static void source(const double* U, const P& q, double* S) {
+#pragma unroll
+        for (int i = 0; i < NU; i++) S[i] = 0.0;
+        const double a1 = R2::clamp_alpha(U[1] / U[0]), a2 = 1.0 - a1;
+        const double ch2 = (a1 * q.ch2) + (a2 * q.ch2), cp2 = (a1 * q.cp2) + (a2 * q.cp2);
+        S[11] = (-(ch2 / cp2)) * U[11];
+    }
+    // MHDWaveSpeeds::compute{X,Y}FastMagnetoAcousticSpeed (MHD/mhdwavespeeds.cpp:7-17, :43-63) of material (g, pinf)
+    // at density rho and normal field bn; the Alfven speed is computeNorm(B) / sqrt(rho), the norm summed from 0.0
+    __device__ static double fast(double rho, double p, double bx, double by, double bz, double g, double pinf,
+                                  double bn) {
+        const double c = sqrt((g * (p + pinf)) / rho);
+        const double a = sqrt(((0.0 + (bx * bx)) + (by * by)) + (bz * bz)) / sqrt(rho);
+        const double c2 = c * c, a2 = a * a;
+        return sqrt(0.5 * ((c2 + a2) + sqrt(((c2 + a2) * (c2 + a2)) - (4.0 * ((c2 * (bn * bn)) / rho)))));
+    }
+    // MHDSolvers::computeMaximumWaveSpeed{,2D} of the reduced model (Solvers/mhdsolvers.cpp:345-363, :416-440).  Both
+    // materials' speeds take material 2's density, as computeMaterial{1,2}{X,Y}FastMagnetoAcousticSpeed (:393-401,
+    // :433-441) do.
+    __device__ static double wave(const double* W, const P& q, int dims) {
+        const double r = W[5], p = W[6], bx = W[7], by = W[8], bz = W[9];
+        const double f1x = fabs(fast(r, p, bx, by, bz, q.g1, q.pinf1, bx));
+        const double f2x = fabs(fast(r, p, bx, by, bz, q.g2, q.pinf2, bx));
+        if (dims == 1) return fabs(W[1]) + std_max(f1x, f2x);
+        const double f1y = fabs(fast(r, p, bx, by, bz, q.g1, q.pinf1, by));
+        const double f2y = fabs(fast(r, p, bx, by, bz, q.g2, q.pinf2, by));
+        return std_max(fabs(W[1]), fabs(W[2])) + std_max(std_max(f1x, f1y), std_max(f2x, f2y));
+    }
+    // MHDReducedStateVector() (:3-16)
+    __device__ static void default_state(double* W) {
+        for (int i = 0; i < NW; i++) W[i] = 0.0;
+        W[0] = 0.999;
+        W[4] = 1.0;
+        W[5] = 1.0;
+        W[6] = 1.0;
+    }
+    // the smaller material density (bad-state check) and the interface pressure
+    __device__ static double density(const double* W) { return W[4] < W[5] ? W[4] : W[5]; }
+    __device__ static double pressure(const double* W) { return W[6]; }
+};
+
 }  // namespace vg

@@ -2,9 +2,10 @@
 // MultiphysicsSolvers::reinitialiseVolumeFraction (Solvers/multiphysicssolvers.cpp:164-191 in 1D, :193-... in 2D),
 // which solve{,2D} call after every reinitialisationFrequency-th step.  In place on a.out (the step's result);
 // the device step counter decides (ctrl->it, already advanced by the step), so the whole time loop stays in one
-// CUDA graph.  MPH selects the multiphysics model: planes alpha1 0, rho1 3, p1 4, rho2 5, p2 6, and its cells also
-// relax both pressures to their volume-fraction mean (relaxTotalPressure); the reduced model's planes are alpha1 0,
-// rho1 3, rho2 4.
+// CUDA graph.  The layout L names the planes of the two densities (L::R1, L::R2) and, for the multiphysics model
+// whose cells also relax both pressures to their volume-fraction mean (relaxTotalPressure), of the two pressures
+// (L::PRESSURE, L::P1, L::P2); alpha1 is plane 0 in every model.  The MHD reduced model's reinitialisation
+// (Solvers/multiphysicssolvers.cpp:656-... in 1D and 2D) is the Euler reduced model's on its own planes.
 //
 // A crossing is a cell j >= 1 with alpha_j < 0.5 <= alpha_{j-1} (descending) or, in 2D, alpha_j > 0.5 >= alpha_{j-1}
 // (ascending).  The four cells j-2 .. j+1 take the mixture density in both materials (relaxTotalDensity) and the
@@ -18,19 +19,32 @@
 
 namespace vg {
 
-// relaxTotalDensity (Euler/Multiphysics/eulerreducedstatevector.cpp:281-287, eulermultiphysicsstatevector.cpp:308-314),
-// for the multiphysics model relaxTotalPressure (:316-329), then the cell's volume fraction
-template <bool MPH>
+struct ReinitEulerReduced {  // alpha1, u, v, rho1, rho2, p
+    static constexpr int R1 = 3, R2 = 4, P1 = 0, P2 = 0;
+    static constexpr bool PRESSURE = false;
+};
+struct ReinitEulerMultiphysics {  // alpha1, u, v, rho1, p1, rho2, p2
+    static constexpr int R1 = 3, R2 = 5, P1 = 4, P2 = 6;
+    static constexpr bool PRESSURE = true;
+};
+struct ReinitMHDReduced {  // alpha1, u, v, w, rho1, rho2, p, Bx, By, Bz, psi
+    static constexpr int R1 = 4, R2 = 5, P1 = 0, P2 = 0;
+    static constexpr bool PRESSURE = false;
+};
+
+// relaxTotalDensity (Euler/Multiphysics/eulerreducedstatevector.cpp:281-287, eulermultiphysicsstatevector.cpp:308-314,
+// MHD/Multiphysics/mhdreducedstatevector.cpp's relaxTotalDensity), for the multiphysics model relaxTotalPressure
+// (:316-329), then the cell's volume fraction
+template <class L>
 __device__ inline void reduced_reset_cell(const SweepArgs& a, long idx, double alpha) {
-    constexpr int I1 = 3, I2 = MPH ? 5 : 4;
     const double a1 = a.out[idx];
-    const double rho = (a1 * a.out[I1 * a.plane + idx]) + ((1.0 - a1) * a.out[I2 * a.plane + idx]);
-    a.out[I1 * a.plane + idx] = rho;
-    a.out[I2 * a.plane + idx] = rho;
-    if constexpr (MPH) {
-        const double p = (a1 * a.out[4 * a.plane + idx]) + ((1.0 - a1) * a.out[6 * a.plane + idx]);
-        a.out[4 * a.plane + idx] = p;
-        a.out[6 * a.plane + idx] = p;
+    const double rho = (a1 * a.out[L::R1 * a.plane + idx]) + ((1.0 - a1) * a.out[L::R2 * a.plane + idx]);
+    a.out[L::R1 * a.plane + idx] = rho;
+    a.out[L::R2 * a.plane + idx] = rho;
+    if constexpr (L::PRESSURE) {
+        const double p = (a1 * a.out[L::P1 * a.plane + idx]) + ((1.0 - a1) * a.out[L::P2 * a.plane + idx]);
+        a.out[L::P1 * a.plane + idx] = p;
+        a.out[L::P2 * a.plane + idx] = p;
     }
     a.out[idx] = alpha;
 }
@@ -39,7 +53,7 @@ __device__ inline bool reduced_reinit_due(const SweepArgs& a) {
     return !a.ctrl || (a.ctrl->active && a.reinit_freq > 0 && (a.ctrl->it % a.reinit_freq) == 0);
 }
 
-template <bool MPH, int NT>
+template <class L, int NT>
 __global__ void __launch_bounds__(NT) reduced_reinit1d_kernel(SweepArgs a) {
     if (!reduced_reinit_due(a)) return;
     __shared__ int part[NT / 32];
@@ -53,12 +67,12 @@ __global__ void __launch_bounds__(NT) reduced_reinit1d_kernel(SweepArgs a) {
         loc = 0;
         for (int w = 0; w < NT / 32; w++) loc = max(loc, part[w]);
         const int i = loc - 2 + (int)threadIdx.x;
-        if (i >= 0 && i < a.nx) reduced_reset_cell<MPH>(a, i, i < loc ? 0.999 : 0.001);
+        if (i >= 0 && i < a.nx) reduced_reset_cell<L>(a, i, i < loc ? 0.999 : 0.001);
     }
 }
 
 // one line (row: stride 1, or column: stride pitch) of the 2D reinitialisation, by one thread
-template <bool MPH>
+template <class L>
 __device__ inline void reduced_reinit_line(const SweepArgs& a, long start, long stride, int len) {
     int loc1[100], loc2[100], n1 = 0, n2 = 0;
     for (int j = 1; j < len; j++) {
@@ -68,35 +82,35 @@ __device__ inline void reduced_reinit_line(const SweepArgs& a, long start, long 
     }
     for (int k = 0; k < n1; k++)
         for (int j = loc1[k] - 2; j < loc1[k] + 2; j++)
-            if (j >= 0 && j < len) reduced_reset_cell<MPH>(a, start + j * stride, j < loc1[k] ? 0.999 : 0.001);
+            if (j >= 0 && j < len) reduced_reset_cell<L>(a, start + j * stride, j < loc1[k] ? 0.999 : 0.001);
     for (int k = 0; k < n2; k++)
         for (int j = loc2[k] - 2; j < loc2[k] + 2; j++)
-            if (j >= 0 && j < len) reduced_reset_cell<MPH>(a, start + j * stride, j < loc2[k] ? 0.001 : 0.999);
+            if (j >= 0 && j < len) reduced_reset_cell<L>(a, start + j * stride, j < loc2[k] ? 0.001 : 0.999);
 }
 
-template <bool MPH>
+template <class L>
 __global__ void reduced_reinit_rows_kernel(SweepArgs a) {
     const int row = blockIdx.x * blockDim.x + threadIdx.x;
     if (row >= a.ny || !reduced_reinit_due(a)) return;
-    reduced_reinit_line<MPH>(a, (long)row * a.pitch, 1, a.nx);
+    reduced_reinit_line<L>(a, (long)row * a.pitch, 1, a.nx);
 }
 
-template <bool MPH>
+template <class L>
 __global__ void reduced_reinit_cols_kernel(SweepArgs a) {
     const int col = blockIdx.x * blockDim.x + threadIdx.x;
     if (col >= a.nx || !reduced_reinit_due(a)) return;
-    reduced_reinit_line<MPH>(a, col, a.pitch, a.ny);
+    reduced_reinit_line<L>(a, col, a.pitch, a.ny);
 }
 
 // The reinitialisation of one step (kernels: 1 in 1D, 2 in 2D), in place on a.out.
-template <bool MPH>
+template <class L>
 inline cudaError_t reduced_reinit(const SweepArgs& a, cudaStream_t st) {
     if (a.ny == 1) {
-        reduced_reinit1d_kernel<MPH, 256><<<1, 256, 0, st>>>(a);
+        reduced_reinit1d_kernel<L, 256><<<1, 256, 0, st>>>(a);
     } else {
         constexpr int T = 64;
-        reduced_reinit_rows_kernel<MPH><<<(a.ny + T - 1) / T, T, 0, st>>>(a);
-        reduced_reinit_cols_kernel<MPH><<<(a.nx + T - 1) / T, T, 0, st>>>(a);
+        reduced_reinit_rows_kernel<L><<<(a.ny + T - 1) / T, T, 0, st>>>(a);
+        reduced_reinit_cols_kernel<L><<<(a.nx + T - 1) / T, T, 0, st>>>(a);
     }
     return cudaGetLastError();
 }

@@ -52,6 +52,7 @@ cudaError_t finish_impl(const SweepArgs& a, double* out, cudaStream_t st) {
 
 template <class M>
 cudaError_t forcing_impl(const SweepArgs& a, int subcycles, cudaStream_t st) {
+    static_assert(M::NU <= aux_planes(M::NW), "the forcing scratch holds aux_planes(NW) conserved planes");
     if (!a.aux) return cudaErrorInvalidValue;
     long n = (long)a.nx * a.ny;
     roundtrip_kernel<M><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a);
@@ -114,6 +115,7 @@ constexpr Ops make_ops() {
                0,
                std::is_same<M, EulerReducedF64>::value        ? &reduced_reinit_fp64
                : std::is_same<M, EulerMultiphysicsF64>::value ? &multiphysics_reinit_fp64
+               : std::is_same<M, MHDReducedF64>::value        ? &mhd_reduced_reinit_fp64
                                                               : nullptr};
 }
 
@@ -126,6 +128,7 @@ const Ops kOps[V_COUNT] = {
     make_ops<HPRSolidF64>(),
     make_ops<EulerReducedF64>(),
     make_ops<EulerMultiphysicsF64>(),
+    make_ops<MHDReducedF64>(),
 };
 
 }  // namespace
@@ -140,8 +143,15 @@ cudaError_t hpr_solid_forcing_fp64(const SweepArgs& a, int subcycles, cudaStream
     return forcing_impl<HPRSolidF64>(a, subcycles, st);
 }
 cudaError_t hpr_solid_relax_fp64(const SweepArgs& a, cudaStream_t st) { return relax_impl<HPRSolidF64>(a, st); }
-cudaError_t reduced_reinit_fp64(const SweepArgs& a, cudaStream_t st) { return reduced_reinit<false>(a, st); }
-cudaError_t multiphysics_reinit_fp64(const SweepArgs& a, cudaStream_t st) { return reduced_reinit<true>(a, st); }
+cudaError_t reduced_reinit_fp64(const SweepArgs& a, cudaStream_t st) {
+    return reduced_reinit<ReinitEulerReduced>(a, st);
+}
+cudaError_t multiphysics_reinit_fp64(const SweepArgs& a, cudaStream_t st) {
+    return reduced_reinit<ReinitEulerMultiphysics>(a, st);
+}
+cudaError_t mhd_reduced_reinit_fp64(const SweepArgs& a, cudaStream_t st) {
+    return reduced_reinit<ReinitMHDReduced>(a, st);
+}
 cudaError_t mhd7_forcing_fp64(const SweepArgs& a, int subcycles, cudaStream_t st) {
     return forcing_impl<MHDF64<false>>(a, subcycles, st);
 }

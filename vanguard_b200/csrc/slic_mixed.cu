@@ -101,6 +101,7 @@ const Ops kOps[V_COUNT] = {
     make_ops<HPRSolidMixed>(&hpr_solid_forcing_fp64, &hpr_solid_relax_fp64),
     make_ops<ReducedMixed>(nullptr, nullptr, &reduced_reinit_fp64),
     Ops{},  // V_MPH7: no mixed form (see ops_mixed)
+    Ops{},  // V_MRED11: no mixed form
 };
 
 }  // namespace

@@ -20,7 +20,8 @@ enum Variant : int {
     V_HPR17S = 5,  // HPR solid (ShockMieGruneisen / GodunovRomenski) or plastic material, same planes
     V_RED6 = 6,    // Euler reduced two-material, w == 0:    alpha1, u, v, rho1, rho2, p
     V_MPH7 = 7,    // Euler multiphysics two-material, w == 0: alpha1, u, v, rho1, p1, rho2, p2
-    V_COUNT = 8
+    V_MRED11 = 8,  // MHD reduced two-material: alpha1, u, v, w, rho1, rho2, p, Bx, By, Bz, psi
+    V_COUNT = 9
 };
 
 struct Ops {
@@ -66,6 +67,12 @@ cudaError_t hpr_solid_relax_fp64(const SweepArgs& a, cudaStream_t st);
 // The reduced model's volume-fraction reinitialisation (slic_fp64.cu), shared by both forms.
 cudaError_t reduced_reinit_fp64(const SweepArgs& a, cudaStream_t st);
 cudaError_t multiphysics_reinit_fp64(const SweepArgs& a, cudaStream_t st);
+cudaError_t mhd_reduced_reinit_fp64(const SweepArgs& a, cudaStream_t st);
+
+// Planes of the source sub-cycles' scratch (SweepArgs::aux), which holds conserved vectors: a model carries at most
+// one conserved component more than primitive planes (the two-material models' rho alpha1), which forcing_impl
+// checks at compile time.
+constexpr int aux_planes(int max_nw) { return max_nw + 1; }
 
 // Record the text returned by vg_last_error_string() on this thread.
 void set_last_error(const std::string& msg);

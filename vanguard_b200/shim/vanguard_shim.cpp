@@ -72,9 +72,9 @@ vg_solver* cached_solver(int model, int nx, int ny, int boundary, const double* 
 void run_planes(int model, std::vector<double>& planes, int nx, int ny, const double* params, int nparams, double dx,
                 double cfl, double tEnd, double bias, int limiter, int subcycles, int maxSteps = 0, int order = 2,
                 int reinit = 0) {
-    // the first-order loop runs in the exact form, bit for bit with the reference; the multiphysics two-material model
-    // has no mixed form
-    const bool exact = order == 1 || model == VG_MODEL_EULER_MULTIPHYSICS;
+    // the first-order loop runs in the exact form, bit for bit with the reference; the Euler multiphysics and MHD
+    // reduced two-material models have no mixed form
+    const bool exact = order == 1 || model == VG_MODEL_EULER_MULTIPHYSICS || model == VG_MODEL_MHD_REDUCED;
     SolverPtr s = make_solver(model, nx, ny, VG_TRANSMISSIVE, params, nparams, exact ? VG_FP64 : -1);
     vg_run_config c{};
     c.dx = dx;
@@ -665,6 +665,69 @@ vector<vector<MHDStateVector> > MHDSecondOrderSolver::solve2D(vector<vector<MHDS
     long ny = initialCells.size(), nx = initialCells[0].size();
     run_planes(VG_MODEL_MHD, p, (int)nx, (int)ny, prm, 3, dx, cfl, tEnd, bias, limiter, subcycles, maxSteps);
     return unpack2<MHDStateVector>(p, nx, ny, 9, mhd_make);
+}
+
+// ------------------------------------------------------------------------------------- MHD reduced model
+MHDReducedStateVector::MHDReducedStateVector()
+    : MHDReducedStateVector(0.999, 0.0, 0.0, 0.0, 1.0, 1.0, 1.0, 0.0, 0.0, 0.0, 0.0) {}
+MHDReducedStateVector::MHDReducedStateVector(double a1, double u, double v, double w, double r1, double r2, double p,
+                                             double bx, double by, double bz, double psi)
+    : w_{a1, u, v, w, r1, r2, p, bx, by, bz, psi} {}
+void MHDReducedStateVector::setPrimitiveVariableVector(vector<double> w) {
+    for (int i = 0; i < 11; i++) w_[i] = w[i];
+}
+vector<double> MHDReducedStateVector::computePrimitiveVariableVector() const { return vector<double>(w_, w_ + 11); }
+
+namespace {
+void mred_get(const MHDReducedStateVector& c, double* w) { std::memcpy(w, c.data(), sizeof(double) * 11); }
+MHDReducedStateVector mred_make(const double* w) {
+    MHDReducedStateVector s;
+    std::memcpy(s.data(), w, sizeof(double) * 11);
+    return s;
+}
+// {gamma1, p_inf1, gamma2, p_inf2, c_h}: the second-order loop replaces c_h every step, as solve{,2D} does
+void mred_params(const MHDMaterialParameters& m1, const MHDMaterialParameters& m2, double* prm) {
+    prm[0] = m1.getAdiabaticIndex(), prm[1] = m1.getStiffeningParameter();
+    prm[2] = m2.getAdiabaticIndex(), prm[3] = m2.getStiffeningParameter();
+    prm[4] = m1.getHyperbolicWaveSpeed();
+}
+}  // namespace
+
+vector<MHDReducedStateVector> MHDSecondOrderSolver::solve(vector<MHDReducedStateVector>& initialCells, double dx,
+                                                          double cfl, double tEnd, double bias, int limiter,
+                                                          int subcycles, int reinit, MHDMaterialParameters m1,
+                                                          MHDMaterialParameters m2) {
+    return solve(initialCells, dx, cfl, tEnd, bias, limiter, subcycles, reinit, m1, m2, 0);
+}
+vector<MHDReducedStateVector> MHDSecondOrderSolver::solve(vector<MHDReducedStateVector>& initialCells, double dx,
+                                                          double cfl, double tEnd, double bias, int limiter,
+                                                          int subcycles, int reinit, MHDMaterialParameters m1,
+                                                          MHDMaterialParameters m2, int maxSteps) {
+    double prm[5];
+    mred_params(m1, m2, prm);
+    std::vector<double> p = pack(initialCells, 11, mred_get);
+    run_planes(VG_MODEL_MHD_REDUCED, p, (int)initialCells.size(), 1, prm, 5, dx, cfl, tEnd, bias, limiter, subcycles,
+               maxSteps, 2, reinit);
+    return unpack<MHDReducedStateVector>(p, initialCells.size(), 11, mred_make);
+}
+vector<vector<MHDReducedStateVector> > MHDSecondOrderSolver::solve2D(vector<vector<MHDReducedStateVector> >& initialCells,
+                                                                     double dx, double cfl, double tEnd, double bias,
+                                                                     int limiter, int subcycles, int reinit,
+                                                                     MHDMaterialParameters m1, MHDMaterialParameters m2) {
+    return solve2D(initialCells, dx, cfl, tEnd, bias, limiter, subcycles, reinit, m1, m2, 0);
+}
+vector<vector<MHDReducedStateVector> > MHDSecondOrderSolver::solve2D(vector<vector<MHDReducedStateVector> >& initialCells,
+                                                                     double dx, double cfl, double tEnd, double bias,
+                                                                     int limiter, int subcycles, int reinit,
+                                                                     MHDMaterialParameters m1, MHDMaterialParameters m2,
+                                                                     int maxSteps) {
+    double prm[5];
+    mred_params(m1, m2, prm);
+    std::vector<double> p = pack2(initialCells, 11, mred_get);
+    long ny = initialCells.size(), nx = initialCells[0].size();
+    run_planes(VG_MODEL_MHD_REDUCED, p, (int)nx, (int)ny, prm, 5, dx, cfl, tEnd, bias, limiter, subcycles, maxSteps, 2,
+               reinit);
+    return unpack2<MHDReducedStateVector>(p, nx, ny, 11, mred_make);
 }
 
 // --------------------------------------------------------------------------------------------- HPR solver

@@ -84,7 +84,6 @@ private:
     double density, xVelocity, yVelocity, zVelocity, pressure, reactionProgress;
 };
 
-// --------------------------------------------------------------------------------------------------- MHD
 // EulerReducedStateVector (Euler/Multiphysics/eulerreducedstatevector.h): the reduced two-material state,
 // primitives alpha1, u, v, w, rho1, rho2, p.
 class EulerReducedStateVector {
@@ -141,6 +140,7 @@ private:
     double w_[8];
 };
 
+// --------------------------------------------------------------------------------------------------- MHD
 class MHDMaterialParameters {
 public:
     MHDMaterialParameters();
@@ -191,6 +191,37 @@ public:
 
 private:
     double w_[9];
+};
+
+// MHDReducedStateVector (MHD/Multiphysics/mhdreducedstatevector.h): the MHD reduced two-material state, primitives
+// alpha1, u, v, w, rho1, rho2, p, Bx, By, Bz, psi.
+class MHDReducedStateVector {
+public:
+    MHDReducedStateVector();
+    MHDReducedStateVector(double newMaterial1VolumeFraction, double newInterfaceXVelocity, double newInterfaceYVelocity,
+                          double newInterfaceZVelocity, double newMaterial1Density, double newMaterial2Density,
+                          double newInterfacePressure, double newInterfaceXMagneticField,
+                          double newInterfaceYMagneticField, double newInterfaceZMagneticField,
+                          double newInterfaceAuxiliaryField);
+    void setPrimitiveVariableVector(vector<double> w);
+    vector<double> computePrimitiveVariableVector() const;
+    double getMaterial1VolumeFraction() const { return w_[0]; }
+    double getInterfaceXVelocity() const { return w_[1]; }
+    double getInterfaceYVelocity() const { return w_[2]; }
+    double getInterfaceZVelocity() const { return w_[3]; }
+    double getMaterial1Density() const { return w_[4]; }
+    double getMaterial2Density() const { return w_[5]; }
+    double getInterfacePressure() const { return w_[6]; }
+    double getInterfaceXMagneticField() const { return w_[7]; }
+    double getInterfaceYMagneticField() const { return w_[8]; }
+    double getInterfaceZMagneticField() const { return w_[9]; }
+    double getInterfaceAuxiliaryField() const { return w_[10]; }
+    void setMaterial1VolumeFraction(double v) { w_[0] = v; }
+    double* data() { return w_; }
+    const double* data() const { return w_; }
+
+private:
+    double w_[11];
 };
 
 // --------------------------------------------------------------------------------------------------- HPR
@@ -385,6 +416,30 @@ public:
     static vector<vector<MHDStateVector> > solve2D(vector<vector<MHDStateVector> >& initialCells, double cellSpacing,
                                                    double CFLCoefficient, double finalTime, double bias, int slopeLimiter,
                                                    int subcyclingIterations, MHDMaterialParameters mp, int maxSteps);
+    // the MHD reduced two-material model (Solvers/mhdsecondordersolver.cpp:445-495, :615-675): c_h of both materials
+    // set every step, RK4 GLM damping sub-cycles, reinitialisation every reinitialisationFrequency steps; exact form
+    static vector<MHDReducedStateVector> solve(vector<MHDReducedStateVector>& initialCells, double cellSpacing,
+                                               double CFLCoefficient, double finalTime, double bias, int slopeLimiter,
+                                               int subcyclingIterations, int reinitialisationFrequency,
+                                               MHDMaterialParameters material1Parameters,
+                                               MHDMaterialParameters material2Parameters);
+    static vector<vector<MHDReducedStateVector> > solve2D(vector<vector<MHDReducedStateVector> >& initialCells,
+                                                          double cellSpacing, double CFLCoefficient, double finalTime,
+                                                          double bias, int slopeLimiter, int subcyclingIterations,
+                                                          int reinitialisationFrequency,
+                                                          MHDMaterialParameters material1Parameters,
+                                                          MHDMaterialParameters material2Parameters);
+    static vector<MHDReducedStateVector> solve(vector<MHDReducedStateVector>& initialCells, double cellSpacing,
+                                               double CFLCoefficient, double finalTime, double bias, int slopeLimiter,
+                                               int subcyclingIterations, int reinitialisationFrequency,
+                                               MHDMaterialParameters material1Parameters,
+                                               MHDMaterialParameters material2Parameters, int maxSteps);
+    static vector<vector<MHDReducedStateVector> > solve2D(vector<vector<MHDReducedStateVector> >& initialCells,
+                                                          double cellSpacing, double CFLCoefficient, double finalTime,
+                                                          double bias, int slopeLimiter, int subcyclingIterations,
+                                                          int reinitialisationFrequency,
+                                                          MHDMaterialParameters material1Parameters,
+                                                          MHDMaterialParameters material2Parameters, int maxSteps);
 };
 
 // FirstOrderSolver / MHDFirstOrderSolver / HPRFirstOrderSolver::solve{,2D} (Solvers/firstordersolver.h:86-97,

@@ -313,3 +313,32 @@ def multiphysics_from_reduced(W):
     out[7] = W[6]
     return out
 
+
+
+MHD_REDUCED_NVAR = 11  # alpha1, u, v, w, rho1, rho2, p, Bx, By, Bz, psi (MHD/Multiphysics/mhdreducedstatevector.cpp:91-111)
+
+
+def mhd_reduced_params(gamma1=2.0, p_inf1=0.0, gamma2=2.0, p_inf2=0.0):
+    """The two MHDMaterialParameters of the MHD reduced model: (gamma1, p_inf1, gamma2, p_inf2).  Dumbser test 1
+    uses gamma 2 for both materials, its multimaterial variant 1.4 and 1.67."""
+    return np.array([gamma1, p_inf1, gamma2, p_inf2])
+
+
+_DUMBSER_IN = (0.999, 0.0, 0.0, 0.0, 1.0, 0.125, 1.0, 0.75, 1.0, 0.0, 0.0)
+_DUMBSER_OUT = (0.001, 0.0, 0.0, 0.0, 1.0, 0.125, 0.1, 0.75, -1.0, 0.0, 0.0)
+
+
+def mhd_reduced_dumbser_1d(n):
+    """MHDReducedTests::solveDumbserTest1's layout (MHD/Multiphysics/mhdreducedtests.cpp:7-27): the Brio-Wu states
+    with material 1 (alpha1 = 0.999) at i <= n/2 and material 2 (0.001) to the right."""
+    left = np.arange(n) <= 0.5 * n
+    return np.stack([np.where(left, a, b) for a, b in zip(_DUMBSER_IN, _DUMBSER_OUT)]).astype(np.float64)
+
+
+def mhd_reduced_dumbser_2d(nx, ny=None, radius=0.2):
+    """MHDReducedTests::solve2DDumbserTest1's layout (:53-76): the left Brio-Wu state inside the disc of radius 0.2 n
+    about the grid centre (row index i, column j), the right one outside."""
+    ny = nx if ny is None else ny
+    I, J = np.meshgrid(np.arange(ny), np.arange(nx), indexing="ij")
+    inside = np.sqrt((I - 0.5 * ny) ** 2 + (J - 0.5 * nx) ** 2) <= radius * nx
+    return np.stack([np.where(inside, a, b) for a, b in zip(_DUMBSER_IN, _DUMBSER_OUT)]).astype(np.float64)
