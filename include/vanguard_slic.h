@@ -18,6 +18,8 @@
  *                                      model, Euler/Multiphysics/eulermultiphysicsstatevector.cpp:32-44 (w = 0)
  *   VG_MODEL_MHD_REDUCED (11 planes): alpha1, u, v, w, rho1, rho2, p, Bx, By, Bz, psi   the MHD reduced
  *                                      two-material model, MHD/Multiphysics/mhdreducedstatevector.cpp:91-111
+ *   VG_MODEL_MHD_INTERMEDIATE (12 planes): alpha1, u, v, w, rho1, p1, rho2, p2, Bx, By, Bz, psi   the MHD
+ *                                      intermediate two-material model, mhdintermediatestatevector.cpp:108-130
  * Ownership: a vg_solver owns all device memory it allocates; the caller owns every host buffer.
  * Threading: calls on different solvers are independent and re-entrant; one solver must not be used
  * from two host threads at once.  All work is enqueued on the stream given (NULL: the legacy default
@@ -48,7 +50,8 @@ typedef enum vg_model {
     VG_MODEL_HPR = 2,
     VG_MODEL_EULER_REDUCED = 3,
     VG_MODEL_EULER_MULTIPHYSICS = 4,
-    VG_MODEL_MHD_REDUCED = 5
+    VG_MODEL_MHD_REDUCED = 5,
+    VG_MODEL_MHD_INTERMEDIATE = 6
 } vg_model;
 
 /* VG_FP64: every operation in float64, in the reference's order, no FMA: matches the reference.
@@ -71,7 +74,8 @@ enum { VG_SUPERBEE = 0, VG_VANLEER = 1, VG_MINBEE = 2 };
  *   MHD:   {gamma, p_inf, c_h}                    MHDMaterialParameters; c_h is recomputed every step by
  *                                                 vg_run as solve() does, and read from here by vg_sweep
  *   Euler reduced, multiphysics: {gamma1, p_inf1, gamma2, p_inf2}   the two materials' EulerMaterialParameters
- *   MHD reduced: {gamma1, p_inf1, gamma2, p_inf2, c_h}   the two materials' MHDMaterialParameters; c_h (both
+ *   MHD reduced, intermediate: {gamma1, p_inf1, gamma2, p_inf2, c_h}   the two materials'
+ *                                                 MHDMaterialParameters; c_h (both
  *                                                 materials) as MHD's: recomputed every step by the second-order
  *                                                 loop, read from here by the first-order loop and vg_sweep
  *   HPR:   {gamma, p_inf, c_v, rho0, T0, c_s, alpha, tau1, tau2, T_ref, p_ref, is_thermal,
@@ -103,8 +107,8 @@ typedef struct vg_run_config {
     int subcycles;      /* subcyclingIterations (source integration; HPR, MHD and MHD reduced; second order only) */
     int order;          /* 2 (or 0): SecondOrderSolver's SLIC loop; 1: FirstOrderSolver's FORCE loop
                          * (Solvers/firstordersolver.cpp:435-553 and the MHD / HPR twins: 1-ghost boundary, FORCE
-                         * of the cells themselves, no source, the MHD c_h kept at params[2], the MHD reduced
-                         * model's at params[4]; both forms) */
+                         * of the cells themselves, no source, the MHD c_h kept at params[2], the MHD two-material
+                         * models' at params[4]; both forms) */
     int stiff_source;   /* HPR only, no counterpart in the reference: 1 replaces the RK4 forcing sub-cycles by a
                          * stiff relaxation of dt/2 before and after the sweeps, cell by cell (distortion by implicit
                          * Euler on the eigenvalues of A^T A, heat flux by exponential sub-steps), stable at any tau;
@@ -123,7 +127,7 @@ typedef struct vg_solver vg_solver;
 vg_status vg_create(const vg_grid_desc* desc, vg_solver** out);
 vg_status vg_destroy(vg_solver* s);
 
-/* Number of primitive planes the model takes at this boundary (6, 9, 17, 7, 8, 11). */
+/* Number of primitive planes the model takes at this boundary (6, 9, 17, 7, 8, 11, 12). */
 int vg_model_nvar(int model);
 
 /* Copy the state in / out.  planes: vg_model_nvar(model) planes of nx*ny float64, host or device

@@ -23,7 +23,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libvgref.so")
 
-EULER, MHD, HPR, EULER_REDUCED, EULER_MULTIPHYSICS, MHD_REDUCED = 0, 1, 2, 3, 4, 5
+EULER, MHD, HPR, EULER_REDUCED, EULER_MULTIPHYSICS, MHD_REDUCED, MHD_INTERMEDIATE = 0, 1, 2, 3, 4, 5, 6
 NVAR = {EULER: 6, MHD: 9, HPR: 17}
 TRANSMISSIVE, PERIODIC = 0, 1
 SUPERBEE, VANLEER, MINBEE = 0, 1, 2
@@ -238,19 +238,21 @@ def hpr_cell(w, params, reference=False):
     return (*outs, sp)
 
 
-_TWO_MATERIAL_NW = {EULER_REDUCED: 7, EULER_MULTIPHYSICS: 8, MHD_REDUCED: 11}
+_TWO_MATERIAL_NW = {EULER_REDUCED: 7, EULER_MULTIPHYSICS: 8, MHD_REDUCED: 11, MHD_INTERMEDIATE: 12}
+_MHD_TWO_MATERIAL = (MHD_REDUCED, MHD_INTERMEDIATE)
 
 
 def run_two_material(model, planes, dx, cfl, t_end=0.0, steps=0, bias=0.0, limiter=SUPERBEE, params=None, reinit=0,
                      reference=False, threads=1, bc=TRANSMISSIVE, subcycles=0):
     """(MHD)SecondOrderSolver::solve{,2D} of a two-material model on its primitive planes, in place: EULER_REDUCED
     (7 planes: alpha1, u, v, w, rho1, rho2, p), EULER_MULTIPHYSICS (8: alpha1, u, v, w, rho1, p1, rho2, p2) or
-    MHD_REDUCED (11: alpha1, u, v, w, rho1, rho2, p, Bx, By, Bz, psi), x (n) or (ny, nx); from the restatement or
-    (reference=True) the reference.  params = (gamma1, p_inf1, gamma2, p_inf2); reinit > 0 reinitialises the volume
-    fraction every `reinit` steps; subcycles > 0 (MHD_REDUCED) adds the RK4 GLM damping sub-cycles.
+    MHD_REDUCED (11: alpha1, u, v, w, rho1, rho2, p, Bx, By, Bz, psi) or MHD_INTERMEDIATE (12: alpha1, u, v, w, rho1,
+    p1, rho2, p2, Bx, By, Bz, psi), x (n) or (ny, nx); from the restatement or (reference=True) the reference.
+    params = (gamma1, p_inf1, gamma2, p_inf2); reinit > 0 reinitialises the volume fraction every `reinit` steps;
+    subcycles > 0 (the MHD models) adds the RK4 GLM damping sub-cycles.
     Returns (t, steps)."""
     nw = _TWO_MATERIAL_NW[model]
-    assert subcycles == 0 or model == MHD_REDUCED, "only the MHD reduced model has a source"
+    assert subcycles == 0 or model in _MHD_TWO_MATERIAL, "only the MHD two-material models have a source"
     assert planes.shape[0] == nw and planes.dtype == np.float64 and planes.flags.c_contiguous
     nx = planes.shape[-1]
     ny = 1 if planes.ndim == 2 else planes.shape[1]
@@ -260,8 +262,11 @@ def run_two_material(model, planes, dx, cfl, t_end=0.0, steps=0, bias=0.0, limit
         assert bc == TRANSMISSIVE, "the reference's two-material models have transmissive boundaries only"
         R = ref()
         R.vgref_set_threads(threads)
-        if model == MHD_REDUCED:
-            fn = R.vgref_mhd_reduced_run
+        if model in _MHD_TWO_MATERIAL:
+            # the intermediate model's own solve2D pads with its defective insertBoundaryCells2D
+            # (Solvers/mhdsolvers.cpp:213); the harness's per-step loop builds mirror ghosts instead
+            assert not (model == MHD_INTERMEDIATE and ny > 1 and steps <= 0), "2D intermediate: per-step runs only"
+            fn = R.vgref_mhd_reduced_run if model == MHD_REDUCED else R.vgref_mhd_intermediate_run
             fn.restype = _c_double
             t = fn(_ptr(planes), nx, ny, _c_double(dx), _c_double(cfl), _c_double(t_end), steps, _c_double(bias),
                    limiter, _ptr(prm), subcycles, reinit, ctypes.byref(st))
@@ -274,10 +279,11 @@ def run_two_material(model, planes, dx, cfl, t_end=0.0, steps=0, bias=0.0, limit
     padded = np.zeros((nw + 1,) + planes.shape[1:])  # the restatement carries one unused plane
     padded[:nw] = planes
     L = lib()
-    if model == MHD_REDUCED:
-        L.vo_run_mhd_reduced.restype = _c_double
-        t = L.vo_run_mhd_reduced(_ptr(padded), nx, ny, _c_double(dx), _c_double(cfl), _c_double(t_end), steps,
-                                 _c_double(bias), limiter, _ptr(prm), bc, subcycles, reinit, ctypes.byref(st))
+    if model in _MHD_TWO_MATERIAL:
+        L.vo_run_mhd_two_material.restype = _c_double
+        t = L.vo_run_mhd_two_material(model, _ptr(padded), nx, ny, _c_double(dx), _c_double(cfl), _c_double(t_end),
+                                      steps, _c_double(bias), limiter, _ptr(prm), bc, subcycles, reinit,
+                                      ctypes.byref(st))
     else:
         L.vo_run_two_material.restype = _c_double
         t = L.vo_run_two_material(model, _ptr(padded), nx, ny, _c_double(dx), _c_double(cfl), _c_double(t_end),

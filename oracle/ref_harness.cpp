@@ -42,6 +42,7 @@
 #include <omp.h>
 #include <iostream>
 #include <limits>
+#include <type_traits>
 #include <vector>
 
 using std::vector;
@@ -104,6 +105,28 @@ vector<vector<S> > periodicGhosts2D(vector<vector<S> >& c, int b) {
         for (int k = 0; k < b; k++) {
             g[k][j + b] = c[ny - b + k][j];
             g[ny + b + k][j + b] = c[k][j];
+        }
+    return g;
+}
+
+// The reference's transmissive ghosts (insertBoundaryCells2D: g[-1-k] = c[k], g[n+k] = c[n-1-k], corner blocks
+// default-constructed), built here for the MHD intermediate model, whose own insertBoundaryCells2D fills the outermost
+// bottom row from the padded grid instead of the cells (Solvers/mhdsolvers.cpp:213).
+template <class S>
+vector<vector<S> > mirrorGhosts2D(vector<vector<S> >& c, int b) {
+    int ny = c.size(), nx = c[0].size();
+    vector<vector<S> > g(ny + 2 * b, vector<S>(nx + 2 * b));
+    for (int i = 0; i < ny; i++)
+        for (int j = 0; j < nx; j++) g[i + b][j + b] = c[i][j];
+    for (int i = 0; i < ny; i++)
+        for (int k = 0; k < b; k++) {
+            g[i + b][b - 1 - k] = c[i][k];
+            g[i + b][nx + b + k] = c[i][nx - 1 - k];
+        }
+    for (int j = 0; j < nx; j++)
+        for (int k = 0; k < b; k++) {
+            g[b - 1 - k][j + b] = c[k][j];
+            g[ny + b + k][j + b] = c[ny - 1 - k][j];
         }
     return g;
 }
@@ -782,26 +805,42 @@ extern "C" double vgref_multiphysics_run(double* planes, int nx, int ny, double 
 
 
 
-// ------------------------------------------------------------------------------- MHD reduced two-material model
-// planes: the 11 primitive planes of MHDReducedStateVector (alpha1, u, v, w, rho1, rho2, p, Bx, By, Bz, psi;
-// MHD/Multiphysics/mhdreducedstatevector.cpp:91-111); prm = {gamma1, p_inf1, gamma2, p_inf2}.  max_steps <= 0: the
-// reference's own MHDSecondOrderSolver::solve{,2D} to t_end (Solvers/mhdsecondordersolver.cpp:445-495, :615-675);
-// else its per-step functions for max_steps steps in solve's order: c_h of both materials = the padded grid's maximum
-// wave speed, RK4 GLM damping sub-cycles around the sweeps, reinitialisation every reinit_freq steps.
-static MHDReducedStateVector mredCell(const double* planes, long plane, long k) {
+// ---------------------------------------------------------------- MHD reduced and intermediate two-material models
+// planes: the primitive planes of MHDReducedStateVector (11: alpha1, u, v, w, rho1, rho2, p, Bx, By, Bz, psi;
+// MHD/Multiphysics/mhdreducedstatevector.cpp:91-111) or of MHDIntermediateStateVector (12: alpha1, u, v, w, rho1, p1,
+// rho2, p2, Bx, By, Bz, psi; MHD/Multiphysics/mhdintermediatestatevector.cpp:108-130); prm = {gamma1, p_inf1, gamma2,
+// p_inf2}.  max_steps <= 0: the reference's own MHDSecondOrderSolver::solve{,2D} to t_end (Solvers/
+// mhdsecondordersolver.cpp:387-440, :445-495, :552-..., :615-675); else its per-step functions for max_steps steps in
+// solve's order: c_h of both materials = the padded grid's maximum wave speed, RK4 GLM damping sub-cycles around the
+// sweeps, reinitialisation every reinit_freq steps.  The intermediate model in 2D: per-step only (its solve2D pads the
+// grid with the defective insertBoundaryCells2D, see mirrorGhosts2D), with mirror ghosts built here.
+template <class SV>
+static SV mhdTwoCell(const double* planes, long plane, long k);
+template <>
+MHDReducedStateVector mhdTwoCell<MHDReducedStateVector>(const double* planes, long plane, long k) {
     return MHDReducedStateVector(planes[k], planes[plane + k], planes[2 * plane + k], planes[3 * plane + k],
                                  planes[4 * plane + k], planes[5 * plane + k], planes[6 * plane + k],
                                  planes[7 * plane + k], planes[8 * plane + k], planes[9 * plane + k],
                                  planes[10 * plane + k]);
 }
-static void mredStore(MHDReducedStateVector& c, double* planes, long plane, long k) {
+template <>
+MHDIntermediateStateVector mhdTwoCell<MHDIntermediateStateVector>(const double* planes, long plane, long k) {
+    MHDIntermediateStateVector c;
+    vector<double> w(12);
+    for (int v = 0; v < 12; v++) w[v] = planes[v * plane + k];
+    c.setPrimitiveVariableVector(w);
+    return c;
+}
+template <class SV>
+static void mhdTwoStore(SV& c, double* planes, long plane, long k) {
     vector<double> w = c.computePrimitiveVariableVector();
-    for (int v = 0; v < 11; v++) planes[v * plane + k] = w[v];
+    for (size_t v = 0; v < w.size(); v++) planes[v * plane + k] = w[v];
 }
 
-extern "C" double vgref_mhd_reduced_run(double* planes, int nx, int ny, double dx, double cfl, double t_end,
-                                        int max_steps, double bias, int limiter, const double* prm, int subcycles,
-                                        int reinit_freq, int* steps_out) {
+template <class SV>
+static double mhdTwoMaterialRun(double* planes, int nx, int ny, double dx, double cfl, double t_end, int max_steps,
+                                double bias, int limiter, const double* prm, int subcycles, int reinit_freq,
+                                int* steps_out) {
     QuietCout quiet;
     MHDMaterialParameters m1 = mhdParams(prm), m2 = mhdParams(prm + 2);
     const long plane = (long)nx * ny;
@@ -814,14 +853,14 @@ extern "C" double vgref_mhd_reduced_run(double* planes, int nx, int ny, double d
         m2.configureParabolicDamping();
     };
     if (ny == 1) {
-        vector<MHDReducedStateVector> cells(nx);
-        for (int i = 0; i < nx; i++) cells[i] = mredCell(planes, plane, i);
+        vector<SV> cells(nx);
+        for (int i = 0; i < nx; i++) cells[i] = mhdTwoCell<SV>(planes, plane, i);
         if (max_steps <= 0) {
             cells = MHDSecondOrderSolver::solve(cells, dx, cfl, t_end, bias, limiter, subcycles, reinit_freq, m1, m2);
             t = t_end;
         } else {
             for (; it < max_steps; it++) {
-                vector<MHDReducedStateVector> withB = MHDSolvers::insertBoundaryCells(cells, 2);
+                vector<SV> withB = MHDSolvers::insertBoundaryCells(cells, 2);
                 double dt = MHDSolvers::computeStableTimeStep(withB, dx, cfl, t, 1.0e300, it, m1, m2);
                 glm(MHDSolvers::computeMaximumWaveSpeed(withB, m1, m2));
                 for (int s = 0; s < subcycles; s++) {
@@ -839,31 +878,36 @@ extern "C" double vgref_mhd_reduced_run(double* planes, int nx, int ny, double d
                     MultiphysicsSolvers::reinitialiseVolumeFraction(cells, m1, m2);
             }
         }
-        for (int i = 0; i < nx; i++) mredStore(cells[i], planes, plane, i);
+        for (int i = 0; i < nx; i++) mhdTwoStore(cells[i], planes, plane, i);
     } else {
-        vector<vector<MHDReducedStateVector> > g(ny, vector<MHDReducedStateVector>(nx));
+        vector<vector<SV> > g(ny, vector<SV>(nx));
         for (int i = 0; i < ny; i++)
-            for (int j = 0; j < nx; j++) g[i][j] = mredCell(planes, plane, (long)i * nx + j);
+            for (int j = 0; j < nx; j++) g[i][j] = mhdTwoCell<SV>(planes, plane, (long)i * nx + j);
         if (max_steps <= 0) {
             g = MHDSecondOrderSolver::solve2D(g, dx, cfl, t_end, bias, limiter, subcycles, reinit_freq, m1, m2);
             t = t_end;
         } else {
+            // the intermediate model's own 2-ghost insertion has the defect above: mirror ghosts built here instead
+            auto ghosts = [&](vector<vector<SV> >& c, int b) {
+                return (b == 2 && std::is_same<SV, MHDIntermediateStateVector>::value) ? mirrorGhosts2D(c, b)
+                                                                                       : MHDSolvers::insertBoundaryCells2D(c, b);
+            };
             for (; it < max_steps; it++) {
-                vector<vector<MHDReducedStateVector> > withB = MHDSolvers::insertBoundaryCells2D(g, 2);
+                vector<vector<SV> > withB = ghosts(g, 2);
                 double dt = MHDSolvers::computeStableTimeStep2D(withB, dx, cfl, t, 1.0e300, it, m1, m2);
                 glm(MHDSolvers::computeMaximumWaveSpeed2D(withB, m1, m2));
                 for (int s = 0; s < subcycles; s++) {
-                    withB = MHDSolvers::insertBoundaryCells2D(g, 1);
+                    withB = ghosts(g, 1);
                     MHDForcingSolver::computeRungeKuttaTimeStep2D(g, withB, dx, 0.5 * (dt / subcycles), bias, limiter, m1, m2);
                 }
-                withB = MHDSolvers::insertBoundaryCells2D(g, 2);
+                withB = ghosts(g, 2);
                 MHDSecondOrderSolver::computeXSLICTimeStep2D(g, withB, dx, 0.5 * dt, bias, limiter, m1, m2);
-                withB = MHDSolvers::insertBoundaryCells2D(g, 2);
+                withB = ghosts(g, 2);
                 MHDSecondOrderSolver::computeYSLICTimeStep2D(g, withB, dx, dt, bias, limiter, m1, m2);
-                withB = MHDSolvers::insertBoundaryCells2D(g, 2);
+                withB = ghosts(g, 2);
                 MHDSecondOrderSolver::computeXSLICTimeStep2D(g, withB, dx, 0.5 * dt, bias, limiter, m1, m2);
                 for (int s = 0; s < subcycles; s++) {
-                    withB = MHDSolvers::insertBoundaryCells2D(g, 1);
+                    withB = ghosts(g, 1);
                     MHDForcingSolver::computeRungeKuttaTimeStep2D(g, withB, dx, 0.5 * (dt / subcycles), bias, limiter, m1, m2);
                 }
                 t += dt;
@@ -872,8 +916,22 @@ extern "C" double vgref_mhd_reduced_run(double* planes, int nx, int ny, double d
             }
         }
         for (int i = 0; i < ny; i++)
-            for (int j = 0; j < nx; j++) mredStore(g[i][j], planes, plane, (long)i * nx + j);
+            for (int j = 0; j < nx; j++) mhdTwoStore(g[i][j], planes, plane, (long)i * nx + j);
     }
     if (steps_out) *steps_out = it;
     return t;
+}
+
+extern "C" double vgref_mhd_reduced_run(double* planes, int nx, int ny, double dx, double cfl, double t_end,
+                                        int max_steps, double bias, int limiter, const double* prm, int subcycles,
+                                        int reinit_freq, int* steps_out) {
+    return mhdTwoMaterialRun<MHDReducedStateVector>(planes, nx, ny, dx, cfl, t_end, max_steps, bias, limiter, prm,
+                                                    subcycles, reinit_freq, steps_out);
+}
+
+extern "C" double vgref_mhd_intermediate_run(double* planes, int nx, int ny, double dx, double cfl, double t_end,
+                                             int max_steps, double bias, int limiter, const double* prm, int subcycles,
+                                             int reinit_freq, int* steps_out) {
+    return mhdTwoMaterialRun<MHDIntermediateStateVector>(planes, nx, ny, dx, cfl, t_end, max_steps, bias, limiter,
+                                                         prm, subcycles, reinit_freq, steps_out);
 }

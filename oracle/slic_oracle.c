@@ -1064,6 +1064,118 @@ static void mred_default(const double* prm, double* W) {
     W[0] = 0.999; W[4] = 1.0; W[5] = 1.0; W[6] = 1.0;
 }
 
+/* ---- MHD intermediate two-material model: MHD/Multiphysics/mhdintermediatestatevector.cpp, prm as the MHD reduced
+ * model's.  W = alpha1, u, v, w, rho1, p1, rho2, p2, Bx, By, Bz, psi (the reference's primitive order) and an unused
+ * thirteenth plane; U = rho, rho alpha1, rho u, rho v, rho w, alpha1 rho1, alpha1 E1, alpha2 rho2, alpha2 E2, Bx, By,
+ * Bz, psi, E_k the material's total energy with the shared magnetic energy. */
+/* computeConservedVariableVector (:131-185) */
+static void mint_cons(const double* W, const double* prm, double* U) {
+    double a1 = red_clamp(W[0]), a2 = 1.0 - a1;
+    double u = W[1], v = W[2], w = W[3], r1 = W[4], p1 = W[5], r2 = W[6], p2 = W[7], bx = W[8], by = W[9], bz = W[10];
+    double rho = (a1 * r1) + (a2 * r2);
+    U[0] = rho;
+    U[1] = rho * a1;
+    U[2] = rho * u;
+    U[3] = rho * v;
+    U[4] = rho * w;
+    U[5] = a1 * r1;
+    U[7] = a2 * r2;
+    double b2 = ((bx * bx) + (by * by)) + (bz * bz);
+    double v2 = ((u * u) + (v * v)) + (w * w);
+    double h1 = r1 * ((0.5 * v2) + mhd_e(r1, p1, prm)), h2 = r2 * ((0.5 * v2) + mhd_e(r2, p2, prm + 2));
+    U[6] = a1 * (h1 + (0.5 * b2));
+    U[8] = a2 * (h2 + (0.5 * b2));
+    U[9] = bx;
+    U[10] = by;
+    U[11] = bz;
+    U[12] = W[11];
+}
+/* setConservedVariableVector (:49-106) */
+static void mint_setcons(const double* U, const double* prm, double* W) {
+    double rho = U[0];
+    double a1 = red_clamp(U[1] / rho), a2 = 1.0 - a1;
+    double u = U[2] / rho, v = U[3] / rho, w = U[4] / rho;
+    double r1 = U[5] / a1, r2 = U[7] / a2;
+    double bx = U[9], by = U[10], bz = U[11];
+    double b2 = ((bx * bx) + (by * by)) + (bz * bz);
+    double v2 = ((u * u) + (v * v)) + (w * w);
+    double e1 = ((((U[6] / a1) - (0.5 * b2)) / r1)) - (0.5 * v2);
+    double e2 = ((((U[8] / a2) - (0.5 * b2)) / r2)) - (0.5 * v2);
+    W[0] = a1; W[1] = u; W[2] = v; W[3] = w;
+    W[4] = r1; W[5] = mhd_p(r1, e1, prm);
+    W[6] = r2; W[7] = mhd_p(r2, e2, prm + 2);
+    W[8] = bx; W[9] = by; W[10] = bz; W[11] = U[12];
+    W[12] = 0.0;
+}
+/* compute{X,Y}FluxVector(vector, params, params) (:187-279, :286-378) */
+static void mint_flux(const double* U, int axis, const double* prm, double* F) {
+    double rho = U[0];
+    double a1 = red_clamp(U[1] / rho), a2 = 1.0 - a1;
+    double u = U[2] / rho, v = U[3] / rho, w = U[4] / rho;
+    double r1 = U[5] / a1, r2 = U[7] / a2;
+    double bx = U[9], by = U[10], bz = U[11], psi = U[12];
+    double v2 = ((u * u) + (v * v)) + (w * w);
+    double b2 = ((bx * bx) + (by * by)) + (bz * bz);
+    double E1 = U[6] / a1, E2 = U[8] / a2;
+    double p1 = mhd_p(r1, ((E1 - (0.5 * b2)) / r1) - (0.5 * v2), prm);
+    double p2 = mhd_p(r2, ((E2 - (0.5 * b2)) / r2) - (0.5 * v2), prm + 2);
+    double ch2 = mred_ch2(a1, a2, prm);
+    double vb = ((0.0 + (u * bx)) + (v * by)) + (w * bz);
+    double un = axis == 0 ? u : v, bn = axis == 0 ? bx : by;
+    double pm = (a1 * p1) + (a2 * p2);
+    F[0] = rho * un;
+    F[1] = rho * (un * a1);
+    F[2] = (rho * (un * u)) - (bn * bx);
+    F[3] = (rho * (un * v)) - (bn * by);
+    F[4] = (rho * (un * w)) - (bn * bz);
+    if (axis == 0) F[2] = (((rho * (u * u)) + pm) + (0.5 * b2)) - (bx * bx);
+    else F[3] = (((rho * (v * v)) + pm) + (0.5 * b2)) - (by * by);
+    F[5] = a1 * (r1 * un);
+    F[7] = a2 * (r2 * un);
+    F[6] = (a1 * (((E1 + p1) + (0.5 * b2)) * un)) - (a1 * (vb * bn));
+    F[8] = (a2 * (((E2 + p2) + (0.5 * b2)) * un)) - (a2 * (vb * bn));
+    if (axis == 0) {
+        F[9] = psi;
+        F[10] = (by * u) - (bx * v);
+    } else {
+        F[9] = (bx * v) - (by * u);
+        F[10] = psi;
+    }
+    F[11] = (bz * un) - (bn * w);
+    F[12] = ch2 * bn;
+}
+/* computeSourceTermVector (:385-403): GLM damping of psi, as the reduced model's */
+static void mint_source(const double* U, const double* prm, double* S) {
+    double rho = U[0];
+    double a1 = red_clamp(U[1] / rho), a2 = 1.0 - a1;
+    double cp = sqrt(prm[4] * 0.18);
+    double cp2 = cp * cp;
+    double ch2 = mred_ch2(a1, a2, prm);
+    double cpm = (a1 * cp2) + (a2 * cp2);
+    for (int i = 0; i < 13; i++) S[i] = 0.0;
+    S[12] = (-(ch2 / cpm)) * U[12];
+}
+/* compute{X,Y}FastMagnetoAcousticSpeed of material k at its own density and pressure (:453-511) */
+static double mint_fast(const double* W, int k, const double* prm, double bn) {
+    double V[9] = {W[4 + 2 * k], 0.0, 0.0, 0.0, W[5 + 2 * k], W[8], W[9], W[10], 0.0};
+    return mhd_fast(V, prm + 2 * k, bn);
+}
+/* MHDSolvers::computeMaximumWaveSpeed{,2D} of the intermediate model (Solvers/mhdsolvers.cpp:325-343, :390-414) */
+static double mint_wave1d(const double* W, const double* prm) {
+    return fabs(W[1]) + smax(fabs(mint_fast(W, 0, prm, W[8])), fabs(mint_fast(W, 1, prm, W[8])));
+}
+static double mint_wave2d(const double* W, const double* prm) {
+    return smax(fabs(W[1]), fabs(W[2])) +
+           smax(smax(fabs(mint_fast(W, 0, prm, W[8])), fabs(mint_fast(W, 0, prm, W[9]))),
+                smax(fabs(mint_fast(W, 1, prm, W[8])), fabs(mint_fast(W, 1, prm, W[9]))));
+}
+/* MHDIntermediateStateVector() (:3-22) */
+static void mint_default(const double* prm, double* W) {
+    (void)prm;
+    for (int i = 0; i < 13; i++) W[i] = 0.0;
+    W[0] = 0.999; W[4] = 1.0; W[5] = 1.0; W[6] = 1.0; W[7] = 1.0;
+}
+
 /* A cell of a reinitialisation window: relaxTotalDensity (reduced :281-287, multiphysics :308-314), for the
  * multiphysics model relaxTotalPressure (:316-329, which sets both pressures to the volume-fraction mean), then the
  * volume fraction.  Planes: reduced rho1 4, rho2 5; multiphysics rho1 4, p1 5, rho2 6, p2 7. */
@@ -1121,6 +1233,7 @@ static const model M_HPR = {17, hpr_cons, hpr_setcons, hpr_flux, hpr_wave1d, hpr
 static const model M_RED = {8, red_cons, red_setcons, red_flux, red_wave1d, red_wave2d, red_default, 0};
 static const model M_MPH = {9, mph_cons, mph_setcons, mph_flux, mph_wave1d, mph_wave2d, mph_default, 0};
 static const model M_MRED = {12, mred_cons, mred_setcons, mred_flux, mred_wave1d, mred_wave2d, mred_default, mred_source};
+static const model M_MINT = {13, mint_cons, mint_setcons, mint_flux, mint_wave1d, mint_wave2d, mint_default, mint_source};
 
 static const model* model_of(int id) {
     switch (id) {
@@ -1130,13 +1243,14 @@ static const model* model_of(int id) {
         case VO_EULER_REDUCED: return &M_RED;
         case VO_EULER_MULTIPHYSICS: return &M_MPH;
         case VO_MHD_REDUCED: return &M_MRED;
+        case VO_MHD_INTERMEDIATE: return &M_MINT;
         default: return NULL;
     }
 }
 
 int vo_nvar(int id) { const model* m = model_of(id); return m ? m->nv : 0; }
 int vo_nparams(int id) {
-    return id == VO_EULER ? 6 : id == VO_MHD ? 3 : id == VO_HPR ? 20 : (id == VO_EULER_REDUCED || id == VO_EULER_MULTIPHYSICS) ? 4 : id == VO_MHD_REDUCED ? 5 : 0;
+    return id == VO_EULER ? 6 : id == VO_MHD ? 3 : id == VO_HPR ? 20 : (id == VO_EULER_REDUCED || id == VO_EULER_MULTIPHYSICS) ? 4 : (id == VO_MHD_REDUCED || id == VO_MHD_INTERMEDIATE) ? 5 : 0;
 }
 
 /* ------------------------------------------------------------------------------- SLIC building blocks */
@@ -1484,7 +1598,7 @@ static double run(int id, double* planes, int nx, int ny, int dims, double dx, d
         double smax_ = max_wave(m, planes, plane, dims, prm);
         double dt = stable_dt(cfl * (dx / smax_), t, tEnd, it);
         if (id == VO_MHD) prm[2] = smax_;
-        if (id == VO_MHD_REDUCED) prm[4] = smax_;
+        if (id == VO_MHD_REDUCED || id == VO_MHD_INTERMEDIATE) prm[4] = smax_;
         if (dt_log) dt_log[it] = dt;
         /* HPR relaxation / MHD GLM damping: sub-cycled RK4 source before and after the sweeps
          * (Solvers/hprsecondordersolver.cpp:323-341, :514-541; Solvers/mhdsecondordersolver.cpp:334-348, :517-540) */
@@ -1502,9 +1616,10 @@ static double run(int id, double* planes, int nx, int ny, int dims, double dx, d
         t += dt;
         it += 1;
         /* the reduced model's solve{,2D}: reinitialisation every reinit_freq steps (Solvers/secondordersolver.cpp) */
-        if ((id == VO_EULER_REDUCED || id == VO_EULER_MULTIPHYSICS || id == VO_MHD_REDUCED) && reinit_freq != 0 &&
-            (it % reinit_freq) == 0) {
-            g_reinit_mph = id == VO_EULER_MULTIPHYSICS;
+        if ((id == VO_EULER_REDUCED || id == VO_EULER_MULTIPHYSICS || id == VO_MHD_REDUCED ||
+             id == VO_MHD_INTERMEDIATE) && reinit_freq != 0 && (it % reinit_freq) == 0) {
+            /* the multiphysics and MHD intermediate models also relax the pressures (planes 5 and 7) */
+            g_reinit_mph = id == VO_EULER_MULTIPHYSICS || id == VO_MHD_INTERMEDIATE;
             red_reinit(planes, nx, dims == 1 ? 1 : ny);
         }
     }
@@ -1595,9 +1710,11 @@ double vo_run_two_material(int id, double* planes, int nx, int ny, double dx, do
                steps_out, NULL, reinit_freq);
 }
 
-double vo_run_mhd_reduced(double* planes, int nx, int ny, double dx, double cfl, double t_end, int max_steps, double w,
-                          int lim, const double* prm, int bc, int subcycles, int reinit_freq, int* steps_out) {
-    return run(VO_MHD_REDUCED, planes, nx, ny, ny > 1 ? 2 : 1, dx, cfl, t_end, max_steps, w, lim, prm, bc, subcycles,
+double vo_run_mhd_two_material(int id, double* planes, int nx, int ny, double dx, double cfl, double t_end,
+                                int max_steps, double w, int lim, const double* prm, int bc, int subcycles,
+                                int reinit_freq, int* steps_out) {
+    if (id != VO_MHD_REDUCED && id != VO_MHD_INTERMEDIATE) return -1.0;
+    return run(id, planes, nx, ny, ny > 1 ? 2 : 1, dx, cfl, t_end, max_steps, w, lim, prm, bc, subcycles,
                steps_out, NULL, reinit_freq);
 }
 

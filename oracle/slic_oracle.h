@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-enum { VO_EULER = 0, VO_MHD = 1, VO_HPR = 2, VO_EULER_REDUCED = 3, VO_EULER_MULTIPHYSICS = 4, VO_MHD_REDUCED = 5 };
+enum { VO_EULER = 0, VO_MHD = 1, VO_HPR = 2, VO_EULER_REDUCED = 3, VO_EULER_MULTIPHYSICS = 4, VO_MHD_REDUCED = 5, VO_MHD_INTERMEDIATE = 6 };
 enum { VO_BC_TRANSMISSIVE = 0, VO_BC_PERIODIC = 1 };
 
 /* Number of primitive planes of a model (6, 9, 17). */
@@ -64,11 +64,13 @@ void vo_forcing(int model, double* planes, int nx, int ny, double dx, double dt,
  * rho2, p, unused) or VO_EULER_MULTIPHYSICS (9 planes: alpha1, u, v, w, rho1, p1, rho2, p2, unused), prm = {gamma1,
  * p_inf1, gamma2, p_inf2}; reinit_freq > 0 reinitialises the volume fraction every reinit_freq steps
  * (MultiphysicsSolvers::reinitialiseVolumeFraction). */
-/* MHDSecondOrderSolver::solve{,2D} of the MHD reduced two-material model, id VO_MHD_REDUCED (12 planes: alpha1, u, v,
- * w, rho1, rho2, p, Bx, By, Bz, psi, unused), prm = {gamma1, p_inf1, gamma2, p_inf2, c_h (set every step)}: RK4 GLM
- * damping sub-cycles around the sweeps and the volume-fraction reinitialisation every reinit_freq steps. */
-double vo_run_mhd_reduced(double* planes, int nx, int ny, double dx, double cfl, double t_end, int max_steps, double w,
-                          int lim, const double* prm, int bc, int subcycles, int reinit_freq, int* steps_out);
+/* MHDSecondOrderSolver::solve{,2D} of the MHD two-material models, id VO_MHD_REDUCED (12 planes: alpha1, u, v, w, rho1,
+ * rho2, p, Bx, By, Bz, psi, unused) or VO_MHD_INTERMEDIATE (13 planes: alpha1, u, v, w, rho1, p1, rho2, p2, Bx, By, Bz,
+ * psi, unused), prm = {gamma1, p_inf1, gamma2, p_inf2, c_h (set every step)}: RK4 GLM damping sub-cycles around the
+ * sweeps and the volume-fraction reinitialisation every reinit_freq steps. */
+double vo_run_mhd_two_material(int id, double* planes, int nx, int ny, double dx, double cfl, double t_end,
+                                int max_steps, double w, int lim, const double* prm, int bc, int subcycles,
+                                int reinit_freq, int* steps_out);
 double vo_run_two_material(int id, double* planes, int nx, int ny, double dx, double cfl, double t_end, int max_steps,
                            double w, int lim, const double* prm, int bc, int reinit_freq, int* steps_out);
 

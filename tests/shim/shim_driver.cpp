@@ -5,8 +5,8 @@
 // Output, in order (float64): Euler 1D solve (6 x 200), Euler 2D per-sweep loop (6 x 24 x 20),
 // MHD solve2D (9 x 16 x 16), HPR solve (17 x 50), Euler 1D step-count solve (6 x 150), Euler 1D first-order solve
 // (6 x 150), HPR GodunovRomenski plastic solve (17 x 60), reduced two-material solve (7 x 120), multiphysics
-// two-material solve (8 x 100), MHD reduced two-material solve2D (11 x 24 x 24), then the number of 2D steps the
-// per-sweep loop took.
+// two-material solve (8 x 100), MHD reduced two-material solve2D (11 x 24 x 24), MHD intermediate two-material solve
+// (12 x 80), then the number of 2D steps the per-sweep loop took.
 #include <cmath>
 #include <cstdio>
 #include <vector>
@@ -15,6 +15,7 @@
 #include "Solvers/secondordersolver.h"
 #include "Solvers/mhdsecondordersolver.h"
 #include "MHD/Multiphysics/mhdreducedstatevector.h"
+#include "MHD/Multiphysics/mhdintermediatestatevector.h"
 
 using std::vector;
 
@@ -194,6 +195,24 @@ int main(int argc, char** argv) {
         for (int k = 0; k < 11; k++)
             for (auto& row : out)
                 for (auto& c : row) v.push_back(c.computePrimitiveVariableVector()[k]);
+        put(f, v);
+    }
+    // 11) MHDSecondOrderSolver::solve of the MHD intermediate two-material model, gamma 1.4 | 1.67, one GLM sub-cycle,
+    //     reinitialisation every 5 steps, to t = 0.05
+    {
+        int n = 80;
+        vector<MHDIntermediateStateVector> cells(n);
+        for (int i = 0; i < n; i++) {
+            bool left = i <= 0.5 * n;
+            cells[i].setPrimitiveVariableVector(left ? vector<double>{0.999, 0.0, 0.0, 0.0, 1.0, 1.0, 0.125, 1.0, 0.75, 1.0, 0.0, 0.0}
+                                                     : vector<double>{0.001, 0.0, 0.0, 0.0, 1.0, 0.1, 0.125, 0.1, 0.75, -1.0, 0.0, 0.0});
+        }
+        vector<MHDIntermediateStateVector> out = MHDSecondOrderSolver::solve(cells, 1.0 / n, 0.8, 0.05, 0.0, 2, 1, 5,
+                                                                             MHDMaterialParameters(1.4),
+                                                                             MHDMaterialParameters(1.67));
+        vector<double> v;
+        for (int k = 0; k < 12; k++)
+            for (auto& c : out) v.push_back(c.computePrimitiveVariableVector()[k]);
         put(f, v);
     }
     double st = steps;

@@ -117,5 +117,12 @@ def test_shim_driver_matches_oracle(gpu, oracle_lib, tmp_path):
                        reinit=3, subcycles=1)
     assert np.array_equal(got, ref)
 
+    # 11) MHDSecondOrderSolver::solve of the MHD intermediate two-material model to t = 0.05
+    got = take((12, 80))
+    ref = wl.mhd_intermediate_from_reduced(wl.mhd_reduced_dumbser_1d(80))
+    O.run_two_material(O.MHD_INTERMEDIATE, ref, 1 / 80, 0.8, t_end=0.05, limiter=2,
+                       params=wl.mhd_reduced_params(1.4, 0.0, 1.67, 0.0), reinit=5, subcycles=1)
+    assert np.array_equal(got, ref)
+
     assert take((1,))[0] == 6
     assert off == data.size

@@ -566,4 +566,145 @@ struct MHDReducedF64 {
     __device__ static double pressure(const double* W) { return W[6]; }
 };
 
+// ------------------------------------------------------------------------ MHD intermediate two-material
+// MHDIntermediateStateVector (MHD/Multiphysics/mhdintermediatestatevector.cpp), every plane carried:
+// W = (alpha1, u, v, w, rho1, p1, rho2, p2, Bx, By, Bz, psi), U = (rho, rho alpha1, rho u, rho v, rho w, alpha1 rho1,
+// alpha1 E1, alpha2 rho2, alpha2 E2, Bx, By, Bz, psi), E_k the material's total energy with the shared magnetic energy.
+// Params and GLM coefficients as MHDReducedF64's.
+struct MHDIntermediateF64 {
+    static constexpr int NW = 12;
+    static constexpr int NU = 13;
+    static constexpr bool HAS_Y = true;
+    static constexpr bool HAS_SOURCE = true;
+    using P = MHDReducedF64::P;
+    using R2 = EulerReducedF64;
+    using MR = MHDReducedF64;
+    __device__ static P params(const double* prm, double ch) { return MR::params(prm, ch); }
+
+    // computeConservedVariableVector (:131-185)
+    __device__ static void cons(const double* W, const P& q, double* U) {
+        const double a1 = R2::clamp_alpha(W[0]), a2 = 1.0 - a1;
+        const double u = W[1], v = W[2], w = W[3], r1 = W[4], p1 = W[5], r2 = W[6], p2 = W[7];
+        const double bx = W[8], by = W[9], bz = W[10];
+        U[0] = (a1 * r1) + (a2 * r2);
+        U[1] = U[0] * a1;
+        U[2] = U[0] * u;
+        U[3] = U[0] * v;
+        U[4] = U[0] * w;
+        U[5] = a1 * r1;
+        U[7] = a2 * r2;
+        const double b2 = MR::b2_of(bx, by, bz);
+        const double v2 = ((u * u) + (v * v)) + (w * w);
+        const double h1 = r1 * ((0.5 * v2) + R2::e_of(r1, p1, q.g1, q.pinf1));
+        const double h2 = r2 * ((0.5 * v2) + R2::e_of(r2, p2, q.g2, q.pinf2));
+        U[6] = a1 * (h1 + (0.5 * b2));
+        U[8] = a2 * (h2 + (0.5 * b2));
+        U[9] = bx;
+        U[10] = by;
+        U[11] = bz;
+        U[12] = W[11];
+    }
+    // setConservedVariableVector (:49-106)
+    __device__ static void setcons(const double* U, const P& q, double* W) {
+        const double rho = U[0];
+        const double a1 = R2::clamp_alpha(U[1] / rho), a2 = 1.0 - a1;
+        const double u = U[2] / rho, v = U[3] / rho, w = U[4] / rho;
+        const double r1 = U[5] / a1, r2 = U[7] / a2;
+        const double bx = U[9], by = U[10], bz = U[11];
+        const double b2 = MR::b2_of(bx, by, bz);
+        const double v2 = ((u * u) + (v * v)) + (w * w);
+        const double e1 = (((U[6] / a1) - (0.5 * b2)) / r1) - (0.5 * v2);
+        const double e2 = (((U[8] / a2) - (0.5 * b2)) / r2) - (0.5 * v2);
+        W[0] = a1;
+        W[1] = u;
+        W[2] = v;
+        W[3] = w;
+        W[4] = r1;
+        W[5] = R2::p_of(r1, e1, q.g1, q.pinf1);
+        W[6] = r2;
+        W[7] = R2::p_of(r2, e2, q.g2, q.pinf2);
+        W[8] = bx;
+        W[9] = by;
+        W[10] = bz;
+        W[11] = U[12];
+    }
+    // compute{X,Y}FluxVector(vector, params, params) (:187-279, :286-378)
+    template <int AXIS>
+    __device__ static void flux(const double* U, const P& q, double* F) {
+        const double rho = U[0];
+        const double a1 = R2::clamp_alpha(U[1] / rho), a2 = 1.0 - a1;
+        const double u = U[2] / rho, v = U[3] / rho, w = U[4] / rho;
+        const double r1 = U[5] / a1, r2 = U[7] / a2;
+        const double bx = U[9], by = U[10], bz = U[11], psi = U[12];
+        const double v2 = ((u * u) + (v * v)) + (w * w);
+        const double b2 = MR::b2_of(bx, by, bz);
+        const double E1 = U[6] / a1, E2 = U[8] / a2;
+        const double p1 = R2::p_of(r1, ((E1 - (0.5 * b2)) / r1) - (0.5 * v2), q.g1, q.pinf1);
+        const double p2 = R2::p_of(r2, ((E2 - (0.5 * b2)) / r2) - (0.5 * v2), q.g2, q.pinf2);
+        const double ch2 = (a1 * q.ch2) + (a2 * q.ch2);
+        const double vb = ((0.0 + (u * bx)) + (v * by)) + (w * bz);
+        const double un = AXIS == 0 ? u : v, bn = AXIS == 0 ? bx : by;
+        const double pm = (a1 * p1) + (a2 * p2);
+        F[0] = rho * un;
+        F[1] = rho * (un * a1);
+        if constexpr (AXIS == 0) {
+            F[2] = (((rho * (u * u)) + pm) + (0.5 * b2)) - (bx * bx);
+            F[3] = (rho * (u * v)) - (bx * by);
+        } else {
+            F[2] = (rho * (v * u)) - (by * bx);
+            F[3] = (((rho * (v * v)) + pm) + (0.5 * b2)) - (by * by);
+        }
+        F[4] = (rho * (un * w)) - (bn * bz);
+        F[5] = a1 * (r1 * un);
+        F[6] = (a1 * (((E1 + p1) + (0.5 * b2)) * un)) - (a1 * (vb * bn));
+        F[7] = a2 * (r2 * un);
+        F[8] = (a2 * (((E2 + p2) + (0.5 * b2)) * un)) - (a2 * (vb * bn));
+        if constexpr (AXIS == 0) {
+            F[9] = psi;
+            F[10] = (by * u) - (bx * v);
+        } else {
+            F[9] = (bx * v) - (by * u);
+            F[10] = psi;
+        }
+        F[11] = (bz * un) - (bn * w);
+        F[12] = ch2 * bn;
+    }
+    // computeSourceTermVector (:385-403): GLM damping of psi, as the reduced model's
+    __device__ static void source(const double* U, const P& q, double* S) {
+#pragma unroll
+        for (int i = 0; i < NU; i++) S[i] = 0.0;
+        const double a1 = R2::clamp_alpha(U[1] / U[0]), a2 = 1.0 - a1;
+        const double ch2 = (a1 * q.ch2) + (a2 * q.ch2), cp2 = (a1 * q.cp2) + (a2 * q.cp2);
+        S[12] = (-(ch2 / cp2)) * U[12];
+    }
+    // MHDSolvers::computeMaximumWaveSpeed{,2D} of the intermediate model (Solvers/mhdsolvers.cpp:325-343, :389-414);
+    // each material's fast speed at its own density and pressure (:453-511)
+    __device__ static double wave(const double* W, const P& q, int dims) {
+        const double bx = W[8], by = W[9], bz = W[10];
+        const double f1x = fabs(MR::fast(W[4], W[5], bx, by, bz, q.g1, q.pinf1, bx));
+        const double f2x = fabs(MR::fast(W[6], W[7], bx, by, bz, q.g2, q.pinf2, bx));
+        if (dims == 1) return fabs(W[1]) + std_max(f1x, f2x);
+        const double f1y = fabs(MR::fast(W[4], W[5], bx, by, bz, q.g1, q.pinf1, by));
+        const double f2y = fabs(MR::fast(W[6], W[7], bx, by, bz, q.g2, q.pinf2, by));
+        return std_max(fabs(W[1]), fabs(W[2])) + std_max(std_max(f1x, f1y), std_max(f2x, f2y));
+    }
+    // MHDIntermediateStateVector() (:3-22)
+    __device__ static void default_state(double* W) {
+        for (int i = 0; i < NW; i++) W[i] = 0.0;
+        W[0] = 0.999;
+        W[4] = 1.0;
+        W[5] = 1.0;
+        W[6] = 1.0;
+        W[7] = 1.0;
+    }
+    // bad-state check: the smaller material density and the volume-fraction mixture pressure.  The trace material's
+    // own pressure (alpha clamped at 0.001) goes negative in the reference's runs of this model while the mixture stays
+    // physical, so it is not checked on its own.
+    __device__ static double density(const double* W) { return W[4] < W[6] ? W[4] : W[6]; }
+    __device__ static double pressure(const double* W) {
+        const double a1 = R2::clamp_alpha(W[0]);
+        return (a1 * W[5]) + ((1.0 - a1) * W[7]);
+    }
+};
+
 }  // namespace vg

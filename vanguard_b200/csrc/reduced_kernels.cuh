@@ -5,7 +5,8 @@
 // CUDA graph.  The layout L names the planes of the two densities (L::R1, L::R2) and, for the multiphysics model
 // whose cells also relax both pressures to their volume-fraction mean (relaxTotalPressure), of the two pressures
 // (L::PRESSURE, L::P1, L::P2); alpha1 is plane 0 in every model.  The MHD reduced model's reinitialisation
-// (Solvers/multiphysicssolvers.cpp:656-... in 1D and 2D) is the Euler reduced model's on its own planes.
+// (Solvers/multiphysicssolvers.cpp:656-... in 1D and 2D) is the Euler reduced model's on its own planes, the MHD
+// intermediate model's (:499-...) the multiphysics model's.
 //
 // A crossing is a cell j >= 1 with alpha_j < 0.5 <= alpha_{j-1} (descending) or, in 2D, alpha_j > 0.5 >= alpha_{j-1}
 // (ascending).  The four cells j-2 .. j+1 take the mixture density in both materials (relaxTotalDensity) and the
@@ -30,6 +31,10 @@ struct ReinitEulerMultiphysics {  // alpha1, u, v, rho1, p1, rho2, p2
 struct ReinitMHDReduced {  // alpha1, u, v, w, rho1, rho2, p, Bx, By, Bz, psi
     static constexpr int R1 = 4, R2 = 5, P1 = 0, P2 = 0;
     static constexpr bool PRESSURE = false;
+};
+struct ReinitMHDIntermediate {  // alpha1, u, v, w, rho1, p1, rho2, p2, Bx, By, Bz, psi
+    static constexpr int R1 = 4, R2 = 6, P1 = 5, P2 = 7;
+    static constexpr bool PRESSURE = true;
 };
 
 // relaxTotalDensity (Euler/Multiphysics/eulerreducedstatevector.cpp:281-287, eulermultiphysicsstatevector.cpp:308-314,

@@ -116,6 +116,7 @@ constexpr Ops make_ops() {
                std::is_same<M, EulerReducedF64>::value        ? &reduced_reinit_fp64
                : std::is_same<M, EulerMultiphysicsF64>::value ? &multiphysics_reinit_fp64
                : std::is_same<M, MHDReducedF64>::value        ? &mhd_reduced_reinit_fp64
+               : std::is_same<M, MHDIntermediateF64>::value   ? &mhd_intermediate_reinit_fp64
                                                               : nullptr};
 }
 
@@ -129,6 +130,7 @@ const Ops kOps[V_COUNT] = {
     make_ops<EulerReducedF64>(),
     make_ops<EulerMultiphysicsF64>(),
     make_ops<MHDReducedF64>(),
+    make_ops<MHDIntermediateF64>(),
 };
 
 }  // namespace
@@ -151,6 +153,9 @@ cudaError_t multiphysics_reinit_fp64(const SweepArgs& a, cudaStream_t st) {
 }
 cudaError_t mhd_reduced_reinit_fp64(const SweepArgs& a, cudaStream_t st) {
     return reduced_reinit<ReinitMHDReduced>(a, st);
+}
+cudaError_t mhd_intermediate_reinit_fp64(const SweepArgs& a, cudaStream_t st) {
+    return reduced_reinit<ReinitMHDIntermediate>(a, st);
 }
 cudaError_t mhd7_forcing_fp64(const SweepArgs& a, int subcycles, cudaStream_t st) {
     return forcing_impl<MHDF64<false>>(a, subcycles, st);

@@ -102,6 +102,7 @@ const Ops kOps[V_COUNT] = {
     make_ops<ReducedMixed>(nullptr, nullptr, &reduced_reinit_fp64),
     Ops{},  // V_MPH7: no mixed form (see ops_mixed)
     Ops{},  // V_MRED11: no mixed form
+    Ops{},  // V_MINT12: no mixed form
 };
 
 }  // namespace

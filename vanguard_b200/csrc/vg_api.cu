@@ -42,7 +42,8 @@ vg_status cuda_fail(cudaError_t e, const char* what) {
 
 int ref_nvar(int model) {
     return model == VG_MODEL_EULER ? 6 : model == VG_MODEL_MHD ? 9 : model == VG_MODEL_HPR ? 17 : model == VG_MODEL_EULER_REDUCED ? 7
-           : model == VG_MODEL_EULER_MULTIPHYSICS ? 8 : model == VG_MODEL_MHD_REDUCED ? 11 : 0;
+           : model == VG_MODEL_EULER_MULTIPHYSICS ? 8 : model == VG_MODEL_MHD_REDUCED ? 11
+           : model == VG_MODEL_MHD_INTERMEDIATE ? 12 : 0;
 }
 
 // Reference plane carried in device plane k, per variant.
@@ -56,6 +57,7 @@ const int kPlanes[vg::V_COUNT][17] = {
     {0, 1, 2, 4, 5, 6},             // V_RED6: alpha1, u, v, rho1, rho2, p
     {0, 1, 2, 4, 5, 6, 7},          // V_MPH7: alpha1, u, v, rho1, p1, rho2, p2
     {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10},  // V_MRED11: every plane
+    {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11},  // V_MINT12: every plane
 };
 
 }  // namespace
@@ -219,8 +221,9 @@ SweepArgs base_args(const vg_solver* s) {
     for (int i = 0; i < VG_MAX_PARAMS - 1; i++) a.params[i] = s->d.params[i];
     a.params[VG_MAX_PARAMS - 1] = 1.0 / (s->d.params[0] - 1.0);
     static_assert(vg::kParams == VG_MAX_PARAMS, "device parameter block must match VG_MAX_PARAMS");
-    // the first-order loop's fixed GLM speed: MHD params[2], MHD reduced params[4] (both materials)
-    a.ch_host = s->d.model == VG_MODEL_MHD_REDUCED ? s->d.params[4] : s->d.params[2];
+    // the first-order loop's fixed GLM speed: MHD params[2], the MHD two-material models params[4] (both materials)
+    a.ch_host = (s->d.model == VG_MODEL_MHD_REDUCED || s->d.model == VG_MODEL_MHD_INTERMEDIATE) ? s->d.params[4]
+                                                                                              : s->d.params[2];
     return a;
 }
 
@@ -404,7 +407,7 @@ vg_status vg_create(const vg_grid_desc* desc, vg_solver** out) {
     *out = nullptr;
     if (desc->model != VG_MODEL_EULER && desc->model != VG_MODEL_MHD && desc->model != VG_MODEL_HPR &&
         desc->model != VG_MODEL_EULER_REDUCED && desc->model != VG_MODEL_EULER_MULTIPHYSICS &&
-        desc->model != VG_MODEL_MHD_REDUCED)
+        desc->model != VG_MODEL_MHD_REDUCED && desc->model != VG_MODEL_MHD_INTERMEDIATE)
         return fail(VG_EUNSUPPORTED, "model not available in this build");
     if (desc->nx < 2 || desc->ny < 1 || (desc->ny > 1 && desc->ny < 2))
         return fail(VG_EINVAL, "grid needs at least 2 cells along every swept axis");
@@ -415,8 +418,8 @@ vg_status vg_create(const vg_grid_desc* desc, vg_solver** out) {
     if (desc->precision == VG_MIXED && desc->model == VG_MODEL_EULER_MULTIPHYSICS)
         return fail(VG_EUNSUPPORTED, "the multiphysics two-material model runs in VG_FP64 only (its trace material's "
                                      "energy is not stable under FP32 flux values)");
-    if (desc->precision == VG_MIXED && desc->model == VG_MODEL_MHD_REDUCED)
-        return fail(VG_EUNSUPPORTED, "the MHD reduced two-material model runs in VG_FP64 only");
+    if (desc->precision == VG_MIXED && (desc->model == VG_MODEL_MHD_REDUCED || desc->model == VG_MODEL_MHD_INTERMEDIATE))
+        return fail(VG_EUNSUPPORTED, "the MHD two-material models run in VG_FP64 only");
     if (desc->model == VG_MODEL_HPR) {
         const double eos = desc->params[12];
         if (eos != 0.0 && eos != 1.0 && eos != 2.0)
@@ -429,7 +432,8 @@ vg_status vg_create(const vg_grid_desc* desc, vg_solver** out) {
     s->d = *desc;
     s->dims = desc->ny > 1 ? 2 : 1;
     s->max_nw = desc->model == VG_MODEL_EULER ? 4 : desc->model == VG_MODEL_MHD ? 9 : desc->model == VG_MODEL_EULER_REDUCED ? 6
-                : desc->model == VG_MODEL_EULER_MULTIPHYSICS ? 7 : desc->model == VG_MODEL_MHD_REDUCED ? 11 : 17;
+                : desc->model == VG_MODEL_EULER_MULTIPHYSICS ? 7 : desc->model == VG_MODEL_MHD_REDUCED ? 11
+                : desc->model == VG_MODEL_MHD_INTERMEDIATE ? 12 : 17;
     s->pitch = ((long)desc->nx + 31) / 32 * 32;  // 256-byte aligned rows
     s->plane = s->pitch * desc->ny;
     s->floor5 = std::pow(10.0, -5.0);  // SlopeLimiters::computeSlopeVector's floor (Solvers/slopelimiters.cpp:232-239)
@@ -496,6 +500,8 @@ vg_status vg_upload_primitive(vg_solver* s, const double* planes, int is_device,
         variant = s->d.model == VG_MODEL_EULER_REDUCED ? vg::V_RED6 : vg::V_MPH7;
     } else if (s->d.model == VG_MODEL_MHD_REDUCED) {
         variant = vg::V_MRED11;
+    } else if (s->d.model == VG_MODEL_MHD_INTERMEDIATE) {
+        variant = vg::V_MINT12;
     } else if (s->d.model == VG_MODEL_HPR) {
         // a solid equation of state or plasticity selects the instantiation that carries them
         variant = (s->d.params[12] != 0.0 || s->d.params[17] != 0.0) ? vg::V_HPR17S : vg::V_HPR17;

@@ -21,7 +21,8 @@ enum Variant : int {
     V_RED6 = 6,    // Euler reduced two-material, w == 0:    alpha1, u, v, rho1, rho2, p
     V_MPH7 = 7,    // Euler multiphysics two-material, w == 0: alpha1, u, v, rho1, p1, rho2, p2
     V_MRED11 = 8,  // MHD reduced two-material: alpha1, u, v, w, rho1, rho2, p, Bx, By, Bz, psi
-    V_COUNT = 9
+    V_MINT12 = 9,  // MHD intermediate two-material: alpha1, u, v, w, rho1, p1, rho2, p2, Bx, By, Bz, psi
+    V_COUNT = 10
 };
 
 struct Ops {
@@ -68,6 +69,7 @@ cudaError_t hpr_solid_relax_fp64(const SweepArgs& a, cudaStream_t st);
 cudaError_t reduced_reinit_fp64(const SweepArgs& a, cudaStream_t st);
 cudaError_t multiphysics_reinit_fp64(const SweepArgs& a, cudaStream_t st);
 cudaError_t mhd_reduced_reinit_fp64(const SweepArgs& a, cudaStream_t st);
+cudaError_t mhd_intermediate_reinit_fp64(const SweepArgs& a, cudaStream_t st);
 
 // Planes of the source sub-cycles' scratch (SweepArgs::aux), which holds conserved vectors: a model carries at most
 // one conserved component more than primitive planes (the two-material models' rho alpha1), which forcing_impl

@@ -73,8 +73,9 @@ void run_planes(int model, std::vector<double>& planes, int nx, int ny, const do
                 double cfl, double tEnd, double bias, int limiter, int subcycles, int maxSteps = 0, int order = 2,
                 int reinit = 0) {
     // the first-order loop runs in the exact form, bit for bit with the reference; the Euler multiphysics and MHD
-    // reduced two-material models have no mixed form
-    const bool exact = order == 1 || model == VG_MODEL_EULER_MULTIPHYSICS || model == VG_MODEL_MHD_REDUCED;
+    // two-material models have no mixed form
+    const bool exact = order == 1 || model == VG_MODEL_EULER_MULTIPHYSICS || model == VG_MODEL_MHD_REDUCED ||
+                       model == VG_MODEL_MHD_INTERMEDIATE;
     SolverPtr s = make_solver(model, nx, ny, VG_TRANSMISSIVE, params, nparams, exact ? VG_FP64 : -1);
     vg_run_config c{};
     c.dx = dx;
@@ -728,6 +729,48 @@ vector<vector<MHDReducedStateVector> > MHDSecondOrderSolver::solve2D(vector<vect
     run_planes(VG_MODEL_MHD_REDUCED, p, (int)nx, (int)ny, prm, 5, dx, cfl, tEnd, bias, limiter, subcycles, maxSteps, 2,
                reinit);
     return unpack2<MHDReducedStateVector>(p, nx, ny, 11, mred_make);
+}
+
+// -------------------------------------------------------------------------------- MHD intermediate model
+MHDIntermediateStateVector::MHDIntermediateStateVector()
+    : w_{0.999, 0.0, 0.0, 0.0, 1.0, 1.0, 1.0, 1.0, 0.0, 0.0, 0.0, 0.0} {}
+void MHDIntermediateStateVector::setPrimitiveVariableVector(vector<double> w) {
+    for (int i = 0; i < 12; i++) w_[i] = w[i];
+}
+vector<double> MHDIntermediateStateVector::computePrimitiveVariableVector() const {
+    return vector<double>(w_, w_ + 12);
+}
+
+namespace {
+void mint_get(const MHDIntermediateStateVector& c, double* w) { std::memcpy(w, c.data(), sizeof(double) * 12); }
+MHDIntermediateStateVector mint_make(const double* w) {
+    MHDIntermediateStateVector s;
+    std::memcpy(s.data(), w, sizeof(double) * 12);
+    return s;
+}
+}  // namespace
+
+vector<MHDIntermediateStateVector> MHDSecondOrderSolver::solve(vector<MHDIntermediateStateVector>& initialCells,
+                                                               double dx, double cfl, double tEnd, double bias,
+                                                               int limiter, int subcycles, int reinit,
+                                                               MHDMaterialParameters m1, MHDMaterialParameters m2) {
+    double prm[5];
+    mred_params(m1, m2, prm);
+    std::vector<double> p = pack(initialCells, 12, mint_get);
+    run_planes(VG_MODEL_MHD_INTERMEDIATE, p, (int)initialCells.size(), 1, prm, 5, dx, cfl, tEnd, bias, limiter,
+               subcycles, 0, 2, reinit);
+    return unpack<MHDIntermediateStateVector>(p, initialCells.size(), 12, mint_make);
+}
+vector<vector<MHDIntermediateStateVector> > MHDSecondOrderSolver::solve2D(
+    vector<vector<MHDIntermediateStateVector> >& initialCells, double dx, double cfl, double tEnd, double bias,
+    int limiter, int subcycles, int reinit, MHDMaterialParameters m1, MHDMaterialParameters m2) {
+    double prm[5];
+    mred_params(m1, m2, prm);
+    std::vector<double> p = pack2(initialCells, 12, mint_get);
+    long ny = initialCells.size(), nx = initialCells[0].size();
+    run_planes(VG_MODEL_MHD_INTERMEDIATE, p, (int)nx, (int)ny, prm, 5, dx, cfl, tEnd, bias, limiter, subcycles, 0, 2,
+               reinit);
+    return unpack2<MHDIntermediateStateVector>(p, nx, ny, 12, mint_make);
 }
 
 // --------------------------------------------------------------------------------------------- HPR solver

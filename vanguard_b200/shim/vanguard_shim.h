@@ -224,6 +224,25 @@ private:
     double w_[11];
 };
 
+// MHDIntermediateStateVector (MHD/Multiphysics/mhdintermediatestatevector.h): the MHD intermediate two-material state,
+// primitives alpha1, u, v, w, rho1, p1, rho2, p2, Bx, By, Bz, psi.
+class MHDIntermediateStateVector {
+public:
+    MHDIntermediateStateVector();
+    void setPrimitiveVariableVector(vector<double> w);
+    vector<double> computePrimitiveVariableVector() const;
+    double getMaterial1VolumeFraction() const { return w_[0]; }
+    double getMaterial1Density() const { return w_[4]; }
+    double getMaterial1Pressure() const { return w_[5]; }
+    double getMaterial2Density() const { return w_[6]; }
+    double getMaterial2Pressure() const { return w_[7]; }
+    double* data() { return w_; }
+    const double* data() const { return w_; }
+
+private:
+    double w_[12];
+};
+
 // --------------------------------------------------------------------------------------------------- HPR
 class HPRMaterialParameters {
 public:
@@ -440,6 +459,20 @@ public:
                                                           int reinitialisationFrequency,
                                                           MHDMaterialParameters material1Parameters,
                                                           MHDMaterialParameters material2Parameters, int maxSteps);
+    // the MHD intermediate two-material model (Solvers/mhdsecondordersolver.cpp:387-440, :552-...), exact form; 2D
+    // with mirror ghosts on every side (the reference's own 2D padding of this model misfills its outermost bottom row)
+    static vector<MHDIntermediateStateVector> solve(vector<MHDIntermediateStateVector>& initialCells,
+                                                    double cellSpacing, double CFLCoefficient, double finalTime,
+                                                    double bias, int slopeLimiter, int subcyclingIterations,
+                                                    int reinitialisationFrequency,
+                                                    MHDMaterialParameters material1Parameters,
+                                                    MHDMaterialParameters material2Parameters);
+    static vector<vector<MHDIntermediateStateVector> > solve2D(vector<vector<MHDIntermediateStateVector> >& initialCells,
+                                                               double cellSpacing, double CFLCoefficient,
+                                                               double finalTime, double bias, int slopeLimiter,
+                                                               int subcyclingIterations, int reinitialisationFrequency,
+                                                               MHDMaterialParameters material1Parameters,
+                                                               MHDMaterialParameters material2Parameters);
 };
 
 // FirstOrderSolver / MHDFirstOrderSolver / HPRFirstOrderSolver::solve{,2D} (Solvers/firstordersolver.h:86-97,

@@ -342,3 +342,17 @@ def mhd_reduced_dumbser_2d(nx, ny=None, radius=0.2):
     I, J = np.meshgrid(np.arange(ny), np.arange(nx), indexing="ij")
     inside = np.sqrt((I - 0.5 * ny) ** 2 + (J - 0.5 * nx) ** 2) <= radius * nx
     return np.stack([np.where(inside, a, b) for a, b in zip(_DUMBSER_IN, _DUMBSER_OUT)]).astype(np.float64)
+
+
+MHD_INTERMEDIATE_NVAR = 12  # alpha1, u, v, w, rho1, p1, rho2, p2, Bx, By, Bz, psi (mhdintermediatestatevector.cpp:108-130)
+
+
+def mhd_intermediate_from_reduced(W):
+    """The MHD intermediate model's planes of an MHD reduced state: both materials at the interface pressure."""
+    out = np.zeros((MHD_INTERMEDIATE_NVAR,) + W.shape[1:])
+    out[:5] = W[:5]
+    out[5] = W[6]
+    out[6] = W[5]
+    out[7] = W[6]
+    out[8:] = W[7:]
+    return out
