@@ -23,6 +23,7 @@ import json
 import os
 import statistics
 import subprocess
+import threading
 import sys
 import time
 
@@ -59,35 +60,51 @@ def measured_peak():
 
 
 class ClockSampler:
-    """nvidia-smi sampling during the timed region (SM clock, throttle reasons)."""
+    """nvidia-smi sampling during the timed region (SM clock, throttle reasons).  nvidia-smi needs longer to start
+    than a short timed region lasts, so __enter__ returns only once the first sample has arrived (at most 5 s), a
+    reader thread stamps every line on arrival, and only the lines that arrive between __enter__ and __exit__ count."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    PERIOD_MS = 25
 
     def __init__(self, device_index):
         self.dev = device_index
         self.proc = None
+        self.stamped = []
+        self.lines = []
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.stamped.append((time.monotonic(), line))
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", str(self.PERIOD_MS)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.reader = threading.Thread(target=self._read, daemon=True)
+            self.reader.start()
+            t0 = time.monotonic()
+            while not self.stamped and time.monotonic() - t0 < 5.0:
+                time.sleep(0.005)
         except Exception:
             self.proc = None
+        self.t_start = time.monotonic()
         return self
 
     def __exit__(self, *exc):
-        self.lines = []
+        t_end = time.monotonic()
         if self.proc is not None:
             self.proc.terminate()
             try:
-                out, _ = self.proc.communicate(timeout=5)
+                self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
-                out = ""
-            self.lines = [l for l in out.splitlines() if l.strip()]
+            self.reader.join(timeout=5)
+        late = 0.5 * self.PERIOD_MS / 1e3  # a sample taken inside the region may be read this much after it
+        self.lines = [l for t, l in self.stamped if self.t_start <= t <= t_end + late and l.strip()]
 
     def summary(self):
         mhz, mx, reasons = [], None, set()
@@ -237,6 +254,8 @@ def run_cuda(args, world, rank, local):
     stream = torch.cuda.current_stream()
     sh = ctypes_stream(stream)
     legs = [x for x in args.legs.split(",") if x]
+    global CPU_LEGS
+    CPU_LEGS = world == 1 and rank == 0 and not args.no_cpu_baseline
     if "headline" not in legs:  # profiling / diagnostic runs of single legs (not a bench line)
         out = {}
         for leg in legs:
@@ -356,7 +375,8 @@ def run_cuda(args, world, rank, local):
         d = np.abs(finals["mixed"][0] - finals["fp64"][0])
         line["mixed_error_vs_fp64"] = {"rho_L1": float(d.mean()), "rho_Linf": float(d.max()),
                                        "reference": "the FP64 CUDA form, bitwise equal to the oracle"}
-    names = {"c5": "C5_ragged_batch_adjoint", "c4": "C4_hpr_1024", "c3": "C3_mhd_2048", "c1": "C1_sod_1000"}
+    names = {"c5": "C5_ragged_batch_adjoint", "c4": "C4_hpr_1024", "c3": "C3_mhd_2048", "c1": "C1_sod_1000",
+             "tm": "two_material_2048"}
     extra = {names[leg]: LEGS[leg](local, stream, sh) for leg in legs if leg in names}
     if extra:
         line["configs"] = extra
@@ -560,10 +580,76 @@ def sod_leg(local, stream, sh):
             "cell_updates_per_s": 1000 * it / sec}
 
 
+TM_N, TM_STEPS, TM_REINIT = 2048, 100, 10
+CPU_LEGS = True  # run_cuda clears it unless this is rank 0 of a 1-GPU run with the CPU baseline on
+
+
+def two_material_leg(local, stream, sh, n=TM_N, steps=TM_STEPS):
+    """The two-material models on n^2 grids of the reference scenarios' 2D layouts (EulerReducedTests' bubble,
+    MHDReducedTests' Dumbser disc; gamma 1.4 | 1.67), superbee, CFL 0.8, `steps` steps with the volume fraction
+    reinitialised every TM_REINIT steps and one GLM damping sub-cycle for the MHD models: exact FP64 form (and the
+    mixed form where the model has one), CUDA events on the launching stream; beside each, the compiled reference's
+    per-step loop on a strip of the same grid on the host cores (its CPU baseline)."""
+    import torch
+    import oracle as O
+    import vanguard_b200 as vg
+    from vanguard_b200 import workloads as wl
+
+    eu = wl.reduced_params(1.4, 0.0, 1.67, 0.0)
+    mh = wl.mhd_reduced_params(1.4, 0.0, 1.67, 0.0)
+    bubble, disc = wl.reduced_bubble_2d(n), wl.mhd_reduced_dumbser_2d(n)
+    cases = [
+        ("euler_reduced", vg.EULER_REDUCED, O.EULER_REDUCED, bubble, eu, 0, ("fp64", "mixed")),
+        ("euler_multiphysics", vg.EULER_MULTIPHYSICS, O.EULER_MULTIPHYSICS, wl.multiphysics_from_reduced(bubble), eu, 0,
+         ("fp64",)),
+        ("mhd_reduced", vg.MHD_REDUCED, O.MHD_REDUCED, disc, mh, 1, ("fp64",)),
+        ("mhd_intermediate", vg.MHD_INTERMEDIATE, O.MHD_INTERMEDIATE, wl.mhd_intermediate_from_reduced(disc), mh, 1,
+         ("fp64",)),
+    ]
+    precisions = {"fp64": vg.FP64, "mixed": vg.MIXED}
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    cores = O.ref().vgref_set_threads(0) if (CPU_LEGS and O.ref_available()) else 0
+    out = {"workload": f"2D {n}x{n}, gamma 1.4 | 1.67, superbee, CFL 0.8, {steps} steps, reinitialisation every "
+                       f"{TM_REINIT} steps, MHD models with 1 GLM sub-cycle"}
+    for name, model, omodel, W, prm, sub, forms in cases:
+        res = {}
+        for form in forms:
+            with vg.Solver(model, n, n, prm, precision=precisions[form], device=local) as s:
+                s.upload(W, stream=sh)
+                s.autotune(1.0 / n, CFL, limiter=LIMITER, stream=sh)
+                s.run(1.0 / n, CFL, steps=3, limiter=LIMITER, subcycles=sub, reinit=TM_REINIT, stream=sh,
+                      allow_nan=True)
+                s.upload(W, stream=sh)
+                torch.cuda.synchronize()
+                e0.record(stream)
+                s.run(1.0 / n, CFL, steps=steps, limiter=LIMITER, subcycles=sub, reinit=TM_REINIT, stream=sh,
+                      allow_nan=True)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ms = e0.elapsed_time(e1)
+                final = s.download(stream=sh)
+            res[form] = {"ms": ms, "cell_updates_per_s": n * n * steps / (ms / 1e3),
+                         "finite": bool(np.isfinite(final).all())}
+        if cores:
+            rows = 16
+            strip = np.ascontiguousarray(W[:, n // 2 - rows // 2: n // 2 + rows // 2, :])
+            t0 = time.perf_counter()
+            O.run_two_material(omodel, strip, 1.0 / n, CFL, steps=2, limiter=LIMITER, params=prm, reinit=TM_REINIT,
+                               subcycles=sub, reference=True, threads=cores)
+            dt = time.perf_counter() - t0
+            res["cpu_baseline"] = {"value": n * rows * 2 / dt, "unit": UNIT, "cores": cores, "kind": "reference",
+                                   "sample": f"2 steps of the reference per-step loop on a {n}x{rows} strip "
+                                             f"({dt:.2f} s)"}
+            res["fp64_vs_cpu_reference"] = res["fp64"]["cell_updates_per_s"] / res["cpu_baseline"]["value"]
+        out[name] = res
+    return out
+
+
 LEGS = {"c5": lambda l, st, sh: ragged_adjoint_leg(l, st, sh),
         "c4": lambda l, st, sh: hpr_leg(l, st, sh),
         "c3": lambda l, st, sh: mhd_leg(l, st, sh),
-        "c1": lambda l, st, sh: sod_leg(l, st, sh)}
+        "c1": lambda l, st, sh: sod_leg(l, st, sh),
+        "tm": lambda l, st, sh: two_material_leg(l, st, sh)}
 
 
 def ctypes_stream(stream):
@@ -606,8 +692,9 @@ def main():
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--headline-only", action="store_true", help="skip the C1/C3/C5 measurements")
-    ap.add_argument("--legs", default="headline,c5,c4,c3,c1",
-                    help="comma list of headline (C2), c5, c4, c3, c1; without headline only those legs run (profiling)")
+    ap.add_argument("--legs", default="headline,c5,c4,c3,c1,tm",
+                    help="comma list of headline (C2), c5, c4, c3, c1, tm (two-material models); without headline "
+                         "only those legs run (profiling)")
     ap.add_argument("--forms", default="fp64,mixed", help="C2 forms to run (profiling)")
     ap.add_argument("--c5-ninst", type=int, default=4096, help="C5 instances (smaller is for profiling only)")
     ap.add_argument("--c5-steps", type=int, default=500, help="C5 steps (smaller is for profiling only)")
