@@ -582,9 +582,10 @@ def sod_leg(local, stream, sh):
 
 TM_N, TM_STEPS, TM_REINIT = 2048, 100, 10
 CPU_LEGS = True  # run_cuda clears it unless this is rank 0 of a 1-GPU run with the CPU baseline on
+TM_MODELS = None  # all four; a comma list names a subset (profiling only)
 
 
-def two_material_leg(local, stream, sh, n=TM_N, steps=TM_STEPS):
+def two_material_leg(local, stream, sh, n=TM_N, steps=TM_STEPS, models=None):
     """The two-material models on n^2 grids of the reference scenarios' 2D layouts (EulerReducedTests' bubble,
     MHDReducedTests' Dumbser disc; gamma 1.4 | 1.67), superbee, CFL 0.8, `steps` steps with the volume fraction
     reinitialised every TM_REINIT steps and one GLM damping sub-cycle for the MHD models: exact FP64 form (and the
@@ -606,6 +607,8 @@ def two_material_leg(local, stream, sh, n=TM_N, steps=TM_STEPS):
         ("mhd_intermediate", vg.MHD_INTERMEDIATE, O.MHD_INTERMEDIATE, wl.mhd_intermediate_from_reduced(disc), mh, 1,
          ("fp64",)),
     ]
+    if models:  # profiling runs of a subset
+        cases = [c for c in cases if c[0] in models]
     precisions = {"fp64": vg.FP64, "mixed": vg.MIXED}
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     cores = O.ref().vgref_set_threads(0) if (CPU_LEGS and O.ref_available()) else 0
@@ -649,7 +652,7 @@ LEGS = {"c5": lambda l, st, sh: ragged_adjoint_leg(l, st, sh),
         "c4": lambda l, st, sh: hpr_leg(l, st, sh),
         "c3": lambda l, st, sh: mhd_leg(l, st, sh),
         "c1": lambda l, st, sh: sod_leg(l, st, sh),
-        "tm": lambda l, st, sh: two_material_leg(l, st, sh)}
+        "tm": lambda l, st, sh: two_material_leg(l, st, sh, steps=TM_STEPS, models=TM_MODELS)}
 
 
 def ctypes_stream(stream):
@@ -685,6 +688,7 @@ def load_traffic(form):
 
 
 def main():
+    global NX, NY, C5_NINST, C5_STEPS, C4_STEPS, TM_STEPS, TM_MODELS
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
@@ -699,13 +703,15 @@ def main():
     ap.add_argument("--c5-ninst", type=int, default=4096, help="C5 instances (smaller is for profiling only)")
     ap.add_argument("--c5-steps", type=int, default=500, help="C5 steps (smaller is for profiling only)")
     ap.add_argument("--c4-steps", type=int, default=300, help="C4 steps (smaller is for profiling only)")
+    ap.add_argument("--tm-steps", type=int, default=TM_STEPS, help="two-material steps (smaller is for profiling only)")
+    ap.add_argument("--tm-models", default="", help="two-material models to run, comma list (profiling only)")
     ap.add_argument("--nx", type=int, default=4096, help="grid size (smaller grids are for profiling only)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    global NX, NY, C5_NINST, C5_STEPS, C4_STEPS
     NX = NY = args.nx
     C5_NINST, C5_STEPS, C4_STEPS = args.c5_ninst, args.c5_steps, args.c4_steps
+    TM_STEPS, TM_MODELS = args.tm_steps, [m for m in args.tm_models.split(",") if m] or None
     if args.headline_only:
         args.legs = "headline"
     world, rank, local = dist_setup()
