@@ -652,7 +652,7 @@ LEGS = {"c5": lambda l, st, sh: ragged_adjoint_leg(l, st, sh),
         "c4": lambda l, st, sh: hpr_leg(l, st, sh),
         "c3": lambda l, st, sh: mhd_leg(l, st, sh),
         "c1": lambda l, st, sh: sod_leg(l, st, sh),
-        "tm": lambda l, st, sh: two_material_leg(l, st, sh, steps=TM_STEPS, models=TM_MODELS)}
+        "tm": lambda l, st, sh: two_material_leg(l, st, sh, n=TM_N, steps=TM_STEPS, models=TM_MODELS)}
 
 
 def ctypes_stream(stream):
@@ -688,7 +688,7 @@ def load_traffic(form):
 
 
 def main():
-    global NX, NY, C5_NINST, C5_STEPS, C4_STEPS, TM_STEPS, TM_MODELS
+    global NX, NY, C5_NINST, C5_STEPS, C4_STEPS, TM_N, TM_STEPS, TM_MODELS
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
@@ -705,13 +705,14 @@ def main():
     ap.add_argument("--c4-steps", type=int, default=300, help="C4 steps (smaller is for profiling only)")
     ap.add_argument("--tm-steps", type=int, default=TM_STEPS, help="two-material steps (smaller is for profiling only)")
     ap.add_argument("--tm-models", default="", help="two-material models to run, comma list (profiling only)")
+    ap.add_argument("--tm-n", type=int, default=TM_N, help="two-material grid size (smaller is for profiling only)")
     ap.add_argument("--nx", type=int, default=4096, help="grid size (smaller grids are for profiling only)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     NX = NY = args.nx
     C5_NINST, C5_STEPS, C4_STEPS = args.c5_ninst, args.c5_steps, args.c4_steps
-    TM_STEPS, TM_MODELS = args.tm_steps, [m for m in args.tm_models.split(",") if m] or None
+    TM_N, TM_STEPS, TM_MODELS = args.tm_n, args.tm_steps, [m for m in args.tm_models.split(",") if m] or None
     if args.headline_only:
         args.legs = "headline"
     world, rank, local = dist_setup()
