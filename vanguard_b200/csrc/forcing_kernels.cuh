@@ -69,10 +69,22 @@ __global__ void __launch_bounds__(256) roundtrip_kernel(SweepArgs a) {
     for (int v = 0; v < NU; v++) a.aux[v * a.plane + self] = U[v];
 }
 
-constexpr int FT = 64;  // threads per forcing block; 6 resident blocks (168 registers) measured fastest
+constexpr int FT = 64;  // threads per forcing block
+
+// Minimum resident blocks asked of the register allocator: 6 (168 registers) measured fastest for HPR; a model may
+// ask for more with FORCING_MIN_BLOCKS.  The kernel is FP64-latency bound, so more resident warps can pay for a few
+// spills; the choice never changes a result.
+template <class M, class = void>
+struct forcing_blocks {
+    static constexpr int value = 6;
+};
+template <class M>
+struct forcing_blocks<M, decltype((void)M::FORCING_MIN_BLOCKS)> {
+    static constexpr int value = M::FORCING_MIN_BLOCKS;
+};
 
 template <class M>
-__global__ void __launch_bounds__(FT, 6) forcing_kernel(SweepArgs a, int subcycles) {
+__global__ void __launch_bounds__(FT, forcing_blocks<M>::value) forcing_kernel(SweepArgs a, int subcycles) {
     constexpr int NU = M::NU, NW = M::NW;
     extern __shared__ double ksh[];  // k1, k2, k3 of this block's threads: [stage][component][thread]
     const long n = (long)a.nx * a.ny;
