@@ -24,7 +24,7 @@ from vanguard_b200 import workloads as wl  # noqa: E402
 
 # name -> (model, initial planes, run kwargs).  steps == 0: the reference's own time-driven solve().
 CASES = {
-    # BASELINE config 1 exactly: Sod, 1000 cells, minbee, CFL 0.9, t = 0.25, transmissive
+    # the 1D Sod benchmark case exactly: 1000 cells, minbee, CFL 0.9, t = 0.25, transmissive
     "euler1d_sod1000_minbee_t025": (O.EULER, lambda: wl.sod_1d(1000),
                                      dict(dx=1e-3, cfl=0.9, t_end=0.25, steps=0, limiter=O.MINBEE,
                                           params=wl.euler_params(1.4))),
