@@ -171,6 +171,10 @@ def dist_setup():
 # ----------------------------------------------------------------------------------------- reference arm
 
 def run_reference(args, world, rank):
+    """The reference's own OpenMP C++ loop (compiled unmodified into oracle/_ref) on all host cores: the K timed
+    steps run as ONE call of its per-step loop on a strip through the centre of the 4096^2 grid (ghost insertion,
+    CFL time step, X(dt/2) Y(dt) X(dt/2) per step), after W warm-up steps in another call; the strip is sized from
+    a probe so the timed call lasts about a minute."""
     if rank != 0:
         return 0
     import oracle as O
@@ -181,28 +185,23 @@ def run_reference(args, world, rank):
     cores = O.ref().vgref_set_threads(0)
     prm = wl.euler_params(1.4)
     full = wl.euler_quadrants_2d(NX, NY, seed=SEED)
-    # per-step cost on a thin strip of the same grid, then size the sample so the whole run ends in ~2 min
+    # per-step cost on a thin strip of the same grid, then size the sample so the timed call lasts ~60 s
     probe_rows = 16
     strip = np.ascontiguousarray(full[:, NY // 2 - probe_rows // 2: NY // 2 + probe_rows // 2, :])
     t0 = time.perf_counter()
     O.ref_run(O.EULER, strip.copy(), 1.0 / NX, CFL, steps=1, limiter=LIMITER, params=prm, threads=cores)
     per_cell = (time.perf_counter() - t0) / (NX * probe_rows)
-    budget = 120.0 / max(1, args.steps + args.warmup)
-    rows = int(max(16, min(NY, budget / max(per_cell * NX, 1e-12))))
+    rows = int(max(16, min(NY, 60.0 / max(per_cell * NX * args.steps, 1e-12))))
     rows -= rows % 2
     sample = np.ascontiguousarray(full[:, NY // 2 - rows // 2: NY // 2 + rows // 2, :])
-    for _ in range(args.warmup):
-        O.ref_run(O.EULER, sample.copy(), 1.0 / NX, CFL, steps=1, limiter=LIMITER, params=prm, threads=cores)
-    times = []
+    O.ref_run(O.EULER, sample.copy(), 1.0 / NX, CFL, steps=args.warmup, limiter=LIMITER, params=prm, threads=cores)
     state = sample.copy()
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        O.ref_run(O.EULER, state, 1.0 / NX, CFL, steps=1, limiter=LIMITER, params=prm, threads=cores)
-        times.append(time.perf_counter() - t0)
-    total = sum(times)
+    t0 = time.perf_counter()
+    O.ref_run(O.EULER, state, 1.0 / NX, CFL, steps=args.steps, limiter=LIMITER, params=prm, threads=cores)
+    total = time.perf_counter() - t0
     value = NX * rows * args.steps / total
     desc = (f"reference SecondOrderSolver per-step loop (oracle/_ref, OpenMP {cores} threads) on a {NX}x{rows} "
-            f"strip through the centre of the 4096x4096 grid, {args.steps} steps")
+            f"strip through the centre of the 4096x4096 grid, {args.steps} steps in one call")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1000.0 * total / args.steps, "higher_is_better": True,
@@ -238,6 +237,23 @@ def cpu_baseline_sample():
     return {"value": NX * rows * steps / dt, "unit": UNIT, "cores": cores, "kind": "reference",
             "sample": f"{steps} steps of the reference per-step loop on a {NX}x{rows} strip of the workload "
                       f"({dt:.1f} s, OpenMP {cores} threads)"}
+
+
+def hbm_roofline(rate, bytes_per_cell_update, basis):
+    """HBM roofline of a whole leg: algorithmic bytes per cell-update (SURVEY's passes x 2 x components x 8 B) times
+    the measured cell-update rate, against the measured copy bandwidth."""
+    peak, kind = measured_peak()
+    achieved = rate * bytes_per_cell_update / 1e9
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "bytes_per_cell_update": bytes_per_cell_update, "basis": basis, "peak_source": kind}
+
+
+def ref_cores():
+    """Host threads for the reference's CPU baselines (0 when they are off or the reference was not built)."""
+    import oracle as O
+    if not CPU_LEGS or not O.ref_available():
+        return 0
+    return O.ref().vgref_set_threads(0)
 
 
 # ---------------------------------------------------------------------------------------------- CUDA arm
@@ -320,9 +336,12 @@ def run_cuda(args, world, rank, local):
                          "tuned": {"x": tuned[2], "y": tuned[3], "x_ms": xt, "y_ms": yt}}
         s.close()
 
+    # The headline is the plain FP64 form: the reference's own arithmetic, bit-equal to it (the same grid and seed
+    # are pinned against the oracle in tests/test_zs_config_shapes_gpu.py), so the comparison with the reference
+    # arm is like for like.  The mixed form is reported beside it.
+    head = "fp64" if "fp64" in results else "mixed"
+    prec = vg.FP64 if head == "fp64" else vg.MIXED
     # end-to-end through the host-buffer API (vg_solve: upload + run + download inside the timed region)
-    best = "mixed" if "mixed" in results and mixed_ok(finals) else "fp64"
-    prec = vg.MIXED if best == "mixed" else vg.FP64
     hin = torch.from_numpy(W0).pin_memory()
     hout = torch.empty_like(hin).pin_memory()
     s = vg.Solver(vg.EULER, NX, NY, prm, precision=prec, device=local)
@@ -340,13 +359,13 @@ def run_cuda(args, world, rank, local):
     h2d = carried * NX * NY * 8
     d2h = carried * NX * NY * 8
 
-    r = results[best]
+    r = results[head]
     cells = NX * NY
     value = job_value(world, cells * args.steps, r["ms"] / 1000.0)
     peak, peak_kind = measured_peak()
     x_bytes = cells * BYTES_PER_CELL_SWEEP
     achieved = x_bytes / (r["x_sweep_ms"] / 1000.0) / 1e9
-    traffic = load_traffic(best)
+    traffic = load_traffic(head)
 
     if rank != 0:
         group.close()
@@ -354,27 +373,36 @@ def run_cuda(args, world, rank, local):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": r["ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64" if best == "fp64" else "f32+f64", "data": "synthetic",
-        "config": dict(workload_config(), form=best),
+        "vs_baseline": None, "dtype": "f64" if head == "fp64" else "f32+f64", "data": "synthetic",
+        "config": workload_config(),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic,
-                     "kernel": ("sweep_x_pair_kernel" if best == "mixed" else "sweep_x_kernel") + " (X half-sweep)",
+                     "kernel": ("sweep_x_kernel" if head == "fp64" else "sweep_x_pair_kernel") + " (X half-sweep, "
+                               + r["tuned"]["x"] + ")",
                      "algorithmic_bytes_per_launch": x_bytes, "peak_source": peak_kind},
         "e2e": {"value": job_value(world, cells * args.steps, e2e_s), "unit": UNIT,
                 "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
-                "api": "vg_solve (pinned host buffers; one upload + K steps + one download per call)"},
+                "api": f"vg_solve ({head}; pinned host buffers; one upload + K steps + one download per call)"},
         "gpu_launches": r["launches"],
         "clocks": r["clocks"],
+        "form": head,
         "forms": {k: {"cell_updates_per_s": world * cells * args.steps / (v["ms"] / 1000.0),
                       "ms_per_step": v["ms"] / args.steps, "x_sweep_ms": v["x_sweep_ms"],
                       "y_sweep_ms": v["y_sweep_ms"], "autotune": v["tuned"],
+                      "x_sweep_hbm_frac": x_bytes / (v["x_sweep_ms"] / 1000.0) / 1e9 / peak,
+                      "y_sweep_hbm_frac": x_bytes / (v["y_sweep_ms"] / 1000.0) / 1e9 / peak,
                       "hbm_frac_of_step": world * cells * args.steps * BYTES_PER_CELL_UPDATE / (v["ms"] / 1000.0) / 1e9 / peak}
                   for k, v in results.items()},
     }
+    if "mixed" in results and "fp64" in results:
+        line["mixed_speedup"] = results["fp64"]["ms"] / results["mixed"]["ms"]
     if "mixed" in finals and "fp64" in finals:
         d = np.abs(finals["mixed"][0] - finals["fp64"][0])
-        line["mixed_error_vs_fp64"] = {"rho_L1": float(d.mean()), "rho_Linf": float(d.max()),
-                                       "reference": "the FP64 CUDA form, bitwise equal to the oracle"}
+        line["mixed_error_vs_fp64"] = {
+            "rho_L1": float(d.mean()), "rho_Linf": float(d.max()), "steps": args.steps,
+            "reference": "this run's FP64 form; tests/test_zs_config_shapes_gpu.py::test_euler_4096_five_steps checks "
+                         "that form bit-equal to the oracle on this grid and seed, and the mixed form against the "
+                         "oracle itself"}
     names = {"c5": "C5_ragged_batch_adjoint", "c4": "C4_hpr_1024", "c3": "C3_mhd_2048", "c1": "C1_sod_1000",
              "tm": "two_material_2048"}
     extra = {names[leg]: LEGS[leg](local, stream, sh) for leg in legs if leg in names}
@@ -457,6 +485,34 @@ def ragged_adjoint_leg(local, stream, sh, reps=3):
         out["forward"]["e2e_ms"] = fwd_host_s * 1e3
         out["adjoint_binomial"]["e2e_ms"] = grad_host_s * 1e3
         out["adjoint_binomial"]["e2e_ratio_vs_forward"] = grad_host_s / fwd_host_s
+    out["forward"]["roofline"] = hbm_roofline(out["forward"]["cell_updates_per_s"], 48,
+                                              "one pass per step x 2 x 3 components (rho, rho u, E) x 8 B")
+    cores = ref_cores()
+    if cores:
+        # the reference's way: SecondOrderSolver::solve's loop once per problem, problems in parallel on the host
+        # cores (one thread each); timed on every instance for a few steps
+        import oracle as O
+        probe = W0.copy()
+        t0 = time.perf_counter()
+        O.ref_batch_run(probe, ncell, dx, gamma, CFL, 1, limiter=LIMITER, threads=cores)
+        one = time.perf_counter() - t0
+        steps = int(max(1, min(C5_STEPS, 15.0 / max(one, 1e-9))))
+        sample = W0.copy()
+        t0 = time.perf_counter()
+        O.ref_batch_run(sample, ncell, dx, gamma, CFL, steps, limiter=LIMITER, threads=cores)
+        dt = time.perf_counter() - t0
+        rate = total * steps / dt
+        fwd_s = total * C5_STEPS / rate
+        out["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": "reference",
+                               "sample": f"{steps} steps of all {C5_NINST} problems, each by the reference's 1D solve "
+                                         f"loop, problems in parallel one thread each ({dt:.1f} s)"}
+        out["forward"]["vs_cpu_reference"] = out["forward"]["cell_updates_per_s"] / rate
+        # the reference has no derivatives: its gradient is central differences, 2 forward runs per parameter
+        # (6 initial primitives + gamma per problem, all problems perturbed at once), estimated from the rate above
+        out["cpu_fd_gradient_estimate_s"] = {"value": 14 * fwd_s, "forward_runs": 14, "forward_s": fwd_s,
+                                             "basis": "14 full 500-step forward runs of the reference batch at the "
+                                                      "measured sample rate"}
+        out["adjoint_binomial"]["vs_cpu_fd_gradient"] = 14 * fwd_s / (out["adjoint_binomial"]["ms"] / 1e3)
     return out
 
 
@@ -488,7 +544,22 @@ def mhd_leg(local, stream, sh, steps=500):
     d = np.abs(finals["mixed"][0] - finals["fp64"][0])
     res["mixed_error_vs_fp64"] = {"rho_L1": float(d.mean()), "rho_Linf": float(d.max())}
     res["mixed_speedup"] = res["fp64"]["ms"] / res["mixed"]["ms"]
+    for form in ("fp64", "mixed"):
+        res[form]["roofline"] = hbm_roofline(res[form]["cell_updates_per_s"], 336, "whole step: 3 sweeps x 2 x 7 "
+                                             "components x 8 B (rho, rho u, rho v, E, Bx, By, psi)")
     res["workload"] = f"2D MHD {n}x{n} periodic vortex (seeded noise 1e-3), gamma 5/3, superbee, CFL 0.8, {steps} steps"
+    cores = ref_cores()
+    if cores:
+        import oracle as O
+        rows = 16
+        strip = np.ascontiguousarray(W[:, n // 2 - rows // 2: n // 2 + rows // 2, :])
+        t0 = time.perf_counter()
+        O.ref_run(O.MHD, strip, 1.0 / n, CFL, steps=2, limiter=LIMITER, params=prm, bc=O.PERIODIC, threads=cores)
+        dt = time.perf_counter() - t0
+        res["cpu_baseline"] = {"value": n * rows * 2 / dt, "unit": UNIT, "cores": cores, "kind": "reference",
+                               "sample": f"2 steps of the reference MHD per-step loop (c_h from the padded maximum "
+                                         f"each step) on a {n}x{rows} periodic strip of the workload ({dt:.2f} s)"}
+        res["fp64_vs_cpu_reference"] = res["fp64"]["cell_updates_per_s"] / res["cpu_baseline"]["value"]
     return res
 
 
@@ -531,37 +602,65 @@ def hpr_leg(local, stream, sh):
             finals[name] = s.download(stream=sh)
             res[name] = {"ms": ms, "steps": it, "t": t, "cell_updates_per_s": n * n * it / (ms / 1e3),
                          "launches": s.last_launch_count(), "finite": bool(np.isfinite(finals[name]).all())}
-    # the stiff relaxation mode (FP64): one relaxation of dt/2 before and after the sweeps instead of the forcing
-    with vg.Solver(vg.HPR, n, n, prm, device=local) as s:
-        s.upload(W, stream=sh)
-        s.autotune(1.0 / n, CFL, limiter=LIMITER, stream=sh)
-        s.run(1.0 / n, CFL, steps=2, limiter=LIMITER, stiff=True, stream=sh)
-        s.upload(W, stream=sh)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        e0.record(stream)
-        t, it = s.run(1.0 / n, CFL, steps=C4_STEPS, limiter=LIMITER, stiff=True, stream=sh, allow_nan=True)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1)
-        stiff = s.download(stream=sh)
-    ds = np.abs(stiff - finals["fp64"])
-    res["stiff_fp64"] = {"ms": ms, "steps": it, "t": t, "cell_updates_per_s": n * n * it / (ms / 1e3),
-                         "speedup_vs_forcing": res["fp64"]["ms"] / ms, "finite": bool(np.isfinite(stiff).all()),
-                         "difference_vs_forcing": {"rho_L1": float(ds[0].mean()), "rho_Linf": float(ds[0].max())}}
-    d = np.abs(finals["mixed"] - finals["fp64"])
-    res["mixed_error_vs_fp64"] = {"rho_L1": float(d[0].mean()), "rho_Linf": float(d[0].max()),
-                                  "all_L1": float(d.mean())}
+    # the stiff relaxation mode: one relaxation of dt/2 before and after the sweeps instead of the forcing, in the
+    # FP64 form and in the configuration's chosen form (FP32 flux, FP64 source, pressure recovery, CFL and update)
+    stiff = {}
+    for name, prec in (("stiff_fp64", vg.FP64), ("stiff_mixed", vg.MIXED)):
+        with vg.Solver(vg.HPR, n, n, prm, precision=prec, device=local) as s:
+            s.upload(W, stream=sh)
+            s.autotune(1.0 / n, CFL, limiter=LIMITER, stream=sh)
+            s.run(1.0 / n, CFL, steps=2, limiter=LIMITER, stiff=True, stream=sh)
+            s.upload(W, stream=sh)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            t, it = s.run(1.0 / n, CFL, steps=C4_STEPS, limiter=LIMITER, stiff=True, stream=sh, allow_nan=True)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            stiff[name] = s.download(stream=sh)
+            res[name] = {"ms": ms, "steps": it, "t": t, "cell_updates_per_s": n * n * it / (ms / 1e3),
+                         "launches": s.last_launch_count(), "speedup_vs_forcing_fp64": res["fp64"]["ms"] / ms,
+                         "finite": bool(np.isfinite(stiff[name]).all())}
+
+    def err(a, b):
+        d = np.abs(a - b)
+        return {"rho_L1": float(d[0].mean()), "rho_Linf": float(d[0].max()), "all_L1": float(d.mean())}
+
+    res["stiff_fp64"]["difference_vs_forcing_fp64"] = err(stiff["stiff_fp64"], finals["fp64"])
+    res["stiff_mixed"]["error_vs_stiff_fp64"] = err(stiff["stiff_mixed"], stiff["stiff_fp64"])
+    res["stiff_mixed"]["difference_vs_forcing_fp64"] = err(stiff["stiff_mixed"], finals["fp64"])
+    res["stiff_mixed"]["speedup_vs_stiff_fp64"] = res["stiff_fp64"]["ms"] / res["stiff_mixed"]["ms"]
+    res["mixed_error_vs_fp64"] = err(finals["mixed"], finals["fp64"])
     res["mixed_speedup"] = res["fp64"]["ms"] / res["mixed"]["ms"]
+    # algorithmic bytes: 3 sweeps + 2 source passes, each reading and writing the 11 non-trivial components
+    for form in ("fp64", "mixed", "stiff_fp64", "stiff_mixed"):
+        res[form]["roofline"] = hbm_roofline(res[form]["cell_updates_per_s"], 880, "whole step: (3 sweeps + 2 source "
+                                             "passes) x 2 x 11 components x 8 B")
+    res["chosen_form"] = ("stiff_mixed: the flux in FP32 (reconstruction, half-step evolution, FORCE) with the stiff "
+                          "relaxation source, pressure recovery, CFL maximum and update in FP64")
     res["subcycles"] = sub
     res["workload"] = (f"2D HPR {n}x{n} smooth field (seeded), thermal ideal gas, tau1 {tau1:.3e}, tau2 {tau2:.3e}, "
-                       f"superbee, CFL 0.8, {C4_STEPS} steps, RK4 forcing (FP64 in both forms) with {sub} sub-cycles "
-                       f"per half step")
+                       f"superbee, CFL 0.8, {C4_STEPS} steps; fp64/mixed: the reference's RK4 forcing (FP64 in both "
+                       f"forms) with {sub} sub-cycles per half step; stiff_*: the stiff relaxation source")
+    cores = ref_cores()
+    if cores:
+        import oracle as O
+        rows = 4
+        strip = np.ascontiguousarray(W[:, n // 2 - rows // 2: n // 2 + rows // 2, :])
+        t0 = time.perf_counter()
+        O.ref_run(O.HPR, strip, 1.0 / n, CFL, steps=1, limiter=LIMITER, params=prm, subcycles=sub, threads=cores)
+        dt = time.perf_counter() - t0
+        res["cpu_baseline"] = {"value": n * rows / dt, "unit": UNIT, "cores": cores, "kind": "reference",
+                               "sample": f"1 step of the reference HPR per-step loop with its RK4 forcing ({sub} "
+                                         f"sub-cycles per half step) on a {n}x{rows} strip of the workload ({dt:.2f} s)"}
+        res["fp64_vs_cpu_reference"] = res["fp64"]["cell_updates_per_s"] / res["cpu_baseline"]["value"]
     return res
 
 
 def sod_leg(local, stream, sh):
-    """C1: 1D Sod, 1000 cells, minbee, CFL 0.9, t_end 0.25 (time to solution, FP64)."""
+    """C1: 1D Sod, 1000 cells, minbee, CFL 0.9, t_end 0.25 (time to solution, FP64), beside the reference's own
+    SecondOrderSolver::solve called as-is on one thread and on all host cores."""
     import torch
     import vanguard_b200 as vg
     from vanguard_b200 import workloads as wl
@@ -576,8 +675,26 @@ def sod_leg(local, stream, sh):
         t, it = s.run(1e-3, 0.9, t_end=0.25, limiter=2, stream=sh)
         torch.cuda.synchronize()
         sec = time.perf_counter() - t0
-    return {"workload": "1D Sod 1000 cells, minbee, CFL 0.9, t_end 0.25", "steps": it, "t": t, "ms": sec * 1e3,
-            "cell_updates_per_s": 1000 * it / sec}
+        launches = s.last_launch_count()
+    out = {"workload": "1D Sod 1000 cells, minbee, CFL 0.9, t_end 0.25", "steps": it, "t": t, "ms": sec * 1e3,
+           "cell_updates_per_s": 1000 * it / sec, "launches": launches}
+    out["roofline"] = hbm_roofline(out["cell_updates_per_s"], 48, "one pass per step x 2 x 3 components x 8 B; "
+                                   "a 1000-cell grid is launch-latency bound (8 KB per plane), not HBM bound")
+    cores = ref_cores()
+    if cores:
+        import oracle as O
+        per = {}
+        for thr in (1, cores):
+            ref = W.copy()
+            t0 = time.perf_counter()
+            O.ref_run(O.EULER, ref, 1e-3, 0.9, t_end=0.25, limiter=2, params=wl.euler_params(1.4), threads=thr)
+            per[thr] = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": 1000 * it / per[cores], "unit": UNIT, "cores": cores, "kind": "reference",
+                               "sample": f"the reference's SecondOrderSolver::solve as-is, whole run ({per[cores]:.2f} "
+                                         f"s on {cores} threads, {per[1]:.2f} s on 1)",
+                               "one_thread_value": 1000 * it / per[1]}
+        out["vs_cpu_reference"] = out["cell_updates_per_s"] / out["cpu_baseline"]["value"]
+    return out
 
 
 TM_N, TM_STEPS, TM_REINIT = 2048, 100, 10
@@ -667,14 +784,6 @@ def vg_mixed_available(vg):
         return True
     except Exception:
         return False
-
-
-def mixed_ok(finals):
-    if "mixed" not in finals:
-        return False
-    if "fp64" not in finals:  # a profiling run of the mixed form alone
-        return True
-    return float(np.abs(finals["mixed"][0] - finals["fp64"][0]).mean()) <= 1e-6
 
 
 def load_traffic(form):

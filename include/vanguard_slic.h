@@ -158,6 +158,12 @@ vg_status vg_sweep(vg_solver* s, int axis, double dx, double dt, double bias, in
  * Solvers/mhdsolvers.cpp:286-388), including the default-state corner ghosts in 2D. */
 vg_status vg_max_wave_speed(vg_solver* s, double* out, void* stream);
 
+/* The helper itself, Solvers::computeMaximumWaveSpeed2D (Solvers/solvers.cpp:318-339): the maximum over
+ * exactly the uploaded cells, without adding the default-state corners.  A caller that uploads the
+ * reference's ghosted array (corners included) gets the reference's value; one that uploads interior cells
+ * only gets the maximum over those.  Equal to vg_max_wave_speed on 1D grids. */
+vg_status vg_max_wave_speed_cells(vg_solver* s, double* out, void* stream);
+
 /* Device pointer of plane 0 of the current state buffer and the plane/row strides in elements, so a
  * caller can read or write the resident state without a host round trip.  The carried planes are the
  * non-trivial subset (Euler: rho, u, [v], p; MHD: rho, u, v, [w], p, Bx, By, [Bz], psi). */
@@ -227,12 +233,14 @@ vg_status vg_batch_gradient(vg_batch* b, const double* target_rho, double cfl, i
  * cudaFree would synchronise the device under their other streams).  Computes the maximum wave speed
  * of the padded grid exactly as vg_max_wave_speed does, from a state the caller already holds in device
  * memory: `planes` = the model's reference-order primitive planes (Euler 6, MHD 9) with the given plane
- * and row strides (elements), `params` = the model's parameter block (gamma, p_inf first), `out` = a
- * device pointer to one double.  Calls neither cudaMalloc nor cudaFree: per-row partial maxima go to a
- * file-scope __device__ array of VG_NOALLOC_MAX_ROWS doubles, so ny > VG_NOALLOC_MAX_ROWS returns
- * VG_EINVAL.  Uses the current device.  The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress); make that first call before any stream capture.  Enqueued asynchronously on
- * `stream`.  All calls on a device share the array, so calls that may overlap on the GPU (different
+ * and row strides (elements; rows may be padded, row_stride >= nx, plane_stride >= row_stride * ny),
+ * `params` = the model's parameter block (gamma, p_inf first) in HOST memory (read on the host before the
+ * launch), `out` = a device pointer to one double.  Calls neither cudaMalloc nor cudaFree: per-row partial
+ * maxima go to a file-scope __device__ array of VG_NOALLOC_MAX_ROWS doubles, so ny > VG_NOALLOC_MAX_ROWS
+ * returns VG_EINVAL.  Uses the current device.  Every call looks up the array's device address in the
+ * current context (cudaGetSymbolAddress, which allocates nothing); the first call on a device may load the
+ * library's device code there, so make that first call before any stream capture.  Enqueued asynchronously
+ * on `stream`.  All calls on a device share the array, so calls that may overlap on the GPU (different
  * streams without ordering between them) race and must be serialised by the caller. */
 vg_status vg_max_wave_speed_noalloc(int model, const double* planes, long plane_stride, long row_stride, int nx,
                                     int ny, const double* params, double* out, void* stream);

@@ -101,6 +101,7 @@ def ref():
         R.vgref_first_order_run.argtypes = [_c_int, _D, _c_int, _c_int, _c_double, _c_double, _c_double, _c_int, _D,
                                             _c_int, ctypes.POINTER(_c_int)]
         R.vgref_set_threads.restype = _c_int
+        R.vgref_euler1d_batch_run.argtypes = [_D, _c_int, _I, _D, _D, _c_double, _c_int, _c_double, _c_int]
         R.vgref_set_threads.argtypes = [_c_int]
         R.vgref_euler1d_run.restype = _c_double
         R.vgref_euler1d_run.argtypes = [_D, _c_int, _c_double, _c_double, _c_double, _c_int, _c_double,
@@ -338,6 +339,24 @@ def ref_write(model, planes, directory, params=None):
             R.vgref_write_hpr(_ptr(planes), nx, ny, _ptr(_params(params)))
     finally:
         os.chdir(cwd)
+
+
+def ref_batch_run(planes, ncell, dx, gamma, cfl, steps, bias=0.0, limiter=SUPERBEE, threads=0):
+    """The reference's way of solving a ragged batch of 1D Euler problems: SecondOrderSolver::solve's per-step loop
+    once per problem, `steps` steps each, the problems spread over `threads` OpenMP threads (0: all host cores), one
+    thread per problem.  planes: (6, total) primitives of all problems concatenated, updated in place.  Returns the
+    thread count used."""
+    _check(planes, 6)
+    R = ref()
+    n = R.vgref_set_threads(threads)
+    nc = np.ascontiguousarray(ncell, dtype=np.int32)
+    dxa = np.ascontiguousarray(dx, dtype=np.float64)
+    ga = np.ascontiguousarray(gamma, dtype=np.float64)
+    if planes.shape[1] != int(nc.sum()):
+        raise ValueError("planes must hold sum(ncell) cells")
+    R.vgref_euler1d_batch_run(_ptr(planes), len(nc), nc.ctypes.data_as(_I), _ptr(dxa), _ptr(ga), cfl, steps, bias,
+                              limiter)
+    return n
 
 
 def ref_run(model, planes, dx, cfl, t_end=0.0, steps=0, bias=0.0, limiter=SUPERBEE, params=None,

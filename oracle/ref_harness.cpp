@@ -240,6 +240,35 @@ double vgref_euler1d_run(double* planes, int n, double dx, double cfl, double t_
     return t;
 }
 
+// Many independent 1D problems, each run by SecondOrderSolver::solve's per-step loop as vgref_euler1d_run runs it
+// (`steps` steps, no end time), the problems spread over the OpenMP team with one thread per problem (the
+// reference's own loops inside run single-threaded as nested regions).  planes: 6 x total, the problems'
+// primitive planes concatenated in order (total = sum of ncell); problem k has ncell[k] cells of width dx[k] and
+// adiabatic index gamma[k] (p_inf 0).  This is the reference's way to solve a ragged batch: one solve per problem.
+void vgref_euler1d_batch_run(double* planes, int ninst, const int* ncell, const double* dx, const double* gamma,
+                             double cfl, int steps, double bias, int limiter) {
+    QuietCout quiet;
+    std::vector<long> off(ninst + 1, 0);
+    for (int k = 0; k < ninst; k++) off[k + 1] = off[k] + ncell[k];
+    const long total = off[ninst];
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int k = 0; k < ninst; k++) {
+        const double prm[6] = {gamma[k], 0.0, 25.0, 0.0, 0.25, 250.0};  // EulerMaterialParameters(gamma)'s defaults
+        EulerMaterialParameters mp = eulerParams(prm);
+        const int n = ncell[k];
+        vector<EulerStateVector> cells(n);
+        for (int i = 0; i < n; i++) cells[i] = eulerCell(planes, total, off[k] + i);
+        double t = 0.0;
+        for (int it = 0; it < steps; it++) {
+            vector<EulerStateVector> withB = Solvers::insertBoundaryCells(cells, 2);
+            double dt = Solvers::computeStableTimeStep(withB, dx[k], cfl, t, kNoEnd, it, mp);
+            SecondOrderSolver::computeSLICTimeStep(cells, withB, dx[k], dt, bias, limiter, mp);
+            t += dt;
+        }
+        for (int i = 0; i < n; i++) eulerStore(cells[i], planes, total, off[k] + i);
+    }
+}
+
 // --------------------------------------------------------------------------------------- Euler 2D
 // nx columns (x, inner index j) by ny rows (y, row index i); planes: 6 x (ny*nx), row-major.
 // bc: 0 transmissive (reference ghosts), 1 periodic (harness ghosts).

@@ -6,9 +6,11 @@
 // MHD solve2D (9 x 16 x 16), HPR solve (17 x 50), Euler 1D step-count solve (6 x 150), Euler 1D first-order solve
 // (6 x 150), HPR GodunovRomenski plastic solve (17 x 60), reduced two-material solve (7 x 120), multiphysics
 // two-material solve (8 x 100), MHD reduced two-material solve2D (11 x 24 x 24), MHD intermediate two-material solve
-// (12 x 80), then the number of 2D steps the per-sweep loop took.
+// (12 x 80), the 2D maximum wave speed of an interior-only cold gas (1), whether solve2D refused a single row (1),
+// then the number of 2D steps the per-sweep loop took.
 #include <cmath>
 #include <cstdio>
+#include <stdexcept>
 #include <vector>
 
 #include "Solvers/firstordersolver.h"
@@ -214,6 +216,25 @@ int main(int argc, char** argv) {
         for (int k = 0; k < 12; k++)
             for (auto& c : out) v.push_back(c.computePrimitiveVariableVector()[k]);
         put(f, v);
+    }
+    // 12) Solvers::computeMaximumWaveSpeed2D over interior cells only (no ghosts, so no default-state corners): a cold
+    //     gas whose own speeds are below the default state's; then solve2D on a single row, which the reference's 2D
+    //     ghost insertion does not define: the shim must refuse it (1.0 written when it throws invalid_argument)
+    {
+        int nx = 8, ny = 6;
+        vector<vector<EulerStateVector> > cells(ny, vector<EulerStateVector>(nx));
+        for (int i = 0; i < ny; i++)
+            for (int j = 0; j < nx; j++) cells[i][j] = EulerStateVector(1.0 + 0.01 * j, 0.01 * i, -0.02 * j, 0.0, 0.01 + 0.001 * i);
+        double smax = Solvers::computeMaximumWaveSpeed2D(cells, EulerMaterialParameters(1.4));
+        put(f, vector<double>{smax});
+        vector<vector<EulerStateVector> > row(1, vector<EulerStateVector>(10, EulerStateVector(1.0, 0.0, 0.0, 0.0, 1.0)));
+        double refused = 0.0;
+        try {
+            SecondOrderSolver::solve2D(row, 0.1, 0.8, 0.01, 0.0, 0, 0, EulerMaterialParameters(1.4));
+        } catch (const std::invalid_argument&) {
+            refused = 1.0;
+        }
+        put(f, vector<double>{refused});
     }
     double st = steps;
     std::fwrite(&st, sizeof(double), 1, f);

@@ -189,3 +189,18 @@ def test_oracle_vs_reference_first_order(case):
     tb = O.ref_run_first_order(model, b, dx, 0.8, steps=7, params=prm, bc=bc)
     assert ta == tb
     assert np.array_equal(a, b)
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="the compiled reference (oracle/_ref) was not built")
+def test_reference_batch_harness_matches_per_problem_solves(oracle_lib):
+    """The reference's ragged-batch baseline (one solve loop per problem, problems in parallel) equals the oracle's
+    per-problem run bit for bit: the parallel schedule does not change any problem's arithmetic."""
+    ncell, dx, gamma, theta, W = wl.ragged_riemann_batch(ninst=23, seed=8, nmin=3, nmax=300)
+    out = W.copy()
+    O.ref_batch_run(out, ncell, dx, gamma, 0.8, 25, bias=0.2, limiter=O.MINBEE, threads=4)
+    off = 0
+    for k, n in enumerate(ncell):
+        ref = W[:, off:off + n].copy()
+        O.run(O.EULER, ref, dx[k], 0.8, steps=25, bias=0.2, limiter=O.MINBEE, params=wl.euler_params(gamma[k]))
+        assert np.array_equal(out[:, off:off + n], ref), k
+        off += n

@@ -124,5 +124,15 @@ def test_shim_driver_matches_oracle(gpu, oracle_lib, tmp_path):
                        params=wl.mhd_reduced_params(1.4, 0.0, 1.67, 0.0), reinit=5, subcycles=1)
     assert np.array_equal(got, ref)
 
+    # 12) computeMaximumWaveSpeed2D over exactly the cells given (interior only: no default-state corners), and
+    #     solve2D on a single row refused with std::invalid_argument
+    smax = take((1,))[0]
+    j, i = np.meshgrid(np.arange(8), np.arange(6))
+    rho, u, v, p = 1.0 + 0.01 * j, 0.01 * i, -0.02 * j, 0.01 + 0.001 * i
+    expect = (np.maximum(np.abs(u), np.abs(v)) + np.sqrt((1.4 * (p + 0.0)) / rho)).max()
+    assert smax == expect
+    assert smax < np.sqrt(1.4)  # below the default state's speed, which the padded-grid maximum would add
+    assert take((1,))[0] == 1.0
+
     assert take((1,))[0] == 6
     assert off == data.size

@@ -63,3 +63,26 @@ def test_noalloc_rejects_rows_beyond_scratch(gpu):
         gpu.max_wave_speed_noalloc(0, dev.data_ptr(), 4 * rows, 4, 4, rows, wl.euler_params(1.4), out.data_ptr())
     assert e.value.status == gpu.VG_EINVAL
     assert "VG_NOALLOC_MAX_ROWS" in str(e.value)
+
+
+def test_noalloc_padded_strides(gpu):
+    """Rows padded past nx and planes spaced past row_stride * ny, with the padding holding a state far faster than
+    any cell: the padding must not be read, and the result must equal vg_max_wave_speed's, on two calls in a row."""
+    import ctypes
+    import torch
+    W = wl.euler_quadrants_2d(100, 37, seed=44)
+    nv, ny, nx = W.shape
+    pitch, gap = 128, 96
+    ps = ny * pitch + gap
+    buf = torch.ones(nv * ps, dtype=torch.float64, device="cuda")
+    buf[1 * ps:2 * ps] = 1e10          # u in the padding: a wave speed that would dominate if it were read
+    for v in range(nv):
+        buf[v * ps: v * ps + ny * pitch].view(ny, pitch)[:, :nx] = torch.from_numpy(W[v]).cuda()
+    out = torch.empty(1, dtype=torch.float64, device="cuda")
+    want = _existing(gpu, 0, W, wl.euler_params(1.4))
+    for _ in range(2):
+        out.fill_(-1.0)
+        gpu.max_wave_speed_noalloc(0, buf.data_ptr(), ps, pitch, nx, ny, wl.euler_params(1.4), out.data_ptr(),
+                                   ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+        torch.cuda.synchronize()
+        assert float(out.item()) == want

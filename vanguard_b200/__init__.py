@@ -49,7 +49,7 @@ class RunConfig(ctypes.Structure):
 
 # Every function the C ABI header declares (tests check the library exports them all).
 EXPORTS = ["vg_create", "vg_destroy", "vg_model_nvar", "vg_upload_primitive", "vg_download_primitive",
-           "vg_run", "vg_solve", "vg_sweep", "vg_max_wave_speed", "vg_state_device", "vg_last_launch_count",
+           "vg_run", "vg_solve", "vg_sweep", "vg_max_wave_speed", "vg_max_wave_speed_cells", "vg_state_device", "vg_last_launch_count",
            "vg_last_error_string", "vg_status_string", "vg_max_wave_speed_noalloc", "vg_autotune",
            "vg_set_launch_config", "vg_get_launch_config", "vg_batch_create", "vg_batch_destroy",
            "vg_batch_total_cells", "vg_batch_upload", "vg_batch_download", "vg_batch_run",
@@ -87,6 +87,7 @@ def lib():
         L.vg_solve.argtypes = [vp, vp, vp, ctypes.POINTER(RunConfig), ctypes.POINTER(ctypes.c_int), D, vp]
         L.vg_sweep.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int, vp]
         L.vg_max_wave_speed.argtypes = [vp, D, vp]
+        L.vg_max_wave_speed_cells.argtypes = [vp, D, vp]
         L.vg_state_device.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(ctypes.c_long),
                                       ctypes.POINTER(ctypes.c_long), ctypes.POINTER(ctypes.c_int)]
         L.vg_max_wave_speed_noalloc.argtypes = [ctypes.c_int, vp, ctypes.c_long, ctypes.c_long, ctypes.c_int,
@@ -199,9 +200,12 @@ class Solver:
     def sweep(self, axis, dx, dt, bias=0.0, limiter=SUPERBEE, stream=None):
         return _check(lib().vg_sweep(self._h, axis, dx, dt, bias, limiter, stream))
 
-    def max_wave_speed(self, stream=None):
+    def max_wave_speed(self, stream=None, corners=True):
+        """The CFL maximum of the padded grid (vg_max_wave_speed); corners=False: over exactly the uploaded cells,
+        without the default-state corner ghosts of a 2D grid (vg_max_wave_speed_cells)."""
         v = ctypes.c_double()
-        _check(lib().vg_max_wave_speed(self._h, ctypes.byref(v), stream))
+        f = lib().vg_max_wave_speed if corners else lib().vg_max_wave_speed_cells
+        _check(f(self._h, ctypes.byref(v), stream))
         return v.value
 
     def state_device(self):

@@ -61,8 +61,8 @@ def build(verbose: bool = False, force: bool = False) -> str:
     env.pop("CXX", None)
     env.pop("CC", None)
     headers = _headers()
-    objs = []
-    for src, flags in UNITS:
+    objs, jobs = [], []
+    for src, flags in UNITS:  # the units are independent: compile the stale ones concurrently
         s = os.path.join(CSRC, src)
         o = os.path.join(OBJDIR, src.replace(".cu", ".o"))
         objs.append(o)
@@ -70,7 +70,13 @@ def build(verbose: bool = False, force: bool = False) -> str:
             cmd = [nvcc, *ARCH, *COMMON, *flags, "-c", s, "-o", o]
             if verbose:
                 print(" ".join(cmd), flush=True)
-            subprocess.run(cmd, check=True, env=env)
+            jobs.append((cmd, o, subprocess.Popen(cmd, env=env)))
+    failed = [cmd for cmd, o, p in jobs if p.wait() != 0]
+    if failed:
+        for cmd, o, p in jobs:  # a failed unit must not leave a stale object that looks current
+            if p.returncode != 0 and os.path.exists(o):
+                os.remove(o)
+        raise subprocess.CalledProcessError(1, failed[0])
     if force or _stale(OUT, objs):
         cmd = [nvcc, *ARCH, "-shared", "-Xcompiler", "-fPIC", "-ccbin", "g++", "-o", OUT, *objs]
         if verbose:

@@ -381,6 +381,25 @@ vg_status ensure_graphs(vg_solver* s, const vg_run_config& c) {
     return VG_OK;
 }
 
+// The CFL maximum of the uploaded state; with_corners adds the default-constructed corner ghosts of a 2D grid.
+vg_status max_wave_speed(vg_solver* s, double* out, bool with_corners, void* stream) {
+    if (!s || !out) return fail(VG_EINVAL, "null argument");
+    if (!s->ops) return fail(VG_EINVAL, "no state uploaded");
+    cudaStream_t st = (cudaStream_t)stream;
+    Ctrl* h = s->hctrl;
+    std::memset(h, 0, sizeof(Ctrl));
+    h->dims = with_corners ? s->dims : 0;  // the finishing kernel folds in the corner state for dims == 2 only
+    VG_CUDA(cudaMemcpyAsync(s->ctrl, h, sizeof(Ctrl), cudaMemcpyHostToDevice, st));
+    SweepArgs a = base_args(s);
+    a.in = s->buf[s->cur];
+    VG_CUDA(s->ops->max_wave(a, st));
+    VG_CUDA(s->ops->max_wave_finish(a, s->dout, st));
+    VG_CUDA(cudaMemcpyAsync(s->hout, s->dout, sizeof(double), cudaMemcpyDeviceToHost, st));
+    VG_CUDA(cudaStreamSynchronize(st));
+    *out = *s->hout;
+    s->last_launches = 2;
+    return VG_OK;
+}
 }  // namespace
 
 extern "C" {
@@ -677,23 +696,10 @@ vg_status vg_sweep(vg_solver* s, int axis, double dx, double dt, double bias, in
     return VG_OK;
 }
 
-vg_status vg_max_wave_speed(vg_solver* s, double* out, void* stream) {
-    if (!s || !out) return fail(VG_EINVAL, "null argument");
-    if (!s->ops) return fail(VG_EINVAL, "no state uploaded");
-    cudaStream_t st = (cudaStream_t)stream;
-    Ctrl* h = s->hctrl;
-    std::memset(h, 0, sizeof(Ctrl));
-    h->dims = s->dims;
-    VG_CUDA(cudaMemcpyAsync(s->ctrl, h, sizeof(Ctrl), cudaMemcpyHostToDevice, st));
-    SweepArgs a = base_args(s);
-    a.in = s->buf[s->cur];
-    VG_CUDA(s->ops->max_wave(a, st));
-    VG_CUDA(s->ops->max_wave_finish(a, s->dout, st));
-    VG_CUDA(cudaMemcpyAsync(s->hout, s->dout, sizeof(double), cudaMemcpyDeviceToHost, st));
-    VG_CUDA(cudaStreamSynchronize(st));
-    *out = *s->hout;
-    s->last_launches = 2;
-    return VG_OK;
+vg_status vg_max_wave_speed(vg_solver* s, double* out, void* stream) { return max_wave_speed(s, out, true, stream); }
+
+vg_status vg_max_wave_speed_cells(vg_solver* s, double* out, void* stream) {
+    return max_wave_speed(s, out, false, stream);
 }
 
 vg_status vg_state_device(vg_solver* s, double** plane0, long* plane_stride, long* row_stride, int* nplanes) {

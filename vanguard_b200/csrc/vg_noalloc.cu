@@ -11,7 +11,6 @@
 // result equals vg_max_wave_speed bit for bit.
 #include <cuda_runtime.h>
 
-#include <mutex>
 #include <string>
 
 #include "../../include/vanguard_slic.h"
@@ -25,10 +24,6 @@ namespace {
 // them, so nothing needs to start at zero, and calls that overlap on the GPU (different streams, no
 // ordering between them) race on it.
 __device__ __align__(256) double g_row_max[VG_NOALLOC_MAX_ROWS];
-
-constexpr int kMaxDevices = 64;
-std::mutex g_mutex;
-double* g_scratch[kMaxDevices] = {nullptr};
 
 vg_status noalloc_fail(vg_status st, const std::string& msg) {
     vg::set_last_error(msg);
@@ -101,21 +96,15 @@ __global__ void __launch_bounds__(NT) row_max_finish_kernel(const double* __rest
     }
 }
 
-// Device address of the scratch array on the current device, looked up once per device.
+// Device address of the scratch array in the current device's context.  Looked up on every call: the lookup is a
+// host-side table query that allocates nothing, and a cached address would outlive the module it points into if the
+// host reset the device (cudaDeviceReset) between calls.  The first lookup on a device may load the library's device
+// code into that context, which is why the first call must come before any stream capture.
 vg_status scratch_for_current_device(double** out) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return noalloc_fail(VG_ECUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
-    if (dev < 0 || dev >= kMaxDevices) return noalloc_fail(VG_EUNSUPPORTED, "device ordinal above 63");
-    std::lock_guard<std::mutex> lock(g_mutex);
-    if (!g_scratch[dev]) {
-        double* p = nullptr;
-        e = cudaGetSymbolAddress((void**)&p, g_row_max);
-        if (e != cudaSuccess)
-            return noalloc_fail(VG_ECUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-        g_scratch[dev] = p;
-    }
-    *out = g_scratch[dev];
+    double* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress((void**)&p, g_row_max);
+    if (e != cudaSuccess) return noalloc_fail(VG_ECUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    *out = p;
     return VG_OK;
 }
 

@@ -103,8 +103,18 @@ std::vector<double> pack(const std::vector<S>& cells, int nvar, Get get) {
     }
     return p;
 }
+// Every 2D entry point packs through here.  The reference's 2D ghost insertion reads rows 0 and 1 and columns 0 and 1
+// of the grid (Solvers/solvers.cpp:111-130), so a grid with fewer than 2 rows or columns is outside what its solve2D
+// and per-sweep functions define; the device would otherwise treat a single row as a 1D grid.
+template <class S>
+void require_2d(const std::vector<std::vector<S> >& cells) {
+    if (cells.size() < 2 || cells[0].size() < 2)
+        throw std::invalid_argument("2D solver: the grid needs at least 2 rows and 2 columns (use the 1D solve for a "
+                                    "single row)");
+}
 template <class S, class Get>
 std::vector<double> pack2(const std::vector<std::vector<S> >& cells, int nvar, Get get) {
+    require_2d(cells);
     long ny = cells.size(), nx = cells[0].size(), n = nx * ny;
     std::vector<double> p(nvar * n);
     for (long i = 0; i < ny; i++)
@@ -454,15 +464,15 @@ double Solvers::computeMaximumWaveSpeed(vector<EulerStateVector>& cells, EulerMa
     return out;
 }
 double Solvers::computeMaximumWaveSpeed2D(vector<vector<EulerStateVector> >& cells, EulerMaterialParameters mp) {
-    // the ghosted array the reference passes here contains its default-constructed corners; vg_max_wave_speed adds
-    // the default state's speed for a 2D grid, which is the same set of values
+    // the maximum over exactly the cells given, as the reference helper takes it: a ghosted array brings its own
+    // default-constructed corners, an interior-only array has none
     double prm[6];
     euler_params(mp, prm);
     std::vector<double> p = pack2(cells, 6, euler_get);
     vg_solver* s = cached_solver(VG_MODEL_EULER, (int)cells[0].size(), (int)cells.size(), VG_TRANSMISSIVE, prm, 6);
     check(vg_upload_primitive(s, p.data(), 0, nullptr), "vg_upload_primitive");
     double out = 0.0;
-    check(vg_max_wave_speed(s, &out, nullptr), "vg_max_wave_speed");
+    check(vg_max_wave_speed_cells(s, &out, nullptr), "vg_max_wave_speed_cells");
     return out;
 }
 double Solvers::computeStableTimeStep(double dt, double t, double tEnd, int it) {
