@@ -37,7 +37,8 @@ extern "C" {
 typedef enum vg_status {
     VG_OK = 0,
     VG_EINVAL = 1,       /* bad argument: null pointer, size, model, limiter, plane count */
-    VG_ENAN = 2,         /* the run produced a non-finite value or non-positive density/pressure */
+    VG_ENAN = 2,         /* the run produced a non-finite value, a non-positive density, or a pressure at or
+                          * below -p_inf (no real sound speed; 0 for ideal gases) */
     VG_ETIMEOUT = 3,     /* a bounded device-side wait gave up (persistent kernels) */
     VG_ECUDA = 4,        /* a CUDA runtime call failed; vg_last_error_string() has the text */
     VG_ENOMEM = 5,       /* device allocation failed */
@@ -134,7 +135,8 @@ int vg_model_nvar(int model);
  * memory (is_device).  Upload returns VG_EUNSUPPORTED if the state uses fields the compiled variants
  * do not carry: Euler needs w == 0 and lambda == 1 in every cell; MHD needs w == 0 and Bz == 0 unless
  * the solver was created for the full 9-component variant (it chooses it automatically when they are
- * non-zero). */
+ * non-zero).  Where those checks do not decide the variant they run on host threads while the copies are in
+ * flight; a failed upload leaves the solver without a state until the next successful one. */
 vg_status vg_upload_primitive(vg_solver* s, const double* planes, int is_device, void* stream);
 vg_status vg_download_primitive(vg_solver* s, double* planes, int is_device, void* stream);
 
@@ -178,15 +180,26 @@ long vg_last_launch_count(vg_solver* s);
  * thread, register cap).  The tile shape never changes a cell's arithmetic, so every configuration gives
  * identical results.
  * vg_autotune times every candidate on the uploaded state (`reps` launches each, CUDA events on `stream`),
- * keeps the fastest per axis and caches it by (variant, precision, boundary, nx, ny, SM count) in
+ * keeps the fastest per axis and caches it (with the schedule below) by (variant, precision, boundary, nx,
+ * ny, SM count) in
  * process memory and, when the environment variable VG_TUNE_CACHE names a file, on disk.  With
  * times_ms == NULL a cached choice is applied without timing; otherwise times_ms receives
- * VG_NUM_XCFG + VG_NUM_YCFG averages (X configurations first). */
+ * VG_NUM_XCFG + VG_NUM_YCFG + VG_NUM_SCHED averages (X configurations, Y configurations, then the step's tail
+ * under each schedule below, fused first).
+ * The tuner also picks the step's schedule: where the next step's CFL maximum (Solvers/solvers.cpp:413-452) is
+ * taken.  0 folds it into the last X sweep's epilogue (no extra pass over the state, but the wave speed's
+ * registers ride in the sweep); 1 runs a separate reduction after the step (one more read of the state, a
+ * leaner sweep).  The reference's split order X(dt/2) Y(dt) X(dt/2) itself is fixed: it defines the results.
+ * Both schedules give identical results.  Runs with a source pass or a reinitialisation after the sweeps
+ * always take the separate reduction.  vg_set_schedule / vg_get_schedule set and read it directly. */
 #define VG_NUM_XCFG 5
 #define VG_NUM_YCFG 6
+#define VG_NUM_SCHED 2
 vg_status vg_autotune(vg_solver* s, const vg_run_config* cfg, int reps, float* times_ms, void* stream);
 vg_status vg_set_launch_config(vg_solver* s, int xcfg, int ycfg);
 vg_status vg_get_launch_config(vg_solver* s, int* xcfg, int* ycfg, const char** xname, const char** yname);
+vg_status vg_set_schedule(vg_solver* s, int cfl_separate);
+vg_status vg_get_schedule(vg_solver* s, int* cfl_separate);
 
 /* ---- Ragged batches of independent 1D Euler problems.  No counterpart in the reference, whose scenario drivers
  * call SecondOrderSolver::solve (Solvers/secondordersolver.cpp:288-314) once per problem; a batch runs that same

@@ -153,9 +153,44 @@ def test_autotune_picks_and_keeps_results(gpu, oracle_lib):
         assert all(t > 0 for t in xt) and all(t > 0 for t in yt)
         x, y, _, _ = s.launch_config()
         assert xt[x] == min(xt) and yt[y] == min(yt)
+        fused, separate = s.schedule_times
+        assert fused > 0 and separate > 0
+        assert s.schedule() == (1 if separate < fused else 0)
         s.upload(W)
         s.run(1.0 / nx, 0.8, steps=10, limiter=0)
         _bitwise(s.download(), ref)
+
+
+@pytest.mark.parametrize("model,precision", [(0, 0), (0, 1), (1, 0), (2, 0)])
+def test_cfl_schedules_give_identical_results(gpu, oracle_lib, model, precision):
+    """The step schedule (the next step's CFL maximum folded into the last X sweep, or a separate reduction pass)
+    changes where the maximum is taken, not its value: both schedules give the same bits, time-driven and
+    step-driven, and the FP64 form stays bit-equal to the oracle; a separate pass is one more launch per step."""
+    nx, ny = 96, 72
+    if model == 0:
+        W, prm = wl.euler_quadrants_2d(nx, ny, seed=64), wl.euler_params(1.4)
+    elif model == 1:
+        W, prm = wl.mhd_vortex_2d(nx, ny, seed=65), wl.mhd_params(5.0 / 3.0)
+    else:
+        W, prm = wl.hpr_smooth_2d(nx, ny, seed=66), wl.hpr_params(tau1=1e-2, tau2=1e-2)
+    outs, launches = {}, {}
+    with gpu.Solver(model, nx, ny, prm, precision=precision) as s:
+        for sched in (0, 1):
+            s.set_schedule(sched)
+            assert s.schedule() == sched
+            s.upload(W)
+            t, it = s.run(1.0 / nx, 0.8, steps=9, limiter=0)
+            launches[sched] = s.last_launch_count()
+            s.upload(W)
+            t2, it2 = s.run(1.0 / nx, 0.8, t_end=0.02, limiter=0)
+            outs[sched] = (s.download(), t, it, t2, it2)
+    a, b = outs[0], outs[1]
+    assert np.array_equal(a[0], b[0]) and a[1:] == b[1:]
+    assert launches[1] == launches[0] + 9
+    if precision == 0:
+        ref = W.copy()
+        O.run(model, ref, 1.0 / nx, 0.8, t_end=0.02, limiter=0, params=prm)
+        _bitwise(a[0], ref)
 
 
 @pytest.mark.parametrize("bc", [0, 1])

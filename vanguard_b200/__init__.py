@@ -48,13 +48,13 @@ class RunConfig(ctypes.Structure):
 
 
 # Every function the C ABI header declares (tests check the library exports them all).
-EXPORTS = ["vg_create", "vg_destroy", "vg_model_nvar", "vg_upload_primitive", "vg_download_primitive",
-           "vg_run", "vg_solve", "vg_sweep", "vg_max_wave_speed", "vg_max_wave_speed_cells", "vg_state_device", "vg_last_launch_count",
-           "vg_last_error_string", "vg_status_string", "vg_max_wave_speed_noalloc", "vg_autotune",
-           "vg_set_launch_config", "vg_get_launch_config", "vg_batch_create", "vg_batch_destroy",
-           "vg_batch_total_cells", "vg_batch_upload", "vg_batch_download", "vg_batch_run",
-           "vg_batch_last_launch_count", "vg_batch_gradient"]
-NUM_XCFG, NUM_YCFG = 5, 6
+EXPORTS = ["vg_create", "vg_destroy", "vg_model_nvar", "vg_upload_primitive", "vg_download_primitive", "vg_run",
+           "vg_solve", "vg_sweep", "vg_max_wave_speed", "vg_max_wave_speed_cells", "vg_state_device",
+           "vg_last_launch_count", "vg_last_error_string", "vg_status_string", "vg_max_wave_speed_noalloc",
+           "vg_autotune", "vg_set_launch_config", "vg_get_launch_config", "vg_set_schedule", "vg_get_schedule",
+           "vg_batch_create", "vg_batch_destroy", "vg_batch_total_cells", "vg_batch_upload", "vg_batch_download",
+           "vg_batch_run", "vg_batch_last_launch_count", "vg_batch_gradient"]
+NUM_XCFG, NUM_YCFG, NUM_SCHED = 5, 6, 2
 
 NOALLOC_MAX_ROWS = 65536
 
@@ -94,6 +94,8 @@ def lib():
                                                 ctypes.c_int, D, vp, vp]
         L.vg_autotune.argtypes = [vp, ctypes.POINTER(RunConfig), ctypes.c_int, ctypes.POINTER(ctypes.c_float), vp]
         L.vg_set_launch_config.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+        L.vg_set_schedule.argtypes = [vp, ctypes.c_int]
+        L.vg_get_schedule.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
         L.vg_get_launch_config.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                            ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_char_p)]
         L.vg_last_launch_count.argtypes = [vp]
@@ -220,11 +222,21 @@ class Solver:
     def autotune(self, dx, cfl, bias=0.0, limiter=SUPERBEE, reps=3, measure=True, stream=None):
         """Pick the fastest sweep tile shapes on the uploaded state; returns (x_times, y_times) in ms."""
         c = RunConfig(dx, cfl, 0.0, 1, bias, limiter, 0, 2)
-        times = (ctypes.c_float * (NUM_XCFG + NUM_YCFG))() if measure else None
+        times = (ctypes.c_float * (NUM_XCFG + NUM_YCFG + NUM_SCHED))() if measure else None
         _check(lib().vg_autotune(self._h, ctypes.byref(c), reps, times, stream))
         if times is None:
             return None
-        return list(times[:NUM_XCFG]), list(times[NUM_XCFG:])
+        self.schedule_times = list(times[NUM_XCFG + NUM_YCFG:])  # step tail: CFL maximum fused, separate
+        return list(times[:NUM_XCFG]), list(times[NUM_XCFG:NUM_XCFG + NUM_YCFG])
+
+    def schedule(self):
+        """0: the next step's CFL maximum folded into the last X sweep; 1: a separate reduction pass."""
+        v = ctypes.c_int()
+        _check(lib().vg_get_schedule(self._h, ctypes.byref(v)))
+        return v.value
+
+    def set_schedule(self, cfl_separate):
+        return _check(lib().vg_set_schedule(self._h, int(cfl_separate)))
 
     def launch_config(self):
         x, y = ctypes.c_int(), ctypes.c_int()

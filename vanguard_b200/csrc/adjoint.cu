@@ -673,6 +673,7 @@ extern "C" vg_status vg_batch_gradient(vg_batch* b, const double* target_rho, do
     if (!b || !target_rho || steps < 1 || !(cfl > 0.0) || limiter < 0 || limiter > 2)
         return afail(VG_EINVAL, "bad vg_batch_gradient argument");
     if (checkpoints < 1) return afail(VG_EINVAL, "need at least one checkpoint slot (the initial state)");
+    if (!b->has_state) return afail(VG_EINVAL, "no state uploaded");
     checkpoints = std::min(checkpoints, steps);
     cudaStream_t st = (cudaStream_t)stream;
     VA_CUDA(cudaSetDevice(b->device));
@@ -724,7 +725,7 @@ extern "C" vg_status vg_batch_gradient(vg_batch* b, const double* target_rho, do
         e = cudaMemcpyAsync(grad_gamma, b->d_ggam, sizeof(double) * b->ninst, out_kind, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return afail(VG_ECUDA, std::string("vg_batch_gradient: ") + cudaGetErrorString(e));
-    if (err) return afail(VG_ENAN, "non-finite or non-positive density/pressure produced");
+    if (err) return afail(VG_ENAN, "non-finite value, non-positive density or pressure at or below -p_inf produced");
     if (grad_planes && !is_device)
         for (long i = 0; i < n; i++) grad_planes[2 * n + i] = grad_planes[3 * n + i] = grad_planes[5 * n + i] = 0.0;
     if (loss) {

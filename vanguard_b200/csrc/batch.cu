@@ -17,9 +17,11 @@
 #include <cmath>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/vanguard_slic.h"
+#include "host_planes.h"
 #include "batch_internal.cuh"
 #include "physics_fp64.cuh"
 #include "slic_kernels.cuh"
@@ -390,46 +392,57 @@ vg_status vg_batch_upload(vg_batch* b, const double* planes, int is_device, void
     if (!b || !planes) return bfail(VG_EINVAL, "null argument");
     cudaStream_t st = (cudaStream_t)stream;
     const long n = b->total;
-    if (!is_device) {
-        for (long i = 0; i < n; i++)
-            if (planes[2 * n + i] != 0.0 || planes[3 * n + i] != 0.0 || planes[5 * n + i] != 1.0)
-                return bfail(VG_EUNSUPPORTED, "batched 1D Euler needs v == w == 0 and lambda == 1");
-    }
+    // v, w and lambda are not carried: their check runs on host threads while rho, u and p are in flight, and a
+    // failed check leaves the batch without a state
+    b->has_state = false;
+    bool bad = false;
+    std::thread checker;
+    if (!is_device)
+        checker = std::thread([&]() {
+            bad = vg::host::any_differs({planes + 2 * n, planes + 3 * n}, 0.0, n) ||
+                  vg::host::any_differs({planes + 5 * n}, 1.0, n);
+        });
     const int ref[3] = {0, 1, 4};
-    for (int k = 0; k < 3; k++)
-        VB_CUDA(cudaMemcpyAsync(b->buf[0] + k * n, planes + ref[k] * n, sizeof(double) * n,
-                                is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
-    VB_CUDA(cudaStreamSynchronize(st));
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; k < 3 && e == cudaSuccess; k++)
+        e = cudaMemcpyAsync(b->buf[0] + k * n, planes + ref[k] * n, sizeof(double) * n,
+                            is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (checker.joinable()) checker.join();
+    VB_CUDA(e);
+    if (bad) return bfail(VG_EUNSUPPORTED, "batched 1D Euler needs v == w == 0 and lambda == 1");
     b->cur = 0;
+    b->has_state = true;
     return VG_OK;
 }
 
 vg_status vg_batch_download(vg_batch* b, double* planes, int is_device, void* stream) {
     if (!b || !planes) return bfail(VG_EINVAL, "null argument");
+    if (!b->has_state) return bfail(VG_EINVAL, "no state uploaded");
     cudaStream_t st = (cudaStream_t)stream;
     const long n = b->total;
     const int ref[3] = {0, 1, 4};
     for (int k = 0; k < 3; k++)
         VB_CUDA(cudaMemcpyAsync(planes + ref[k] * n, b->buf[b->cur] + k * n, sizeof(double) * n,
                                 is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
-    VB_CUDA(cudaStreamSynchronize(st));
-    if (!is_device) {
-        for (long i = 0; i < n; i++) {
-            planes[2 * n + i] = 0.0;
-            planes[3 * n + i] = 0.0;
-            planes[5 * n + i] = 1.0;
-        }
+    if (!is_device) {  // the constant planes are filled while the copies run
+        vg::host::fill_plane(planes + 2 * n, 0.0, n);
+        vg::host::fill_plane(planes + 3 * n, 0.0, n);
+        vg::host::fill_plane(planes + 5 * n, 1.0, n);
     } else {
         std::vector<double> z(n, 0.0), o(n, 1.0);
-        VB_CUDA(cudaMemcpy(planes + 2 * n, z.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
-        VB_CUDA(cudaMemcpy(planes + 3 * n, z.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
-        VB_CUDA(cudaMemcpy(planes + 5 * n, o.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+        VB_CUDA(cudaMemcpyAsync(planes + 2 * n, z.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st));
+        VB_CUDA(cudaMemcpyAsync(planes + 3 * n, z.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st));
+        VB_CUDA(cudaMemcpyAsync(planes + 5 * n, o.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st));
+        VB_CUDA(cudaStreamSynchronize(st));
     }
+    VB_CUDA(cudaStreamSynchronize(st));
     return VG_OK;
 }
 
 vg_status vg_batch_run(vg_batch* b, double cfl, int steps, double bias, int limiter, double* dt_last, void* stream) {
     if (!b || steps < 1 || !(cfl > 0.0)) return bfail(VG_EINVAL, "bad vg_batch_run argument");
+    if (!b->has_state) return bfail(VG_EINVAL, "no state uploaded");
     cudaStream_t st = (cudaStream_t)stream;
     VB_CUDA(cudaSetDevice(b->device));
     // state to buffer 0 so the captured graph always starts there
@@ -470,7 +483,7 @@ vg_status vg_batch_run(vg_batch* b, double cfl, int steps, double bias, int limi
     VB_CUDA(cudaMemcpyAsync(&err, b->d_err, sizeof(err), cudaMemcpyDeviceToHost, st));
     if (dt_last) VB_CUDA(cudaMemcpyAsync(dt_last, b->d_dt, sizeof(double) * b->ninst, cudaMemcpyDeviceToHost, st));
     VB_CUDA(cudaStreamSynchronize(st));
-    if (err) return bfail(VG_ENAN, "non-finite or non-positive density/pressure produced");
+    if (err) return bfail(VG_ENAN, "non-finite value, non-positive density or pressure at or below -p_inf produced");
     return VG_OK;
 }
 

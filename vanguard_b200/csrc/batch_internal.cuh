@@ -72,6 +72,7 @@ struct vg_batch {
     unsigned int* d_done = nullptr;
     unsigned int* d_err = nullptr;
     int cur = 0;
+    bool has_state = false;  // a successful vg_batch_upload has filled buf[0]
     int grid = 0;
     cudaStream_t cap = nullptr;
     cudaGraphExec_t graph = nullptr;

@@ -13,6 +13,8 @@
 // sliding window of the stencil in registers; a warp reads 32 consecutive doubles per plane-row.
 #pragma once
 
+#include <utility>
+
 #include "vg_common.cuh"
 
 namespace vg {
@@ -153,11 +155,22 @@ struct pressure_rule<M, decltype((void)&M::positive_pressure)> {
     __device__ static bool positive(const typename M::P& q) { return M::positive_pressure(q); }
 };
 
+// The pressure at or below which a state has no real sound speed: -p_inf for the stiffened-gas models whose
+// parameters carry p_inf (c^2 = gamma (p + p_inf) / rho, Euler/eulerequationofstate.cpp:23-29), 0 for the others.
+template <class P, class = void>
+struct pressure_floor {
+    __device__ static double of(const P&) { return 0.0; }
+};
+template <class P>
+struct pressure_floor<P, decltype((void)std::declval<P>().pinf)> {
+    __device__ static double of(const P& q) { return -q.pinf; }
+};
+
 template <class M>
 __device__ __forceinline__ bool bad_state(const double* W, const typename M::P& q) {
     double rho = M::density(W), p = M::pressure(W);
     if (!pressure_rule<M>::positive(q)) return !(rho > 0.0) || !isfinite(rho) || !isfinite(p);
-    return !(rho > 0.0) || !(p > 0.0) || !isfinite(rho) || !isfinite(p);
+    return !(rho > 0.0) || !(p > pressure_floor<typename M::P>::of(q)) || !isfinite(rho) || !isfinite(p);
 }
 
 // ----------------------------------------------------------------------------------------- X sweep

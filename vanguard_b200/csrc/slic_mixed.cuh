@@ -184,7 +184,7 @@ template <class M>
 __device__ __forceinline__ bool bad_state_mixed(const double* W, const typename M::P& q) {
     double rho = M::density(W), p = M::pressure(W);
     if (!pressure_rule<M>::positive(q)) return !(rho > 0.0) || !isfinite(rho) || !isfinite(p);
-    return !(rho > 0.0) || !(p > 0.0) || !isfinite(rho) || !isfinite(p);
+    return !(rho > 0.0) || !(p > pressure_floor<typename M::P>::of(q)) || !isfinite(rho) || !isfinite(p);
 }
 
 // ----------------------------------------------------------------------------------------- X sweep

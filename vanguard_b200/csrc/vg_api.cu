@@ -4,6 +4,7 @@
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <climits>
 #include <cmath>
 #include <cstdio>
@@ -11,9 +12,11 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/vanguard_slic.h"
+#include "host_planes.h"
 #include "vg_ops.h"
 
 using vg::Ctrl;
@@ -91,6 +94,7 @@ struct vg_solver {
     } g;
     long last_launches = 0;
     int xcfg = 0, ycfg = 0;   // launch configuration of each sweep (sweep_table.cuh)
+    int cfl_sep = 0;          // schedule: 0 folds the next step's CFL maximum into the last sweep, 1 a separate pass
     // TMA tensor maps over buf[0] and buf[1] for the TMA-staged X sweep (device memory; null: none)
     CUtensorMap* d_tmaps = nullptr;
     int tmap_planes = 0;
@@ -160,7 +164,7 @@ void build_tmaps(vg_solver* s, int planes) {
 // optionally persisted in the text file named by VG_TUNE_CACHE ("key xcfg ycfg" per line).
 struct TuneEntry {
     std::string key;
-    int xcfg, ycfg;
+    int xcfg, ycfg, sched;
 };
 std::vector<TuneEntry> g_tune_cache;
 bool g_tune_loaded = false;
@@ -181,26 +185,30 @@ void tune_cache_load() {
     if (!path) return;
     FILE* f = std::fopen(path, "r");
     if (!f) return;
-    char key[160];
-    int x, y;
-    while (std::fscanf(f, "%159s %d %d", key, &x, &y) == 3)
-        if (x >= 0 && x < vg::kNumXCfg && y >= 0 && y < vg::kNumYCfg) g_tune_cache.push_back({key, x, y});
+    char line[256], key[160];
+    while (std::fgets(line, sizeof(line), f)) {
+        int x, y, sc = 0;
+        const int got = std::sscanf(line, "%159s %d %d %d", key, &x, &y, &sc);  // lines without a schedule: fused
+        if (got >= 3 && x >= 0 && x < vg::kNumXCfg && y >= 0 && y < vg::kNumYCfg && (sc == 0 || sc == 1))
+            g_tune_cache.push_back({key, x, y, sc});
+    }
     std::fclose(f);
 }
 
-void tune_cache_store(const std::string& key, int x, int y) {
+void tune_cache_store(const std::string& key, int x, int y, int sched) {
     for (auto& e : g_tune_cache)
         if (e.key == key) {
             e.xcfg = x;
             e.ycfg = y;
+            e.sched = sched;
             return;
         }
-    g_tune_cache.push_back({key, x, y});
+    g_tune_cache.push_back({key, x, y, sched});
     const char* path = std::getenv("VG_TUNE_CACHE");
     if (!path) return;
     FILE* f = std::fopen(path, "a");
     if (!f) return;
-    std::fprintf(f, "%s %d %d\n", key.c_str(), x, y);
+    std::fprintf(f, "%s %d %d %d\n", key.c_str(), x, y, sched);
     std::fclose(f);
 }
 
@@ -274,7 +282,7 @@ int enqueue_step(vg_solver* s, const vg_run_config& c, int from, cudaStream_t st
     if (stiff) relax();
     // Without a trailing source pass the last sweep folds the next step's CFL maximum into its epilogue;
     // with one, a separate reduction runs after it.
-    const int fuse_wave = sub == 0 && !stiff && !reinit;
+    const int fuse_wave = sub == 0 && !stiff && !reinit && !s->cfl_sep;
     if (s->dims == 1) {
         a.in = s->buf[from];
         a.out = s->buf[1 - from];
@@ -328,7 +336,7 @@ int kernels_per_step(const vg_solver* s, int sub, bool stiff = false, bool reini
     if (forcing) n += 2 * sub * vg::kForcingLaunches;                                  // source sub-cycles
     if (stiff) n += 2;                                                                 // two relaxations
     if (reinit) n += s->dims == 1 ? 1 : 2;                                             // the reinitialisation
-    if (forcing || stiff || reinit) n += 1;                                            // the separate CFL maximum
+    if (forcing || stiff || reinit || s->cfl_sep) n += 1;                              // the separate CFL maximum
     return n;
 }
 
@@ -379,6 +387,15 @@ vg_status ensure_graphs(vg_solver* s, const vg_run_config& c) {
     s->g.cfg = c;
     s->g.variant = s->variant;
     return VG_OK;
+}
+
+// One plane between a pitched device buffer and a dense one (or any two buffers): a single linear copy when both
+// are dense, a 2D copy otherwise.
+cudaError_t copy_plane(double* dst, long dpitch, const double* src, long spitch, int nx, int ny, cudaMemcpyKind kind,
+                       cudaStream_t st) {
+    if (dpitch == nx && spitch == nx) return cudaMemcpyAsync(dst, src, sizeof(double) * nx * ny, kind, st);
+    return cudaMemcpy2DAsync(dst, sizeof(double) * dpitch, src, sizeof(double) * spitch, sizeof(double) * nx, ny, kind,
+                             st);
 }
 
 // The CFL maximum of the uploaded state; with_corners adds the default-constructed corner ghosts of a 2D grid.
@@ -494,60 +511,72 @@ vg_status vg_upload_primitive(vg_solver* s, const double* planes, int is_device,
     if (!s || !planes) return fail(VG_EINVAL, "null argument");
     cudaStream_t st = (cudaStream_t)stream;
     const long n = (long)s->d.nx * s->d.ny;
+    const int model = s->d.model;
+    // Planes the compiled variants do not carry must hold their constant (0, or Euler's lambda = 1).  Where the
+    // variant does not depend on them, the check runs on host threads while the carried planes are in flight;
+    // where it does (1D Euler's v, MHD's w and Bz), it runs first.
     int variant;
-    if (s->d.model == VG_MODEL_EULER) {
-        // Euler carries rho, u, [v], p: w must be 0 and lambda 1 (then rho*lambda tracks rho exactly).
-        bool zero_v = true;
+    std::vector<const double*> zero_planes;
+    const double* one_plane = nullptr;
+    bool check_after = false;
+    if (model == VG_MODEL_EULER) {
         if (is_device) {
-            variant = vg::V_EULER2;  // device input: checked on the host is not possible; carry v, trust w/lambda
+            variant = vg::V_EULER2;  // device input cannot be scanned on the host: carry v, trust w and lambda
+        } else if (s->dims == 2) {
+            variant = vg::V_EULER2;
+            zero_planes = {planes + 3 * n};
+            one_plane = planes + 5 * n;
+            check_after = true;
         } else {
-            const double *v = planes + 2 * n, *w = planes + 3 * n, *lam = planes + 5 * n;
-            for (long i = 0; i < n; i++) {
-                if (w[i] != 0.0 || lam[i] != 1.0)
-                    return fail(VG_EUNSUPPORTED, "Euler state with w != 0 or lambda != 1 needs the 6-component variant");
-                if (v[i] != 0.0) zero_v = false;
-            }
-            variant = (s->dims == 1 && zero_v) ? vg::V_EULER1 : vg::V_EULER2;
+            if (vg::host::any_differs({planes + 3 * n}, 0.0, n) || vg::host::any_differs({planes + 5 * n}, 1.0, n))
+                return fail(VG_EUNSUPPORTED, "Euler state with w != 0 or lambda != 1 needs the 6-component variant");
+            variant = vg::host::any_differs({planes + 2 * n}, 0.0, n) ? vg::V_EULER2 : vg::V_EULER1;
         }
-    } else if (s->d.model == VG_MODEL_EULER_REDUCED || s->d.model == VG_MODEL_EULER_MULTIPHYSICS) {
+    } else if (model == VG_MODEL_EULER_REDUCED || model == VG_MODEL_EULER_MULTIPHYSICS) {
         // the two-material models carry every plane but w, which must be 0
         if (!is_device) {
-            const double* w = planes + 3 * n;
-            for (long i = 0; i < n; i++)
-                if (w[i] != 0.0) return fail(VG_EUNSUPPORTED, "two-material state with w != 0");
+            zero_planes = {planes + 3 * n};
+            check_after = true;
         }
-        variant = s->d.model == VG_MODEL_EULER_REDUCED ? vg::V_RED6 : vg::V_MPH7;
-    } else if (s->d.model == VG_MODEL_MHD_REDUCED) {
+        variant = model == VG_MODEL_EULER_REDUCED ? vg::V_RED6 : vg::V_MPH7;
+    } else if (model == VG_MODEL_MHD_REDUCED) {
         variant = vg::V_MRED11;
-    } else if (s->d.model == VG_MODEL_MHD_INTERMEDIATE) {
+    } else if (model == VG_MODEL_MHD_INTERMEDIATE) {
         variant = vg::V_MINT12;
-    } else if (s->d.model == VG_MODEL_HPR) {
+    } else if (model == VG_MODEL_HPR) {
         // a solid equation of state or plasticity selects the instantiation that carries them
         variant = (s->d.params[12] != 0.0 || s->d.params[17] != 0.0) ? vg::V_HPR17S : vg::V_HPR17;
     } else {
-        bool reduced = true;
-        if (!is_device) {
-            const double *w = planes + 3 * n, *bz = planes + 7 * n;
-            for (long i = 0; i < n && reduced; i++)
-                if (w[i] != 0.0 || bz[i] != 0.0) reduced = false;
-        } else {
-            reduced = false;
-        }
+        const bool reduced = !is_device && !vg::host::any_differs({planes + 3 * n, planes + 7 * n}, 0.0, n);
         variant = reduced ? vg::V_MHD7 : vg::V_MHD9;
     }
     const Ops* ops = s->d.precision == VG_MIXED ? vg::ops_mixed(variant) : vg::ops_fp64(variant);
     if (!ops) return fail(VG_EUNSUPPORTED, "no kernel variant for this state");
+    // the device state is replaced from here on: until this call succeeds the solver holds none
+    s->ops = nullptr;
     s->variant = variant;
-    s->ops = ops;
     s->cur = 0;
     if (ops->tma_planes > 0) build_tmaps(s, ops->tma_planes);
-    for (int k = 0; k < ops->nw; k++) {
-        const double* src = planes + (long)kPlanes[variant][k] * n;
-        VG_CUDA(cudaMemcpy2DAsync(s->buf[0] + k * s->plane, sizeof(double) * s->pitch, src, sizeof(double) * s->d.nx,
-                                  sizeof(double) * s->d.nx, s->d.ny, is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
-                                  st));
+    bool bad = false;
+    std::thread checker;
+    if (check_after)
+        checker = std::thread([&]() {
+            bad = vg::host::any_differs(zero_planes, 0.0, n) || (one_plane && vg::host::any_differs({one_plane}, 1.0, n));
+        });
+    const cudaMemcpyKind kind = is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; k < ops->nw && e == cudaSuccess; k++)
+        e = copy_plane(s->buf[0] + k * s->plane, s->pitch, planes + (long)kPlanes[variant][k] * n, s->d.nx, s->d.nx,
+                       s->d.ny, kind, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (checker.joinable()) checker.join();
+    if (e != cudaSuccess) return cuda_fail(e, "vg_upload_primitive");
+    if (bad) {
+        if (model == VG_MODEL_EULER)
+            return fail(VG_EUNSUPPORTED, "Euler state with w != 0 or lambda != 1 needs the 6-component variant");
+        return fail(VG_EUNSUPPORTED, "two-material state with w != 0");
     }
-    VG_CUDA(cudaStreamSynchronize(st));
+    s->ops = ops;
     return VG_OK;
 }
 
@@ -558,14 +587,14 @@ vg_status vg_download_primitive(vg_solver* s, double* planes, int is_device, voi
     const long n = (long)s->d.nx * s->d.ny;
     const int nref = ref_nvar(s->d.model);
     bool carried[17] = {false};
+    const cudaMemcpyKind kind = is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
     for (int k = 0; k < s->ops->nw; k++) {
         int r = kPlanes[s->variant][k];
         carried[r] = true;
-        VG_CUDA(cudaMemcpy2DAsync(planes + (long)r * n, sizeof(double) * s->d.nx, s->buf[s->cur] + k * s->plane,
-                                  sizeof(double) * s->pitch, sizeof(double) * s->d.nx, s->d.ny,
-                                  is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
+        VG_CUDA(copy_plane(planes + (long)r * n, s->d.nx, s->buf[s->cur] + k * s->plane, s->pitch, s->d.nx, s->d.ny,
+                           kind, st));
     }
-    // planes that are not carried hold their constant value (0, or lambda = 1)
+    // planes that are not carried hold their constant value (0, or lambda = 1): filled while the copies run
     for (int r = 0; r < nref; r++) {
         if (carried[r]) continue;
         double val = (s->d.model == VG_MODEL_EULER && r == 5) ? 1.0 : 0.0;
@@ -574,7 +603,7 @@ vg_status vg_download_primitive(vg_solver* s, double* planes, int is_device, voi
             VG_CUDA(cudaMemcpyAsync(planes + (long)r * n, tmp.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st));
             VG_CUDA(cudaStreamSynchronize(st));
         } else {
-            for (long i = 0; i < n; i++) planes[(long)r * n + i] = val;
+            vg::host::fill_plane(planes + (long)r * n, val, n);
         }
     }
     VG_CUDA(cudaStreamSynchronize(st));
@@ -661,7 +690,7 @@ vg_status vg_run(vg_solver* s, const vg_run_config* cfg, int* steps_taken, doubl
     if (steps_taken) *steps_taken = h->it;
     if (t_reached) *t_reached = h->t;
     if (h->err & vg::ERR_TIMEOUT) return fail(VG_ETIMEOUT, "a bounded wait of the TMA-staged sweep gave up");
-    if (h->err) return fail(VG_ENAN, "non-finite or non-positive density/pressure produced");
+    if (h->err) return fail(VG_ENAN, "non-finite value, non-positive density or pressure at or below -p_inf produced");
     return VG_OK;
 }
 
@@ -742,7 +771,10 @@ vg_status vg_autotune(vg_solver* s, const vg_run_config* cfg, int reps, float* t
     std::string key = tune_key(s);
     if (!times_ms) {
         for (auto& e : g_tune_cache)
-            if (e.key == key) return vg_set_launch_config(s, e.xcfg, e.ycfg);
+            if (e.key == key) {
+                vg_status vs = vg_set_launch_config(s, e.xcfg, e.ycfg);
+                return vs != VG_OK ? vs : vg_set_schedule(s, e.sched);
+            }
     }
     cudaStream_t st = (cudaStream_t)stream;
     // Time every candidate on the uploaded state: out-of-place sweeps into the spare buffer, with the
@@ -790,11 +822,61 @@ vg_status vg_autotune(vg_solver* s, const vg_run_config* cfg, int reps, float* t
             }
         }
     }
+    // Schedule: where the next step's CFL maximum is taken.  Folded into the last X sweep's epilogue it costs no
+    // extra pass over the state but adds the wave speed's registers to the sweep; a separate reduction reads the
+    // state once more.  Both give the same bits (the maximum of the same values); time the step's tail each way
+    // with the chosen X shape.
+    int sched = 0;
+    {
+        const vg::SweepFn xfn = s->ops->x[pick[0]];
+        a.tmap = tmap_for(s, a.in);
+        float t2[2] = {0.0f, 0.0f};
+        for (int sc = 0; sc < 2; sc++) {
+            SweepArgs b = a;
+            b.accumulate_wave = sc == 0;
+            SweepArgs m = base_args(s);
+            m.in = a.out;
+            auto tail = [&]() {
+                cudaError_t e = xfn(b, st);
+                if (sc == 1 && e == cudaSuccess) e = s->ops->max_wave(m, st);
+                return e;
+            };
+            cudaError_t e = tail();  // warm-up
+            if (e != cudaSuccess) {
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                return cuda_fail(e, "autotune launch");
+            }
+            VG_CUDA(cudaEventRecord(e0, st));
+            for (int r = 0; r < reps; r++) tail();
+            VG_CUDA(cudaEventRecord(e1, st));
+            VG_CUDA(cudaEventSynchronize(e1));
+            VG_CUDA(cudaEventElapsedTime(&t2[sc], e0, e1));
+            t2[sc] /= reps;
+            if (times_ms) times_ms[vg::kNumXCfg + vg::kNumYCfg + sc] = t2[sc];
+        }
+        sched = t2[1] < t2[0] ? 1 : 0;
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     VG_CUDA(cudaGetLastError());
-    tune_cache_store(key, pick[0], pick[1]);
-    return vg_set_launch_config(s, pick[0], pick[1]);
+    tune_cache_store(key, pick[0], pick[1], sched);
+    vg_status vs2 = vg_set_launch_config(s, pick[0], pick[1]);
+    return vs2 != VG_OK ? vs2 : vg_set_schedule(s, sched);
+}
+
+vg_status vg_set_schedule(vg_solver* s, int cfl_separate) {
+    if (!s) return fail(VG_EINVAL, "null solver");
+    if (cfl_separate != 0 && cfl_separate != 1) return fail(VG_EINVAL, "cfl_separate must be 0 or 1");
+    if (s->cfl_sep != cfl_separate) destroy_graphs(s);
+    s->cfl_sep = cfl_separate;
+    return VG_OK;
+}
+
+vg_status vg_get_schedule(vg_solver* s, int* cfl_separate) {
+    if (!s || !cfl_separate) return fail(VG_EINVAL, "null argument");
+    *cfl_separate = s->cfl_sep;
+    return VG_OK;
 }
 
 }  // extern "C"
