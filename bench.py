@@ -637,6 +637,7 @@ def hpr_leg(local, stream, sh):
     for form in ("fp64", "mixed", "stiff_fp64", "stiff_mixed"):
         res[form]["roofline"] = hbm_roofline(res[form]["cell_updates_per_s"], 880, "whole step: (3 sweeps + 2 source "
                                              "passes) x 2 x 11 components x 8 B")
+    res["source_adjoint"] = source_adjoint_cost(local, stream, sh, W, prm, tau1, tau2, S_dt=dt_sub_of(res, sub))
     res["chosen_form"] = ("stiff_mixed: the flux in FP32 (reconstruction, half-step evolution, FORCE) with the stiff "
                           "relaxation source, pressure recovery, CFL maximum and update in FP64")
     res["subcycles"] = sub
@@ -656,6 +657,54 @@ def hpr_leg(local, stream, sh):
                                          f"sub-cycles per half step) on a {n}x{rows} strip of the workload ({dt:.2f} s)"}
         res["fp64_vs_cpu_reference"] = res["fp64"]["cell_updates_per_s"] / res["cpu_baseline"]["value"]
     return res
+
+
+def dt_sub_of(res, sub):
+    """The RK4 forcing sub-step of the C4 run's last time step: 0.5 dt / sub (Solvers/hprsecondordersolver.cpp:516)."""
+    t, it = res["fp64"]["t"], res["fp64"]["steps"]
+    return 0.5 * (t / max(it, 1)) / sub
+
+
+def source_adjoint_cost(local, stream, sh, W, prm, tau1, tau2, S_dt):
+    """The HPR relaxation source's discrete adjoint at the C4 scale: every cell of the 1024^2 initial field as a
+    homogeneous relaxation problem (vg_source_batch), one time step's worth of the forcing's sub-steps (2 sub of
+    length S_dt), forward against the gradient of L = <lambda, W(T)> with binomial checkpointing and with every
+    state stored; device-timed (CUDA events on the launching stream)."""
+    import torch
+    import vanguard_b200 as vg
+    n = W.shape[1] * W.shape[2]
+    W0 = np.ascontiguousarray(W.reshape(17, n))
+    tau = np.stack([np.full(n, tau1), np.full(n, tau2)])
+    steps = 26
+    dev = f"cuda:{local}"
+    lam = torch.from_numpy(np.random.default_rng(SEED + 7).standard_normal((17, n))).to(dev)
+    g, gt = torch.empty((17, n), dtype=torch.float64, device=dev), torch.empty((2, n), dtype=torch.float64, device=dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    out = {"workload": f"{n} homogeneous HPR cells (the C4 initial field), {steps} source steps of {S_dt:.3e}",
+           "cells": n, "steps": steps}
+    with vg.SourceBatch(n, prm, device=local) as b:
+        b.upload(W0, tau, stream=sh)
+        b.run(S_dt, steps, stream=sh)
+        b.upload(W0, tau, stream=sh)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        b.run(S_dt, steps, stream=sh)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        fwd = e0.elapsed_time(e1)
+        out["forward_ms"] = fwd
+        b.upload(W0, tau, stream=sh)
+        for name, ck in (("binomial", 6), ("store_all", steps)):
+            b.gradient(lam, S_dt, steps, checkpoints=ck, out=(g, gt), stream=sh)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            _, _, fw, aw = b.gradient(lam, S_dt, steps, checkpoints=ck, out=(g, gt), stream=sh)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            out[f"adjoint_{name}"] = {"checkpoints": ck, "ms": ms, "ratio_vs_forward": ms / fwd, "forward_steps": fw,
+                                      "reversed_steps": aw}
+    return out
 
 
 def sod_leg(local, stream, sh):

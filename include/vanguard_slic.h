@@ -236,6 +236,37 @@ vg_status vg_batch_gradient(vg_batch* b, const double* target_rho, double cfl, i
                             int checkpoints, double* loss, double* grad_planes, double* grad_gamma, int is_device,
                             long* forward_steps, long* adjoint_steps, void* stream);
 
+/* ---- Homogeneous HPR relaxation batches and their discrete adjoint.  No counterpart in the reference (it has no
+ * batches and no derivatives); each step is the reference's own source step on a spatially uniform field: one
+ * sub-cycle of HPRForcingSolver's RK4 (Solvers/hprforcingsolver.cpp:332-357, the source terms of
+ * HPRStateVector::computeSourceTermVector, HPR/hprstatevector.cpp:312-366, and HPRSourceTerms,
+ * HPR/hprsourceterms.cpp:7-39) with zero limiter bias, where the fractional flux predictor reduces to its
+ * primitive round trip; steps equal that forcing bit for bit up to pow's last place.  A batch holds `ncell`
+ * independent cells of one HPR material (params: the HPR block of vg_grid_desc; StiffenedGas equation of state and
+ * elastic strain relaxation only) with relaxation times tau1, tau2 per cell.
+ * Planes at this boundary: the 17 HPR primitive planes of all cells (17 x ncell, HPR/hprstatevector.cpp:50-73);
+ * tau: 2 x ncell (all tau1, then all tau2), or NULL for the params' tau1 and tau2 in every cell.
+ * vg_source_batch_run advances the batch's state by `steps` steps of length h.
+ * vg_source_batch_gradient is the adjoint of vg_source_batch_run(h, steps) from the batch's current state, which
+ * it leaves unchanged: given the cotangent dL/dW(T) (17 x ncell) of any loss of the final primitives, it returns
+ * dL/dW(0) (17 x ncell, nullable) and dL/dtau (2 x ncell, nullable).  The source is smooth where det A > 0, so no
+ * subgradient choice arises; the primitive round trips are identities of exact arithmetic and are differentiated
+ * as such; a non-thermal material's J passes through unchanged.  `checkpoints` >= 1 state slots per cell (slot 0
+ * the initial state; capped at steps) bound the memory to (checkpoints + 1) states; steps are recomputed on
+ * Griewank's binomial schedule (checkpoints == steps stores every state).  forward_steps / adjoint_steps
+ * (nullable) receive the forward steps advanced (recomputation included) and the steps reversed.  Host or device
+ * arrays per is_device; returns when done. */
+typedef struct vg_source_batch vg_source_batch;
+vg_status vg_source_batch_create(int ncell, const double* params, int device, vg_source_batch** out);
+vg_status vg_source_batch_destroy(vg_source_batch* b);
+vg_status vg_source_batch_upload(vg_source_batch* b, const double* planes, const double* tau, int is_device,
+                                 void* stream);
+vg_status vg_source_batch_download(vg_source_batch* b, double* planes, int is_device, void* stream);
+vg_status vg_source_batch_run(vg_source_batch* b, double h, int steps, void* stream);
+vg_status vg_source_batch_gradient(vg_source_batch* b, const double* cotangent, double h, int steps, int checkpoints,
+                                   double* grad_planes, double* grad_tau, int is_device, long* forward_steps,
+                                   long* adjoint_steps, void* stream);
+
 /* Rows accepted by vg_max_wave_speed_noalloc: the size of its static scratch array (8 bytes per row,
  * 512 KiB, held on every GPU that loads the library until the process exits). */
 #define VG_NOALLOC_MAX_ROWS 65536

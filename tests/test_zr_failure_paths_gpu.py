@@ -2,9 +2,10 @@
 
 The reference has no error reporting: solve() and the per-sweep functions return whatever the arithmetic gives,
 NaN and negative pressures included (Solvers/secondordersolver.cpp:288-314).  The device keeps those results bit
-for bit (NaN where the reference has NaN) and, in addition, flags every update that leaves a non-finite or
-non-positive density or pressure: vg_run and vg_solve return VG_ENAN after the run, and vg_solve still delivers
-the planes.  No device fault is involved: the poison is ordinary floating-point data.
+for bit, NaN where the reference has NaN (in the planes it does not carry too: a non-finite cell's w and lambda
+are NaN in the reference), and, in addition, flags every update that leaves a non-finite value, a non-positive
+density or a pressure at or below -p_inf: vg_run and vg_solve return VG_ENAN after the run, and vg_solve still
+delivers the planes.  No device fault is involved: the poison is ordinary floating-point data.
 """
 import ctypes
 

@@ -53,7 +53,9 @@ EXPORTS = ["vg_create", "vg_destroy", "vg_model_nvar", "vg_upload_primitive", "v
            "vg_last_launch_count", "vg_last_error_string", "vg_status_string", "vg_max_wave_speed_noalloc",
            "vg_autotune", "vg_set_launch_config", "vg_get_launch_config", "vg_set_schedule", "vg_get_schedule",
            "vg_batch_create", "vg_batch_destroy", "vg_batch_total_cells", "vg_batch_upload", "vg_batch_download",
-           "vg_batch_run", "vg_batch_last_launch_count", "vg_batch_gradient"]
+           "vg_batch_run", "vg_batch_last_launch_count", "vg_batch_gradient", "vg_source_batch_create",
+           "vg_source_batch_destroy", "vg_source_batch_upload", "vg_source_batch_download", "vg_source_batch_run",
+           "vg_source_batch_gradient"]
 NUM_XCFG, NUM_YCFG, NUM_SCHED = 5, 6, 2
 
 NOALLOC_MAX_ROWS = 65536
@@ -113,6 +115,13 @@ def lib():
         Lp = ctypes.POINTER(ctypes.c_long)
         L.vg_batch_gradient.argtypes = [vp, vp, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                         ctypes.c_int, D, vp, vp, ctypes.c_int, Lp, Lp, vp]
+        L.vg_source_batch_create.argtypes = [ctypes.c_int, D, ctypes.c_int, ctypes.POINTER(vp)]
+        L.vg_source_batch_destroy.argtypes = [vp]
+        L.vg_source_batch_upload.argtypes = [vp, vp, vp, ctypes.c_int, vp]
+        L.vg_source_batch_download.argtypes = [vp, vp, ctypes.c_int, vp]
+        L.vg_source_batch_run.argtypes = [vp, ctypes.c_double, ctypes.c_int, vp]
+        L.vg_source_batch_gradient.argtypes = [vp, vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, vp, vp, ctypes.c_int,
+                                               Lp, Lp, vp]
         L.vg_last_error_string.restype = ctypes.c_char_p
         L.vg_status_string.restype = ctypes.c_char_p
         L.vg_status_string.argtypes = [ctypes.c_int]
@@ -337,3 +346,77 @@ class Batch:
                                        gg.ctypes.data_as(ctypes.c_void_p), 0, ctypes.byref(fw), ctypes.byref(aw),
                                        stream))
         return L.value, g, gg, fw.value, aw.value
+
+
+class SourceBatch:
+    """Homogeneous HPR relaxation cells (vg_source_batch_*): each cell advanced by the reference's source step on a
+    uniform field, and the discrete adjoint of that evolution."""
+
+    def __init__(self, ncell, params, device=0):
+        self.n = int(ncell)
+        prm = np.zeros(MAX_PARAMS)
+        prm[:len(params)] = params
+        self._h = ctypes.c_void_p()
+        _check(lib().vg_source_batch_create(self.n, prm.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), device,
+                                            ctypes.byref(self._h)))
+
+    def close(self):
+        if self._h:
+            lib().vg_source_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @staticmethod
+    def _host(a, shape):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        if a.shape != shape:
+            raise ValueError(f"expected shape {shape}, got {a.shape}")
+        return a
+
+    def upload(self, planes, tau=None, stream=None):
+        """planes: (17, ncell) HPR primitives; tau: (2, ncell) relaxation times or None (the params')."""
+        if hasattr(planes, "data_ptr"):
+            tp = ctypes.c_void_p(tau.data_ptr()) if tau is not None else None
+            return _check(lib().vg_source_batch_upload(self._h, ctypes.c_void_p(planes.data_ptr()), tp, 1, stream))
+        p = self._host(planes, (17, self.n))
+        t = None if tau is None else self._host(tau, (2, self.n))
+        return _check(lib().vg_source_batch_upload(self._h, p.ctypes.data_as(ctypes.c_void_p),
+                                                   None if t is None else t.ctypes.data_as(ctypes.c_void_p), 0, stream))
+
+    def download(self, stream=None):
+        a = np.empty((17, self.n))
+        _check(lib().vg_source_batch_download(self._h, a.ctypes.data_as(ctypes.c_void_p), 0, stream))
+        return a
+
+    def run(self, h, steps, stream=None):
+        return _check(lib().vg_source_batch_run(self._h, h, steps, stream))
+
+    def gradient(self, cotangent, h, steps, checkpoints=None, out=None, stream=None):
+        """Adjoint of run(h, steps) from the current state: returns (dL/dW0 (17, n), dL/dtau (2, n), forward steps,
+        reversed steps) for the cotangent dL/dW(T) (17, n).  With a torch CUDA tensor for the cotangent and out =
+        (grad_planes (17, n), grad_tau (2, n)) CUDA tensors everything stays on the device."""
+        fw, aw = ctypes.c_long(), ctypes.c_long()
+        ck = steps if checkpoints is None else checkpoints
+        if hasattr(cotangent, "data_ptr"):
+            g, gt = out
+            _check(lib().vg_source_batch_gradient(self._h, ctypes.c_void_p(cotangent.data_ptr()), h, steps, ck,
+                                                  ctypes.c_void_p(g.data_ptr()), ctypes.c_void_p(gt.data_ptr()), 1,
+                                                  ctypes.byref(fw), ctypes.byref(aw), stream))
+            return g, gt, fw.value, aw.value
+        lam = self._host(cotangent, (17, self.n))
+        g, gt = np.empty((17, self.n)), np.empty((2, self.n))
+        _check(lib().vg_source_batch_gradient(self._h, lam.ctypes.data_as(ctypes.c_void_p), h, steps, ck,
+                                              g.ctypes.data_as(ctypes.c_void_p), gt.ctypes.data_as(ctypes.c_void_p), 0,
+                                              ctypes.byref(fw), ctypes.byref(aw), stream))
+        return g, gt, fw.value, aw.value

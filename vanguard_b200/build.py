@@ -4,6 +4,7 @@ Each translation unit is compiled by nvcc with its own floating-point contract:
   slic_fp64.cu  -fmad=false  (exact FP64: no FMA contraction, bitwise parity with the reference)
   slic_mixed.cu -fmad=true   (mixed FP32/FP64 form)
   adjoint.cu    -fmad=true   (derivatives; the operands of the forward's branches use explicit __d*_rn operations)
+  source_batch.cu -fmad=false (the HPR source batch: its forward equals the reference's forcing step)
   *.cu (rest)   host code and helpers
 The objects are linked into one shared library with the CUDA runtime linked statically, so the library
 only depends on the driver.  Run `python -m vanguard_b200.build` or call build().
@@ -30,6 +31,7 @@ UNITS = [
     ("vg_noalloc.cu", ["-fmad=false"]),
     ("batch.cu", ["-fmad=false"]),
     ("adjoint.cu", ["-fmad=true"]),
+    ("source_batch.cu", ["-fmad=false"]),
 ]
 
 

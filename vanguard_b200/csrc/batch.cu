@@ -413,6 +413,7 @@ vg_status vg_batch_upload(vg_batch* b, const double* planes, int is_device, void
     if (bad) return bfail(VG_EUNSUPPORTED, "batched 1D Euler needs v == w == 0 and lambda == 1");
     b->cur = 0;
     b->has_state = true;
+    b->nonfinite = false;
     return VG_OK;
 }
 
@@ -429,6 +430,10 @@ vg_status vg_batch_download(vg_batch* b, double* planes, int is_device, void* st
         vg::host::fill_plane(planes + 2 * n, 0.0, n);
         vg::host::fill_plane(planes + 3 * n, 0.0, n);
         vg::host::fill_plane(planes + 5 * n, 1.0, n);
+        if (b->nonfinite) {  // where a cell's state is non-finite the reference's v, w and lambda are NaN too
+            VB_CUDA(cudaStreamSynchronize(st));
+            vg::host::mark_nonfinite(planes, n, 6, 0x13u, 0x2cu);
+        }
     } else {
         std::vector<double> z(n, 0.0), o(n, 1.0);
         VB_CUDA(cudaMemcpyAsync(planes + 2 * n, z.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st));
@@ -483,7 +488,10 @@ vg_status vg_batch_run(vg_batch* b, double cfl, int steps, double bias, int limi
     VB_CUDA(cudaMemcpyAsync(&err, b->d_err, sizeof(err), cudaMemcpyDeviceToHost, st));
     if (dt_last) VB_CUDA(cudaMemcpyAsync(dt_last, b->d_dt, sizeof(double) * b->ninst, cudaMemcpyDeviceToHost, st));
     VB_CUDA(cudaStreamSynchronize(st));
-    if (err) return bfail(VG_ENAN, "non-finite value, non-positive density or pressure at or below -p_inf produced");
+    if (err) {
+        b->nonfinite = true;
+        return bfail(VG_ENAN, "non-finite value, non-positive density or pressure at or below -p_inf produced");
+    }
     return VG_OK;
 }
 

@@ -73,6 +73,7 @@ struct vg_batch {
     unsigned int* d_err = nullptr;
     int cur = 0;
     bool has_state = false;  // a successful vg_batch_upload has filled buf[0]
+    bool nonfinite = false;  // a run since the upload flagged a non-finite or unphysical state
     int grid = 0;
     cudaStream_t cap = nullptr;
     cudaGraphExec_t graph = nullptr;

@@ -8,6 +8,8 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cmath>
+#include <limits>
 #include <thread>
 #include <vector>
 
@@ -44,6 +46,20 @@ inline bool any_differs(const std::vector<const double*>& ps, double val, long n
 
 inline void fill_plane(double* p, double val, long n) {
     parallel(n, [&](long lo, long hi) { std::fill(p + lo, p + hi, val); });
+}
+
+// NaN into the `constant` planes (bit r: plane r) of every cell whose `carried` planes hold a non-finite value.
+inline void mark_nonfinite(double* planes, long n, int nref, unsigned carried, unsigned constant) {
+    parallel(n, [&](long lo, long hi) {
+        for (long i = lo; i < hi; i++) {
+            bool bad = false;
+            for (int r = 0; r < nref; r++)
+                if (carried >> r & 1u) bad |= !std::isfinite(planes[(long)r * n + i]);
+            if (bad)
+                for (int r = 0; r < nref; r++)
+                    if (constant >> r & 1u) planes[(long)r * n + i] = std::numeric_limits<double>::quiet_NaN();
+        }
+    });
 }
 
 }  // namespace host

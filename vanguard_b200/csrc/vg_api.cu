@@ -69,6 +69,25 @@ namespace vg {
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 }  // namespace vg
 
+namespace vg {
+// Device-side fills of the planes a variant does not carry, for downloads into device memory.
+__global__ void fill_plane_kernel(double* p, long n, double val) {
+    const long i = blockIdx.x * 256L + threadIdx.x;
+    if (i < n) p[i] = val;
+}
+// NaN into the `constant` planes of every cell whose `carried` planes hold a non-finite value.
+__global__ void mark_nonfinite_kernel(double* planes, long n, int nref, unsigned carried, unsigned constant) {
+    const long i = blockIdx.x * 256L + threadIdx.x;
+    if (i >= n) return;
+    bool bad = false;
+    for (int r = 0; r < nref; r++)
+        if (carried >> r & 1u) bad |= !isfinite(planes[(long)r * n + i]);
+    if (bad)
+        for (int r = 0; r < nref; r++)
+            if (constant >> r & 1u) planes[(long)r * n + i] = __longlong_as_double(0x7ff8000000000000LL);
+}
+}  // namespace vg
+
 struct vg_solver {
     vg_grid_desc d{};
     int dims = 2;
@@ -568,6 +587,7 @@ vg_status vg_upload_primitive(vg_solver* s, const double* planes, int is_device,
     for (int k = 0; k < ops->nw && e == cudaSuccess; k++)
         e = copy_plane(s->buf[0] + k * s->plane, s->pitch, planes + (long)kPlanes[variant][k] * n, s->d.nx, s->d.nx,
                        s->d.ny, kind, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(&s->ctrl->err, 0, sizeof(unsigned), st);  // a fresh state: no error yet
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (checker.joinable()) checker.join();
     if (e != cudaSuccess) return cuda_fail(e, "vg_upload_primitive");
@@ -586,27 +606,41 @@ vg_status vg_download_primitive(vg_solver* s, double* planes, int is_device, voi
     cudaStream_t st = (cudaStream_t)stream;
     const long n = (long)s->d.nx * s->d.ny;
     const int nref = ref_nvar(s->d.model);
-    bool carried[17] = {false};
+    unsigned carried = 0, constant = 0;
     const cudaMemcpyKind kind = is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    // the error word of the runs and sweeps since the upload: set when a cell became non-finite (or unphysical)
+    VG_CUDA(cudaMemcpyAsync(&s->hctrl->err, &s->ctrl->err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
     for (int k = 0; k < s->ops->nw; k++) {
         int r = kPlanes[s->variant][k];
-        carried[r] = true;
+        carried |= 1u << r;
         VG_CUDA(copy_plane(planes + (long)r * n, s->d.nx, s->buf[s->cur] + k * s->plane, s->pitch, s->d.nx, s->d.ny,
                            kind, st));
     }
     // planes that are not carried hold their constant value (0, or lambda = 1): filled while the copies run
     for (int r = 0; r < nref; r++) {
-        if (carried[r]) continue;
-        double val = (s->d.model == VG_MODEL_EULER && r == 5) ? 1.0 : 0.0;
+        if (carried >> r & 1u) continue;
+        constant |= 1u << r;
+        const double val = (s->d.model == VG_MODEL_EULER && r == 5) ? 1.0 : 0.0;
         if (is_device) {
-            std::vector<double> tmp(n, val);
-            VG_CUDA(cudaMemcpyAsync(planes + (long)r * n, tmp.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st));
-            VG_CUDA(cudaStreamSynchronize(st));
+            vg::fill_plane_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(planes + (long)r * n, n, val);
+            VG_CUDA(cudaGetLastError());
         } else {
             vg::host::fill_plane(planes + (long)r * n, val, n);
         }
     }
     VG_CUDA(cudaStreamSynchronize(st));
+    // The reference recovers every primitive of a cell from its conserved vector (setConservedVariableVector), so
+    // once a cell's state is non-finite its w = (rho w) / rho and lambda = (rho lambda) / rho (MHD: w, Bz) are NaN
+    // as well; the constants above hold only where the carried state is finite.
+    if (constant && s->hctrl->err) {
+        if (is_device) {
+            vg::mark_nonfinite_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(planes, n, nref, carried, constant);
+            VG_CUDA(cudaGetLastError());
+            VG_CUDA(cudaStreamSynchronize(st));
+        } else {
+            vg::host::mark_nonfinite(planes, n, nref, carried, constant);
+        }
+    }
     return VG_OK;
 }
 

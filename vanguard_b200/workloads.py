@@ -356,3 +356,20 @@ def mhd_intermediate_from_reduced(W):
     out[7] = W[6]
     out[8:] = W[7:]
     return out
+
+
+def hpr_relaxation_cells(n, seed=0, thermal=True, tau_range=(1e-3, 1e-2), distortion=0.05):
+    """n homogeneous HPR cells for the source batch: distorted A (I + N(0, distortion^2) per entry), heat flux J,
+    rho ~ U[0.8, 1.2], p ~ U[0.5, 1.5], |u| ~ 0.1; tau1, tau2 log-uniform on tau_range per cell.
+    Returns (W (17, n), tau (2, n), params)."""
+    rng = np.random.default_rng(seed)
+    W = np.zeros((17, n))
+    W[0] = rng.uniform(0.8, 1.2, n)
+    W[1] = rng.uniform(0.5, 1.5, n)
+    A = np.eye(3)[:, :, None] + distortion * rng.standard_normal((3, 3, n))
+    W[2:11] = A.reshape(9, n)
+    W[11:14] = 0.1 * rng.standard_normal((3, n))
+    W[14:17] = 0.1 * rng.standard_normal((3, n))
+    lo, hi = np.log10(tau_range[0]), np.log10(tau_range[1])
+    tau = 10.0 ** rng.uniform(lo, hi, (2, n))
+    return W, tau, hpr_params(tau1=tau[0, 0], tau2=tau[1, 0], thermal=thermal)
