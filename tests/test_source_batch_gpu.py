@@ -107,7 +107,8 @@ def test_checkpoint_schedules_are_bit_identical(gpu):
         g, gt, fw, aw = _adjoint(gpu, W, tau, prm, h, steps, lam, checkpoints=ck)
         assert np.array_equal(g, base[0]) and np.array_equal(gt, base[1]), ck
         assert aw == steps and fw >= base[2]
-    assert base[2] == steps  # every state stored: no recomputation
+    # every state stored: one advance per checkpoint and the step's own recomputation inside each reverse step
+    assert base[2] == 2 * steps - 1
 
 
 def test_autograd_wrapper_gradcheck(gpu):
@@ -118,21 +119,24 @@ def test_autograd_wrapper_gradcheck(gpu):
     W, tau, prm = wl.hpr_relaxation_cells(n, seed=9)
 
     class SourceRun(torch.autograd.Function):
+        """W(T) from W(0) and log(tau): the relaxation times enter through their logarithm, so one finite-difference
+        step size suits both inputs."""
+
         @staticmethod
-        def forward(ctx, w0, t):
-            ctx.save_for_backward(w0, t)
+        def forward(ctx, w0, logtau):
+            ctx.save_for_backward(w0, logtau)
             with gpu.SourceBatch(n, prm) as b:
-                b.upload(w0.detach().numpy(), t.detach().numpy())
+                b.upload(w0.detach().numpy(), np.exp(logtau.detach().numpy()))
                 b.run(h, steps)
                 return torch.from_numpy(b.download())
 
         @staticmethod
         def backward(ctx, grad_out):
-            w0, t = ctx.saved_tensors
-            g, gt, _, _ = _adjoint(gpu, w0.detach().numpy(), t.detach().numpy(), prm, h, steps,
-                                   grad_out.contiguous().numpy())
-            return torch.from_numpy(g), torch.from_numpy(gt)
+            w0, logtau = ctx.saved_tensors
+            tau_ = np.exp(logtau.detach().numpy())
+            g, gt, _, _ = _adjoint(gpu, w0.detach().numpy(), tau_, prm, h, steps, grad_out.contiguous().numpy())
+            return torch.from_numpy(g), torch.from_numpy(gt * tau_)
 
     w0 = torch.tensor(W, dtype=torch.float64, requires_grad=True)
-    t = torch.tensor(tau, dtype=torch.float64, requires_grad=True)
-    assert torch.autograd.gradcheck(SourceRun.apply, (w0, t), eps=1e-6, atol=1e-7, rtol=1e-6)
+    lt = torch.tensor(np.log(tau), dtype=torch.float64, requires_grad=True)
+    assert torch.autograd.gradcheck(SourceRun.apply, (w0, lt), eps=1e-6, atol=1e-7, rtol=1e-6)

@@ -5,6 +5,7 @@ Each translation unit is compiled by nvcc with its own floating-point contract:
   slic_mixed.cu -fmad=true   (mixed FP32/FP64 form)
   adjoint.cu    -fmad=true   (derivatives; the operands of the forward's branches use explicit __d*_rn operations)
   source_batch.cu -fmad=false (the HPR source batch: its forward equals the reference's forcing step)
+  source_adjoint.cu -fmad=true (its reverse pass)
   *.cu (rest)   host code and helpers
 The objects are linked into one shared library with the CUDA runtime linked statically, so the library
 only depends on the driver.  Run `python -m vanguard_b200.build` or call build().
@@ -32,6 +33,7 @@ UNITS = [
     ("batch.cu", ["-fmad=false"]),
     ("adjoint.cu", ["-fmad=true"]),
     ("source_batch.cu", ["-fmad=false"]),
+    ("source_adjoint.cu", ["-fmad=true"]),
 ]
 
 

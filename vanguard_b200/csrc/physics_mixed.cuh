@@ -309,6 +309,87 @@ struct MHDMixed {
     __device__ static double pressure(const double* W) { return W[IP]; }
 };
 
+// MHD (GLM, w = Bz = 0) with FP32 reconstruction, as EulerF32 for Euler: the limited edge states, the half-step
+// evolved states, the Richtmyer state and every flux evaluation (with its pressure p = (gamma - 1)(E - (|m|^2 / rho
+// + |B|^2) / 2) - gamma p_inf) are FP32; the cell states, the conversions of the stored state (its pressure
+// recovery from total energy), the fast-magnetosonic CFL speed and the update accumulation stay FP64 as in
+// MHDMixed.  The X sweep carries two rows per thread through packed FP32x2 arithmetic (flux2).
+struct MHDF32 : MHDMixed<false> {
+    using Base = MHDMixed<false>;
+    using R = float;
+    static constexpr bool PAIR_X = true;
+    struct P : Base::P {
+        float gm1_f, gpinf_f, ch2_f;
+    };
+    __device__ static P params(const double* prm, double ch) {
+        P q;
+        static_cast<Base::P&>(q) = Base::params(prm, ch);
+        q.gm1_f = (float)q.gm1;
+        q.gpinf_f = (float)q.gpinf;
+        q.ch2_f = (float)q.ch2;
+        return q;
+    }
+    // W = (rho, u, v, p, Bx, By, psi), U = (rho, mx, my, E, Bx, By, psi)
+    template <int AXIS>
+    __device__ static void flux(const float* U, const P& q, float* F) {
+        const float inv = rcp_approx_f(U[0]);
+        const float mx = U[1], my = U[2], E = U[3], bx = U[4], by = U[5], psi = U[6];
+        const float u = mx * inv, v = my * inv;
+        const float ke2 = fmaf(mx, u, my * v);
+        const float b2 = fmaf(bx, bx, by * by);
+        const float p = fmaf(q.gm1_f, fmaf(-0.5f, ke2 + b2, E), -q.gpinf_f);
+        const float pt = fmaf(0.5f, b2, p);
+        const float vb = fmaf(u, bx, v * by);
+        if constexpr (AXIS == 0) {
+            F[0] = mx;
+            F[1] = fmaf(mx, u, pt) - bx * bx;
+            F[2] = fmaf(mx, v, -bx * by);
+            F[3] = fmaf(E + pt, u, -vb * bx);
+            F[4] = psi;
+            F[5] = fmaf(by, u, -bx * v);
+            F[6] = q.ch2_f * bx;
+        } else {
+            F[0] = my;
+            F[1] = fmaf(my, u, -by * bx);
+            F[2] = fmaf(my, v, pt) - by * by;
+            F[3] = fmaf(E + pt, v, -vb * by);
+            F[4] = fmaf(bx, v, -by * u);
+            F[5] = psi;
+            F[6] = q.ch2_f * by;
+        }
+    }
+    // flux of two states at once, one per lane, with the same operations as flux()
+    template <int AXIS>
+    __device__ static void flux2(const f2* U, const P& q, f2* F) {
+        const f2 inv = rcp2(U[0]);
+        const f2 mx = U[1], my = U[2], E = U[3], bx = U[4], by = U[5], psi = U[6];
+        const f2 u = mx * inv, v = my * inv;
+        const f2 ke2 = fma2(mx, u, my * v);
+        const f2 b2 = fma2(bx, bx, by * by);
+        const f2 p = fma2(splat2(q.gm1_f), fma2(splat2(-0.5f), ke2 + b2, E), splat2(-q.gpinf_f));
+        const f2 pt = fma2(splat2(0.5f), b2, p);
+        const f2 vb = fma2(u, bx, v * by);
+        const f2 neg = splat2(-1.0f);
+        if constexpr (AXIS == 0) {
+            F[0] = mx;
+            F[1] = fma2(mx, u, pt) - bx * bx;
+            F[2] = fma2(mx, v, neg * (bx * by));
+            F[3] = fma2(E + pt, u, neg * (vb * bx));
+            F[4] = psi;
+            F[5] = fma2(by, u, neg * (bx * v));
+            F[6] = splat2(q.ch2_f) * bx;
+        } else {
+            F[0] = my;
+            F[1] = fma2(my, u, neg * (by * bx));
+            F[2] = fma2(my, v, pt) - by * by;
+            F[3] = fma2(E + pt, v, neg * (vb * by));
+            F[4] = fma2(bx, v, neg * (by * u));
+            F[5] = psi;
+            F[6] = splat2(q.ch2_f) * by;
+        }
+    }
+};
+
 // ---------------------------------------------------------------------------------------------- HPR
 // HPR (GPR) in the mixed form.  The state and its conversions, the pressure recovered from total energy inside the
 // flux, the acoustic-tensor CFL speed and the relaxation source (run by the exact forcing kernel) are the exact

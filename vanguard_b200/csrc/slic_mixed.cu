@@ -95,7 +95,7 @@ constexpr Ops make_ops(ForcingFn forcing = nullptr, SweepFn relax = nullptr, Swe
 const Ops kOps[V_COUNT] = {
     make_ops<EulerF32<1>>(),
     make_ops<EulerF32<2>>(),
-    make_ops<MHDMixed<false>>(&mhd7_forcing_fp64),
+    make_ops<MHDF32>(&mhd7_forcing_fp64),
     make_ops<MHDMixed<true>>(&mhd9_forcing_fp64),
     make_ops<HPRMixed>(&hpr_forcing_fp64, &hpr_relax_fp64),
     make_ops<HPRSolidMixed>(&hpr_solid_forcing_fp64, &hpr_solid_relax_fp64),

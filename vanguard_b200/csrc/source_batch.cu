@@ -27,16 +27,11 @@
 #include <vector>
 
 #include "../../include/vanguard_slic.h"
-#include "physics_hpr.cuh"
-#include "source_adjoint.cuh"
+#include "source_step.cuh"
 #include "vg_ops.h"
 
 namespace vg {
 namespace srcb {
-
-using H = HPRModel<false>;
-constexpr int NV = 17;
-constexpr int BT = 128;  // threads per block
 
 struct Args {
     double* W;           // 17 x n current state (primitives)
@@ -47,56 +42,6 @@ struct Args {
     double params[kParams];
 };
 
-__device__ __forceinline__ H::P cell_params(const double* prm, const double* tau, long n, long c) {
-    H::P q = H::params(prm, 0.0);
-    q.tau1 = tau[c];
-    q.tau2 = tau[n + c];
-    return q;
-}
-
-// The primitive round trip of the forcing's fractional predictor: setcons into a default-constructed state.
-__device__ __forceinline__ void set_default(const double* U, const H::P& q, double* W) {
-    H::default_state(W);
-    H::setcons(U, q, W);
-}
-
-// One source step from conserved U; keeps the stage states (conserved, after their round trips) for the reverse
-// pass when `stages` is given; returns U'.
-__device__ __forceinline__ void step_u(const double* U, const H::P& q, double h, double* Unew, double (*stages)[NV]) {
-    double k[4][NV], S[NV], wm[NV], ut[NV];
-    H::source(U, q, S);
-    for (int v = 0; v < NV; v++) k[0][v] = h * S[v];
-    if (stages)
-        for (int v = 0; v < NV; v++) stages[0][v] = U[v];
-#pragma unroll 1
-    for (int s = 0; s < 3; s++) {
-        for (int v = 0; v < NV; v++) ut[v] = U[v] + (s < 2 ? (0.5 * k[s][v]) : k[s][v]);
-        set_default(ut, q, wm);
-        // the 1D predictor X(f): cons of the stage state, plus the zero flux difference (F(U) - F(U) = +0, which
-        // turns a -0 component into +0), set into a default-constructed state
-        H::cons(wm, q, ut);
-        for (int v = 0; v < NV; v++) ut[v] = ut[v] + 0.0;
-        set_default(ut, q, wm);
-        H::cons(wm, q, ut);
-        if (stages)
-            for (int v = 0; v < NV; v++) stages[s + 1][v] = ut[v];
-        H::source(ut, q, S);
-        for (int v = 0; v < NV; v++) k[s + 1][v] = h * S[v];
-    }
-    for (int v = 0; v < NV; v++) Unew[v] = U[v] + ((1.0 / 6.0) * (k[0][v] + ((2.0 * k[1][v]) + ((2.0 * k[2][v]) + k[3][v]))));
-}
-
-// W <- W after `steps` steps (the cell keeps the fields setConservedVariableVector leaves alone: J when not thermal)
-__device__ __forceinline__ void advance(double* W, const H::P& q, double h, int steps) {
-    double U[NV], Un[NV];
-#pragma unroll 1
-    for (int i = 0; i < steps; i++) {
-        H::cons(W, q, U);
-        step_u(U, q, h, Un, nullptr);
-        H::setcons(Un, q, W);
-    }
-}
-
 __global__ void __launch_bounds__(BT) run_kernel(Args a) {
     const long c = blockIdx.x * (long)BT + threadIdx.x;
     if (c >= a.n) return;
@@ -105,97 +50,6 @@ __global__ void __launch_bounds__(BT) run_kernel(Args a) {
     for (int v = 0; v < NV; v++) W[v] = a.W[v * a.n + c];
     advance(W, q, a.h, a.steps);
     for (int v = 0; v < NV; v++) a.W[v * a.n + c] = W[v];
-}
-
-// One operation of the reversal: advance slot `src` by `count` steps into slot `dst`, or reverse step `step` from
-// the state held in slot `src`.
-struct Op {
-    int kind;  // 0 advance, 1 reverse
-    int src, dst, count, step;
-};
-
-struct GradArgs {
-    const double* W0;      // 17 x n initial state (slot 0)
-    double* slots;         // nslot x 17 x n checkpoint slots (slot k at k * 17 * n; slot 0 unused: W0)
-    const double* tau;     // 2 x n
-    const double* lamT;    // 17 x n  dL/dW(T)
-    double* gW;            // 17 x n  dL/dW(0)
-    double* gtau;          // 2 x n   dL/dtau
-    const Op* ops;
-    int nops;
-    long n;
-    double h;
-    int steps;
-    double params[kParams];
-};
-
-__device__ __forceinline__ const double* slot_ptr(const GradArgs& a, int s) {
-    return s == 0 ? a.W0 : a.slots + (long)s * NV * a.n;
-}
-
-__global__ void __launch_bounds__(BT) gradient_kernel(GradArgs a) {
-    const long c = blockIdx.x * (long)BT + threadIdx.x;
-    if (c >= a.n) return;
-    const H::P q = cell_params(a.params, a.tau, a.n, c);
-    double lam[NV];          // dL/dU of the state after the step being reversed
-    double lamJ[3] = {0.0, 0.0, 0.0};  // a non-thermal material's J passes through unchanged
-    double gt1 = 0.0, gt2 = 0.0;
-    for (int v = 0; v < NV; v++) lam[v] = 0.0;
-#pragma unroll 1
-    for (int o = 0; o < a.nops; o++) {
-        const Op op = a.ops[o];
-        double W[NV];
-        const double* src = slot_ptr(a, op.src);
-        for (int v = 0; v < NV; v++) W[v] = src[v * a.n + c];
-        if (op.kind == 0) {
-            advance(W, q, a.h, op.count);
-            double* dst = a.slots + (long)op.dst * NV * a.n;
-            for (int v = 0; v < NV; v++) dst[v * a.n + c] = W[v];
-            continue;
-        }
-        // reverse step op.step from W = W(step)
-        double U[NV], Un[NV], st[4][NV];
-        H::cons(W, q, U);
-        step_u(U, q, a.h, Un, st);
-        if (op.step == a.steps - 1) {  // dL/dU(T) from dL/dW(T) through W(T) = setcons(U(T))
-            double lw[NV];
-            for (int v = 0; v < NV; v++) lw[v] = a.lamT[v * a.n + c];
-            srcadj::setcons_vjp(Un, q, lw, lam);
-            if (!q.thermal)
-                for (int k = 0; k < 3; k++) lamJ[k] = lw[14 + k];
-        }
-        // U' = U + (k1 + 2 k2 + 2 k3 + k4) / 6, k_s = h S(stage_s), stage_{s} = U + c_s k_{s-1}
-        double lk[4][NV], nu[NV];
-        for (int v = 0; v < NV; v++) {
-            lk[0][v] = lam[v] / 6.0;
-            lk[1][v] = lam[v] / 3.0;
-            lk[2][v] = lam[v] / 3.0;
-            lk[3][v] = lam[v] / 6.0;
-        }
-        const double cs[4] = {0.0, 0.5, 0.5, 1.0};
-#pragma unroll 1
-        for (int s = 3; s >= 0; s--) {
-            double mu[NV];
-            for (int v = 0; v < NV; v++) {
-                mu[v] = a.h * lk[s][v];
-                nu[v] = 0.0;
-            }
-            srcadj::source_vjp(st[s], q, mu, nu, gt1, gt2);
-            for (int v = 0; v < NV; v++) {
-                lam[v] += nu[v];
-                if (s > 0) lk[s - 1][v] += cs[s] * nu[v];
-            }
-        }
-    }
-    // dL/dW(0) from dL/dU(0) through U(0) = cons(W(0))
-    double W0[NV], g[NV];
-    for (int v = 0; v < NV; v++) W0[v] = a.W0[v * a.n + c];
-    srcadj::cons_vjp(W0, q, lam, g);
-    if (!q.thermal)
-        for (int k = 0; k < 3; k++) g[14 + k] += lamJ[k];
-    for (int v = 0; v < NV; v++) a.gW[v * a.n + c] = g[v];
-    a.gtau[c] = gt1;
-    a.gtau[a.n + c] = gt2;
 }
 
 }  // namespace srcb
@@ -421,8 +275,7 @@ vg_status vg_source_batch_gradient(vg_source_batch* b, const double* cotangent, 
     a.h = h;
     a.steps = steps;
     std::memcpy(a.params, b->params, sizeof(a.params));
-    vg::srcb::gradient_kernel<<<(unsigned)((n + vg::srcb::BT - 1) / vg::srcb::BT), vg::srcb::BT, 0, st>>>(a);
-    VS_CUDA(cudaGetLastError());
+    VS_CUDA(vg::srcb::launch_gradient(a, (unsigned)((n + vg::srcb::BT - 1) / vg::srcb::BT), st));
     const cudaMemcpyKind back = is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
     if (grad_planes) VS_CUDA(cudaMemcpyAsync(grad_planes, gW, sizeof(double) * 17 * n, back, st));
     if (grad_tau) VS_CUDA(cudaMemcpyAsync(grad_tau, gtau, sizeof(double) * 2 * n, back, st));

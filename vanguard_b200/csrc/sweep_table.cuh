@@ -58,10 +58,11 @@ struct pair_sweeps<M, decltype((void)M::PAIR_X)> {
 
 // Models with more than 9 conserved components (HPR, 17) use shorter X segments so that the three FP64
 // shared-memory tiles stay inside the 48 KB static limit (kind 1).  The PAIR_X models (two rows per thread in the
-// X sweep) add the TMA-staged X shapes (kind 2).
+// X sweep) add the TMA-staged X shapes for the four-plane Euler state (kind 2); other PAIR_X models (MHD) keep the
+// plain two-row shapes (kind 3).
 template <class M>
 constexpr int tile_kind() {
-    return (M::NU > 9) ? 1 : pair_sweeps<M>::value ? 2 : 0;
+    return (M::NU > 9) ? 1 : pair_sweeps<M>::value ? (M::NW == 4 ? 2 : 3) : 0;
 }
 
 template <class K, class M, int KIND = tile_kind<M>()>
@@ -103,12 +104,25 @@ struct SweepTable<K, M, 2> {
     };
 };
 
+template <class K, class M>
+struct SweepTable<K, M, 3> {
+    static constexpr SweepFn x[kNumXCfg] = {
+        launch_x<K, M, 128, 1, 1>, launch_x<K, M, 64, 2, 1>, launch_x<K, M, 128, 1, 4>,
+        launch_x<K, M, 128, 1, 6>, launch_x<K, M, 128, 1, 8>,
+    };
+    static constexpr SweepFn y[kNumYCfg] = {
+        launch_y<K, M, 64, 64, 1>, launch_y<K, M, 64, 32, 1>, launch_y<K, M, 64, 64, 12>,
+        launch_y<K, M, 64, 64, 16>, launch_y<K, M, 128, 32, 5>, launch_y<K, M, 32, 64, 1>,
+    };
+};
+
 // Names of the shapes of SweepTable<K, M, kind>.
 inline const char* x_cfg_name(int i, int kind = 0) {
     static const char* n[kNumXCfg] = {"P128xL1", "P64xL2", "P192xL1", "P128xL1/min6", "P128xL1/min8"};
     static const char* nb[kNumXCfg] = {"P64xL1", "P32xL2", "P96xL1", "P64xL1/min2", "P32xL1"};
     static const char* np[kNumXCfg] = {"P128x2", "TMA P128x2/min7", "TMA P128x2/min8", "P128x2/min6", "P128x2/min8"};
-    return (i >= 0 && i < kNumXCfg) ? (kind == 1 ? nb[i] : kind == 2 ? np[i] : n[i]) : "?";
+    static const char* nq[kNumXCfg] = {"P128x2", "P64xL2x2", "P128x2/min4", "P128x2/min6", "P128x2/min8"};
+    return (i >= 0 && i < kNumXCfg) ? (kind == 1 ? nb[i] : kind == 2 ? np[i] : kind == 3 ? nq[i] : n[i]) : "?";
 }
 inline const char* y_cfg_name(int i, int kind = 0) {
     static const char* n[kNumYCfg] = {"TX64xTY64", "TX64xTY32", "TX64xTY64/min12", "TX64xTY64/min16",
