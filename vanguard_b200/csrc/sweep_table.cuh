@@ -58,11 +58,11 @@ struct pair_sweeps<M, decltype((void)M::PAIR_X)> {
 
 // Models with more than 9 conserved components (HPR, 17) use shorter X segments so that the three FP64
 // shared-memory tiles stay inside the 48 KB static limit (kind 1).  The PAIR_X models (two rows per thread in the
-// X sweep) add the TMA-staged X shapes for the four-plane Euler state (kind 2); other PAIR_X models (MHD) keep the
-// plain two-row shapes (kind 3).
+// X sweep) add the TMA-staged X shapes for the Euler states of up to four planes (kind 2); other PAIR_X models (MHD)
+// keep the plain two-row shapes (kind 3).
 template <class M>
 constexpr int tile_kind() {
-    return (M::NU > 9) ? 1 : pair_sweeps<M>::value ? (M::NW == 4 ? 2 : 3) : 0;
+    return (M::NU > 9) ? 1 : pair_sweeps<M>::value ? (M::NW <= 4 ? 2 : 3) : 0;
 }
 
 template <class K, class M, int KIND = tile_kind<M>()>
