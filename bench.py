@@ -516,13 +516,16 @@ def ragged_adjoint_leg(local, stream, sh, reps=3):
     return out
 
 
-def mhd_leg(local, stream, sh, steps=500):
-    """C3: 2D ideal MHD (GLM) 2048^2 periodic smooth vortex, superbee, CFL 0.8, `steps` steps, FP64 and mixed."""
+C3_N, C3_STEPS = 2048, 500
+
+
+def mhd_leg(local, stream, sh):
+    """C3: 2D ideal MHD (GLM) 2048^2 periodic smooth vortex, superbee, CFL 0.8, 500 steps, FP64 and mixed."""
     import torch
     import vanguard_b200 as vg
     from vanguard_b200 import workloads as wl
 
-    n = 2048
+    n, steps = C3_N, C3_STEPS
     W = wl.mhd_vortex_2d(n, seed=SEED)
     prm = wl.mhd_params()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -846,7 +849,7 @@ def load_traffic(form):
 
 
 def main():
-    global NX, NY, C5_NINST, C5_STEPS, C4_STEPS, TM_N, TM_STEPS, TM_MODELS
+    global NX, NY, C5_NINST, C5_STEPS, C4_STEPS, TM_N, TM_STEPS, TM_MODELS, C3_N, C3_STEPS
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
@@ -861,6 +864,8 @@ def main():
     ap.add_argument("--c5-ninst", type=int, default=4096, help="C5 instances (smaller is for profiling only)")
     ap.add_argument("--c5-steps", type=int, default=500, help="C5 steps (smaller is for profiling only)")
     ap.add_argument("--c4-steps", type=int, default=300, help="C4 steps (smaller is for profiling only)")
+    ap.add_argument("--c3-steps", type=int, default=C3_STEPS, help="C3 steps (smaller is for profiling only)")
+    ap.add_argument("--c3-n", type=int, default=C3_N, help="C3 grid size (smaller is for profiling only)")
     ap.add_argument("--tm-steps", type=int, default=TM_STEPS, help="two-material steps (smaller is for profiling only)")
     ap.add_argument("--tm-models", default="", help="two-material models to run, comma list (profiling only)")
     ap.add_argument("--tm-n", type=int, default=TM_N, help="two-material grid size (smaller is for profiling only)")
@@ -870,6 +875,7 @@ def main():
         args.warmup = 3
     NX = NY = args.nx
     C5_NINST, C5_STEPS, C4_STEPS = args.c5_ninst, args.c5_steps, args.c4_steps
+    C3_N, C3_STEPS = args.c3_n, args.c3_steps
     TM_N, TM_STEPS, TM_MODELS = args.tm_n, args.tm_steps, [m for m in args.tm_models.split(",") if m] or None
     if args.headline_only:
         args.legs = "headline"

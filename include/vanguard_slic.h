@@ -39,7 +39,8 @@ typedef enum vg_status {
     VG_EINVAL = 1,       /* bad argument: null pointer, size, model, limiter, plane count */
     VG_ENAN = 2,         /* the run produced a non-finite value, a non-positive density, or a pressure at or
                           * below -p_inf (no real sound speed; 0 for ideal gases) */
-    VG_ETIMEOUT = 3,     /* a bounded device-side wait gave up (persistent kernels) */
+    VG_ETIMEOUT = 3,     /* a bounded device-side wait gave up (the TMA-staged sweep): treat the CUDA context as
+                          * lost (a copy may still be in flight), launch nothing more on it and reset the device */
     VG_ECUDA = 4,        /* a CUDA runtime call failed; vg_last_error_string() has the text */
     VG_ENOMEM = 5,       /* device allocation failed */
     VG_EUNSUPPORTED = 6  /* the input needs a variant this build does not provide (see below) */

@@ -10,7 +10,9 @@
 // The copies carry no multicast.  Cells outside [0, nx) come back as the copy's zero fill and are replaced by the
 // boundary's ghost values (ghost_index) with plain loads; rows beyond ny are computed from the fill and never
 // stored.  Every mbarrier wait is bounded: a wait that runs out sets ERR_TIMEOUT, waits (bounded again) for the
-// copy still in flight and returns, so the context stays usable and the host reports VG_ETIMEOUT.
+// copy still in flight and returns, and the host reports VG_ETIMEOUT.  If that second wait also runs out, a copy may
+// still be writing into the exited block's shared memory, so the host must treat VG_ETIMEOUT as the end of the
+// context: launch nothing more on it and reset the device before reusing it.
 #pragma once
 
 #include <cstdint>
