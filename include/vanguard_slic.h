@@ -20,6 +20,9 @@
  *                                      two-material model, MHD/Multiphysics/mhdreducedstatevector.cpp:91-111
  *   VG_MODEL_MHD_INTERMEDIATE (12 planes): alpha1, u, v, w, rho1, p1, rho2, p2, Bx, By, Bz, psi   the MHD
  *                                      intermediate two-material model, mhdintermediatestatevector.cpp:108-130
+ *   VG_MODEL_HPR_REDUCED (19 planes): alpha1, p, A(9, row-major), u, v, w, Jx, Jy, Jz, rho1, rho2   the HPR
+ *                                      reduced two-material model, HPR/Multiphysics/hprreducedstatevector.cpp:
+ *                                      154-185 (VG_FP64 only)
  * Ownership: a vg_solver owns all device memory it allocates; the caller owns every host buffer.
  * Threading: calls on different solvers are independent and re-entrant; one solver must not be used
  * from two host threads at once.  All work is enqueued on the stream given (NULL: the legacy default
@@ -53,7 +56,8 @@ typedef enum vg_model {
     VG_MODEL_EULER_REDUCED = 3,
     VG_MODEL_EULER_MULTIPHYSICS = 4,
     VG_MODEL_MHD_REDUCED = 5,
-    VG_MODEL_MHD_INTERMEDIATE = 6
+    VG_MODEL_MHD_INTERMEDIATE = 6,
+    VG_MODEL_HPR_REDUCED = 7
 } vg_model;
 
 /* VG_FP64: every operation in float64, in the reference's order, no FMA: matches the reference.
@@ -88,7 +92,10 @@ enum { VG_SUPERBEE = 0, VG_VANLEER = 1, VG_MINBEE = 2 };
  *                                                 with p_ref the reference pressure), 2 GodunovRomenski (c0 and
  *                                                 the exponent alpha_eos); is_plastic selects the plastic strain
  *                                                 relaxation with transition stress sigma0 and power-law index n
- *                                                 (HPR/hprsourceterms.cpp:12-23).  The last slot is reserved. */
+ *                                                 (HPR/hprsourceterms.cpp:12-23).
+ *   HPR reduced: 11 per material, material k at params[11 k]: {gamma, p_inf, c_v, rho0, T0, c_s, alpha, tau1, tau2,
+ *                T_ref, is_thermal}   the two materials' StiffenedGas HPRMaterialParameters (elastic relaxation)
+ * The last slot is reserved. */
 typedef struct vg_grid_desc {
     int model;                        /* vg_model */
     int nx;                           /* cells along X (columns) */
@@ -106,7 +113,8 @@ typedef struct vg_run_config {
     int max_steps;      /* > 0: stop after this many steps; <= 0: run until t_end */
     double bias;        /* slope-limiter bias omega */
     int limiter;        /* slopeLimiter id */
-    int subcycles;      /* subcyclingIterations (source integration; HPR, MHD and MHD reduced; second order only) */
+    int subcycles;      /* subcyclingIterations (source integration; HPR, HPR reduced, MHD and the MHD two-material
+                         * models; second order only) */
     int order;          /* 2 (or 0): SecondOrderSolver's SLIC loop; 1: FirstOrderSolver's FORCE loop
                          * (Solvers/firstordersolver.cpp:435-553 and the MHD / HPR twins: 1-ghost boundary, FORCE
                          * of the cells themselves, no source, the MHD c_h kept at params[2], the MHD two-material
@@ -116,9 +124,10 @@ typedef struct vg_run_config {
                          * Euler on the eigenvalues of A^T A, heat flux by exponential sub-steps), stable at any tau;
                          * subcycles is then ignored.  Results approach the forcing's as its sub-cycles grow, not bit
                          * for bit. */
-    int reinit_frequency;  /* two-material models: reinitialisationFrequency of (MHD)SecondOrderSolver::solve{,2D}
-                            * (Solvers/secondordersolver.cpp:314-350, :354-385; Solvers/mhdsecondordersolver.cpp:
-                            * 445-495, :615-675): MultiphysicsSolvers::reinitialiseVolumeFraction after every
+    int reinit_frequency;  /* two-material models: reinitialisationFrequency of (MHD, HPR)SecondOrderSolver::
+                            * solve{,2D} (Solvers/secondordersolver.cpp:314-350, :354-385; Solvers/
+                            * mhdsecondordersolver.cpp:445-495, :615-675; Solvers/hprsecondordersolver.cpp:452-500,
+                            * :604-658): MultiphysicsSolvers::reinitialiseVolumeFraction after every
                             * reinit_frequency-th step; 0: never */
 } vg_run_config;
 
@@ -129,7 +138,7 @@ typedef struct vg_solver vg_solver;
 vg_status vg_create(const vg_grid_desc* desc, vg_solver** out);
 vg_status vg_destroy(vg_solver* s);
 
-/* Number of primitive planes the model takes at this boundary (6, 9, 17, 7, 8, 11, 12). */
+/* Number of primitive planes the model takes at this boundary (6, 9, 17, 7, 8, 11, 12, 19). */
 int vg_model_nvar(int model);
 
 /* Copy the state in / out.  planes: vg_model_nvar(model) planes of nx*ny float64, host or device

@@ -964,3 +964,101 @@ extern "C" double vgref_mhd_intermediate_run(double* planes, int nx, int ny, dou
     return mhdTwoMaterialRun<MHDIntermediateStateVector>(planes, nx, ny, dx, cfl, t_end, max_steps, bias, limiter,
                                                          prm, subcycles, reinit_freq, steps_out);
 }
+
+// ------------------------------------------------------------------------------------ HPR reduced two-material
+// Planes: the 19 primitives of HPRReducedStateVector (alpha1, p, A(9), u, v, w, Jx, Jy, Jz, rho1, rho2;
+// HPR/Multiphysics/hprreducedstatevector.cpp:154-185).  prm packs 11 values per material, material k at prm[11 k]:
+// {gamma, p_inf, c_v, rho0, T0, c_s, alpha, tau1, tau2, T_ref, is_thermal} of a StiffenedGas HPRMaterialParameters.
+// max_steps <= 0: the reference's own HPRSecondOrderSolver::solve{,2D} to t_end (Solvers/hprsecondordersolver.cpp:
+// 452-..., :604-...); else its per-step functions for max_steps steps in solve's order: the RK4 forcing sub-cycles
+// around the sweeps and the reinitialisation every reinit_freq steps.
+static HPRMaterialParameters hredParams(const double* prm, int k) {
+    double b[20] = {0.0};
+    for (int i = 0; i < 10; i++) b[i] = prm[11 * k + i];
+    b[11] = prm[11 * k + 10];
+    return hprParams(b);
+}
+static HPRReducedStateVector hredCell(const double* planes, long plane, long k, HPRMaterialParameters& m1,
+                                      HPRMaterialParameters& m2) {
+    HPRReducedStateVector c;
+    vector<double> w(19);
+    for (int v = 0; v < 19; v++) w[v] = planes[v * plane + k];
+    c.setPrimitiveVariableVector(w, m1, m2);
+    return c;
+}
+static void hredStore(HPRReducedStateVector& c, double* planes, long plane, long k, HPRMaterialParameters& m1,
+                      HPRMaterialParameters& m2) {
+    vector<double> w = c.computePrimitiveVariableVector(m1, m2);
+    for (int v = 0; v < 19; v++) planes[v * plane + k] = w[v];
+}
+
+extern "C" double vgref_hpr_reduced_run(double* planes, int nx, int ny, double dx, double cfl, double t_end,
+                                        int max_steps, double bias, int limiter, const double* prm, int subcycles,
+                                        int reinit_freq, int* steps_out) {
+    QuietCout quiet;
+    HPRMaterialParameters m1 = hredParams(prm, 0), m2 = hredParams(prm, 1);
+    const long plane = (long)nx * ny;
+    double t = 0.0;
+    int it = 0;
+    if (ny == 1) {
+        vector<HPRReducedStateVector> cells(nx);
+        for (int i = 0; i < nx; i++) cells[i] = hredCell(planes, plane, i, m1, m2);
+        if (max_steps <= 0) {
+            cells = HPRSecondOrderSolver::solve(cells, dx, cfl, t_end, bias, limiter, subcycles, reinit_freq, m1, m2);
+            t = t_end;
+        } else {
+            for (; it < max_steps; it++) {
+                vector<HPRReducedStateVector> withB = HPRSolvers::insertBoundaryCells(cells, 2);
+                double dt = HPRSolvers::computeStableTimeStep(withB, dx, cfl, t, 1.0e300, it, m1, m2);
+                for (int s = 0; s < subcycles; s++) {
+                    withB = HPRSolvers::insertBoundaryCells(cells, 1);
+                    HPRForcingSolver::computeRungeKuttaTimeStep(cells, withB, dx, 0.5 * (dt / subcycles), bias, limiter, m1, m2);
+                }
+                withB = HPRSolvers::insertBoundaryCells(cells, 2);
+                HPRSecondOrderSolver::computeSLICTimeStep(cells, withB, dx, dt, bias, limiter, m1, m2);
+                for (int s = 0; s < subcycles; s++) {
+                    withB = HPRSolvers::insertBoundaryCells(cells, 1);
+                    HPRForcingSolver::computeRungeKuttaTimeStep(cells, withB, dx, 0.5 * (dt / subcycles), bias, limiter, m1, m2);
+                }
+                t += dt;
+                if (reinit_freq != 0 && ((it + 1) % reinit_freq) == 0)
+                    MultiphysicsSolvers::reinitialiseVolumeFraction(cells, m1, m2);
+            }
+        }
+        for (int i = 0; i < nx; i++) hredStore(cells[i], planes, plane, i, m1, m2);
+    } else {
+        vector<vector<HPRReducedStateVector> > g(ny, vector<HPRReducedStateVector>(nx));
+        for (int i = 0; i < ny; i++)
+            for (int j = 0; j < nx; j++) g[i][j] = hredCell(planes, plane, (long)i * nx + j, m1, m2);
+        if (max_steps <= 0) {
+            g = HPRSecondOrderSolver::solve2D(g, dx, cfl, t_end, bias, limiter, subcycles, reinit_freq, m1, m2);
+            t = t_end;
+        } else {
+            for (; it < max_steps; it++) {
+                vector<vector<HPRReducedStateVector> > withB = HPRSolvers::insertBoundaryCells2D(g, 2);
+                double dt = HPRSolvers::computeStableTimeStep2D(withB, dx, cfl, t, 1.0e300, it, m1, m2);
+                for (int s = 0; s < subcycles; s++) {
+                    withB = HPRSolvers::insertBoundaryCells2D(g, 1);
+                    HPRForcingSolver::computeRungeKuttaTimeStep2D(g, withB, dx, 0.5 * (dt / subcycles), bias, limiter, m1, m2);
+                }
+                withB = HPRSolvers::insertBoundaryCells2D(g, 2);
+                HPRSecondOrderSolver::computeXSLICTimeStep2D(g, withB, dx, 0.5 * dt, bias, limiter, m1, m2);
+                withB = HPRSolvers::insertBoundaryCells2D(g, 2);
+                HPRSecondOrderSolver::computeYSLICTimeStep2D(g, withB, dx, dt, bias, limiter, m1, m2);
+                withB = HPRSolvers::insertBoundaryCells2D(g, 2);
+                HPRSecondOrderSolver::computeXSLICTimeStep2D(g, withB, dx, 0.5 * dt, bias, limiter, m1, m2);
+                for (int s = 0; s < subcycles; s++) {
+                    withB = HPRSolvers::insertBoundaryCells2D(g, 1);
+                    HPRForcingSolver::computeRungeKuttaTimeStep2D(g, withB, dx, 0.5 * (dt / subcycles), bias, limiter, m1, m2);
+                }
+                t += dt;
+                if (reinit_freq != 0 && ((it + 1) % reinit_freq) == 0)
+                    MultiphysicsSolvers::reinitialiseVolumeFraction(g, m1, m2);
+            }
+        }
+        for (int i = 0; i < ny; i++)
+            for (int j = 0; j < nx; j++) hredStore(g[i][j], planes, plane, (long)i * nx + j, m1, m2);
+    }
+    if (steps_out) *steps_out = it;
+    return t;
+}

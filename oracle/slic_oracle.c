@@ -14,7 +14,7 @@
 #include <stdlib.h>
 #include <string.h>
 
-#define MAXV 17
+#define MAXV 20
 
 /* std::min / std::max semantics: min(a,b) = (b < a) ? b : a; max(a,b) = (a < b) ? b : a. */
 static double smin(double a, double b) { return (b < a) ? b : a; }
@@ -1176,13 +1176,209 @@ static void mint_default(const double* prm, double* W) {
     W[0] = 0.999; W[4] = 1.0; W[5] = 1.0; W[6] = 1.0; W[7] = 1.0;
 }
 
+/* ---- HPR reduced two-material model: HPR/Multiphysics/hprreducedstatevector.cpp.  Both materials are StiffenedGas
+ * (elastic strain relaxation); prm packs 11 values per material, material k at prm[11 k]: {gamma, p_inf, c_v, rho0, T0,
+ * c_s, alpha, tau1, tau2, T_ref, is_thermal}, expanded into the single-material HPR block for the shared functions.
+ * W = alpha1, p, A (9, row-major), u, v, w, Jx, Jy, Jz, rho1, rho2 (the reference's primitive order, :154-185) and an
+ * unused twentieth plane; U = rho, rho alpha1, rho E, A, rho u (3), rho J (3), alpha1 rho1, alpha2 rho2 (:187-231).
+ * J is carried when either material is thermal (:104-109).  Every volume fraction is clamped to [0.001, 0.999]. */
+static void hred_mat(const double* prm, int k, double* b) {
+    for (int i = 0; i < 24; i++) b[i] = 0.0;
+    for (int i = 0; i < 10; i++) b[i] = prm[11 * k + i];
+    b[11] = prm[11 * k + 10];
+}
+static int hred_thermal(const double* prm) { return prm[10] != 0.0 || prm[21] != 0.0; }
+/* computeConservedVariableVector (:187-231): the state's volume fraction is clamped first; the total energy is the
+ * volume-fraction mean of each material's HPREquationOfState::computeTotalEnergy at the mixture density */
+static void hred_cons(const double* W, const double* prm, double* U) {
+    double b1[24], b2[24];
+    hred_mat(prm, 0, b1);
+    hred_mat(prm, 1, b2);
+    double a1 = red_clamp(W[0]), a2 = 1.0 - a1;
+    double p = W[1], u = W[11], v = W[12], w = W[13], jx = W[14], jy = W[15], jz = W[16], r1 = W[17], r2 = W[18];
+    mat3 A = load_A(W + 2);
+    double rho = (a1 * r1) + (a2 * r2);
+    for (int i = 0; i < 20; i++) U[i] = 0.0;
+    U[0] = rho;
+    U[1] = rho * a1;
+    double E1 = hpr_total_energy(rho, p, u, v, w, &A, jx, jy, jz, b1);
+    double E2 = hpr_total_energy(rho, p, u, v, w, &A, jx, jy, jz, b2);
+    U[2] = rho * ((a1 * E1) + (a2 * E2));
+    for (int i = 0; i < 9; i++) U[3 + i] = W[2 + i];
+    U[12] = rho * u;
+    U[13] = rho * v;
+    U[14] = rho * w;
+    if (hred_thermal(prm)) {
+        U[15] = rho * jx;
+        U[16] = rho * jy;
+        U[17] = rho * jz;
+    }
+    U[18] = a1 * r1;
+    U[19] = a2 * r2;
+}
+/* setConservedVariableVector (:111-152): each material's pressure from the mixture density and total energy */
+static void hred_setcons(const double* U, const double* prm, double* W) {
+    double b1[24], b2[24];
+    hred_mat(prm, 0, b1);
+    hred_mat(prm, 1, b2);
+    double rho = U[0];
+    double a1 = red_clamp(U[1] / rho), a2 = 1.0 - a1;
+    for (int i = 0; i < 9; i++) W[2 + i] = U[3 + i];
+    W[11] = U[12] / rho;
+    W[12] = U[13] / rho;
+    W[13] = U[14] / rho;
+    if (hred_thermal(prm)) {
+        W[14] = U[15] / rho;
+        W[15] = U[16] / rho;
+        W[16] = U[17] / rho;
+    }
+    W[17] = U[18] / a1;
+    W[18] = U[19] / a2;
+    mat3 A = load_A(W + 2);
+    double E = U[2] / rho;
+    double p1 = hpr_pressure(rho, E, W[11], W[12], W[13], &A, W[14], W[15], W[16], b1);
+    double p2 = hpr_pressure(rho, E, W[11], W[12], W[13], &A, W[14], W[15], W[16], b2);
+    W[0] = a1;
+    W[1] = (a1 * p1) + (a2 * p2);
+}
+/* compute{X,Y}FluxVector (:233-330, :337-432).  Kept as the reference has them: the X flux's mixture temperature
+ * alpha1 T1 + alpha1 T2 (:315; the Y flux's is alpha1 T1 + alpha2 T2), and the Y flux's volume-fraction component
+ * (rho v) alpha1 against the X flux's rho (u alpha1) (:310, :414). */
+static void hred_flux(const double* U, int axis, const double* prm, double* F) {
+    double b1[24], b2[24];
+    hred_mat(prm, 0, b1);
+    hred_mat(prm, 1, b2);
+    double rho = U[0];
+    double a1 = red_clamp(U[1] / rho), a2 = 1.0 - a1;
+    mat3 A = load_A(U + 3);
+    double u = U[12] / rho, v = U[13] / rho, w = U[14] / rho;
+    double jx = U[15] / rho, jy = U[16] / rho, jz = U[17] / rho;
+    double r1 = U[18] / a1, r2 = U[19] / a2;
+    double E = U[2] / rho;
+    double p1 = hpr_pressure(rho, E, u, v, w, &A, jx, jy, jz, b1);
+    double p2 = hpr_pressure(rho, E, u, v, w, &A, jx, jy, jz, b2);
+    double p = (a1 * p1) + (a2 * p2);
+    mat3 s1 = shear_stress(rho, &A, b1), s2 = shear_stress(rho, &A, b2), sig;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) sig.m[i][j] = (a1 * s1.m[i][j]) + (a2 * s2.m[i][j]);
+    double vel[3] = {u, v, w};
+    double un = axis == 0 ? u : v;
+    for (int i = 0; i < 20; i++) F[i] = 0.0;
+    F[0] = rho * un;
+    F[1] = axis == 0 ? rho * (u * a1) : (rho * v) * a1;
+    F[2] = (rho * (un * E)) + (p * un);
+    if (axis == 0) {
+        F[12] = (rho * (u * u)) + p;
+        F[13] = rho * (u * v);
+        F[14] = rho * (u * w);
+    } else {
+        F[12] = rho * (v * u);
+        F[13] = (rho * (v * v)) + p;
+        F[14] = rho * (v * w);
+    }
+    double Av[3];
+    for (int i = 0; i < 3; i++) Av[i] = ((0.0 + (A.m[i][0] * u)) + (A.m[i][1] * v)) + (A.m[i][2] * w);
+    F[2] -= ((0.0 + (sig.m[axis][0] * vel[0])) + (sig.m[axis][1] * vel[1])) + (sig.m[axis][2] * vel[2]);
+    for (int i = 0; i < 3; i++) F[12 + i] -= sig.m[axis][i];
+    for (int i = 0; i < 3; i++) F[3 + (i * 3) + axis] = Av[i];
+    if (hred_thermal(prm)) {
+        double T1 = mg_temperature(r1, p, b1), T2 = mg_temperature(r2, p, b2);
+        double a21 = b1[6] * b1[6], a22 = b2[6] * b2[6];
+        double j3[3] = {jx, jy, jz}, q[3];
+        for (int i = 0; i < 3; i++) q[i] = (a1 * (T1 * (a21 * j3[i]))) + (a2 * (T2 * (a22 * j3[i])));
+        double T = axis == 0 ? (a1 * T1) + (a1 * T2) : (a1 * T1) + (a2 * T2);
+        F[2] += q[axis];
+        if (axis == 0) {
+            F[15] = (rho * (u * jx)) + T;
+            F[16] = rho * (u * jy);
+            F[17] = rho * (u * jz);
+        } else {
+            F[15] = rho * (v * jx);
+            F[16] = (rho * (v * jy)) + T;
+            F[17] = rho * (v * jz);
+        }
+    }
+    F[18] = a1 * (r1 * un);
+    F[19] = a2 * (r2 * un);
+}
+/* computeSourceTermVector (:439-520): the mixture of both materials' distortion relaxation at each material's
+ * density and, when either is thermal, of their heat-flux relaxation at the mixture temperature, with each material's
+ * pressure from its own density */
+static void hred_source(const double* U, const double* prm, double* S) {
+    double b1[24], b2[24];
+    hred_mat(prm, 0, b1);
+    hred_mat(prm, 1, b2);
+    double rho = U[0];
+    double a1 = red_clamp(U[1] / rho), a2 = 1.0 - a1;
+    mat3 A = load_A(U + 3);
+    double r1 = U[18] / a1, r2 = U[19] / a2;
+    mat3 d1 = dE_dA(&A, b1), d2 = dE_dA(&A, b2);
+    double th1 = (a1 * hpr_theta1(r1, &A, b1)) + (a2 * hpr_theta1(r2, &A, b2));
+    for (int i = 0; i < 20; i++) S[i] = 0.0;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) S[3 + (i * 3) + j] = -((a1 * d1.m[i][j]) + (a2 * d2.m[i][j])) * th1;
+    if (hred_thermal(prm)) {
+        double E = U[2] / rho;
+        double u = U[12] / rho, v = U[13] / rho, w = U[14] / rho;
+        double jx = U[15] / rho, jy = U[16] / rho, jz = U[17] / rho;
+        double p1 = hpr_pressure(r1, E, u, v, w, &A, jx, jy, jz, b1);
+        double p2 = hpr_pressure(r2, E, u, v, w, &A, jx, jy, jz, b2);
+        double p = (a1 * p1) + (a2 * p2);
+        double T = (a1 * mg_temperature(r1, p, b1)) + (a2 * mg_temperature(r2, p, b2));
+        double a21 = b1[6] * b1[6], a22 = b2[6] * b2[6];
+        /* HPRSourceTerms::computeTheta2Reciprocal (HPR/hprsourceterms.cpp:29-39) of each material */
+        double t21 = 1.0 / ((a21 * b1[8]) * ((r1 / b1[3]) * (b1[4] / T)));
+        double t22 = 1.0 / ((a22 * b2[8]) * ((r2 / b2[3]) * (b2[4] / T)));
+        double th2 = (a1 * t21) + (a2 * t22);
+        double j3[3] = {jx, jy, jz};
+        for (int i = 0; i < 3; i++) S[15 + i] = ((-rho) * th2) * ((a1 * (a21 * j3[i])) + (a2 * (a22 * j3[i])));
+    }
+}
+/* HPRReducedAcousticTensor::computeMaximumWaveSpeed (HPR/Multiphysics/hprreducedacoustictensor.cpp:169-183): the
+ * larger of the two materials' acoustic speeds, each the single-material tensor (HPR/hpracoustictensor.cpp) at that
+ * material's density, the interface pressure and distortion, with that material's parameters */
+static double hred_speed(const double* W, int d, const double* prm, int k) {
+    double b[24], Wk[17];
+    hred_mat(prm, k, b);
+    Wk[0] = W[17 + k];
+    for (int i = 1; i < 17; i++) Wk[i] = W[i];
+    return hpr_acoustic_speed(Wk, d, b);
+}
+/* HPRSolvers::computeMaximumWaveSpeed{,2D} for the reduced model (Solvers/hprsolvers.cpp:343-360, :412-436) */
+static double hred_wave1d(const double* W, const double* prm) {
+    return fabs(W[11]) + smax(hred_speed(W, 0, prm, 0), hred_speed(W, 0, prm, 1));
+}
+static double hred_wave2d(const double* W, const double* prm) {
+    return smax(fabs(W[11]), fabs(W[12])) +
+           smax(smax(hred_speed(W, 0, prm, 0), hred_speed(W, 0, prm, 1)), smax(hred_speed(W, 1, prm, 0), hred_speed(W, 1, prm, 1)));
+}
+/* HPRReducedStateVector::setPrimitiveVariableVector (:78-104) takes J only when either material is thermal; otherwise
+ * the cells keep the default J = 0, which nothing reads */
+static void hred_drop_cold_heat_flux(int id, double* planes, long n, const double* prm) {
+    if (id == VO_HPR_REDUCED && !hred_thermal(prm))
+        for (long i = 14 * n; i < 17 * n; i++) planes[i] = 0.0;
+}
+/* HPRReducedStateVector() (:3-19) */
+static void hred_default(const double* prm, double* W) {
+    (void)prm;
+    for (int i = 0; i < 20; i++) W[i] = 0.0;
+    W[0] = 0.999;
+    W[1] = 1.0 / 1.4;
+    W[2] = 1.0;
+    W[6] = 1.0;
+    W[10] = 1.0;
+    W[17] = 1.0;
+    W[18] = 1.0;
+}
+
 /* A cell of a reinitialisation window: relaxTotalDensity (reduced :281-287, multiphysics :308-314), for the
  * multiphysics model relaxTotalPressure (:316-329, which sets both pressures to the volume-fraction mean), then the
  * volume fraction.  Planes: reduced rho1 4, rho2 5; multiphysics rho1 4, p1 5, rho2 6, p2 7. */
 static int g_reinit_mph = 0;
+static int g_reinit_r1 = 4, g_reinit_r2 = 5;  /* density planes of the reduced models (HPR reduced: 17, 18) */
 static void red_reset_cell(double* planes, long plane, long idx, double alpha) {
     double a1 = planes[idx];
-    int i1 = 4, i2 = g_reinit_mph ? 6 : 5;
+    int i1 = g_reinit_mph ? 4 : g_reinit_r1, i2 = g_reinit_mph ? 6 : g_reinit_r2;
     double rho = (a1 * planes[i1 * plane + idx]) + ((1.0 - a1) * planes[i2 * plane + idx]);
     planes[i1 * plane + idx] = rho;
     planes[i2 * plane + idx] = rho;
@@ -1234,6 +1430,7 @@ static const model M_RED = {8, red_cons, red_setcons, red_flux, red_wave1d, red_
 static const model M_MPH = {9, mph_cons, mph_setcons, mph_flux, mph_wave1d, mph_wave2d, mph_default, 0};
 static const model M_MRED = {12, mred_cons, mred_setcons, mred_flux, mred_wave1d, mred_wave2d, mred_default, mred_source};
 static const model M_MINT = {13, mint_cons, mint_setcons, mint_flux, mint_wave1d, mint_wave2d, mint_default, mint_source};
+static const model M_HRED = {20, hred_cons, hred_setcons, hred_flux, hred_wave1d, hred_wave2d, hred_default, hred_source};
 
 static const model* model_of(int id) {
     switch (id) {
@@ -1244,13 +1441,14 @@ static const model* model_of(int id) {
         case VO_EULER_MULTIPHYSICS: return &M_MPH;
         case VO_MHD_REDUCED: return &M_MRED;
         case VO_MHD_INTERMEDIATE: return &M_MINT;
+        case VO_HPR_REDUCED: return &M_HRED;
         default: return NULL;
     }
 }
 
 int vo_nvar(int id) { const model* m = model_of(id); return m ? m->nv : 0; }
 int vo_nparams(int id) {
-    return id == VO_EULER ? 6 : id == VO_MHD ? 3 : id == VO_HPR ? 20 : (id == VO_EULER_REDUCED || id == VO_EULER_MULTIPHYSICS) ? 4 : (id == VO_MHD_REDUCED || id == VO_MHD_INTERMEDIATE) ? 5 : 0;
+    return id == VO_EULER ? 6 : id == VO_MHD ? 3 : id == VO_HPR ? 20 : (id == VO_EULER_REDUCED || id == VO_EULER_MULTIPHYSICS) ? 4 : (id == VO_MHD_REDUCED || id == VO_MHD_INTERMEDIATE) ? 5 : id == VO_HPR_REDUCED ? 22 : 0;
 }
 
 /* ------------------------------------------------------------------------------- SLIC building blocks */
@@ -1617,9 +1815,11 @@ static double run(int id, double* planes, int nx, int ny, int dims, double dx, d
         it += 1;
         /* the reduced model's solve{,2D}: reinitialisation every reinit_freq steps (Solvers/secondordersolver.cpp) */
         if ((id == VO_EULER_REDUCED || id == VO_EULER_MULTIPHYSICS || id == VO_MHD_REDUCED ||
-             id == VO_MHD_INTERMEDIATE) && reinit_freq != 0 && (it % reinit_freq) == 0) {
+             id == VO_MHD_INTERMEDIATE || id == VO_HPR_REDUCED) && reinit_freq != 0 && (it % reinit_freq) == 0) {
             /* the multiphysics and MHD intermediate models also relax the pressures (planes 5 and 7) */
             g_reinit_mph = id == VO_EULER_MULTIPHYSICS || id == VO_MHD_INTERMEDIATE;
+            g_reinit_r1 = id == VO_HPR_REDUCED ? 17 : 4;
+            g_reinit_r2 = id == VO_HPR_REDUCED ? 18 : 5;
             red_reinit(planes, nx, dims == 1 ? 1 : ny);
         }
     }
@@ -1670,6 +1870,7 @@ double vo_run_first_order(int id, double* planes, int nx, int ny, double dx, dou
                           const double* prm, int bc, int* steps_out) {
     const model* m = model_of(id);
     if (!m) return -1.0;
+    hred_drop_cold_heat_flux(id, planes, (long)nx * ny, prm);
     int dims = ny > 1 ? 2 : 1;
     double tEnd = t_end > 0.0 ? t_end : 1.0e300;
     int limit = max_steps > 0 ? max_steps : 0x7fffffff;
@@ -1713,7 +1914,8 @@ double vo_run_two_material(int id, double* planes, int nx, int ny, double dx, do
 double vo_run_mhd_two_material(int id, double* planes, int nx, int ny, double dx, double cfl, double t_end,
                                 int max_steps, double w, int lim, const double* prm, int bc, int subcycles,
                                 int reinit_freq, int* steps_out) {
-    if (id != VO_MHD_REDUCED && id != VO_MHD_INTERMEDIATE) return -1.0;
+    if (id != VO_MHD_REDUCED && id != VO_MHD_INTERMEDIATE && id != VO_HPR_REDUCED) return -1.0;
+    hred_drop_cold_heat_flux(id, planes, (long)nx * ny, prm);
     return run(id, planes, nx, ny, ny > 1 ? 2 : 1, dx, cfl, t_end, max_steps, w, lim, prm, bc, subcycles,
                steps_out, NULL, reinit_freq);
 }

@@ -126,8 +126,26 @@ MHD_INTERMEDIATE_CASES = {
         dict(dx=1 / 24, cfl=0.8, steps=6, limiter=O.SUPERBEE, reinit=3, subcycles=1,
              params=wl.mhd_reduced_params(1.4, 0.0, 1.67, 0.0))),
 }
+# The HPR reduced two-material model (model id O.HPR_REDUCED): a seeded Riemann problem with distortion and heat flux
+# (material 1 left, the stiffened material 2 right) in 1D, to t_end through the reference's own solve and per step with
+# neither material thermal (the reference then drops the input J), and a 2D bubble with the reinitialisation.
+HPR_REDUCED_PRM = wl.hpr_reduced_params(gamma2=2.0, p_inf2=0.5)
+HPR_REDUCED_CASES = {
+    "hprreduced1d_riemann80_solve_t002_sub1_reinit4": (
+        lambda: wl.hpr_reduced_riemann(80, 1, seed=80),
+        dict(dx=1 / 80, cfl=0.8, t_end=0.02, steps=0, limiter=O.MINBEE, reinit=4, subcycles=1,
+             params=HPR_REDUCED_PRM)),
+    "hprreduced1d_riemann60_minbee_cold_sub1_reinit2_12": (
+        lambda: wl.hpr_reduced_riemann(60, 1, seed=60),
+        dict(dx=1 / 60, cfl=0.8, steps=12, limiter=O.MINBEE, reinit=2, subcycles=1,
+             params=wl.hpr_reduced_params(gamma2=2.0, p_inf2=0.5, thermal=(False, False)))),
+    "hprreduced2d_bubble20_minbee_reinit2_6": (
+        lambda: wl.hpr_reduced_riemann(20, 20, seed=20, bubble=True),
+        dict(dx=1 / 20, cfl=0.8, steps=6, limiter=O.MINBEE, reinit=2, subcycles=0, params=HPR_REDUCED_PRM)),
+}
 TWO_MATERIAL = {O.EULER_REDUCED: REDUCED_CASES, O.EULER_MULTIPHYSICS: MULTIPHYSICS_CASES,
-                O.MHD_REDUCED: MHD_REDUCED_CASES, O.MHD_INTERMEDIATE: MHD_INTERMEDIATE_CASES}
+                O.MHD_REDUCED: MHD_REDUCED_CASES, O.MHD_INTERMEDIATE: MHD_INTERMEDIATE_CASES,
+                O.HPR_REDUCED: HPR_REDUCED_CASES}
 
 
 def make_two_material(name):

@@ -41,6 +41,9 @@ def test_status_strings():
     assert L.vg_status_string(vg.VG_OK) == b"VG_OK"
     assert L.vg_status_string(vg.VG_EUNSUPPORTED) == b"VG_EUNSUPPORTED"
     assert L.vg_model_nvar(vg.EULER) == 6 and L.vg_model_nvar(vg.MHD) == 9 and L.vg_model_nvar(vg.HPR) == 17
+    for model, nvar in vg.NVAR.items():
+        assert L.vg_model_nvar(model) == nvar
+    assert L.vg_model_nvar(len(vg.NVAR)) == 0
 
 
 def test_invalid_arguments_are_rejected_on_the_host():
@@ -50,7 +53,7 @@ def test_invalid_arguments_are_rejected_on_the_host():
     d = vg.GridDesc()
     d.model, d.nx, d.ny = vg.EULER, 1, 1
     assert L.vg_create(ctypes.byref(d), ctypes.byref(h)) == vg.VG_EINVAL  # needs >= 2 cells per swept axis
-    d.model, d.nx, d.ny = 7, 16, 16
+    d.model, d.nx, d.ny = len(vg.NVAR), 16, 16  # the first id past the last model
     assert L.vg_create(ctypes.byref(d), ctypes.byref(h)) == vg.VG_EUNSUPPORTED
     assert L.vg_run(None, None, None, None, None) == vg.VG_EINVAL
     assert L.vg_sweep(None, 0, 1.0, 1.0, 0.0, 0, None) == vg.VG_EINVAL

@@ -436,4 +436,215 @@ struct HPRModel {
 using HPRF64 = HPRModel<false>;
 using HPRSolidF64 = HPRModel<true>;
 
+// ---------------------------------------------------------------------------- HPR reduced two-material
+// HPRReducedStateVector (HPR/Multiphysics/hprreducedstatevector.cpp) for two StiffenedGas materials with elastic strain
+// relaxation, every plane carried: W = (alpha1, p, A (9, row-major), u, v, w, Jx, Jy, Jz, rho1, rho2),
+// U = (rho, rho alpha1, rho E, A, rho u (3), rho J (3), alpha1 rho1, alpha2 rho2).  Each material's single-material
+// formulas (HPRModel<false>) enter with that material's parameters: its pressure and total energy at the mixture
+// density in the conversions and fluxes, at its own density in the source; its acoustic speed at its own density.
+// Parameters: 11 per material, material k at params[11 k]: {gamma, p_inf, c_v, rho0, T0, c_s, alpha, tau1, tau2,
+// T_ref, is_thermal}.  J is carried when either material is thermal (:104-109); otherwise the cell keeps its own.
+struct HPRReducedF64 {
+    static constexpr int NW = 19;
+    static constexpr int NU = 20;
+    static constexpr bool HAS_Y = true;
+    static constexpr bool HAS_SOURCE = true;
+    using H = HPRModel<false>;
+    using M3 = H::M3;
+    struct P {
+        H::P m1, m2;
+        int thermal;   // either material thermal
+        double pinf;   // the smaller stiffening pressure: the state check's pressure floor is -pinf
+        double ch2;
+    };
+    __device__ static H::P material(const double* prm, int k) {
+        double b[kParams];
+#pragma unroll
+        for (int i = 0; i < kParams; i++) b[i] = 0.0;
+#pragma unroll
+        for (int i = 0; i < 10; i++) b[i] = prm[11 * k + i];
+        b[11] = prm[11 * k + 10];
+        return H::params(b, 0.0);
+    }
+    __device__ static P params(const double* prm, double /*ch*/) {
+        P q;
+        q.m1 = material(prm, 0);
+        q.m2 = material(prm, 1);
+        q.thermal = q.m1.thermal || q.m2.thermal;
+        q.pinf = q.m1.pinf < q.m2.pinf ? q.m1.pinf : q.m2.pinf;
+        q.ch2 = 0.0;
+        return q;
+    }
+    __device__ static double clamp_alpha(double a) { return a < 0.001 ? 0.001 : (a > 0.999 ? 0.999 : a); }
+
+    // computeConservedVariableVector (:187-231)
+    __device__ static void cons(const double* W, const P& q, double* U) {
+        const double a1 = clamp_alpha(W[0]), a2 = 1.0 - a1;
+        const double p = W[1], u = W[11], v = W[12], w = W[13], jx = W[14], jy = W[15], jz = W[16];
+        const double r1 = W[17], r2 = W[18];
+        const M3 A = H::load(W + 2);
+        const double rho = (a1 * r1) + (a2 * r2);
+        U[0] = rho;
+        U[1] = rho * a1;
+        const double E1 = H::total_energy(rho, p, u, v, w, A, jx, jy, jz, q.m1);
+        const double E2 = H::total_energy(rho, p, u, v, w, A, jx, jy, jz, q.m2);
+        U[2] = rho * ((a1 * E1) + (a2 * E2));
+#pragma unroll
+        for (int i = 0; i < 9; i++) U[3 + i] = W[2 + i];
+        U[12] = rho * u;
+        U[13] = rho * v;
+        U[14] = rho * w;
+        U[15] = q.thermal ? rho * jx : 0.0;
+        U[16] = q.thermal ? rho * jy : 0.0;
+        U[17] = q.thermal ? rho * jz : 0.0;
+        U[18] = a1 * r1;
+        U[19] = a2 * r2;
+    }
+    // setConservedVariableVector (:111-152); J kept when no material is thermal
+    __device__ static void setcons(const double* U, const P& q, double* W) {
+        const double rho = U[0];
+        const double a1 = clamp_alpha(U[1] / rho), a2 = 1.0 - a1;
+#pragma unroll
+        for (int i = 0; i < 9; i++) W[2 + i] = U[3 + i];
+        W[11] = U[12] / rho;
+        W[12] = U[13] / rho;
+        W[13] = U[14] / rho;
+        if (q.thermal) {
+            W[14] = U[15] / rho;
+            W[15] = U[16] / rho;
+            W[16] = U[17] / rho;
+        }
+        W[17] = U[18] / a1;
+        W[18] = U[19] / a2;
+        const M3 A = H::load(W + 2);
+        const double E = U[2] / rho;
+        const double p1 = H::pressure_of(rho, E, W[11], W[12], W[13], A, W[14], W[15], W[16], q.m1);
+        const double p2 = H::pressure_of(rho, E, W[11], W[12], W[13], A, W[14], W[15], W[16], q.m2);
+        W[0] = a1;
+        W[1] = (a1 * p1) + (a2 * p2);
+    }
+    // compute{X,Y}FluxVector (:233-330, :337-432), with the reference's X-flux mixture temperature alpha1 T1 + alpha1
+    // T2 (:315; alpha1 T1 + alpha2 T2 in Y) and its Y-flux volume-fraction component (rho v) alpha1 (:414)
+    template <int AXIS>
+    __device__ static void flux(const double* U, const P& q, double* F) {
+        const double rho = U[0];
+        const double a1 = clamp_alpha(U[1] / rho), a2 = 1.0 - a1;
+        const M3 A = H::load(U + 3);
+        const double u = U[12] / rho, v = U[13] / rho, w = U[14] / rho;
+        const double jx = U[15] / rho, jy = U[16] / rho, jz = U[17] / rho;
+        const double r1 = U[18] / a1, r2 = U[19] / a2;
+        const double E = U[2] / rho;
+        const double p1 = H::pressure_of(rho, E, u, v, w, A, jx, jy, jz, q.m1);
+        const double p2 = H::pressure_of(rho, E, u, v, w, A, jx, jy, jz, q.m2);
+        const double p = (a1 * p1) + (a2 * p2);
+        // HPREquationOfState::computeShearStressTensor (HPR/hprequationofstate.cpp:76-81) of each material at the
+        // mixture density, mixed by volume fraction; only row AXIS enters
+        const M3 P1 = H::tmul(A, H::dEdA(A, q.m1)), P2 = H::tmul(A, H::dEdA(A, q.m2));
+        double sig[3];
+#pragma unroll
+        for (int i = 0; i < 3; i++) sig[i] = (a1 * ((-rho) * P1.m[AXIS][i])) + (a2 * ((-rho) * P2.m[AXIS][i]));
+        const double un = AXIS == 0 ? u : v;
+#pragma unroll
+        for (int i = 0; i < NU; i++) F[i] = 0.0;
+        F[0] = rho * un;
+        F[1] = AXIS == 0 ? rho * (u * a1) : (rho * v) * a1;
+        F[2] = (rho * (un * E)) + (p * un);
+        if constexpr (AXIS == 0) {
+            F[12] = (rho * (u * u)) + p;
+            F[13] = rho * (u * v);
+            F[14] = rho * (u * w);
+        } else {
+            F[12] = rho * (v * u);
+            F[13] = (rho * (v * v)) + p;
+            F[14] = rho * (v * w);
+        }
+        F[2] -= ((0.0 + (sig[0] * u)) + (sig[1] * v)) + (sig[2] * w);
+#pragma unroll
+        for (int i = 0; i < 3; i++) F[12 + i] -= sig[i];
+#pragma unroll
+        for (int i = 0; i < 3; i++) F[3 + (i * 3) + AXIS] = ((0.0 + (A.m[i][0] * u)) + (A.m[i][1] * v)) + (A.m[i][2] * w);
+        if (q.thermal) {
+            const double T1 = H::mg_temperature(r1, p, q.m1), T2 = H::mg_temperature(r2, p, q.m2);
+            const double a21 = q.m1.alpha * q.m1.alpha, a22 = q.m2.alpha * q.m2.alpha;
+            const double jn = AXIS == 0 ? jx : jy;
+            F[2] += (a1 * (T1 * (a21 * jn))) + (a2 * (T2 * (a22 * jn)));
+            const double T = AXIS == 0 ? (a1 * T1) + (a1 * T2) : (a1 * T1) + (a2 * T2);
+            if constexpr (AXIS == 0) {
+                F[15] = (rho * (u * jx)) + T;
+                F[16] = rho * (u * jy);
+                F[17] = rho * (u * jz);
+            } else {
+                F[15] = rho * (v * jx);
+                F[16] = (rho * (v * jy)) + T;
+                F[17] = rho * (v * jz);
+            }
+        }
+        F[18] = a1 * (r1 * un);
+        F[19] = a2 * (r2 * un);
+    }
+    // computeSourceTermVector (:439-520)
+    __device__ static void source(const double* U, const P& q, double* S) {
+        const double rho = U[0];
+        const double a1 = clamp_alpha(U[1] / rho), a2 = 1.0 - a1;
+        const M3 A = H::load(U + 3);
+        const double r1 = U[18] / a1, r2 = U[19] / a2;
+        const M3 d1 = H::dEdA(A, q.m1), d2 = H::dEdA(A, q.m2);
+        const double th1 = (a1 * H::theta1(r1, A, d1, q.m1)) + (a2 * H::theta1(r2, A, d2, q.m2));
+#pragma unroll
+        for (int i = 0; i < NU; i++) S[i] = 0.0;
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) S[3 + (i * 3) + j] = -((a1 * d1.m[i][j]) + (a2 * d2.m[i][j])) * th1;
+        if (q.thermal) {
+            const double E = U[2] / rho;
+            const double u = U[12] / rho, v = U[13] / rho, w = U[14] / rho;
+            const double jx = U[15] / rho, jy = U[16] / rho, jz = U[17] / rho;
+            const double p1 = H::pressure_of(r1, E, u, v, w, A, jx, jy, jz, q.m1);
+            const double p2 = H::pressure_of(r2, E, u, v, w, A, jx, jy, jz, q.m2);
+            const double p = (a1 * p1) + (a2 * p2);
+            const double T = (a1 * H::mg_temperature(r1, p, q.m1)) + (a2 * H::mg_temperature(r2, p, q.m2));
+            const double a21 = q.m1.alpha * q.m1.alpha, a22 = q.m2.alpha * q.m2.alpha;
+            // HPRSourceTerms::computeTheta2Reciprocal (HPR/hprsourceterms.cpp:29-39) of each material
+            const double t21 = 1.0 / ((a21 * q.m1.tau2) * ((r1 / q.m1.rho0) * (q.m1.T0 / T)));
+            const double t22 = 1.0 / ((a22 * q.m2.tau2) * ((r2 / q.m2.rho0) * (q.m2.T0 / T)));
+            const double th2 = (a1 * t21) + (a2 * t22);
+            const double j3[3] = {jx, jy, jz};
+#pragma unroll
+            for (int i = 0; i < 3; i++) S[15 + i] = ((-rho) * th2) * ((a1 * (a21 * j3[i])) + (a2 * (a22 * j3[i])));
+        }
+    }
+    // HPRReducedAcousticTensor::computeMaximumWaveSpeed (HPR/Multiphysics/hprreducedacoustictensor.cpp:169-183): each
+    // material's single-material acoustic speed at its own density with the interface pressure and distortion
+    __device__ static double speed(const double* W, int d, const H::P& qk, double rho_k) {
+        double Wk[17];
+        Wk[0] = rho_k;
+#pragma unroll
+        for (int i = 1; i < 17; i++) Wk[i] = W[i];
+        return H::acoustic_speed(Wk, d, qk);
+    }
+    // HPRSolvers::computeMaximumWaveSpeed{,2D} of the reduced model (Solvers/hprsolvers.cpp:343-360, :412-436)
+    __device__ static double wave(const double* W, const P& q, int dims) {
+        const double sx = std_max(speed(W, 0, q.m1, W[17]), speed(W, 0, q.m2, W[18]));
+        if (dims == 1) return fabs(W[11]) + sx;
+        const double sy = std_max(speed(W, 1, q.m1, W[17]), speed(W, 1, q.m2, W[18]));
+        return std_max(fabs(W[11]), fabs(W[12])) + std_max(sx, sy);
+    }
+    // HPRReducedStateVector() (:3-19)
+    __device__ static void default_state(double* W) {
+#pragma unroll
+        for (int i = 0; i < NW; i++) W[i] = 0.0;
+        W[0] = 0.999;
+        W[1] = 1.0 / 1.4;
+        W[2] = 1.0;
+        W[6] = 1.0;
+        W[10] = 1.0;
+        W[17] = 1.0;
+        W[18] = 1.0;
+    }
+    // the smaller material density (bad-state check) and the interface pressure
+    __device__ static double density(const double* W) { return W[17] < W[18] ? W[17] : W[18]; }
+    __device__ static double pressure(const double* W) { return W[1]; }
+};
+
 }  // namespace vg

@@ -6,7 +6,8 @@
 // whose cells also relax both pressures to their volume-fraction mean (relaxTotalPressure), of the two pressures
 // (L::PRESSURE, L::P1, L::P2); alpha1 is plane 0 in every model.  The MHD reduced model's reinitialisation
 // (Solvers/multiphysicssolvers.cpp:656-... in 1D and 2D) is the Euler reduced model's on its own planes, the MHD
-// intermediate model's (:499-...) the multiphysics model's.
+// intermediate model's (:499-...) the multiphysics model's, and the HPR reduced model's (:997-1024 in 1D, :1026-...
+// in 2D) the Euler reduced model's on its density planes.
 //
 // A crossing is a cell j >= 1 with alpha_j < 0.5 <= alpha_{j-1} (descending) or, in 2D, alpha_j > 0.5 >= alpha_{j-1}
 // (ascending).  The four cells j-2 .. j+1 take the mixture density in both materials (relaxTotalDensity) and the
@@ -35,6 +36,10 @@ struct ReinitMHDReduced {  // alpha1, u, v, w, rho1, rho2, p, Bx, By, Bz, psi
 struct ReinitMHDIntermediate {  // alpha1, u, v, w, rho1, p1, rho2, p2, Bx, By, Bz, psi
     static constexpr int R1 = 4, R2 = 6, P1 = 5, P2 = 7;
     static constexpr bool PRESSURE = true;
+};
+struct ReinitHPRReduced {  // alpha1, p, A (9), u, v, w, Jx, Jy, Jz, rho1, rho2
+    static constexpr int R1 = 17, R2 = 18, P1 = 0, P2 = 0;
+    static constexpr bool PRESSURE = false;
 };
 
 // relaxTotalDensity (Euler/Multiphysics/eulerreducedstatevector.cpp:281-287, eulermultiphysicsstatevector.cpp:308-314,

@@ -117,6 +117,7 @@ constexpr Ops make_ops() {
                : std::is_same<M, EulerMultiphysicsF64>::value ? &multiphysics_reinit_fp64
                : std::is_same<M, MHDReducedF64>::value        ? &mhd_reduced_reinit_fp64
                : std::is_same<M, MHDIntermediateF64>::value   ? &mhd_intermediate_reinit_fp64
+               : std::is_same<M, HPRReducedF64>::value        ? &hpr_reduced_reinit_fp64
                                                               : nullptr};
 }
 
@@ -131,6 +132,7 @@ const Ops kOps[V_COUNT] = {
     make_ops<EulerMultiphysicsF64>(),
     make_ops<MHDReducedF64>(),
     make_ops<MHDIntermediateF64>(),
+    make_ops<HPRReducedF64>(),
 };
 
 }  // namespace
@@ -156,6 +158,9 @@ cudaError_t mhd_reduced_reinit_fp64(const SweepArgs& a, cudaStream_t st) {
 }
 cudaError_t mhd_intermediate_reinit_fp64(const SweepArgs& a, cudaStream_t st) {
     return reduced_reinit<ReinitMHDIntermediate>(a, st);
+}
+cudaError_t hpr_reduced_reinit_fp64(const SweepArgs& a, cudaStream_t st) {
+    return reduced_reinit<ReinitHPRReduced>(a, st);
 }
 cudaError_t mhd7_forcing_fp64(const SweepArgs& a, int subcycles, cudaStream_t st) {
     return forcing_impl<MHDF64<false>>(a, subcycles, st);

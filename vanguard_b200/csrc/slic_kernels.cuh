@@ -134,11 +134,12 @@ __device__ __forceinline__ void store_w(const SweepArgs& a, long idx, const doub
 }
 
 // Fields setConservedVariableVector leaves alone keep the cell's own values, as when the reference updates the
-// cell object in place (Solvers/firstordersolver.cpp:428-433): HPR's J when the material is not thermal
-// (HPR/hprstatevector.cpp:78-103).
+// cell object in place (Solvers/firstordersolver.cpp:428-433): HPR's J (planes 14-16) when the material is not
+// thermal (HPR/hprstatevector.cpp:78-103), and the HPR reduced two-material model's J (the same planes) when neither
+// material is (HPR/Multiphysics/hprreducedstatevector.cpp:111-152).
 template <class M>
 __device__ __forceinline__ void keep_fields(const SweepArgs& a, long idx, const typename M::P& q, double* W) {
-    if constexpr (M::NW == 17) {
+    if constexpr (M::NW == 17 || M::NW == 19) {
         if (!q.thermal)
             for (int v = 14; v < 17; v++) W[v] = a.in[v * a.plane + idx];
     }

@@ -103,6 +103,7 @@ const Ops kOps[V_COUNT] = {
     Ops{},  // V_MPH7: no mixed form (see ops_mixed)
     Ops{},  // V_MRED11: no mixed form
     Ops{},  // V_MINT12: no mixed form
+    Ops{},  // V_HRED19: no mixed form
 };
 
 }  // namespace

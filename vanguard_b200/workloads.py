@@ -373,3 +373,39 @@ def hpr_relaxation_cells(n, seed=0, thermal=True, tau_range=(1e-3, 1e-2), distor
     lo, hi = np.log10(tau_range[0]), np.log10(tau_range[1])
     tau = 10.0 ** rng.uniform(lo, hi, (2, n))
     return W, tau, hpr_params(tau1=tau[0, 0], tau2=tau[1, 0], thermal=thermal)
+
+
+def hpr_reduced_params(gamma1=1.4, p_inf1=0.0, gamma2=1.67, p_inf2=0.0, c_v=2.5, rho0=1.0, T0=1.0, c_s=1.0, alpha=1.0,
+                       tau1=1e-2, tau2=1e-2, T_ref=0.0, thermal=(True, True)):
+    """Two StiffenedGas HPR materials for the HPR reduced two-material model, packed 11 values per material:
+    {gamma, p_inf, c_v, rho0, T0, c_s, alpha, tau1, tau2, T_ref, is_thermal} (HPRMaterialParameters' gas fields)."""
+    def one(g, pinf, th):
+        return [g, pinf, c_v, rho0, T0, c_s, alpha, tau1, tau2, T_ref, 1.0 if th else 0.0]
+    return np.array(one(gamma1, p_inf1, thermal[0]) + one(gamma2, p_inf2, thermal[1]))
+
+
+def hpr_reduced_riemann(nx, ny=1, seed=0, distortion=0.02, heat=0.05, bubble=False):
+    """A two-material HPR Riemann problem (material 1 in the left half, material 2 in the right; the reference's
+    i <= n/2 convention; bubble=True in 2D: material 1 inside a disc of radius 0.3 about the centre), with a seeded
+    distortion A = I + perturbation and heat flux J, as 19 primitive planes: alpha1, p, A(9), u, v, w, Jx, Jy, Jz,
+    rho1, rho2; shape (19, n) or (19, ny, nx)."""
+    rng = np.random.default_rng(seed)
+    shape = (ny, nx) if ny > 1 else (nx,)
+    W = np.zeros((19,) + shape)
+    x = np.arange(nx)
+    if bubble and ny > 1:
+        yy, xx = np.meshgrid((np.arange(ny) + 0.5) / ny, (x + 0.5) / nx, indexing="ij")
+        left = (xx - 0.5) ** 2 + (yy - 0.5) ** 2 <= 0.09
+    else:
+        left = (x <= 0.5 * nx) if ny == 1 else np.broadcast_to(x <= 0.5 * nx, shape)
+    W[0] = np.where(left, 0.999, 0.001)
+    W[1] = np.where(left, 1.0, 0.3)
+    A = np.eye(3).reshape(9, *([1] * len(shape))) + distortion * rng.standard_normal((9,) + shape)
+    W[2:11] = A
+    W[11] = np.where(left, 0.2, -0.1)
+    if ny > 1:
+        W[12] = 0.05 * rng.standard_normal(shape)
+    W[14:17] = heat * rng.standard_normal((3,) + shape)
+    W[17] = np.where(left, 1.0, 0.8)
+    W[18] = np.where(left, 0.5, 0.25)
+    return W
