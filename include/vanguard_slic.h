@@ -23,6 +23,9 @@
  *   VG_MODEL_HPR_REDUCED (19 planes): alpha1, p, A(9, row-major), u, v, w, Jx, Jy, Jz, rho1, rho2   the HPR
  *                                      reduced two-material model, HPR/Multiphysics/hprreducedstatevector.cpp:
  *                                      154-185 (VG_FP64 only)
+ *   VG_MODEL_HPR_INTERMEDIATE (20 planes): alpha1, A(9, row-major), u, v, w, Jx, Jy, Jz, rho1, p1, rho2, p2   the
+ *                                      HPR intermediate two-material model, HPR/Multiphysics/
+ *                                      hprintermediatestatevector.cpp:161-193 (VG_FP64 only)
  * Ownership: a vg_solver owns all device memory it allocates; the caller owns every host buffer.
  * Threading: calls on different solvers are independent and re-entrant; one solver must not be used
  * from two host threads at once.  All work is enqueued on the stream given (NULL: the legacy default
@@ -57,7 +60,8 @@ typedef enum vg_model {
     VG_MODEL_EULER_MULTIPHYSICS = 4,
     VG_MODEL_MHD_REDUCED = 5,
     VG_MODEL_MHD_INTERMEDIATE = 6,
-    VG_MODEL_HPR_REDUCED = 7
+    VG_MODEL_HPR_REDUCED = 7,
+    VG_MODEL_HPR_INTERMEDIATE = 8
 } vg_model;
 
 /* VG_FP64: every operation in float64, in the reference's order, no FMA: matches the reference.
@@ -93,8 +97,9 @@ enum { VG_SUPERBEE = 0, VG_VANLEER = 1, VG_MINBEE = 2 };
  *                                                 the exponent alpha_eos); is_plastic selects the plastic strain
  *                                                 relaxation with transition stress sigma0 and power-law index n
  *                                                 (HPR/hprsourceterms.cpp:12-23).
- *   HPR reduced: 11 per material, material k at params[11 k]: {gamma, p_inf, c_v, rho0, T0, c_s, alpha, tau1, tau2,
- *                T_ref, is_thermal}   the two materials' StiffenedGas HPRMaterialParameters (elastic relaxation)
+ *   HPR reduced, HPR intermediate: 11 per material, material k at params[11 k]: {gamma, p_inf, c_v, rho0, T0, c_s,
+ *                alpha, tau1, tau2, T_ref, is_thermal}   the two materials' StiffenedGas HPRMaterialParameters (elastic
+ *                relaxation)
  * The last slot is reserved. */
 typedef struct vg_grid_desc {
     int model;                        /* vg_model */
@@ -113,8 +118,8 @@ typedef struct vg_run_config {
     int max_steps;      /* > 0: stop after this many steps; <= 0: run until t_end */
     double bias;        /* slope-limiter bias omega */
     int limiter;        /* slopeLimiter id */
-    int subcycles;      /* subcyclingIterations (source integration; HPR, HPR reduced, MHD and the MHD two-material
-                         * models; second order only) */
+    int subcycles;      /* subcyclingIterations (source integration; HPR, the HPR two-material models, MHD and the
+                         * MHD two-material models; second order only) */
     int order;          /* 2 (or 0): SecondOrderSolver's SLIC loop; 1: FirstOrderSolver's FORCE loop
                          * (Solvers/firstordersolver.cpp:435-553 and the MHD / HPR twins: 1-ghost boundary, FORCE
                          * of the cells themselves, no source, the MHD c_h kept at params[2], the MHD two-material
@@ -126,8 +131,8 @@ typedef struct vg_run_config {
                          * for bit. */
     int reinit_frequency;  /* two-material models: reinitialisationFrequency of (MHD, HPR)SecondOrderSolver::
                             * solve{,2D} (Solvers/secondordersolver.cpp:314-350, :354-385; Solvers/
-                            * mhdsecondordersolver.cpp:445-495, :615-675; Solvers/hprsecondordersolver.cpp:452-500,
-                            * :604-658): MultiphysicsSolvers::reinitialiseVolumeFraction after every
+                            * mhdsecondordersolver.cpp:445-495, :615-675; Solvers/hprsecondordersolver.cpp:402-500,
+                            * :548-658): MultiphysicsSolvers::reinitialiseVolumeFraction after every
                             * reinit_frequency-th step; 0: never */
 } vg_run_config;
 
@@ -138,7 +143,7 @@ typedef struct vg_solver vg_solver;
 vg_status vg_create(const vg_grid_desc* desc, vg_solver** out);
 vg_status vg_destroy(vg_solver* s);
 
-/* Number of primitive planes the model takes at this boundary (6, 9, 17, 7, 8, 11, 12, 19). */
+/* Number of primitive planes the model takes at this boundary (6, 9, 17, 7, 8, 11, 12, 19, 20). */
 int vg_model_nvar(int model);
 
 /* Copy the state in / out.  planes: vg_model_nvar(model) planes of nx*ny float64, host or device

@@ -23,7 +23,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libvgref.so")
 
-EULER, MHD, HPR, EULER_REDUCED, EULER_MULTIPHYSICS, MHD_REDUCED, MHD_INTERMEDIATE, HPR_REDUCED = 0, 1, 2, 3, 4, 5, 6, 7
+EULER, MHD, HPR, EULER_REDUCED, EULER_MULTIPHYSICS, MHD_REDUCED, MHD_INTERMEDIATE, HPR_REDUCED, HPR_INTERMEDIATE = (
+    0, 1, 2, 3, 4, 5, 6, 7, 8)
 NVAR = {EULER: 6, MHD: 9, HPR: 17}
 TRANSMISSIVE, PERIODIC = 0, 1
 SUPERBEE, VANLEER, MINBEE = 0, 1, 2
@@ -247,9 +248,10 @@ def hpr_cell(w, params, reference=False):
     return (*outs, sp)
 
 
-_TWO_MATERIAL_NW = {EULER_REDUCED: 7, EULER_MULTIPHYSICS: 8, MHD_REDUCED: 11, MHD_INTERMEDIATE: 12, HPR_REDUCED: 19}
+_TWO_MATERIAL_NW = {EULER_REDUCED: 7, EULER_MULTIPHYSICS: 8, MHD_REDUCED: 11, MHD_INTERMEDIATE: 12, HPR_REDUCED: 19,
+                    HPR_INTERMEDIATE: 20}
 # the two-material models with a source (their loops take sub-cycles: MHD GLM damping, HPR relaxation)
-_MHD_TWO_MATERIAL = (MHD_REDUCED, MHD_INTERMEDIATE, HPR_REDUCED)
+_MHD_TWO_MATERIAL = (MHD_REDUCED, MHD_INTERMEDIATE, HPR_REDUCED, HPR_INTERMEDIATE)
 
 
 def run_two_material(model, planes, dx, cfl, t_end=0.0, steps=0, bias=0.0, limiter=SUPERBEE, params=None, reinit=0,
@@ -257,14 +259,15 @@ def run_two_material(model, planes, dx, cfl, t_end=0.0, steps=0, bias=0.0, limit
     """(MHD)SecondOrderSolver::solve{,2D} of a two-material model on its primitive planes, in place: EULER_REDUCED
     (7 planes: alpha1, u, v, w, rho1, rho2, p), EULER_MULTIPHYSICS (8: alpha1, u, v, w, rho1, p1, rho2, p2) or
     MHD_REDUCED (11: alpha1, u, v, w, rho1, rho2, p, Bx, By, Bz, psi), MHD_INTERMEDIATE (12: alpha1, u, v, w, rho1,
-    p1, rho2, p2, Bx, By, Bz, psi) or HPR_REDUCED (19: alpha1, p, A(9), u, v, w, Jx, Jy, Jz, rho1, rho2), x (n) or
-    (ny, nx); from the restatement or (reference=True) the reference.  params = (gamma1, p_inf1, gamma2, p_inf2);
-    HPR_REDUCED: 11 per material, {gamma, p_inf, c_v, rho0, T0, c_s, alpha, tau1, tau2, T_ref, is_thermal} each;
-    reinit > 0 reinitialises the volume fraction every `reinit` steps; subcycles > 0 (the MHD models: GLM damping;
-    HPR reduced: the relaxation source) adds the RK4 forcing sub-cycles.
+    p1, rho2, p2, Bx, By, Bz, psi), HPR_REDUCED (19: alpha1, p, A(9), u, v, w, Jx, Jy, Jz, rho1, rho2) or
+    HPR_INTERMEDIATE (20: alpha1, A(9), u, v, w, Jx, Jy, Jz, rho1, p1, rho2, p2), x (n) or (ny, nx); from the
+    restatement or (reference=True) the reference.  params = (gamma1, p_inf1, gamma2, p_inf2); the HPR models: 11 per
+    material, {gamma, p_inf, c_v, rho0, T0, c_s, alpha, tau1, tau2, T_ref, is_thermal} each; reinit > 0
+    reinitialises the volume fraction every `reinit` steps; subcycles > 0 (the MHD models: GLM damping; the HPR
+    models: the relaxation source) adds the RK4 forcing sub-cycles.
     Returns (t, steps)."""
     nw = _TWO_MATERIAL_NW[model]
-    assert subcycles == 0 or model in _MHD_TWO_MATERIAL, "only the MHD two-material models and the HPR reduced model have a source"
+    assert subcycles == 0 or model in _MHD_TWO_MATERIAL, "only the MHD and HPR two-material models have a source"
     assert planes.shape[0] == nw and planes.dtype == np.float64 and planes.flags.c_contiguous
     nx = planes.shape[-1]
     ny = 1 if planes.ndim == 2 else planes.shape[1]
@@ -278,8 +281,8 @@ def run_two_material(model, planes, dx, cfl, t_end=0.0, steps=0, bias=0.0, limit
             # the intermediate model's own solve2D pads with its defective insertBoundaryCells2D
             # (Solvers/mhdsolvers.cpp:213); the harness's per-step loop builds mirror ghosts instead
             assert not (model == MHD_INTERMEDIATE and ny > 1 and steps <= 0), "2D intermediate: per-step runs only"
-            fn = (R.vgref_mhd_reduced_run if model == MHD_REDUCED else R.vgref_hpr_reduced_run if model == HPR_REDUCED
-                  else R.vgref_mhd_intermediate_run)
+            fn = {MHD_REDUCED: R.vgref_mhd_reduced_run, HPR_REDUCED: R.vgref_hpr_reduced_run,
+                  HPR_INTERMEDIATE: R.vgref_hpr_intermediate_run}.get(model, R.vgref_mhd_intermediate_run)
             fn.restype = _c_double
             t = fn(_ptr(planes), nx, ny, _c_double(dx), _c_double(cfl), _c_double(t_end), steps, _c_double(bias),
                    limiter, _ptr(prm), subcycles, reinit, ctypes.byref(st))

@@ -978,37 +978,43 @@ static HPRMaterialParameters hredParams(const double* prm, int k) {
     b[11] = prm[11 * k + 10];
     return hprParams(b);
 }
-static HPRReducedStateVector hredCell(const double* planes, long plane, long k, HPRMaterialParameters& m1,
-                                      HPRMaterialParameters& m2) {
-    HPRReducedStateVector c;
-    vector<double> w(19);
-    for (int v = 0; v < 19; v++) w[v] = planes[v * plane + k];
+template <class SV>
+static SV hprTwoCell(const double* planes, long plane, long k, int nw, HPRMaterialParameters& m1,
+                     HPRMaterialParameters& m2) {
+    SV c;
+    vector<double> w(nw);
+    for (int v = 0; v < nw; v++) w[v] = planes[v * plane + k];
     c.setPrimitiveVariableVector(w, m1, m2);
     return c;
 }
-static void hredStore(HPRReducedStateVector& c, double* planes, long plane, long k, HPRMaterialParameters& m1,
-                      HPRMaterialParameters& m2) {
+template <class SV>
+static void hprTwoStore(SV& c, double* planes, long plane, long k, int nw, HPRMaterialParameters& m1,
+                        HPRMaterialParameters& m2) {
     vector<double> w = c.computePrimitiveVariableVector(m1, m2);
-    for (int v = 0; v < 19; v++) planes[v * plane + k] = w[v];
+    for (int v = 0; v < nw; v++) planes[v * plane + k] = w[v];
 }
 
-extern "C" double vgref_hpr_reduced_run(double* planes, int nx, int ny, double dx, double cfl, double t_end,
-                                        int max_steps, double bias, int limiter, const double* prm, int subcycles,
-                                        int reinit_freq, int* steps_out) {
+// The HPR two-material solve loop of HPRSecondOrderSolver::solve{,2D} (Solvers/hprsecondordersolver.cpp:402-450,
+// :452-500 in 1D, :548-602, :604-658 in 2D) for a state type SV with nw primitives: the reference's own solve to t_end
+// when max_steps <= 0, else its per-step functions for max_steps steps in solve's order.
+template <class SV>
+static double hprTwoMaterialRun(double* planes, int nw, int nx, int ny, double dx, double cfl, double t_end,
+                                int max_steps, double bias, int limiter, const double* prm, int subcycles,
+                                int reinit_freq, int* steps_out) {
     QuietCout quiet;
     HPRMaterialParameters m1 = hredParams(prm, 0), m2 = hredParams(prm, 1);
     const long plane = (long)nx * ny;
     double t = 0.0;
     int it = 0;
     if (ny == 1) {
-        vector<HPRReducedStateVector> cells(nx);
-        for (int i = 0; i < nx; i++) cells[i] = hredCell(planes, plane, i, m1, m2);
+        vector<SV> cells(nx);
+        for (int i = 0; i < nx; i++) cells[i] = hprTwoCell<SV>(planes, plane, i, nw, m1, m2);
         if (max_steps <= 0) {
             cells = HPRSecondOrderSolver::solve(cells, dx, cfl, t_end, bias, limiter, subcycles, reinit_freq, m1, m2);
             t = t_end;
         } else {
             for (; it < max_steps; it++) {
-                vector<HPRReducedStateVector> withB = HPRSolvers::insertBoundaryCells(cells, 2);
+                vector<SV> withB = HPRSolvers::insertBoundaryCells(cells, 2);
                 double dt = HPRSolvers::computeStableTimeStep(withB, dx, cfl, t, 1.0e300, it, m1, m2);
                 for (int s = 0; s < subcycles; s++) {
                     withB = HPRSolvers::insertBoundaryCells(cells, 1);
@@ -1025,17 +1031,17 @@ extern "C" double vgref_hpr_reduced_run(double* planes, int nx, int ny, double d
                     MultiphysicsSolvers::reinitialiseVolumeFraction(cells, m1, m2);
             }
         }
-        for (int i = 0; i < nx; i++) hredStore(cells[i], planes, plane, i, m1, m2);
+        for (int i = 0; i < nx; i++) hprTwoStore(cells[i], planes, plane, i, nw, m1, m2);
     } else {
-        vector<vector<HPRReducedStateVector> > g(ny, vector<HPRReducedStateVector>(nx));
+        vector<vector<SV> > g(ny, vector<SV>(nx));
         for (int i = 0; i < ny; i++)
-            for (int j = 0; j < nx; j++) g[i][j] = hredCell(planes, plane, (long)i * nx + j, m1, m2);
+            for (int j = 0; j < nx; j++) g[i][j] = hprTwoCell<SV>(planes, plane, (long)i * nx + j, nw, m1, m2);
         if (max_steps <= 0) {
             g = HPRSecondOrderSolver::solve2D(g, dx, cfl, t_end, bias, limiter, subcycles, reinit_freq, m1, m2);
             t = t_end;
         } else {
             for (; it < max_steps; it++) {
-                vector<vector<HPRReducedStateVector> > withB = HPRSolvers::insertBoundaryCells2D(g, 2);
+                vector<vector<SV> > withB = HPRSolvers::insertBoundaryCells2D(g, 2);
                 double dt = HPRSolvers::computeStableTimeStep2D(withB, dx, cfl, t, 1.0e300, it, m1, m2);
                 for (int s = 0; s < subcycles; s++) {
                     withB = HPRSolvers::insertBoundaryCells2D(g, 1);
@@ -1057,8 +1063,25 @@ extern "C" double vgref_hpr_reduced_run(double* planes, int nx, int ny, double d
             }
         }
         for (int i = 0; i < ny; i++)
-            for (int j = 0; j < nx; j++) hredStore(g[i][j], planes, plane, (long)i * nx + j, m1, m2);
+            for (int j = 0; j < nx; j++) hprTwoStore(g[i][j], planes, plane, (long)i * nx + j, nw, m1, m2);
     }
     if (steps_out) *steps_out = it;
     return t;
+}
+
+extern "C" double vgref_hpr_reduced_run(double* planes, int nx, int ny, double dx, double cfl, double t_end,
+                                        int max_steps, double bias, int limiter, const double* prm, int subcycles,
+                                        int reinit_freq, int* steps_out) {
+    return hprTwoMaterialRun<HPRReducedStateVector>(planes, 19, nx, ny, dx, cfl, t_end, max_steps, bias, limiter, prm,
+                                                    subcycles, reinit_freq, steps_out);
+}
+
+// ------------------------------------------------------------------------------- HPR intermediate two-material
+// Planes: the 20 primitives of HPRIntermediateStateVector (alpha1, A(9), u, v, w, Jx, Jy, Jz, rho1, p1, rho2, p2;
+// HPR/Multiphysics/hprintermediatestatevector.cpp:161-193); prm as for the reduced model.
+extern "C" double vgref_hpr_intermediate_run(double* planes, int nx, int ny, double dx, double cfl, double t_end,
+                                             int max_steps, double bias, int limiter, const double* prm, int subcycles,
+                                             int reinit_freq, int* steps_out) {
+    return hprTwoMaterialRun<HPRIntermediateStateVector>(planes, 20, nx, ny, dx, cfl, t_end, max_steps, bias, limiter,
+                                                         prm, subcycles, reinit_freq, steps_out);
 }

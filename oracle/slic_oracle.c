@@ -14,7 +14,7 @@
 #include <stdlib.h>
 #include <string.h>
 
-#define MAXV 20
+#define MAXV 21
 
 /* std::min / std::max semantics: min(a,b) = (b < a) ? b : a; max(a,b) = (a < b) ? b : a. */
 static double smin(double a, double b) { return (b < a) ? b : a; }
@@ -1353,10 +1353,202 @@ static double hred_wave2d(const double* W, const double* prm) {
            smax(smax(hred_speed(W, 0, prm, 0), hred_speed(W, 0, prm, 1)), smax(hred_speed(W, 1, prm, 0), hred_speed(W, 1, prm, 1)));
 }
 /* HPRReducedStateVector::setPrimitiveVariableVector (:78-104) takes J only when either material is thermal; otherwise
- * the cells keep the default J = 0, which nothing reads */
+ * the cells keep the default J = 0, which nothing reads.  HPRIntermediateStateVector's (hprintermediatestatevector.cpp:
+ * 82-110) does the same with its J planes 13-15. */
 static void hred_drop_cold_heat_flux(int id, double* planes, long n, const double* prm) {
     if (id == VO_HPR_REDUCED && !hred_thermal(prm))
         for (long i = 14 * n; i < 17 * n; i++) planes[i] = 0.0;
+    if (id == VO_HPR_INTERMEDIATE && !hred_thermal(prm))
+        for (long i = 13 * n; i < 16 * n; i++) planes[i] = 0.0;
+}
+
+/* ---- HPR intermediate two-material model: HPR/Multiphysics/hprintermediatestatevector.cpp.  Each material carries
+ * its own density, pressure and total energy; the distortion, velocity and heat flux are shared.  prm as for the
+ * reduced model (11 values per material).
+ * W = alpha1, A (9, row-major), u, v, w, Jx, Jy, Jz, rho1, p1, rho2, p2 (:161-193) and an unused twenty-first plane;
+ * U = rho, rho alpha1, A, rho u (3), rho J (3), alpha1 rho1, alpha1 rho1 E1, alpha2 rho2, alpha2 rho2 E2 (:195-247).
+ * Each material's EOS terms take that material's own density and pressure. */
+/* computeConservedVariableVector (:195-247) */
+static void hint_cons(const double* W, const double* prm, double* U) {
+    double b1[24], b2[24];
+    hred_mat(prm, 0, b1);
+    hred_mat(prm, 1, b2);
+    double a1 = red_clamp(W[0]), a2 = 1.0 - a1;
+    mat3 A = load_A(W + 1);
+    double u = W[10], v = W[11], w = W[12], jx = W[13], jy = W[14], jz = W[15];
+    double r1 = W[16], p1 = W[17], r2 = W[18], p2 = W[19];
+    double rho = (a1 * r1) + (a2 * r2);
+    for (int i = 0; i < 21; i++) U[i] = 0.0;
+    U[0] = rho;
+    U[1] = rho * a1;
+    for (int i = 0; i < 9; i++) U[2 + i] = W[1 + i];
+    U[11] = rho * u;
+    U[12] = rho * v;
+    U[13] = rho * w;
+    if (hred_thermal(prm)) {
+        U[14] = rho * jx;
+        U[15] = rho * jy;
+        U[16] = rho * jz;
+    }
+    U[17] = a1 * r1;
+    U[19] = a2 * r2;
+    double E1 = hpr_total_energy(r1, p1, u, v, w, &A, jx, jy, jz, b1);
+    U[18] = a1 * (r1 * E1);
+    double E2 = hpr_total_energy(r2, p2, u, v, w, &A, jx, jy, jz, b2);
+    U[20] = a2 * (r2 * E2);
+}
+/* setConservedVariableVector (:112-159): each material's pressure from its own density and total energy; J kept when
+ * neither material is thermal */
+static void hint_setcons(const double* U, const double* prm, double* W) {
+    double b1[24], b2[24];
+    hred_mat(prm, 0, b1);
+    hred_mat(prm, 1, b2);
+    double rho = U[0];
+    double a1 = red_clamp(U[1] / rho), a2 = 1.0 - a1;
+    for (int i = 0; i < 9; i++) W[1 + i] = U[2 + i];
+    W[10] = U[11] / rho;
+    W[11] = U[12] / rho;
+    W[12] = U[13] / rho;
+    if (hred_thermal(prm)) {
+        W[13] = U[14] / rho;
+        W[14] = U[15] / rho;
+        W[15] = U[16] / rho;
+    }
+    W[16] = U[17] / a1;
+    W[18] = U[19] / a2;
+    mat3 A = load_A(W + 1);
+    double E1 = U[18] / (a1 * W[16]);
+    W[17] = hpr_pressure(W[16], E1, W[10], W[11], W[12], &A, W[13], W[14], W[15], b1);
+    double E2 = U[20] / (a2 * W[18]);
+    W[19] = hpr_pressure(W[18], E2, W[10], W[11], W[12], &A, W[13], W[14], W[15], b2);
+    W[0] = a1;
+}
+/* compute{X,Y}FluxVector (:249-367, :374-492): per-material energy fluxes with that material's own stress and heat
+ * flux; the momentum takes the volume-fraction mean of the two stresses and the mixture pressure */
+static void hint_flux(const double* U, int axis, const double* prm, double* F) {
+    double b1[24], b2[24];
+    hred_mat(prm, 0, b1);
+    hred_mat(prm, 1, b2);
+    double rho = U[0];
+    double a1 = red_clamp(U[1] / rho), a2 = 1.0 - a1;
+    mat3 A = load_A(U + 2);
+    double u = U[11] / rho, v = U[12] / rho, w = U[13] / rho;
+    double jx = U[14] / rho, jy = U[15] / rho, jz = U[16] / rho;
+    double r1 = U[17] / a1, r2 = U[19] / a2;
+    double E1 = U[18] / (a1 * r1);
+    double p1 = hpr_pressure(r1, E1, u, v, w, &A, jx, jy, jz, b1);
+    double E2 = U[20] / (a2 * r2);
+    double p2 = hpr_pressure(r2, E2, u, v, w, &A, jx, jy, jz, b2);
+    double p = (a1 * p1) + (a2 * p2);
+    mat3 s1 = shear_stress(r1, &A, b1), s2 = shear_stress(r2, &A, b2), sig;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) sig.m[i][j] = (a1 * s1.m[i][j]) + (a2 * s2.m[i][j]);
+    double vel[3] = {u, v, w};
+    double un = axis == 0 ? u : v;
+    for (int i = 0; i < 21; i++) F[i] = 0.0;
+    F[0] = rho * un;
+    F[1] = rho * (un * a1);
+    F[18] = a1 * ((r1 * (un * E1)) + (p1 * un));
+    F[20] = a2 * ((r2 * (un * E2)) + (p2 * un));
+    if (axis == 0) {
+        F[11] = (rho * (u * u)) + p;
+        F[12] = rho * (u * v);
+        F[13] = rho * (u * w);
+    } else {
+        F[11] = rho * (v * u);
+        F[12] = (rho * (v * v)) + p;
+        F[13] = rho * (v * w);
+    }
+    double Av[3];
+    for (int i = 0; i < 3; i++) Av[i] = ((0.0 + (A.m[i][0] * u)) + (A.m[i][1] * v)) + (A.m[i][2] * w);
+    F[18] -= a1 * (((0.0 + (s1.m[axis][0] * vel[0])) + (s1.m[axis][1] * vel[1])) + (s1.m[axis][2] * vel[2]));
+    F[20] -= a2 * (((0.0 + (s2.m[axis][0] * vel[0])) + (s2.m[axis][1] * vel[1])) + (s2.m[axis][2] * vel[2]));
+    for (int i = 0; i < 3; i++) F[11 + i] -= sig.m[axis][i];
+    for (int i = 0; i < 3; i++) F[2 + (i * 3) + axis] = Av[i];
+    if (hred_thermal(prm)) {
+        double T1 = mg_temperature(r1, p1, b1), T2 = mg_temperature(r2, p2, b2);
+        double a21 = b1[6] * b1[6], a22 = b2[6] * b2[6];
+        double j3[3] = {jx, jy, jz};
+        double T = (a1 * T1) + (a2 * T2);
+        F[18] += a1 * (T1 * (a21 * j3[axis]));
+        F[20] += a2 * (T2 * (a22 * j3[axis]));
+        if (axis == 0) {
+            F[14] = (rho * (u * jx)) + T;
+            F[15] = rho * (u * jy);
+            F[16] = rho * (u * jz);
+        } else {
+            F[14] = rho * (v * jx);
+            F[15] = (rho * (v * jy)) + T;
+            F[16] = rho * (v * jz);
+        }
+    }
+    F[17] = a1 * (r1 * un);
+    F[19] = a2 * (r2 * un);
+}
+/* computeSourceTermVector (:499-592): distortion relaxation with the volume-fraction means of both materials'
+ * dE/dA and theta1 (each at its own density); heat-flux relaxation, when either material is thermal, with each
+ * material's theta2 at its own temperature.  The heat-flux rows are 0.0 - (rho theta2) dE/dJ, as the reference's
+ * -= on a zeroed vector forms them. */
+static void hint_source(const double* U, const double* prm, double* S) {
+    double b1[24], b2[24];
+    hred_mat(prm, 0, b1);
+    hred_mat(prm, 1, b2);
+    double rho = U[0];
+    double a1 = red_clamp(U[1] / rho), a2 = 1.0 - a1;
+    mat3 A = load_A(U + 2);
+    double r1 = U[17] / a1, r2 = U[19] / a2;
+    mat3 d1 = dE_dA(&A, b1), d2 = dE_dA(&A, b2);
+    double th1 = (a1 * hpr_theta1(r1, &A, b1)) + (a2 * hpr_theta1(r2, &A, b2));
+    for (int i = 0; i < 21; i++) S[i] = 0.0;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) S[2 + (i * 3) + j] = (-((a1 * d1.m[i][j]) + (a2 * d2.m[i][j]))) * th1;
+    if (hred_thermal(prm)) {
+        double E1 = U[18] / (a1 * r1), E2 = U[20] / (a2 * r2);
+        double u = U[11] / rho, v = U[12] / rho, w = U[13] / rho;
+        double jx = U[14] / rho, jy = U[15] / rho, jz = U[16] / rho;
+        double p1 = hpr_pressure(r1, E1, u, v, w, &A, jx, jy, jz, b1);
+        double p2 = hpr_pressure(r2, E2, u, v, w, &A, jx, jy, jz, b2);
+        double T1 = mg_temperature(r1, p1, b1), T2 = mg_temperature(r2, p2, b2);
+        double a21 = b1[6] * b1[6], a22 = b2[6] * b2[6];
+        double j3[3] = {jx, jy, jz};
+        /* HPRSourceTerms::computeTheta2Reciprocal (HPR/hprsourceterms.cpp:29-39) of each material */
+        double t21 = 1.0 / ((a21 * b1[8]) * ((r1 / b1[3]) * (b1[4] / T1)));
+        double t22 = 1.0 / ((a22 * b2[8]) * ((r2 / b2[3]) * (b2[4] / T2)));
+        double th2 = (a1 * t21) + (a2 * t22);
+        for (int i = 0; i < 3; i++) S[14 + i] = 0.0 - ((rho * th2) * ((a1 * (a21 * j3[i])) + (a2 * (a22 * j3[i]))));
+    }
+}
+/* HPRIntermediateAcousticTensor::computeMaximumWaveSpeed (HPR/Multiphysics/hprintermediateacoustictensor.cpp:
+ * 177-184): the larger of the two materials' single-material acoustic speeds, each at that material's own density
+ * and pressure with the shared distortion */
+static double hint_speed(const double* W, int d, const double* prm, int k) {
+    double b[24], Wk[17];
+    hred_mat(prm, k, b);
+    Wk[0] = W[16 + 2 * k];
+    Wk[1] = W[17 + 2 * k];
+    for (int i = 0; i < 15; i++) Wk[2 + i] = W[1 + i];
+    return hpr_acoustic_speed(Wk, d, b);
+}
+/* HPRSolvers::computeMaximumWaveSpeed{,2D} for the intermediate model (Solvers/hprsolvers.cpp:324-341, :387-410) */
+static double hint_wave1d(const double* W, const double* prm) {
+    return fabs(W[10]) + smax(hint_speed(W, 0, prm, 0), hint_speed(W, 0, prm, 1));
+}
+static double hint_wave2d(const double* W, const double* prm) {
+    return smax(fabs(W[10]), fabs(W[11])) +
+           smax(smax(hint_speed(W, 0, prm, 0), hint_speed(W, 0, prm, 1)), smax(hint_speed(W, 1, prm, 0), hint_speed(W, 1, prm, 1)));
+}
+/* HPRIntermediateStateVector() (:3-21) */
+static void hint_default(const double* prm, double* W) {
+    (void)prm;
+    for (int i = 0; i < 21; i++) W[i] = 0.0;
+    W[0] = 0.999;
+    W[1] = 1.0;
+    W[5] = 1.0;
+    W[9] = 1.0;
+    W[16] = 1.0;
+    W[17] = 1.0 / 1.4;
+    W[18] = 1.0;
+    W[19] = 1.0 / 1.4;
 }
 /* HPRReducedStateVector() (:3-19) */
 static void hred_default(const double* prm, double* W) {
@@ -1375,17 +1567,19 @@ static void hred_default(const double* prm, double* W) {
  * multiphysics model relaxTotalPressure (:316-329, which sets both pressures to the volume-fraction mean), then the
  * volume fraction.  Planes: reduced rho1 4, rho2 5; multiphysics rho1 4, p1 5, rho2 6, p2 7. */
 static int g_reinit_mph = 0;
-static int g_reinit_r1 = 4, g_reinit_r2 = 5;  /* density planes of the reduced models (HPR reduced: 17, 18) */
+/* density and pressure planes: reduced models rho1 4, rho2 5 (HPR reduced 17, 18); multiphysics and MHD intermediate
+ * rho1 4, p1 5, rho2 6, p2 7; HPR intermediate rho1 16, p1 17, rho2 18, p2 19 */
+static int g_reinit_r1 = 4, g_reinit_r2 = 5, g_reinit_p1 = 5, g_reinit_p2 = 7;
 static void red_reset_cell(double* planes, long plane, long idx, double alpha) {
     double a1 = planes[idx];
-    int i1 = g_reinit_mph ? 4 : g_reinit_r1, i2 = g_reinit_mph ? 6 : g_reinit_r2;
+    int i1 = g_reinit_r1, i2 = g_reinit_r2;
     double rho = (a1 * planes[i1 * plane + idx]) + ((1.0 - a1) * planes[i2 * plane + idx]);
     planes[i1 * plane + idx] = rho;
     planes[i2 * plane + idx] = rho;
     if (g_reinit_mph) {
-        double p = (a1 * planes[5 * plane + idx]) + ((1.0 - a1) * planes[7 * plane + idx]);
-        planes[5 * plane + idx] = p;
-        planes[7 * plane + idx] = p;
+        double p = (a1 * planes[g_reinit_p1 * plane + idx]) + ((1.0 - a1) * planes[g_reinit_p2 * plane + idx]);
+        planes[g_reinit_p1 * plane + idx] = p;
+        planes[g_reinit_p2 * plane + idx] = p;
     }
     planes[idx] = alpha;
 }
@@ -1431,6 +1625,7 @@ static const model M_MPH = {9, mph_cons, mph_setcons, mph_flux, mph_wave1d, mph_
 static const model M_MRED = {12, mred_cons, mred_setcons, mred_flux, mred_wave1d, mred_wave2d, mred_default, mred_source};
 static const model M_MINT = {13, mint_cons, mint_setcons, mint_flux, mint_wave1d, mint_wave2d, mint_default, mint_source};
 static const model M_HRED = {20, hred_cons, hred_setcons, hred_flux, hred_wave1d, hred_wave2d, hred_default, hred_source};
+static const model M_HINT = {21, hint_cons, hint_setcons, hint_flux, hint_wave1d, hint_wave2d, hint_default, hint_source};
 
 static const model* model_of(int id) {
     switch (id) {
@@ -1442,13 +1637,14 @@ static const model* model_of(int id) {
         case VO_MHD_REDUCED: return &M_MRED;
         case VO_MHD_INTERMEDIATE: return &M_MINT;
         case VO_HPR_REDUCED: return &M_HRED;
+        case VO_HPR_INTERMEDIATE: return &M_HINT;
         default: return NULL;
     }
 }
 
 int vo_nvar(int id) { const model* m = model_of(id); return m ? m->nv : 0; }
 int vo_nparams(int id) {
-    return id == VO_EULER ? 6 : id == VO_MHD ? 3 : id == VO_HPR ? 20 : (id == VO_EULER_REDUCED || id == VO_EULER_MULTIPHYSICS) ? 4 : (id == VO_MHD_REDUCED || id == VO_MHD_INTERMEDIATE) ? 5 : id == VO_HPR_REDUCED ? 22 : 0;
+    return id == VO_EULER ? 6 : id == VO_MHD ? 3 : id == VO_HPR ? 20 : (id == VO_EULER_REDUCED || id == VO_EULER_MULTIPHYSICS) ? 4 : (id == VO_MHD_REDUCED || id == VO_MHD_INTERMEDIATE) ? 5 : (id == VO_HPR_REDUCED || id == VO_HPR_INTERMEDIATE) ? 22 : 0;
 }
 
 /* ------------------------------------------------------------------------------- SLIC building blocks */
@@ -1815,11 +2011,14 @@ static double run(int id, double* planes, int nx, int ny, int dims, double dx, d
         it += 1;
         /* the reduced model's solve{,2D}: reinitialisation every reinit_freq steps (Solvers/secondordersolver.cpp) */
         if ((id == VO_EULER_REDUCED || id == VO_EULER_MULTIPHYSICS || id == VO_MHD_REDUCED ||
-             id == VO_MHD_INTERMEDIATE || id == VO_HPR_REDUCED) && reinit_freq != 0 && (it % reinit_freq) == 0) {
-            /* the multiphysics and MHD intermediate models also relax the pressures (planes 5 and 7) */
-            g_reinit_mph = id == VO_EULER_MULTIPHYSICS || id == VO_MHD_INTERMEDIATE;
-            g_reinit_r1 = id == VO_HPR_REDUCED ? 17 : 4;
-            g_reinit_r2 = id == VO_HPR_REDUCED ? 18 : 5;
+             id == VO_MHD_INTERMEDIATE || id == VO_HPR_REDUCED || id == VO_HPR_INTERMEDIATE) && reinit_freq != 0 &&
+            (it % reinit_freq) == 0) {
+            /* the multiphysics and both intermediate models also relax the pressures (relaxTotalPressure) */
+            g_reinit_mph = id == VO_EULER_MULTIPHYSICS || id == VO_MHD_INTERMEDIATE || id == VO_HPR_INTERMEDIATE;
+            g_reinit_r1 = id == VO_HPR_REDUCED ? 17 : id == VO_HPR_INTERMEDIATE ? 16 : 4;
+            g_reinit_r2 = id == VO_HPR_REDUCED ? 18 : id == VO_HPR_INTERMEDIATE ? 18 : g_reinit_mph ? 6 : 5;
+            g_reinit_p1 = id == VO_HPR_INTERMEDIATE ? 17 : 5;
+            g_reinit_p2 = id == VO_HPR_INTERMEDIATE ? 19 : 7;
             red_reinit(planes, nx, dims == 1 ? 1 : ny);
         }
     }
@@ -1914,7 +2113,8 @@ double vo_run_two_material(int id, double* planes, int nx, int ny, double dx, do
 double vo_run_mhd_two_material(int id, double* planes, int nx, int ny, double dx, double cfl, double t_end,
                                 int max_steps, double w, int lim, const double* prm, int bc, int subcycles,
                                 int reinit_freq, int* steps_out) {
-    if (id != VO_MHD_REDUCED && id != VO_MHD_INTERMEDIATE && id != VO_HPR_REDUCED) return -1.0;
+    if (id != VO_MHD_REDUCED && id != VO_MHD_INTERMEDIATE && id != VO_HPR_REDUCED && id != VO_HPR_INTERMEDIATE)
+        return -1.0;
     hred_drop_cold_heat_flux(id, planes, (long)nx * ny, prm);
     return run(id, planes, nx, ny, ny > 1 ? 2 : 1, dx, cfl, t_end, max_steps, w, lim, prm, bc, subcycles,
                steps_out, NULL, reinit_freq);

@@ -143,9 +143,29 @@ HPR_REDUCED_CASES = {
         lambda: wl.hpr_reduced_riemann(20, 20, seed=20, bubble=True),
         dict(dx=1 / 20, cfl=0.8, steps=6, limiter=O.MINBEE, reinit=2, subcycles=0, params=HPR_REDUCED_PRM)),
 }
+# The HPR intermediate two-material model (model id O.HPR_INTERMEDIATE): the reduced model's problems in its planes,
+# material 2 at 1.2 times the interface pressure, through the reference's own solve and solve2D to t_end and per step
+# with cold materials.
+HPR_INTERMEDIATE_CASES = {
+    "hprintermediate1d_riemann80_solve_t002_sub1_reinit4": (
+        lambda: wl.hpr_intermediate_riemann(80, 1, seed=80, p2_scale=1.2),
+        dict(dx=1 / 80, cfl=0.8, t_end=0.02, steps=0, limiter=O.MINBEE, reinit=4, subcycles=1,
+             params=HPR_REDUCED_PRM)),
+    "hprintermediate1d_riemann60_superbee_cold_sub1_reinit2_12": (
+        lambda: wl.hpr_intermediate_riemann(60, 1, seed=60),
+        dict(dx=1 / 60, cfl=0.8, steps=12, limiter=O.SUPERBEE, reinit=2, subcycles=1,
+             params=wl.hpr_reduced_params(gamma2=2.0, p_inf2=0.5, thermal=(False, False)))),
+    "hprintermediate2d_bubble16_solve_t002_sub1_reinit4": (
+        lambda: wl.hpr_intermediate_riemann(16, 16, seed=16, bubble=True, p2_scale=1.2),
+        dict(dx=1 / 16, cfl=0.8, t_end=0.02, steps=0, limiter=O.MINBEE, reinit=4, subcycles=1,
+             params=HPR_REDUCED_PRM)),
+    "hprintermediate2d_bubble20_vanleer_reinit2_6": (
+        lambda: wl.hpr_intermediate_riemann(20, 20, seed=20, bubble=True),
+        dict(dx=1 / 20, cfl=0.8, steps=6, limiter=O.VANLEER, reinit=2, subcycles=0, params=HPR_REDUCED_PRM)),
+}
 TWO_MATERIAL = {O.EULER_REDUCED: REDUCED_CASES, O.EULER_MULTIPHYSICS: MULTIPHYSICS_CASES,
                 O.MHD_REDUCED: MHD_REDUCED_CASES, O.MHD_INTERMEDIATE: MHD_INTERMEDIATE_CASES,
-                O.HPR_REDUCED: HPR_REDUCED_CASES}
+                O.HPR_REDUCED: HPR_REDUCED_CASES, O.HPR_INTERMEDIATE: HPR_INTERMEDIATE_CASES}
 
 
 def make_two_material(name):

@@ -7,7 +7,8 @@
 // (6 x 150), HPR GodunovRomenski plastic solve (17 x 60), reduced two-material solve (7 x 120), multiphysics
 // two-material solve (8 x 100), MHD reduced two-material solve2D (11 x 24 x 24), MHD intermediate two-material solve
 // (12 x 80), the 2D maximum wave speed of an interior-only cold gas (1), whether solve2D refused a single row (1),
-// then the number of 2D steps the per-sweep loop took.
+// HPR reduced two-material solve2D (19 x 16 x 16), HPR intermediate two-material solve (20 x 60), then the number of
+// 2D steps the per-sweep loop took.
 #include <cmath>
 #include <cstdio>
 #include <stdexcept>
@@ -18,6 +19,9 @@
 #include "Solvers/mhdsecondordersolver.h"
 #include "MHD/Multiphysics/mhdreducedstatevector.h"
 #include "MHD/Multiphysics/mhdintermediatestatevector.h"
+#include "Solvers/hprsecondordersolver.h"
+#include "HPR/Multiphysics/hprreducedstatevector.h"
+#include "HPR/Multiphysics/hprintermediatestatevector.h"
 
 using std::vector;
 
@@ -235,6 +239,45 @@ int main(int argc, char** argv) {
             refused = 1.0;
         }
         put(f, vector<double>{refused});
+    }
+    // 13) HPRSecondOrderSolver::solve2D of the HPR reduced two-material model: a disc of material 1 in material 2
+    //     (ideal gas gamma 1.4 | stiffened gas gamma 2, p_inf 0.5, both thermal), one relaxation sub-cycle,
+    //     reinitialisation every 2 steps, 4 steps
+    HPRMaterialParameters hm1("StiffenedGas", true, false, 8.31445985, 1.0, 1.0, 0.0, 1.0, 2.5, 1.4, 0.0, 0.0, 0.0, 0.0,
+                              0.0, 1.0, 1e-2, 1e-2, 0.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0);
+    HPRMaterialParameters hm2("StiffenedGas", true, false, 8.31445985, 1.0, 1.0, 0.0, 1.0, 2.5, 2.0, 0.5, 0.0, 0.0, 0.0,
+                              0.0, 1.0, 1e-2, 1e-2, 0.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0);
+    vector<vector<double> > eye = {{1.0, 0.0, 0.0}, {0.0, 1.0, 0.0}, {0.0, 0.0, 1.0}};
+    {
+        int n = 16;
+        vector<vector<HPRReducedStateVector> > cells(n, vector<HPRReducedStateVector>(n));
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) {
+                double r = std::sqrt(((i - (0.5 * n)) * (i - (0.5 * n))) + ((j - (0.5 * n)) * (j - (0.5 * n))));
+                cells[i][j] = r <= 0.3 * n ? HPRReducedStateVector(0.999, 1.0, eye, 0.2, 0.0, 0.0, 0.02, 0.0, 0.0, 1.0, 0.5)
+                                           : HPRReducedStateVector(0.001, 0.3, eye, -0.1, 0.0, 0.0, 0.0, 0.01, 0.0, 0.8, 0.25);
+            }
+        vector<vector<HPRReducedStateVector> > out =
+            HPRSecondOrderSolver::solve2D(cells, 1.0 / n, 0.8, 1.0, 0.0, 2, 1, 2, hm1, hm2, 4);
+        vector<double> v;
+        for (int k = 0; k < 19; k++)
+            for (auto& row : out)
+                for (auto& c : row) v.push_back(c.computePrimitiveVariableVector(hm1, hm2)[k]);
+        put(f, v);
+    }
+    // 14) HPRSecondOrderSolver::solve of the HPR intermediate two-material model: a shock tube with unequal material
+    //     pressures, one relaxation sub-cycle, reinitialisation every 4 steps, to t = 0.02
+    {
+        int n = 60;
+        vector<HPRIntermediateStateVector> cells(n);
+        for (int i = 0; i < n; i++)
+            cells[i] = i <= 0.5 * n ? HPRIntermediateStateVector(0.999, eye, 0.2, 0.0, 0.0, 0.02, 0.0, 0.0, 1.0, 1.0, 0.5, 1.0)
+                                    : HPRIntermediateStateVector(0.001, eye, -0.1, 0.0, 0.0, 0.0, 0.01, 0.0, 0.8, 0.3, 0.25, 0.36);
+        vector<HPRIntermediateStateVector> out = HPRSecondOrderSolver::solve(cells, 1.0 / n, 0.8, 0.02, 0.0, 2, 1, 4, hm1, hm2);
+        vector<double> v;
+        for (int k = 0; k < 20; k++)
+            for (auto& c : out) v.push_back(c.computePrimitiveVariableVector(hm1, hm2)[k]);
+        put(f, v);
     }
     double st = steps;
     std::fwrite(&st, sizeof(double), 1, f);

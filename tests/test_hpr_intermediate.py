@@ -1,0 +1,104 @@
+"""The HPR intermediate two-material model in the oracle (oracle/slic_oracle.c, M_HINT) against the reference
+(HPR/Multiphysics/hprintermediatestatevector.cpp through HPRSecondOrderSolver::solve{,2D} and its per-step functions,
+compiled into oracle/_ref): bit for bit on seeded cases beyond the golden fixtures -- thermal and cold materials, a
+stiffened second material, unequal material pressures, every limiter, a bias, the RK4 relaxation sub-cycles and the
+volume-fraction reinitialisation (densities and pressures) in 1D and 2D."""
+import numpy as np
+import pytest
+
+import oracle as O
+import vanguard_b200 as vg
+from vanguard_b200 import workloads as wl
+
+needs_ref = pytest.mark.skipif(not O.ref_available(), reason="reference not built (oracle/_ref)")
+STIFF2 = dict(gamma2=2.0, p_inf2=0.5)
+
+
+def _pair(W, nx, prm, **kw):
+    a, b = W.copy(), W.copy()
+    ta = O.run_two_material(O.HPR_INTERMEDIATE, a, 1 / nx, 0.8, params=prm, **kw)
+    tb = O.run_two_material(O.HPR_INTERMEDIATE, b, 1 / nx, 0.8, params=prm, reference=True, **kw)
+    return a, b, ta, tb
+
+
+@needs_ref
+@pytest.mark.parametrize("nx,kw,thermal,p2", [
+    (40, dict(steps=4, limiter=O.SUPERBEE), (True, True), 1.0),
+    (50, dict(steps=8, limiter=O.MINBEE, bias=0.3, subcycles=2), (True, False), 1.2),
+    (60, dict(steps=10, limiter=O.VANLEER, subcycles=1), (False, True), 0.8),
+    (60, dict(steps=12, limiter=O.MINBEE, subcycles=1, reinit=2), (False, False), 1.0),
+    (60, dict(steps=9, limiter=O.MINBEE, reinit=3), (True, True), 1.1),
+], ids=["superbee", "bias_sub2_mixed_thermal", "vanleer_sub1", "cold_reinit2", "reinit3"])
+def test_oracle_matches_reference_1d(oracle_lib, nx, kw, thermal, p2):
+    prm = wl.hpr_reduced_params(thermal=thermal, **STIFF2)
+    a, b, ta, tb = _pair(wl.hpr_intermediate_riemann(nx, seed=nx, p2_scale=p2), nx, prm, **kw)
+    assert np.isfinite(a).all()
+    assert ta == tb
+    assert np.array_equal(a, b), f"max diff {np.abs(a - b).max():.3e}"
+
+
+@needs_ref
+def test_oracle_matches_reference_solve_t_end(oracle_lib):
+    # the reference's own HPRSecondOrderSolver::solve (Solvers/hprsecondordersolver.cpp:402-450)
+    prm = wl.hpr_reduced_params(**STIFF2)
+    a, b, ta, _ = _pair(wl.hpr_intermediate_riemann(80, seed=80), 80, prm, t_end=0.02, limiter=O.MINBEE, subcycles=1,
+                        reinit=4)
+    assert ta[0] == 0.02 and ta[1] > 10
+    assert np.array_equal(a, b)
+
+
+@needs_ref
+@pytest.mark.parametrize("ny,nx,kw,thermal,bubble", [
+    (10, 12, dict(steps=5, limiter=O.VANLEER, subcycles=1, reinit=2), (True, True), False),
+    (12, 16, dict(steps=6, limiter=O.MINBEE, bias=-0.2, subcycles=1, reinit=3), (False, False), False),
+    (14, 10, dict(steps=4, limiter=O.SUPERBEE, bias=0.1, subcycles=2), (True, True), False),
+    (20, 20, dict(steps=6, limiter=O.MINBEE, reinit=2), (True, False), True),
+], ids=["vanleer_sub1_reinit2", "cold_bias_reinit3", "superbee_sub2", "bubble_reinit2"])
+def test_oracle_matches_reference_2d(oracle_lib, ny, nx, kw, thermal, bubble):
+    prm = wl.hpr_reduced_params(thermal=thermal, **STIFF2)
+    a, b, ta, tb = _pair(wl.hpr_intermediate_riemann(nx, ny, seed=nx, bubble=bubble), nx, prm, **kw)
+    assert np.isfinite(a).all()
+    assert ta == tb
+    assert np.array_equal(a, b), f"max diff {np.abs(a - b).max():.3e}"
+
+
+@needs_ref
+def test_oracle_matches_reference_solve2d_t_end(oracle_lib):
+    # the reference's own HPRSecondOrderSolver::solve2D (Solvers/hprsecondordersolver.cpp:548-602)
+    prm = wl.hpr_reduced_params(**STIFF2)
+    a, b, ta, _ = _pair(wl.hpr_intermediate_riemann(16, 16, seed=16, bubble=True), 16, prm, t_end=0.02,
+                        limiter=O.MINBEE, subcycles=1, reinit=4)
+    assert ta[0] == 0.02
+    assert np.array_equal(a, b)
+
+
+def test_cold_materials_drop_the_heat_flux(oracle_lib):
+    # setPrimitiveVariableVector takes J only when either material is thermal (:82-110); computePrimitiveVariableVector
+    # then returns the default J = 0
+    W = wl.hpr_intermediate_riemann(30, seed=1)
+    assert np.abs(W[13:16]).max() > 0.0
+    O.run_two_material(O.HPR_INTERMEDIATE, W, 1 / 30, 0.8, steps=2,
+                       params=wl.hpr_reduced_params(thermal=(False, False)))
+    assert not W[13:16].any()
+
+
+def test_reinitialisation_relaxes_densities_and_pressures(oracle_lib):
+    W = wl.hpr_intermediate_riemann(60, seed=60, p2_scale=1.3)
+    O.run_two_material(O.HPR_INTERMEDIATE, W, 1 / 60, 0.8, steps=3, limiter=O.MINBEE, reinit=3,
+                       params=wl.hpr_reduced_params(**STIFF2))
+    a = W[0]
+    loc = max(i for i in range(1, 60) if a[i] < 0.5 <= a[i - 1])
+    assert list(a[loc - 2:loc + 2]) == [0.999, 0.999, 0.001, 0.001]
+    assert np.array_equal(W[16, loc - 2:loc + 2], W[18, loc - 2:loc + 2])
+    assert np.array_equal(W[17, loc - 2:loc + 2], W[19, loc - 2:loc + 2])
+    assert not np.array_equal(W[17, :loc - 2], W[19, :loc - 2])
+
+
+def test_layouts():
+    assert vg.NVAR[vg.HPR_INTERMEDIATE] == 20 and vg.HPR_INTERMEDIATE == O.HPR_INTERMEDIATE == 8
+    R = wl.hpr_reduced_riemann(16, 12, seed=2, bubble=True)
+    W = wl.hpr_intermediate_riemann(16, 12, seed=2, bubble=True, p2_scale=2.0)
+    assert W.shape == (20, 12, 16)
+    assert np.array_equal(W[0], R[0]) and np.array_equal(W[1:16], R[2:17])
+    assert np.array_equal(W[16], R[17]) and np.array_equal(W[18], R[18])
+    assert np.array_equal(W[17], R[1]) and np.array_equal(W[19], 2.0 * R[1])

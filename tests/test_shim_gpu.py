@@ -134,5 +134,33 @@ def test_shim_driver_matches_oracle(gpu, oracle_lib, tmp_path):
     assert smax < np.sqrt(1.4)  # below the default state's speed, which the padded-grid maximum would add
     assert take((1,))[0] == 1.0
 
+    # 13) HPRSecondOrderSolver::solve2D of the HPR reduced two-material model, one sub-cycle (pow in the source: 1e-12
+    #     per cell), reinitialisation every 2 steps, 4 steps
+    import math as m
+    hprm = wl.hpr_reduced_params(gamma2=2.0, p_inf2=0.5)
+    got = take((19, 16, 16))
+    n = 16
+    ref = np.zeros((19, n, n))
+    for i in range(n):
+        for j in range(n):
+            r = m.sqrt(((i - 0.5 * n) * (i - 0.5 * n)) + ((j - 0.5 * n) * (j - 0.5 * n)))
+            A = [1.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0, 1.0]
+            ref[:, i, j] = ([0.999, 1.0, *A, 0.2, 0.0, 0.0, 0.02, 0.0, 0.0, 1.0, 0.5] if r <= 0.3 * n
+                            else [0.001, 0.3, *A, -0.1, 0.0, 0.0, 0.0, 0.01, 0.0, 0.8, 0.25])
+    O.run_two_material(O.HPR_REDUCED, ref, 1 / n, 0.8, t_end=1.0, steps=4, limiter=2, params=hprm, subcycles=1,
+                       reinit=2)
+    assert _rel(got, ref) <= 1e-12
+
+    # 14) HPRSecondOrderSolver::solve of the HPR intermediate two-material model to t = 0.02, one sub-cycle
+    got = take((20, 60))
+    n = 60
+    ref = np.zeros((20, n))
+    for i in range(n):
+        A = [1.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0, 1.0]
+        ref[:, i] = ([0.999, *A, 0.2, 0.0, 0.0, 0.02, 0.0, 0.0, 1.0, 1.0, 0.5, 1.0] if i <= 0.5 * n
+                     else [0.001, *A, -0.1, 0.0, 0.0, 0.0, 0.01, 0.0, 0.8, 0.3, 0.25, 0.36])
+    O.run_two_material(O.HPR_INTERMEDIATE, ref, 1 / n, 0.8, t_end=0.02, limiter=2, params=hprm, subcycles=1, reinit=4)
+    assert _rel(got, ref) <= 1e-12
+
     assert take((1,))[0] == 6
     assert off == data.size

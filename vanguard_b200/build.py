@@ -1,7 +1,8 @@
 """Build the in-tree CUDA library vanguard_b200/libvanguard_slic.so for sm_100a.
 
 Each translation unit is compiled by nvcc with its own floating-point contract:
-  slic_fp64.cu  -fmad=false  (exact FP64: no FMA contraction, bitwise parity with the reference)
+  slic_fp64*.cu -fmad=false  (exact FP64: no FMA contraction, bitwise parity with the reference; one unit per
+                             model family so that ptxas runs on them in parallel)
   slic_mixed.cu -fmad=true   (mixed FP32/FP64 form)
   adjoint.cu    -fmad=true   (derivatives; the operands of the forward's branches use explicit __d*_rn operations)
   source_batch.cu -fmad=false (the HPR source batch: its forward equals the reference's forcing step)
@@ -27,6 +28,11 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
 # (source, extra flags)
 UNITS = [
     ("slic_fp64.cu", ["-fmad=false"]),
+    ("slic_fp64_euler.cu", ["-fmad=false"]),
+    ("slic_fp64_mhd.cu", ["-fmad=false"]),
+    ("slic_fp64_hpr.cu", ["-fmad=false"]),
+    ("slic_fp64_hpr_solid.cu", ["-fmad=false"]),
+    ("slic_fp64_hpr_two.cu", ["-fmad=false"]),
     ("slic_mixed.cu", ["-fmad=true"]),
     ("vg_api.cu", []),
     ("vg_noalloc.cu", ["-fmad=false"]),

@@ -32,6 +32,7 @@ struct HPRModel {
     static constexpr int NU = 17;
     static constexpr bool HAS_Y = true;
     static constexpr bool HAS_SOURCE = true;
+    static constexpr int J_PLANE = 14;  // first heat-flux plane (kept by setConservedVariableVector when cold)
     struct P {
         double g, pinf, cv, rho0, T0, cs, alpha, tau1, tau2, Tref;
         int thermal;
@@ -449,6 +450,7 @@ struct HPRReducedF64 {
     static constexpr int NU = 20;
     static constexpr bool HAS_Y = true;
     static constexpr bool HAS_SOURCE = true;
+    static constexpr int J_PLANE = 14;
     using H = HPRModel<false>;
     using M3 = H::M3;
     struct P {
@@ -645,6 +647,208 @@ struct HPRReducedF64 {
     // the smaller material density (bad-state check) and the interface pressure
     __device__ static double density(const double* W) { return W[17] < W[18] ? W[17] : W[18]; }
     __device__ static double pressure(const double* W) { return W[1]; }
+    // The interface pressure of this model goes below zero within steps of runs the reference completes (a stiffened
+    // material, the volume-fraction mixing of both materials' pressures at the mixture density), so the bad-state
+    // check asks for finite values and positive densities only.
+    __device__ static bool positive_pressure(const P&) { return false; }
+};
+
+// ---------------------------------------------------------------------------- HPR intermediate two-material
+// HPRIntermediateStateVector (HPR/Multiphysics/hprintermediatestatevector.cpp) for two StiffenedGas materials: a
+// density, pressure and total energy per material, with a shared distortion, velocity and heat flux.
+// W = (alpha1, A (9, row-major), u, v, w, Jx, Jy, Jz, rho1, p1, rho2, p2) (:161-193),
+// U = (rho, rho alpha1, A, rho u (3), rho J (3), alpha1 rho1, alpha1 rho1 E1, alpha2 rho2, alpha2 rho2 E2) (:195-247).
+// Each material's EOS terms take that material's own density and pressure.  Parameters as for HPRReducedF64.
+struct HPRIntermediateF64 {
+    static constexpr int NW = 20;
+    static constexpr int NU = 21;
+    static constexpr bool HAS_Y = true;
+    static constexpr bool HAS_SOURCE = true;
+    static constexpr int J_PLANE = 13;  // first heat-flux plane (kept by setConservedVariableVector when cold)
+    using H = HPRModel<false>;
+    using M3 = H::M3;
+    using P = HPRReducedF64::P;
+    __device__ static P params(const double* prm, double ch) { return HPRReducedF64::params(prm, ch); }
+    __device__ static double clamp_alpha(double a) { return HPRReducedF64::clamp_alpha(a); }
+
+    // computeConservedVariableVector (:195-247)
+    __device__ static void cons(const double* W, const P& q, double* U) {
+        const double a1 = clamp_alpha(W[0]), a2 = 1.0 - a1;
+        const double u = W[10], v = W[11], w = W[12], jx = W[13], jy = W[14], jz = W[15];
+        const double r1 = W[16], p1 = W[17], r2 = W[18], p2 = W[19];
+        const M3 A = H::load(W + 1);
+        const double rho = (a1 * r1) + (a2 * r2);
+        U[0] = rho;
+        U[1] = rho * a1;
+#pragma unroll
+        for (int i = 0; i < 9; i++) U[2 + i] = W[1 + i];
+        U[11] = rho * u;
+        U[12] = rho * v;
+        U[13] = rho * w;
+        U[14] = q.thermal ? rho * jx : 0.0;
+        U[15] = q.thermal ? rho * jy : 0.0;
+        U[16] = q.thermal ? rho * jz : 0.0;
+        U[17] = a1 * r1;
+        U[18] = a1 * (r1 * H::total_energy(r1, p1, u, v, w, A, jx, jy, jz, q.m1));
+        U[19] = a2 * r2;
+        U[20] = a2 * (r2 * H::total_energy(r2, p2, u, v, w, A, jx, jy, jz, q.m2));
+    }
+    // setConservedVariableVector (:112-159); J kept when neither material is thermal
+    __device__ static void setcons(const double* U, const P& q, double* W) {
+        const double rho = U[0];
+        const double a1 = clamp_alpha(U[1] / rho), a2 = 1.0 - a1;
+#pragma unroll
+        for (int i = 0; i < 9; i++) W[1 + i] = U[2 + i];
+        W[10] = U[11] / rho;
+        W[11] = U[12] / rho;
+        W[12] = U[13] / rho;
+        if (q.thermal) {
+            W[13] = U[14] / rho;
+            W[14] = U[15] / rho;
+            W[15] = U[16] / rho;
+        }
+        W[16] = U[17] / a1;
+        W[18] = U[19] / a2;
+        const M3 A = H::load(W + 1);
+        const double E1 = U[18] / (a1 * W[16]);
+        W[17] = H::pressure_of(W[16], E1, W[10], W[11], W[12], A, W[13], W[14], W[15], q.m1);
+        const double E2 = U[20] / (a2 * W[18]);
+        W[19] = H::pressure_of(W[18], E2, W[10], W[11], W[12], A, W[13], W[14], W[15], q.m2);
+        W[0] = a1;
+    }
+    // compute{X,Y}FluxVector (:249-367, :374-492): each material's energy flux with its own stress and heat flux; the
+    // momentum takes the mixture pressure and the volume-fraction mean of both stresses
+    template <int AXIS>
+    __device__ static void flux(const double* U, const P& q, double* F) {
+        const double rho = U[0];
+        const double a1 = clamp_alpha(U[1] / rho), a2 = 1.0 - a1;
+        const M3 A = H::load(U + 2);
+        const double u = U[11] / rho, v = U[12] / rho, w = U[13] / rho;
+        const double jx = U[14] / rho, jy = U[15] / rho, jz = U[16] / rho;
+        const double r1 = U[17] / a1, r2 = U[19] / a2;
+        const double E1 = U[18] / (a1 * r1);
+        const double p1 = H::pressure_of(r1, E1, u, v, w, A, jx, jy, jz, q.m1);
+        const double E2 = U[20] / (a2 * r2);
+        const double p2 = H::pressure_of(r2, E2, u, v, w, A, jx, jy, jz, q.m2);
+        const double p = (a1 * p1) + (a2 * p2);
+        // HPREquationOfState::computeShearStressTensor (HPR/hprequationofstate.cpp:76-81) of each material at its own
+        // density; only row AXIS enters
+        const M3 P1 = H::tmul(A, H::dEdA(A, q.m1)), P2 = H::tmul(A, H::dEdA(A, q.m2));
+        double s1[3], s2[3];
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            s1[i] = (-r1) * P1.m[AXIS][i];
+            s2[i] = (-r2) * P2.m[AXIS][i];
+        }
+        const double un = AXIS == 0 ? u : v;
+#pragma unroll
+        for (int i = 0; i < NU; i++) F[i] = 0.0;
+        F[0] = rho * un;
+        F[1] = rho * (un * a1);
+        F[18] = a1 * ((r1 * (un * E1)) + (p1 * un));
+        F[20] = a2 * ((r2 * (un * E2)) + (p2 * un));
+        if constexpr (AXIS == 0) {
+            F[11] = (rho * (u * u)) + p;
+            F[12] = rho * (u * v);
+            F[13] = rho * (u * w);
+        } else {
+            F[11] = rho * (v * u);
+            F[12] = (rho * (v * v)) + p;
+            F[13] = rho * (v * w);
+        }
+        F[18] -= a1 * (((0.0 + (s1[0] * u)) + (s1[1] * v)) + (s1[2] * w));
+        F[20] -= a2 * (((0.0 + (s2[0] * u)) + (s2[1] * v)) + (s2[2] * w));
+#pragma unroll
+        for (int i = 0; i < 3; i++) F[11 + i] -= (a1 * s1[i]) + (a2 * s2[i]);
+#pragma unroll
+        for (int i = 0; i < 3; i++) F[2 + (i * 3) + AXIS] = ((0.0 + (A.m[i][0] * u)) + (A.m[i][1] * v)) + (A.m[i][2] * w);
+        if (q.thermal) {
+            const double T1 = H::mg_temperature(r1, p1, q.m1), T2 = H::mg_temperature(r2, p2, q.m2);
+            const double a21 = q.m1.alpha * q.m1.alpha, a22 = q.m2.alpha * q.m2.alpha;
+            const double jn = AXIS == 0 ? jx : jy;
+            const double T = (a1 * T1) + (a2 * T2);
+            F[18] += a1 * (T1 * (a21 * jn));
+            F[20] += a2 * (T2 * (a22 * jn));
+            if constexpr (AXIS == 0) {
+                F[14] = (rho * (u * jx)) + T;
+                F[15] = rho * (u * jy);
+                F[16] = rho * (u * jz);
+            } else {
+                F[14] = rho * (v * jx);
+                F[15] = (rho * (v * jy)) + T;
+                F[16] = rho * (v * jz);
+            }
+        }
+        F[17] = a1 * (r1 * un);
+        F[19] = a2 * (r2 * un);
+    }
+    // computeSourceTermVector (:499-592); the heat-flux rows are 0.0 - (rho theta2) dE/dJ, as the reference's -= on a
+    // zeroed vector forms them
+    __device__ static void source(const double* U, const P& q, double* S) {
+        const double rho = U[0];
+        const double a1 = clamp_alpha(U[1] / rho), a2 = 1.0 - a1;
+        const M3 A = H::load(U + 2);
+        const double r1 = U[17] / a1, r2 = U[19] / a2;
+        const M3 d1 = H::dEdA(A, q.m1), d2 = H::dEdA(A, q.m2);
+        const double th1 = (a1 * H::theta1(r1, A, d1, q.m1)) + (a2 * H::theta1(r2, A, d2, q.m2));
+#pragma unroll
+        for (int i = 0; i < NU; i++) S[i] = 0.0;
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) S[2 + (i * 3) + j] = -((a1 * d1.m[i][j]) + (a2 * d2.m[i][j])) * th1;
+        if (q.thermal) {
+            const double E1 = U[18] / (a1 * r1), E2 = U[20] / (a2 * r2);
+            const double u = U[11] / rho, v = U[12] / rho, w = U[13] / rho;
+            const double jx = U[14] / rho, jy = U[15] / rho, jz = U[16] / rho;
+            const double p1 = H::pressure_of(r1, E1, u, v, w, A, jx, jy, jz, q.m1);
+            const double p2 = H::pressure_of(r2, E2, u, v, w, A, jx, jy, jz, q.m2);
+            const double T1 = H::mg_temperature(r1, p1, q.m1), T2 = H::mg_temperature(r2, p2, q.m2);
+            const double a21 = q.m1.alpha * q.m1.alpha, a22 = q.m2.alpha * q.m2.alpha;
+            // HPRSourceTerms::computeTheta2Reciprocal (HPR/hprsourceterms.cpp:29-39) of each material
+            const double t21 = 1.0 / ((a21 * q.m1.tau2) * ((r1 / q.m1.rho0) * (q.m1.T0 / T1)));
+            const double t22 = 1.0 / ((a22 * q.m2.tau2) * ((r2 / q.m2.rho0) * (q.m2.T0 / T2)));
+            const double th2 = (a1 * t21) + (a2 * t22);
+            const double j3[3] = {jx, jy, jz};
+#pragma unroll
+            for (int i = 0; i < 3; i++) S[14 + i] = 0.0 - ((rho * th2) * ((a1 * (a21 * j3[i])) + (a2 * (a22 * j3[i]))));
+        }
+    }
+    // HPRIntermediateAcousticTensor::computeMaximumWaveSpeed (HPR/Multiphysics/hprintermediateacoustictensor.cpp:
+    // 177-184): each material's single-material acoustic speed at its own density and pressure
+    __device__ static double speed(const double* W, int d, const H::P& qk, int k) {
+        double Wk[17];
+        Wk[0] = W[16 + 2 * k];
+        Wk[1] = W[17 + 2 * k];
+#pragma unroll
+        for (int i = 0; i < 15; i++) Wk[2 + i] = W[1 + i];
+        return H::acoustic_speed(Wk, d, qk);
+    }
+    // HPRSolvers::computeMaximumWaveSpeed{,2D} of the intermediate model (Solvers/hprsolvers.cpp:324-341, :387-410)
+    __device__ static double wave(const double* W, const P& q, int dims) {
+        const double sx = std_max(speed(W, 0, q.m1, 0), speed(W, 0, q.m2, 1));
+        if (dims == 1) return fabs(W[10]) + sx;
+        const double sy = std_max(speed(W, 1, q.m1, 0), speed(W, 1, q.m2, 1));
+        return std_max(fabs(W[10]), fabs(W[11])) + std_max(sx, sy);
+    }
+    // HPRIntermediateStateVector() (:3-21)
+    __device__ static void default_state(double* W) {
+#pragma unroll
+        for (int i = 0; i < NW; i++) W[i] = 0.0;
+        W[0] = 0.999;
+        W[1] = 1.0;
+        W[5] = 1.0;
+        W[9] = 1.0;
+        W[16] = 1.0;
+        W[17] = 1.0 / 1.4;
+        W[18] = 1.0;
+        W[19] = 1.0 / 1.4;
+    }
+    // the smaller material density (bad-state check); the mixture pressure
+    __device__ static double density(const double* W) { return W[16] < W[18] ? W[16] : W[18]; }
+    __device__ static double pressure(const double* W) { return (clamp_alpha(W[0]) * W[17]) + ((1.0 - clamp_alpha(W[0])) * W[19]); }
+    // as for the reduced model: finite values and positive densities only
+    __device__ static bool positive_pressure(const P&) { return false; }
 };
 
 }  // namespace vg

@@ -400,6 +400,7 @@ struct HPRMixedT {
     static constexpr int NW = 17;
     static constexpr int NU = 17;
     static constexpr bool HAS_Y = true;
+    static constexpr int J_PLANE = 14;
     using R = double;
     static constexpr bool PAIR_X = false;
     using P = typename HPRModel<SOLID>::P;

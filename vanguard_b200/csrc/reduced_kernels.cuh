@@ -6,8 +6,9 @@
 // whose cells also relax both pressures to their volume-fraction mean (relaxTotalPressure), of the two pressures
 // (L::PRESSURE, L::P1, L::P2); alpha1 is plane 0 in every model.  The MHD reduced model's reinitialisation
 // (Solvers/multiphysicssolvers.cpp:656-... in 1D and 2D) is the Euler reduced model's on its own planes, the MHD
-// intermediate model's (:499-...) the multiphysics model's, and the HPR reduced model's (:997-1024 in 1D, :1026-...
-// in 2D) the Euler reduced model's on its density planes.
+// intermediate model's (:499-...) the multiphysics model's, the HPR reduced model's (:997-1024 in 1D, :1026-...
+// in 2D) the Euler reduced model's on its density planes, and the HPR intermediate model's (:841-869 in 1D,
+// :871-995 in 2D) the multiphysics model's on its density and pressure planes.
 //
 // A crossing is a cell j >= 1 with alpha_j < 0.5 <= alpha_{j-1} (descending) or, in 2D, alpha_j > 0.5 >= alpha_{j-1}
 // (ascending).  The four cells j-2 .. j+1 take the mixture density in both materials (relaxTotalDensity) and the
@@ -40,6 +41,10 @@ struct ReinitMHDIntermediate {  // alpha1, u, v, w, rho1, p1, rho2, p2, Bx, By, 
 struct ReinitHPRReduced {  // alpha1, p, A (9), u, v, w, Jx, Jy, Jz, rho1, rho2
     static constexpr int R1 = 17, R2 = 18, P1 = 0, P2 = 0;
     static constexpr bool PRESSURE = false;
+};
+struct ReinitHPRIntermediate {  // alpha1, A (9), u, v, w, Jx, Jy, Jz, rho1, p1, rho2, p2
+    static constexpr int R1 = 16, R2 = 18, P1 = 17, P2 = 19;
+    static constexpr bool PRESSURE = true;
 };
 
 // relaxTotalDensity (Euler/Multiphysics/eulerreducedstatevector.cpp:281-287, eulermultiphysicsstatevector.cpp:308-314,

@@ -135,13 +135,23 @@ __device__ __forceinline__ void store_w(const SweepArgs& a, long idx, const doub
 
 // Fields setConservedVariableVector leaves alone keep the cell's own values, as when the reference updates the
 // cell object in place (Solvers/firstordersolver.cpp:428-433): HPR's J (planes 14-16) when the material is not
-// thermal (HPR/hprstatevector.cpp:78-103), and the HPR reduced two-material model's J (the same planes) when neither
-// material is (HPR/Multiphysics/hprreducedstatevector.cpp:111-152).
+// thermal (HPR/hprstatevector.cpp:78-103), and the HPR two-material models' J when neither material is (planes 14-16
+// of the reduced model, HPR/Multiphysics/hprreducedstatevector.cpp:111-152; 13-15 of the intermediate model,
+// hprintermediatestatevector.cpp:112-159).  Models with heat flux name its first plane in J_PLANE.
+template <class M, class = void>
+struct heat_flux_plane {
+    static constexpr int value = -1;
+};
+template <class M>
+struct heat_flux_plane<M, decltype((void)M::J_PLANE)> {
+    static constexpr int value = M::J_PLANE;
+};
 template <class M>
 __device__ __forceinline__ void keep_fields(const SweepArgs& a, long idx, const typename M::P& q, double* W) {
-    if constexpr (M::NW == 17 || M::NW == 19) {
+    constexpr int j0 = heat_flux_plane<M>::value;
+    if constexpr (j0 >= 0) {
         if (!q.thermal)
-            for (int v = 14; v < 17; v++) W[v] = a.in[v * a.plane + idx];
+            for (int v = j0; v < j0 + 3; v++) W[v] = a.in[v * a.plane + idx];
     }
 }
 

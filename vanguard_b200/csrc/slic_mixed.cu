@@ -104,6 +104,7 @@ const Ops kOps[V_COUNT] = {
     Ops{},  // V_MRED11: no mixed form
     Ops{},  // V_MINT12: no mixed form
     Ops{},  // V_HRED19: no mixed form
+    Ops{},  // V_HINT20: no mixed form
 };
 
 }  // namespace

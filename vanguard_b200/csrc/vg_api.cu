@@ -46,11 +46,12 @@ vg_status cuda_fail(cudaError_t e, const char* what) {
 int ref_nvar(int model) {
     return model == VG_MODEL_EULER ? 6 : model == VG_MODEL_MHD ? 9 : model == VG_MODEL_HPR ? 17 : model == VG_MODEL_EULER_REDUCED ? 7
            : model == VG_MODEL_EULER_MULTIPHYSICS ? 8 : model == VG_MODEL_MHD_REDUCED ? 11
-           : model == VG_MODEL_MHD_INTERMEDIATE ? 12 : model == VG_MODEL_HPR_REDUCED ? 19 : 0;
+           : model == VG_MODEL_MHD_INTERMEDIATE ? 12 : model == VG_MODEL_HPR_REDUCED ? 19
+           : model == VG_MODEL_HPR_INTERMEDIATE ? 20 : 0;
 }
 
 // Reference plane carried in device plane k, per variant.
-const int kPlanes[vg::V_COUNT][19] = {
+const int kPlanes[vg::V_COUNT][20] = {
     {0, 1, 4},                      // V_EULER1: rho, u, p
     {0, 1, 2, 4},                   // V_EULER2: rho, u, v, p
     {0, 1, 2, 4, 5, 6, 8},          // V_MHD7:   rho, u, v, p, Bx, By, psi
@@ -62,6 +63,7 @@ const int kPlanes[vg::V_COUNT][19] = {
     {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10},  // V_MRED11: every plane
     {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11},  // V_MINT12: every plane
     {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17, 18},  // V_HRED19: every plane
+    {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17, 18, 19},  // V_HINT20: every plane
 };
 
 }  // namespace
@@ -464,7 +466,7 @@ vg_status vg_create(const vg_grid_desc* desc, vg_solver** out) {
     if (desc->model != VG_MODEL_EULER && desc->model != VG_MODEL_MHD && desc->model != VG_MODEL_HPR &&
         desc->model != VG_MODEL_EULER_REDUCED && desc->model != VG_MODEL_EULER_MULTIPHYSICS &&
         desc->model != VG_MODEL_MHD_REDUCED && desc->model != VG_MODEL_MHD_INTERMEDIATE &&
-        desc->model != VG_MODEL_HPR_REDUCED)
+        desc->model != VG_MODEL_HPR_REDUCED && desc->model != VG_MODEL_HPR_INTERMEDIATE)
         return fail(VG_EUNSUPPORTED, "model not available in this build");
     if (desc->nx < 2 || desc->ny < 1 || (desc->ny > 1 && desc->ny < 2))
         return fail(VG_EINVAL, "grid needs at least 2 cells along every swept axis");
@@ -477,8 +479,8 @@ vg_status vg_create(const vg_grid_desc* desc, vg_solver** out) {
                                      "energy is not stable under FP32 flux values)");
     if (desc->precision == VG_MIXED && (desc->model == VG_MODEL_MHD_REDUCED || desc->model == VG_MODEL_MHD_INTERMEDIATE))
         return fail(VG_EUNSUPPORTED, "the MHD two-material models run in VG_FP64 only");
-    if (desc->precision == VG_MIXED && desc->model == VG_MODEL_HPR_REDUCED)
-        return fail(VG_EUNSUPPORTED, "the HPR reduced two-material model runs in VG_FP64 only");
+    if (desc->precision == VG_MIXED && (desc->model == VG_MODEL_HPR_REDUCED || desc->model == VG_MODEL_HPR_INTERMEDIATE))
+        return fail(VG_EUNSUPPORTED, "the HPR two-material models run in VG_FP64 only");
     if (desc->model == VG_MODEL_HPR) {
         const double eos = desc->params[12];
         if (eos != 0.0 && eos != 1.0 && eos != 2.0)
@@ -492,7 +494,8 @@ vg_status vg_create(const vg_grid_desc* desc, vg_solver** out) {
     s->dims = desc->ny > 1 ? 2 : 1;
     s->max_nw = desc->model == VG_MODEL_EULER ? 4 : desc->model == VG_MODEL_MHD ? 9 : desc->model == VG_MODEL_EULER_REDUCED ? 6
                 : desc->model == VG_MODEL_EULER_MULTIPHYSICS ? 7 : desc->model == VG_MODEL_MHD_REDUCED ? 11
-                : desc->model == VG_MODEL_MHD_INTERMEDIATE ? 12 : desc->model == VG_MODEL_HPR_REDUCED ? 19 : 17;
+                : desc->model == VG_MODEL_MHD_INTERMEDIATE ? 12 : desc->model == VG_MODEL_HPR_REDUCED ? 19
+                : desc->model == VG_MODEL_HPR_INTERMEDIATE ? 20 : 17;
     s->pitch = ((long)desc->nx + 31) / 32 * 32;  // 256-byte aligned rows
     s->plane = s->pitch * desc->ny;
     s->floor5 = std::pow(10.0, -5.0);  // SlopeLimiters::computeSlopeVector's floor (Solvers/slopelimiters.cpp:232-239)
@@ -568,6 +571,8 @@ vg_status vg_upload_primitive(vg_solver* s, const double* planes, int is_device,
         variant = vg::V_MINT12;
     } else if (model == VG_MODEL_HPR_REDUCED) {
         variant = vg::V_HRED19;
+    } else if (model == VG_MODEL_HPR_INTERMEDIATE) {
+        variant = vg::V_HINT20;
     } else if (model == VG_MODEL_HPR) {
         // a solid equation of state or plasticity selects the instantiation that carries them
         variant = (s->d.params[12] != 0.0 || s->d.params[17] != 0.0) ? vg::V_HPR17S : vg::V_HPR17;
@@ -593,10 +598,13 @@ vg_status vg_upload_primitive(vg_solver* s, const double* planes, int is_device,
     for (int k = 0; k < ops->nw && e == cudaSuccess; k++)
         e = copy_plane(s->buf[0] + k * s->plane, s->pitch, planes + (long)kPlanes[variant][k] * n, s->d.nx, s->d.nx,
                        s->d.ny, kind, st);
-    // HPRReducedStateVector::setPrimitiveVariableVector (HPR/Multiphysics/hprreducedstatevector.cpp:78-104) takes J
-    // only when either material is thermal; otherwise the cells keep the default J = 0, which nothing reads
-    if (e == cudaSuccess && variant == vg::V_HRED19 && s->d.params[10] == 0.0 && s->d.params[21] == 0.0)
-        e = cudaMemsetAsync(s->buf[0] + 14 * s->plane, 0, sizeof(double) * 3 * s->plane, st);
+    // HPRReducedStateVector::setPrimitiveVariableVector (HPR/Multiphysics/hprreducedstatevector.cpp:78-104) and
+    // HPRIntermediateStateVector's (hprintermediatestatevector.cpp:82-110) take J only when either material is
+    // thermal; otherwise the cells keep the default J = 0, which nothing reads
+    if (e == cudaSuccess && (variant == vg::V_HRED19 || variant == vg::V_HINT20) && s->d.params[10] == 0.0 &&
+        s->d.params[21] == 0.0)
+        e = cudaMemsetAsync(s->buf[0] + (variant == vg::V_HRED19 ? 14 : 13) * s->plane, 0, sizeof(double) * 3 * s->plane,
+                            st);
     if (e == cudaSuccess) e = cudaMemsetAsync(&s->ctrl->err, 0, sizeof(unsigned), st);  // a fresh state: no error yet
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (checker.joinable()) checker.join();

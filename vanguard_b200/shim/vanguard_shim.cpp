@@ -72,10 +72,11 @@ vg_solver* cached_solver(int model, int nx, int ny, int boundary, const double* 
 void run_planes(int model, std::vector<double>& planes, int nx, int ny, const double* params, int nparams, double dx,
                 double cfl, double tEnd, double bias, int limiter, int subcycles, int maxSteps = 0, int order = 2,
                 int reinit = 0) {
-    // the first-order loop runs in the exact form, bit for bit with the reference; the Euler multiphysics and MHD
+    // the first-order loop runs in the exact form, bit for bit with the reference; the Euler multiphysics, MHD and HPR
     // two-material models have no mixed form
     const bool exact = order == 1 || model == VG_MODEL_EULER_MULTIPHYSICS || model == VG_MODEL_MHD_REDUCED ||
-                       model == VG_MODEL_MHD_INTERMEDIATE;
+                       model == VG_MODEL_MHD_INTERMEDIATE || model == VG_MODEL_HPR_REDUCED ||
+                       model == VG_MODEL_HPR_INTERMEDIATE;
     SolverPtr s = make_solver(model, nx, ny, VG_TRANSMISSIVE, params, nparams, exact ? VG_FP64 : -1);
     vg_run_config c{};
     c.dx = dx;
@@ -92,12 +93,13 @@ void run_planes(int model, std::vector<double>& planes, int nx, int ny, const do
 }
 
 // ---- packing between reference-style cells and SoA primitive planes
+constexpr int kMaxPlanes = 20;  // the most primitive planes of any model (the HPR intermediate state)
 template <class S, class Get>
 std::vector<double> pack(const std::vector<S>& cells, int nvar, Get get) {
     long n = cells.size();
     std::vector<double> p(nvar * n);
     for (long i = 0; i < n; i++) {
-        double w[17];
+        double w[kMaxPlanes];
         get(cells[i], w);
         for (int v = 0; v < nvar; v++) p[v * n + i] = w[v];
     }
@@ -119,7 +121,7 @@ std::vector<double> pack2(const std::vector<std::vector<S> >& cells, int nvar, G
     std::vector<double> p(nvar * n);
     for (long i = 0; i < ny; i++)
         for (long j = 0; j < nx; j++) {
-            double w[17];
+            double w[kMaxPlanes];
             get(cells[i][j], w);
             for (int v = 0; v < nvar; v++) p[v * n + i * nx + j] = w[v];
         }
@@ -155,7 +157,7 @@ std::vector<S> unpack(const std::vector<double>& p, long n, int nvar, Make make)
     std::vector<S> out;
     out.reserve(n);
     for (long i = 0; i < n; i++) {
-        double w[17];
+        double w[kMaxPlanes];
         for (int v = 0; v < nvar; v++) w[v] = p[v * n + i];
         out.push_back(make(w));
     }
@@ -168,7 +170,7 @@ std::vector<std::vector<S> > unpack2(const std::vector<double>& p, long nx, long
     for (long i = 0; i < ny; i++) {
         out[i].reserve(nx);
         for (long j = 0; j < nx; j++) {
-            double w[17];
+            double w[kMaxPlanes];
             for (int v = 0; v < nvar; v++) w[v] = p[v * n + i * nx + j];
             out[i].push_back(make(w));
         }
@@ -210,7 +212,7 @@ int boundary_kind(long n, Eq same) {
 
 template <class S, class Get>
 bool equal_cells(const S& a, const S& b, int nvar, Get get) {
-    double wa[17], wb[17];
+    double wa[kMaxPlanes], wb[kMaxPlanes];
     get(a, wa);
     get(b, wb);
     return std::memcmp(wa, wb, sizeof(double) * nvar) == 0;
@@ -893,4 +895,187 @@ vector<vector<HPRStateVector> > HPRFirstOrderSolver::solve2D(vector<vector<HPRSt
     long ny = initialCells.size(), nx = initialCells[0].size();
     run_planes(VG_MODEL_HPR, p, (int)nx, (int)ny, prm, 20, dx, cfl, tEnd, 0.0, 0, 0, maxSteps, 1);
     return unpack2<HPRStateVector>(p, nx, ny, 17, hpr_make);
+}
+
+// ------------------------------------------------------------------------------- HPR two-material models
+namespace {
+vector<vector<double> > tensor_of(const double* a9) {
+    vector<vector<double> > A(3, vector<double>(3));
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) A[i][j] = a9[3 * i + j];
+    return A;
+}
+void tensor_into(const vector<vector<double> >& A, double* a9) {
+    if (A.size() != 3 || A[0].size() != 3 || A[1].size() != 3 || A[2].size() != 3)
+        throw std::invalid_argument("HPR: the distortion tensor must be 3x3");
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) a9[3 * i + j] = A[i][j];
+}
+bool either_thermal(const HPRMaterialParameters& m1, const HPRMaterialParameters& m2) {
+    return m1.getIsThermal() || m2.getIsThermal();
+}
+// 11 values per material, material k at prm[11 k]: {gamma, p_inf, c_v, rho0, T0, c_s, alpha, tau1, tau2, T_ref,
+// is_thermal}.  The device carries the StiffenedGas gas with elastic relaxation for both materials.
+void hpr_two_params(const HPRMaterialParameters& m1, const HPRMaterialParameters& m2, double* prm) {
+    const HPRMaterialParameters* m[2] = {&m1, &m2};
+    for (int k = 0; k < 2; k++) {
+        if (m[k]->getEquationOfState() != "StiffenedGas" || m[k]->getIsPlastic())
+            throw std::runtime_error("HPR two-material models: both materials must be elastic StiffenedGas materials");
+        double b[20];
+        hpr_params(*m[k], b);
+        for (int i = 0; i < 10; i++) prm[11 * k + i] = b[i];
+        prm[11 * k + 10] = b[11];
+    }
+}
+void hred_get(const HPRReducedStateVector& c, double* w) { std::memcpy(w, c.data(), sizeof(double) * 19); }
+HPRReducedStateVector hred_make(const double* w) {
+    HPRReducedStateVector s;
+    std::memcpy(s.data(), w, sizeof(double) * 19);
+    return s;
+}
+void hint_get(const HPRIntermediateStateVector& c, double* w) { std::memcpy(w, c.data(), sizeof(double) * 20); }
+HPRIntermediateStateVector hint_make(const double* w) {
+    HPRIntermediateStateVector s;
+    std::memcpy(s.data(), w, sizeof(double) * 20);
+    return s;
+}
+// With neither material thermal, setConservedVariableVector leaves a cell's J alone, so every cell keeps the J it
+// was given (the device, which never reads it then, carries zeros)
+int heat_flux_plane(const HPRReducedStateVector&) { return 14; }
+int heat_flux_plane(const HPRIntermediateStateVector&) { return 13; }
+template <class S>
+void keep_cold_heat_flux(S* out, const S* in, long n, const HPRMaterialParameters& m1, const HPRMaterialParameters& m2) {
+    if (either_thermal(m1, m2)) return;
+    for (long i = 0; i < n; i++) {
+        const int j0 = heat_flux_plane(in[i]);
+        for (int k = 0; k < 3; k++) out[i].data()[j0 + k] = in[i].data()[j0 + k];
+    }
+}
+template <class S, class Get, class Make>
+vector<S> hpr_two_run(int model, int nvar, vector<S>& cells, const HPRMaterialParameters& m1,
+                      const HPRMaterialParameters& m2, double dx, double cfl, double tEnd, double bias, int limiter,
+                      int subcycles, int maxSteps, int order, int reinit, Get get, Make make) {
+    double prm[22];
+    hpr_two_params(m1, m2, prm);
+    std::vector<double> p = pack(cells, nvar, get);
+    run_planes(model, p, (int)cells.size(), 1, prm, 22, dx, cfl, tEnd, bias, limiter, subcycles, maxSteps, order,
+               reinit);
+    vector<S> out = unpack<S>(p, cells.size(), nvar, make);
+    keep_cold_heat_flux(out.data(), cells.data(), (long)cells.size(), m1, m2);
+    return out;
+}
+template <class S, class Get, class Make>
+vector<vector<S> > hpr_two_run2(int model, int nvar, vector<vector<S> >& cells, const HPRMaterialParameters& m1,
+                                const HPRMaterialParameters& m2, double dx, double cfl, double tEnd, double bias,
+                                int limiter, int subcycles, int maxSteps, int order, int reinit, Get get, Make make) {
+    double prm[22];
+    hpr_two_params(m1, m2, prm);
+    std::vector<double> p = pack2(cells, nvar, get);
+    long ny = cells.size(), nx = cells[0].size();
+    run_planes(model, p, (int)nx, (int)ny, prm, 22, dx, cfl, tEnd, bias, limiter, subcycles, maxSteps, order, reinit);
+    vector<vector<S> > out = unpack2<S>(p, nx, ny, nvar, make);
+    for (long i = 0; i < ny; i++) keep_cold_heat_flux(out[i].data(), cells[i].data(), nx, m1, m2);
+    return out;
+}
+}  // namespace
+
+// HPRReducedStateVector() (HPR/Multiphysics/hprreducedstatevector.cpp:3-19)
+HPRReducedStateVector::HPRReducedStateVector()
+    : w_{0.999, 1.0 / 1.4, 1.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 1.0, 1.0} {}
+HPRReducedStateVector::HPRReducedStateVector(double a1, double p, vector<vector<double> > A, double u, double v, double w,
+                                             double jx, double jy, double jz, double r1, double r2)
+    : w_{a1, p, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, u, v, w, jx, jy, jz, r1, r2} {
+    tensor_into(A, w_ + 2);
+}
+void HPRReducedStateVector::setPrimitiveVariableVector(vector<double> w, HPRMaterialParameters m1,
+                                                       HPRMaterialParameters m2) {
+    const bool thermal = either_thermal(m1, m2);
+    for (int i = 0; i < 19; i++)
+        if (thermal || i < 14 || i > 16) w_[i] = w[i];
+}
+vector<double> HPRReducedStateVector::computePrimitiveVariableVector(HPRMaterialParameters m1,
+                                                                     HPRMaterialParameters m2) const {
+    vector<double> w(w_, w_ + 19);
+    if (!either_thermal(m1, m2)) w[14] = w[15] = w[16] = 0.0;
+    return w;
+}
+vector<vector<double> > HPRReducedStateVector::getInterfaceDistortionTensor() const { return tensor_of(w_ + 2); }
+
+// HPRIntermediateStateVector() (HPR/Multiphysics/hprintermediatestatevector.cpp:3-21)
+HPRIntermediateStateVector::HPRIntermediateStateVector()
+    : w_{0.999, 1.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 1.0, 1.0 / 1.4, 1.0, 1.0 / 1.4} {}
+HPRIntermediateStateVector::HPRIntermediateStateVector(double a1, vector<vector<double> > A, double u, double v,
+                                                       double w, double jx, double jy, double jz, double r1, double p1,
+                                                       double r2, double p2)
+    : w_{a1, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, u, v, w, jx, jy, jz, r1, p1, r2, p2} {
+    tensor_into(A, w_ + 1);
+}
+void HPRIntermediateStateVector::setPrimitiveVariableVector(vector<double> w, HPRMaterialParameters m1,
+                                                            HPRMaterialParameters m2) {
+    const bool thermal = either_thermal(m1, m2);
+    for (int i = 0; i < 20; i++)
+        if (thermal || i < 13 || i > 15) w_[i] = w[i];
+}
+vector<double> HPRIntermediateStateVector::computePrimitiveVariableVector(HPRMaterialParameters m1,
+                                                                          HPRMaterialParameters m2) const {
+    vector<double> w(w_, w_ + 20);
+    if (!either_thermal(m1, m2)) w[13] = w[14] = w[15] = 0.0;
+    return w;
+}
+vector<vector<double> > HPRIntermediateStateVector::getInterfaceDistortionTensor() const { return tensor_of(w_ + 1); }
+
+vector<HPRReducedStateVector> HPRSecondOrderSolver::solve(vector<HPRReducedStateVector>& initialCells, double dx,
+                                                          double cfl, double tEnd, double bias, int limiter,
+                                                          int subcycles, int reinit, HPRMaterialParameters m1,
+                                                          HPRMaterialParameters m2, int maxSteps) {
+    return hpr_two_run(VG_MODEL_HPR_REDUCED, 19, initialCells, m1, m2, dx, cfl, tEnd, bias, limiter, subcycles,
+                       maxSteps, 2, reinit, hred_get, hred_make);
+}
+vector<vector<HPRReducedStateVector> > HPRSecondOrderSolver::solve2D(vector<vector<HPRReducedStateVector> >& initialCells,
+                                                                     double dx, double cfl, double tEnd, double bias,
+                                                                     int limiter, int subcycles, int reinit,
+                                                                     HPRMaterialParameters m1, HPRMaterialParameters m2,
+                                                                     int maxSteps) {
+    return hpr_two_run2(VG_MODEL_HPR_REDUCED, 19, initialCells, m1, m2, dx, cfl, tEnd, bias, limiter, subcycles,
+                        maxSteps, 2, reinit, hred_get, hred_make);
+}
+vector<HPRIntermediateStateVector> HPRSecondOrderSolver::solve(vector<HPRIntermediateStateVector>& initialCells,
+                                                               double dx, double cfl, double tEnd, double bias,
+                                                               int limiter, int subcycles, int reinit,
+                                                               HPRMaterialParameters m1, HPRMaterialParameters m2,
+                                                               int maxSteps) {
+    return hpr_two_run(VG_MODEL_HPR_INTERMEDIATE, 20, initialCells, m1, m2, dx, cfl, tEnd, bias, limiter, subcycles,
+                       maxSteps, 2, reinit, hint_get, hint_make);
+}
+vector<vector<HPRIntermediateStateVector> > HPRSecondOrderSolver::solve2D(
+    vector<vector<HPRIntermediateStateVector> >& initialCells, double dx, double cfl, double tEnd, double bias,
+    int limiter, int subcycles, int reinit, HPRMaterialParameters m1, HPRMaterialParameters m2, int maxSteps) {
+    return hpr_two_run2(VG_MODEL_HPR_INTERMEDIATE, 20, initialCells, m1, m2, dx, cfl, tEnd, bias, limiter, subcycles,
+                        maxSteps, 2, reinit, hint_get, hint_make);
+}
+vector<HPRReducedStateVector> HPRFirstOrderSolver::solve(vector<HPRReducedStateVector>& initialCells, double dx,
+                                                         double cfl, double tEnd, int, HPRMaterialParameters m1,
+                                                         HPRMaterialParameters m2, int maxSteps) {
+    return hpr_two_run(VG_MODEL_HPR_REDUCED, 19, initialCells, m1, m2, dx, cfl, tEnd, 0.0, 0, 0, maxSteps, 1, 0,
+                       hred_get, hred_make);
+}
+vector<vector<HPRReducedStateVector> > HPRFirstOrderSolver::solve2D(vector<vector<HPRReducedStateVector> >& initialCells,
+                                                                    double dx, double cfl, double tEnd, int,
+                                                                    HPRMaterialParameters m1, HPRMaterialParameters m2,
+                                                                    int maxSteps) {
+    return hpr_two_run2(VG_MODEL_HPR_REDUCED, 19, initialCells, m1, m2, dx, cfl, tEnd, 0.0, 0, 0, maxSteps, 1, 0,
+                        hred_get, hred_make);
+}
+vector<HPRIntermediateStateVector> HPRFirstOrderSolver::solve(vector<HPRIntermediateStateVector>& initialCells,
+                                                              double dx, double cfl, double tEnd, int,
+                                                              HPRMaterialParameters m1, HPRMaterialParameters m2,
+                                                              int maxSteps) {
+    return hpr_two_run(VG_MODEL_HPR_INTERMEDIATE, 20, initialCells, m1, m2, dx, cfl, tEnd, 0.0, 0, 0, maxSteps, 1, 0,
+                       hint_get, hint_make);
+}
+vector<vector<HPRIntermediateStateVector> > HPRFirstOrderSolver::solve2D(
+    vector<vector<HPRIntermediateStateVector> >& initialCells, double dx, double cfl, double tEnd, int,
+    HPRMaterialParameters m1, HPRMaterialParameters m2, int maxSteps) {
+    return hpr_two_run2(VG_MODEL_HPR_INTERMEDIATE, 20, initialCells, m1, m2, dx, cfl, tEnd, 0.0, 0, 0, maxSteps, 1, 0,
+                        hint_get, hint_make);
 }

@@ -329,6 +329,75 @@ private:
 };
 
 // ------------------------------------------------------------------------------------------- slope limiters
+// HPRReducedStateVector (HPR/Multiphysics/hprreducedstatevector.h): the HPR reduced two-material state, primitives
+// alpha1, p, A (9, row-major), u, v, w, Jx, Jy, Jz, rho1, rho2.  As in the reference, the heat flux J is taken and
+// returned only when either material is thermal (hprreducedstatevector.cpp:78-109, :154-185).
+class HPRReducedStateVector {
+public:
+    HPRReducedStateVector();
+    HPRReducedStateVector(double newMaterial1VolumeFraction, double newInterfacePressure,
+                          vector<vector<double> > newInterfaceDistortionTensor, double newInterfaceXVelocity,
+                          double newInterfaceYVelocity, double newInterfaceZVelocity, double newInterfaceXThermalImpulse,
+                          double newInterfaceYThermalImpulse, double newInterfaceZThermalImpulse,
+                          double newMaterial1Density, double newMaterial2Density);
+    void setPrimitiveVariableVector(vector<double> w, HPRMaterialParameters material1Parameters,
+                                    HPRMaterialParameters material2Parameters);
+    vector<double> computePrimitiveVariableVector(HPRMaterialParameters material1Parameters,
+                                                  HPRMaterialParameters material2Parameters) const;
+    double getMaterial1VolumeFraction() const { return w_[0]; }
+    double getInterfacePressure() const { return w_[1]; }
+    vector<vector<double> > getInterfaceDistortionTensor() const;
+    double getInterfaceXVelocity() const { return w_[11]; }
+    double getInterfaceYVelocity() const { return w_[12]; }
+    double getInterfaceZVelocity() const { return w_[13]; }
+    double getInterfaceXThermalImpulse() const { return w_[14]; }
+    double getInterfaceYThermalImpulse() const { return w_[15]; }
+    double getInterfaceZThermalImpulse() const { return w_[16]; }
+    double getMaterial1Density() const { return w_[17]; }
+    double getMaterial2Density() const { return w_[18]; }
+    void setMaterial1VolumeFraction(double v) { w_[0] = v; }
+    double* data() { return w_; }
+    const double* data() const { return w_; }
+
+private:
+    double w_[19];
+};
+
+// HPRIntermediateStateVector (HPR/Multiphysics/hprintermediatestatevector.h): the HPR intermediate two-material state,
+// primitives alpha1, A (9, row-major), u, v, w, Jx, Jy, Jz, rho1, p1, rho2, p2; J as for the reduced state
+// (hprintermediatestatevector.cpp:82-110, :161-193).
+class HPRIntermediateStateVector {
+public:
+    HPRIntermediateStateVector();
+    HPRIntermediateStateVector(double newMaterial1VolumeFraction, vector<vector<double> > newInterfaceDistortionTensor,
+                               double newInterfaceXVelocity, double newInterfaceYVelocity, double newInterfaceZVelocity,
+                               double newInterfaceXThermalImpulse, double newInterfaceYThermalImpulse,
+                               double newInterfaceZThermalImpulse, double newMaterial1Density, double newMaterial1Pressure,
+                               double newMaterial2Density, double newMaterial2Pressure);
+    void setPrimitiveVariableVector(vector<double> w, HPRMaterialParameters material1Parameters,
+                                    HPRMaterialParameters material2Parameters);
+    vector<double> computePrimitiveVariableVector(HPRMaterialParameters material1Parameters,
+                                                  HPRMaterialParameters material2Parameters) const;
+    double getMaterial1VolumeFraction() const { return w_[0]; }
+    vector<vector<double> > getInterfaceDistortionTensor() const;
+    double getInterfaceXVelocity() const { return w_[10]; }
+    double getInterfaceYVelocity() const { return w_[11]; }
+    double getInterfaceZVelocity() const { return w_[12]; }
+    double getInterfaceXThermalImpulse() const { return w_[13]; }
+    double getInterfaceYThermalImpulse() const { return w_[14]; }
+    double getInterfaceZThermalImpulse() const { return w_[15]; }
+    double getMaterial1Density() const { return w_[16]; }
+    double getMaterial1Pressure() const { return w_[17]; }
+    double getMaterial2Density() const { return w_[18]; }
+    double getMaterial2Pressure() const { return w_[19]; }
+    void setMaterial1VolumeFraction(double v) { w_[0] = v; }
+    double* data() { return w_; }
+    const double* data() const { return w_; }
+
+private:
+    double w_[20];
+};
+
 class SlopeLimiters {
 public:
     static double computeRCoefficient(double steepness, double bias);
@@ -509,6 +578,27 @@ public:
 
 class HPRFirstOrderSolver {
 public:
+    // the HPR two-material models (Solvers/hprfirstordersolver.cpp:501-546, :576-638), exact form; maxSteps > 0 also
+    // stops after that many steps (not in the reference)
+    static vector<HPRReducedStateVector> solve(vector<HPRReducedStateVector>& initialCells, double cellSpacing,
+                                               double CFLCoefficient, double finalTime, int subcyclingIterations,
+                                               HPRMaterialParameters material1Parameters,
+                                               HPRMaterialParameters material2Parameters, int maxSteps = 0);
+    static vector<vector<HPRReducedStateVector> > solve2D(vector<vector<HPRReducedStateVector> >& initialCells,
+                                                          double cellSpacing, double CFLCoefficient, double finalTime,
+                                                          int subcyclingIterations,
+                                                          HPRMaterialParameters material1Parameters,
+                                                          HPRMaterialParameters material2Parameters, int maxSteps = 0);
+    static vector<HPRIntermediateStateVector> solve(vector<HPRIntermediateStateVector>& initialCells, double cellSpacing,
+                                                    double CFLCoefficient, double finalTime, int subcyclingIterations,
+                                                    HPRMaterialParameters material1Parameters,
+                                                    HPRMaterialParameters material2Parameters, int maxSteps = 0);
+    static vector<vector<HPRIntermediateStateVector> > solve2D(vector<vector<HPRIntermediateStateVector> >& initialCells,
+                                                               double cellSpacing, double CFLCoefficient,
+                                                               double finalTime, int subcyclingIterations,
+                                                               HPRMaterialParameters material1Parameters,
+                                                               HPRMaterialParameters material2Parameters,
+                                                               int maxSteps = 0);
     static vector<HPRStateVector> solve(vector<HPRStateVector>& initialCells, double cellSpacing, double CFLCoefficient,
                                         double finalTime, int subcyclingIterations, HPRMaterialParameters mp);
     static vector<vector<HPRStateVector> > solve2D(vector<vector<HPRStateVector> >& initialCells, double cellSpacing,
@@ -535,4 +625,31 @@ public:
     static vector<vector<HPRStateVector> > solve2D(vector<vector<HPRStateVector> >& initialCells, double cellSpacing,
                                                    double CFLCoefficient, double finalTime, double bias, int slopeLimiter,
                                                    int subcyclingIterations, HPRMaterialParameters mp, int maxSteps);
+    // the HPR two-material models (Solvers/hprsecondordersolver.cpp:402-500, :548-658): RK4 relaxation sub-cycles
+    // around the sweeps, reinitialisation every reinitialisationFrequency steps; exact form; maxSteps > 0 also stops
+    // after that many steps (not in the reference)
+    static vector<HPRReducedStateVector> solve(vector<HPRReducedStateVector>& initialCells, double cellSpacing,
+                                               double CFLCoefficient, double finalTime, double bias, int slopeLimiter,
+                                               int subcyclingIterations, int reinitialisationFrequency,
+                                               HPRMaterialParameters material1Parameters,
+                                               HPRMaterialParameters material2Parameters, int maxSteps = 0);
+    static vector<vector<HPRReducedStateVector> > solve2D(vector<vector<HPRReducedStateVector> >& initialCells,
+                                                          double cellSpacing, double CFLCoefficient, double finalTime,
+                                                          double bias, int slopeLimiter, int subcyclingIterations,
+                                                          int reinitialisationFrequency,
+                                                          HPRMaterialParameters material1Parameters,
+                                                          HPRMaterialParameters material2Parameters, int maxSteps = 0);
+    static vector<HPRIntermediateStateVector> solve(vector<HPRIntermediateStateVector>& initialCells, double cellSpacing,
+                                                    double CFLCoefficient, double finalTime, double bias,
+                                                    int slopeLimiter, int subcyclingIterations,
+                                                    int reinitialisationFrequency,
+                                                    HPRMaterialParameters material1Parameters,
+                                                    HPRMaterialParameters material2Parameters, int maxSteps = 0);
+    static vector<vector<HPRIntermediateStateVector> > solve2D(vector<vector<HPRIntermediateStateVector> >& initialCells,
+                                                               double cellSpacing, double CFLCoefficient,
+                                                               double finalTime, double bias, int slopeLimiter,
+                                                               int subcyclingIterations, int reinitialisationFrequency,
+                                                               HPRMaterialParameters material1Parameters,
+                                                               HPRMaterialParameters material2Parameters,
+                                                               int maxSteps = 0);
 };

@@ -409,3 +409,26 @@ def hpr_reduced_riemann(nx, ny=1, seed=0, distortion=0.02, heat=0.05, bubble=Fal
     W[17] = np.where(left, 1.0, 0.8)
     W[18] = np.where(left, 0.5, 0.25)
     return W
+
+
+HPR_INTERMEDIATE_NVAR = 20
+
+
+def hpr_intermediate_from_reduced(W, p2_scale=1.0):
+    """The HPR intermediate model's 20 planes (alpha1, A(9), u, v, w, Jx, Jy, Jz, rho1, p1, rho2, p2) of an HPR reduced
+    state (alpha1, p, A(9), u, v, w, Jx, Jy, Jz, rho1, rho2): material 1 at the interface pressure, material 2 at
+    p2_scale times it."""
+    out = np.zeros((HPR_INTERMEDIATE_NVAR,) + W.shape[1:])
+    out[0] = W[0]
+    out[1:16] = W[2:17]
+    out[16] = W[17]
+    out[17] = W[1]
+    out[18] = W[18]
+    out[19] = p2_scale * W[1]
+    return out
+
+
+def hpr_intermediate_riemann(nx, ny=1, seed=0, distortion=0.02, heat=0.05, bubble=False, p2_scale=1.0):
+    """hpr_reduced_riemann's two-material HPR Riemann problem in the intermediate model's planes, shape (20, n) or
+    (20, ny, nx)."""
+    return hpr_intermediate_from_reduced(hpr_reduced_riemann(nx, ny, seed, distortion, heat, bubble), p2_scale)
