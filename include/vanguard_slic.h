@@ -26,6 +26,10 @@
  *   VG_MODEL_HPR_INTERMEDIATE (20 planes): alpha1, A(9, row-major), u, v, w, Jx, Jy, Jz, rho1, p1, rho2, p2   the
  *                                      HPR intermediate two-material model, HPR/Multiphysics/
  *                                      hprintermediatestatevector.cpp:161-193 (VG_FP64 only)
+ *   VG_MODEL_HPR_MULTIPHYSICS (32 planes): alpha1, u, v, w, rho1, p1, A1(9), J1(3), rho2, p2, A2(9), J2(3)   the HPR
+ *                                      multiphysics two-material model, HPR/Multiphysics/
+ *                                      hprmultiphysicsstatevector.cpp:204-249 (VG_FP64 only; 1D: ny = 1; a cold
+ *                                      material's J is taken and returned as 0)
  * Ownership: a vg_solver owns all device memory it allocates; the caller owns every host buffer.
  * Threading: calls on different solvers are independent and re-entrant; one solver must not be used
  * from two host threads at once.  All work is enqueued on the stream given (NULL: the legacy default
@@ -61,7 +65,8 @@ typedef enum vg_model {
     VG_MODEL_MHD_REDUCED = 5,
     VG_MODEL_MHD_INTERMEDIATE = 6,
     VG_MODEL_HPR_REDUCED = 7,
-    VG_MODEL_HPR_INTERMEDIATE = 8
+    VG_MODEL_HPR_INTERMEDIATE = 8,
+    VG_MODEL_HPR_MULTIPHYSICS = 9
 } vg_model;
 
 /* VG_FP64: every operation in float64, in the reference's order, no FMA: matches the reference.
@@ -97,7 +102,7 @@ enum { VG_SUPERBEE = 0, VG_VANLEER = 1, VG_MINBEE = 2 };
  *                                                 the exponent alpha_eos); is_plastic selects the plastic strain
  *                                                 relaxation with transition stress sigma0 and power-law index n
  *                                                 (HPR/hprsourceterms.cpp:12-23).
- *   HPR reduced, HPR intermediate: 11 per material, material k at params[11 k]: {gamma, p_inf, c_v, rho0, T0, c_s,
+ *   HPR reduced, intermediate, multiphysics: 11 per material, material k at params[11 k]: {gamma, p_inf, c_v, rho0, T0, c_s,
  *                alpha, tau1, tau2, T_ref, is_thermal}   the two materials' StiffenedGas HPRMaterialParameters (elastic
  *                relaxation)
  * The last slot is reserved. */
@@ -143,7 +148,7 @@ typedef struct vg_solver vg_solver;
 vg_status vg_create(const vg_grid_desc* desc, vg_solver** out);
 vg_status vg_destroy(vg_solver* s);
 
-/* Number of primitive planes the model takes at this boundary (6, 9, 17, 7, 8, 11, 12, 19, 20). */
+/* Number of primitive planes the model takes at this boundary (6, 9, 17, 7, 8, 11, 12, 19, 20, 32). */
 int vg_model_nvar(int model);
 
 /* Copy the state in / out.  planes: vg_model_nvar(model) planes of nx*ny float64, host or device

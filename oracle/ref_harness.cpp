@@ -1085,3 +1085,38 @@ extern "C" double vgref_hpr_intermediate_run(double* planes, int nx, int ny, dou
     return hprTwoMaterialRun<HPRIntermediateStateVector>(planes, 20, nx, ny, dx, cfl, t_end, max_steps, bias, limiter,
                                                          prm, subcycles, reinit_freq, steps_out);
 }
+
+// ------------------------------------------------------------------------------- HPR multiphysics two-material
+// Planes: the 32 primitives of HPRMultiphysicsStateVector (alpha1, u, v, w, rho1, p1, A1(9), J1(3), rho2, p2, A2(9),
+// J2(3); HPR/Multiphysics/hprmultiphysicsstatevector.cpp:204-249); prm as for the reduced model; 1D only, as the
+// reference has it.  max_steps <= 0: the reference's own HPRSecondOrderSolver::solve to t_end (Solvers/
+// hprsecondordersolver.cpp:354-400, whose sub-cycle loops only pad the grid); else its per-step functions for max_steps
+// steps in solve's order, with the reinitialisation every reinit_freq steps.
+extern "C" double vgref_hpr_multiphysics_run(double* planes, int nx, double dx, double cfl, double t_end, int max_steps,
+                                             double bias, int limiter, const double* prm, int subcycles,
+                                             int reinit_freq, int* steps_out) {
+    QuietCout quiet;
+    HPRMaterialParameters m1 = hredParams(prm, 0), m2 = hredParams(prm, 1);
+    const long plane = nx;
+    double t = 0.0;
+    int it = 0;
+    vector<HPRMultiphysicsStateVector> cells(nx);
+    for (int i = 0; i < nx; i++) cells[i] = hprTwoCell<HPRMultiphysicsStateVector>(planes, plane, i, 32, m1, m2);
+    if (max_steps <= 0) {
+        cells = HPRSecondOrderSolver::solve(cells, dx, cfl, t_end, bias, limiter, subcycles, reinit_freq, m1, m2);
+        t = t_end;
+    } else {
+        for (; it < max_steps; it++) {
+            vector<HPRMultiphysicsStateVector> withB = HPRSolvers::insertBoundaryCells(cells, 2);
+            double dt = HPRSolvers::computeStableTimeStep(withB, dx, cfl, t, 1.0e300, it, m1, m2);
+            withB = HPRSolvers::insertBoundaryCells(cells, 2);
+            HPRSecondOrderSolver::computeSLICTimeStep(cells, withB, dx, dt, bias, limiter, m1, m2);
+            t += dt;
+            if (reinit_freq != 0 && ((it + 1) % reinit_freq) == 0)
+                MultiphysicsSolvers::reinitialiseVolumeFraction(cells, m1, m2);
+        }
+    }
+    for (int i = 0; i < nx; i++) hprTwoStore(cells[i], planes, plane, i, 32, m1, m2);
+    if (steps_out) *steps_out = it;
+    return t;
+}

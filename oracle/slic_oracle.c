@@ -14,7 +14,7 @@
 #include <stdlib.h>
 #include <string.h>
 
-#define MAXV 21
+#define MAXV 33
 
 /* std::min / std::max semantics: min(a,b) = (b < a) ? b : a; max(a,b) = (a < b) ? b : a. */
 static double smin(double a, double b) { return (b < a) ? b : a; }
@@ -701,7 +701,11 @@ static void hpr_relax_cell(double* U, double h, const double* prm) {
  * Only the entries dsigma/dA[d][i][j][d] of HPREquationOfState::computeShearStressTensorDerivativeDistortionTensor
  * (HPR/hprequationofstate.cpp:83-113) enter; they are rebuilt here with the same sums and the same order of
  * the two += updates (the i == d entries receive the update twice, in the same loop iteration). */
-static double hpr_acoustic_speed(const double* W, int d, const double* prm) {
+static double hpr_acoustic_speed_q(const double* W, int d, const double* prm, int diag);
+static double hpr_acoustic_speed(const double* W, int d, const double* prm) { return hpr_acoustic_speed_q(W, d, prm, 0); }
+/* diag != 0: the second tensor block reads dsigma/dA[d][i][i][d] for every column j, as the HPR multiphysics model's
+ * material-2 tensor does (HPR/Multiphysics/hprmultiphysicsacoustictensor.cpp:61) */
+static double hpr_acoustic_speed_q(const double* W, int d, const double* prm, int diag) {
     double rho = W[0], p = W[1];
     mat3 A = load_A(W + 2);
     mat3 At = tr3(&A), G = mm3(&At, &A), D = deviator3(&G);
@@ -732,7 +736,7 @@ static double hpr_acoustic_speed(const double* W, int d, const double* prm) {
     c1[0][1] = 1.0 / rho;
     for (int i = 0; i < 3; i++) c1[i][0] = -(1.0 / rho) * dsdrho.m[d][i];
     for (int i = 0; i < 3; i++)
-        for (int j = 0; j < 3; j++) c1[i][2 + j] = -(1.0 / rho) * dsdA[i][j];
+        for (int j = 0; j < 3; j++) c1[i][2 + j] = -(1.0 / rho) * dsdA[i][diag ? i : j];
     if (hpr_thermal(prm)) {
         c1[3][0] = mg_dTdrho(rho, p, prm) / rho;
         c1[3][1] = mg_dTdp(rho, prm) / rho;
@@ -1550,6 +1554,197 @@ static void hint_default(const double* prm, double* W) {
     W[18] = 1.0;
     W[19] = 1.0 / 1.4;
 }
+/* ---- HPR multiphysics two-material model: HPR/Multiphysics/hprmultiphysicsstatevector.cpp (1D only in the
+ * reference).  Each material carries its own density, pressure, distortion tensor and heat flux; the velocity is
+ * shared.  prm as for the reduced model (11 values per material); each material's J is carried when that material is
+ * thermal.  The distortion enters the conserved vector as pow(alpha_k, 1/3) A_k.
+ * W = alpha1, u, v, w, rho1, p1, A1 (9), J1 (3), rho2, p2, A2 (9), J2 (3) (:204-249) and an unused plane;
+ * U = rho, rho alpha1, rho u (3), alpha1 rho1, alpha1 rho1 E1, alpha1^(1/3) A1, alpha1 rho1 J1, then the same five
+ * groups of material 2 from 19 (:251-317). */
+static int hmph_thermal(const double* prm, int k) { return prm[11 * k + 10] != 0.0; }
+/* computeConservedVariableVector (:251-317) */
+static void hmph_cons(const double* W, const double* prm, double* U) {
+    double a1 = red_clamp(W[0]), a2 = 1.0 - a1;
+    double rho = (a1 * W[4]) + (a2 * W[18]);
+    for (int i = 0; i < 33; i++) U[i] = 0.0;
+    U[0] = rho;
+    U[1] = rho * a1;
+    U[2] = rho * W[1];
+    U[3] = rho * W[2];
+    U[4] = rho * W[3];
+    for (int k = 0; k < 2; k++) {
+        double b[24];
+        hred_mat(prm, k, b);
+        double a = k == 0 ? a1 : a2;
+        const double* w = W + 4 + 14 * k; /* rho_k, p_k, A_k (9), J_k (3) */
+        double* u = U + 5 + 14 * k;       /* a rho_k, a rho_k E_k, a^(1/3) A_k (9), a rho_k J_k (3) */
+        u[0] = a * w[0];
+        for (int i = 0; i < 9; i++) u[2 + i] = pow(a, (1.0 / 3.0)) * w[2 + i];
+        if (hmph_thermal(prm, k))
+            for (int i = 0; i < 3; i++) u[11 + i] = a * (w[0] * w[11 + i]);
+        mat3 A = load_A(w + 2);
+        double E = hpr_total_energy(w[0], w[1], W[1], W[2], W[3], &A, w[11], w[12], w[13], b);
+        u[1] = a * (w[0] * E);
+    }
+}
+/* setConservedVariableVector (:141-202): J_k kept when material k is not thermal */
+static void hmph_setcons(const double* U, const double* prm, double* W) {
+    double rho = U[0];
+    double a1 = red_clamp(U[1] / rho), a2 = 1.0 - a1;
+    W[1] = U[2] / rho;
+    W[2] = U[3] / rho;
+    W[3] = U[4] / rho;
+    for (int k = 0; k < 2; k++) {
+        double b[24];
+        hred_mat(prm, k, b);
+        double a = k == 0 ? a1 : a2;
+        double* w = W + 4 + 14 * k;
+        const double* u = U + 5 + 14 * k;
+        w[0] = u[0] / a;
+        for (int i = 0; i < 9; i++) w[2 + i] = u[2 + i] / pow(a, (1.0 / 3.0));
+        if (hmph_thermal(prm, k))
+            for (int i = 0; i < 3; i++) w[11 + i] = u[11 + i] / (a * w[0]);
+        double E = u[1] / (a * w[0]);
+        mat3 A = load_A(w + 2);
+        w[1] = hpr_pressure(w[0], E, W[1], W[2], W[3], &A, w[11], w[12], w[13], b);
+    }
+    W[0] = a1;
+}
+/* computeXFluxVector (:319-463); the reference has no Y flux for this model */
+static void hmph_flux(const double* U, int axis, const double* prm, double* F) {
+    (void)axis;
+    double rho = U[0];
+    double a1 = red_clamp(U[1] / rho), a2 = 1.0 - a1;
+    double u = U[2] / rho, v = U[3] / rho, w = U[4] / rho;
+    double vel[3] = {u, v, w};
+    double r[2], p[2], E[2], J[2][3];
+    mat3 A[2], sg[2];
+    for (int k = 0; k < 2; k++) {
+        double b[24];
+        hred_mat(prm, k, b);
+        double a = k == 0 ? a1 : a2;
+        const double* c = U + 5 + 14 * k;
+        r[k] = c[0] / a;
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) A[k].m[i][j] = c[2 + (i * 3) + j] / pow(a, (1.0 / 3.0));
+        for (int i = 0; i < 3; i++) J[k][i] = c[11 + i] / (a * r[k]);
+        E[k] = c[1] / (a * r[k]);
+        p[k] = hpr_pressure(r[k], E[k], u, v, w, &A[k], J[k][0], J[k][1], J[k][2], b);
+        sg[k] = shear_stress(r[k], &A[k], b);
+    }
+    double pi = (a1 * p[0]) + (a2 * p[1]);
+    for (int i = 0; i < 33; i++) F[i] = 0.0;
+    F[0] = rho * u;
+    F[1] = rho * (u * a1);
+    F[2] = (rho * (u * u)) + pi;
+    F[3] = rho * (u * v);
+    F[4] = rho * (u * w);
+    for (int k = 0; k < 2; k++) {
+        double a = k == 0 ? a1 : a2;
+        F[5 + 14 * k] = a * (r[k] * u);
+        F[6 + 14 * k] = a * ((r[k] * (u * E[k])) + (p[k] * u));
+    }
+    for (int k = 0; k < 2; k++) {
+        double a = k == 0 ? a1 : a2;
+        F[6 + 14 * k] -= a * (((0.0 + (sg[k].m[0][0] * vel[0])) + (sg[k].m[0][1] * vel[1])) + (sg[k].m[0][2] * vel[2]));
+    }
+    for (int i = 0; i < 3; i++) F[2 + i] -= (a1 * sg[0].m[0][i]) + (a2 * sg[1].m[0][i]);
+    for (int k = 0; k < 2; k++) {
+        double a = k == 0 ? a1 : a2;
+        for (int i = 0; i < 3; i++) {
+            double Av = ((0.0 + (A[k].m[i][0] * u)) + (A[k].m[i][1] * v)) + (A[k].m[i][2] * w);
+            F[7 + 14 * k + (i * 3)] = pow(a, (1.0 / 3.0)) * Av;
+        }
+    }
+    for (int k = 0; k < 2; k++) {
+        if (!hmph_thermal(prm, k)) continue;
+        double b[24];
+        hred_mat(prm, k, b);
+        double a = k == 0 ? a1 : a2;
+        double T = mg_temperature(r[k], p[k], b);
+        F[6 + 14 * k] += a * (T * ((b[6] * b[6]) * J[k][0]));
+        F[16 + 14 * k] = a * ((r[k] * (u * J[k][0])) + T);
+        F[17 + 14 * k] = a * (r[k] * (u * J[k][1]));
+        F[18 + 14 * k] = a * (r[k] * (u * J[k][2]));
+    }
+}
+/* HPRMultiphysicsAcousticTensor::computeMaximumWaveSpeed (HPR/Multiphysics/hprmultiphysicsacoustictensor.cpp:177-184):
+ * each material's single-material acoustic speed at its own density, pressure and distortion; material 2's reads the
+ * diagonal dsigma/dA entries in its second block (:61) */
+static double hmph_speed(const double* W, int d, const double* prm, int k) {
+    double b[24], Wk[17];
+    hred_mat(prm, k, b);
+    const double* w = W + 4 + 14 * k;
+    Wk[0] = w[0];
+    Wk[1] = w[1];
+    for (int i = 0; i < 9; i++) Wk[2 + i] = w[2 + i];
+    Wk[11] = W[1];
+    Wk[12] = W[2];
+    Wk[13] = W[3];
+    for (int i = 0; i < 3; i++) Wk[14 + i] = w[11 + i];
+    return hpr_acoustic_speed_q(Wk, d, b, k == 1);
+}
+/* HPRSolvers::computeMaximumWaveSpeed for the multiphysics model (Solvers/hprsolvers.cpp:305-322) */
+static double hmph_wave1d(const double* W, const double* prm) {
+    return fabs(W[1]) + smax(hmph_speed(W, 0, prm, 0), hmph_speed(W, 0, prm, 1));
+}
+static double hmph_wave2d(const double* W, const double* prm) { (void)W; (void)prm; return NAN; }
+/* HPRMultiphysicsStateVector() (:3-26) */
+static void hmph_default(const double* prm, double* W) {
+    (void)prm;
+    for (int i = 0; i < 33; i++) W[i] = 0.0;
+    W[0] = 0.999;
+    for (int k = 0; k < 2; k++) {
+        double* w = W + 4 + 14 * k;
+        w[0] = 1.0;
+        w[1] = 1.0 / 1.4;
+        w[2] = 1.0;
+        w[6] = 1.0;
+        w[10] = 1.0;
+    }
+}
+/* setPrimitiveVariableVector (:98-139) takes material k's J only when that material is thermal; otherwise the cells
+ * keep the default J_k = 0, which nothing reads */
+static void hmph_drop_cold_heat_flux(int id, double* planes, long n, const double* prm) {
+    if (id != VO_HPR_MULTIPHYSICS) return;
+    for (int k = 0; k < 2; k++)
+        if (!hmph_thermal(prm, k))
+            for (long i = (15 + 14 * k) * n; i < (18 + 14 * k) * n; i++) planes[i] = 0.0;
+}
+/* MultiphysicsSolvers::reinitialiseVolumeFraction for the HPR multiphysics model (Solvers/multiphysicssolvers.cpp:
+ * 807-839; 1D): the last cell i >= 1 with alpha_i < 0.5 <= alpha_{i-1}, or 0, and the window i-2 .. i+1, whose cells
+ * relax the density, pressure, distortion (pow(alpha_k, 1/3)-weighted) and heat flux components of both materials to
+ * their mixtures (:614-704) with the cell's own alpha, then take 0.999 | 0.001.  Window cells outside the grid, which
+ * the reference writes out of bounds, are skipped. */
+static void hmph_reinit(double* planes, int nx) {
+    long plane = nx;
+    int loc = 0;
+    for (int i = 1; i < nx; i++)
+        if (planes[i] < 0.5 && planes[i - 1] >= 0.5) loc = i;
+    for (int i = loc - 2; i < loc + 2; i++) {
+        if (i < 0 || i >= nx) continue;
+        double a1 = planes[i], a2 = 1.0 - a1;
+#define HM(v) planes[(long)(v) * plane + i]
+        double rho = (a1 * HM(4)) + (a2 * HM(18));
+        HM(4) = rho;
+        HM(18) = rho;
+        double p = (a1 * HM(5)) + (a2 * HM(19));
+        HM(5) = p;
+        HM(19) = p;
+        for (int e = 0; e < 9; e++) {
+            double A = (pow(a1, (1.0 / 3.0)) * HM(6 + e)) + (pow(a2, (1.0 / 3.0)) * HM(20 + e));
+            HM(6 + e) = A;
+            HM(20 + e) = A;
+        }
+        for (int e = 0; e < 3; e++) {
+            double J = (a1 * HM(15 + e)) + (a2 * HM(29 + e));
+            HM(15 + e) = J;
+            HM(29 + e) = J;
+        }
+#undef HM
+        planes[i] = i < loc ? 0.999 : 0.001;
+    }
+}
 /* HPRReducedStateVector() (:3-19) */
 static void hred_default(const double* prm, double* W) {
     (void)prm;
@@ -1626,6 +1821,7 @@ static const model M_MRED = {12, mred_cons, mred_setcons, mred_flux, mred_wave1d
 static const model M_MINT = {13, mint_cons, mint_setcons, mint_flux, mint_wave1d, mint_wave2d, mint_default, mint_source};
 static const model M_HRED = {20, hred_cons, hred_setcons, hred_flux, hred_wave1d, hred_wave2d, hred_default, hred_source};
 static const model M_HINT = {21, hint_cons, hint_setcons, hint_flux, hint_wave1d, hint_wave2d, hint_default, hint_source};
+static const model M_HMPH = {33, hmph_cons, hmph_setcons, hmph_flux, hmph_wave1d, hmph_wave2d, hmph_default, 0};
 
 static const model* model_of(int id) {
     switch (id) {
@@ -1638,13 +1834,14 @@ static const model* model_of(int id) {
         case VO_MHD_INTERMEDIATE: return &M_MINT;
         case VO_HPR_REDUCED: return &M_HRED;
         case VO_HPR_INTERMEDIATE: return &M_HINT;
+        case VO_HPR_MULTIPHYSICS: return &M_HMPH;
         default: return NULL;
     }
 }
 
 int vo_nvar(int id) { const model* m = model_of(id); return m ? m->nv : 0; }
 int vo_nparams(int id) {
-    return id == VO_EULER ? 6 : id == VO_MHD ? 3 : id == VO_HPR ? 20 : (id == VO_EULER_REDUCED || id == VO_EULER_MULTIPHYSICS) ? 4 : (id == VO_MHD_REDUCED || id == VO_MHD_INTERMEDIATE) ? 5 : (id == VO_HPR_REDUCED || id == VO_HPR_INTERMEDIATE) ? 22 : 0;
+    return id == VO_EULER ? 6 : id == VO_MHD ? 3 : id == VO_HPR ? 20 : (id == VO_EULER_REDUCED || id == VO_EULER_MULTIPHYSICS) ? 4 : (id == VO_MHD_REDUCED || id == VO_MHD_INTERMEDIATE) ? 5 : (id == VO_HPR_REDUCED || id == VO_HPR_INTERMEDIATE || id == VO_HPR_MULTIPHYSICS) ? 22 : 0;
 }
 
 /* ------------------------------------------------------------------------------- SLIC building blocks */
@@ -2021,6 +2218,7 @@ static double run(int id, double* planes, int nx, int ny, int dims, double dx, d
             g_reinit_p2 = id == VO_HPR_INTERMEDIATE ? 19 : 7;
             red_reinit(planes, nx, dims == 1 ? 1 : ny);
         }
+        if (id == VO_HPR_MULTIPHYSICS && reinit_freq != 0 && (it % reinit_freq) == 0) hmph_reinit(planes, nx);
     }
     if (steps_out) *steps_out = it;
     return t;
@@ -2070,6 +2268,7 @@ double vo_run_first_order(int id, double* planes, int nx, int ny, double dx, dou
     const model* m = model_of(id);
     if (!m) return -1.0;
     hred_drop_cold_heat_flux(id, planes, (long)nx * ny, prm);
+    hmph_drop_cold_heat_flux(id, planes, (long)nx * ny, prm);
     int dims = ny > 1 ? 2 : 1;
     double tEnd = t_end > 0.0 ? t_end : 1.0e300;
     int limit = max_steps > 0 ? max_steps : 0x7fffffff;
@@ -2113,11 +2312,18 @@ double vo_run_two_material(int id, double* planes, int nx, int ny, double dx, do
 double vo_run_mhd_two_material(int id, double* planes, int nx, int ny, double dx, double cfl, double t_end,
                                 int max_steps, double w, int lim, const double* prm, int bc, int subcycles,
                                 int reinit_freq, int* steps_out) {
-    if (id != VO_MHD_REDUCED && id != VO_MHD_INTERMEDIATE && id != VO_HPR_REDUCED && id != VO_HPR_INTERMEDIATE)
+    if (id != VO_MHD_REDUCED && id != VO_MHD_INTERMEDIATE && id != VO_HPR_REDUCED && id != VO_HPR_INTERMEDIATE &&
+        id != VO_HPR_MULTIPHYSICS)
         return -1.0;
+    if (id == VO_HPR_MULTIPHYSICS && ny > 1) return -1.0;  /* the reference's model is 1D only */
     hred_drop_cold_heat_flux(id, planes, (long)nx * ny, prm);
-    return run(id, planes, nx, ny, ny > 1 ? 2 : 1, dx, cfl, t_end, max_steps, w, lim, prm, bc, subcycles,
-               steps_out, NULL, reinit_freq);
+    hmph_drop_cold_heat_flux(id, planes, (long)nx * ny, prm);
+    double t = run(id, planes, nx, ny, ny > 1 ? 2 : 1, dx, cfl, t_end, max_steps, w, lim, prm, bc, subcycles,
+                   steps_out, NULL, reinit_freq);
+    /* a cold material's J is state (the reinitialisation mixes it in) that computePrimitiveVariableVector does not
+     * return: the returned planes hold 0 there */
+    hmph_drop_cold_heat_flux(id, planes, (long)nx * ny, prm);
+    return t;
 }
 
 /* ------------------------------------------------------------------------- unit-test building blocks */

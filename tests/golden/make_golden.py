@@ -163,9 +163,23 @@ HPR_INTERMEDIATE_CASES = {
         lambda: wl.hpr_intermediate_riemann(20, 20, seed=20, bubble=True),
         dict(dx=1 / 20, cfl=0.8, steps=6, limiter=O.VANLEER, reinit=2, subcycles=0, params=HPR_REDUCED_PRM)),
 }
+# The HPR multiphysics two-material model (model id O.HPR_MULTIPHYSICS, 1D only): the reduced model's problem with a
+# distortion and heat flux per material, through the reference's own solve to t_end, and per step up to its
+# reinitialisation with material 2 cold.
+HPR_MULTIPHYSICS_CASES = {
+    "hprmultiphysics1d_riemann80_solve_t0015_sub2": (
+        lambda: wl.hpr_multiphysics_riemann(80, seed=80, p2_scale=1.2),
+        dict(dx=1 / 80, cfl=0.8, t_end=0.015, steps=0, limiter=O.MINBEE, reinit=0, subcycles=2,
+             params=HPR_REDUCED_PRM)),
+    "hprmultiphysics1d_riemann50_vanleer_cold2_reinit1_2": (
+        lambda: wl.hpr_multiphysics_riemann(50, seed=5, p2_scale=1.1, a2_scale=1.01),
+        dict(dx=1 / 50, cfl=0.8, steps=2, limiter=O.VANLEER, reinit=1, subcycles=0,
+             params=wl.hpr_reduced_params(gamma2=2.0, p_inf2=0.5, thermal=(True, False)))),
+}
 TWO_MATERIAL = {O.EULER_REDUCED: REDUCED_CASES, O.EULER_MULTIPHYSICS: MULTIPHYSICS_CASES,
                 O.MHD_REDUCED: MHD_REDUCED_CASES, O.MHD_INTERMEDIATE: MHD_INTERMEDIATE_CASES,
-                O.HPR_REDUCED: HPR_REDUCED_CASES, O.HPR_INTERMEDIATE: HPR_INTERMEDIATE_CASES}
+                O.HPR_REDUCED: HPR_REDUCED_CASES, O.HPR_INTERMEDIATE: HPR_INTERMEDIATE_CASES,
+                O.HPR_MULTIPHYSICS: HPR_MULTIPHYSICS_CASES}
 
 
 def make_two_material(name):

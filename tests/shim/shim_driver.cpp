@@ -7,8 +7,8 @@
 // (6 x 150), HPR GodunovRomenski plastic solve (17 x 60), reduced two-material solve (7 x 120), multiphysics
 // two-material solve (8 x 100), MHD reduced two-material solve2D (11 x 24 x 24), MHD intermediate two-material solve
 // (12 x 80), the 2D maximum wave speed of an interior-only cold gas (1), whether solve2D refused a single row (1),
-// HPR reduced two-material solve2D (19 x 16 x 16), HPR intermediate two-material solve (20 x 60), then the number of
-// 2D steps the per-sweep loop took.
+// HPR reduced two-material solve2D (19 x 16 x 16), HPR intermediate two-material solve (20 x 60), HPR multiphysics
+// two-material solve (32 x 60), then the number of 2D steps the per-sweep loop took.
 #include <cmath>
 #include <cstdio>
 #include <stdexcept>
@@ -22,6 +22,7 @@
 #include "Solvers/hprsecondordersolver.h"
 #include "HPR/Multiphysics/hprreducedstatevector.h"
 #include "HPR/Multiphysics/hprintermediatestatevector.h"
+#include "HPR/Multiphysics/hprmultiphysicsstatevector.h"
 
 using std::vector;
 
@@ -276,6 +277,23 @@ int main(int argc, char** argv) {
         vector<HPRIntermediateStateVector> out = HPRSecondOrderSolver::solve(cells, 1.0 / n, 0.8, 0.02, 0.0, 2, 1, 4, hm1, hm2);
         vector<double> v;
         for (int k = 0; k < 20; k++)
+            for (auto& c : out) v.push_back(c.computePrimitiveVariableVector(hm1, hm2)[k]);
+        put(f, v);
+    }
+    // 15) HPRSecondOrderSolver::solve of the HPR multiphysics two-material model (1D): a distortion and a heat flux per
+    //     material, two sub-cycles (empty in the reference's loop for this model), to t = 0.015
+    {
+        int n = 60;
+        vector<vector<double> > A2 = {{1.01, 0.0, 0.0}, {0.0, 1.0, 0.0}, {0.0, 0.0, 0.99}};
+        vector<HPRMultiphysicsStateVector> cells(n);
+        for (int i = 0; i < n; i++)
+            cells[i] = i <= 0.5 * n ? HPRMultiphysicsStateVector(0.999, 0.2, 0.0, 0.0, 1.0, 1.0, eye, 0.02, 0.0, 0.0, 0.5,
+                                                                 1.1, A2, 0.01, 0.0, 0.0)
+                                    : HPRMultiphysicsStateVector(0.001, -0.1, 0.0, 0.0, 0.8, 0.3, eye, 0.0, 0.01, 0.0,
+                                                                 0.25, 0.33, A2, 0.0, 0.005, 0.0);
+        vector<HPRMultiphysicsStateVector> out = HPRSecondOrderSolver::solve(cells, 1.0 / n, 0.8, 0.015, 0.0, 2, 2, 0, hm1, hm2);
+        vector<double> v;
+        for (int k = 0; k < 32; k++)
             for (auto& c : out) v.push_back(c.computePrimitiveVariableVector(hm1, hm2)[k]);
         put(f, v);
     }

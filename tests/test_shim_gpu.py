@@ -162,5 +162,19 @@ def test_shim_driver_matches_oracle(gpu, oracle_lib, tmp_path):
     O.run_two_material(O.HPR_INTERMEDIATE, ref, 1 / n, 0.8, t_end=0.02, limiter=2, params=hprm, subcycles=1, reinit=4)
     assert _rel(got, ref) <= 1e-12
 
+    # 15) HPRSecondOrderSolver::solve of the HPR multiphysics two-material model to t = 0.015 (pow(alpha, 1/3) in the
+    #     conserved distortion: 1e-12 of each plane's largest magnitude)
+    got = take((32, 60))
+    n = 60
+    ref = np.zeros((32, n))
+    I3 = [1.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0, 1.0]
+    A2 = [1.01, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0, 0.99]
+    for i in range(n):
+        ref[:, i] = ([0.999, 0.2, 0.0, 0.0, 1.0, 1.0, *I3, 0.02, 0.0, 0.0, 0.5, 1.1, *A2, 0.01, 0.0, 0.0] if i <= 0.5 * n
+                     else [0.001, -0.1, 0.0, 0.0, 0.8, 0.3, *I3, 0.0, 0.01, 0.0, 0.25, 0.33, *A2, 0.0, 0.005, 0.0])
+    O.run_two_material(O.HPR_MULTIPHYSICS, ref, 1 / n, 0.8, t_end=0.015, limiter=2, params=hprm, subcycles=2)
+    d = np.abs(got - ref).max(axis=1) / np.maximum(np.abs(ref).max(axis=1), 1e-300)
+    assert np.isfinite(got).all() and d.max() <= 1e-12
+
     assert take((1,))[0] == 6
     assert off == data.size

@@ -340,7 +340,9 @@ struct HPRModel {
     // MatrixAlgebra::computeLargestEigenvalue (Mathematics/matrixalgebra.cpp:182-199).  Only the entries
     // d sigma / d A [d][i][j][d] of HPREquationOfState::computeShearStressTensorDerivativeDistortionTensor
     // (HPR/hprequationofstate.cpp:83-113) enter; the i == d entries receive its += update twice.
-    __device__ static double acoustic_speed(const double* W, int d, const P& q) {
+    // diag: the first block reads dsigma/dA[d][i][i][d] for every column j, as the HPR multiphysics model's material-2
+    // tensor does (HPR/Multiphysics/hprmultiphysicsacoustictensor.cpp:61)
+    __device__ static double acoustic_speed(const double* W, int d, const P& q, bool diag = false) {
         double rho = W[0], p = W[1];
         M3 A = load(W + 2);
         M3 G = tmul(A, A), D = dev(G), AD = mul(A, D);
@@ -359,14 +361,15 @@ struct HPRModel {
 #pragma unroll
         for (int i = 0; i < 3; i++)
 #pragma unroll
-            for (int j = 0; j < 3; j++) {
+            for (int j0 = 0; j0 < 3; j0++) {
+                const int j = diag ? i : j0;
                 double s1 = 0.0 + (G.m[d][i] * A.m[j][d]);
                 double s2 = 0.0 + (G.m[d][d] * A.m[j][i]);
                 double pp = 0.0 + (G.m[d][i] * A.m[j][d]);
                 double t = (s1 + s2) + (-1.0 * ((2.0 / 3.0) * pp));
                 t += AD.m[j][i];
                 if (i == d) t += AD.m[j][d];
-                c1[i][2 + j] = -ir * ((-(rho * cs2)) * t);
+                c1[i][2 + j0] = -ir * ((-(rho * cs2)) * t);
             }
         M3 dd = dEdA(A, q);
         M3 Pm = tmul(A, dd);
@@ -650,6 +653,183 @@ struct HPRReducedF64 {
     // The interface pressure of this model goes below zero within steps of runs the reference completes (a stiffened
     // material, the volume-fraction mixing of both materials' pressures at the mixture density), so the bad-state
     // check asks for finite values and positive densities only.
+    __device__ static bool positive_pressure(const P&) { return false; }
+};
+
+// ---------------------------------------------------------------------------- HPR multiphysics two-material
+// HPRMultiphysicsStateVector (HPR/Multiphysics/hprmultiphysicsstatevector.cpp; 1D only in the reference) for two
+// StiffenedGas materials: each material carries its own density, pressure, distortion and heat flux, the velocity is
+// shared.  W = (alpha1, u, v, w, rho1, p1, A1 (9), J1 (3), rho2, p2, A2 (9), J2 (3)) (:204-249),
+// U = (rho, rho alpha1, rho u (3), then per material k at 5 + 14 k: alpha rho, alpha rho E, alpha^(1/3) A (9),
+// alpha rho J (3)) (:251-317).  A material's J is carried when that material is thermal.  pow(alpha, 1/3) scales the
+// distortion: CUDA's pow and glibc's may differ in the last place, so results agree with the reference to round-off
+// rather than bitwise.  Parameters as for HPRReducedF64.
+struct HPRMultiphysicsF64 {
+    static constexpr int NW = 32;
+    static constexpr int NU = 33;
+    static constexpr bool HAS_Y = false;
+    static constexpr bool HAS_SOURCE = false;
+    using H = HPRModel<false>;
+    using M3 = H::M3;
+    using P = HPRReducedF64::P;
+    __device__ static P params(const double* prm, double ch) { return HPRReducedF64::params(prm, ch); }
+    __device__ static double clamp_alpha(double a) { return HPRReducedF64::clamp_alpha(a); }
+    __device__ static const H::P& mat(const P& q, int k) { return k == 0 ? q.m1 : q.m2; }
+
+    // computeConservedVariableVector (:251-317)
+    __device__ static void cons(const double* W, const P& q, double* U) {
+        const double a1 = clamp_alpha(W[0]), a2 = 1.0 - a1;
+        const double u = W[1], v = W[2], w = W[3];
+        const double rho = (a1 * W[4]) + (a2 * W[18]);
+#pragma unroll
+        for (int i = 0; i < NU; i++) U[i] = 0.0;
+        U[0] = rho;
+        U[1] = rho * a1;
+        U[2] = rho * u;
+        U[3] = rho * v;
+        U[4] = rho * w;
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const H::P& m = mat(q, k);
+            const double a = k == 0 ? a1 : a2;
+            const double* wk = W + 4 + 14 * k;  // rho, p, A (9), J (3)
+            double* uk = U + 5 + 14 * k;        // a rho, a rho E, a^(1/3) A (9), a rho J (3)
+            uk[0] = a * wk[0];
+#pragma unroll
+            for (int i = 0; i < 9; i++) uk[2 + i] = pow(a, (1.0 / 3.0)) * wk[2 + i];
+            if (m.thermal)
+#pragma unroll
+                for (int i = 0; i < 3; i++) uk[11 + i] = a * (wk[0] * wk[11 + i]);
+            const M3 A = H::load(wk + 2);
+            uk[1] = a * (wk[0] * H::total_energy(wk[0], wk[1], u, v, w, A, wk[11], wk[12], wk[13], m));
+        }
+    }
+    // setConservedVariableVector (:141-202); material k's J kept when it is not thermal
+    __device__ static void setcons(const double* U, const P& q, double* W) {
+        const double rho = U[0];
+        const double a1 = clamp_alpha(U[1] / rho), a2 = 1.0 - a1;
+        W[1] = U[2] / rho;
+        W[2] = U[3] / rho;
+        W[3] = U[4] / rho;
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const H::P& m = mat(q, k);
+            const double a = k == 0 ? a1 : a2;
+            double* wk = W + 4 + 14 * k;
+            const double* uk = U + 5 + 14 * k;
+            wk[0] = uk[0] / a;
+#pragma unroll
+            for (int i = 0; i < 9; i++) wk[2 + i] = uk[2 + i] / pow(a, (1.0 / 3.0));
+            if (m.thermal)
+#pragma unroll
+                for (int i = 0; i < 3; i++) wk[11 + i] = uk[11 + i] / (a * wk[0]);
+            const double E = uk[1] / (a * wk[0]);
+            const M3 A = H::load(wk + 2);
+            wk[1] = H::pressure_of(wk[0], E, W[1], W[2], W[3], A, wk[11], wk[12], wk[13], m);
+        }
+        W[0] = a1;
+    }
+    // computeXFluxVector (:319-463); the model has no Y flux
+    template <int AXIS>
+    __device__ static void flux(const double* U, const P& q, double* F) {
+        static_assert(AXIS == 0, "the HPR multiphysics model is 1D");
+        const double rho = U[0];
+        const double a1 = clamp_alpha(U[1] / rho), a2 = 1.0 - a1;
+        const double u = U[2] / rho, v = U[3] / rho, w = U[4] / rho;
+#pragma unroll
+        for (int i = 0; i < NU; i++) F[i] = 0.0;
+        double pk[2], sig0[2][3];
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const H::P& m = mat(q, k);
+            const double a = k == 0 ? a1 : a2;
+            const double* uk = U + 5 + 14 * k;
+            const double r = uk[0] / a;
+            M3 A;
+#pragma unroll
+            for (int i = 0; i < 3; i++)
+#pragma unroll
+                for (int j = 0; j < 3; j++) A.m[i][j] = uk[2 + (i * 3) + j] / pow(a, (1.0 / 3.0));
+            const double jx = uk[11] / (a * r), jy = uk[12] / (a * r), jz = uk[13] / (a * r);
+            const double E = uk[1] / (a * r);
+            const double p = H::pressure_of(r, E, u, v, w, A, jx, jy, jz, m);
+            pk[k] = p;
+            // HPREquationOfState::computeShearStressTensor (HPR/hprequationofstate.cpp:76-81), row 0
+            const M3 Pm = H::tmul(A, H::dEdA(A, m));
+#pragma unroll
+            for (int i = 0; i < 3; i++) sig0[k][i] = (-r) * Pm.m[0][i];
+            double* fk = F + 5 + 14 * k;
+            fk[0] = a * (r * u);
+            fk[1] = a * ((r * (u * E)) + (p * u));
+            fk[1] -= a * (((0.0 + (sig0[k][0] * u)) + (sig0[k][1] * v)) + (sig0[k][2] * w));
+#pragma unroll
+            for (int i = 0; i < 3; i++)
+                fk[2 + (i * 3)] = pow(a, (1.0 / 3.0)) * (((0.0 + (A.m[i][0] * u)) + (A.m[i][1] * v)) + (A.m[i][2] * w));
+            if (m.thermal) {
+                const double T = H::mg_temperature(r, p, m);
+                fk[1] += a * (T * ((m.alpha * m.alpha) * jx));
+                fk[11] = a * ((r * (u * jx)) + T);
+                fk[12] = a * (r * (u * jy));
+                fk[13] = a * (r * (u * jz));
+            }
+        }
+        F[0] = rho * u;
+        F[1] = rho * (u * a1);
+        F[2] = (rho * (u * u)) + ((a1 * pk[0]) + (a2 * pk[1]));
+        F[3] = rho * (u * v);
+        F[4] = rho * (u * w);
+#pragma unroll
+        for (int i = 0; i < 3; i++) F[2 + i] -= (a1 * sig0[0][i]) + (a2 * sig0[1][i]);
+    }
+    __device__ static void source(const double*, const P&, double* S) {
+#pragma unroll
+        for (int i = 0; i < NU; i++) S[i] = 0.0;
+    }
+    // HPRMultiphysicsAcousticTensor::computeMaximumWaveSpeed (HPR/Multiphysics/hprmultiphysicsacoustictensor.cpp:
+    // 177-184): each material's acoustic speed at its own state; material 2's with the diagonal quirk (:61)
+    __device__ static double speed(const double* W, int d, const H::P& qk, int k) {
+        double Wk[17];
+        const double* wk = W + 4 + 14 * k;
+        Wk[0] = wk[0];
+        Wk[1] = wk[1];
+#pragma unroll
+        for (int i = 0; i < 9; i++) Wk[2 + i] = wk[2 + i];
+        Wk[11] = W[1];
+        Wk[12] = W[2];
+        Wk[13] = W[3];
+#pragma unroll
+        for (int i = 0; i < 3; i++) Wk[14 + i] = wk[11 + i];
+        return H::acoustic_speed(Wk, d, qk, k == 1);
+    }
+    // HPRSolvers::computeMaximumWaveSpeed of the multiphysics model (Solvers/hprsolvers.cpp:305-322)
+    __device__ static double wave(const double* W, const P& q, int) {
+        return fabs(W[1]) + std_max(speed(W, 0, q.m1, 0), speed(W, 0, q.m2, 1));
+    }
+    // HPRMultiphysicsStateVector() (:3-26)
+    __device__ static void default_state(double* W) {
+#pragma unroll
+        for (int i = 0; i < NW; i++) W[i] = 0.0;
+        W[0] = 0.999;
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            W[4 + 14 * k] = 1.0;
+            W[5 + 14 * k] = 1.0 / 1.4;
+            W[6 + 14 * k] = 1.0;
+            W[10 + 14 * k] = 1.0;
+            W[14 + 14 * k] = 1.0;
+        }
+    }
+    // setConservedVariableVector leaves a cold material's J alone (:167-172, :191-196)
+    __device__ static void keep_cold(const SweepArgs& a, long idx, const P& q, double* W) {
+        if (!q.m1.thermal)
+            for (int v = 15; v < 18; v++) W[v] = a.in[v * a.plane + idx];
+        if (!q.m2.thermal)
+            for (int v = 29; v < 32; v++) W[v] = a.in[v * a.plane + idx];
+    }
+    // the smaller material density (bad-state check); the mixture pressure, which as in the other HPR two-material
+    // models is not required positive
+    __device__ static double density(const double* W) { return W[4] < W[18] ? W[4] : W[18]; }
+    __device__ static double pressure(const double* W) { return (clamp_alpha(W[0]) * W[5]) + ((1.0 - clamp_alpha(W[0])) * W[19]); }
     __device__ static bool positive_pressure(const P&) { return false; }
 };
 

@@ -46,22 +46,62 @@ struct ReinitHPRIntermediate {  // alpha1, A (9), u, v, w, Jx, Jy, Jz, rho1, p1,
     static constexpr int R1 = 16, R2 = 18, P1 = 17, P2 = 19;
     static constexpr bool PRESSURE = true;
 };
+// The HPR multiphysics model (1D; Solvers/multiphysicssolvers.cpp:807-839): relaxTotalDensity, relaxTotalPressure,
+// relaxTotalDistortionTensor (pow(alpha_k, 1/3)-weighted) and relaxTotal{X,Y,Z}ThermalImpulse
+// (HPR/Multiphysics/hprmultiphysicsstatevector.cpp:614-704), each with the cell's own alpha, then the volume fraction.
+// Planes: alpha1, u, v, w, rho1, p1, A1 (9), J1 (3), rho2, p2, A2 (9), J2 (3).
+struct ReinitHPRMultiphysics {
+    __device__ static void reset(const SweepArgs& a, long idx, double alpha) {
+        double* o = a.out;
+        const long n = a.plane;
+        const double a1 = o[idx], a2 = 1.0 - a1;
+        const double rho = (a1 * o[4 * n + idx]) + (a2 * o[18 * n + idx]);
+        o[4 * n + idx] = rho;
+        o[18 * n + idx] = rho;
+        const double p = (a1 * o[5 * n + idx]) + (a2 * o[19 * n + idx]);
+        o[5 * n + idx] = p;
+        o[19 * n + idx] = p;
+        for (int e = 0; e < 9; e++) {
+            const double A = (pow(a1, (1.0 / 3.0)) * o[(6 + e) * n + idx]) + (pow(a2, (1.0 / 3.0)) * o[(20 + e) * n + idx]);
+            o[(6 + e) * n + idx] = A;
+            o[(20 + e) * n + idx] = A;
+        }
+        for (int e = 0; e < 3; e++) {
+            const double J = (a1 * o[(15 + e) * n + idx]) + (a2 * o[(29 + e) * n + idx]);
+            o[(15 + e) * n + idx] = J;
+            o[(29 + e) * n + idx] = J;
+        }
+        o[idx] = alpha;
+    }
+};
+template <class L, class = void>
+struct custom_reset {
+    static constexpr bool value = false;
+};
+template <class L>
+struct custom_reset<L, decltype((void)&L::reset)> {
+    static constexpr bool value = true;
+};
 
 // relaxTotalDensity (Euler/Multiphysics/eulerreducedstatevector.cpp:281-287, eulermultiphysicsstatevector.cpp:308-314,
 // MHD/Multiphysics/mhdreducedstatevector.cpp's relaxTotalDensity), for the multiphysics model relaxTotalPressure
 // (:316-329), then the cell's volume fraction
 template <class L>
 __device__ inline void reduced_reset_cell(const SweepArgs& a, long idx, double alpha) {
-    const double a1 = a.out[idx];
-    const double rho = (a1 * a.out[L::R1 * a.plane + idx]) + ((1.0 - a1) * a.out[L::R2 * a.plane + idx]);
-    a.out[L::R1 * a.plane + idx] = rho;
-    a.out[L::R2 * a.plane + idx] = rho;
-    if constexpr (L::PRESSURE) {
-        const double p = (a1 * a.out[L::P1 * a.plane + idx]) + ((1.0 - a1) * a.out[L::P2 * a.plane + idx]);
-        a.out[L::P1 * a.plane + idx] = p;
-        a.out[L::P2 * a.plane + idx] = p;
+    if constexpr (custom_reset<L>::value) {
+        L::reset(a, idx, alpha);
+    } else {
+        const double a1 = a.out[idx];
+        const double rho = (a1 * a.out[L::R1 * a.plane + idx]) + ((1.0 - a1) * a.out[L::R2 * a.plane + idx]);
+        a.out[L::R1 * a.plane + idx] = rho;
+        a.out[L::R2 * a.plane + idx] = rho;
+        if constexpr (L::PRESSURE) {
+            const double p = (a1 * a.out[L::P1 * a.plane + idx]) + ((1.0 - a1) * a.out[L::P2 * a.plane + idx]);
+            a.out[L::P1 * a.plane + idx] = p;
+            a.out[L::P2 * a.plane + idx] = p;
+        }
+        a.out[idx] = alpha;
     }
-    a.out[idx] = alpha;
 }
 
 __device__ inline bool reduced_reinit_due(const SweepArgs& a) {

@@ -65,7 +65,7 @@ cudaError_t forcing_impl(const SweepArgs& a, int subcycles, cudaStream_t st) {
 
 template <class M>
 cudaError_t force1_x(const SweepArgs& a, cudaStream_t st) {
-    constexpr int P = 128;
+    constexpr int P = M::NU > 21 ? 64 : 128;  // the two shared tiles within the 48 KB static limit
     force1_x_kernel<M, P><<<dim3((a.nx + P - 1) / P, a.ny), P, 0, st>>>(a);
     return cudaGetLastError();
 }
@@ -122,6 +122,7 @@ constexpr Ops make_ops() {
                : std::is_same<M, MHDIntermediateF64>::value   ? &mhd_intermediate_reinit_fp64
                : std::is_same<M, HPRReducedF64>::value        ? &hpr_reduced_reinit_fp64
                : std::is_same<M, HPRIntermediateF64>::value   ? &hpr_intermediate_reinit_fp64
+               : std::is_same<M, HPRMultiphysicsF64>::value   ? &hpr_multiphysics_reinit_fp64
                                                               : nullptr};
 }
 

@@ -137,7 +137,8 @@ __device__ __forceinline__ void store_w(const SweepArgs& a, long idx, const doub
 // cell object in place (Solvers/firstordersolver.cpp:428-433): HPR's J (planes 14-16) when the material is not
 // thermal (HPR/hprstatevector.cpp:78-103), and the HPR two-material models' J when neither material is (planes 14-16
 // of the reduced model, HPR/Multiphysics/hprreducedstatevector.cpp:111-152; 13-15 of the intermediate model,
-// hprintermediatestatevector.cpp:112-159).  Models with heat flux name its first plane in J_PLANE.
+// hprintermediatestatevector.cpp:112-159).  Models with heat flux name its first plane in J_PLANE; a model whose
+// materials keep their heat fluxes separately (the HPR multiphysics model) has its own keep_cold.
 template <class M, class = void>
 struct heat_flux_plane {
     static constexpr int value = -1;
@@ -146,13 +147,25 @@ template <class M>
 struct heat_flux_plane<M, decltype((void)M::J_PLANE)> {
     static constexpr int value = M::J_PLANE;
 };
+template <class M, class = void>
+struct cold_fields {
+    __device__ static void keep(const SweepArgs& a, long idx, const typename M::P& q, double* W) {
+        constexpr int j0 = heat_flux_plane<M>::value;
+        if constexpr (j0 >= 0) {
+            if (!q.thermal)
+                for (int v = j0; v < j0 + 3; v++) W[v] = a.in[v * a.plane + idx];
+        }
+    }
+};
+template <class M>
+struct cold_fields<M, decltype((void)&M::keep_cold)> {
+    __device__ static void keep(const SweepArgs& a, long idx, const typename M::P& q, double* W) {
+        M::keep_cold(a, idx, q, W);
+    }
+};
 template <class M>
 __device__ __forceinline__ void keep_fields(const SweepArgs& a, long idx, const typename M::P& q, double* W) {
-    constexpr int j0 = heat_flux_plane<M>::value;
-    if constexpr (j0 >= 0) {
-        if (!q.thermal)
-            for (int v = j0; v < j0 + 3; v++) W[v] = a.in[v * a.plane + idx];
-    }
+    cold_fields<M>::keep(a, idx, q, W);
 }
 
 // Whether a state of model M must have a positive pressure: models with a positive_pressure(q) member decide

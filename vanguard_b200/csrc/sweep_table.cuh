@@ -57,12 +57,13 @@ struct pair_sweeps<M, decltype((void)M::PAIR_X)> {
 };
 
 // Models with more than 9 conserved components (HPR, 17) use shorter X segments so that the three FP64
-// shared-memory tiles stay inside the 48 KB static limit (kind 1).  The PAIR_X models (two rows per thread in the
-// X sweep) add the TMA-staged X shapes for the Euler states of up to four planes (kind 2); other PAIR_X models (MHD)
-// keep the plain two-row shapes (kind 3).
+// shared-memory tiles stay inside the 48 KB static limit (kind 1); models with more than 21 (the HPR multiphysics
+// model, 33) shorter still (kind 4).  The PAIR_X models (two rows per thread in the X sweep) add the TMA-staged X
+// shapes for the Euler states of up to four planes (kind 2); other PAIR_X models (MHD) keep the plain two-row shapes
+// (kind 3).
 template <class M>
 constexpr int tile_kind() {
-    return (M::NU > 9) ? 1 : pair_sweeps<M>::value ? (M::NW <= 4 ? 2 : 3) : 0;
+    return (M::NU > 21) ? 4 : (M::NU > 9) ? 1 : pair_sweeps<M>::value ? (M::NW <= 4 ? 2 : 3) : 0;
 }
 
 template <class K, class M, int KIND = tile_kind<M>()>
@@ -73,6 +74,18 @@ struct SweepTable<K, M, 1> {
     static constexpr SweepFn x[kNumXCfg] = {
         launch_x<K, M, 64, 1, 1>, launch_x<K, M, 32, 2, 1>, launch_x<K, M, 96, 1, 1>,
         launch_x<K, M, 64, 1, 2>, launch_x<K, M, 32, 1, 1>,
+    };
+    static constexpr SweepFn y[kNumYCfg] = {
+        launch_y<K, M, 64, 64, 1>, launch_y<K, M, 64, 32, 1>, launch_y<K, M, 32, 32, 1>,
+        launch_y<K, M, 32, 64, 1>, launch_y<K, M, 128, 32, 1>, launch_y<K, M, 64, 16, 1>,
+    };
+};
+
+template <class K, class M>
+struct SweepTable<K, M, 4> {
+    static constexpr SweepFn x[kNumXCfg] = {
+        launch_x<K, M, 32, 1, 1>, launch_x<K, M, 40, 1, 1>, launch_x<K, M, 48, 1, 1>,
+        launch_x<K, M, 56, 1, 1>, launch_x<K, M, 32, 1, 2>,
     };
     static constexpr SweepFn y[kNumYCfg] = {
         launch_y<K, M, 64, 64, 1>, launch_y<K, M, 64, 32, 1>, launch_y<K, M, 32, 32, 1>,
@@ -122,13 +135,16 @@ inline const char* x_cfg_name(int i, int kind = 0) {
     static const char* nb[kNumXCfg] = {"P64xL1", "P32xL2", "P96xL1", "P64xL1/min2", "P32xL1"};
     static const char* np[kNumXCfg] = {"P128x2", "TMA P128x2/min7", "TMA P128x2/min8", "P128x2/min6", "P128x2/min8"};
     static const char* nq[kNumXCfg] = {"P128x2", "P64xL2x2", "P128x2/min4", "P128x2/min6", "P128x2/min8"};
-    return (i >= 0 && i < kNumXCfg) ? (kind == 1 ? nb[i] : kind == 2 ? np[i] : kind == 3 ? nq[i] : n[i]) : "?";
+    static const char* nw[kNumXCfg] = {"P32xL1", "P40xL1", "P48xL1", "P56xL1", "P32xL1/min2"};
+    return (i >= 0 && i < kNumXCfg)
+               ? (kind == 1 ? nb[i] : kind == 2 ? np[i] : kind == 3 ? nq[i] : kind == 4 ? nw[i] : n[i])
+               : "?";
 }
 inline const char* y_cfg_name(int i, int kind = 0) {
     static const char* n[kNumYCfg] = {"TX64xTY64", "TX64xTY32", "TX64xTY64/min12", "TX64xTY64/min16",
                                       "TX128xTY32/min5", "TX32xTY64"};
     static const char* nb[kNumYCfg] = {"TX64xTY64", "TX64xTY32", "TX32xTY32", "TX32xTY64", "TX128xTY32", "TX64xTY16"};
-    return (i >= 0 && i < kNumYCfg) ? (kind == 1 ? nb[i] : n[i]) : "?";
+    return (i >= 0 && i < kNumYCfg) ? ((kind == 1 || kind == 4) ? nb[i] : n[i]) : "?";
 }
 
 }  // namespace vg

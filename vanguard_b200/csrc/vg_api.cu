@@ -47,11 +47,11 @@ int ref_nvar(int model) {
     return model == VG_MODEL_EULER ? 6 : model == VG_MODEL_MHD ? 9 : model == VG_MODEL_HPR ? 17 : model == VG_MODEL_EULER_REDUCED ? 7
            : model == VG_MODEL_EULER_MULTIPHYSICS ? 8 : model == VG_MODEL_MHD_REDUCED ? 11
            : model == VG_MODEL_MHD_INTERMEDIATE ? 12 : model == VG_MODEL_HPR_REDUCED ? 19
-           : model == VG_MODEL_HPR_INTERMEDIATE ? 20 : 0;
+           : model == VG_MODEL_HPR_INTERMEDIATE ? 20 : model == VG_MODEL_HPR_MULTIPHYSICS ? 32 : 0;
 }
 
 // Reference plane carried in device plane k, per variant.
-const int kPlanes[vg::V_COUNT][20] = {
+const int kPlanes[vg::V_COUNT][32] = {
     {0, 1, 4},                      // V_EULER1: rho, u, p
     {0, 1, 2, 4},                   // V_EULER2: rho, u, v, p
     {0, 1, 2, 4, 5, 6, 8},          // V_MHD7:   rho, u, v, p, Bx, By, psi
@@ -64,6 +64,8 @@ const int kPlanes[vg::V_COUNT][20] = {
     {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11},  // V_MINT12: every plane
     {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17, 18},  // V_HRED19: every plane
     {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17, 18, 19},  // V_HINT20: every plane
+    {0,  1,  2,  3,  4,  5,  6,  7,  8,  9,  10, 11, 12, 13, 14, 15,
+     16, 17, 18, 19, 20, 21, 22, 23, 24, 25, 26, 27, 28, 29, 30, 31},  // V_HMPH32: every plane
 };
 
 }  // namespace
@@ -466,7 +468,8 @@ vg_status vg_create(const vg_grid_desc* desc, vg_solver** out) {
     if (desc->model != VG_MODEL_EULER && desc->model != VG_MODEL_MHD && desc->model != VG_MODEL_HPR &&
         desc->model != VG_MODEL_EULER_REDUCED && desc->model != VG_MODEL_EULER_MULTIPHYSICS &&
         desc->model != VG_MODEL_MHD_REDUCED && desc->model != VG_MODEL_MHD_INTERMEDIATE &&
-        desc->model != VG_MODEL_HPR_REDUCED && desc->model != VG_MODEL_HPR_INTERMEDIATE)
+        desc->model != VG_MODEL_HPR_REDUCED && desc->model != VG_MODEL_HPR_INTERMEDIATE &&
+        desc->model != VG_MODEL_HPR_MULTIPHYSICS)
         return fail(VG_EUNSUPPORTED, "model not available in this build");
     if (desc->nx < 2 || desc->ny < 1 || (desc->ny > 1 && desc->ny < 2))
         return fail(VG_EINVAL, "grid needs at least 2 cells along every swept axis");
@@ -479,8 +482,11 @@ vg_status vg_create(const vg_grid_desc* desc, vg_solver** out) {
                                      "energy is not stable under FP32 flux values)");
     if (desc->precision == VG_MIXED && (desc->model == VG_MODEL_MHD_REDUCED || desc->model == VG_MODEL_MHD_INTERMEDIATE))
         return fail(VG_EUNSUPPORTED, "the MHD two-material models run in VG_FP64 only");
-    if (desc->precision == VG_MIXED && (desc->model == VG_MODEL_HPR_REDUCED || desc->model == VG_MODEL_HPR_INTERMEDIATE))
+    if (desc->precision == VG_MIXED && (desc->model == VG_MODEL_HPR_REDUCED || desc->model == VG_MODEL_HPR_INTERMEDIATE ||
+                                        desc->model == VG_MODEL_HPR_MULTIPHYSICS))
         return fail(VG_EUNSUPPORTED, "the HPR two-material models run in VG_FP64 only");
+    if (desc->model == VG_MODEL_HPR_MULTIPHYSICS && desc->ny != 1)
+        return fail(VG_EUNSUPPORTED, "the HPR multiphysics two-material model is 1D (ny = 1), as the reference's is");
     if (desc->model == VG_MODEL_HPR) {
         const double eos = desc->params[12];
         if (eos != 0.0 && eos != 1.0 && eos != 2.0)
@@ -495,7 +501,7 @@ vg_status vg_create(const vg_grid_desc* desc, vg_solver** out) {
     s->max_nw = desc->model == VG_MODEL_EULER ? 4 : desc->model == VG_MODEL_MHD ? 9 : desc->model == VG_MODEL_EULER_REDUCED ? 6
                 : desc->model == VG_MODEL_EULER_MULTIPHYSICS ? 7 : desc->model == VG_MODEL_MHD_REDUCED ? 11
                 : desc->model == VG_MODEL_MHD_INTERMEDIATE ? 12 : desc->model == VG_MODEL_HPR_REDUCED ? 19
-                : desc->model == VG_MODEL_HPR_INTERMEDIATE ? 20 : 17;
+                : desc->model == VG_MODEL_HPR_INTERMEDIATE ? 20 : desc->model == VG_MODEL_HPR_MULTIPHYSICS ? 32 : 17;
     s->pitch = ((long)desc->nx + 31) / 32 * 32;  // 256-byte aligned rows
     s->plane = s->pitch * desc->ny;
     s->floor5 = std::pow(10.0, -5.0);  // SlopeLimiters::computeSlopeVector's floor (Solvers/slopelimiters.cpp:232-239)
@@ -573,6 +579,8 @@ vg_status vg_upload_primitive(vg_solver* s, const double* planes, int is_device,
         variant = vg::V_HRED19;
     } else if (model == VG_MODEL_HPR_INTERMEDIATE) {
         variant = vg::V_HINT20;
+    } else if (model == VG_MODEL_HPR_MULTIPHYSICS) {
+        variant = vg::V_HMPH32;
     } else if (model == VG_MODEL_HPR) {
         // a solid equation of state or plasticity selects the instantiation that carries them
         variant = (s->d.params[12] != 0.0 || s->d.params[17] != 0.0) ? vg::V_HPR17S : vg::V_HPR17;
@@ -605,6 +613,11 @@ vg_status vg_upload_primitive(vg_solver* s, const double* planes, int is_device,
         s->d.params[21] == 0.0)
         e = cudaMemsetAsync(s->buf[0] + (variant == vg::V_HRED19 ? 14 : 13) * s->plane, 0, sizeof(double) * 3 * s->plane,
                             st);
+    // HPRMultiphysicsStateVector::setPrimitiveVariableVector (hprmultiphysicsstatevector.cpp:98-139) takes each
+    // material's J only when that material is thermal
+    for (int k = 0; k < 2 && variant == vg::V_HMPH32; k++)
+        if (e == cudaSuccess && s->d.params[11 * k + 10] == 0.0)
+            e = cudaMemsetAsync(s->buf[0] + (15 + 14 * k) * s->plane, 0, sizeof(double) * 3 * s->plane, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(&s->ctrl->err, 0, sizeof(unsigned), st);  // a fresh state: no error yet
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (checker.joinable()) checker.join();
@@ -647,6 +660,23 @@ vg_status vg_download_primitive(vg_solver* s, double* planes, int is_device, voi
         }
     }
     VG_CUDA(cudaStreamSynchronize(st));
+    // HPRMultiphysicsStateVector::computePrimitiveVariableVector (hprmultiphysicsstatevector.cpp:204-249) returns a
+    // cold material's J as 0; the device state keeps the J that the reinitialisation mixes in, as the reference's
+    // cells do
+    if (s->variant == vg::V_HMPH32) {
+        for (int k = 0; k < 2; k++) {
+            if (s->d.params[11 * k + 10] != 0.0) continue;
+            for (int r = 15 + 14 * k; r < 18 + 14 * k; r++) {
+                if (is_device) {
+                    vg::fill_plane_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(planes + (long)r * n, n, 0.0);
+                    VG_CUDA(cudaGetLastError());
+                } else {
+                    vg::host::fill_plane(planes + (long)r * n, 0.0, n);
+                }
+            }
+        }
+        VG_CUDA(cudaStreamSynchronize(st));
+    }
     // The reference recovers every primitive of a cell from its conserved vector (setConservedVariableVector), so
     // once a cell's state is non-finite its w = (rho w) / rho and lambda = (rho lambda) / rho (MHD: w, Bz) are NaN
     // as well; the constants above hold only where the carried state is finite.
@@ -668,7 +698,9 @@ vg_status vg_run(vg_solver* s, const vg_run_config* cfg, int* steps_taken, doubl
     if (!(cfg->dx > 0.0) || !(cfg->cfl > 0.0)) return fail(VG_EINVAL, "dx and cfl must be positive");
     if (cfg->max_steps <= 0 && !(cfg->t_end > 0.0)) return fail(VG_EINVAL, "need t_end > 0 or max_steps > 0");
     if (cfg->subcycles < 0) return fail(VG_EINVAL, "subcycles must be >= 0");
-    if (cfg->subcycles > 0 && !s->ops->forcing)
+    // HPRSecondOrderSolver::solve of the HPR multiphysics model takes subcyclingIterations and runs an empty loop
+    // (Solvers/hprsecondordersolver.cpp:368-373, :378-383): accepted and ignored, as there
+    if (cfg->subcycles > 0 && !s->ops->forcing && s->d.model != VG_MODEL_HPR_MULTIPHYSICS)
         return fail(VG_EUNSUPPORTED, "source sub-cycling needs a model with a source (HPR relaxation, MHD GLM damping)");
     if (cfg->order != 0 && cfg->order != 1 && cfg->order != 2) return fail(VG_EINVAL, "order must be 1 or 2");
     if (cfg->order == 1 && !s->ops->x1) return fail(VG_EUNSUPPORTED, "this kernel form has no first-order loop");

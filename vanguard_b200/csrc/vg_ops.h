@@ -24,7 +24,8 @@ enum Variant : int {
     V_MINT12 = 9,  // MHD intermediate two-material: alpha1, u, v, w, rho1, p1, rho2, p2, Bx, By, Bz, psi
     V_HRED19 = 10,  // HPR reduced two-material: alpha1, p, A(9), u, v, w, Jx, Jy, Jz, rho1, rho2
     V_HINT20 = 11,  // HPR intermediate two-material: alpha1, A(9), u, v, w, Jx, Jy, Jz, rho1, p1, rho2, p2
-    V_COUNT = 12
+    V_HMPH32 = 12,  // HPR multiphysics two-material (1D): alpha1, u, v, w, rho1, p1, A1(9), J1(3), rho2, p2, A2(9), J2(3)
+    V_COUNT = 13
 };
 
 struct Ops {
@@ -74,6 +75,7 @@ cudaError_t mhd_reduced_reinit_fp64(const SweepArgs& a, cudaStream_t st);
 cudaError_t mhd_intermediate_reinit_fp64(const SweepArgs& a, cudaStream_t st);
 cudaError_t hpr_reduced_reinit_fp64(const SweepArgs& a, cudaStream_t st);
 cudaError_t hpr_intermediate_reinit_fp64(const SweepArgs& a, cudaStream_t st);
+cudaError_t hpr_multiphysics_reinit_fp64(const SweepArgs& a, cudaStream_t st);
 
 // Planes of the source sub-cycles' scratch (SweepArgs::aux), which holds conserved vectors: a model carries at most
 // one conserved component more than primitive planes (the two-material models' rho alpha1), which forcing_impl

@@ -76,7 +76,7 @@ void run_planes(int model, std::vector<double>& planes, int nx, int ny, const do
     // two-material models have no mixed form
     const bool exact = order == 1 || model == VG_MODEL_EULER_MULTIPHYSICS || model == VG_MODEL_MHD_REDUCED ||
                        model == VG_MODEL_MHD_INTERMEDIATE || model == VG_MODEL_HPR_REDUCED ||
-                       model == VG_MODEL_HPR_INTERMEDIATE;
+                       model == VG_MODEL_HPR_INTERMEDIATE || model == VG_MODEL_HPR_MULTIPHYSICS;
     SolverPtr s = make_solver(model, nx, ny, VG_TRANSMISSIVE, params, nparams, exact ? VG_FP64 : -1);
     vg_run_config c{};
     c.dx = dx;
@@ -93,7 +93,7 @@ void run_planes(int model, std::vector<double>& planes, int nx, int ny, const do
 }
 
 // ---- packing between reference-style cells and SoA primitive planes
-constexpr int kMaxPlanes = 20;  // the most primitive planes of any model (the HPR intermediate state)
+constexpr int kMaxPlanes = 32;  // the most primitive planes of any model (the HPR multiphysics state)
 template <class S, class Get>
 std::vector<double> pack(const std::vector<S>& cells, int nvar, Get get) {
     long n = cells.size();
@@ -1078,4 +1078,78 @@ vector<vector<HPRIntermediateStateVector> > HPRFirstOrderSolver::solve2D(
     HPRMaterialParameters m1, HPRMaterialParameters m2, int maxSteps) {
     return hpr_two_run2(VG_MODEL_HPR_INTERMEDIATE, 20, initialCells, m1, m2, dx, cfl, tEnd, 0.0, 0, 0, maxSteps, 1, 0,
                         hint_get, hint_make);
+}
+
+// ---------------------------------------------------------------------------------- HPR multiphysics model
+namespace {
+void hmph_get(const HPRMultiphysicsStateVector& c, double* w) { std::memcpy(w, c.data(), sizeof(double) * 32); }
+HPRMultiphysicsStateVector hmph_make(const double* w) {
+    HPRMultiphysicsStateVector s;
+    std::memcpy(s.data(), w, sizeof(double) * 32);
+    return s;
+}
+}  // namespace
+
+// HPRMultiphysicsStateVector() (HPR/Multiphysics/hprmultiphysicsstatevector.cpp:3-26)
+HPRMultiphysicsStateVector::HPRMultiphysicsStateVector() : w_{} {
+    w_[0] = 0.999;
+    for (int k = 0; k < 2; k++) {
+        w_[4 + 14 * k] = 1.0;
+        w_[5 + 14 * k] = 1.0 / 1.4;
+        w_[6 + 14 * k] = w_[10 + 14 * k] = w_[14 + 14 * k] = 1.0;
+    }
+}
+HPRMultiphysicsStateVector::HPRMultiphysicsStateVector(double a1, double u, double v, double w, double r1, double p1,
+                                                       vector<vector<double> > A1, double j1x, double j1y, double j1z,
+                                                       double r2, double p2, vector<vector<double> > A2, double j2x,
+                                                       double j2y, double j2z)
+    : w_{} {
+    const double head[6] = {a1, u, v, w, r1, p1};
+    for (int i = 0; i < 6; i++) w_[i] = head[i];
+    tensor_into(A1, w_ + 6);
+    w_[15] = j1x, w_[16] = j1y, w_[17] = j1z;
+    w_[18] = r2, w_[19] = p2;
+    tensor_into(A2, w_ + 20);
+    w_[29] = j2x, w_[30] = j2y, w_[31] = j2z;
+}
+void HPRMultiphysicsStateVector::setPrimitiveVariableVector(vector<double> w, HPRMaterialParameters m1,
+                                                            HPRMaterialParameters m2) {
+    for (int i = 0; i < 32; i++) {
+        if (i >= 15 && i < 18 && !m1.getIsThermal()) continue;
+        if (i >= 29 && !m2.getIsThermal()) continue;
+        w_[i] = w[i];
+    }
+}
+vector<double> HPRMultiphysicsStateVector::computePrimitiveVariableVector(HPRMaterialParameters m1,
+                                                                          HPRMaterialParameters m2) const {
+    vector<double> w(w_, w_ + 32);
+    if (!m1.getIsThermal()) w[15] = w[16] = w[17] = 0.0;
+    if (!m2.getIsThermal()) w[29] = w[30] = w[31] = 0.0;
+    return w;
+}
+vector<vector<double> > HPRMultiphysicsStateVector::getMaterial1DistortionTensor() const { return tensor_of(w_ + 6); }
+vector<vector<double> > HPRMultiphysicsStateVector::getMaterial2DistortionTensor() const { return tensor_of(w_ + 20); }
+
+vector<HPRMultiphysicsStateVector> HPRSecondOrderSolver::solve(vector<HPRMultiphysicsStateVector>& initialCells,
+                                                               double dx, double cfl, double tEnd, double bias,
+                                                               int limiter, int subcycles, int reinit,
+                                                               HPRMaterialParameters m1, HPRMaterialParameters m2,
+                                                               int maxSteps) {
+    double prm[22];
+    hpr_two_params(m1, m2, prm);
+    std::vector<double> p = pack(initialCells, 32, hmph_get);
+    run_planes(VG_MODEL_HPR_MULTIPHYSICS, p, (int)initialCells.size(), 1, prm, 22, dx, cfl, tEnd, bias, limiter,
+               subcycles, maxSteps, 2, reinit);
+    return unpack<HPRMultiphysicsStateVector>(p, initialCells.size(), 32, hmph_make);
+}
+vector<HPRMultiphysicsStateVector> HPRFirstOrderSolver::solve(vector<HPRMultiphysicsStateVector>& initialCells,
+                                                              double dx, double cfl, double tEnd, int,
+                                                              HPRMaterialParameters m1, HPRMaterialParameters m2,
+                                                              int maxSteps) {
+    double prm[22];
+    hpr_two_params(m1, m2, prm);
+    std::vector<double> p = pack(initialCells, 32, hmph_get);
+    run_planes(VG_MODEL_HPR_MULTIPHYSICS, p, (int)initialCells.size(), 1, prm, 22, dx, cfl, tEnd, 0.0, 0, 0, maxSteps,
+               1, 0);
+    return unpack<HPRMultiphysicsStateVector>(p, initialCells.size(), 32, hmph_make);
 }

@@ -398,6 +398,42 @@ private:
     double w_[20];
 };
 
+// HPRMultiphysicsStateVector (HPR/Multiphysics/hprmultiphysicsstatevector.h; 1D): the HPR multiphysics two-material
+// state, primitives alpha1, u, v, w, rho1, p1, A1 (9), J1 (3), rho2, p2, A2 (9), J2 (3).  A material's J is taken and
+// returned only when that material is thermal (hprmultiphysicsstatevector.cpp:98-139, :204-249); a cold material's J
+// enters the solve as 0.
+class HPRMultiphysicsStateVector {
+public:
+    HPRMultiphysicsStateVector();
+    HPRMultiphysicsStateVector(double newMaterial1VolumeFraction, double newInterfaceXVelocity,
+                               double newInterfaceYVelocity, double newInterfaceZVelocity, double newMaterial1Density,
+                               double newMaterial1Pressure, vector<vector<double> > newMaterial1DistortionTensor,
+                               double newMaterial1XThermalImpulse, double newMaterial1YThermalImpulse,
+                               double newMaterial1ZThermalImpulse, double newMaterial2Density, double newMaterial2Pressure,
+                               vector<vector<double> > newMaterial2DistortionTensor, double newMaterial2XThermalImpulse,
+                               double newMaterial2YThermalImpulse, double newMaterial2ZThermalImpulse);
+    void setPrimitiveVariableVector(vector<double> w, HPRMaterialParameters material1Parameters,
+                                    HPRMaterialParameters material2Parameters);
+    vector<double> computePrimitiveVariableVector(HPRMaterialParameters material1Parameters,
+                                                  HPRMaterialParameters material2Parameters) const;
+    double getMaterial1VolumeFraction() const { return w_[0]; }
+    double getInterfaceXVelocity() const { return w_[1]; }
+    double getInterfaceYVelocity() const { return w_[2]; }
+    double getInterfaceZVelocity() const { return w_[3]; }
+    double getMaterial1Density() const { return w_[4]; }
+    double getMaterial1Pressure() const { return w_[5]; }
+    vector<vector<double> > getMaterial1DistortionTensor() const;
+    double getMaterial2Density() const { return w_[18]; }
+    double getMaterial2Pressure() const { return w_[19]; }
+    vector<vector<double> > getMaterial2DistortionTensor() const;
+    void setMaterial1VolumeFraction(double v) { w_[0] = v; }
+    double* data() { return w_; }
+    const double* data() const { return w_; }
+
+private:
+    double w_[32];
+};
+
 class SlopeLimiters {
 public:
     static double computeRCoefficient(double steepness, double bias);
@@ -599,6 +635,10 @@ public:
                                                                HPRMaterialParameters material1Parameters,
                                                                HPRMaterialParameters material2Parameters,
                                                                int maxSteps = 0);
+    static vector<HPRMultiphysicsStateVector> solve(vector<HPRMultiphysicsStateVector>& initialCells, double cellSpacing,
+                                                    double CFLCoefficient, double finalTime, int subcyclingIterations,
+                                                    HPRMaterialParameters material1Parameters,
+                                                    HPRMaterialParameters material2Parameters, int maxSteps = 0);
     static vector<HPRStateVector> solve(vector<HPRStateVector>& initialCells, double cellSpacing, double CFLCoefficient,
                                         double finalTime, int subcyclingIterations, HPRMaterialParameters mp);
     static vector<vector<HPRStateVector> > solve2D(vector<vector<HPRStateVector> >& initialCells, double cellSpacing,
@@ -652,4 +692,11 @@ public:
                                                                HPRMaterialParameters material1Parameters,
                                                                HPRMaterialParameters material2Parameters,
                                                                int maxSteps = 0);
+    // the HPR multiphysics model, 1D (Solvers/hprsecondordersolver.cpp:354-400; its sub-cycle loops are empty)
+    static vector<HPRMultiphysicsStateVector> solve(vector<HPRMultiphysicsStateVector>& initialCells, double cellSpacing,
+                                                    double CFLCoefficient, double finalTime, double bias,
+                                                    int slopeLimiter, int subcyclingIterations,
+                                                    int reinitialisationFrequency,
+                                                    HPRMaterialParameters material1Parameters,
+                                                    HPRMaterialParameters material2Parameters, int maxSteps = 0);
 };

@@ -432,3 +432,30 @@ def hpr_intermediate_riemann(nx, ny=1, seed=0, distortion=0.02, heat=0.05, bubbl
     """hpr_reduced_riemann's two-material HPR Riemann problem in the intermediate model's planes, shape (20, n) or
     (20, ny, nx)."""
     return hpr_intermediate_from_reduced(hpr_reduced_riemann(nx, ny, seed, distortion, heat, bubble), p2_scale)
+
+
+HPR_MULTIPHYSICS_NVAR = 32
+
+
+def hpr_multiphysics_from_reduced(W, p2_scale=1.0, a2_scale=1.0):
+    """The HPR multiphysics model's 32 planes (alpha1, u, v, w, rho1, p1, A1(9), J1(3), rho2, p2, A2(9), J2(3)) of a 1D
+    HPR reduced state: material 1 at the interface pressure with the state's distortion and heat flux, material 2 at
+    p2_scale times the pressure, with a2_scale times the distortion and half the heat flux."""
+    assert W.ndim == 2, "the HPR multiphysics model is 1D only"
+    out = np.zeros((HPR_MULTIPHYSICS_NVAR, W.shape[1]))
+    out[0] = W[0]
+    out[1:4] = W[11:14]
+    out[4] = W[17]
+    out[5] = W[1]
+    out[6:15] = W[2:11]
+    out[15:18] = W[14:17]
+    out[18] = W[18]
+    out[19] = p2_scale * W[1]
+    out[20:29] = a2_scale * W[2:11]
+    out[29:32] = 0.5 * W[14:17]
+    return out
+
+
+def hpr_multiphysics_riemann(nx, seed=0, distortion=0.02, heat=0.05, p2_scale=1.0, a2_scale=1.0):
+    """hpr_reduced_riemann's 1D two-material HPR Riemann problem in the multiphysics model's planes, shape (32, nx)."""
+    return hpr_multiphysics_from_reduced(hpr_reduced_riemann(nx, 1, seed, distortion, heat), p2_scale, a2_scale)
