@@ -30,6 +30,9 @@
  *                                      multiphysics two-material model, HPR/Multiphysics/
  *                                      hprmultiphysicsstatevector.cpp:204-249 (VG_FP64 only; 1D: ny = 1; a cold
  *                                      material's J is taken and returned as 0)
+ *   VG_MODEL_MHD_MULTIPHYSICS (16 planes): alpha1, u, v, w, rho1, p1, B1(3), psi1, rho2, p2, B2(3), psi2   the MHD
+ *                                      multiphysics two-material model, MHD/Multiphysics/
+ *                                      mhdmultiphysicsstatevector.cpp:135-163 (VG_FP64 only; 1D: ny = 1)
  * Ownership: a vg_solver owns all device memory it allocates; the caller owns every host buffer.
  * Threading: calls on different solvers are independent and re-entrant; one solver must not be used
  * from two host threads at once.  All work is enqueued on the stream given (NULL: the legacy default
@@ -66,7 +69,8 @@ typedef enum vg_model {
     VG_MODEL_MHD_INTERMEDIATE = 6,
     VG_MODEL_HPR_REDUCED = 7,
     VG_MODEL_HPR_INTERMEDIATE = 8,
-    VG_MODEL_HPR_MULTIPHYSICS = 9
+    VG_MODEL_HPR_MULTIPHYSICS = 9,
+    VG_MODEL_MHD_MULTIPHYSICS = 10
 } vg_model;
 
 /* VG_FP64: every operation in float64, in the reference's order, no FMA: matches the reference.
@@ -102,6 +106,7 @@ enum { VG_SUPERBEE = 0, VG_VANLEER = 1, VG_MINBEE = 2 };
  *                                                 the exponent alpha_eos); is_plastic selects the plastic strain
  *                                                 relaxation with transition stress sigma0 and power-law index n
  *                                                 (HPR/hprsourceterms.cpp:12-23).
+ *   MHD multiphysics: {gamma1, p_inf1, gamma2, p_inf2, c_h1, c_h2}   each material's c_h stays as given
  *   HPR reduced, intermediate, multiphysics: 11 per material, material k at params[11 k]: {gamma, p_inf, c_v, rho0, T0, c_s,
  *                alpha, tau1, tau2, T_ref, is_thermal}   the two materials' StiffenedGas HPRMaterialParameters (elastic
  *                relaxation)
@@ -148,7 +153,7 @@ typedef struct vg_solver vg_solver;
 vg_status vg_create(const vg_grid_desc* desc, vg_solver** out);
 vg_status vg_destroy(vg_solver* s);
 
-/* Number of primitive planes the model takes at this boundary (6, 9, 17, 7, 8, 11, 12, 19, 20, 32). */
+/* Number of primitive planes the model takes at this boundary (6, 9, 17, 7, 8, 11, 12, 19, 20, 32, 16). */
 int vg_model_nvar(int model);
 
 /* Copy the state in / out.  planes: vg_model_nvar(model) planes of nx*ny float64, host or device

@@ -24,7 +24,7 @@ ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libvgref.so")
 
 (EULER, MHD, HPR, EULER_REDUCED, EULER_MULTIPHYSICS, MHD_REDUCED, MHD_INTERMEDIATE, HPR_REDUCED, HPR_INTERMEDIATE,
- HPR_MULTIPHYSICS) = 0, 1, 2, 3, 4, 5, 6, 7, 8, 9
+ HPR_MULTIPHYSICS, MHD_MULTIPHYSICS) = 0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10
 NVAR = {EULER: 6, MHD: 9, HPR: 17}
 TRANSMISSIVE, PERIODIC = 0, 1
 SUPERBEE, VANLEER, MINBEE = 0, 1, 2
@@ -249,9 +249,9 @@ def hpr_cell(w, params, reference=False):
 
 
 _TWO_MATERIAL_NW = {EULER_REDUCED: 7, EULER_MULTIPHYSICS: 8, MHD_REDUCED: 11, MHD_INTERMEDIATE: 12, HPR_REDUCED: 19,
-                    HPR_INTERMEDIATE: 20, HPR_MULTIPHYSICS: 32}
+                    HPR_INTERMEDIATE: 20, HPR_MULTIPHYSICS: 32, MHD_MULTIPHYSICS: 16}
 # the two-material models with a source (their loops take sub-cycles: MHD GLM damping, HPR relaxation)
-_MHD_TWO_MATERIAL = (MHD_REDUCED, MHD_INTERMEDIATE, HPR_REDUCED, HPR_INTERMEDIATE, HPR_MULTIPHYSICS)
+_MHD_TWO_MATERIAL = (MHD_REDUCED, MHD_INTERMEDIATE, HPR_REDUCED, HPR_INTERMEDIATE, HPR_MULTIPHYSICS, MHD_MULTIPHYSICS)
 
 
 def run_two_material(model, planes, dx, cfl, t_end=0.0, steps=0, bias=0.0, limiter=SUPERBEE, params=None, reinit=0,
@@ -261,8 +261,9 @@ def run_two_material(model, planes, dx, cfl, t_end=0.0, steps=0, bias=0.0, limit
     MHD_REDUCED (11: alpha1, u, v, w, rho1, rho2, p, Bx, By, Bz, psi), MHD_INTERMEDIATE (12: alpha1, u, v, w, rho1,
     p1, rho2, p2, Bx, By, Bz, psi), HPR_REDUCED (19: alpha1, p, A(9), u, v, w, Jx, Jy, Jz, rho1, rho2) or
     HPR_INTERMEDIATE (20: alpha1, A(9), u, v, w, Jx, Jy, Jz, rho1, p1, rho2, p2) or HPR_MULTIPHYSICS (32, 1D only:
-    alpha1, u, v, w, rho1, p1, A1(9), J1(3), rho2, p2, A2(9), J2(3)), x (n) or (ny, nx); from the restatement or
-    (reference=True) the reference.  params = (gamma1, p_inf1, gamma2, p_inf2); the HPR models: 11 per
+    alpha1, u, v, w, rho1, p1, A1(9), J1(3), rho2, p2, A2(9), J2(3)) or MHD_MULTIPHYSICS (16, 1D only: alpha1, u, v,
+    w, rho1, p1, B1(3), psi1, rho2, p2, B2(3), psi2; params (gamma1, p_inf1, gamma2, p_inf2, c_h1, c_h2); its loop has
+    no source and no reinitialisation), x (n) or (ny, nx); from the restatement or (reference=True) the reference.  params = (gamma1, p_inf1, gamma2, p_inf2); the HPR models: 11 per
     material, {gamma, p_inf, c_v, rho0, T0, c_s, alpha, tau1, tau2, T_ref, is_thermal} each; reinit > 0
     reinitialises the volume fraction every `reinit` steps; subcycles > 0 (the MHD models: GLM damping; the HPR
     models: the relaxation source) adds the RK4 forcing sub-cycles.
@@ -282,6 +283,13 @@ def run_two_material(model, planes, dx, cfl, t_end=0.0, steps=0, bias=0.0, limit
             # the intermediate model's own solve2D pads with its defective insertBoundaryCells2D
             # (Solvers/mhdsolvers.cpp:213); the harness's per-step loop builds mirror ghosts instead
             assert not (model == MHD_INTERMEDIATE and ny > 1 and steps <= 0), "2D intermediate: per-step runs only"
+            if model == MHD_MULTIPHYSICS:
+                assert ny == 1, "the reference's MHD multiphysics model is 1D only"
+                fn = R.vgref_mhd_multiphysics_run
+                fn.restype = _c_double
+                t = fn(_ptr(planes), nx, _c_double(dx), _c_double(cfl), _c_double(t_end), steps, _c_double(bias),
+                       limiter, _ptr(prm), ctypes.byref(st))
+                return t, st.value
             if model == HPR_MULTIPHYSICS:
                 assert ny == 1, "the reference's HPR multiphysics model is 1D only"
                 fn = R.vgref_hpr_multiphysics_run

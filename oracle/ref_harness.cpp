@@ -1120,3 +1120,42 @@ extern "C" double vgref_hpr_multiphysics_run(double* planes, int nx, double dx, 
     if (steps_out) *steps_out = it;
     return t;
 }
+
+// ------------------------------------------------------------------------------- MHD multiphysics two-material
+// Planes: the 16 primitives of MHDMultiphysicsStateVector (alpha1, u, v, w, rho1, p1, B1(3), psi1, rho2, p2, B2(3),
+// psi2; MHD/Multiphysics/mhdmultiphysicsstatevector.cpp:135-163); prm = {gamma1, p_inf1, gamma2, p_inf2, c_h1, c_h2};
+// 1D only, as the reference has it.  max_steps <= 0: the reference's own MHDSecondOrderSolver::solve to t_end
+// (Solvers/mhdsecondordersolver.cpp:362-385: no source, no reinitialisation, the materials' c_h as given); else its
+// per-step functions for max_steps steps in solve's order.
+extern "C" double vgref_mhd_multiphysics_run(double* planes, int nx, double dx, double cfl, double t_end, int max_steps,
+                                             double bias, int limiter, const double* prm, int* steps_out) {
+    QuietCout quiet;
+    MHDMaterialParameters m1 = mhdParams(prm), m2 = mhdParams(prm + 2);
+    m1.setHyperbolicWaveSpeed(prm[4]);
+    m2.setHyperbolicWaveSpeed(prm[5]);
+    double t = 0.0;
+    int it = 0;
+    vector<MHDMultiphysicsStateVector> cells(nx);
+    for (int i = 0; i < nx; i++) {
+        vector<double> w(16);
+        for (int v = 0; v < 16; v++) w[v] = planes[(long)v * nx + i];
+        cells[i].setPrimitiveVariableVector(w);
+    }
+    if (max_steps <= 0) {
+        cells = MHDSecondOrderSolver::solve(cells, dx, cfl, t_end, bias, limiter, 0, 0, m1, m2);
+        t = t_end;
+    } else {
+        for (; it < max_steps; it++) {
+            vector<MHDMultiphysicsStateVector> withB = MHDSolvers::insertBoundaryCells(cells, 2);
+            double dt = MHDSolvers::computeStableTimeStep(withB, dx, cfl, t, 1.0e300, it, m1, m2);
+            MHDSecondOrderSolver::computeSLICTimeStep(cells, withB, dx, dt, bias, limiter, m1, m2);
+            t += dt;
+        }
+    }
+    for (int i = 0; i < nx; i++) {
+        vector<double> w = cells[i].computePrimitiveVariableVector();
+        for (int v = 0; v < 16; v++) planes[(long)v * nx + i] = w[v];
+    }
+    if (steps_out) *steps_out = it;
+    return t;
+}

@@ -1745,6 +1745,124 @@ static void hmph_reinit(double* planes, int nx) {
         planes[i] = i < loc ? 0.999 : 0.001;
     }
 }
+/* ---- MHD multiphysics two-material model: MHD/Multiphysics/mhdmultiphysicsstatevector.cpp (1D only in the
+ * reference).  Each material carries its own density, pressure, magnetic field and GLM scalar; the velocity is shared.
+ * prm = {gamma1, p_inf1, gamma2, p_inf2, c_h1, c_h2}: the materials' hyperbolic wave speeds stay as given, since the
+ * reference's solve sets none (Solvers/mhdsecondordersolver.cpp:362-385).
+ * W = alpha1, u, v, w, rho1, p1, B1 (3), psi1, rho2, p2, B2 (3), psi2 (:135-163) and an unused plane;
+ * U = rho, rho alpha1, rho u (3), then per material k at 5 + 6 k: alpha rho, alpha E, alpha^(1/2) B (3), alpha psi
+ * (:165-220). */
+/* computeConservedVariableVector (:165-220) */
+static void mmph_cons(const double* W, const double* prm, double* U) {
+    double a1 = red_clamp(W[0]), a2 = 1.0 - a1;
+    double u = W[1], v = W[2], w = W[3];
+    double rho = (a1 * W[4]) + (a2 * W[10]);
+    for (int i = 0; i < 17; i++) U[i] = 0.0;
+    U[0] = rho;
+    U[1] = rho * a1;
+    U[2] = rho * u;
+    U[3] = rho * v;
+    U[4] = rho * w;
+    double v2 = ((u * u) + (v * v)) + (w * w);
+    for (int k = 0; k < 2; k++) {
+        double a = k == 0 ? a1 : a2;
+        const double* wk = W + 4 + 6 * k; /* rho, p, B (3), psi */
+        double* uk = U + 5 + 6 * k;
+        uk[0] = a * wk[0];
+        double b2 = ((wk[2] * wk[2]) + (wk[3] * wk[3])) + (wk[4] * wk[4]);
+        double h = wk[0] * ((0.5 * v2) + mhd_e(wk[0], wk[1], prm + 2 * k));
+        uk[1] = a * (h + (0.5 * b2));
+        for (int i = 0; i < 3; i++) uk[2 + i] = pow(a, 1.0 / 2.0) * wk[2 + i];
+        uk[5] = a * wk[5];
+    }
+}
+/* setConservedVariableVector (:84-133) */
+static void mmph_setcons(const double* U, const double* prm, double* W) {
+    double rho = U[0];
+    double a1 = red_clamp(U[1] / rho), a2 = 1.0 - a1;
+    double u = U[2] / rho, v = U[3] / rho, w = U[4] / rho;
+    double v2 = ((u * u) + (v * v)) + (w * w);
+    W[1] = u;
+    W[2] = v;
+    W[3] = w;
+    for (int k = 0; k < 2; k++) {
+        double a = k == 0 ? a1 : a2;
+        double* wk = W + 4 + 6 * k;
+        const double* uk = U + 5 + 6 * k;
+        wk[0] = uk[0] / a;
+        for (int i = 0; i < 3; i++) wk[2 + i] = uk[2 + i] / pow(a, 1.0 / 2.0);
+        double b2 = ((wk[2] * wk[2]) + (wk[3] * wk[3])) + (wk[4] * wk[4]);
+        double E = ((uk[1] / a) - (0.5 * b2)) / wk[0];
+        wk[1] = mhd_p(wk[0], E - (0.5 * v2), prm + 2 * k);
+        wk[5] = uk[5] / a;
+    }
+    W[0] = a1;
+}
+/* computeXFluxVector (:222-358); the reference has no Y flux for this model.  The interface field components are
+ * pow(alpha1 B1^2 + alpha2 B2^2, 1/2) per component; each material's energy flux carries its own field. */
+static void mmph_flux(const double* U, int axis, const double* prm, double* F) {
+    (void)axis;
+    double rho = U[0];
+    double a1 = red_clamp(U[1] / rho), a2 = 1.0 - a1;
+    double u = U[2] / rho, v = U[3] / rho, w = U[4] / rho;
+    double r[2], B[2][3], psi[2], Et[2], p[2], b2[2];
+    for (int k = 0; k < 2; k++) {
+        double a = k == 0 ? a1 : a2;
+        const double* uk = U + 5 + 6 * k;
+        r[k] = uk[0] / a;
+        for (int i = 0; i < 3; i++) B[k][i] = uk[2 + i] / pow(a, 1.0 / 2.0);
+        psi[k] = uk[5] / a;
+    }
+    double IB2[3], IB[3];
+    for (int i = 0; i < 3; i++) {
+        IB2[i] = (a1 * (B[0][i] * B[0][i])) + (a2 * (B[1][i] * B[1][i]));
+        IB[i] = pow(IB2[i], 1.0 / 2.0);
+    }
+    double v2 = ((u * u) + (v * v)) + (w * w);
+    double ib2 = (IB2[0] + IB2[1]) + IB2[2];
+    for (int k = 0; k < 2; k++) {
+        double a = k == 0 ? a1 : a2;
+        b2[k] = ((B[k][0] * B[k][0]) + (B[k][1] * B[k][1])) + (B[k][2] * B[k][2]);
+        Et[k] = U[6 + 6 * k] / a;
+        double e = ((Et[k] - (0.5 * b2[k])) / r[k]) - (0.5 * v2);
+        p[k] = mhd_p(r[k], e, prm + 2 * k);
+    }
+    for (int i = 0; i < 17; i++) F[i] = 0.0;
+    F[0] = rho * u;
+    F[1] = rho * (u * a1);
+    F[2] = (((rho * (u * u)) + ((a1 * p[0]) + (a2 * p[1]))) + (0.5 * ib2)) - IB2[0];
+    F[3] = (rho * (u * v)) - (IB[0] * IB[1]);
+    F[4] = (rho * (u * w)) - (IB[0] * IB[2]);
+    for (int k = 0; k < 2; k++) {
+        double a = k == 0 ? a1 : a2, ch = prm[4 + k];
+        double* fk = F + 5 + 6 * k;
+        fk[0] = a * (r[k] * u);
+        double bv = ((0.0 + (u * B[k][0])) + (v * B[k][1])) + (w * B[k][2]);
+        fk[1] = (a * (((Et[k] + p[k]) + (0.5 * b2[k])) * u)) - (a * (bv * B[k][0]));
+        fk[2] = pow(a, 1.0 / 2.0) * psi[k];
+        fk[3] = pow(a, 1.0 / 2.0) * ((B[k][1] * u) - (B[k][0] * v));
+        fk[4] = pow(a, 1.0 / 2.0) * ((B[k][2] * u) - (B[k][0] * w));
+        fk[5] = a * ((ch * ch) * B[k][0]);
+    }
+}
+/* MHDSolvers::computeMaximumWaveSpeed for the multiphysics model (Solvers/mhdsolvers.cpp:305-323): each material's
+ * fast magneto-acoustic speed at its own density, pressure and field */
+static double mmph_wave1d(const double* W, const double* prm) {
+    double V1[9] = {W[4], 0.0, 0.0, 0.0, W[5], W[6], W[7], W[8], 0.0};
+    double V2[9] = {W[10], 0.0, 0.0, 0.0, W[11], W[12], W[13], W[14], 0.0};
+    return fabs(W[1]) + smax(fabs(mhd_fast(V1, prm, W[6])), fabs(mhd_fast(V2, prm + 2, W[12])));
+}
+static double mmph_wave2d(const double* W, const double* prm) { (void)W; (void)prm; return NAN; }
+/* MHDMultiphysicsStateVector() (:3-27) */
+static void mmph_default(const double* prm, double* W) {
+    (void)prm;
+    for (int i = 0; i < 17; i++) W[i] = 0.0;
+    W[0] = 0.999;
+    W[4] = 1.0;
+    W[5] = 1.0;
+    W[10] = 1.0;
+    W[11] = 1.0;
+}
 /* HPRReducedStateVector() (:3-19) */
 static void hred_default(const double* prm, double* W) {
     (void)prm;
@@ -1822,6 +1940,7 @@ static const model M_MINT = {13, mint_cons, mint_setcons, mint_flux, mint_wave1d
 static const model M_HRED = {20, hred_cons, hred_setcons, hred_flux, hred_wave1d, hred_wave2d, hred_default, hred_source};
 static const model M_HINT = {21, hint_cons, hint_setcons, hint_flux, hint_wave1d, hint_wave2d, hint_default, hint_source};
 static const model M_HMPH = {33, hmph_cons, hmph_setcons, hmph_flux, hmph_wave1d, hmph_wave2d, hmph_default, 0};
+static const model M_MMPH = {17, mmph_cons, mmph_setcons, mmph_flux, mmph_wave1d, mmph_wave2d, mmph_default, 0};
 
 static const model* model_of(int id) {
     switch (id) {
@@ -1835,13 +1954,14 @@ static const model* model_of(int id) {
         case VO_HPR_REDUCED: return &M_HRED;
         case VO_HPR_INTERMEDIATE: return &M_HINT;
         case VO_HPR_MULTIPHYSICS: return &M_HMPH;
+        case VO_MHD_MULTIPHYSICS: return &M_MMPH;
         default: return NULL;
     }
 }
 
 int vo_nvar(int id) { const model* m = model_of(id); return m ? m->nv : 0; }
 int vo_nparams(int id) {
-    return id == VO_EULER ? 6 : id == VO_MHD ? 3 : id == VO_HPR ? 20 : (id == VO_EULER_REDUCED || id == VO_EULER_MULTIPHYSICS) ? 4 : (id == VO_MHD_REDUCED || id == VO_MHD_INTERMEDIATE) ? 5 : (id == VO_HPR_REDUCED || id == VO_HPR_INTERMEDIATE || id == VO_HPR_MULTIPHYSICS) ? 22 : 0;
+    return id == VO_EULER ? 6 : id == VO_MHD ? 3 : id == VO_HPR ? 20 : (id == VO_EULER_REDUCED || id == VO_EULER_MULTIPHYSICS) ? 4 : (id == VO_MHD_REDUCED || id == VO_MHD_INTERMEDIATE) ? 5 : id == VO_MHD_MULTIPHYSICS ? 6 : (id == VO_HPR_REDUCED || id == VO_HPR_INTERMEDIATE || id == VO_HPR_MULTIPHYSICS) ? 22 : 0;
 }
 
 /* ------------------------------------------------------------------------------- SLIC building blocks */
@@ -2313,9 +2433,9 @@ double vo_run_mhd_two_material(int id, double* planes, int nx, int ny, double dx
                                 int max_steps, double w, int lim, const double* prm, int bc, int subcycles,
                                 int reinit_freq, int* steps_out) {
     if (id != VO_MHD_REDUCED && id != VO_MHD_INTERMEDIATE && id != VO_HPR_REDUCED && id != VO_HPR_INTERMEDIATE &&
-        id != VO_HPR_MULTIPHYSICS)
+        id != VO_HPR_MULTIPHYSICS && id != VO_MHD_MULTIPHYSICS)
         return -1.0;
-    if (id == VO_HPR_MULTIPHYSICS && ny > 1) return -1.0;  /* the reference's model is 1D only */
+    if ((id == VO_HPR_MULTIPHYSICS || id == VO_MHD_MULTIPHYSICS) && ny > 1) return -1.0;  /* 1D only, as the reference */
     hred_drop_cold_heat_flux(id, planes, (long)nx * ny, prm);
     hmph_drop_cold_heat_flux(id, planes, (long)nx * ny, prm);
     double t = run(id, planes, nx, ny, ny > 1 ? 2 : 1, dx, cfl, t_end, max_steps, w, lim, prm, bc, subcycles,

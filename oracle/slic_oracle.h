@@ -24,7 +24,7 @@ extern "C" {
 
 enum { VO_EULER = 0, VO_MHD = 1, VO_HPR = 2, VO_EULER_REDUCED = 3, VO_EULER_MULTIPHYSICS = 4, VO_MHD_REDUCED = 5, VO_MHD_INTERMEDIATE = 6,
        VO_HPR_REDUCED = 7, VO_HPR_INTERMEDIATE = 8,
-       VO_HPR_MULTIPHYSICS = 9 };
+       VO_HPR_MULTIPHYSICS = 9, VO_MHD_MULTIPHYSICS = 10 };
 enum { VO_BC_TRANSMISSIVE = 0, VO_BC_PERIODIC = 1 };
 
 /* Number of primitive planes of a model (6, 9, 17). */

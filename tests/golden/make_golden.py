@@ -176,10 +176,23 @@ HPR_MULTIPHYSICS_CASES = {
         dict(dx=1 / 50, cfl=0.8, steps=2, limiter=O.VANLEER, reinit=1, subcycles=0,
              params=wl.hpr_reduced_params(gamma2=2.0, p_inf2=0.5, thermal=(True, False)))),
 }
+# The MHD multiphysics two-material model (model id O.MHD_MULTIPHYSICS, 1D only): MHDMultiphysicsTests'
+# solveDumbserMultimaterialTest1 setting through the reference's own solve, and a perturbed layout per step with
+# non-zero hyperbolic wave speeds.
+MHD_MULTIPHYSICS_CASES = {
+    "mhdmultiphysics1d_dumbsermm80_solve_t005": (
+        lambda: wl.mhd_multiphysics_dumbser_1d(80),
+        dict(dx=1 / 80, cfl=0.8, t_end=0.05, steps=0, limiter=O.SUPERBEE, reinit=0, subcycles=0,
+             params=wl.mhd_multiphysics_params(1.4, 0.0, 1.67, 0.0))),
+    "mhdmultiphysics1d_dumbser60_noise_glm_minbee_20": (
+        lambda: wl.mhd_multiphysics_dumbser_1d(60, seed=6, noise=1e-2),
+        dict(dx=1 / 60, cfl=0.8, steps=20, limiter=O.MINBEE, reinit=0, subcycles=0,
+             params=wl.mhd_multiphysics_params(1.4, 0.1, 1.67, 0.0, 0.5, 0.7))),
+}
 TWO_MATERIAL = {O.EULER_REDUCED: REDUCED_CASES, O.EULER_MULTIPHYSICS: MULTIPHYSICS_CASES,
                 O.MHD_REDUCED: MHD_REDUCED_CASES, O.MHD_INTERMEDIATE: MHD_INTERMEDIATE_CASES,
                 O.HPR_REDUCED: HPR_REDUCED_CASES, O.HPR_INTERMEDIATE: HPR_INTERMEDIATE_CASES,
-                O.HPR_MULTIPHYSICS: HPR_MULTIPHYSICS_CASES}
+                O.HPR_MULTIPHYSICS: HPR_MULTIPHYSICS_CASES, O.MHD_MULTIPHYSICS: MHD_MULTIPHYSICS_CASES}
 
 
 def make_two_material(name):

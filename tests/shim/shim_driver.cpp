@@ -8,7 +8,8 @@
 // two-material solve (8 x 100), MHD reduced two-material solve2D (11 x 24 x 24), MHD intermediate two-material solve
 // (12 x 80), the 2D maximum wave speed of an interior-only cold gas (1), whether solve2D refused a single row (1),
 // HPR reduced two-material solve2D (19 x 16 x 16), HPR intermediate two-material solve (20 x 60), HPR multiphysics
-// two-material solve (32 x 60), then the number of 2D steps the per-sweep loop took.
+// two-material solve (32 x 60), MHD multiphysics two-material solve (16 x 80), then the number of 2D steps the
+// per-sweep loop took.
 #include <cmath>
 #include <cstdio>
 #include <stdexcept>
@@ -19,6 +20,7 @@
 #include "Solvers/mhdsecondordersolver.h"
 #include "MHD/Multiphysics/mhdreducedstatevector.h"
 #include "MHD/Multiphysics/mhdintermediatestatevector.h"
+#include "MHD/Multiphysics/mhdmultiphysicsstatevector.h"
 #include "Solvers/hprsecondordersolver.h"
 #include "HPR/Multiphysics/hprreducedstatevector.h"
 #include "HPR/Multiphysics/hprintermediatestatevector.h"
@@ -295,6 +297,22 @@ int main(int argc, char** argv) {
         vector<double> v;
         for (int k = 0; k < 32; k++)
             for (auto& c : out) v.push_back(c.computePrimitiveVariableVector(hm1, hm2)[k]);
+        put(f, v);
+    }
+    // 16) MHDSecondOrderSolver::solve of the MHD multiphysics two-material model (1D), MHDMultiphysicsTests::
+    //     solveDumbserMultimaterialTest1's layout (gamma 1.4 | 1.67), to t = 0.05
+    {
+        int n = 80;
+        vector<MHDMultiphysicsStateVector> cells(n);
+        for (int i = 0; i < n; i++)
+            cells[i] = MHDMultiphysicsStateVector(i <= 0.5 * n ? 0.999 : 0.001, 0.0, 0.0, 0.0, 1.0, 1.0, 0.75, 1.0, 0.0, 0.0,
+                                                  0.125, 0.1, 0.75, -1.0, 0.0, 0.0);
+        vector<MHDMultiphysicsStateVector> out = MHDSecondOrderSolver::solve(cells, 1.0 / n, 0.8, 0.05, 0.0, 0, 0, 0,
+                                                                             MHDMaterialParameters(1.4),
+                                                                             MHDMaterialParameters(1.67));
+        vector<double> v;
+        for (int k = 0; k < 16; k++)
+            for (auto& c : out) v.push_back(c.computePrimitiveVariableVector()[k]);
         put(f, v);
     }
     double st = steps;

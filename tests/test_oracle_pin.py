@@ -26,7 +26,7 @@ def test_oracle_matches_golden(path, oracle_lib):
     kw = {k: (z[k].item() if z[k].ndim == 0 else z[k]) for k in z.files if k not in ("model", "w0", "out")}
     dx, cfl = kw.pop("dx"), kw.pop("cfl")
     if model in (O.EULER_REDUCED, O.EULER_MULTIPHYSICS, O.MHD_REDUCED, O.MHD_INTERMEDIATE, O.HPR_REDUCED,
-                 O.HPR_INTERMEDIATE, O.HPR_MULTIPHYSICS):
+                 O.HPR_INTERMEDIATE, O.HPR_MULTIPHYSICS, O.MHD_MULTIPHYSICS):
         O.run_two_material(model, w, dx, cfl, **kw)
     else:
         O.run(model, w, dx, cfl, **kw)

@@ -176,5 +176,14 @@ def test_shim_driver_matches_oracle(gpu, oracle_lib, tmp_path):
     d = np.abs(got - ref).max(axis=1) / np.maximum(np.abs(ref).max(axis=1), 1e-300)
     assert np.isfinite(got).all() and d.max() <= 1e-12
 
+    # 16) MHDSecondOrderSolver::solve of the MHD multiphysics two-material model to t = 0.05 (pow(alpha, 1/2) in the
+    #     conserved fields: 1e-12 of each plane's largest magnitude)
+    got = take((16, 80))
+    ref = wl.mhd_multiphysics_dumbser_1d(80)
+    O.run_two_material(O.MHD_MULTIPHYSICS, ref, 1 / 80, 0.8, t_end=0.05, limiter=0,
+                       params=wl.mhd_multiphysics_params(1.4, 0.0, 1.67, 0.0))
+    d = np.abs(got - ref).max(axis=1) / np.maximum(np.abs(ref).max(axis=1), 1e-300)
+    assert np.isfinite(got).all() and d.max() <= 1e-12
+
     assert take((1,))[0] == 6
     assert off == data.size

@@ -17,12 +17,12 @@ LIB_PATH = os.path.join(HERE, "libvanguard_slic.so")
 
 VG_OK, VG_EINVAL, VG_ENAN, VG_ETIMEOUT, VG_ECUDA, VG_ENOMEM, VG_EUNSUPPORTED = range(7)
 (EULER, MHD, HPR, EULER_REDUCED, EULER_MULTIPHYSICS, MHD_REDUCED, MHD_INTERMEDIATE, HPR_REDUCED, HPR_INTERMEDIATE,
- HPR_MULTIPHYSICS) = 0, 1, 2, 3, 4, 5, 6, 7, 8, 9
+ HPR_MULTIPHYSICS, MHD_MULTIPHYSICS) = 0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10
 FP64, MIXED = 0, 1
 TRANSMISSIVE, PERIODIC = 0, 1
 SUPERBEE, VANLEER, MINBEE = 0, 1, 2
 NVAR = {EULER: 6, MHD: 9, HPR: 17, EULER_REDUCED: 7, EULER_MULTIPHYSICS: 8, MHD_REDUCED: 11, MHD_INTERMEDIATE: 12,
-        HPR_REDUCED: 19, HPR_INTERMEDIATE: 20, HPR_MULTIPHYSICS: 32}
+        HPR_REDUCED: 19, HPR_INTERMEDIATE: 20, HPR_MULTIPHYSICS: 32, MHD_MULTIPHYSICS: 16}
 MAX_PARAMS = 24
 
 

@@ -710,4 +710,150 @@ struct MHDIntermediateF64 {
     }
 };
 
+// ------------------------------------------------------------------------ MHD multiphysics two-material
+// MHDMultiphysicsStateVector (MHD/Multiphysics/mhdmultiphysicsstatevector.cpp; 1D only in the reference): each
+// material carries its own density, pressure, magnetic field and GLM scalar, the velocity is shared.
+// W = (alpha1, u, v, w, rho1, p1, B1 (3), psi1, rho2, p2, B2 (3), psi2) (:135-163),
+// U = (rho, rho alpha1, rho u (3), then per material k at 5 + 6 k: alpha rho, alpha E, alpha^(1/2) B (3), alpha psi)
+// (:165-220).  Parameters {gamma1, p_inf1, gamma2, p_inf2, c_h1, c_h2}: the reference's solve for this model sets no
+// c_h (Solvers/mhdsecondordersolver.cpp:362-385), so each material keeps its own.  pow(alpha, 1/2) and the interface
+// field pow(alpha1 B1^2 + alpha2 B2^2, 1/2) are CUDA's pow, which may differ from glibc's in the last place.
+struct MHDMultiphysicsF64 {
+    static constexpr int NW = 16;
+    static constexpr int NU = 17;
+    static constexpr bool HAS_Y = false;
+    static constexpr bool HAS_SOURCE = false;
+    struct P {
+        double g[2], pinfk[2], ch2[2];  // per material (no member named pinf: the state check's floor is 0)
+    };
+    using R2 = EulerReducedF64;
+    using MR = MHDReducedF64;
+    __device__ static P params(const double* prm, double /*ch*/) {
+        return P{{prm[0], prm[2]}, {prm[1], prm[3]}, {prm[4] * prm[4], prm[5] * prm[5]}};
+    }
+    // computeConservedVariableVector (:165-220)
+    __device__ static void cons(const double* W, const P& q, double* U) {
+        const double a1 = R2::clamp_alpha(W[0]), a2 = 1.0 - a1;
+        const double u = W[1], v = W[2], w = W[3];
+        const double rho = (a1 * W[4]) + (a2 * W[10]);
+        U[0] = rho;
+        U[1] = rho * a1;
+        U[2] = rho * u;
+        U[3] = rho * v;
+        U[4] = rho * w;
+        const double v2 = ((u * u) + (v * v)) + (w * w);
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const double a = k == 0 ? a1 : a2;
+            const double* wk = W + 4 + 6 * k;
+            double* uk = U + 5 + 6 * k;
+            uk[0] = a * wk[0];
+            const double b2 = MR::b2_of(wk[2], wk[3], wk[4]);
+            const double h = wk[0] * ((0.5 * v2) + R2::e_of(wk[0], wk[1], q.g[k], q.pinfk[k]));
+            uk[1] = a * (h + (0.5 * b2));
+#pragma unroll
+            for (int i = 0; i < 3; i++) uk[2 + i] = pow(a, 1.0 / 2.0) * wk[2 + i];
+            uk[5] = a * wk[5];
+        }
+    }
+    // setConservedVariableVector (:84-133)
+    __device__ static void setcons(const double* U, const P& q, double* W) {
+        const double rho = U[0];
+        const double a1 = R2::clamp_alpha(U[1] / rho), a2 = 1.0 - a1;
+        const double u = U[2] / rho, v = U[3] / rho, w = U[4] / rho;
+        const double v2 = ((u * u) + (v * v)) + (w * w);
+        W[0] = a1;
+        W[1] = u;
+        W[2] = v;
+        W[3] = w;
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const double a = k == 0 ? a1 : a2;
+            double* wk = W + 4 + 6 * k;
+            const double* uk = U + 5 + 6 * k;
+            wk[0] = uk[0] / a;
+#pragma unroll
+            for (int i = 0; i < 3; i++) wk[2 + i] = uk[2 + i] / pow(a, 1.0 / 2.0);
+            const double b2 = MR::b2_of(wk[2], wk[3], wk[4]);
+            const double E = ((uk[1] / a) - (0.5 * b2)) / wk[0];
+            wk[1] = R2::p_of(wk[0], E - (0.5 * v2), q.g[k], q.pinfk[k]);
+            wk[5] = uk[5] / a;
+        }
+    }
+    // computeXFluxVector (:222-358); the model has no Y flux
+    template <int AXIS>
+    __device__ static void flux(const double* U, const P& q, double* F) {
+        static_assert(AXIS == 0, "the MHD multiphysics model is 1D");
+        const double rho = U[0];
+        const double a1 = R2::clamp_alpha(U[1] / rho), a2 = 1.0 - a1;
+        const double u = U[2] / rho, v = U[3] / rho, w = U[4] / rho;
+        double B[2][3];
+#pragma unroll
+        for (int k = 0; k < 2; k++)
+#pragma unroll
+            for (int i = 0; i < 3; i++) B[k][i] = U[7 + 6 * k + i] / pow(k == 0 ? a1 : a2, 1.0 / 2.0);
+        double ib2[3], ib[3];
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            ib2[i] = (a1 * (B[0][i] * B[0][i])) + (a2 * (B[1][i] * B[1][i]));
+            ib[i] = pow(ib2[i], 1.0 / 2.0);
+        }
+        const double v2 = ((u * u) + (v * v)) + (w * w);
+        double pk[2];
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const double a = k == 0 ? a1 : a2;
+            const double* uk = U + 5 + 6 * k;
+            double* fk = F + 5 + 6 * k;
+            const double r = uk[0] / a;
+            const double Et = uk[1] / a;
+            const double b2 = MR::b2_of(B[k][0], B[k][1], B[k][2]);
+            const double p = R2::p_of(r, ((Et - (0.5 * b2)) / r) - (0.5 * v2), q.g[k], q.pinfk[k]);
+            pk[k] = p;
+            const double bv = ((0.0 + (u * B[k][0])) + (v * B[k][1])) + (w * B[k][2]);
+            const double s = pow(a, 1.0 / 2.0);
+            fk[0] = a * (r * u);
+            fk[1] = (a * (((Et + p) + (0.5 * b2)) * u)) - (a * (bv * B[k][0]));
+            fk[2] = s * (uk[5] / a);
+            fk[3] = s * ((B[k][1] * u) - (B[k][0] * v));
+            fk[4] = s * ((B[k][2] * u) - (B[k][0] * w));
+            fk[5] = a * (q.ch2[k] * B[k][0]);
+        }
+        F[0] = rho * u;
+        F[1] = rho * (u * a1);
+        F[2] = (((rho * (u * u)) + ((a1 * pk[0]) + (a2 * pk[1]))) + (0.5 * ((ib2[0] + ib2[1]) + ib2[2]))) - ib2[0];
+        F[3] = (rho * (u * v)) - (ib[0] * ib[1]);
+        F[4] = (rho * (u * w)) - (ib[0] * ib[2]);
+    }
+    __device__ static void source(const double*, const P&, double* S) {
+#pragma unroll
+        for (int i = 0; i < NU; i++) S[i] = 0.0;
+    }
+    // MHDSolvers::computeMaximumWaveSpeed of the multiphysics model (Solvers/mhdsolvers.cpp:305-323): each material's
+    // fast magneto-acoustic speed at its own density, pressure and field
+    __device__ static double wave(const double* W, const P& q, int) {
+        const double f1 = fabs(MR::fast(W[4], W[5], W[6], W[7], W[8], q.g[0], q.pinfk[0], W[6]));
+        const double f2 = fabs(MR::fast(W[10], W[11], W[12], W[13], W[14], q.g[1], q.pinfk[1], W[12]));
+        return fabs(W[1]) + std_max(f1, f2);
+    }
+    // MHDMultiphysicsStateVector() (:3-27)
+    __device__ static void default_state(double* W) {
+        for (int i = 0; i < NW; i++) W[i] = 0.0;
+        W[0] = 0.999;
+        W[4] = 1.0;
+        W[5] = 1.0;
+        W[10] = 1.0;
+        W[11] = 1.0;
+    }
+    // bad-state check: finite values and positive material densities.  The trace material's pressure, and with it the
+    // volume-fraction mixture, goes below zero in the reference's own runs of this model (its Dumbser multimaterial
+    // layout at t = 0.05: mixture -2.9e-3), so no pressure is required positive.
+    __device__ static double density(const double* W) { return W[4] < W[10] ? W[4] : W[10]; }
+    __device__ static double pressure(const double* W) {
+        const double a1 = R2::clamp_alpha(W[0]);
+        return (a1 * W[5]) + ((1.0 - a1) * W[11]);
+    }
+    __device__ static bool positive_pressure(const P&) { return false; }
+};
+
 }  // namespace vg

@@ -106,6 +106,7 @@ const Ops kOps[V_COUNT] = {
     Ops{},  // V_HRED19: no mixed form
     Ops{},  // V_HINT20: no mixed form
     Ops{},  // V_HMPH32: no mixed form
+    Ops{},  // V_MMPH16: no mixed form
 };
 
 }  // namespace

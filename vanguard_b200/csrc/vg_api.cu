@@ -47,7 +47,8 @@ int ref_nvar(int model) {
     return model == VG_MODEL_EULER ? 6 : model == VG_MODEL_MHD ? 9 : model == VG_MODEL_HPR ? 17 : model == VG_MODEL_EULER_REDUCED ? 7
            : model == VG_MODEL_EULER_MULTIPHYSICS ? 8 : model == VG_MODEL_MHD_REDUCED ? 11
            : model == VG_MODEL_MHD_INTERMEDIATE ? 12 : model == VG_MODEL_HPR_REDUCED ? 19
-           : model == VG_MODEL_HPR_INTERMEDIATE ? 20 : model == VG_MODEL_HPR_MULTIPHYSICS ? 32 : 0;
+           : model == VG_MODEL_HPR_INTERMEDIATE ? 20 : model == VG_MODEL_HPR_MULTIPHYSICS ? 32
+           : model == VG_MODEL_MHD_MULTIPHYSICS ? 16 : 0;
 }
 
 // Reference plane carried in device plane k, per variant.
@@ -66,6 +67,7 @@ const int kPlanes[vg::V_COUNT][32] = {
     {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17, 18, 19},  // V_HINT20: every plane
     {0,  1,  2,  3,  4,  5,  6,  7,  8,  9,  10, 11, 12, 13, 14, 15,
      16, 17, 18, 19, 20, 21, 22, 23, 24, 25, 26, 27, 28, 29, 30, 31},  // V_HMPH32: every plane
+    {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15},  // V_MMPH16: every plane
 };
 
 }  // namespace
@@ -469,7 +471,7 @@ vg_status vg_create(const vg_grid_desc* desc, vg_solver** out) {
         desc->model != VG_MODEL_EULER_REDUCED && desc->model != VG_MODEL_EULER_MULTIPHYSICS &&
         desc->model != VG_MODEL_MHD_REDUCED && desc->model != VG_MODEL_MHD_INTERMEDIATE &&
         desc->model != VG_MODEL_HPR_REDUCED && desc->model != VG_MODEL_HPR_INTERMEDIATE &&
-        desc->model != VG_MODEL_HPR_MULTIPHYSICS)
+        desc->model != VG_MODEL_HPR_MULTIPHYSICS && desc->model != VG_MODEL_MHD_MULTIPHYSICS)
         return fail(VG_EUNSUPPORTED, "model not available in this build");
     if (desc->nx < 2 || desc->ny < 1 || (desc->ny > 1 && desc->ny < 2))
         return fail(VG_EINVAL, "grid needs at least 2 cells along every swept axis");
@@ -485,8 +487,11 @@ vg_status vg_create(const vg_grid_desc* desc, vg_solver** out) {
     if (desc->precision == VG_MIXED && (desc->model == VG_MODEL_HPR_REDUCED || desc->model == VG_MODEL_HPR_INTERMEDIATE ||
                                         desc->model == VG_MODEL_HPR_MULTIPHYSICS))
         return fail(VG_EUNSUPPORTED, "the HPR two-material models run in VG_FP64 only");
-    if (desc->model == VG_MODEL_HPR_MULTIPHYSICS && desc->ny != 1)
-        return fail(VG_EUNSUPPORTED, "the HPR multiphysics two-material model is 1D (ny = 1), as the reference's is");
+    if ((desc->model == VG_MODEL_HPR_MULTIPHYSICS || desc->model == VG_MODEL_MHD_MULTIPHYSICS) && desc->ny != 1)
+        return fail(VG_EUNSUPPORTED, "the multiphysics two-material models of HPR and MHD are 1D (ny = 1), as the "
+                                     "reference's are");
+    if (desc->precision == VG_MIXED && desc->model == VG_MODEL_MHD_MULTIPHYSICS)
+        return fail(VG_EUNSUPPORTED, "the MHD two-material models run in VG_FP64 only");
     if (desc->model == VG_MODEL_HPR) {
         const double eos = desc->params[12];
         if (eos != 0.0 && eos != 1.0 && eos != 2.0)
@@ -501,7 +506,8 @@ vg_status vg_create(const vg_grid_desc* desc, vg_solver** out) {
     s->max_nw = desc->model == VG_MODEL_EULER ? 4 : desc->model == VG_MODEL_MHD ? 9 : desc->model == VG_MODEL_EULER_REDUCED ? 6
                 : desc->model == VG_MODEL_EULER_MULTIPHYSICS ? 7 : desc->model == VG_MODEL_MHD_REDUCED ? 11
                 : desc->model == VG_MODEL_MHD_INTERMEDIATE ? 12 : desc->model == VG_MODEL_HPR_REDUCED ? 19
-                : desc->model == VG_MODEL_HPR_INTERMEDIATE ? 20 : desc->model == VG_MODEL_HPR_MULTIPHYSICS ? 32 : 17;
+                : desc->model == VG_MODEL_HPR_INTERMEDIATE ? 20 : desc->model == VG_MODEL_HPR_MULTIPHYSICS ? 32
+                : desc->model == VG_MODEL_MHD_MULTIPHYSICS ? 16 : 17;
     s->pitch = ((long)desc->nx + 31) / 32 * 32;  // 256-byte aligned rows
     s->plane = s->pitch * desc->ny;
     s->floor5 = std::pow(10.0, -5.0);  // SlopeLimiters::computeSlopeVector's floor (Solvers/slopelimiters.cpp:232-239)
@@ -581,6 +587,8 @@ vg_status vg_upload_primitive(vg_solver* s, const double* planes, int is_device,
         variant = vg::V_HINT20;
     } else if (model == VG_MODEL_HPR_MULTIPHYSICS) {
         variant = vg::V_HMPH32;
+    } else if (model == VG_MODEL_MHD_MULTIPHYSICS) {
+        variant = vg::V_MMPH16;
     } else if (model == VG_MODEL_HPR) {
         // a solid equation of state or plasticity selects the instantiation that carries them
         variant = (s->d.params[12] != 0.0 || s->d.params[17] != 0.0) ? vg::V_HPR17S : vg::V_HPR17;
@@ -699,15 +707,18 @@ vg_status vg_run(vg_solver* s, const vg_run_config* cfg, int* steps_taken, doubl
     if (cfg->max_steps <= 0 && !(cfg->t_end > 0.0)) return fail(VG_EINVAL, "need t_end > 0 or max_steps > 0");
     if (cfg->subcycles < 0) return fail(VG_EINVAL, "subcycles must be >= 0");
     // HPRSecondOrderSolver::solve of the HPR multiphysics model takes subcyclingIterations and runs an empty loop
-    // (Solvers/hprsecondordersolver.cpp:368-373, :378-383): accepted and ignored, as there
-    if (cfg->subcycles > 0 && !s->ops->forcing && s->d.model != VG_MODEL_HPR_MULTIPHYSICS)
+    // (Solvers/hprsecondordersolver.cpp:368-373, :378-383); MHDSecondOrderSolver::solve of the MHD multiphysics model
+    // takes subcyclingIterations and reinitialisationFrequency and uses neither (Solvers/mhdsecondordersolver.cpp:
+    // 362-385): accepted and ignored, as there
+    const bool multiphysics = s->d.model == VG_MODEL_HPR_MULTIPHYSICS || s->d.model == VG_MODEL_MHD_MULTIPHYSICS;
+    if (cfg->subcycles > 0 && !s->ops->forcing && !multiphysics)
         return fail(VG_EUNSUPPORTED, "source sub-cycling needs a model with a source (HPR relaxation, MHD GLM damping)");
     if (cfg->order != 0 && cfg->order != 1 && cfg->order != 2) return fail(VG_EINVAL, "order must be 1 or 2");
     if (cfg->order == 1 && !s->ops->x1) return fail(VG_EUNSUPPORTED, "this kernel form has no first-order loop");
     if (cfg->stiff_source && cfg->order != 1 && !s->ops->relax)
         return fail(VG_EUNSUPPORTED, "the stiff source relaxation exists for the HPR model only");
     if (cfg->reinit_frequency < 0) return fail(VG_EINVAL, "reinit_frequency must be >= 0");
-    if (cfg->reinit_frequency > 0 && (!s->ops->reinit || cfg->order == 1))
+    if (cfg->reinit_frequency > 0 && (!s->ops->reinit || cfg->order == 1) && s->d.model != VG_MODEL_MHD_MULTIPHYSICS)
         return fail(VG_EUNSUPPORTED, "volume-fraction reinitialisation belongs to the reduced two-material model's "
                                      "second-order loop");
     if (cfg->stiff_source && cfg->order != 1 && s->d.params[17] != 0.0)

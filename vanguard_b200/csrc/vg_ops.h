@@ -25,7 +25,8 @@ enum Variant : int {
     V_HRED19 = 10,  // HPR reduced two-material: alpha1, p, A(9), u, v, w, Jx, Jy, Jz, rho1, rho2
     V_HINT20 = 11,  // HPR intermediate two-material: alpha1, A(9), u, v, w, Jx, Jy, Jz, rho1, p1, rho2, p2
     V_HMPH32 = 12,  // HPR multiphysics two-material (1D): alpha1, u, v, w, rho1, p1, A1(9), J1(3), rho2, p2, A2(9), J2(3)
-    V_COUNT = 13
+    V_MMPH16 = 13,  // MHD multiphysics two-material (1D): alpha1, u, v, w, rho1, p1, B1(3), psi1, rho2, p2, B2(3), psi2
+    V_COUNT = 14
 };
 
 struct Ops {

@@ -76,7 +76,8 @@ void run_planes(int model, std::vector<double>& planes, int nx, int ny, const do
     // two-material models have no mixed form
     const bool exact = order == 1 || model == VG_MODEL_EULER_MULTIPHYSICS || model == VG_MODEL_MHD_REDUCED ||
                        model == VG_MODEL_MHD_INTERMEDIATE || model == VG_MODEL_HPR_REDUCED ||
-                       model == VG_MODEL_HPR_INTERMEDIATE || model == VG_MODEL_HPR_MULTIPHYSICS;
+                       model == VG_MODEL_HPR_INTERMEDIATE || model == VG_MODEL_HPR_MULTIPHYSICS ||
+                       model == VG_MODEL_MHD_MULTIPHYSICS;
     SolverPtr s = make_solver(model, nx, ny, VG_TRANSMISSIVE, params, nparams, exact ? VG_FP64 : -1);
     vg_run_config c{};
     c.dx = dx;
@@ -1152,4 +1153,55 @@ vector<HPRMultiphysicsStateVector> HPRFirstOrderSolver::solve(vector<HPRMultiphy
     run_planes(VG_MODEL_HPR_MULTIPHYSICS, p, (int)initialCells.size(), 1, prm, 22, dx, cfl, tEnd, 0.0, 0, 0, maxSteps,
                1, 0);
     return unpack<HPRMultiphysicsStateVector>(p, initialCells.size(), 32, hmph_make);
+}
+
+// ---------------------------------------------------------------------------------- MHD multiphysics model
+// MHDMultiphysicsStateVector() (MHD/Multiphysics/mhdmultiphysicsstatevector.cpp:3-27)
+MHDMultiphysicsStateVector::MHDMultiphysicsStateVector()
+    : w_{0.999, 0.0, 0.0, 0.0, 1.0, 1.0, 0.0, 0.0, 0.0, 0.0, 1.0, 1.0, 0.0, 0.0, 0.0, 0.0} {}
+MHDMultiphysicsStateVector::MHDMultiphysicsStateVector(double a1, double u, double v, double w, double r1, double p1,
+                                                       double b1x, double b1y, double b1z, double psi1, double r2,
+                                                       double p2, double b2x, double b2y, double b2z, double psi2)
+    : w_{a1, u, v, w, r1, p1, b1x, b1y, b1z, psi1, r2, p2, b2x, b2y, b2z, psi2} {}
+void MHDMultiphysicsStateVector::setPrimitiveVariableVector(vector<double> w) {
+    for (int i = 0; i < 16; i++) w_[i] = w[i];
+}
+
+namespace {
+void mmph_get(const MHDMultiphysicsStateVector& c, double* w) { std::memcpy(w, c.data(), sizeof(double) * 16); }
+MHDMultiphysicsStateVector mmph_make(const double* w) {
+    MHDMultiphysicsStateVector s;
+    std::memcpy(s.data(), w, sizeof(double) * 16);
+    return s;
+}
+// {gamma1, p_inf1, gamma2, p_inf2, c_h1, c_h2}
+void mmph_params(const MHDMaterialParameters& m1, const MHDMaterialParameters& m2, double* prm) {
+    prm[0] = m1.getAdiabaticIndex(), prm[1] = m1.getStiffeningParameter();
+    prm[2] = m2.getAdiabaticIndex(), prm[3] = m2.getStiffeningParameter();
+    prm[4] = m1.getHyperbolicWaveSpeed(), prm[5] = m2.getHyperbolicWaveSpeed();
+}
+}  // namespace
+
+vector<MHDMultiphysicsStateVector> MHDSecondOrderSolver::solve(vector<MHDMultiphysicsStateVector>& initialCells,
+                                                               double dx, double cfl, double tEnd, double bias,
+                                                               int limiter, int subcycles, int reinit,
+                                                               MHDMaterialParameters m1, MHDMaterialParameters m2,
+                                                               int maxSteps) {
+    double prm[6];
+    mmph_params(m1, m2, prm);
+    std::vector<double> p = pack(initialCells, 16, mmph_get);
+    run_planes(VG_MODEL_MHD_MULTIPHYSICS, p, (int)initialCells.size(), 1, prm, 6, dx, cfl, tEnd, bias, limiter,
+               subcycles, maxSteps, 2, reinit);
+    return unpack<MHDMultiphysicsStateVector>(p, initialCells.size(), 16, mmph_make);
+}
+vector<MHDMultiphysicsStateVector> MHDFirstOrderSolver::solve(vector<MHDMultiphysicsStateVector>& initialCells,
+                                                              double dx, double cfl, double tEnd, int,
+                                                              MHDMaterialParameters m1, MHDMaterialParameters m2,
+                                                              int maxSteps) {
+    double prm[6];
+    mmph_params(m1, m2, prm);
+    std::vector<double> p = pack(initialCells, 16, mmph_get);
+    run_planes(VG_MODEL_MHD_MULTIPHYSICS, p, (int)initialCells.size(), 1, prm, 6, dx, cfl, tEnd, 0.0, 0, 0, maxSteps,
+               1, 0);
+    return unpack<MHDMultiphysicsStateVector>(p, initialCells.size(), 16, mmph_make);
 }

@@ -243,6 +243,33 @@ private:
     double w_[12];
 };
 
+// MHDMultiphysicsStateVector (MHD/Multiphysics/mhdmultiphysicsstatevector.h; 1D): the MHD multiphysics two-material
+// state, primitives alpha1, u, v, w, rho1, p1, B1 (3), psi1, rho2, p2, B2 (3), psi2.
+class MHDMultiphysicsStateVector {
+public:
+    MHDMultiphysicsStateVector();
+    MHDMultiphysicsStateVector(double newMaterial1VolumeFraction, double newInterfaceXVelocity,
+                               double newInterfaceYVelocity, double newInterfaceZVelocity, double newMaterial1Density,
+                               double newMaterial1Pressure, double newMaterial1XMagneticField,
+                               double newMaterial1YMagneticField, double newMaterial1ZMagneticField,
+                               double newMaterial1AuxiliaryField, double newMaterial2Density, double newMaterial2Pressure,
+                               double newMaterial2XMagneticField, double newMaterial2YMagneticField,
+                               double newMaterial2ZMagneticField, double newMaterial2AuxiliaryField);
+    void setPrimitiveVariableVector(vector<double> w);
+    vector<double> computePrimitiveVariableVector() const { return vector<double>(w_, w_ + 16); }
+    double getMaterial1VolumeFraction() const { return w_[0]; }
+    double getInterfaceXVelocity() const { return w_[1]; }
+    double getMaterial1Density() const { return w_[4]; }
+    double getMaterial1Pressure() const { return w_[5]; }
+    double getMaterial2Density() const { return w_[10]; }
+    double getMaterial2Pressure() const { return w_[11]; }
+    double* data() { return w_; }
+    const double* data() const { return w_; }
+
+private:
+    double w_[16];
+};
+
 // --------------------------------------------------------------------------------------------------- HPR
 class HPRMaterialParameters {
 public:
@@ -564,6 +591,14 @@ public:
                                                           int reinitialisationFrequency,
                                                           MHDMaterialParameters material1Parameters,
                                                           MHDMaterialParameters material2Parameters, int maxSteps);
+    // the MHD multiphysics two-material model, 1D (Solvers/mhdsecondordersolver.cpp:362-385): no source, no
+    // reinitialisation, each material's c_h as given; exact form; maxSteps > 0 also stops after that many steps
+    static vector<MHDMultiphysicsStateVector> solve(vector<MHDMultiphysicsStateVector>& initialCells,
+                                                    double cellSpacing, double CFLCoefficient, double finalTime,
+                                                    double bias, int slopeLimiter, int subcyclingIterations,
+                                                    int reinitialisationFrequency,
+                                                    MHDMaterialParameters material1Parameters,
+                                                    MHDMaterialParameters material2Parameters, int maxSteps = 0);
     // the MHD intermediate two-material model (Solvers/mhdsecondordersolver.cpp:387-440, :552-...), exact form; 2D
     // with mirror ghosts on every side (the reference's own 2D padding of this model misfills its outermost bottom row)
     static vector<MHDIntermediateStateVector> solve(vector<MHDIntermediateStateVector>& initialCells,
@@ -600,6 +635,12 @@ public:
 
 class MHDFirstOrderSolver {
 public:
+    // the MHD multiphysics model, 1D (Solvers/mhdfirstordersolver.cpp:480-…); maxSteps > 0 also stops after that
+    // many steps (not in the reference)
+    static vector<MHDMultiphysicsStateVector> solve(vector<MHDMultiphysicsStateVector>& initialCells, double cellSpacing,
+                                                    double CFLCoefficient, double finalTime, int subcyclingIterations,
+                                                    MHDMaterialParameters material1Parameters,
+                                                    MHDMaterialParameters material2Parameters, int maxSteps = 0);
     static vector<MHDStateVector> solve(vector<MHDStateVector>& initialCells, double cellSpacing, double CFLCoefficient,
                                         double finalTime, int subcyclingIterations, MHDMaterialParameters mp);
     static vector<vector<MHDStateVector> > solve2D(vector<vector<MHDStateVector> >& initialCells, double cellSpacing,

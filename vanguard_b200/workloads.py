@@ -459,3 +459,32 @@ def hpr_multiphysics_from_reduced(W, p2_scale=1.0, a2_scale=1.0):
 def hpr_multiphysics_riemann(nx, seed=0, distortion=0.02, heat=0.05, p2_scale=1.0, a2_scale=1.0):
     """hpr_reduced_riemann's 1D two-material HPR Riemann problem in the multiphysics model's planes, shape (32, nx)."""
     return hpr_multiphysics_from_reduced(hpr_reduced_riemann(nx, 1, seed, distortion, heat), p2_scale, a2_scale)
+
+
+MHD_MULTIPHYSICS_NVAR = 16  # alpha1, u, v, w, rho1, p1, B1 (3), psi1, rho2, p2, B2 (3), psi2
+
+
+def mhd_multiphysics_params(gamma1=2.0, p_inf1=0.0, gamma2=2.0, p_inf2=0.0, c_h1=0.0, c_h2=0.0):
+    """The two MHDMaterialParameters of the MHD multiphysics model: (gamma1, p_inf1, gamma2, p_inf2, c_h1, c_h2).  The
+    reference's solve leaves each material's hyperbolic wave speed as given (0 from MHDMaterialParameters(gamma))."""
+    return np.array([gamma1, p_inf1, gamma2, p_inf2, c_h1, c_h2])
+
+
+def mhd_multiphysics_dumbser_1d(n, seed=None, noise=0.0):
+    """MHDMultiphysicsTests::solveDumbserTest1's layout (MHD/Multiphysics/mhdmultiphysicstests.cpp:7-26): material 1
+    (rho 1, p 1, B (0.75, 1, 0)) and material 2 (rho 0.125, p 0.1, B (0.75, -1, 0)) in every cell, alpha1 0.999 at
+    i <= n/2 and 0.001 to the right; optionally seeded noise of relative amplitude `noise` on the velocities, densities,
+    pressures, fields and GLM scalars."""
+    left = np.arange(n) <= 0.5 * n
+    W = np.zeros((MHD_MULTIPHYSICS_NVAR, n))
+    W[0] = np.where(left, 0.999, 0.001)
+    W[4:10] = np.array([1.0, 1.0, 0.75, 1.0, 0.0, 0.0])[:, None]
+    W[10:16] = np.array([0.125, 0.1, 0.75, -1.0, 0.0, 0.0])[:, None]
+    if noise:
+        rng = np.random.default_rng(seed)
+        W[1:4] = noise * rng.standard_normal((3, n))
+        for k in (4, 5, 6, 7, 8, 10, 11, 12, 13, 14):
+            W[k] *= 1.0 + noise * rng.standard_normal(n)
+        W[9] = noise * rng.standard_normal(n)
+        W[15] = noise * rng.standard_normal(n)
+    return W
