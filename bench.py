@@ -751,7 +751,9 @@ def sod_leg(local, stream, sh):
 
 TM_N, TM_STEPS, TM_REINIT = 2048, 100, 10
 CPU_LEGS = True  # run_cuda clears it unless this is rank 0 of a 1-GPU run with the CPU baseline on
-TM_MODELS = None  # all four; a comma list names a subset (profiling only)
+TM_MODELS = None  # all of them; a comma list names a subset (profiling only)
+TM_HPR_N, TM_HPR_STEPS = 1024, 20  # the HPR two-material models in 2D (19-20 planes, RK4 relaxation sub-cycle)
+TM_1D_CELLS = 1 << 20  # the 1D-only multiphysics models (HPR multiphysics, MHD multiphysics)
 
 
 def two_material_leg(local, stream, sh, n=TM_N, steps=TM_STEPS, models=None):
@@ -759,7 +761,11 @@ def two_material_leg(local, stream, sh, n=TM_N, steps=TM_STEPS, models=None):
     MHDReducedTests' Dumbser disc; gamma 1.4 | 1.67), superbee, CFL 0.8, `steps` steps with the volume fraction
     reinitialised every TM_REINIT steps and one GLM damping sub-cycle for the MHD models: exact FP64 form (and the
     mixed form where the model has one), CUDA events on the launching stream; beside each, the compiled reference's
-    per-step loop on a strip of the same grid on the host cores (its CPU baseline)."""
+    per-step loop on a strip of the same grid on the host cores (its CPU baseline).  The HPR reduced and intermediate
+    models run an elastic | plastic pair of ShockMieGruneisen solids in the layout of the reference's Zhang scenario
+    (its deformation gradients and velocities) on TM_HPR_N^2 for TM_HPR_STEPS steps with one RK4 relaxation sub-cycle;
+    the 1D-only multiphysics models run the same solids (HPR) and the Dumbser layout (MHD) on TM_1D_CELLS cells, the
+    reference's sample being a TM_1D_CELLS / 64 cell segment about the interface."""
     import torch
     import oracle as O
     import vanguard_b200 as vg
@@ -769,12 +775,30 @@ def two_material_leg(local, stream, sh, n=TM_N, steps=TM_STEPS, models=None):
     mh = wl.mhd_reduced_params(1.4, 0.0, 1.67, 0.0)
     bubble, disc = wl.reduced_bubble_2d(n), wl.mhd_reduced_dumbser_2d(n)
     cases = [
-        ("euler_reduced", vg.EULER_REDUCED, O.EULER_REDUCED, bubble, eu, 0, ("fp64", "mixed")),
-        ("euler_multiphysics", vg.EULER_MULTIPHYSICS, O.EULER_MULTIPHYSICS, wl.multiphysics_from_reduced(bubble), eu, 0,
-         ("fp64",)),
-        ("mhd_reduced", vg.MHD_REDUCED, O.MHD_REDUCED, disc, mh, 1, ("fp64",)),
-        ("mhd_intermediate", vg.MHD_INTERMEDIATE, O.MHD_INTERMEDIATE, wl.mhd_intermediate_from_reduced(disc), mh, 1,
-         ("fp64",)),
+        ("euler_reduced", vg.EULER_REDUCED, O.EULER_REDUCED, lambda: bubble, eu, 0, ("fp64", "mixed"), n, n, steps),
+        ("euler_multiphysics", vg.EULER_MULTIPHYSICS, O.EULER_MULTIPHYSICS, lambda: wl.multiphysics_from_reduced(bubble),
+         eu, 0, ("fp64",), n, n, steps),
+        ("mhd_reduced", vg.MHD_REDUCED, O.MHD_REDUCED, lambda: disc, mh, 1, ("fp64",), n, n, steps),
+        ("mhd_intermediate", vg.MHD_INTERMEDIATE, O.MHD_INTERMEDIATE, lambda: wl.mhd_intermediate_from_reduced(disc),
+         mh, 1, ("fp64",), n, n, steps),
+    ]
+    hn, hs, m1d = TM_HPR_N, TM_HPR_STEPS, TM_1D_CELLS
+    # two ShockMieGruneisen solids, elastic | plastic, in the layout of the reference's Zhang scenario of these models
+    s1 = wl.hpr_shock_mg_params(tau1=0.05)
+    s2 = wl.hpr_shock_mg_params(plastic=True, sigma0=1.0, n=1.0, tau1=1.0)
+    hp = wl.hpr_two_params(s1, s2)
+    zv = ((0.0, 0.2, 0.1), (0.0, -0.03, -0.01))
+    cases += [
+        ("hpr_reduced", vg.HPR_REDUCED, O.HPR_REDUCED,
+         lambda: wl.hpr_two_solid_riemann(hn, s1, s2, *wl.ZHANG_F, *zv, ny=hn), hp, 1, ("fp64",), hn, hn, hs),
+        ("hpr_intermediate", vg.HPR_INTERMEDIATE, O.HPR_INTERMEDIATE,
+         lambda: wl.hpr_intermediate_from_reduced(wl.hpr_two_solid_riemann(hn, s1, s2, *wl.ZHANG_F, *zv, ny=hn)), hp,
+         1, ("fp64",), hn, hn, hs),
+        ("hpr_multiphysics", vg.HPR_MULTIPHYSICS, O.HPR_MULTIPHYSICS,
+         lambda: wl.hpr_multiphysics_from_reduced(wl.hpr_two_solid_riemann(m1d, s1, s2, *wl.ZHANG_F, *zv)), hp, 0,
+         ("fp64",), m1d, 1, steps),
+        ("mhd_multiphysics", vg.MHD_MULTIPHYSICS, O.MHD_MULTIPHYSICS, lambda: wl.mhd_multiphysics_dumbser_1d(m1d),
+         wl.mhd_multiphysics_params(1.4, 0.0, 1.67, 0.0), 0, ("fp64",), m1d, 1, steps),
     ]
     if models:  # profiling runs of a subset
         cases = [c for c in cases if c[0] in models]
@@ -782,36 +806,44 @@ def two_material_leg(local, stream, sh, n=TM_N, steps=TM_STEPS, models=None):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     cores = O.ref().vgref_set_threads(0) if (CPU_LEGS and O.ref_available()) else 0
     out = {"workload": f"2D {n}x{n}, gamma 1.4 | 1.67, superbee, CFL 0.8, {steps} steps, reinitialisation every "
-                       f"{TM_REINIT} steps, MHD models with 1 GLM sub-cycle"}
-    for name, model, omodel, W, prm, sub, forms in cases:
-        res = {}
+                       f"{TM_REINIT} steps, MHD models with 1 GLM sub-cycle; HPR reduced and intermediate 2D {hn}x{hn} "
+                       f"ShockMieGruneisen solids elastic | plastic, {hs} steps, 1 RK4 relaxation sub-cycle; HPR and "
+                       f"MHD multiphysics 1D {m1d} cells, {steps} steps"}
+    for name, model, omodel, make, prm, sub, forms, nx, ny, nsteps in cases:
+        W = make()
+        dx = 1.0 / nx
+        res = {"grid": [nx, ny], "steps": nsteps}
         for form in forms:
-            with vg.Solver(model, n, n, prm, precision=precisions[form], device=local) as s:
+            with vg.Solver(model, nx, ny, prm, precision=precisions[form], device=local) as s:
                 s.upload(W, stream=sh)
-                s.autotune(1.0 / n, CFL, limiter=LIMITER, stream=sh)
-                s.run(1.0 / n, CFL, steps=3, limiter=LIMITER, subcycles=sub, reinit=TM_REINIT, stream=sh,
-                      allow_nan=True)
+                s.autotune(dx, CFL, limiter=LIMITER, stream=sh)
+                s.run(dx, CFL, steps=3, limiter=LIMITER, subcycles=sub, reinit=TM_REINIT, stream=sh, allow_nan=True)
                 s.upload(W, stream=sh)
                 torch.cuda.synchronize()
                 e0.record(stream)
-                s.run(1.0 / n, CFL, steps=steps, limiter=LIMITER, subcycles=sub, reinit=TM_REINIT, stream=sh,
+                s.run(dx, CFL, steps=nsteps, limiter=LIMITER, subcycles=sub, reinit=TM_REINIT, stream=sh,
                       allow_nan=True)
                 e1.record(stream)
                 torch.cuda.synchronize()
                 ms = e0.elapsed_time(e1)
                 final = s.download(stream=sh)
-            res[form] = {"ms": ms, "cell_updates_per_s": n * n * steps / (ms / 1e3),
+            res[form] = {"ms": ms, "cell_updates_per_s": nx * ny * nsteps / (ms / 1e3),
                          "finite": bool(np.isfinite(final).all())}
         if cores:
-            rows = 16
-            strip = np.ascontiguousarray(W[:, n // 2 - rows // 2: n // 2 + rows // 2, :])
+            if ny > 1:
+                rows = 4 if name.startswith("hpr") else 16  # the reference's HPR models run ~3e3 cell-updates/s
+                strip = np.ascontiguousarray(W[:, ny // 2 - rows // 2: ny // 2 + rows // 2, :])
+                what = f"a {nx}x{rows} strip"
+            else:
+                seg = nx // 64
+                strip = np.ascontiguousarray(W[:, nx // 2 - seg // 2: nx // 2 + seg // 2])
+                what = f"a {seg}-cell segment about the interface"
             t0 = time.perf_counter()
-            O.run_two_material(omodel, strip, 1.0 / n, CFL, steps=2, limiter=LIMITER, params=prm, reinit=TM_REINIT,
+            O.run_two_material(omodel, strip, dx, CFL, steps=2, limiter=LIMITER, params=prm, reinit=TM_REINIT,
                                subcycles=sub, reference=True, threads=cores)
             dt = time.perf_counter() - t0
-            res["cpu_baseline"] = {"value": n * rows * 2 / dt, "unit": UNIT, "cores": cores, "kind": "reference",
-                                   "sample": f"2 steps of the reference per-step loop on a {n}x{rows} strip "
-                                             f"({dt:.2f} s)"}
+            res["cpu_baseline"] = {"value": strip[0].size * 2 / dt, "unit": UNIT, "cores": cores, "kind": "reference",
+                                   "sample": f"2 steps of the reference per-step loop on {what} ({dt:.2f} s)"}
             res["fp64_vs_cpu_reference"] = res["fp64"]["cell_updates_per_s"] / res["cpu_baseline"]["value"]
         out[name] = res
     return out

@@ -86,7 +86,7 @@ typedef enum vg_boundary { VG_TRANSMISSIVE = 0, VG_PERIODIC = 1 } vg_boundary;
  * any other value minbee. */
 enum { VG_SUPERBEE = 0, VG_VANLEER = 1, VG_MINBEE = 2 };
 
-#define VG_MAX_PARAMS 24
+#define VG_MAX_PARAMS 48
 
 /* Material parameter blocks (params[] below):
  *   Euler: {gamma, p_inf, c_v, E0, T_ign, rate}   EulerMaterialParameters (Euler/eulermaterialparameters.h)
@@ -107,9 +107,8 @@ enum { VG_SUPERBEE = 0, VG_VANLEER = 1, VG_MINBEE = 2 };
  *                                                 relaxation with transition stress sigma0 and power-law index n
  *                                                 (HPR/hprsourceterms.cpp:12-23).
  *   MHD multiphysics: {gamma1, p_inf1, gamma2, p_inf2, c_h1, c_h2}   each material's c_h stays as given
- *   HPR reduced, intermediate, multiphysics: 11 per material, material k at params[11 k]: {gamma, p_inf, c_v, rho0, T0, c_s,
- *                alpha, tau1, tau2, T_ref, is_thermal}   the two materials' StiffenedGas HPRMaterialParameters (elastic
- *                relaxation)
+ *   HPR reduced, intermediate, multiphysics: the HPR block above for each material, material k at params[20 k]
+ *                (40 values): any equation of state, elastic or plastic
  * The last slot is reserved. */
 typedef struct vg_grid_desc {
     int model;                        /* vg_model */

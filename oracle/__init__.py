@@ -136,7 +136,7 @@ def ref():
 
 # ------------------------------------------------------------------------------------ restatement
 
-NPARAMS = 24  # size of every parameter block handed to the C libraries (VG_MAX_PARAMS)
+NPARAMS = 48  # size of every parameter block handed to the C libraries (VG_MAX_PARAMS)
 
 
 def _params(params):

@@ -967,17 +967,12 @@ extern "C" double vgref_mhd_intermediate_run(double* planes, int nx, int ny, dou
 
 // ------------------------------------------------------------------------------------ HPR reduced two-material
 // Planes: the 19 primitives of HPRReducedStateVector (alpha1, p, A(9), u, v, w, Jx, Jy, Jz, rho1, rho2;
-// HPR/Multiphysics/hprreducedstatevector.cpp:154-185).  prm packs 11 values per material, material k at prm[11 k]:
-// {gamma, p_inf, c_v, rho0, T0, c_s, alpha, tau1, tau2, T_ref, is_thermal} of a StiffenedGas HPRMaterialParameters.
+// HPR/Multiphysics/hprreducedstatevector.cpp:154-185).  prm holds each material's HPRMaterialParameters as the 20-value
+// block of hprParams, material k at prm[20 k].
 // max_steps <= 0: the reference's own HPRSecondOrderSolver::solve{,2D} to t_end (Solvers/hprsecondordersolver.cpp:
 // 452-..., :604-...); else its per-step functions for max_steps steps in solve's order: the RK4 forcing sub-cycles
 // around the sweeps and the reinitialisation every reinit_freq steps.
-static HPRMaterialParameters hredParams(const double* prm, int k) {
-    double b[20] = {0.0};
-    for (int i = 0; i < 10; i++) b[i] = prm[11 * k + i];
-    b[11] = prm[11 * k + 10];
-    return hprParams(b);
-}
+static HPRMaterialParameters hredParams(const double* prm, int k) { return hprParams(prm + 20 * k); }
 template <class SV>
 static SV hprTwoCell(const double* planes, long plane, long k, int nw, HPRMaterialParameters& m1,
                      HPRMaterialParameters& m2) {

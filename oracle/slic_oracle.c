@@ -1180,18 +1180,19 @@ static void mint_default(const double* prm, double* W) {
     W[0] = 0.999; W[4] = 1.0; W[5] = 1.0; W[6] = 1.0; W[7] = 1.0;
 }
 
-/* ---- HPR reduced two-material model: HPR/Multiphysics/hprreducedstatevector.cpp.  Both materials are StiffenedGas
- * (elastic strain relaxation); prm packs 11 values per material, material k at prm[11 k]: {gamma, p_inf, c_v, rho0, T0,
- * c_s, alpha, tau1, tau2, T_ref, is_thermal}, expanded into the single-material HPR block for the shared functions.
+/* ---- HPR reduced two-material model: HPR/Multiphysics/hprreducedstatevector.cpp.  prm holds the two materials'
+ * HPRMaterialParameters as the single-material 20-value block each, material k at prm[20 k] ({gamma, p_inf, c_v, rho0,
+ * T0, c_s, alpha, tau1, tau2, T_ref, p_ref, is_thermal, eos, Gamma0, c0, s, alpha_eos, is_plastic, sigma0, n}): any
+ * equation of state of HPRMieGruneisen, elastic or plastic, as the reference's scenarios of these models use
+ * (GodunovRomenski solids, HPR/Multiphysics/hprreducedtests.cpp).
  * W = alpha1, p, A (9, row-major), u, v, w, Jx, Jy, Jz, rho1, rho2 (the reference's primitive order, :154-185) and an
  * unused twentieth plane; U = rho, rho alpha1, rho E, A, rho u (3), rho J (3), alpha1 rho1, alpha2 rho2 (:187-231).
  * J is carried when either material is thermal (:104-109).  Every volume fraction is clamped to [0.001, 0.999]. */
 static void hred_mat(const double* prm, int k, double* b) {
     for (int i = 0; i < 24; i++) b[i] = 0.0;
-    for (int i = 0; i < 10; i++) b[i] = prm[11 * k + i];
-    b[11] = prm[11 * k + 10];
+    for (int i = 0; i < 20; i++) b[i] = prm[20 * k + i];
 }
-static int hred_thermal(const double* prm) { return prm[10] != 0.0 || prm[21] != 0.0; }
+static int hred_thermal(const double* prm) { return prm[11] != 0.0 || prm[31] != 0.0; }
 /* computeConservedVariableVector (:187-231): the state's volume fraction is clamped first; the total energy is the
  * volume-fraction mean of each material's HPREquationOfState::computeTotalEnergy at the mixture density */
 static void hred_cons(const double* W, const double* prm, double* U) {
@@ -1368,7 +1369,7 @@ static void hred_drop_cold_heat_flux(int id, double* planes, long n, const doubl
 
 /* ---- HPR intermediate two-material model: HPR/Multiphysics/hprintermediatestatevector.cpp.  Each material carries
  * its own density, pressure and total energy; the distortion, velocity and heat flux are shared.  prm as for the
- * reduced model (11 values per material).
+ * reduced model (the 20-value block of each material).
  * W = alpha1, A (9, row-major), u, v, w, Jx, Jy, Jz, rho1, p1, rho2, p2 (:161-193) and an unused twenty-first plane;
  * U = rho, rho alpha1, A, rho u (3), rho J (3), alpha1 rho1, alpha1 rho1 E1, alpha2 rho2, alpha2 rho2 E2 (:195-247).
  * Each material's EOS terms take that material's own density and pressure. */
@@ -1556,12 +1557,12 @@ static void hint_default(const double* prm, double* W) {
 }
 /* ---- HPR multiphysics two-material model: HPR/Multiphysics/hprmultiphysicsstatevector.cpp (1D only in the
  * reference).  Each material carries its own density, pressure, distortion tensor and heat flux; the velocity is
- * shared.  prm as for the reduced model (11 values per material); each material's J is carried when that material is
- * thermal.  The distortion enters the conserved vector as pow(alpha_k, 1/3) A_k.
+ * shared.  prm as for the reduced model (the 20-value block of each material); each material's J is carried when that
+ * material is thermal.  The distortion enters the conserved vector as pow(alpha_k, 1/3) A_k.
  * W = alpha1, u, v, w, rho1, p1, A1 (9), J1 (3), rho2, p2, A2 (9), J2 (3) (:204-249) and an unused plane;
  * U = rho, rho alpha1, rho u (3), alpha1 rho1, alpha1 rho1 E1, alpha1^(1/3) A1, alpha1 rho1 J1, then the same five
  * groups of material 2 from 19 (:251-317). */
-static int hmph_thermal(const double* prm, int k) { return prm[11 * k + 10] != 0.0; }
+static int hmph_thermal(const double* prm, int k) { return prm[20 * k + 11] != 0.0; }
 /* computeConservedVariableVector (:251-317) */
 static void hmph_cons(const double* W, const double* prm, double* U) {
     double a1 = red_clamp(W[0]), a2 = 1.0 - a1;
@@ -1961,7 +1962,7 @@ static const model* model_of(int id) {
 
 int vo_nvar(int id) { const model* m = model_of(id); return m ? m->nv : 0; }
 int vo_nparams(int id) {
-    return id == VO_EULER ? 6 : id == VO_MHD ? 3 : id == VO_HPR ? 20 : (id == VO_EULER_REDUCED || id == VO_EULER_MULTIPHYSICS) ? 4 : (id == VO_MHD_REDUCED || id == VO_MHD_INTERMEDIATE) ? 5 : id == VO_MHD_MULTIPHYSICS ? 6 : (id == VO_HPR_REDUCED || id == VO_HPR_INTERMEDIATE || id == VO_HPR_MULTIPHYSICS) ? 22 : 0;
+    return id == VO_EULER ? 6 : id == VO_MHD ? 3 : id == VO_HPR ? 20 : (id == VO_EULER_REDUCED || id == VO_EULER_MULTIPHYSICS) ? 4 : (id == VO_MHD_REDUCED || id == VO_MHD_INTERMEDIATE) ? 5 : id == VO_MHD_MULTIPHYSICS ? 6 : (id == VO_HPR_REDUCED || id == VO_HPR_INTERMEDIATE || id == VO_HPR_MULTIPHYSICS) ? 40 : 0;
 }
 
 /* ------------------------------------------------------------------------------- SLIC building blocks */
@@ -2295,7 +2296,7 @@ static double run(int id, double* planes, int nx, int ny, int dims, double dx, d
                   double* dt_log, int reinit_freq) {
     const model* m = model_of(id);
     if (!m) return -1.0;
-    double prm[24];
+    double prm[48];
     memcpy(prm, prm_in, sizeof(double) * vo_nparams(id));
     double tEnd = t_end > 0.0 ? t_end : 1.0e300;
     int limit = max_steps > 0 ? max_steps : 0x7fffffff;

@@ -176,6 +176,34 @@ HPR_MULTIPHYSICS_CASES = {
         dict(dx=1 / 50, cfl=0.8, steps=2, limiter=O.VANLEER, reinit=1, subcycles=0,
              params=wl.hpr_reduced_params(gamma2=2.0, p_inf2=0.5, thermal=(True, False)))),
 }
+# The HPR two-material models with solid materials, the reference's own scenarios for them (HPR/Multiphysics/
+# hprintermediatetests.cpp): an elastic ShockMieGruneisen solid against a plastic one, in the layout of the reference's
+# Zhang test (its deformation gradients and velocities), through the reference's own solve to t_end, and in 2D with the
+# Barton deformation gradients.  GodunovRomenski solids cannot be run here: the reference's acoustic tensors of these
+# models call computeGruneisenCoefficientDerivative, which has no GodunovRomenski return (HPR/hprmiegruneisen.cpp:
+# 104-119) and compiled with -O2 does not return.
+HPR_SOLID1 = wl.hpr_shock_mg_params(tau1=0.05)
+HPR_SOLID2 = wl.hpr_shock_mg_params(plastic=True, sigma0=0.3, n=2.0, tau1=1.0)
+HPR_SOLID_PRM = wl.hpr_two_params(HPR_SOLID1, HPR_SOLID2)
+HPR_SOLID2_MILD = wl.hpr_shock_mg_params(plastic=True, sigma0=1.0, n=1.0, tau1=1.0)
+
+
+def _zhang_solids(nx, ny=1):
+    return wl.hpr_two_solid_riemann(nx, HPR_SOLID1, HPR_SOLID2, *wl.ZHANG_F, (0.0, 0.2, 0.1), (0.0, -0.03, -0.01),
+                                    ny=ny)
+
+
+HPR_REDUCED_CASES["hprreduced1d_smgplastic60_solve_t002_sub2_reinit4"] = (
+    lambda: _zhang_solids(60),
+    dict(dx=1 / 60, cfl=0.8, t_end=0.02, steps=0, limiter=O.MINBEE, reinit=4, subcycles=2, params=HPR_SOLID_PRM))
+HPR_INTERMEDIATE_CASES["hprintermediate2d_smgplastic16x12_minbee_sub2_6"] = (
+    lambda: wl.hpr_intermediate_from_reduced(wl.hpr_two_solid_riemann(16, HPR_SOLID1, HPR_SOLID2_MILD, *wl.BARTON_F,
+                                                                      (0.0, 0.3, 0.5), (0.0, 0.0, 0.0), ny=12)),
+    dict(dx=1 / 16, cfl=0.8, steps=6, limiter=O.MINBEE, reinit=0, subcycles=2,
+         params=wl.hpr_two_params(HPR_SOLID1, HPR_SOLID2_MILD)))
+HPR_MULTIPHYSICS_CASES["hprmultiphysics1d_smgplastic60_solve_t003_sub1_reinit3"] = (
+    lambda: wl.hpr_multiphysics_from_reduced(_zhang_solids(60)),
+    dict(dx=1 / 60, cfl=0.8, t_end=0.03, steps=0, limiter=O.MINBEE, reinit=3, subcycles=1, params=HPR_SOLID_PRM))
 # The MHD multiphysics two-material model (model id O.MHD_MULTIPHYSICS, 1D only): MHDMultiphysicsTests'
 # solveDumbserMultimaterialTest1 setting through the reference's own solve, and a perturbed layout per step with
 # non-zero hyperbolic wave speeds.

@@ -315,6 +315,36 @@ int main(int argc, char** argv) {
             for (auto& c : out) v.push_back(c.computePrimitiveVariableVector()[k]);
         put(f, v);
     }
+    // 17) HPRSecondOrderSolver::solve of the HPR intermediate two-material model with GodunovRomenski solids:
+    //     HPRIntermediateTests::solveZhangTest's aluminium | copper and its deformation gradients (A = F^-1 on each
+    //     side, each material at rho0 det A and the interface at the dominant material's cold pressure), one
+    //     relaxation sub-cycle, reinitialisation every 3 steps, to t = 0.01
+    {
+        HPRMaterialParameters al("GodunovRomenski", false, false, 8.31445985, 2.71, 73.0, 300.0, 300.0, 9.0e-4, 1.0, 0.0,
+                                 5.037, 1.0, 1.338, 0.0, 3.16, 1e8, 0.0, 0.0, 0.75, 0.0, 1.338, 2.0, 1.0, 3.577, 2.088);
+        HPRMaterialParameters cu("GodunovRomenski", false, false, 8.31445985, 8.9, 0.0, 300.0, 300.0, 3.94e-4, 1.0, 0.0,
+                                 3.909, 0.0, 0.0, 0.0, 2.1, 1e8, 0.0, 0.0, 0.75, 0.0, 1.0,
+                                 8.9 * 3.909 * std::sqrt(4.0e-4 / 300.0), 1.0, 3.0, 2.0);
+        vector<vector<double> > AL = {{1.0, 0.0, 0.0},
+                                      {0.010175438596491228, 1.0526315789473684, -0.023391812865497075},
+                                      {0.016666666666666666, 0.0, 1.1111111111111112}};
+        vector<vector<double> > AR = {{1.0, 0.0, 0.0},
+                                      {-0.015789473684210523, 1.0526315789473684, 0.0},
+                                      {0.011111111111111112, 0.0, 1.1111111111111112}};
+        int n = 60;
+        vector<HPRIntermediateStateVector> cells(n);
+        for (int i = 0; i < n; i++)
+            cells[i] = i <= 0.5 * n
+                           ? HPRIntermediateStateVector(0.999, AL, 2.0, 0.0, 0.1, 0.0, 0.0, 0.0, 3.1695906432748537,
+                                                        15.950813993329472, 10.409356725146198, 15.950813993329472)
+                           : HPRIntermediateStateVector(0.001, AR, 0.0, -0.03, -0.01, 0.0, 0.0, 0.0, 3.1695906432748537,
+                                                        31.54939282442279, 10.409356725146198, 31.54939282442279);
+        vector<HPRIntermediateStateVector> out = HPRSecondOrderSolver::solve(cells, 1.0 / n, 0.8, 0.01, 0.0, 2, 1, 3, al, cu);
+        vector<double> v;
+        for (int k = 0; k < 20; k++)
+            for (auto& c : out) v.push_back(c.computePrimitiveVariableVector(al, cu)[k]);
+        put(f, v);
+    }
     double st = steps;
     std::fwrite(&st, sizeof(double), 1, f);
     std::fclose(f);

@@ -87,7 +87,7 @@ def test_reinitialisation_relaxes_both_densities(oracle_lib):
 def test_layouts():
     assert vg.NVAR[vg.HPR_REDUCED] == 19 and vg.HPR_REDUCED == O.HPR_REDUCED == 7
     prm = wl.hpr_reduced_params(gamma1=1.3, thermal=(True, False))
-    assert prm.shape == (22,) and prm[0] == 1.3 and prm[10] == 1.0 and prm[21] == 0.0
+    assert prm.shape == (40,) and prm[0] == 1.3 and prm[11] == 1.0 and prm[31] == 0.0 and prm[12] == prm[32] == 0.0
     W = wl.hpr_reduced_riemann(16, 12, bubble=True)
     assert W.shape == (19, 12, 16)
     assert set(np.unique(W[0])) == {0.001, 0.999}

@@ -28,6 +28,8 @@ PRM = wl.hpr_reduced_params(**STIFF2)
 
 
 REL = 1e-12
+# solid materials take pow in their equations of state (the ShockMieGruneisen cold curve, the plastic relaxation)
+REL_SOLID = 1e-10
 
 
 def _bitwise(a, b):
@@ -36,14 +38,14 @@ def _bitwise(a, b):
         raise AssertionError(f"max |diff| {np.nanmax(d):.3e}; {np.count_nonzero(d)} values differ")
 
 
-def _matches(a, b, subcycles):
-    """Bit for bit without the relaxation source, else every plane within REL of its largest magnitude."""
+def _matches(a, b, subcycles, rel=REL):
+    """Bit for bit without the relaxation source, else every plane within rel of its largest magnitude."""
     if subcycles == 0:
         return _bitwise(a, b)
     assert np.isfinite(a).all()
     d = np.abs(a - b).reshape(b.shape[0], -1).max(axis=1)
     scale = np.maximum(np.abs(b).reshape(b.shape[0], -1).max(axis=1), 1e-300)
-    assert (d / scale).max() <= REL, f"max normwise diff {(d / scale).max():.3e}"
+    assert (d / scale).max() <= rel, f"max normwise diff {(d / scale).max():.3e}"
 
 
 def _device(gpu, W, prm, dx, boundary=None, **run):
@@ -67,7 +69,8 @@ def test_hpr_reduced_golden(gpu, path):
         assert n == steps
     else:
         assert t == t_end
-    _matches(out, z["out"], int(z["subcycles"]))
+    solid = z["params"][12] != 0.0 or z["params"][32] != 0.0
+    _matches(out, z["out"], int(z["subcycles"]) or solid, rel=REL_SOLID if solid else REL)
 
 
 @pytest.mark.parametrize("thermal", [(True, True), (True, False), (False, False)], ids=["hot", "mixed", "cold"])

@@ -185,5 +185,22 @@ def test_shim_driver_matches_oracle(gpu, oracle_lib, tmp_path):
     d = np.abs(got - ref).max(axis=1) / np.maximum(np.abs(ref).max(axis=1), 1e-300)
     assert np.isfinite(got).all() and d.max() <= 1e-12
 
+    # 17) HPRSecondOrderSolver::solve of the HPR intermediate two-material model with the GodunovRomenski aluminium |
+    #     copper of HPRIntermediateTests::solveZhangTest to t = 0.01 (pow in the equation of state: 1e-10 of each
+    #     plane's largest magnitude).  The driver's literals are these states' shortest round-trip decimals.
+    got = take((20, 60))
+    al = wl.hpr_params(gamma=1.0, p_inf=0.0, c_v=9.0e-4, rho0=2.71, T0=300.0, c_s=3.16, alpha=2.0, tau1=1e8, tau2=0.0,
+                       T_ref=300.0, p_ref=73.0, thermal=False, eos="GodunovRomenski", Gamma0=1.0, c0=5.037, s=1.338,
+                       alpha_eos=1.0, n=1.338)
+    cu = wl.hpr_params(gamma=1.0, p_inf=0.0, c_v=3.94e-4, rho0=8.9, T0=300.0, c_s=2.1,
+                       alpha=8.9 * 3.909 * np.sqrt(4.0e-4 / 300.0), tau1=1e8, tau2=0.0, T_ref=300.0, p_ref=0.0,
+                       thermal=False, eos="GodunovRomenski", c0=3.909, alpha_eos=1.0, n=1.0)
+    ref = wl.hpr_intermediate_from_reduced(
+        wl.hpr_two_solid_riemann(60, al, cu, *wl.ZHANG_F, (2.0, 0.0, 0.1), (0.0, -0.03, -0.01)))
+    O.run_two_material(O.HPR_INTERMEDIATE, ref, 1 / 60, 0.8, t_end=0.01, limiter=2, params=wl.hpr_two_params(al, cu),
+                       subcycles=1, reinit=3)
+    d = np.abs(got - ref).max(axis=1) / np.maximum(np.abs(ref).max(axis=1), 1e-300)
+    assert np.isfinite(got).all() and d.max() <= 1e-10
+
     assert take((1,))[0] == 6
     assert off == data.size

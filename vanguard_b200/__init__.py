@@ -23,7 +23,7 @@ TRANSMISSIVE, PERIODIC = 0, 1
 SUPERBEE, VANLEER, MINBEE = 0, 1, 2
 NVAR = {EULER: 6, MHD: 9, HPR: 17, EULER_REDUCED: 7, EULER_MULTIPHYSICS: 8, MHD_REDUCED: 11, MHD_INTERMEDIATE: 12,
         HPR_REDUCED: 19, HPR_INTERMEDIATE: 20, HPR_MULTIPHYSICS: 32, MHD_MULTIPHYSICS: 16}
-MAX_PARAMS = 24
+MAX_PARAMS = 48
 
 
 class VgError(RuntimeError):

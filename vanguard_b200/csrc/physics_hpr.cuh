@@ -441,20 +441,22 @@ using HPRF64 = HPRModel<false>;
 using HPRSolidF64 = HPRModel<true>;
 
 // ---------------------------------------------------------------------------- HPR reduced two-material
-// HPRReducedStateVector (HPR/Multiphysics/hprreducedstatevector.cpp) for two StiffenedGas materials with elastic strain
-// relaxation, every plane carried: W = (alpha1, p, A (9, row-major), u, v, w, Jx, Jy, Jz, rho1, rho2),
-// U = (rho, rho alpha1, rho E, A, rho u (3), rho J (3), alpha1 rho1, alpha2 rho2).  Each material's single-material
-// formulas (HPRModel<false>) enter with that material's parameters: its pressure and total energy at the mixture
-// density in the conversions and fluxes, at its own density in the source; its acoustic speed at its own density.
-// Parameters: 11 per material, material k at params[11 k]: {gamma, p_inf, c_v, rho0, T0, c_s, alpha, tau1, tau2,
-// T_ref, is_thermal}.  J is carried when either material is thermal (:104-109); otherwise the cell keeps its own.
+// HPRReducedStateVector (HPR/Multiphysics/hprreducedstatevector.cpp), every plane carried: W = (alpha1, p, A (9,
+// row-major), u, v, w, Jx, Jy, Jz, rho1, rho2), U = (rho, rho alpha1, rho E, A, rho u (3), rho J (3), alpha1 rho1,
+// alpha2 rho2).  Each material's single-material formulas enter with that material's parameters: its pressure and
+// total energy at the mixture density in the conversions and fluxes, at its own density in the source; its acoustic
+// speed at its own density.  The materials take every HPRMieGruneisen branch and the plastic relaxation
+// (HPRModel<true>), as the reference's scenarios of the two-material models run GodunovRomenski solids
+// (HPR/Multiphysics/hprreducedtests.cpp); with a StiffenedGas material those branches compute the gas formulas.
+// Parameters: the single-material 20-value block of each material, material k at params[20 k].  J is carried when
+// either material is thermal (:104-109); otherwise the cell keeps its own.
 struct HPRReducedF64 {
     static constexpr int NW = 19;
     static constexpr int NU = 20;
     static constexpr bool HAS_Y = true;
     static constexpr bool HAS_SOURCE = true;
     static constexpr int J_PLANE = 14;
-    using H = HPRModel<false>;
+    using H = HPRModel<true>;
     using M3 = H::M3;
     struct P {
         H::P m1, m2;
@@ -462,15 +464,7 @@ struct HPRReducedF64 {
         double pinf;   // the smaller stiffening pressure: the state check's pressure floor is -pinf
         double ch2;
     };
-    __device__ static H::P material(const double* prm, int k) {
-        double b[kParams];
-#pragma unroll
-        for (int i = 0; i < kParams; i++) b[i] = 0.0;
-#pragma unroll
-        for (int i = 0; i < 10; i++) b[i] = prm[11 * k + i];
-        b[11] = prm[11 * k + 10];
-        return H::params(b, 0.0);
-    }
+    __device__ static H::P material(const double* prm, int k) { return H::params(prm + 20 * k, 0.0); }
     __device__ static P params(const double* prm, double /*ch*/) {
         P q;
         q.m1 = material(prm, 0);
@@ -669,7 +663,7 @@ struct HPRMultiphysicsF64 {
     static constexpr int NU = 33;
     static constexpr bool HAS_Y = false;
     static constexpr bool HAS_SOURCE = false;
-    using H = HPRModel<false>;
+    using H = HPRReducedF64::H;
     using M3 = H::M3;
     using P = HPRReducedF64::P;
     __device__ static P params(const double* prm, double ch) { return HPRReducedF64::params(prm, ch); }
@@ -845,7 +839,7 @@ struct HPRIntermediateF64 {
     static constexpr bool HAS_Y = true;
     static constexpr bool HAS_SOURCE = true;
     static constexpr int J_PLANE = 13;  // first heat-flux plane (kept by setConservedVariableVector when cold)
-    using H = HPRModel<false>;
+    using H = HPRReducedF64::H;
     using M3 = H::M3;
     using P = HPRReducedF64::P;
     __device__ static P params(const double* prm, double ch) { return HPRReducedF64::params(prm, ch); }

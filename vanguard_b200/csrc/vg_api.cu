@@ -23,6 +23,8 @@ using vg::Ctrl;
 using vg::Ops;
 using vg::SweepArgs;
 
+static_assert(vg::kNumXCfg == VG_NUM_XCFG && vg::kNumYCfg == VG_NUM_YCFG, "the header names the tile-shape counts");
+
 namespace {
 
 thread_local std::string g_last_error;
@@ -617,14 +619,14 @@ vg_status vg_upload_primitive(vg_solver* s, const double* planes, int is_device,
     // HPRReducedStateVector::setPrimitiveVariableVector (HPR/Multiphysics/hprreducedstatevector.cpp:78-104) and
     // HPRIntermediateStateVector's (hprintermediatestatevector.cpp:82-110) take J only when either material is
     // thermal; otherwise the cells keep the default J = 0, which nothing reads
-    if (e == cudaSuccess && (variant == vg::V_HRED19 || variant == vg::V_HINT20) && s->d.params[10] == 0.0 &&
-        s->d.params[21] == 0.0)
+    if (e == cudaSuccess && (variant == vg::V_HRED19 || variant == vg::V_HINT20) && s->d.params[11] == 0.0 &&
+        s->d.params[31] == 0.0)
         e = cudaMemsetAsync(s->buf[0] + (variant == vg::V_HRED19 ? 14 : 13) * s->plane, 0, sizeof(double) * 3 * s->plane,
                             st);
     // HPRMultiphysicsStateVector::setPrimitiveVariableVector (hprmultiphysicsstatevector.cpp:98-139) takes each
     // material's J only when that material is thermal
     for (int k = 0; k < 2 && variant == vg::V_HMPH32; k++)
-        if (e == cudaSuccess && s->d.params[11 * k + 10] == 0.0)
+        if (e == cudaSuccess && s->d.params[20 * k + 11] == 0.0)
             e = cudaMemsetAsync(s->buf[0] + (15 + 14 * k) * s->plane, 0, sizeof(double) * 3 * s->plane, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(&s->ctrl->err, 0, sizeof(unsigned), st);  // a fresh state: no error yet
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
@@ -673,7 +675,7 @@ vg_status vg_download_primitive(vg_solver* s, double* planes, int is_device, voi
     // cells do
     if (s->variant == vg::V_HMPH32) {
         for (int k = 0; k < 2; k++) {
-            if (s->d.params[11 * k + 10] != 0.0) continue;
+            if (s->d.params[20 * k + 11] != 0.0) continue;
             for (int r = 15 + 14 * k; r < 18 + 14 * k; r++) {
                 if (is_device) {
                     vg::fill_plane_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(planes + (long)r * n, n, 0.0);

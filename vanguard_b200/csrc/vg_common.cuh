@@ -61,7 +61,7 @@ struct SweepConst {
     int limiter;
 };
 
-constexpr int kParams = 24;           // VG_MAX_PARAMS
+constexpr int kParams = 48;           // VG_MAX_PARAMS
 constexpr int kTmaTile = 128;         // threads (cells per row, halo included: kTmaTile + 2) of the TMA X sweep
 constexpr int kInvGm1 = kParams - 1;  // slot the host fills with 1 / (gamma - 1)
 

@@ -915,18 +915,10 @@ void tensor_into(const vector<vector<double> >& A, double* a9) {
 bool either_thermal(const HPRMaterialParameters& m1, const HPRMaterialParameters& m2) {
     return m1.getIsThermal() || m2.getIsThermal();
 }
-// 11 values per material, material k at prm[11 k]: {gamma, p_inf, c_v, rho0, T0, c_s, alpha, tau1, tau2, T_ref,
-// is_thermal}.  The device carries the StiffenedGas gas with elastic relaxation for both materials.
+// each material's 20-value HPR block (hpr_params), material k at prm[20 k]: any equation of state, elastic or plastic
 void hpr_two_params(const HPRMaterialParameters& m1, const HPRMaterialParameters& m2, double* prm) {
-    const HPRMaterialParameters* m[2] = {&m1, &m2};
-    for (int k = 0; k < 2; k++) {
-        if (m[k]->getEquationOfState() != "StiffenedGas" || m[k]->getIsPlastic())
-            throw std::runtime_error("HPR two-material models: both materials must be elastic StiffenedGas materials");
-        double b[20];
-        hpr_params(*m[k], b);
-        for (int i = 0; i < 10; i++) prm[11 * k + i] = b[i];
-        prm[11 * k + 10] = b[11];
-    }
+    hpr_params(m1, prm);
+    hpr_params(m2, prm + 20);
 }
 void hred_get(const HPRReducedStateVector& c, double* w) { std::memcpy(w, c.data(), sizeof(double) * 19); }
 HPRReducedStateVector hred_make(const double* w) {
@@ -956,10 +948,10 @@ template <class S, class Get, class Make>
 vector<S> hpr_two_run(int model, int nvar, vector<S>& cells, const HPRMaterialParameters& m1,
                       const HPRMaterialParameters& m2, double dx, double cfl, double tEnd, double bias, int limiter,
                       int subcycles, int maxSteps, int order, int reinit, Get get, Make make) {
-    double prm[22];
+    double prm[40];
     hpr_two_params(m1, m2, prm);
     std::vector<double> p = pack(cells, nvar, get);
-    run_planes(model, p, (int)cells.size(), 1, prm, 22, dx, cfl, tEnd, bias, limiter, subcycles, maxSteps, order,
+    run_planes(model, p, (int)cells.size(), 1, prm, 40, dx, cfl, tEnd, bias, limiter, subcycles, maxSteps, order,
                reinit);
     vector<S> out = unpack<S>(p, cells.size(), nvar, make);
     keep_cold_heat_flux(out.data(), cells.data(), (long)cells.size(), m1, m2);
@@ -969,11 +961,11 @@ template <class S, class Get, class Make>
 vector<vector<S> > hpr_two_run2(int model, int nvar, vector<vector<S> >& cells, const HPRMaterialParameters& m1,
                                 const HPRMaterialParameters& m2, double dx, double cfl, double tEnd, double bias,
                                 int limiter, int subcycles, int maxSteps, int order, int reinit, Get get, Make make) {
-    double prm[22];
+    double prm[40];
     hpr_two_params(m1, m2, prm);
     std::vector<double> p = pack2(cells, nvar, get);
     long ny = cells.size(), nx = cells[0].size();
-    run_planes(model, p, (int)nx, (int)ny, prm, 22, dx, cfl, tEnd, bias, limiter, subcycles, maxSteps, order, reinit);
+    run_planes(model, p, (int)nx, (int)ny, prm, 40, dx, cfl, tEnd, bias, limiter, subcycles, maxSteps, order, reinit);
     vector<vector<S> > out = unpack2<S>(p, nx, ny, nvar, make);
     for (long i = 0; i < ny; i++) keep_cold_heat_flux(out[i].data(), cells[i].data(), nx, m1, m2);
     return out;
@@ -1136,10 +1128,10 @@ vector<HPRMultiphysicsStateVector> HPRSecondOrderSolver::solve(vector<HPRMultiph
                                                                int limiter, int subcycles, int reinit,
                                                                HPRMaterialParameters m1, HPRMaterialParameters m2,
                                                                int maxSteps) {
-    double prm[22];
+    double prm[40];
     hpr_two_params(m1, m2, prm);
     std::vector<double> p = pack(initialCells, 32, hmph_get);
-    run_planes(VG_MODEL_HPR_MULTIPHYSICS, p, (int)initialCells.size(), 1, prm, 22, dx, cfl, tEnd, bias, limiter,
+    run_planes(VG_MODEL_HPR_MULTIPHYSICS, p, (int)initialCells.size(), 1, prm, 40, dx, cfl, tEnd, bias, limiter,
                subcycles, maxSteps, 2, reinit);
     return unpack<HPRMultiphysicsStateVector>(p, initialCells.size(), 32, hmph_make);
 }
@@ -1147,10 +1139,10 @@ vector<HPRMultiphysicsStateVector> HPRFirstOrderSolver::solve(vector<HPRMultiphy
                                                               double dx, double cfl, double tEnd, int,
                                                               HPRMaterialParameters m1, HPRMaterialParameters m2,
                                                               int maxSteps) {
-    double prm[22];
+    double prm[40];
     hpr_two_params(m1, m2, prm);
     std::vector<double> p = pack(initialCells, 32, hmph_get);
-    run_planes(VG_MODEL_HPR_MULTIPHYSICS, p, (int)initialCells.size(), 1, prm, 22, dx, cfl, tEnd, 0.0, 0, 0, maxSteps,
+    run_planes(VG_MODEL_HPR_MULTIPHYSICS, p, (int)initialCells.size(), 1, prm, 40, dx, cfl, tEnd, 0.0, 0, 0, maxSteps,
                1, 0);
     return unpack<HPRMultiphysicsStateVector>(p, initialCells.size(), 32, hmph_make);
 }

@@ -186,6 +186,10 @@ def hpr_shock_riemann(nx, ny, prm, seed=0):
 
 BARTON_F = ([[0.98, 0.0, 0.0], [0.02, 1.0, 0.1], [0.0, 0.0, 1.0]],
             [[1.0, 0.0, 0.0], [0.0, 1.0, 0.1], [0.0, 0.0, 1.0]])
+# the left and right deformation gradients of the reference's Zhang scenarios of the two-material HPR models
+# (HPR/Multiphysics/hprintermediatetests.cpp:64-84)
+ZHANG_F = ([[1.0, 0.0, 0.0], [-0.01, 0.95, 0.02], [-0.015, 0.0, 0.9]],
+           [[1.0, 0.0, 0.0], [0.015, 0.95, 0.0], [-0.01, 0.0, 0.9]])
 
 
 def hpr_relaxation_times(seed):
@@ -375,13 +379,61 @@ def hpr_relaxation_cells(n, seed=0, thermal=True, tau_range=(1e-3, 1e-2), distor
     return W, tau, hpr_params(tau1=tau[0, 0], tau2=tau[1, 0], thermal=thermal)
 
 
+def hpr_two_params(m1, m2):
+    """The parameter block of the HPR two-material models (reduced, intermediate, multiphysics): the two materials'
+    20-value hpr_params blocks, material k at [20 k] -- any equation of state, elastic or plastic."""
+    m1, m2 = np.asarray(m1, dtype=np.float64), np.asarray(m2, dtype=np.float64)
+    assert m1.shape == (20,) and m2.shape == (20,)
+    return np.concatenate([m1, m2])
+
+
 def hpr_reduced_params(gamma1=1.4, p_inf1=0.0, gamma2=1.67, p_inf2=0.0, c_v=2.5, rho0=1.0, T0=1.0, c_s=1.0, alpha=1.0,
                        tau1=1e-2, tau2=1e-2, T_ref=0.0, thermal=(True, True)):
-    """Two StiffenedGas HPR materials for the HPR reduced two-material model, packed 11 values per material:
-    {gamma, p_inf, c_v, rho0, T0, c_s, alpha, tau1, tau2, T_ref, is_thermal} (HPRMaterialParameters' gas fields)."""
+    """Two StiffenedGas HPR materials with elastic strain relaxation for the HPR two-material models, as
+    hpr_two_params' 40 values (p_ref 0, which the StiffenedGas branch does not read)."""
     def one(g, pinf, th):
-        return [g, pinf, c_v, rho0, T0, c_s, alpha, tau1, tau2, T_ref, 1.0 if th else 0.0]
-    return np.array(one(gamma1, p_inf1, thermal[0]) + one(gamma2, p_inf2, thermal[1]))
+        return hpr_params(gamma=g, p_inf=pinf, c_v=c_v, rho0=rho0, T0=T0, c_s=c_s, alpha=alpha, tau1=tau1, tau2=tau2,
+                          T_ref=T_ref, p_ref=0.0, thermal=th)
+    return hpr_two_params(one(gamma1, p_inf1, thermal[0]), one(gamma2, p_inf2, thermal[1]))
+
+
+def _cold_pressure(rho, prm):
+    """The reference pressure p_ref(rho) of a material's equation of state (HPR/hprmiegruneisen.cpp:30-66):
+    ShockMieGruneisen and GodunovRomenski cold curves, -p_inf for StiffenedGas."""
+    eos = int(prm[12])
+    if eos == HPR_EOS["ShockMieGruneisen"]:
+        return smg_reference_pressure(rho, prm)
+    if eos == HPR_EOS["GodunovRomenski"]:
+        return gr_reference_pressure(rho, prm)
+    return -prm[1] + 0.0 * np.asarray(rho, dtype=np.float64)
+
+
+def hpr_two_solid_riemann(nx, m1, m2, F_left, F_right, v_left, v_right, ny=1, p_offset=0.0, heat=0.0, seed=0):
+    """A two-material solid Riemann problem in the shape of the reference's Barton and Zhang scenarios of the HPR
+    two-material models (HPR/Multiphysics/hprreducedtests.cpp, hprintermediatetests.cpp:7-55): alpha1 0.999 at
+    i <= nx/2 and 0.001 to the right, A = F^-1 and velocity v on each side, each material's density rho0_k det A, and
+    the interface pressure the cold pressure of the side's dominant material plus p_offset (the reference takes it
+    from its Elasticity module's hyperelastic equation of state, which this package does not carry); seeded heat flux
+    of amplitude `heat`.  HPR reduced planes (19, nx) or (19, ny, nx), split along x."""
+    m1, m2 = np.asarray(m1, dtype=np.float64), np.asarray(m2, dtype=np.float64)
+    rng = np.random.default_rng(seed)
+    shape = (ny, nx) if ny > 1 else (nx,)
+    W = np.zeros((19,) + shape)
+    left = np.broadcast_to(np.arange(nx) <= 0.5 * nx, shape)
+    for side, F, v, dom, a1 in ((left, F_left, v_left, m1, 0.999), (~left, F_right, v_right, m2, 0.001)):
+        A = np.linalg.inv(np.asarray(F, dtype=np.float64))
+        d = np.linalg.det(A)
+        W[0][side] = a1
+        W[1][side] = _cold_pressure(dom[3] * d, dom) + p_offset
+        for k in range(9):
+            W[2 + k][side] = A.reshape(9)[k]
+        for k in range(3):
+            W[11 + k][side] = float(v[k])
+        W[17][side] = m1[3] * d
+        W[18][side] = m2[3] * d
+    if heat:
+        W[14:17] = heat * rng.standard_normal((3,) + shape)
+    return W
 
 
 def hpr_reduced_riemann(nx, ny=1, seed=0, distortion=0.02, heat=0.05, bubble=False):
