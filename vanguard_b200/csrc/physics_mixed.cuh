@@ -14,13 +14,14 @@
 // steps x <- x + x (1 - a x), each of which doubles the number of correct bits.
 //
 // On B200 the XU pipe that executes reciprocal approximations and every float<->double conversion has a
-// quarter of the FP64 pipe's lanes.  MHD and HPR (EulerMixed's split) evaluate the physical flux function in
-// FP64 with FMA and round only its outputs to FP32; the arithmetic that combines fluxes (half-step evolution
-// increment, Lax-Friedrichs, Richtmyer and FORCE averages) runs in FP32.  Euler (EulerF32) goes further: the
-// limited edge states, the evolved and Richtmyer states and their fluxes are FP32 (the states are rounded
-// once, after the FP64 slope differences), which halves the sweeps' instruction count; FP64 stays in the cell
-// states, the conserved/primitive conversion of the stored state with its pressure recovery, the wave speed and
-// the update accumulation.  Each model's `R` names the type of its reconstructed states.
+// quarter of the FP64 pipe's lanes.  The 9-component MHD variant and the HPR solids (EulerMixed's split) evaluate
+// the physical flux function in FP64 with FMA and round only its outputs to FP32; the arithmetic that combines
+// fluxes (half-step evolution increment, Lax-Friedrichs, Richtmyer and FORCE averages) runs in FP32.  Euler
+// (EulerF32), MHD with w = Bz = 0 (MHDF32) and HPR gas (HPRF32) go further: the limited edge states, the evolved
+// and Richtmyer states and their fluxes are FP32 (the states are rounded once, after the FP64 slope differences),
+// which halves the sweeps' instruction count; FP64 stays in the cell states, the conserved/primitive conversion of
+// the stored state with its pressure recovery, the wave speed and the update accumulation.  Each model's `R`
+// names the type of its reconstructed states.
 #pragma once
 
 #include "physics_fp64.cuh"
@@ -420,7 +421,101 @@ struct HPRMixedT {
     __device__ static double density(const double* W) { return W[0]; }
     __device__ static double pressure(const double* W) { return W[1]; }
 };
-using HPRMixed = HPRMixedT<false>;
+// HPR (GPR) gas with FP32 reconstruction, as EulerF32 and MHDF32: the limited edge states, the half-step evolved
+// states, the Richtmyer state and every flux evaluation are FP32 -- the stress c_s^2 rho A^T A dev(A^T A), the
+// pressure recovered inside the flux from total energy (StiffenedGas: p = (gamma - 1)(rho e - p_inf) - p_inf with
+// e = E - |v|^2 / 2 - c_s^2 |dev(A^T A)|^2 / 4 [- alpha^2 |J|^2 / 2]) and the temperature of the heat flux.  The cell
+// states, the conversions of the stored state (its pressure recovery), the acoustic-tensor CFL speed, the update
+// accumulation and the relaxation source (the exact forcing and stiff-relaxation kernels) stay FP64
+// (HPR/hprstatevector.cpp:164-298 for the fluxes).
+struct HPRF32 : HPRMixedT<false> {
+    using Base = HPRMixedT<false>;
+    using R = float;
+    static constexpr bool PAIR_X = false;
+    struct P : Base::P {
+        float gm1_f, pinf_f, cs2_f, qcs2_f, ha2_f, a2_f, tref_f, inv_gm1cv_f;
+    };
+    __device__ static P params(const double* prm, double ch) {
+        P q;
+        static_cast<Base::P&>(q) = Base::params(prm, ch);
+        q.gm1_f = (float)(q.g - 1.0);
+        q.pinf_f = (float)q.pinf;
+        q.cs2_f = (float)(q.cs * q.cs);
+        q.qcs2_f = (float)(0.25 * (q.cs * q.cs));
+        q.ha2_f = (float)(0.5 * (q.alpha * q.alpha));
+        q.a2_f = (float)(q.alpha * q.alpha);
+        q.tref_f = (float)q.Tref;
+        q.inv_gm1cv_f = (float)(1.0 / ((q.g - 1.0) * q.cv));
+        return q;
+    }
+    // U = (rho, rho E, A (9, row-major), rho u, rho v, rho w, rho Jx, rho Jy, rho Jz)
+    template <int AXIS>
+    __device__ static void flux(const float* U, const P& q, float* F) {
+        const float rho = U[0];
+        const float inv = rcp_approx_f(rho);
+        float A[3][3];
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) A[i][j] = U[2 + 3 * i + j];
+        // D = dev(A^T A)
+        float D[3][3];
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) D[i][j] = fmaf(A[0][i], A[0][j], fmaf(A[1][i], A[1][j], A[2][i] * A[2][j]));
+        const float third = (D[0][0] + D[1][1] + D[2][2]) * (1.0f / 3.0f);
+        D[0][0] -= third;
+        D[1][1] -= third;
+        D[2][2] -= third;
+        // row AXIS of A^T (A D): (A^T A D)[AXIS][j] = sum_k G[AXIS][k] D[k][j], G = A^T A = D + third I
+        float s[3];
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            float acc = third * D[AXIS][j];
+#pragma unroll
+            for (int k = 0; k < 3; k++) acc = fmaf(D[AXIS][k], D[k][j], acc);
+            s[j] = (q.cs2_f * rho) * acc;  // -sigma[AXIS][j]
+        }
+        float dd = 0.0f;
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) dd = fmaf(D[i][j], D[i][j], dd);
+        const float mx = U[11], my = U[12], mz = U[13];
+        const float u = mx * inv, v = my * inv, w = mz * inv;
+        const float E = U[1] * inv;
+        float e = E - fmaf(0.5f, fmaf(u, u, fmaf(v, v, w * w)), q.qcs2_f * dd);
+        float jx = 0.0f, jy = 0.0f, jz = 0.0f;
+        if (q.thermal) {
+            jx = U[14] * inv;
+            jy = U[15] * inv;
+            jz = U[16] * inv;
+            e = e - q.ha2_f * fmaf(jx, jx, fmaf(jy, jy, jz * jz));
+        }
+        const float p = fmaf(q.gm1_f, fmaf(rho, e, -q.pinf_f), -q.pinf_f);
+        const float un = AXIS == 0 ? u : v;
+        const float mn = AXIS == 0 ? mx : my;
+#pragma unroll
+        for (int i = 0; i < 17; i++) F[i] = 0.0f;
+        F[0] = mn;
+        F[1] = fmaf(U[1] + p, un, fmaf(s[0], u, fmaf(s[1], v, s[2] * w)));
+        F[11] = fmaf(mx, un, s[0]);
+        F[12] = fmaf(my, un, s[1]);
+        F[13] = fmaf(mz, un, s[2]);
+        F[11 + AXIS] += p;
+#pragma unroll
+        for (int i = 0; i < 3; i++) F[2 + 3 * i + AXIS] = fmaf(A[i][0], u, fmaf(A[i][1], v, A[i][2] * w));
+        if (q.thermal) {
+            const float T = fmaf(p + q.pinf_f, inv * q.inv_gm1cv_f, q.tref_f);
+            F[1] = fmaf(T * q.a2_f, AXIS == 0 ? jx : jy, F[1]);
+            F[14] = U[14] * un;
+            F[15] = U[15] * un;
+            F[16] = U[16] * un;
+            F[14 + AXIS] += T;
+        }
+    }
+};
 
 // The Euler two-material models in the mixed form: FP64 states and flux function (its pressure
 // recovery from total energy), flux values rounded to FP32, FP32 flux combinations (EulerMixed's split for MHD

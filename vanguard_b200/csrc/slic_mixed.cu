@@ -97,7 +97,7 @@ const Ops kOps[V_COUNT] = {
     make_ops<EulerF32<2>>(),
     make_ops<MHDF32>(&mhd7_forcing_fp64),
     make_ops<MHDMixed<true>>(&mhd9_forcing_fp64),
-    make_ops<HPRMixed>(&hpr_forcing_fp64, &hpr_relax_fp64),
+    make_ops<HPRF32>(&hpr_forcing_fp64, &hpr_relax_fp64),
     make_ops<HPRSolidMixed>(&hpr_solid_forcing_fp64, &hpr_solid_relax_fp64),
     make_ops<ReducedMixed>(nullptr, nullptr, &reduced_reinit_fp64),
     Ops{},  // V_MPH7: no mixed form (see ops_mixed)
