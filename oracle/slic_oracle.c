@@ -572,8 +572,11 @@ static void hpr_source(const double* U, const double* prm, double* S) {
  * c_s^2 A dev(A^T A)).  det A is conserved (dev is traceless), so c is constant; G = A^T A keeps its eigenvectors
  * and its eigenvalues obey d(ln l_i)/dt = -2 c (l_i - mean(l)).  That system is integrated by implicit Euler
  * (L-stable; Newton on three unknowns), then A <- A V diag(sqrt(l_i' / l_i)) V^T.
- * Heat flux: d(rho J)/dt = -(rho0 T / (tau2 T0 rho)) rho J, integrated by exponential sub-steps with T from the
- * current state.  rho, rho v and rho E do not change. */
+ * Heat flux: d(rho J)/dt = -(rho0 T / (tau2 T0 rho)) rho J with rho, v, E and the relaxed A fixed.  Every equation
+ * of state here has T = T_ref + (e - e_ref(rho)) / c_v, and e = e_J0 - alpha^2 |J|^2 / 2, so T = T_J0 - beta s with
+ * s = |J|^2, beta = alpha^2 / (2 c_v): s obeys the Bernoulli equation ds/dt = -2 kappa (T_J0 - beta s) s
+ * (kappa = rho0 / (tau2 T0 rho)), solved exactly over h: J scales by sqrt(E / ((1 - r) + r E)),
+ * E = exp(-2 kappa T_J0 h), r = beta s0 / T_J0.  J is left alone where T <= 0.  rho, rho v and rho E do not change. */
 
 /* cyclic Jacobi eigen-decomposition of a symmetric 3x3 matrix: g = V diag(l) V^T (published method) */
 static void sym_eig3(const mat3* g, double l[3], double V[3][3]) {
@@ -612,34 +615,36 @@ static void sym_eig3(const mat3* g, double l[3], double V[3][3]) {
     for (int i = 0; i < 3; i++) l[i] = a[i][i];
 }
 
-/* n implicit-Euler steps of d(mu_i)/dt = -2 c (exp(mu_i) - mean(exp(mu))) with k = 2 c h / n per step */
+/* n implicit-Euler steps of d(mu_i)/dt = -2 c (exp(mu_i) - mean(exp(mu))) with k = 2 c h / n per step.  Newton
+ * starts from the linear extrapolation of the last two step values and stops once a correction below 1e-8 has been
+ * applied (quadratic convergence: the next correction would be below the double resolution of mu). */
 static void relax_log_eigs(double mu[3], double k, int n) {
+    double prev[3] = {mu[0], mu[1], mu[2]};
     for (int s = 0; s < n; s++) {
-        double m0[3] = {mu[0], mu[1], mu[2]}, x[3] = {mu[0], mu[1], mu[2]};
+        double m0[3] = {mu[0], mu[1], mu[2]}, x[3];
+        for (int i = 0; i < 3; i++) x[i] = m0[i] + (m0[i] - prev[i]);
+        for (int i = 0; i < 3; i++) prev[i] = m0[i];
         for (int it = 0; it < 100; it++) {
             double e[3] = {exp(x[0]), exp(x[1]), exp(x[2])};
             double mean = (e[0] + e[1] + e[2]) / 3.0;
-            double F[3], J[3][3];
+            /* J dx = -F with J = diag(1 + k e_i) - (k / 3) 1 e^T, by the Sherman-Morrison formula:
+             * dx = y + k z (e . y) / sum(z), z_i = 1 / (1 + k e_i), y_i = -F_i z_i
+             * (1 - (k / 3) e . z = sum(z) / 3 exactly, so the denominator takes no cancellation) */
+            double z[3], y[3];
             for (int i = 0; i < 3; i++) {
-                F[i] = (x[i] - m0[i]) + k * (e[i] - mean);
-                for (int j = 0; j < 3; j++) J[i][j] = (i == j ? 1.0 + k * e[i] : 0.0) - k * e[j] / 3.0;
+                double F = (x[i] - m0[i]) + k * (e[i] - mean);
+                z[i] = 1.0 / (1.0 + k * e[i]);
+                y[i] = -F * z[i];
             }
-            /* J dx = -F by Cramer's rule */
-            double det = J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) - J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
-                         J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
+            double g = k * (((e[0] * y[0]) + (e[1] * y[1]) + (e[2] * y[2])) / ((z[0] + z[1]) + z[2]));
             double dx[3], big = 0.0;
             for (int c = 0; c < 3; c++) {
-                double M[3][3];
-                for (int i = 0; i < 3; i++)
-                    for (int j = 0; j < 3; j++) M[i][j] = j == c ? -F[i] : J[i][j];
-                double dc = M[0][0] * (M[1][1] * M[2][2] - M[1][2] * M[2][1]) - M[0][1] * (M[1][0] * M[2][2] - M[1][2] * M[2][0]) +
-                            M[0][2] * (M[1][0] * M[2][1] - M[1][1] * M[2][0]);
-                dx[c] = dc / det;
+                dx[c] = y[c] + z[c] * g;
                 if (fabs(dx[c]) > big) big = fabs(dx[c]);
             }
             double damp = big > 0.5 ? 0.5 / big : 1.0;
             for (int i = 0; i < 3; i++) x[i] += damp * dx[i];
-            if (big < 1e-15) break;
+            if (big < 1e-8) break;
         }
         for (int i = 0; i < 3; i++) mu[i] = x[i];
     }
@@ -683,17 +688,17 @@ static void hpr_relax_cell(double* U, double h, const double* prm) {
     if (!hpr_thermal(prm)) return;
     mat3 An = load_A(U + 2);
     double E = U[1] / rho, u = U[11] / rho, v = U[12] / rho, w = U[13] / rho;
-    double p0 = hpr_pressure(rho, E, u, v, w, &An, U[14] / rho, U[15] / rho, U[16] / rho, prm);
-    double k0 = (prm[3] * mg_temperature(rho, p0, prm)) / (prm[8] * prm[4] * rho);
-    int nJ = clampi(k0 * h, 1, 32);
-    double hs = h / nJ;
-    for (int s = 0; s < nJ; s++) {
-        double p = hpr_pressure(rho, E, u, v, w, &An, U[14] / rho, U[15] / rho, U[16] / rho, prm);
-        double T = mg_temperature(rho, p, prm);
-        double k = T > 0.0 ? (prm[3] * T) / (prm[8] * prm[4] * rho) : 0.0;
-        double fac = exp(-k * hs);
-        for (int i = 14; i < 17; i++) U[i] *= fac;
-    }
+    double jx = U[14] / rho, jy = U[15] / rho, jz = U[16] / rho;
+    double s0 = ((jx * jx) + (jy * jy)) + (jz * jz);
+    double T = mg_temperature(rho, hpr_pressure(rho, E, u, v, w, &An, jx, jy, jz, prm), prm);
+    if (!(s0 > 0.0) || !(T > 0.0)) return;
+    double beta = (0.5 * (prm[6] * prm[6])) / prm[2];
+    double TJ0 = T + (beta * s0); /* the temperature at J = 0 */
+    double kappa = prm[3] / (prm[8] * prm[4] * rho);
+    double Eh = exp(-2.0 * (kappa * (TJ0 * h)));
+    double r = (beta * s0) / TJ0;
+    double fac = sqrt(Eh / ((1.0 - r) + (r * Eh)));
+    for (int i = 14; i < 17; i++) U[i] *= fac;
 }
 
 /* HPRAcousticTensor::computeMaximumWaveSpeed (HPR/hpracoustictensor.cpp:7-97) with the 10-step power

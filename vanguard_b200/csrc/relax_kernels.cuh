@@ -5,8 +5,11 @@
 //     dE/dA = c_s^2 A dev(A^T A)).  det A is conserved (dev is traceless), so c is constant; G = A^T A keeps its
 //     eigenvectors and its eigenvalues obey d(ln l_i)/dt = -2 c (l_i - mean(l)).  That system is integrated by
 //     implicit Euler (L-stable, Newton on three unknowns), then A <- A V diag(sqrt(l_i' / l_i)) V^T;
-//   * heat flux: d(rho J)/dt = -(rho0 T / (tau2 T0 rho)) rho J, integrated by exponential sub-steps with T
-//     re-evaluated from the current state.
+//   * heat flux: d(rho J)/dt = -(rho0 T / (tau2 T0 rho)) rho J with rho, v, E and the relaxed A fixed.  Every
+//     equation of state here has T = T_ref + (e - e_ref(rho)) / c_v, and e = e_J0 - alpha^2 |J|^2 / 2, so
+//     T = T_J0 - beta s with s = |J|^2, beta = alpha^2 / (2 c_v): s obeys the Bernoulli equation
+//     ds/dt = -2 kappa (T_J0 - beta s) s (kappa = rho0 / (tau2 T0 rho)), whose exact solution over h scales J by
+//     sqrt(E / ((1 - r) + r E)), E = exp(-2 kappa T_J0 h), r = beta s0 / T_J0.  J is left alone where T <= 0.
 // rho, rho v and rho E do not change.  The eigen-decomposition is the published cyclic Jacobi method.
 #pragma once
 
@@ -52,36 +55,38 @@ __device__ inline void sym_eig3(const double g[3][3], double l[3], double V[3][3
     for (int i = 0; i < 3; i++) l[i] = a[i][i];
 }
 
-__device__ inline double det3x3(const double M[3][3]) {
-    return M[0][0] * (M[1][1] * M[2][2] - M[1][2] * M[2][1]) - M[0][1] * (M[1][0] * M[2][2] - M[1][2] * M[2][0]) +
-           M[0][2] * (M[1][0] * M[2][1] - M[1][1] * M[2][0]);
-}
-
-// n implicit-Euler steps of d(mu_i)/dt = -2 c (exp(mu_i) - mean(exp(mu))), k = 2 c h / n per step
+// n implicit-Euler steps of d(mu_i)/dt = -2 c (exp(mu_i) - mean(exp(mu))), k = 2 c h / n per step.  Newton starts
+// from the linear extrapolation of the last two step values and stops once a correction below 1e-8 has been
+// applied: Newton converges quadratically here (the Jacobian is I plus a positive diagonal and a rank-one term),
+// so the next correction would be of the order of its square, below the double resolution of mu.
 __device__ inline void relax_log_eigs(double mu[3], double k, int n) {
+    double prev[3] = {mu[0], mu[1], mu[2]};
     for (int s = 0; s < n; s++) {
         const double m0[3] = {mu[0], mu[1], mu[2]};
-        double x[3] = {mu[0], mu[1], mu[2]};
+        double x[3];
+        for (int i = 0; i < 3; i++) x[i] = m0[i] + (m0[i] - prev[i]);
+        for (int i = 0; i < 3; i++) prev[i] = m0[i];
         for (int it = 0; it < 100; it++) {
             const double e[3] = {exp(x[0]), exp(x[1]), exp(x[2])};
             const double mean = (e[0] + e[1] + e[2]) / 3.0;
-            double F[3], J[3][3];
+            // J dx = -F with J = diag(1 + k e_i) - (k / 3) 1 e^T, by the Sherman-Morrison formula:
+            // dx = y + k z (e . y) / sum(z), z_i = 1 / (1 + k e_i), y_i = -F_i z_i
+            // (1 - (k / 3) e . z = sum(z) / 3 exactly, so the denominator takes no cancellation)
+            double z[3], y[3];
             for (int i = 0; i < 3; i++) {
-                F[i] = (x[i] - m0[i]) + k * (e[i] - mean);
-                for (int j = 0; j < 3; j++) J[i][j] = (i == j ? 1.0 + k * e[i] : 0.0) - k * e[j] / 3.0;
+                const double F = (x[i] - m0[i]) + k * (e[i] - mean);
+                z[i] = 1.0 / (1.0 + k * e[i]);
+                y[i] = -F * z[i];
             }
-            const double det = det3x3(J);
+            const double g = k * (((e[0] * y[0]) + (e[1] * y[1]) + (e[2] * y[2])) / ((z[0] + z[1]) + z[2]));
             double dx[3], big = 0.0;
-            for (int c = 0; c < 3; c++) {  // J dx = -F by Cramer's rule
-                double M[3][3];
-                for (int i = 0; i < 3; i++)
-                    for (int j = 0; j < 3; j++) M[i][j] = j == c ? -F[i] : J[i][j];
-                dx[c] = det3x3(M) / det;
+            for (int c = 0; c < 3; c++) {
+                dx[c] = y[c] + z[c] * g;
                 big = fmax(big, fabs(dx[c]));
             }
             const double damp = big > 0.5 ? 0.5 / big : 1.0;
             for (int i = 0; i < 3; i++) x[i] += damp * dx[i];
-            if (big < 1e-15) break;
+            if (big < 1e-8) break;
         }
         for (int i = 0; i < 3; i++) mu[i] = x[i];
     }
@@ -126,17 +131,17 @@ __device__ inline void hpr_relax_cell(double* U, double h, const typename M::P& 
     if (!q.thermal) return;
     const typename M::M3 An = M::load(U + 2);
     const double E = U[1] / rho, u = U[11] / rho, v = U[12] / rho, w = U[13] / rho;
-    const double p0 = M::pressure_of(rho, E, u, v, w, An, U[14] / rho, U[15] / rho, U[16] / rho, q);
-    const double k0 = (q.rho0 * M::mg_temperature(rho, p0, q)) / (q.tau2 * q.T0 * rho);
-    const int nJ = clamp_steps(k0 * h, 1, 32);
-    const double hs = h / nJ;
-    for (int s = 0; s < nJ; s++) {
-        const double p = M::pressure_of(rho, E, u, v, w, An, U[14] / rho, U[15] / rho, U[16] / rho, q);
-        const double T = M::mg_temperature(rho, p, q);
-        const double k = T > 0.0 ? (q.rho0 * T) / (q.tau2 * q.T0 * rho) : 0.0;
-        const double fac = exp(-k * hs);
-        for (int i = 14; i < 17; i++) U[i] *= fac;
-    }
+    const double jx = U[14] / rho, jy = U[15] / rho, jz = U[16] / rho;
+    const double s0 = ((jx * jx) + (jy * jy)) + (jz * jz);
+    const double T = M::mg_temperature(rho, M::pressure_of(rho, E, u, v, w, An, jx, jy, jz, q), q);
+    if (!(s0 > 0.0) || !(T > 0.0)) return;
+    const double beta = (0.5 * (q.alpha * q.alpha)) / q.cv;
+    const double TJ0 = T + (beta * s0);  // the temperature at J = 0
+    const double kappa = q.rho0 / (q.tau2 * q.T0 * rho);
+    const double Eh = exp(-2.0 * (kappa * (TJ0 * h)));
+    const double r = (beta * s0) / TJ0;
+    const double fac = sqrt(Eh / ((1.0 - r) + (r * Eh)));
+    for (int i = 14; i < 17; i++) U[i] *= fac;
 }
 
 // One relaxation of length h = dt * a.dt_scale of every cell, in place on a.out (a.in == a.out allowed).
