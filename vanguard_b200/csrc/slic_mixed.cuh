@@ -307,7 +307,8 @@ __global__ void __launch_bounds__(TX, MINB) sweep_y_mixed_kernel(SweepArgs a) {
     };
 
     using R = typename M::R;
-    double um1[NU], u0[NU], up1[NU], f_prev[NU], wnext[NW];
+    double um1[NU], u0[NU], up1[NU], wnext[NW];
+    float f_prev[NU];  // FP32 interface flux, widened exactly at its use
     R ua_prev[NU], dummy[NU];
     double wave = 0.0;
     load(r0 - 2, wnext);
@@ -328,7 +329,7 @@ __global__ void __launch_bounds__(TX, MINB) sweep_y_mixed_kernel(SweepArgs a) {
         if (r > r0 && col_ok) {
             double Un[NU], W[NW];
 #pragma unroll
-            for (int v = 0; v < NU; v++) Un[v] = fma(k.r, f_prev[v] - (double)F[v], um1[v]);
+            for (int v = 0; v < NU; v++) Un[v] = fma(k.r, (double)f_prev[v] - (double)F[v], um1[v]);
             keep_fields<M>(a, (long)(r - 1) * a.pitch + c, q, W);
             M::setcons(Un, q, W);
 #pragma unroll
@@ -341,7 +342,7 @@ __global__ void __launch_bounds__(TX, MINB) sweep_y_mixed_kernel(SweepArgs a) {
         }
 #pragma unroll
         for (int v = 0; v < NU; v++) {
-            f_prev[v] = (double)F[v];
+            f_prev[v] = F[v];
             ua_prev[v] = ua_next[v];
             um1[v] = u0[v];
             u0[v] = up1[v];
