@@ -146,7 +146,7 @@ __device__ inline void hpr_relax_cell(double* U, double h, const typename M::P& 
 
 // One relaxation of length h = dt * a.dt_scale of every cell, in place on a.out (a.in == a.out allowed).
 template <class M>
-__global__ void __launch_bounds__(128) relax_kernel(SweepArgs a) {
+__global__ void __launch_bounds__(128, 4) relax_kernel(SweepArgs a) {
     constexpr int NU = M::NU, NW = M::NW;
     const long n = (long)a.nx * a.ny;
     const long idx = blockIdx.x * 128L + threadIdx.x;
