@@ -729,6 +729,37 @@ vg_status vg_run(vg_solver* s, const vg_run_config* cfg, int* steps_taken, doubl
     cudaStream_t st = (cudaStream_t)stream;
     VG_CUDA(cudaSetDevice(s->d.device));
 
+    // A plain second-order run of a small 1D row runs in one launch (solve1d_kernels.cuh): the whole loop on the
+    // chip, in a cluster of blocks that share the row through distributed shared memory
+    const bool plain = cfg->order != 1 && !(cfg->stiff_source && s->ops->relax) && !(cfg->subcycles > 0 && s->ops->forcing) &&
+                       !(cfg->reinit_frequency > 0 && s->ops->reinit);
+    if (plain && s->ops->solve1d && s->dims == 1 && s->d.nx >= s->ops->solve1d_min && s->d.nx <= s->ops->solve1d_max) {
+        Ctrl* h = s->hctrl;
+        std::memset(h, 0, sizeof(Ctrl));
+        h->t_end = cfg->t_end > 0.0 ? cfg->t_end : 1.0e300;
+        h->cfl = cfg->cfl;
+        h->dx = cfg->dx;
+        h->max_steps = cfg->max_steps > 0 ? cfg->max_steps : INT_MAX;
+        h->active = 1;
+        h->dims = 1;
+        VG_CUDA(cudaMemcpyAsync(s->ctrl, h, sizeof(Ctrl), cudaMemcpyHostToDevice, st));
+        SweepArgs a = base_args(s);
+        a.in = a.out = s->buf[s->cur];
+        a.dx = cfg->dx;
+        a.bias = cfg->bias;
+        a.limiter = cfg->limiter;
+        VG_CUDA(s->ops->solve1d(a, st));
+        VG_CUDA(cudaMemcpyAsync(h, s->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
+        VG_CUDA(cudaStreamSynchronize(st));
+        s->last_launches = 1;
+        if (steps_taken) *steps_taken = h->it;
+        if (t_reached) *t_reached = h->t;
+        if (h->err) return fail(VG_ENAN, "non-finite value, non-positive density or pressure at or below -p_inf produced");
+        if (h->t < h->t_end && h->it < h->max_steps)
+            return fail(VG_EINVAL, "the time step stopped advancing: the one-launch 1D loop ended at its step cap");
+        return VG_OK;
+    }
+
     // Normalise so that the state starts in buffer 0 (graphs are captured from buffer 0).
     if (s->cur != 0) {
         VG_CUDA(cudaMemcpyAsync(s->buf[0], s->buf[1], sizeof(double) * s->plane * s->ops->nw, cudaMemcpyDeviceToDevice, st));

@@ -53,6 +53,10 @@ struct Ops {
     int tma_planes = 0;
     // Volume-fraction reinitialisation of one step, in place on a.out (Euler reduced model), null for the others.
     SweepFn reinit = nullptr;
+    // The whole second-order 1D run in one thread block, in place on a.in == a.out (solve1d_kernels.cuh), for rows of
+    // solve1d_min .. solve1d_max cells; null where the model has none (models with a source or a per-step c_h).
+    SweepFn solve1d = nullptr;
+    long solve1d_min = 0, solve1d_max = 0;
 };
 
 constexpr int kForcingLaunches = 2;  // kernels per forcing sub-cycle
