@@ -168,7 +168,9 @@ vg_status vg_download_primitive(vg_solver* s, double* planes, int is_device, voi
  * and its MHD/HPR counterparts, on the uploaded state, entirely on the device: CFL maximum, dt schedule
  * (x0.2 for the first six steps, clamp to t_end; Solvers/solvers.cpp:437-452), X(dt/2) Y(dt) X(dt/2)
  * sweeps in 2D, one sweep in 1D.  The loop is replayed from captured CUDA graphs; dt never returns to
- * the host.  steps_taken / t_reached may be NULL. */
+ * the host.  A plain second-order exact-FP64 Euler run of a 1D row of 16 .. 2032 cells runs instead as one kernel
+ * launch (the whole loop inside one thread-block cluster), with the same results; a run there that stops advancing
+ * ends after 2^22 steps with VG_EINVAL.  steps_taken / t_reached may be NULL. */
 vg_status vg_run(vg_solver* s, const vg_run_config* cfg, int* steps_taken, double* t_reached, void* stream);
 
 /* Host-buffer convenience: upload, vg_run, download (the reference's solve(): copy in, return by value). */
