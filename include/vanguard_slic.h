@@ -203,8 +203,10 @@ long vg_last_launch_count(vg_solver* s);
 /* Launch configurations of the sweeps.  No counterpart in the reference (its sweeps are OpenMP loops).
  * Each model and precision is compiled for VG_NUM_XCFG X-sweep tile shapes (cells per segment, segments
  * per block, register cap) and VG_NUM_YCFG Y-sweep tile shapes (columns per block, rows marched per
- * thread, register cap).  The tile shape never changes a cell's arithmetic, so every configuration gives
- * identical results.
+ * thread, register cap).  Each Y shape runs either with its own rows per thread or with row segments sized so
+ * that its blocks fill whole waves of the device's resident slots; the tuner times both and keeps the faster
+ * (a Y configuration's reported time is the better of the two).  The tile shape never changes a cell's
+ * arithmetic, so every configuration gives identical results.
  * vg_autotune times every candidate on the uploaded state (`reps` launches each, CUDA events on `stream`),
  * keeps the fastest per axis and caches it (with the schedule below) by (variant, precision, boundary, nx,
  * ny, SM count) in

@@ -27,6 +27,12 @@ struct Fp64Kernels {
         sweep_x_kernel<M, P, LPB, MINB><<<grid, nt, 0, st>>>(a);
     }
     template <class M, int TX, int TY, int MINB>
+    static int y_resident() {
+        int b = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, sweep_y_kernel<M, TX, TY, MINB>, TX, 0);
+        return b;
+    }
+    template <class M, int TX, int TY, int MINB>
     static void y(dim3 grid, int nt, cudaStream_t st, const SweepArgs& a) {
         sweep_y_kernel<M, TX, TY, MINB><<<grid, nt, 0, st>>>(a);
     }

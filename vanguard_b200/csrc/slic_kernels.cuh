@@ -294,8 +294,9 @@ __global__ void __launch_bounds__(TX, MINB) sweep_y_kernel(SweepArgs a) {
     const int col = blockIdx.x * TX + threadIdx.x;
     const bool col_ok = col < a.nx;
     const int len = a.ny;
-    const int r0 = blockIdx.y * TY;
-    const int r1 = min(r0 + TY, len);
+    const int ty = a.ty_rows > 0 ? a.ty_rows : TY;
+    const int r0 = blockIdx.y * ty;
+    const int r1 = min(r0 + ty, len);
     const int c = col_ok ? col : 0;
 
     if (a.ctrl && !a.ctrl->active) {

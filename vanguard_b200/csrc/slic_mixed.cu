@@ -38,6 +38,12 @@ struct MixedKernels {
         sweep_x_tma_kernel<M, P, MINB><<<grid, P, 0, st>>>(a);
     }
     template <class M, int TX, int TY, int MINB>
+    static int y_resident() {
+        int b = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, sweep_y_mixed_kernel<M, TX, TY, MINB>, TX, 0);
+        return b;
+    }
+    template <class M, int TX, int TY, int MINB>
     static void y(dim3 grid, int nt, cudaStream_t st, const SweepArgs& a) {
         sweep_y_mixed_kernel<M, TX, TY, MINB><<<grid, nt, 0, st>>>(a);
     }

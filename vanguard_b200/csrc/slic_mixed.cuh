@@ -123,19 +123,19 @@ struct roundtrip_evolved<M, decltype((void)M::ROUNDTRIP_EVOLVED)> {
     static constexpr bool value = M::ROUNDTRIP_EVOLVED;
 };
 
-// Both evolved edge states of one cell (type M::R), from the FP64 conserved vectors of the cell and its
-// neighbours; the slope differences are formed in FP64.  ua_left_side: x_L + dt/2 evolution; ua_right_side:
-// x_R + dt/2 evolution.
+// Both evolved edge states of one cell (type M::R), from the cell's FP64 conserved vector u and its slope
+// differences dm = u - uL and dp = uR - u, formed in FP64 and rounded to R.  ua_left_side: x_L + dt/2 evolution;
+// ua_right_side: x_R + dt/2 evolution.
 template <class M, int AXIS>
-__device__ __forceinline__ void evolve_edges_mixed(const double* uL, const double* u, const double* uR,
-                                                   const MixedConst& k, const typename M::P& q,
-                                                   typename M::R* ua_left_side, typename M::R* ua_right_side) {
+__device__ __forceinline__ void evolve_edges_mixed_d(const typename M::R* dm, const typename M::R* dp, const double* u,
+                                                     const MixedConst& k, const typename M::P& q,
+                                                     typename M::R* ua_left_side, typename M::R* ua_right_side) {
     using R = typename M::R;
     constexpr int NU = M::NU;
     R xl[NU], xr[NU];
 #pragma unroll
     for (int i = 0; i < NU; i++) {
-        R hs = half_slope_mixed((R)(u[i] - uL[i]), (R)(uR[i] - u[i]), k);
+        R hs = half_slope_mixed(dm[i], dp[i], k);
         R uc = (R)u[i];
         xl[i] = uc - hs;
         xr[i] = uc + hs;
@@ -158,6 +158,21 @@ __device__ __forceinline__ void evolve_edges_mixed(const double* uL, const doubl
         M::setcons(ua_right_side, q, w);
         M::cons(w, q, ua_right_side);
     }
+}
+
+// evolve_edges_mixed_d from the FP64 conserved vectors of the cell and its neighbours.
+template <class M, int AXIS>
+__device__ __forceinline__ void evolve_edges_mixed(const double* uL, const double* u, const double* uR,
+                                                   const MixedConst& k, const typename M::P& q,
+                                                   typename M::R* ua_left_side, typename M::R* ua_right_side) {
+    using R = typename M::R;
+    R dm[M::NU], dp[M::NU];
+#pragma unroll
+    for (int i = 0; i < M::NU; i++) {
+        dm[i] = (R)(u[i] - uL[i]);
+        dp[i] = (R)(uR[i] - u[i]);
+    }
+    evolve_edges_mixed_d<M, AXIS>(dm, dp, u, k, q, ua_left_side, ua_right_side);
 }
 
 // FORCE flux of the evolved states ua (left) and ub (right), FP32 result.
@@ -286,8 +301,9 @@ __global__ void __launch_bounds__(TX, MINB) sweep_y_mixed_kernel(SweepArgs a) {
     const int col = blockIdx.x * TX + threadIdx.x;
     const bool col_ok = col < a.nx;
     const int len = a.ny;
-    const int r0 = blockIdx.y * TY;
-    const int r1 = min(r0 + TY, len);
+    const int ty = a.ty_rows > 0 ? a.ty_rows : TY;
+    const int r0 = blockIdx.y * ty;
+    const int r1 = min(r0 + ty, len);
     const int c = col_ok ? col : 0;
 
     if (a.ctrl && !a.ctrl->active) {
@@ -318,12 +334,23 @@ __global__ void __launch_bounds__(TX, MINB) sweep_y_mixed_kernel(SweepArgs a) {
     load(r0, wnext);
     M::cons(wnext, q, u0);
     load(r0 + 1, wnext);  // prefetched one row ahead of its use
-    evolve_edges_mixed<M, 1>(up1, um1, u0, k, q, dummy, ua_prev);
+    // slope differences: the lower one of a row is the upper one of the row before, carried down the march
+    R dlo[NU], dhi[NU];
+#pragma unroll
+    for (int v = 0; v < NU; v++) {
+        dlo[v] = (R)(um1[v] - up1[v]);  // up1 holds row r0 - 2 here
+        dhi[v] = (R)(u0[v] - um1[v]);
+    }
+    evolve_edges_mixed_d<M, 1>(dlo, dhi, um1, k, q, dummy, ua_prev);
+#pragma unroll
+    for (int v = 0; v < NU; v++) dlo[v] = dhi[v];
     for (int r = r0; r <= r1; r++) {
         M::cons(wnext, q, up1);
         if (r < r1) load(r + 2, wnext);
+#pragma unroll
+        for (int v = 0; v < NU; v++) dhi[v] = (R)(up1[v] - u0[v]);
         R ub[NU], ua_next[NU];
-        evolve_edges_mixed<M, 1>(um1, u0, up1, k, q, ub, ua_next);
+        evolve_edges_mixed_d<M, 1>(dlo, dhi, u0, k, q, ub, ua_next);
         float F[NU];
         force_flux_mixed<M, 1>(ua_prev, ub, k, q, F);
         if (r > r0 && col_ok) {
@@ -346,6 +373,7 @@ __global__ void __launch_bounds__(TX, MINB) sweep_y_mixed_kernel(SweepArgs a) {
             ua_prev[v] = ua_next[v];
             um1[v] = u0[v];
             u0[v] = up1[v];
+            dlo[v] = dhi[v];
         }
     }
     if (a.accumulate_wave) block_max_to<TX>(wave, a.wave_acc);

@@ -123,6 +123,7 @@ struct vg_solver {
     long last_launches = 0;
     int xcfg = 0, ycfg = 0;   // launch configuration of each sweep (sweep_table.cuh)
     int cfl_sep = 0;          // schedule: 0 folds the next step's CFL maximum into the last sweep, 1 a separate pass
+    int yseg = 0;             // Y segments: 0 the shape's TY, 1 sized for whole waves (sweep_table.cuh)
     // TMA tensor maps over buf[0] and buf[1] for the TMA-staged X sweep (device memory; null: none)
     CUtensorMap* d_tmaps = nullptr;
     int tmap_planes = 0;
@@ -154,6 +155,7 @@ const void* tmap_for(const vg_solver* s, const double* in) {
 cudaError_t run_sweep(const vg_solver* s, int axis, const SweepArgs& a0, cudaStream_t st) {
     SweepArgs a = prepared(a0);
     a.tmap = axis == 0 ? tmap_for(s, a.in) : nullptr;
+    a.y_waves = s->yseg;
     return axis == 0 ? s->ops->x[s->xcfg](a, st) : s->ops->y[s->ycfg](a, st);
 }
 
@@ -192,7 +194,7 @@ void build_tmaps(vg_solver* s, int planes) {
 // optionally persisted in the text file named by VG_TUNE_CACHE ("key xcfg ycfg" per line).
 struct TuneEntry {
     std::string key;
-    int xcfg, ycfg, sched;
+    int xcfg, ycfg, sched, yseg;
 };
 std::vector<TuneEntry> g_tune_cache;
 bool g_tune_loaded = false;
@@ -215,28 +217,31 @@ void tune_cache_load() {
     if (!f) return;
     char line[256], key[160];
     while (std::fgets(line, sizeof(line), f)) {
-        int x, y, sc = 0;
-        const int got = std::sscanf(line, "%159s %d %d %d", key, &x, &y, &sc);  // lines without a schedule: fused
-        if (got >= 3 && x >= 0 && x < vg::kNumXCfg && y >= 0 && y < vg::kNumYCfg && (sc == 0 || sc == 1))
-            g_tune_cache.push_back({key, x, y, sc});
+        int x, y, sc = 0, ys = 0;
+        // lines without a schedule: fused; without a Y segment mode: the shape's TY
+        const int got = std::sscanf(line, "%159s %d %d %d %d", key, &x, &y, &sc, &ys);
+        if (got >= 3 && x >= 0 && x < vg::kNumXCfg && y >= 0 && y < vg::kNumYCfg && (sc == 0 || sc == 1) &&
+            (ys == 0 || ys == 1))
+            g_tune_cache.push_back({key, x, y, sc, ys});
     }
     std::fclose(f);
 }
 
-void tune_cache_store(const std::string& key, int x, int y, int sched) {
+void tune_cache_store(const std::string& key, int x, int y, int sched, int yseg) {
     for (auto& e : g_tune_cache)
         if (e.key == key) {
             e.xcfg = x;
             e.ycfg = y;
             e.sched = sched;
+            e.yseg = yseg;
             return;
         }
-    g_tune_cache.push_back({key, x, y, sched});
+    g_tune_cache.push_back({key, x, y, sched, yseg});
     const char* path = std::getenv("VG_TUNE_CACHE");
     if (!path) return;
     FILE* f = std::fopen(path, "a");
     if (!f) return;
-    std::fprintf(f, "%s %d %d %d\n", key.c_str(), x, y, sched);
+    std::fprintf(f, "%s %d %d %d %d\n", key.c_str(), x, y, sched, yseg);
     std::fclose(f);
 }
 
@@ -407,6 +412,11 @@ bool same_cfg(const vg_run_config& a, const vg_run_config& b) {
 vg_status ensure_graphs(vg_solver* s, const vg_run_config& c) {
     if (s->g.valid && s->g.variant == s->variant && same_cfg(s->g.cfg, c)) return VG_OK;
     destroy_graphs(s);
+    // the Y launchers look their occupancy up on first use: let them do it outside the capture
+    if (s->dims == 2) {
+        SweepArgs probe{};
+        for (int i = 0; i < vg::kNumYCfg; i++) VG_CUDA(s->ops->y[i](probe, s->cap));
+    }
     vg_status st;
     if ((st = capture(s, c, kChunk, 0, &s->g.chunk)) != VG_OK) return st;
     if ((st = capture(s, c, 1, 0, &s->g.single[0])) != VG_OK) return st;
@@ -901,6 +911,10 @@ vg_status vg_autotune(vg_solver* s, const vg_run_config* cfg, int reps, float* t
         for (auto& e : g_tune_cache)
             if (e.key == key) {
                 vg_status vs = vg_set_launch_config(s, e.xcfg, e.ycfg);
+                if (vs == VG_OK && s->yseg != e.yseg) {
+                    destroy_graphs(s);
+                    s->yseg = e.yseg;
+                }
                 return vs != VG_OK ? vs : vg_set_schedule(s, e.sched);
             }
     }
@@ -924,12 +938,15 @@ vg_status vg_autotune(vg_solver* s, const vg_run_config* cfg, int reps, float* t
     VG_CUDA(cudaEventCreate(&e0));
     VG_CUDA(cudaEventCreate(&e1));
     float best[2] = {1e30f, 1e30f};
-    int pick[2] = {0, 0};
+    int pick[2] = {0, 0}, pick_yseg = 0;
     for (int axis = 0; axis < s->dims; axis++) {
         int n = axis == 0 ? vg::kNumXCfg : vg::kNumYCfg;
-        for (int c = 0; c < n; c++) {
-            const vg::SweepFn fn = axis == 0 ? s->ops->x[c] : s->ops->y[c];
+        // each Y shape is timed with its own segment length and with segments sized for whole waves
+        for (int c = 0; c < n * (axis == 0 ? 1 : 2); c++) {
+            const int shape = c % n;
+            const vg::SweepFn fn = axis == 0 ? s->ops->x[shape] : s->ops->y[shape];
             a.tmap = axis == 0 ? tmap_for(s, a.in) : nullptr;
+            a.y_waves = axis == 1 && c >= n;
             cudaError_t e = fn(a, st);  // warm-up (module load, caches)
             if (e != cudaSuccess) {
                 cudaEventDestroy(e0);
@@ -943,13 +960,16 @@ vg_status vg_autotune(vg_solver* s, const vg_run_config* cfg, int reps, float* t
             float ms = 0.0f;
             VG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
             ms /= reps;
-            if (times_ms) times_ms[axis * vg::kNumXCfg + c] = ms;
+            float& slot_ms = times_ms ? times_ms[axis * vg::kNumXCfg + shape] : ms;
+            if (times_ms && (c < n || ms < slot_ms)) slot_ms = ms;  // a shape's time: the better of its two modes
             if (ms < best[axis]) {
                 best[axis] = ms;
-                pick[axis] = c;
+                pick[axis] = shape;
+                if (axis == 1) pick_yseg = c >= n;
             }
         }
     }
+    a.y_waves = 0;
     // Schedule: where the next step's CFL maximum is taken.  Folded into the last X sweep's epilogue it costs no
     // extra pass over the state but adds the wave speed's registers to the sweep; a separate reduction reads the
     // state once more.  Both give the same bits (the maximum of the same values); time the step's tail each way
@@ -988,8 +1008,12 @@ vg_status vg_autotune(vg_solver* s, const vg_run_config* cfg, int reps, float* t
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     VG_CUDA(cudaGetLastError());
-    tune_cache_store(key, pick[0], pick[1], sched);
+    tune_cache_store(key, pick[0], pick[1], sched, pick_yseg);
     vg_status vs2 = vg_set_launch_config(s, pick[0], pick[1]);
+    if (vs2 == VG_OK && s->yseg != pick_yseg) {
+        destroy_graphs(s);
+        s->yseg = pick_yseg;
+    }
     return vs2 != VG_OK ? vs2 : vg_set_schedule(s, sched);
 }
 

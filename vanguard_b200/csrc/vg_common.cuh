@@ -96,6 +96,8 @@ struct SweepArgs {
     // params[] changed the register allocation of the two-row X sweep (56 -> 60)
     const void* tmap;
     int reinit_freq;  // volume-fraction reinitialisation every reinit_freq steps (Euler reduced model; 0: none)
+    int ty_rows;      // rows marched per Y-sweep block (0: the shape's TY), set by launch_y
+    int y_waves;      // launch_y sizes the Y segments for whole waves of resident blocks (else the shape's TY)
 };
 
 // Sweep constants of one sweep of length ts = dt * scale, formed as the reference forms them
