@@ -5,6 +5,8 @@
 // the autotuner (vg_autotune in vg_api.cu) times them on the caller's grid and keeps the fastest.
 #pragma once
 
+#include <atomic>
+
 #include <cuda_runtime.h>
 
 #include "vg_common.cuh"
@@ -53,13 +55,15 @@ cudaError_t launch_y(const SweepArgs& a0, cudaStream_t st) {
     if constexpr (!M::HAS_Y) {
         return cudaErrorInvalidValue;
     } else {
-        static long slots = 0;  // resident blocks of this shape on the device
+        static std::atomic<long> cached{0};  // resident blocks of this shape on the device (every thread stores the same)
+        long slots = cached.load(std::memory_order_relaxed);
         if (slots == 0) {
             int dev = 0, sms = 0;
             cudaGetDevice(&dev);
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
             slots = (long)K::template y_resident<M, TX, TY, MINB>() * sms;
             if (slots <= 0) slots = -1;
+            cached.store(slots, std::memory_order_relaxed);
         }
         if (a0.nx <= 0) return cudaSuccess;  // a call that only looks the occupancy up (before a graph capture)
         SweepArgs a = a0;
