@@ -73,3 +73,31 @@ def test_runs_continue_where_they_stopped(gpu, oracle_lib):
         s.run(1e-3, 0.9, steps=60, limiter=O.MINBEE)
         out = s.download()
     _bitwise(out, ref)
+
+
+def _same_with_nan(a, b):
+    assert np.array_equal(np.isnan(a), np.isnan(b))
+    assert np.array_equal(np.nan_to_num(a, nan=0.0), np.nan_to_num(b, nan=0.0))
+
+
+@pytest.mark.parametrize("nx", [600, 2033])
+@pytest.mark.parametrize("poison", ["nan_density", "negative_pressure"])
+def test_poisoned_row_reports_enan(gpu, oracle_lib, nx, poison):
+    # the one-launch loop (600 cells) and the graph-driven one (2033) report VG_ENAN alike and leave the same state
+    W = wl.sod_1d(nx)
+    if poison == "nan_density":
+        W[0, 200] = np.nan
+    else:
+        W[4, 150:170] = -0.5
+    prm = wl.euler_params(1.4)
+    ref = W.copy()
+    O.run(O.EULER, ref, 1.0 / nx, 0.8, steps=4, limiter=O.MINBEE, params=prm)
+    with gpu.Solver(gpu.EULER, nx, 1, prm) as s:
+        s.upload(W)
+        with pytest.raises(gpu.VgError) as e:
+            s.run(1.0 / nx, 0.8, steps=4, limiter=O.MINBEE)
+        assert e.value.status == gpu.VG_ENAN
+        _same_with_nan(s.download(), ref)
+        s.upload(wl.sod_1d(nx))  # the handle stays usable
+        t, n = s.run(1.0 / nx, 0.8, steps=3, limiter=O.MINBEE)
+        assert n == 3
