@@ -67,7 +67,11 @@ __global__ void __launch_bounds__(P, MINB) sweep_x_tma_kernel(SweepArgs a) {
     constexpr int NU = M::NU, NW = M::NW, S = P + 2;
     static_assert(NU == NW, "conserved and primitive planes coincide for the PAIR_X models");
     static_assert((P - 2) % 2 == 0, "tile starts must be even cell indices (16-byte TMA x alignment of FP64)");
-    __shared__ __align__(128) double Ws[2][NW][2][S];  // TMA destination; converted in place to conserved
+    // Two staging buffers, each a TMA destination, so each must start on a 128-byte boundary: the per-buffer stride is
+    // rounded up to 16 doubles (without it the second buffer of a 3- or 7-plane state starts 16-byte aligned only, and
+    // a 7-plane copy into it faulted with a misaligned address).
+    constexpr int WST = ((NW * 2 * S + 15) / 16) * 16;
+    __shared__ __align__(128) double Wsm[2 * WST];  // TMA destinations; converted in place to conserved
     __shared__ float2 Es[NU][P];
     __shared__ float2 Fs[NU][P];  // interface fluxes; widened to FP64 where the update reads them
     __shared__ __align__(8) uint64_t bar[2];
@@ -103,7 +107,7 @@ __global__ void __launch_bounds__(P, MINB) sweep_x_tma_kernel(SweepArgs a) {
     if (p == 0 && (int)blockIdx.x < ntiles) {
         const int t = blockIdx.x;
         mbar_expect_tx(&bar[0], kBytes);
-        tma_load_3d(&Ws[0][0][0][0], a.tmap, &bar[0], (t % ntx) * (P - 2) - 2, 2 * (t / ntx), 0);
+        tma_load_3d(Wsm, a.tmap, &bar[0], (t % ntx) * (P - 2) - 2, 2 * (t / ntx), 0);
     }
 
     uint32_t phase = 0u;  // bit b: parity of the next completion of bar[b]
@@ -115,7 +119,7 @@ __global__ void __launch_bounds__(P, MINB) sweep_x_tma_kernel(SweepArgs a) {
         if (p == 0 && tn < ntiles) {  // the other buffer was released by the barrier that ended the previous tile
             fence_proxy_async_smem();
             mbar_expect_tx(&bar[buf ^ 1], kBytes);
-            tma_load_3d(&Ws[buf ^ 1][0][0][0], a.tmap, &bar[buf ^ 1], (tn % ntx) * (P - 2) - 2, 2 * (tn / ntx), 0);
+            tma_load_3d(Wsm + (buf ^ 1) * WST, a.tmap, &bar[buf ^ 1], (tn % ntx) * (P - 2) - 2, 2 * (tn / ntx), 0);
         }
         const bool arrived = mbar_wait_bounded(&bar[buf], (phase >> buf) & 1u);
         if (__syncthreads_or(!arrived)) {
@@ -132,7 +136,7 @@ __global__ void __launch_bounds__(P, MINB) sweep_x_tma_kernel(SweepArgs a) {
         const int s0 = tx * (P - 2);
         const int row0 = 2 * (t / ntx);
         const int cell = s0 - 1 + p;
-        double(*U)[2][S] = Ws[buf];
+        double(*U)[2][S] = reinterpret_cast<double(*)[2][S]>(Wsm + buf * WST);
 
         // cells outside [0, nx): the boundary's ghost values (the copy filled them with zeros)
         if (s0 - 2 < 0 || s0 - 2 + S > len) {
@@ -205,7 +209,7 @@ __global__ void __launch_bounds__(P, MINB) sweep_x_tma_kernel(SweepArgs a) {
                 }
             }
         }
-        __syncthreads();  // Ws[buf], Es and Fs are free for the next tile
+        __syncthreads();  // this tile's staging buffer, Es and Fs are free for the next tile
     }
     if (timed_out) return;
     if (a.accumulate_wave) block_max_to<P>(wave, a.wave_acc);
