@@ -379,7 +379,11 @@ def run_cuda(args, world, rank, local):
                      "traffic": traffic,
                      "kernel": ("sweep_x_kernel" if head == "fp64" else "sweep_x_pair_kernel") + " (X half-sweep, "
                                + r["tuned"]["x"] + ")",
-                     "algorithmic_bytes_per_launch": x_bytes, "peak_source": peak_kind},
+                     "algorithmic_bytes_per_launch": x_bytes, "peak_source": peak_kind,
+                     "note": ("the exact FP64 form is bound by the FP64 pipe (correctly rounded divisions and square "
+                              "roots, no contraction), not by HBM: ncu shows the FP64 pipe 61 % busy and DRAM 10 % "
+                              "(profiles/sweep_x_kernel_euler_fp64_2048.md); the mixed form's X sweep reaches 0.62 of "
+                              "HBM (forms.mixed.x_sweep_hbm_frac)") if head == "fp64" else ""},
         "e2e": {"value": job_value(world, cells * args.steps, e2e_s), "unit": UNIT,
                 "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                 "api": f"vg_solve ({head}; pinned host buffers; one upload + K steps + one download per call)"},
