@@ -102,12 +102,16 @@ __global__ void __cluster_dims__(S1D_CL, 1, 1) __launch_bounds__(S1D_NT) solve1d
     int it = a.ctrl->it, b = 0;
 
     for (;;) {
-        // step_begin_kernel, taken identically by every block: S from every block's partial maximum
-        double S = 0.0;
-        for (int r = 0; r < S1D_CL; r++) {
-            const double m = cluster.map_shared_rank(part, r)[b];
-            S = (m > S) ? m : S;
+        // step_begin_kernel, taken identically by every block: S from every block's partial maximum (never NaN), lane r
+        // of each warp reading block r's through distributed shared memory and the warp combining them
+        double m = 0.0;
+        if ((tid & 31) < S1D_CL) m = cluster.map_shared_rank(part, tid & 31)[b];
+#pragma unroll
+        for (int o = S1D_CL / 2; o > 0; o >>= 1) {
+            const double w = __shfl_xor_sync(0xffffffffu, m, o);
+            m = (w > m) ? w : m;
         }
+        const double S = __shfl_sync(0xffffffffu, m, 0);
         if (!((t < t_end) && (it < max_steps) && (it < S1D_STEP_CAP))) break;
         dt = cfl * (dx / S);
         if (it <= 5) dt *= 0.2;
